@@ -1,0 +1,128 @@
+/*
+ * petl_device.h -- device-resident entry points of libpetl.so (B200 build).
+ *
+ * These have no single counterpart in the reference: the reference C ABI
+ * (petl.h) copies host arrays to the GPU and back inside every call
+ * (src/projectors.cu:379-497, src/cuda_utils.cu:1146-1361).  The functions
+ * here take DEVICE pointers and a CUDA stream (passed as void*), keep no
+ * hidden state between calls except cached per-device scratch, and are what
+ * the reference-compatible entry points of petl.h call after staging host
+ * data.  Each one names the reference routine whose result it reproduces.
+ *
+ * Layouts: planogram float32 [N_v1][N_v0][N_u1][N_u0], volume float32
+ * [numZ][numY][numX], rebinned planogram [N_v0][N_u1][N_u0] (one v1 slice).
+ * Return value: 0 on success, nonzero on error; petl_last_error() gives the
+ * message for the calling thread.
+ */
+#ifndef PETL_B200_PETL_DEVICE_H
+#define PETL_B200_PETL_DEVICE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One planogram together with the volume it projects to.  Lengths are the
+ * HALF lengths the reference stores internally (src/planogram.h:41-51), psi
+ * in radians, start values are the coordinates of sample 0. */
+typedef struct petl_geom {
+    float psi, R, L, H, v_m0, v_m1;
+    int   N_v1, N_v0, N_u1, N_u0;
+    float T_v1, T_v0, T_u1, T_u0;
+    float v1_0, v0_0, u1_0, u0_0;
+    float cos_psi, sin_psi;
+    int   numX, numY, numZ;
+    float T_x, T_z;            /* voxelWidth (x and y), voxelHeight (z) */
+    float x_0, y_0, z_0;       /* coordinates of voxel (0,0,0) */
+} petl_geom;
+
+/* Backprojector semantics. */
+enum {
+    PETL_BP_REFERENCE = 0, /* the reference backprojector's visibility rules
+                              (src/projectors.cu:240-377) with exact weights */
+    PETL_BP_ADJOINT   = 1  /* the exact transpose of petl_project_dev */
+};
+
+const char* petl_last_error(void);
+int petl_version(void);
+
+/* planogram::init (src/planogram.cpp:143-186) with the C-ABI conventions of
+ * add_planogram (src/petl_c_interface.cpp:216-219): psi in degrees, D/L/H
+ * full lengths. */
+int petl_geom_init(petl_geom* G, float psi_deg, float D, float L, float H, float v_m0, float v_m1, float T);
+/* parameters::set_volume + x_0/y_0/z_0 (src/parameters.cpp:250-284). */
+int petl_geom_set_volume(petl_geom* G, int numX, int numY, int numZ, float voxelWidth, float voxelHeight,
+                         float offsetX, float offsetY, float offsetZ);
+/* optimalFFTsize (src/vector_ops.cpp:481-505). */
+int petl_optimal_fft_size(int N);
+
+/* Forward SF projection (src/projectors.cu:11-238).  Computes the views
+ * iv0 = iv0_first + k*iv0_step (k = 0.., iv0 < N_v0) of every v1 slice and
+ * writes them into the full-size planogram g; other views are untouched.
+ * iv0_first = 0, iv0_step = 1 is the whole planogram. */
+int petl_project_dev(const petl_geom* G, const float* f, float* g, int iv0_first, int iv0_step, void* stream);
+
+/* Backprojection (src/projectors.cu:240-377, summed over v1 as
+ * backproject_SF does).  Only views iv0 = iv0_first + k*iv0_step contribute.
+ * f = accumulate ? f + scale*P^T g : scale*P^T g. */
+int petl_backproject_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
+                         int iv0_first, int iv0_step, void* stream);
+
+/* nnz of the forward operator: the number of (ray, voxel) pairs with a
+ * nonzero footprint weight, counted on the device; *nnz_host receives it
+ * (synchronizes the stream). */
+int petl_project_nnz_dev(const petl_geom* G, double* nnz_host, void* stream);
+
+/* PFDR rebinning (src/pfdr.cu:159-315): g [N_v1][N_v0][N_u1][N_u0] ->
+ * g_reb [N_v0][N_u1][N_u0]. */
+int petl_pfdr_dev(const petl_geom* G, const float* g, float* g_reb, void* stream);
+
+/* rampFilter1D (src/ramp_filter.cu:156-333) on every u0 row of a rebinned
+ * planogram, in place, followed (if apply_weight) by the inverse planogram
+ * weight sqrt(1+v1^2+v0^2) of apply_planogram_weight(true)
+ * (src/planogram.cpp:304-333) with v1 = v1_0 of G. */
+int petl_ramp_dev(const petl_geom* G, float* g_reb, int apply_weight, void* stream);
+
+/* FBP (PETL::doFBP, src/petl.cpp:310-355) of one planogram into f:
+ * f = accumulate ? f + fbp : fbp.  Needs N_v1 > 1 data (PFDR first) or an
+ * already rebinned planogram when G->N_v1 == 1. */
+int petl_fbp_dev(const petl_geom* G, const float* g, float* f, int accumulate, void* stream);
+
+/* --- regularizers, volume [N1][N2][N3] ------------------------------------ */
+/* aTV_RelativeDifferencesLoss_gradient (src/relative_differences.cu:481-532) */
+int petl_rd_gradient_dev(const float* f, float* Df, int N1, int N2, int N3, float delta, float beta, void* stream);
+/* Relative-difference penalty value, summed as the reference cost kernel does
+ * (each pair from both sides) with the neighbour index taken correctly; *out
+ * is a DEVICE double. */
+int petl_rd_cost_dev(const float* f, int N1, int N2, int N3, float delta, float beta, double* out, void* stream);
+/* anisotropicTotalVariation_gradient / _cost / _quadraticForm
+ * (src/total_variation.cu:588-811), p-Huber, 6 or 26 neighbours. cost and
+ * quadform write a DEVICE double. */
+int petl_tv_gradient_dev(const float* f, float* Df, int N1, int N2, int N3, float delta, float beta, float p,
+                         int numNeighbors, void* stream);
+int petl_tv_cost_dev(const float* f, int N1, int N2, int N3, float delta, float beta, float p, int numNeighbors,
+                     double* out, void* stream);
+int petl_tv_quadform_dev(const float* f, const float* d, int N1, int N2, int N3, float delta, float beta, float p,
+                         int numNeighbors, double* out, void* stream);
+
+/* --- elementwise / reductions (dataCube rules, src/data_cube.cpp:97-166) --- */
+/* denom = num/denom, 0 where denom == 0 (RDIV) */
+int petl_rdivide_dev(const float* num, float* denom, long long n, void* stream);
+/* x = x/y, 0 where y == 0 (DIV) */
+int petl_divide_dev(float* x, const float* y, long long n, void* stream);
+int petl_multiply_dev(float* x, const float* y, long long n, void* stream);
+/* x = (x == 0) ? v : 1/x */
+int petl_reciprocal_dev(float* x, long long n, float divide_by_zero_value, void* stream);
+/* *out (device double) = sum x*y*(w ? w : 1), FP64 accumulation */
+int petl_dot_dev(const float* x, const float* y, const float* w, long long n, double* out, void* stream);
+/* *out (device double) = sum over Pf>0 of g*log(Pf) - Pf (Poisson log-likelihood) */
+int petl_loglik_dev(const float* g, const float* Pf, long long n, double* out, void* stream);
+/* MLEM image update f *= d / sens with the DIV rule (d/0 -> 0) */
+int petl_mlem_update_dev(float* f, const float* d, const float* sens, long long n, void* stream);
+/* one-step-late RD update (src/petl_server.py:1597-1602):
+ * den = max(0.1*sens, sens + Df); f *= (den == 0 ? 0 : d/den) */
+int petl_osl_update_dev(float* f, const float* d, const float* sens, const float* Df, long long n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,752 @@
+// CPU oracle for the planogram reconstruction path -- TEST INFRASTRUCTURE ONLY.
+//
+// A restatement of the reference PETL algorithms in portable C++ (templated on
+// the arithmetic type, OpenMP over independent outputs).  It is the checker of
+// the CUDA library and the CPU baseline of the benchmark; the product never
+// links it.  Every routine cites the reference file:line it follows (paths are
+// relative to the reference project root).  Its agreement with the reference
+// itself is pinned by golden vectors produced from the reference library
+// (tests/golden).
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+#include <omp.h>
+
+namespace {
+
+const double kPI = 3.141592653589793;  // src/petl_defines.h
+
+template <class T> inline T tabs(T x) { return x < T(0) ? -x : x; }
+template <class T> inline T tmin(T a, T b) { return a < b ? a : b; }
+template <class T> inline T tmax(T a, T b) { return a > b ? a : b; }
+
+inline void set_threads(int n) {
+    if (n > 0) omp_set_num_threads(n);
+}
+
+// The forward projector's ray masks (src/projectors.cu:19-43) in float with
+// fused multiply-adds, as nvcc compiles them: v = fma(i, T, start),
+// |u| - T/2 > L + R|v0|  and  |u1| - T/2 > H - R|v1|.
+inline bool ray_visible(const oracle_geom& G, int iv1, int iv0, int iu1, int iu0)
+{
+    const float v1 = std::fma(float(iv1), G.T_v1, G.v1_0);
+    const float v0 = std::fma(float(iv0), G.T_v0, G.v0_0);
+    const float u1 = std::fma(float(iu1), G.T_u1, G.u1_0);
+    const float u0 = std::fma(float(iu0), G.T_u0, G.u0_0);
+    if (std::fabs(u0) - 0.5f * G.T_u0 > std::fma(G.R, std::fabs(v0), G.L)) return false;
+    if (std::fabs(u1) - 0.5f * G.T_u1 > std::fma(-G.R, std::fabs(v1), G.H)) return false;
+    return true;
+}
+
+// The reference backprojector's voxel visibility test (src/projectors.cu:289)
+// in float: u1 = fma(v1, t, z) with v1 = fma(iv1, T_v1, v1_0).
+inline bool voxel_visible(const oracle_geom& G, int iv1, float z, float t)
+{
+    const float v1 = std::fma(float(iv1), G.T_v1, G.v1_0);
+    const float u1 = std::fma(v1, t, z);
+    return std::fabs(u1) - 0.5f * G.T_u1 <= std::fma(-G.R, std::fabs(v1), G.H);
+}
+
+// ---------------------------------------------------------------------------
+// Forward projector: src/projectors.cu:11-238 (one ray per (iv1,iv0,iu1,iu0)).
+// Texture reads at voxel centres are exact; out-of-volume voxels are never
+// touched because the index ranges are clamped (lines 95-101, 150-156).
+// ---------------------------------------------------------------------------
+template <class T>
+T project_ray(const oracle_geom& G, const T* f, int iv1, int iv0, int iu1, int iu0, double* nnz)
+{
+    const T cos_psi = T(G.cos_psi), sin_psi = T(G.sin_psi);
+    const T R = T(G.R), L = T(G.L), H = T(G.H);
+    const T Tg_w = T(G.T_v1), Tg_x = T(G.T_v0), Tg_y = T(G.T_u1), Tg_z = T(G.T_u0);
+    const T sg_w = T(G.v1_0), sg_x = T(G.v0_0), sg_y = T(G.u1_0), sg_z = T(G.u0_0);
+    const T Tf_x = T(G.voxelWidth), Tf_y = T(G.voxelWidth), Tf_z = T(G.voxelHeight);
+    const T sf_x = T(G.x_0), sf_y = T(G.y_0), sf_z = T(G.z_0);
+    const int Nx = G.numX, Ny = G.numY, Nz = G.numZ;
+
+    const T v1 = T(iv1) * Tg_w + sg_w;
+    const T v0 = T(iv0) * Tg_x + sg_x;
+    const T u1 = T(iu1) * Tg_y + sg_y;
+    const T u0 = T(iu0) * Tg_z + sg_z;
+
+    // early exits, lines 30-43.  These are yes/no decisions that sit exactly
+    // on ties for some geometries, so they are taken in float the way the
+    // reference's compiled kernel takes them (a*b+c contracted into one fma).
+    (void)L; (void)H; (void)R;
+    if (!ray_visible(G, iv1, iv0, iu1, iu0)) return T(0);
+
+    const T iu0_min = T(iu0) - T(0.5), iu0_max = T(iu0) + T(0.5);
+    const T iu1_min = T(iu1) - T(0.5), iu1_max = T(iu1) + T(0.5);
+
+    const T p_x = u0 * cos_psi, p_y = u0 * sin_psi, p_z = u1;
+    const T r_x = -(v0 * cos_psi + sin_psi), r_y = -(v0 * sin_psi - cos_psi), r_z = -v1;
+
+    const T Tx_inv = T(1) / Tf_x, Ty_inv = T(1) / Tf_y, Tz_inv = T(1) / Tf_z;
+    const T Tu1_inv = T(1) / Tg_y, Tu0_inv = T(1) / Tg_z;
+    const T width_z = T(0.5) * Tg_y;
+    const T Tz_over_Tu1 = Tf_z * Tu1_inv;
+    const T z_fw = T(0.5) * Tf_z * Tu1_inv;
+
+    T val = T(0);
+    double count = 0.0;
+    const T* fz;
+    if (tabs(r_x) >= tabs(r_y)) {
+        // x-driven branch, lines 77-130
+        const T width_y = T(0.5) * Tg_z * tabs(sin_psi);
+        const T sin_psi_inv = T(1) / sin_psi;
+        const T rx_inv = T(1) / r_x;
+        const T l_phi = Tf_x * tabs(sin_psi_inv);
+        const T y_fw = T(0.5) * Tf_y * tabs(sin_psi_inv) * Tu0_inv;
+        for (int ix = 0; ix < Nx; ix++) {
+            const T x = T(ix) * Tf_x + sf_x;
+            const T t = (x - p_x) * rx_inv;
+            const T y_c = p_y + t * r_y, z_c = p_z + t * r_z;
+            const T y_A = y_c - width_y, y_B = y_c + width_y;
+            const int iy_min = std::max(0, int(std::ceil((y_A - T(0.5) * Tf_y - sf_y) * Ty_inv)));
+            const int iy_max = std::min(Ny - 1, int(std::floor((y_B + T(0.5) * Tf_y - sf_y) * Ty_inv)));
+            const T z_A = z_c - width_z, z_B = z_c + width_z;
+            const int iz_min = std::max(0, int(std::ceil((z_A - T(0.5) * Tf_z - sf_z) * Tz_inv)));
+            const int iz_max = std::min(Nz - 1, int(std::floor((z_B + T(0.5) * Tf_z - sf_z) * Tz_inv)));
+            T y = T(iy_min) * Tf_y + sf_y - t * r_y;
+            const T z_start = (T(iz_min) * Tf_z + sf_z - t * r_z - sg_y) * Tu1_inv;
+            for (int iy = iy_min; iy <= iy_max; iy++) {
+                const T c = (y * sin_psi_inv - sg_z) * Tu0_inv;
+                const T fp = tmin(iu0_max, c + y_fw) - tmax(iu0_min, c - y_fw);
+                if (fp > T(0)) {
+                    T z = z_start;
+                    for (int iz = iz_min; iz <= iz_max; iz++) {
+                        const T fz1 = tmax(T(0), tmin(iu1_max, z + z_fw) - tmax(iu1_min, z - z_fw));
+                        if (fz1 > T(0)) {
+                            if (f) val += f[(size_t(iz) * Ny + iy) * Nx + ix] * fp * fz1;
+                            count += 1.0;
+                        }
+                        z += Tz_over_Tu1;
+                    }
+                }
+                y += Tf_y;
+            }
+        }
+        val *= l_phi;
+    } else {
+        // y-driven branch, lines 131-185
+        const T width_x = T(0.5) * Tg_z * tabs(cos_psi);
+        const T cos_psi_inv = T(1) / cos_psi;
+        const T ry_inv = T(1) / r_y;
+        const T l_phi = Tf_x * tabs(cos_psi_inv);
+        const T x_fw = T(0.5) * Tf_x * tabs(cos_psi_inv) * Tu0_inv;
+        for (int iy = 0; iy < Ny; iy++) {
+            const T y = T(iy) * Tf_y + sf_y;
+            const T t = (y - p_y) * ry_inv;
+            const T x_c = p_x + t * r_x, z_c = p_z + t * r_z;
+            const T x_A = x_c - width_x, x_B = x_c + width_x;
+            const int ix_min = std::max(0, int(std::ceil((x_A - T(0.5) * Tf_x - sf_x) * Tx_inv)));
+            const int ix_max = std::min(Nx - 1, int(std::floor((x_B + T(0.5) * Tf_x - sf_x) * Tx_inv)));
+            const T z_A = z_c - width_z, z_B = z_c + width_z;
+            const int iz_min = std::max(0, int(std::ceil((z_A - T(0.5) * Tf_z - sf_z) * Tz_inv)));
+            const int iz_max = std::min(Nz - 1, int(std::floor((z_B + T(0.5) * Tf_z - sf_z) * Tz_inv)));
+            T x = T(ix_min) * Tf_x + sf_x - t * r_x;
+            const T z_start = (T(iz_min) * Tf_z + sf_z - t * r_z - sg_y) * Tu1_inv;
+            for (int ix = ix_min; ix <= ix_max; ix++) {
+                const T c = (x * cos_psi_inv - sg_z) * Tu0_inv;
+                const T fp = tmin(iu0_max, c + x_fw) - tmax(iu0_min, c - x_fw);
+                if (fp > T(0)) {
+                    T z = z_start;
+                    for (int iz = iz_min; iz <= iz_max; iz++) {
+                        const T fz1 = tmax(T(0), tmin(iu1_max, z + z_fw) - tmax(iu1_min, z - z_fw));
+                        if (fz1 > T(0)) {
+                            if (f) val += f[(size_t(iz) * Ny + iy) * Nx + ix] * fp * fz1;
+                            count += 1.0;
+                        }
+                        z += Tz_over_Tu1;
+                    }
+                }
+                x += Tf_x;
+            }
+        }
+        val *= l_phi;
+    }
+    (void)fz;
+    if (nnz) *nnz += count;
+    // line 237
+    return val * (T(1) / std::sqrt(T(1) + v0 * v0 + v1 * v1));
+}
+
+template <class T>
+void project(const oracle_geom& G, const T* f, T* g, int nthreads)
+{
+    set_threads(nthreads);
+    const long nview = long(G.N_v1) * G.N_v0;
+#pragma omp parallel for schedule(dynamic)
+    for (long v = 0; v < nview; v++) {
+        const int iv1 = int(v / G.N_v0), iv0 = int(v % G.N_v0);
+        T* gv = g + size_t(v) * G.N_u1 * G.N_u0;
+        for (int iu1 = 0; iu1 < G.N_u1; iu1++)
+            for (int iu0 = 0; iu0 < G.N_u0; iu0++)
+                gv[size_t(iu1) * G.N_u0 + iu0] = project_ray<T>(G, f, iv1, iv0, iu1, iu0, nullptr);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Backprojector: src/projectors.cu:240-377 and the per-v1 loop of
+// backproject_SF (src/projectors.cu:480-489): f = sum_v1 (val_v1 * T_x).
+// Each 2x2 texture fetch of the reference (line 368) is a bilinear read at
+// iu0 + w_b/(w_a+w_b) scaled by (w_a+w_b); with exact weights this is
+// w_a*g[iu0] + w_b*g[iu0+1], border texels read as zero.
+// ---------------------------------------------------------------------------
+template <class T>
+inline T gat(const T* g, const oracle_geom& G, int iv0, int iu1, int iu0)
+{
+    if (iu0 < 0 || iu0 >= G.N_u0 || iu1 < 0 || iu1 >= G.N_u1) return T(0);
+    return g[(size_t(iv0) * G.N_u1 + iu1) * G.N_u0 + iu0];
+}
+
+// one axis of the hardware linear filter: x is the texel-space coordinate as
+// the reference passes it (index + shift + 0.5), returns base index and weight
+inline void texaxis(float x, int mode, int& i, double& a)
+{
+    const float xb = x - 0.5f;
+    const float fl = std::floor(xb);
+    i = int(fl);
+    double frac = double(xb - fl);
+    if (mode == 1) frac = std::nearbyint(frac * 256.0) / 256.0;
+    else if (mode == 2) frac = std::floor(frac * 256.0) / 256.0;
+    a = frac;
+}
+
+template <class T>
+void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthreads)
+{
+    set_threads(nthreads);
+    const T cos_psi = T(G.cos_psi), sin_psi = T(G.sin_psi);
+    const T R = T(G.R), H = T(G.H);
+    const T Tg_w = T(G.T_v1), Tg_x = T(G.T_v0), Tg_y = T(G.T_u1), Tg_z = T(G.T_u0);
+    const T sg_w = T(G.v1_0), sg_x = T(G.v0_0), sg_y = T(G.u1_0), sg_z = T(G.u0_0);
+    const T Tf_x = T(G.voxelWidth), Tf_y = T(G.voxelWidth), Tf_z = T(G.voxelHeight);
+    const T sf_x = T(G.x_0), sf_y = T(G.y_0), sf_z = T(G.z_0);
+    const size_t plan_sz = size_t(G.N_v0) * G.N_u1 * G.N_u0;
+    const long nrows = long(G.numZ) * G.numY;
+#pragma omp parallel for schedule(dynamic)
+    for (long r = 0; r < nrows; r++) {
+        const int iz = int(r / G.numY), iy = int(r % G.numY);
+        for (int ix = 0; ix < G.numX; ix++) {
+            const T x = T(ix) * Tf_x + sf_x, y = T(iy) * Tf_y + sf_y, z = T(iz) * Tf_z + sf_z;
+            T acc = T(0);
+            for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
+                const T* gs = g + size_t(iv1) * plan_sz;
+                const T v1 = T(iv1) * Tg_w + sg_w;
+                const T t = y * cos_psi - x * sin_psi;
+                const T u1 = z + v1 * t;
+                T val = T(0);
+                const float xf = std::fma(float(ix), G.voxelWidth, G.x_0);
+                const float yf = std::fma(float(iy), G.voxelWidth, G.y_0);
+                const float zf = std::fma(float(iz), G.voxelHeight, G.z_0);
+                const float tf = std::fma(yf, G.cos_psi, -(xf * G.sin_psi));
+                (void)R; (void)H;
+                if (voxel_visible(G, iv1, zf, tf)) {
+                    const T x_dot_theta = x * cos_psi + y * sin_psi;
+                    const T Tu1_inv = T(1) / Tg_y, Tu0_inv = T(1) / Tg_z;
+                    const T iu1_mid = (u1 - sg_y) * Tu1_inv;
+                    const T iu1_A = iu1_mid - T(0.5) * Tf_z * Tu1_inv;
+                    const T iu1_B = iu1_mid + T(0.5) * Tf_z * Tu1_inv;
+                    const int iu1_min = int(std::ceil(iu1_A - T(0.5)));
+                    const int iu1_max = int(std::floor(iu1_B + T(0.5)));
+                    const T xdt_dy = T(0.5) * Tf_y * sin_psi, t_dy = T(0.5) * Tf_y * cos_psi;
+                    const T xdt_dx = T(0.5) * Tf_x * cos_psi, t_dx = -T(0.5) * Tf_x * sin_psi;
+                    for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+                        const T v0 = T(iv0) * Tg_x + sg_x;
+                        const T width_y = v0 * cos_psi + sin_psi;
+                        const T width_x = cos_psi - v0 * sin_psi;
+                        const T l_phi = T(1) / tmax(tabs(width_y), tabs(width_x)) *
+                                        (T(1) / std::sqrt(T(1) + v0 * v0 + v1 * v1));
+                        T A, B;
+                        if (tabs(width_y) > tabs(width_x)) {
+                            const T lo = (x_dot_theta - xdt_dy + v0 * (t - t_dy) - sg_z) * Tu0_inv;
+                            const T hi = (x_dot_theta + xdt_dy + v0 * (t + t_dy) - sg_z) * Tu0_inv;
+                            if (width_y >= T(0)) { A = lo; B = hi; } else { A = hi; B = lo; }
+                        } else {
+                            const T lo = (x_dot_theta - xdt_dx + v0 * (t - t_dx) - sg_z) * Tu0_inv;
+                            const T hi = (x_dot_theta + xdt_dx + v0 * (t + t_dx) - sg_z) * Tu0_inv;
+                            if (width_x >= T(0)) { A = lo; B = hi; } else { A = hi; B = lo; }
+                        }
+                        const int iu0_min = int(std::ceil(A - T(0.5)));
+                        const int iu0_max = int(std::floor(B + T(0.5)));
+                        for (int iu0 = iu0_min; iu0 <= iu0_max; iu0 += 2) {
+                            const T w0b = tmax(T(0), tmin(T(iu0 + 1) + T(0.5), B) - tmax(T(iu0 + 1) - T(0.5), A));
+                            const T w0a = tmax(T(0), tmin(T(iu0) + T(0.5), B) - tmax(T(iu0) - T(0.5), A));
+                            const T w0s = w0b + w0a;
+                            if (!(w0s > T(0))) continue;
+                            for (int iu1 = iu1_min; iu1 <= iu1_max; iu1 += 2) {
+                                const T w1b = tmax(T(0), tmin(T(iu1 + 1) + T(0.5), iu1_B) - tmax(T(iu1 + 1) - T(0.5), iu1_A));
+                                const T w1a = tmax(T(0), tmin(T(iu1) + T(0.5), iu1_B) - tmax(T(iu1) - T(0.5), iu1_A));
+                                const T w1s = w1b + w1a;
+                                if (!(w1s > T(0))) continue;
+                                T sample;
+                                if (texmode == 0) {
+                                    sample = (w0a * w1a * gat(gs, G, iv0, iu1, iu0) +
+                                              w0b * w1a * gat(gs, G, iv0, iu1, iu0 + 1) +
+                                              w0a * w1b * gat(gs, G, iv0, iu1 + 1, iu0) +
+                                              w0b * w1b * gat(gs, G, iv0, iu1 + 1, iu0 + 1));
+                                    sample *= l_phi;
+                                } else {
+                                    // coordinates exactly as the reference forms them (float)
+                                    const float s0 = float(w0b) / float(w0s), s1 = float(w1b) / float(w1s);
+                                    const float cx = float(iu0) + s0 + 0.5f, cy = float(iu1) + s1 + 0.5f;
+                                    int i0, i1; double a0, a1;
+                                    texaxis(cx, texmode, i0, a0);
+                                    texaxis(cy, texmode, i1, a1);
+                                    const double b = (1 - a0) * (1 - a1) * double(gat(gs, G, iv0, i1, i0)) +
+                                                     a0 * (1 - a1) * double(gat(gs, G, iv0, i1, i0 + 1)) +
+                                                     (1 - a0) * a1 * double(gat(gs, G, iv0, i1 + 1, i0)) +
+                                                     a0 * a1 * double(gat(gs, G, iv0, i1 + 1, i0 + 1));
+                                    sample = T(b) * l_phi * w0s * w1s;
+                                }
+                                val += sample;
+                            }
+                        }
+                    }
+                }
+                acc += val * Tf_x;
+            }
+            f[(size_t(iz) * G.numY + iy) * G.numX + ix] = acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FFT helpers.  A plain recursive mixed-radix DFT in double precision.
+// ---------------------------------------------------------------------------
+typedef std::complex<double> cd;
+
+void fft_rec(cd* x, int n, int sign, cd* scratch)
+{
+    if (n == 1) return;
+    int p = 2;
+    while (p * p <= n && n % p) p++;
+    if (n % p) p = n;
+    const int m = n / p;
+    for (int r = 0; r < p; r++)
+        for (int j = 0; j < m; j++) scratch[r * m + j] = x[j * p + r];
+    for (int r = 0; r < p; r++) fft_rec(scratch + r * m, m, sign, x);
+    std::vector<cd> out(n);
+    for (int k = 0; k < n; k++) {
+        cd s = 0;
+        const int kk = k % m;
+        for (int r = 0; r < p; r++) {
+            const double ang = sign * 2.0 * kPI * double((long long)r * k % n) / n;
+            s += scratch[r * m + kk] * cd(std::cos(ang), std::sin(ang));
+        }
+        out[k] = s;
+    }
+    for (int k = 0; k < n; k++) x[k] = out[k];
+}
+
+void fft(cd* x, int n, int sign)
+{
+    std::vector<cd> scratch(n);
+    fft_rec(x, n, sign, scratch.data());
+}
+
+// R2C of a real row of length n -> n/2+1 bins
+void r2c(const double* in, cd* out, int n)
+{
+    std::vector<cd> t(n);
+    for (int i = 0; i < n; i++) t[i] = in[i];
+    fft(t.data(), n, -1);
+    for (int k = 0; k <= n / 2; k++) out[k] = t[k];
+}
+
+// unnormalized C2R of n/2+1 bins -> n reals; the imaginary parts of bin 0 and
+// bin n/2 are ignored (the Hermitian completion of the half spectrum)
+void c2r(const cd* in, double* out, int n)
+{
+    std::vector<cd> t(n);
+    for (int k = 0; k <= n / 2; k++) t[k] = in[k];
+    t[0] = cd(in[0].real(), 0);
+    if (n % 2 == 0) t[n / 2] = cd(in[n / 2].real(), 0);
+    for (int k = n / 2 + 1; k < n; k++) t[k] = std::conj(in[n - k]);
+    fft(t.data(), n, +1);
+    for (int i = 0; i < n; i++) out[i] = t[i].real();
+}
+
+// ---------------------------------------------------------------------------
+// Regularizer helpers (src/relative_differences.cu:13-28,
+// src/total_variation.cu:33-78 with USE_P_HUBER).
+// ---------------------------------------------------------------------------
+inline double rd(double x, double y, double delta)
+{
+    if (x == y) return 0.0;
+    return (x - y) * (x - y) / ((x + y) + delta * std::fabs(x - y));
+}
+inline double drd(double x, double y, double delta)
+{
+    if (x == 0.0 && y == 0.0) return 0.0;
+    const double s = x + y + delta * std::fabs(x - y);
+    return (x - y) * (delta * std::fabs(x - y) + x + 3.0 * y) / (s * s);
+}
+
+struct Huber {
+    double p, delta, slope, shift;
+    Huber(double delta_, double p_) : p(p_), delta(delta_)
+    {
+        // setConstantMemoryParameters, src/total_variation.cu:574-586 (float constants)
+        slope = double(float(std::pow(delta, 2.0 - p) / p));
+        shift = double(float(delta * delta * (0.5 - 1.0 / p)));
+    }
+    double h(double x) const { return std::fabs(x) <= delta ? 0.5 * x * x : slope * std::pow(std::fabs(x), p) + shift; }
+    double dh(double x) const { return std::fabs(x) <= delta ? x : p * slope * std::pow(std::fabs(x), p) / x; }
+    double ddh(double x) const { return std::fabs(x) <= delta ? 1.0 : p * slope * std::pow(std::fabs(x), p - 2.0); }
+};
+
+// neighbourhood offsets of the 26-neighbour stencil grouped by distance
+struct Nbr { int di, dj, dk, cls; };
+std::vector<Nbr> neighbours(bool planar, int numNeighbors)
+{
+    std::vector<Nbr> v;
+    for (int di = -1; di <= 1; di++)
+        for (int dj = -1; dj <= 1; dj++)
+            for (int dk = -1; dk <= 1; dk++) {
+                if (!di && !dj && !dk) continue;
+                if (planar && di) continue;
+                const int cls = std::abs(di) + std::abs(dj) + std::abs(dk);
+                if (numNeighbors == 6 && cls > 1) continue;
+                if (planar && numNeighbors == 6 && cls > 1) continue;
+                v.push_back({di, dj, dk, cls});
+            }
+    return v;
+}
+inline double dist_w(int cls, double beta)
+{
+    return cls == 1 ? double(1.0f * float(beta))
+         : cls == 2 ? double(0.7071067811865475f * float(beta))
+                    : double(0.5773502691896258f * float(beta));
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_optimal_fft_size(int N)
+{
+    // src/vector_ops.cpp:481-505: smallest 2^(n+1)*3^m >= N
+    if (N <= 2) return 2;
+    const double c1 = std::log2(double(N) / 2.0) / std::log2(3);
+    const double c2 = 1.0 / std::log2(3);
+    const double xbar = std::log2(double(N) / 2.0);
+    int minValue = int(std::pow(2, int(std::ceil(xbar)) + 1));
+    for (int x = 0; x < int(std::ceil(xbar)); x++) {
+        const int y = int(std::ceil(c1 - c2 * double(x)));
+        const int v = int(std::pow(2, x + 1) * std::pow(3, y));
+        if (v < minValue && y >= 0) minValue = v;
+    }
+    return minValue;
+}
+
+int oracle_planogram_init(oracle_geom* G, float psi, float R, float L, float H, float v_m0, float v_m1, float T)
+{
+    // src/planogram.cpp:143-186 (float storage, mixed float/double arithmetic)
+    if (R <= 0.0 || L <= 0.0 || H <= 0.0 || v_m0 <= 0.0 || v_m1 < 0.0 || T <= 0.0) return 0;
+    G->psi = psi; G->R = R; G->L = L; G->H = H;
+    G->v_m0 = v_m0;
+    G->v_m1 = std::min(H / R, v_m1);
+    G->T_u0 = T; G->T_u1 = T;
+    G->T_v0 = G->T_u0 / R;
+    G->T_v1 = G->T_u1 / R;
+    G->N_u0 = 2 * int((L + R * v_m0) / G->T_u0);
+    G->N_u1 = 2 * int(H / G->T_u1);
+    G->N_v0 = 2 * int(v_m0 / G->T_v0) + 1;
+    G->N_v1 = 2 * int(G->v_m1 / G->T_v1) + 1;
+    G->T_v0 = float(v_m0 * 2.0 / float(G->N_v0));
+    G->u0_0 = float(-G->T_u0 * float(G->N_u0 - 1) / 2.0);
+    G->u1_0 = float(-G->T_u1 * float(G->N_u1 - 1) / 2.0);
+    G->v0_0 = float(-G->T_v0 * float(G->N_v0 - 1) / 2.0);
+    G->v1_0 = float(-G->T_v1 * float(G->N_v1 - 1) / 2.0);
+    G->cos_psi = float(std::cos(double(psi)));
+    G->sin_psi = float(std::sin(double(psi)));
+    return 1;
+}
+
+void oracle_set_volume(oracle_geom* G, int numX, int numY, int numZ, float voxelWidth, float voxelHeight,
+                       float offsetX, float offsetY, float offsetZ)
+{
+    // src/parameters.cpp:250-284
+    G->numX = numX; G->numY = numY; G->numZ = numZ;
+    G->voxelWidth = voxelWidth; G->voxelHeight = voxelHeight;
+    G->x_0 = float((0.0 - 0.5 * (numX - 1)) * voxelWidth + offsetX);
+    G->y_0 = float((0.0 - 0.5 * (numY - 1)) * voxelWidth + offsetY);
+    G->z_0 = float((0.0 - 0.5 * (numZ - 1)) * voxelHeight + offsetZ);
+}
+
+void oracle_project_f64(const oracle_geom* G, const double* f, double* g, int n) { project<double>(*G, f, g, n); }
+void oracle_project_f32(const oracle_geom* G, const float* f, float* g, int n) { project<float>(*G, f, g, n); }
+void oracle_backproject_f64(const oracle_geom* G, const double* g, double* f, int tm, int n) { backproject<double>(*G, g, f, tm, n); }
+void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int tm, int n) { backproject<float>(*G, g, f, tm, n); }
+
+double oracle_project_nnz(const oracle_geom* G, int nthreads)
+{
+    set_threads(nthreads);
+    const long nview = long(G->N_v1) * G->N_v0;
+    double total = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : total)
+    for (long v = 0; v < nview; v++) {
+        const int iv1 = int(v / G->N_v0), iv0 = int(v % G->N_v0);
+        double c = 0.0;
+        for (int iu1 = 0; iu1 < G->N_u1; iu1++)
+            for (int iu0 = 0; iu0 < G->N_u0; iu0++)
+                project_ray<double>(*G, (const double*)nullptr, iv1, iv0, iu1, iu0, &c);
+        total += c;
+    }
+    return total;
+}
+
+void oracle_fft_c2c(double* data, int n, int sign) { fft(reinterpret_cast<cd*>(data), n, sign); }
+
+void oracle_pfdr_f64(const oracle_geom* G, const double* g, double* g_reb, int nthreads)
+{
+    // src/pfdr.cu:159-315 with the kernels at 43-157.
+    set_threads(nthreads);
+    const int NX = oracle_optimal_fft_size(G->N_u0), NXH = NX / 2 + 1;
+    const int NY = oracle_optimal_fft_size(G->N_v0);
+    const int B = G->N_u1;
+    const float T_U = float(1.0 / (NX * G->T_u0));
+    const float T_V = float(1.0 / (NY * G->T_v0));
+    const float aperture = float(1 / (2.0 * G->T_u1 * 2.0 * G->v_m0));
+    (void)T_V;
+    std::vector<cd> Greb(size_t(B) * NY * NXH, cd(0, 0));
+    std::vector<double> W(size_t(B) * NY * NXH, 0.0);
+    const size_t plan_sz = size_t(G->N_v0) * G->N_u1 * G->N_u0;
+    for (int iv1 = 0; iv1 < G->N_v1; iv1++) {
+        const float v1 = float(iv1) * G->T_v1 + G->v1_0;  // planogram::v1
+        const double* gs = g + size_t(iv1) * plan_sz;
+#pragma omp parallel for schedule(dynamic)
+        for (int iu1 = 0; iu1 < B; iu1++) {
+            // copy_data_to_2d_fft_buffer, weighted by 1/sqrt(1+v1^2+v0^2)
+            std::vector<cd> buf(size_t(NY) * NX, cd(0, 0));
+            for (int iv0 = 0; iv0 < G->N_v0; iv0++) {
+                const double v0 = double(float(G->T_v0 * float(iv0) + G->v0_0));
+                const double w = 1.0 / std::sqrt(1.0 + double(v1) * v1 + v0 * v0);
+                for (int iu0 = 0; iu0 < G->N_u0; iu0++)
+                    buf[size_t(iv0) * NX + iu0] = gs[(size_t(iv0) * G->N_u1 + iu1) * G->N_u0 + iu0] * w;
+            }
+            // 2-D forward transform: rows (NX) then columns (NY)
+            for (int r = 0; r < NY; r++) fft(&buf[size_t(r) * NX], NX, -1);
+            std::vector<cd> col(NY);
+            for (int k = 0; k < NXH; k++) {
+                for (int r = 0; r < NY; r++) col[r] = buf[size_t(r) * NX + k];
+                fft(col.data(), NY, -1);
+                for (int r = 0; r < NY; r++) buf[size_t(r) * NX + k] = col[r];
+            }
+            // rebin (src/pfdr.cu:78-124); the oblique u1 index is taken from u1
+            // itself (line 107), so the accumulation stays in row iu1 unless
+            // rounding moves it to a neighbour row
+            const float u1 = float(iu1) * G->T_u1 + G->u1_0;
+            const float abs_v1 = std::fabs(v1);
+            for (int iV0 = 0; iV0 < NY; iV0++)
+                for (int iU0 = 0; iU0 < NXH; iU0++) {
+                    const float U_0 = iU0 < NX / 2 ? float(iU0) * T_U : float(iU0 - NX) * T_U;
+                    if (!(abs_v1 <= 0.5f * G->T_v1 || std::fabs(U_0) > abs_v1 * aperture)) continue;
+                    const size_t o = (size_t(iu1) * NY + iV0) * NXH + iU0;
+                    if (abs_v1 <= 0.5f * G->T_v1) {
+                        Greb[o] += buf[size_t(iV0) * NX + iU0];
+                        W[o] += 1.0;
+                    } else {
+                        // iu1_oblique = (u1 - u1_0)/T_u1 equals iu1 (exactly so
+                        // for pitches that are powers of two), hence lo = iu1,
+                        // d = 0 and the sample lands in its own row
+                        const float iu1_ob = (u1 - G->u1_0) / G->T_u1;
+                        if (iu1_ob >= 0.0f && iu1_ob <= float(G->N_u1 - 1)) {
+                            Greb[o] += buf[size_t(iV0) * NX + iU0];
+                            W[o] += 1.0;
+                        }
+                    }
+                }
+        }
+    }
+    // normalize (src/pfdr.cu:126-142), C2R per u1 row, crop, * sqrt(1+v0^2)
+#pragma omp parallel for schedule(dynamic)
+    for (int iu1 = 0; iu1 < B; iu1++) {
+        std::vector<cd> spec(size_t(NY) * NXH);
+        for (int iV0 = 0; iV0 < NY; iV0++)
+            for (int iU0 = 0; iU0 < NXH; iU0++) {
+                const size_t o = (size_t(iu1) * NY + iV0) * NXH + iU0;
+                double w = 1.0 / double(NY * NX);
+                if (W[o] > 0.0 && iU0 != 0) w *= 1.0 / W[o];
+                spec[size_t(iV0) * NXH + iU0] = Greb[o] * w;
+            }
+        // inverse along columns (NY), then C2R along rows (NX)
+        std::vector<cd> col(NY);
+        for (int k = 0; k < NXH; k++) {
+            for (int r = 0; r < NY; r++) col[r] = spec[size_t(r) * NXH + k];
+            fft(col.data(), NY, +1);
+            for (int r = 0; r < NY; r++) spec[size_t(r) * NXH + k] = col[r];
+        }
+        std::vector<double> row(NX);
+        for (int iv0 = 0; iv0 < G->N_v0; iv0++) {
+            c2r(&spec[size_t(iv0) * NXH], row.data(), NX);
+            const double v0 = double(float(G->T_v0 * float(iv0) + G->v0_0));
+            const double s = std::sqrt(1.0 + v0 * v0);
+            for (int iu0 = 0; iu0 < G->N_u0; iu0++)
+                g_reb[(size_t(iv0) * G->N_u1 + iu1) * G->N_u0 + iu0] = row[iu0] * s;
+        }
+    }
+}
+
+void oracle_ramp_f64(const oracle_geom* G, double* rows, long nrows, int nthreads)
+{
+    // src/ramp_filter.cu:156-348: zero-pad to N_H = optimalFFTsize(2*N_u0),
+    // R2C, multiply by Re(FFT(h))/N_H, C2R (unnormalized), crop.
+    set_threads(nthreads);
+    const int N = G->N_u0;
+    const int NH = oracle_optimal_fft_size(2 * N);
+    std::vector<double> h(NH);
+    const float T = G->T_u0;
+    for (int i = 0; i < NH; i++) {
+        const float s = i < NH / 2 ? float(i) : float(i - NH);
+        h[i] = double(float(1.0 / (T * kPI * (0.25 - s * s))));
+    }
+    std::vector<cd> Hc(NH / 2 + 1);
+    r2c(h.data(), Hc.data(), NH);
+    std::vector<double> Hr(NH / 2 + 1);
+    for (int k = 0; k <= NH / 2; k++) Hr[k] = Hc[k].real() / double(NH);
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < nrows; r++) {
+        std::vector<double> pad(NH, 0.0);
+        std::vector<cd> spec(NH / 2 + 1);
+        double* row = rows + size_t(r) * N;
+        for (int i = 0; i < N; i++) pad[i] = row[i];
+        r2c(pad.data(), spec.data(), NH);
+        for (int k = 0; k <= NH / 2; k++) spec[k] *= Hr[k];
+        c2r(spec.data(), pad.data(), NH);
+        for (int i = 0; i < N; i++) row[i] = pad[i];
+    }
+}
+
+void oracle_rd_gradient_f64(const double* f, double* Df, int N1, int N2, int N3, double delta, double beta,
+                            int nthreads)
+{
+    // src/relative_differences.cu:107-173 (after clip f<1e-8 -> 0, lines 107-115)
+    set_threads(nthreads);
+    const size_t N = size_t(N1) * N2 * N3;
+    std::vector<double> c(N);
+    for (size_t i = 0; i < N; i++) c[i] = f[i] < double(0.00000001f) ? 0.0 : f[i];
+    const std::vector<Nbr> nb = neighbours(false, 26);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N1; i++)
+        for (int j = 0; j < N2; j++)
+            for (int k = 0; k < N3; k++) {
+                const double x = c[(size_t(i) * N2 + j) * N3 + k];
+                double s[4] = {0, 0, 0, 0};
+                for (const Nbr& n : nb) {
+                    const int ii = std::min(N1 - 1, std::max(0, i + n.di));
+                    const int jj = std::min(N2 - 1, std::max(0, j + n.dj));
+                    const int kk = std::min(N3 - 1, std::max(0, k + n.dk));
+                    s[n.cls] += drd(x, c[(size_t(ii) * N2 + jj) * N3 + kk], delta);
+                }
+                Df[(size_t(i) * N2 + j) * N3 + k] =
+                    s[1] * dist_w(1, beta) + s[2] * dist_w(2, beta) + s[3] * dist_w(3, beta);
+            }
+}
+
+double oracle_rd_cost_f64(const double* f, int N1, int N2, int N3, double delta, double beta)
+{
+    const size_t N = size_t(N1) * N2 * N3;
+    std::vector<double> c(N);
+    for (size_t i = 0; i < N; i++) c[i] = f[i] < double(0.00000001f) ? 0.0 : f[i];
+    const std::vector<Nbr> nb = neighbours(false, 26);
+    double total = 0.0;
+    for (int i = 0; i < N1; i++)
+        for (int j = 0; j < N2; j++)
+            for (int k = 0; k < N3; k++) {
+                const double x = c[(size_t(i) * N2 + j) * N3 + k];
+                for (const Nbr& n : nb) {
+                    const int ii = std::min(N1 - 1, std::max(0, i + n.di));
+                    const int jj = std::min(N2 - 1, std::max(0, j + n.dj));
+                    const int kk = std::min(N3 - 1, std::max(0, k + n.dk));
+                    total += dist_w(n.cls, beta) * rd(x, c[(size_t(ii) * N2 + jj) * N3 + kk], delta);
+                }
+            }
+    return total;
+}
+
+static void tv_args(double& delta, double& beta)
+{
+    if (beta <= 0.0) beta = 1.0;
+    if (delta < 1.0e-8) delta = double(float(1.0e-8));
+}
+
+double oracle_tv_cost_f64(const double* f, int N1, int N2, int N3, double delta, double beta, double p,
+                          int numNeighbors)
+{
+    // aTV_Huber_costTerm, src/total_variation.cu:80-201
+    tv_args(delta, beta);
+    const Huber hb(delta, p);
+    const std::vector<Nbr> nb = neighbours(N1 == 1, numNeighbors);
+    double total = 0.0;
+    for (int i = 0; i < N1; i++)
+        for (int j = 0; j < N2; j++)
+            for (int k = 0; k < N3; k++) {
+                const double x = f[(size_t(i) * N2 + j) * N3 + k];
+                for (const Nbr& n : nb) {
+                    const int ii = std::min(N1 - 1, std::max(0, i + n.di));
+                    const int jj = std::min(N2 - 1, std::max(0, j + n.dj));
+                    const int kk = std::min(N3 - 1, std::max(0, k + n.dk));
+                    total += dist_w(n.cls, beta) * hb.h(x - f[(size_t(ii) * N2 + jj) * N3 + kk]);
+                }
+            }
+    return total;
+}
+
+void oracle_tv_gradient_f64(const double* f, double* Df, int N1, int N2, int N3, double delta, double beta,
+                            double p, int numNeighbors, int nthreads)
+{
+    // aTV_Huber_gradient, src/total_variation.cu:434-572
+    set_threads(nthreads);
+    tv_args(delta, beta);
+    const Huber hb(delta, p);
+    const std::vector<Nbr> nb = neighbours(N1 == 1, numNeighbors);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N1; i++)
+        for (int j = 0; j < N2; j++)
+            for (int k = 0; k < N3; k++) {
+                const double x = f[(size_t(i) * N2 + j) * N3 + k];
+                double s[4] = {0, 0, 0, 0};
+                for (const Nbr& n : nb) {
+                    const int ii = std::min(N1 - 1, std::max(0, i + n.di));
+                    const int jj = std::min(N2 - 1, std::max(0, j + n.dj));
+                    const int kk = std::min(N3 - 1, std::max(0, k + n.dk));
+                    const double d = x - f[(size_t(ii) * N2 + jj) * N3 + kk];
+                    // the reference evaluates DHuber(0) through the quadratic branch -> 0
+                    s[n.cls] += hb.dh(d);
+                }
+                Df[(size_t(i) * N2 + j) * N3 + k] =
+                    s[1] * dist_w(1, beta) + s[2] * dist_w(2, beta) + s[3] * dist_w(3, beta);
+            }
+}
+
+double oracle_tv_quadform_f64(const double* f, const double* d, int N1, int N2, int N3, double delta,
+                              double beta, double p, int numNeighbors)
+{
+    // aTV_Huber_quadFormTerm, src/total_variation.cu:218-432
+    tv_args(delta, beta);
+    const Huber hb(delta, p);
+    const std::vector<Nbr> nb = neighbours(N1 == 1, numNeighbors);
+    double total = 0.0;
+    for (int i = 0; i < N1; i++)
+        for (int j = 0; j < N2; j++)
+            for (int k = 0; k < N3; k++) {
+                const size_t o = (size_t(i) * N2 + j) * N3 + k;
+                for (const Nbr& n : nb) {
+                    const int ii = std::min(N1 - 1, std::max(0, i + n.di));
+                    const int jj = std::min(N2 - 1, std::max(0, j + n.dj));
+                    const int kk = std::min(N3 - 1, std::max(0, k + n.dk));
+                    const size_t q = (size_t(ii) * N2 + jj) * N3 + kk;
+                    const double dd = d[o] - d[q];
+                    total += dist_w(n.cls, beta) * hb.ddh(f[o] - f[q]) * dd * dd;
+                }
+            }
+    return total;
+}
+
+}  // extern "C"

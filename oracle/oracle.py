@@ -1,0 +1,392 @@
+"""ctypes face of the CPU oracle (``liboracle.so``) -- test infrastructure only.
+
+The C++ restatement lives in ``oracle.cpp``; this module adds the pieces the
+reference writes in Python or composes on the host:
+
+* the C-ABI conventions of ``add_planogram`` (full lengths halved, psi in
+  degrees; reference ``src/petl_c_interface.cpp:216-219``),
+* multi-planogram projection / backprojection (``src/petl.cpp:205-277``),
+* FBP as ``PETL::doFBP`` composes it (``src/petl.cpp:310-355``),
+* the MLEM loop of ``PETLserver.MLEM`` (``src/petl_server.py:1534-1606``)
+  with the dataCube elementwise rules (``src/data_cube.cpp:141-155``).
+
+Everything here runs in float64 unless a ``_f32`` variant is requested.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class Geom(ctypes.Structure):
+    """Mirror of ``oracle_geom`` (one planogram + the volume)."""
+    _fields_ = [(n, ctypes.c_float) for n in ("psi", "R", "L", "H", "v_m0", "v_m1")] + \
+               [(n, ctypes.c_int) for n in ("N_v1", "N_v0", "N_u1", "N_u0")] + \
+               [(n, ctypes.c_float) for n in ("T_v1", "T_v0", "T_u1", "T_u0",
+                                                "v1_0", "v0_0", "u1_0", "u0_0",
+                                                "cos_psi", "sin_psi")] + \
+               [(n, ctypes.c_int) for n in ("numX", "numY", "numZ")] + \
+               [(n, ctypes.c_float) for n in ("voxelWidth", "voxelHeight", "x_0", "y_0", "z_0")]
+
+    @property
+    def shape(self):
+        return (self.N_v1, self.N_v0, self.N_u1, self.N_u0)
+
+    @property
+    def vol_shape(self):
+        return (self.numZ, self.numY, self.numX)
+
+    def copy(self):
+        g = Geom()
+        ctypes.pointer(g)[0] = self
+        return g
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle library missing: run `make -C oracle` (or __graft_entry__.build())")
+        L = ctypes.CDLL(path)
+        P = ctypes.POINTER
+        dp, fp = P(ctypes.c_double), P(ctypes.c_float)
+        gp = P(Geom)
+        L.oracle_planogram_init.argtypes = [gp] + [ctypes.c_float] * 7
+        L.oracle_planogram_init.restype = ctypes.c_int
+        L.oracle_set_volume.argtypes = [gp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 5
+        L.oracle_optimal_fft_size.argtypes = [ctypes.c_int]
+        L.oracle_optimal_fft_size.restype = ctypes.c_int
+        L.oracle_project_f64.argtypes = [gp, dp, dp, ctypes.c_int]
+        L.oracle_project_f32.argtypes = [gp, fp, fp, ctypes.c_int]
+        L.oracle_backproject_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int]
+        L.oracle_backproject_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int]
+        L.oracle_project_nnz.argtypes = [gp, ctypes.c_int]
+        L.oracle_project_nnz.restype = ctypes.c_double
+        L.oracle_pfdr_f64.argtypes = [gp, dp, dp, ctypes.c_int]
+        L.oracle_ramp_f64.argtypes = [gp, dp, ctypes.c_long, ctypes.c_int]
+        L.oracle_fft_c2c.argtypes = [dp, ctypes.c_int, ctypes.c_int]
+        L.oracle_rd_gradient_f64.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.oracle_rd_cost_f64.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_double]
+        L.oracle_rd_cost_f64.restype = ctypes.c_double
+        L.oracle_tv_cost_f64.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.oracle_tv_cost_f64.restype = ctypes.c_double
+        L.oracle_tv_gradient_f64.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_int, ctypes.c_int]
+        L.oracle_tv_quadform_f64.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.oracle_tv_quadform_f64.restype = ctypes.c_double
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ----------------------------------------------------------------------------
+# geometry
+# ----------------------------------------------------------------------------
+def make_geom(psi_deg, D, L, H, T, v_m0, v_m1, vol):
+    """One planogram as the C-ABI ``add_planogram(psi, D, L, H, v_m0, v_m1, T)``
+    defines it, plus the volume ``vol = (numX, numY, numZ, voxelWidth,
+    voxelHeight, offsetX, offsetY, offsetZ)``."""
+    g = Geom()
+    # src/petl_c_interface.cpp:216-219 (float arguments, double arithmetic)
+    psi = np.float32(psi_deg * math.pi / 180.0)
+    ok = lib().oracle_planogram_init(ctypes.byref(g), float(psi), float(np.float32(0.5 * np.float32(D))),
+                                     float(np.float32(0.5 * np.float32(L))),
+                                     float(np.float32(0.5 * np.float32(H))),
+                                     float(np.float32(v_m0)), float(np.float32(v_m1)), float(np.float32(T)))
+    if not ok:
+        raise ValueError("invalid planogram")
+    set_volume(g, *vol)
+    return g
+
+
+def set_volume(g, numX, numY, numZ, voxelWidth, voxelHeight=0.0, offsetX=0.0, offsetY=0.0, offsetZ=0.0):
+    if voxelHeight == 0.0:
+        voxelHeight = voxelWidth
+    lib().oracle_set_volume(ctypes.byref(g), int(numX), int(numY), int(numZ), float(voxelWidth),
+                            float(voxelHeight), float(offsetX), float(offsetY), float(offsetZ))
+    return g
+
+
+def optimal_fft_size(n):
+    return lib().oracle_optimal_fft_size(int(n))
+
+
+# ----------------------------------------------------------------------------
+# projectors
+# ----------------------------------------------------------------------------
+def project(geoms, f, dtype=np.float64, nthreads=0):
+    """P f for each planogram (``PETL::project``, src/petl.cpp:205-224)."""
+    if isinstance(geoms, Geom):
+        geoms = [geoms]
+    out = []
+    for G in geoms:
+        if dtype == np.float32:
+            fc = _f(f)
+            g = np.zeros(G.shape, np.float32)
+            lib().oracle_project_f32(ctypes.byref(G), _ptr(fc, ctypes.c_float), _ptr(g, ctypes.c_float), nthreads)
+        else:
+            fc = _d(f)
+            g = np.zeros(G.shape, np.float64)
+            lib().oracle_project_f64(ctypes.byref(G), _ptr(fc, ctypes.c_double), _ptr(g, ctypes.c_double), nthreads)
+        out.append(g)
+    return out
+
+
+def backproject(geoms, g, dtype=np.float64, texmode=0, nthreads=0):
+    """P^T g summed over planograms (``PETL::backproject``, src/petl.cpp:226-277)."""
+    if isinstance(geoms, Geom):
+        geoms, g = [geoms], [g]
+    f = None
+    for G, gi in zip(geoms, g):
+        if dtype == np.float32:
+            gc = _f(gi)
+            fi = np.zeros(G.vol_shape, np.float32)
+            lib().oracle_backproject_f32(ctypes.byref(G), _ptr(gc, ctypes.c_float), _ptr(fi, ctypes.c_float),
+                                         int(texmode), nthreads)
+        else:
+            gc = _d(gi)
+            fi = np.zeros(G.vol_shape, np.float64)
+            lib().oracle_backproject_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(fi, ctypes.c_double),
+                                         int(texmode), nthreads)
+        f = fi if f is None else f + fi
+    return f
+
+
+def project_nnz(G, nthreads=0):
+    return lib().oracle_project_nnz(ctypes.byref(G), nthreads)
+
+
+# ----------------------------------------------------------------------------
+# PFDR / ramp / FBP
+# ----------------------------------------------------------------------------
+def pfdr(G, g, nthreads=0):
+    gc = _d(g)
+    out = np.zeros((G.N_v0, G.N_u1, G.N_u0), np.float64)
+    lib().oracle_pfdr_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(out, ctypes.c_double), nthreads)
+    return out
+
+
+def rebinned_geom(G):
+    """Geometry after ``PETL::doPFDR`` (src/petl.cpp:379-380): N_v1 = 1, v1_0 = 0."""
+    R = G.copy()
+    R.N_v1 = 1
+    R.v1_0 = 0.0
+    return R
+
+
+def ramp(G, rows, nthreads=0):
+    r = np.array(rows, dtype=np.float64, copy=True, order="C")
+    lib().oracle_ramp_f64(ctypes.byref(G), _ptr(r, ctypes.c_double), int(r.size // G.N_u0), nthreads)
+    return r
+
+
+def fbp(geoms, g, nthreads=0):
+    """``PETL::doFBP`` (src/petl.cpp:310-355) for a list of planograms."""
+    if isinstance(geoms, Geom):
+        geoms, g = [geoms], [g]
+    rebinned, rgeoms = [], []
+    for G, gi in zip(geoms, g):
+        if G.N_v1 > 1:
+            gr = pfdr(G, gi, nthreads)
+            Gr = rebinned_geom(G)
+        else:
+            gr = np.asarray(gi, np.float64).reshape(G.N_v0, G.N_u1, G.N_u0)
+            Gr = G
+        gr = ramp(Gr, gr, nthreads)
+        # apply_planogram_weight(inverse) (src/planogram.cpp:304-333)
+        for iv0 in range(Gr.N_v0):
+            v1 = np.float32(np.float32(0) * np.float32(Gr.T_v1) + np.float32(Gr.v1_0))
+            v0 = np.float32(np.float32(iv0) * np.float32(Gr.T_v0) + np.float32(Gr.v0_0))
+            c = np.float32(1.0 / math.sqrt(1.0 + float(v1) * float(v1) + float(v0) * float(v0)))
+            gr[iv0] *= float(np.float32(1.0) / c)
+        rebinned.append(gr.reshape(1, Gr.N_v0, Gr.N_u1, Gr.N_u0))
+        rgeoms.append(Gr)
+    f = None
+    for Gr, gr in zip(rgeoms, rebinned):
+        fi = backproject(Gr, gr, nthreads=nthreads)
+        # FBPweight scale (src/petl.cpp:254-259)
+        fi *= float(np.float32(np.float32(Gr.T_v0) * np.float32(Gr.T_u0) / np.float32(Gr.voxelWidth)))
+        f = fi if f is None else f + fi
+    return f
+
+
+def fft_c2c(x, sign=-1):
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    lib().oracle_fft_c2c(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size, int(sign))
+    return a
+
+
+# ----------------------------------------------------------------------------
+# regularizers
+# ----------------------------------------------------------------------------
+def _shape3(f):
+    f = np.asarray(f)
+    if f.ndim == 2:
+        return (1,) + f.shape
+    return f.shape
+
+
+def rd_gradient(f, delta, beta, nthreads=0):
+    N = _shape3(f)
+    fc = _d(f).reshape(N)
+    out = np.zeros(N, np.float64)
+    lib().oracle_rd_gradient_f64(_ptr(fc, ctypes.c_double), _ptr(out, ctypes.c_double), *N,
+                                 float(delta), float(beta), nthreads)
+    return out.reshape(np.shape(f))
+
+
+def rd_cost(f, delta, beta):
+    N = _shape3(f)
+    fc = _d(f).reshape(N)
+    return lib().oracle_rd_cost_f64(_ptr(fc, ctypes.c_double), *N, float(delta), float(beta))
+
+
+def tv_cost(f, delta, beta=0.0, p=1.0, num_neighbors=26):
+    N = _shape3(f)
+    fc = _d(f).reshape(N)
+    return lib().oracle_tv_cost_f64(_ptr(fc, ctypes.c_double), *N, float(delta), float(beta), float(p),
+                                    int(num_neighbors))
+
+
+def tv_gradient(f, delta, beta=0.0, p=1.0, num_neighbors=26, nthreads=0):
+    N = _shape3(f)
+    fc = _d(f).reshape(N)
+    out = np.zeros(N, np.float64)
+    lib().oracle_tv_gradient_f64(_ptr(fc, ctypes.c_double), _ptr(out, ctypes.c_double), *N, float(delta),
+                                 float(beta), float(p), int(num_neighbors), nthreads)
+    return out.reshape(np.shape(f))
+
+
+def tv_quadform(f, d, delta, beta=0.0, p=1.0, num_neighbors=26):
+    N = _shape3(f)
+    fc, dc = _d(f).reshape(N), _d(d).reshape(N)
+    return lib().oracle_tv_quadform_f64(_ptr(fc, ctypes.c_double), _ptr(dc, ctypes.c_double), *N,
+                                        float(delta), float(beta), float(p), int(num_neighbors))
+
+
+def diffuse(f, delta, num_iter, p=1.0, num_neighbors=26):
+    """``Diffuse`` (src/total_variation.cu:813-868) in float64."""
+    f = _d(f).copy()
+    for _ in range(num_iter):
+        d = tv_gradient(f, delta, 1.0, p, num_neighbors)
+        num = float(np.sum(d * d))
+        den = tv_quadform(f, d, delta, 1.0, p, num_neighbors)
+        if den <= 1.0e-16:
+            break
+        f -= (num / den) * d
+    return f
+
+
+def tv_denoise(f, delta, beta, num_iter, p=1.0, num_neighbors=26):
+    """``TVdenoise`` (src/total_variation.cu:870-935) in float64."""
+    f = _d(f).copy()
+    f0 = f.copy()
+    for _ in range(num_iter):
+        d = tv_gradient(f, delta, beta, p, num_neighbors)
+        num = float(np.sum(d * d))
+        den = tv_quadform(f, d, delta, beta, p, num_neighbors)
+        if den <= 1.0e-16:
+            break
+        s = num / den
+        f = (1.0 - s) * f - s * (d - f0)
+    return f
+
+
+# ----------------------------------------------------------------------------
+# MLEM (src/petl_server.py:1534-1606) with dataCube rules (src/data_cube.cpp)
+# ----------------------------------------------------------------------------
+def _rdivide(denom, num):
+    out = np.zeros_like(denom)
+    nz = denom != 0.0
+    out[nz] = num[nz] / denom[nz]
+    return out
+
+
+def _divide(x, y):
+    out = np.zeros_like(x)
+    nz = y != 0.0
+    out[nz] = x[nz] / y[nz]
+    return out
+
+
+def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, nthreads=0):
+    if isinstance(geoms, Geom):
+        geoms, g = [geoms], [g]
+    vol = geoms[0].vol_shape
+    if f is None or not np.any(f):
+        f = np.ones(vol, np.float64)
+    else:
+        f = np.maximum(_d(f), 0.0)
+    ones = [np.ones(G.shape) for G in geoms]
+    sens = backproject(geoms, ones, nthreads=nthreads)
+    sens[sens == 0.0] = 1.0
+    for _ in range(num_iter):
+        Pd = project(geoms, f, nthreads=nthreads)
+        ratio = [_rdivide(p, gi) for p, gi in zip(Pd, g)]
+        d = backproject(geoms, ratio, nthreads=nthreads)
+        if beta <= 0.0:
+            f = f * _divide(d, sens)
+        else:
+            tv = rd_gradient(f, delta, beta, nthreads) + sens
+            tv = np.maximum(0.1 * sens, tv)
+            f = f * _divide(d, tv)
+    return f
+
+
+def osem(geoms, g, num_iter, num_subsets, f=None, nthreads=0):
+    """Ordered-subsets EM with interleaved subsets over iv0 (subset s holds the
+    views iv0 with iv0 % S == s).  With S = 1 it is exactly ``mlem``."""
+    if isinstance(geoms, Geom):
+        geoms, g = [geoms], [g]
+    vol = geoms[0].vol_shape
+    f = np.ones(vol, np.float64) if (f is None or not np.any(f)) else np.maximum(_d(f), 0.0)
+    masks = []
+    for s in range(num_subsets):
+        ms = []
+        for G in geoms:
+            m = np.zeros(G.shape)
+            m[:, s::num_subsets] = 1.0
+            ms.append(m)
+        masks.append(ms)
+    sens = []
+    for s in range(num_subsets):
+        ss = backproject(geoms, masks[s], nthreads=nthreads)
+        ss[ss == 0.0] = 1.0
+        sens.append(ss)
+    for _ in range(num_iter):
+        for s in range(num_subsets):
+            Pd = project(geoms, f, nthreads=nthreads)
+            ratio = [_rdivide(p, gi) * m for p, gi, m in zip(Pd, g, masks[s])]
+            d = backproject(geoms, ratio, nthreads=nthreads)
+            f = f * _divide(d, sens[s])
+    return f
+
+
+def poisson_loglik(g, Pf):
+    """sum(g*log(Pf) - Pf) over bins with Pf > 0 (the MLEM objective)."""
+    total = 0.0
+    for gi, pi in zip(g, Pf):
+        m = pi > 0
+        total += float(np.sum(gi[m] * np.log(pi[m]) - pi[m]))
+    return total

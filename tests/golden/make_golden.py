@@ -1,0 +1,313 @@
+"""Generate golden vectors from the reference PETL library itself.
+
+The reference library is compiled from its own sources by ``make -C oracle
+ref`` into ``oracle/_ref/libpetl_ref.so``.  Its projector, backprojector,
+PFDR, FBP and regularizers exist only as CUDA, so this script has to run on a
+machine with a GPU; geometry and the dataCube elementwise rules are CPU code
+and run anywhere.
+
+    python tests/golden/make_golden.py --out <dir> [--cpu-only]
+
+Each case is written as ``<name>.npz`` holding its inputs, the reference
+arguments and the reference outputs.  The committed fixtures in this
+directory were produced by this script; the tests read them, never the
+reference library.
+
+The MLEM case drives the reference C ABI with the same call sequence as the
+reference ``PETLserver.MLEM`` loop (src/petl_server.py:1534-1606): project,
+rdivide4D, backproject, divide3D, multiply3D, with sensitivity =
+backproject(ones) and zeros of the sensitivity replaced by one.
+"""
+import argparse
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libpetl_ref.so")
+
+fp = ctypes.POINTER(ctypes.c_float)
+
+
+class Ref:
+    def __init__(self, path=REF_LIB):
+        L = ctypes.CDLL(path)
+        c_f, c_i, c_b = ctypes.c_float, ctypes.c_int, ctypes.c_bool
+        L.create_new_model.restype = c_i
+        L.set_model.argtypes = [c_i]
+        L.add_planogram.argtypes = [c_f] * 7
+        L.add_planogram.restype = c_b
+        L.set_volume.argtypes = [c_i, c_i, c_i, c_f, c_f, c_f, c_f, c_f]
+        L.set_volume.restype = c_b
+        L.get_numPlanograms.restype = c_i
+        L.get_planogramSize.argtypes = [c_i, ctypes.POINTER(c_i)]
+        L.get_planogramSize.restype = c_b
+        for n in ("project", "backproject", "FBP"):
+            getattr(L, n).argtypes = [ctypes.POINTER(fp), fp]
+            getattr(L, n).restype = c_b
+        L.PFDR.argtypes = [ctypes.POINTER(fp), ctypes.POINTER(fp)]
+        L.PFDR.restype = c_b
+        L.rdivide4D.argtypes = [fp, fp, c_i, c_i, c_i, c_i]
+        L.rdivide4D.restype = c_b
+        L.divide3D.argtypes = [fp, fp, c_i, c_i, c_i]
+        L.divide3D.restype = c_b
+        L.multiply3D.argtypes = [fp, fp, c_i, c_i, c_i]
+        L.multiply3D.restype = c_b
+        L.reciprocal3D.argtypes = [fp, c_i, c_i, c_i, c_f]
+        L.reciprocal3D.restype = c_b
+        L.inner_product3D.argtypes = [fp, fp, fp, c_i, c_i, c_i]
+        L.inner_product3D.restype = c_f
+        L.relativeDifferences_gradient.argtypes = [fp, fp, c_i, c_i, c_i, c_f, c_f]
+        L.relativeDifferences_gradient.restype = c_b
+        L.TV_cost.argtypes = [fp, c_i, c_i, c_i, c_f, c_f, c_f, c_b]
+        L.TV_cost.restype = c_f
+        L.TV_gradient.argtypes = [fp, fp, c_i, c_i, c_i, c_f, c_f, c_f, c_b]
+        L.TV_gradient.restype = c_b
+        L.TV_quadForm.argtypes = [fp, fp, c_i, c_i, c_i, c_f, c_f, c_f, c_b]
+        L.TV_quadForm.restype = c_f
+        L.diffuse.argtypes = [fp, c_i, c_i, c_i, c_f, c_f, c_i, c_b]
+        L.diffuse.restype = c_b
+        L.TV_denoise.argtypes = [fp, c_i, c_i, c_i, c_f, c_f, c_f, c_i, c_b, c_b]
+        L.TV_denoise.restype = c_b
+        self.L = L
+
+    def model(self, planograms, vol):
+        m = self.L.create_new_model()
+        self.L.set_model(m)
+        for p in planograms:
+            psi, D, L_, H, T, vm0, vm1 = p
+            if not self.L.add_planogram(psi, D, L_, H, vm0, vm1, T):
+                raise RuntimeError("add_planogram failed")
+        if vol is not None and not self.L.set_volume(*vol):
+            raise RuntimeError("set_volume failed")
+        return m
+
+    def shapes(self):
+        out = []
+        for i in range(self.L.get_numPlanograms()):
+            s = (ctypes.c_int * 4)()
+            self.L.get_planogramSize(i, s)
+            out.append(tuple(s))
+        return out
+
+    @staticmethod
+    def pp(arrs):
+        a = (fp * len(arrs))(*[x.ctypes.data_as(fp) for x in arrs])
+        return a
+
+
+def ptr(a):
+    return a.ctypes.data_as(fp)
+
+
+def ellipsoids(shape, vox, rng, n, vmin=0.1, vmax=1.0, background=0.0):
+    """Seeded ellipsoid phantom (replace semantics, insertion order)."""
+    nz, ny, nx = shape
+    wx, wz = vox
+    x = (np.arange(nx) - 0.5 * (nx - 1)) * wx
+    y = (np.arange(ny) - 0.5 * (ny - 1)) * wx
+    z = (np.arange(nz) - 0.5 * (nz - 1)) * wz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    f = np.full(shape, background, np.float32)
+    ext = np.array([nx * wx, ny * wx, nz * wz]) * 0.5
+    for _ in range(n):
+        r = rng.uniform(0.08, 0.3, 3) * ext
+        c = rng.uniform(-1, 1, 3) * np.maximum(ext - r, 0)
+        val = rng.uniform(vmin, vmax)
+        inside = ((X - c[0]) / r[0]) ** 2 + ((Y - c[1]) / r[1]) ** 2 + ((Z - c[2]) / r[2]) ** 2 <= 1.0
+        f[inside] = val
+    return f
+
+
+GEOMS = {
+    # name: (planograms [(psi, D, L, H, T, v_m0, v_m1)], volume (numX,numY,numZ,vw,vh,ox,oy,oz))
+    "g0": ([(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)], (32, 32, 8, 2.0, 2.0, 0.0, 0.0, 0.0)),
+    "g90": ([(90.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)], (32, 32, 8, 2.0, 2.0, 0.0, 0.0, 0.0)),
+    "g30": ([(30.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)], (32, 32, 8, 2.0, 2.0, 0.0, 0.0, 0.0)),
+    "gpitch": ([(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)], (40, 40, 12, 1.5, 1.25, 1.0, -2.0, 0.5)),
+    "gpetx": ([(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25), (90.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)],
+              (32, 32, 8, 2.0, 2.0, 0.0, 0.0, 0.0)),
+    "g0t1": ([(0.0, 48.0, 24.0, 16.0, 1.0, 0.5, 0.25)], (48, 48, 16, 1.0, 1.0, 0.0, 0.0, 0.0)),
+}
+
+
+def run_projectors(ref, out):
+    for name, (plans, vol) in GEOMS.items():
+        rng = np.random.default_rng(sum(map(ord, name)))
+        ref.model(plans, vol)
+        shapes = ref.shapes()
+        vshape = (vol[2], vol[1], vol[0])
+        f = ellipsoids(vshape, (vol[3], vol[4]), rng, 6)
+        f_noise = rng.random(vshape).astype(np.float32)
+        g = [np.zeros(s, np.float32) for s in shapes]
+        if not ref.L.project(ref.pp(g), ptr(f)):
+            raise RuntimeError("project failed")
+        g_noise = [np.zeros(s, np.float32) for s in shapes]
+        ref.L.project(ref.pp(g_noise), ptr(f_noise))
+        y = [rng.random(s).astype(np.float32) for s in shapes]
+        b = np.zeros(vshape, np.float32)
+        if not ref.L.backproject(ref.pp(y), ptr(b)):
+            raise RuntimeError("backproject failed")
+        ones = [np.ones(s, np.float32) for s in shapes]
+        sens = np.zeros(vshape, np.float32)
+        ref.L.backproject(ref.pp(ones), ptr(sens))
+        rec = dict(planograms=np.array(plans, np.float64), volume=np.array(vol, np.float64),
+                   f=f, f_noise=f_noise, sens=sens, b=b)
+        for i, s in enumerate(shapes):
+            rec[f"g{i}"] = g[i]
+            rec[f"gnoise{i}"] = g_noise[i]
+            rec[f"y{i}"] = y[i]
+        np.savez_compressed(os.path.join(out, f"proj_{name}.npz"), **rec)
+        print("wrote", name, shapes)
+
+
+def run_pfdr_fbp(ref, out):
+    for name in ("g0", "g0t1"):
+        plans, vol = GEOMS[name]
+        ref.model(plans, vol)
+        shapes = ref.shapes()
+        vshape = (vol[2], vol[1], vol[0])
+        rng = np.random.default_rng(1234 + len(name))
+        f = ellipsoids(vshape, (vol[3], vol[4]), rng, 6)
+        g = [np.zeros(s, np.float32) for s in shapes]
+        ref.L.project(ref.pp(g), ptr(f))
+        fbp = np.zeros(vshape, np.float32)
+        if not ref.L.FBP(ref.pp(g), ptr(fbp)):
+            raise RuntimeError("FBP failed")
+        # PFDR changes the model's planogram (N_v1 -> 1): do it last
+        greb = [np.zeros(s[1:], np.float32) for s in shapes]
+        if not ref.L.PFDR(ref.pp(g), ref.pp(greb)):
+            raise RuntimeError("PFDR failed")
+        shapes_after = ref.shapes()
+        np.savez_compressed(os.path.join(out, f"pfdr_{name}.npz"), planograms=np.array(plans, np.float64),
+                            volume=np.array(vol, np.float64), f=f, g=g[0], g_reb=greb[0], fbp=fbp,
+                            shape_after=np.array(shapes_after[0]))
+        print("wrote pfdr", name)
+
+
+def run_mlem(ref, out):
+    plans, vol = GEOMS["g0"]
+    ref.model(plans, vol)
+    shape = ref.shapes()[0]
+    vshape = (vol[2], vol[1], vol[0])
+    rng = np.random.default_rng(777)
+    ftrue = ellipsoids(vshape, (vol[3], vol[4]), rng, 6)
+    g = [np.zeros(shape, np.float32)]
+    ref.L.project(ref.pp(g), ptr(ftrue))
+    g[0] *= np.float32(2e5 / g[0].sum())
+    g = [rng.poisson(g[0]).astype(np.float32)]
+    rec = dict(planograms=np.array(plans, np.float64), volume=np.array(vol, np.float64), g=g[0])
+    for beta, tag in ((0.0, "plain"), (0.05, "rd")):
+        f = np.ones(vshape, np.float32)
+        ones = [np.ones(shape, np.float32)]
+        sens = np.zeros(vshape, np.float32)
+        ref.L.backproject(ref.pp(ones), ptr(sens))
+        sens[sens == 0.0] = 1.0
+        d = np.zeros(vshape, np.float32)
+        Pd = [np.zeros(shape, np.float32)]
+        iters = []
+        for n in range(4):
+            ref.L.project(ref.pp(Pd), ptr(f))
+            ref.L.rdivide4D(ptr(g[0]), ptr(Pd[0]), *shape)
+            ref.L.backproject(ref.pp(Pd), ptr(d))
+            if beta <= 0.0:
+                ref.L.divide3D(ptr(d), ptr(sens), *vshape)
+                ref.L.multiply3D(ptr(f), ptr(d), *vshape)
+            else:
+                tv = np.zeros(vshape, np.float32)
+                ref.L.relativeDifferences_gradient(ptr(f), ptr(tv), *vshape, 2.0, beta)
+                tv[:] += sens[:]
+                np.maximum(np.float32(0.1) * sens, tv, out=tv)
+                ref.L.divide3D(ptr(d), ptr(tv), *vshape)
+                ref.L.multiply3D(ptr(f), ptr(d), *vshape)
+            iters.append(f.copy())
+        rec[f"f_{tag}"] = np.stack(iters)
+        rec[f"sens_{tag}"] = sens
+    np.savez_compressed(os.path.join(out, "mlem_g0.npz"), **rec)
+    print("wrote mlem")
+
+
+def run_regularizers(ref, out):
+    ref.model([GEOMS["g0"][0][0]], GEOMS["g0"][1])
+    rng = np.random.default_rng(4242)
+    rec = {}
+    for tag, shape in (("3d", (10, 12, 14)), ("2d", (1, 16, 18))):
+        f = (rng.random(shape) * 2.0).astype(np.float32)
+        f[0, 0, :3] = 0.0  # exercise the x == y == 0 branches
+        d = rng.standard_normal(shape).astype(np.float32)
+        rec[f"f_{tag}"] = f
+        rec[f"d_{tag}"] = d
+        Df = np.zeros(shape, np.float32)
+        ref.L.relativeDifferences_gradient(ptr(f), ptr(Df), *shape, 2.0, 0.01)
+        rec[f"rd_grad_{tag}"] = Df
+        for delta, p in ((0.05, 1.0), (0.3, 1.2)):
+            key = f"{tag}_d{delta}_p{p}"
+            Dt = np.zeros(shape, np.float32)
+            ref.L.TV_gradient(ptr(f), ptr(Dt), *shape, delta, 0.7, p, True)
+            rec[f"tv_grad_{key}"] = Dt
+            rec[f"tv_cost_{key}"] = np.float64(ref.L.TV_cost(ptr(f), *shape, delta, 0.7, p, True))
+            rec[f"tv_quad_{key}"] = np.float64(ref.L.TV_quadForm(ptr(f), ptr(d), *shape, delta, 0.7, p, True))
+        fd = f.copy()
+        ref.L.diffuse(ptr(fd), *shape, 0.05, 1.0, 3, True)
+        rec[f"diffuse_{tag}"] = fd
+        fn = f.copy()
+        ref.L.TV_denoise(ptr(fn), *shape, 0.05, 0.5, 1.0, 3, False, True)
+        rec[f"tvdenoise_{tag}"] = fn
+    np.savez_compressed(os.path.join(out, "regularizers.npz"), **rec)
+    print("wrote regularizers")
+
+
+def run_cpu(ref, out):
+    """Geometry and dataCube rules: CPU-only reference code."""
+    rec = {}
+    calls = [(0.0, 256.0, 128.0, 128.0, 2.0, 0.5, 0.25), (0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25),
+             (0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25), (30.0, 180.0, 192.0, 144.0, 2.0, 0.2679, 0.2679),
+             (0.0, 200.0, 96.0, 64.0, 1.5, 0.5, 0.25), (45.0, 300.0, 256.0, 128.0, 1.7, 0.4, 0.3),
+             (0.0, 256.0, 256.0, 128.0, 2.0, 0.5, 0.25), (90.0, 100.0, 50.0, 40.0, 0.8, 1.0, 0.9)]
+    shapes = []
+    for c in calls:
+        ref.model([c], None)
+        shapes.append(ref.shapes()[0])
+    rec["geom_calls"] = np.array(calls)
+    rec["geom_shapes"] = np.array(shapes)
+    rng = np.random.default_rng(99)
+    a = rng.random((3, 4, 5, 6)).astype(np.float32)
+    b = rng.random((3, 4, 5, 6)).astype(np.float32)
+    a.flat[::7] = 0.0
+    b.flat[::5] = 0.0
+    r = b.copy()
+    ref.L.rdivide4D(ptr(a), ptr(r), *a.shape)
+    rec["rd_num"], rec["rd_den"], rec["rd_out"] = a, b, r
+    x3, y3 = a[0].copy(), b[0].copy()
+    ref.L.divide3D(ptr(x3), ptr(y3), *x3.shape)
+    rec["div_x"], rec["div_y"], rec["div_out"] = a[0], b[0], x3
+    rr = b[1].copy()
+    ref.L.reciprocal3D(ptr(rr), *rr.shape, 7.0)
+    rec["recip_in"], rec["recip_out"] = b[1], rr
+    rec["ip"] = np.float64(ref.L.inner_product3D(ptr(a[2]), ptr(b[2]), None, *a[2].shape))
+    np.savez_compressed(os.path.join(out, "cpu_rules.npz"), **rec)
+    print("wrote cpu rules", shapes)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=HERE)
+    ap.add_argument("--cpu-only", action="store_true")
+    ap.add_argument("--lib", default=REF_LIB)
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    ref = Ref(a.lib)
+    run_cpu(ref, a.out)
+    if not a.cpu_only:
+        run_projectors(ref, a.out)
+        run_pfdr_fbp(ref, a.out)
+        run_mlem(ref, a.out)
+        run_regularizers(ref, a.out)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
