@@ -44,6 +44,8 @@ enum {
 
 const char* petl_last_error(void);
 int petl_version(void);
+/* Number of CUDA kernels this library has launched in this process. */
+unsigned long long petl_launch_count(void);
 
 /* planogram::init (src/planogram.cpp:143-186) with the C-ABI conventions of
  * add_planogram (src/petl_c_interface.cpp:216-219): psi in degrees, D/L/H
@@ -54,6 +56,10 @@ int petl_geom_set_volume(petl_geom* G, int numX, int numY, int numZ, float voxel
                          float offsetX, float offsetY, float offsetZ);
 /* optimalFFTsize (src/vector_ops.cpp:481-505). */
 int petl_optimal_fft_size(int N);
+
+/* The currently selected model's planogram `which` (and its volume, when the
+ * volume is defined) as set through the petl.h setters. */
+int petl_model_geometry(int which, petl_geom* out);
 
 /* Forward SF projection (src/projectors.cu:11-238).  Computes the views
  * iv0 = iv0_first + k*iv0_step (k = 0.., iv0 < N_v0) of every v1 slice and
@@ -66,6 +72,20 @@ int petl_project_dev(const petl_geom* G, const float* f, float* g, int iv0_first
  * f = accumulate ? f + scale*P^T g : scale*P^T g. */
 int petl_backproject_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
                          int iv0_first, int iv0_step, void* stream);
+
+/* Same as petl_project_dev restricted to the v1 slices [iv1_begin, iv1_end). */
+int petl_project_range_dev(const petl_geom* G, const float* f, float* g, int iv1_begin, int iv1_end, int iv0_first,
+                           int iv0_step, void* stream);
+/* Same as petl_backproject_dev restricted to the v1 slices [iv1_begin, iv1_end). */
+int petl_backproject_range_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
+                               int iv1_begin, int iv1_end, int iv0_first, int iv0_step, void* stream);
+
+/* MLEM/OSEM forward step fused with the data ratio: for the selected views
+ * ratio = (P f == 0) ? 0 : meas / (P f), the rule of the reference's rdivide
+ * (src/data_cube.cpp:150-155) applied to the projection without storing it.
+ * ratio may alias meas only if meas is not needed afterwards. */
+int petl_project_ratio_dev(const petl_geom* G, const float* f, const float* meas, float* ratio, int iv1_begin,
+                           int iv1_end, int iv0_first, int iv0_step, void* stream);
 
 /* nnz of the forward operator: the number of (ray, voxel) pairs with a
  * nonzero footprint weight, counted on the device; *nnz_host receives it
@@ -104,6 +124,10 @@ int petl_tv_cost_dev(const float* f, int N1, int N2, int N3, float delta, float 
 int petl_tv_quadform_dev(const float* f, const float* d, int N1, int N2, int N3, float delta, float beta, float p,
                          int numNeighbors, double* out, void* stream);
 
+/* gaussian_filter (src/relative_differences.cu:314-411, 753-800): in place,
+ * numDims 1 filters along N1, 2 along (N2, N3), 3 along all axes. */
+int petl_gaussian_filter_dev(float* f, int N1, int N2, int N3, float FWHM, int numDims, void* stream);
+
 /* --- elementwise / reductions (dataCube rules, src/data_cube.cpp:97-166) --- */
 /* denom = num/denom, 0 where denom == 0 (RDIV) */
 int petl_rdivide_dev(const float* num, float* denom, long long n, void* stream);
@@ -116,6 +140,8 @@ int petl_reciprocal_dev(float* x, long long n, float divide_by_zero_value, void*
 int petl_dot_dev(const float* x, const float* y, const float* w, long long n, double* out, void* stream);
 /* *out (device double) = sum over Pf>0 of g*log(Pf) - Pf (Poisson log-likelihood) */
 int petl_loglik_dev(const float* g, const float* Pf, long long n, double* out, void* stream);
+/* x = a*x + b*y */
+int petl_axpby_dev(float* x, const float* y, float a, float b, long long n, void* stream);
 /* MLEM image update f *= d / sens with the DIV rule (d/0 -> 0) */
 int petl_mlem_update_dev(float* f, const float* d, const float* sens, long long n, void* stream);
 /* one-step-late RD update (src/petl_server.py:1597-1602):

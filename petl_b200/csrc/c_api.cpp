@@ -1,0 +1,798 @@
+// The reference-compatible C ABI (include/petl.h): model registry, geometry
+// setters/getters and host-pointer entry points.
+//
+// Restates src/petl_c_interface.cpp (whole file), src/list_of_models.cpp:37-46
+// (get() appends a model when the list is empty and wraps the index modulo
+// the list size), src/parameters.cpp (volume / planogram bookkeeping,
+// set_default_volume at 205-248) and src/petl.cpp:205-385 (per-planogram
+// orchestration, FBP through PFDR when N_v1 > 1).  Differences by design:
+//  * one stream-ordered device pool replaces cudaMalloc/cudaFree per call;
+//  * projections stream their output back slab by slab (a copy stream runs
+//    behind the compute stream), backprojections stream their input in the
+//    same way and accumulate over slabs, so host<->device transfers overlap
+//    the kernels;
+//  * the elementwise helpers (multiply/divide/rdivide/reciprocal/
+//    inner_product) act on host arrays exactly as the reference's OpenMP
+//    dataCube code does; their device-resident twins are in petl_device.h.
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/petl.h"
+#include "../../include/petl_device.h"
+
+extern "C" {
+int petl_project_range_dev(const petl_geom* G, const float* f, float* g, int iv1_begin, int iv1_end, int iv0_first,
+                           int iv0_step, void* stream);
+int petl_backproject_range_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
+                               int iv1_begin, int iv1_end, int iv0_first, int iv0_step, void* stream);
+int petl_gaussian_filter_dev(float* f, int N1, int N2, int N3, float FWHM, int numDims, void* stream);
+}
+
+namespace petl {
+int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream_t st, float* host_rebinned_out);
+}
+
+namespace {
+
+const char* kVersion = "1.0";
+
+struct Params {
+    std::vector<petl_geom> plans;  // planogram fields only
+    int numX = 0, numY = 0, numZ = 0;
+    float voxelWidth = 0.f, voxelHeight = 0.f;
+    float offsetX = 0.f, offsetY = 0.f, offsetZ = 0.f;
+
+    void clearAll()
+    {
+        numX = numY = numZ = 0;
+        voxelWidth = voxelHeight = 0.f;
+        offsetX = offsetY = offsetZ = 0.f;
+        plans.clear();
+    }
+    bool volumeDefined(bool print = true) const
+    {
+        if (numX <= 0 || numY <= 0 || numZ <= 0 || voxelWidth <= 0.0 || voxelHeight <= 0.0) {
+            if (print) {
+                printf("numZ = %d voxelHeight = %f\n", numZ, voxelHeight);
+                printf("Error: volume voxel sizes and number of data elements must be positive\n");
+            }
+            return false;
+        }
+        return true;
+    }
+    static bool planDefined(const petl_geom& p)
+    {
+        return p.R > 0.0 && p.L > 0.0 && p.H > 0.0 && p.v_m0 > 0.0 && p.v_m1 >= 0.0 && p.T_u0 > 0.0 &&
+               p.T_u1 > 0.0 && p.T_v0 > 0.0 && p.T_v1 > 0.0 && p.N_u0 > 0 && p.N_u1 > 0 && p.N_v0 > 0 && p.N_v1 > 0;
+    }
+    bool geometryDefined() const
+    {
+        if (plans.empty()) return false;
+        for (const auto& p : plans)
+            if (!planDefined(p)) return false;
+        return true;
+    }
+    bool allDefined() const { return geometryDefined() && volumeDefined(); }
+    petl_geom full(size_t i) const
+    {
+        petl_geom G = plans[i];
+        petl_geom_set_volume(&G, numX, numY, numZ, voxelWidth, voxelHeight, offsetX, offsetY, offsetZ);
+        return G;
+    }
+    size_t volElems() const { return size_t(numX) * numY * numZ; }
+};
+
+struct Model {
+    Params params;
+};
+
+std::mutex g_mu;
+std::vector<std::unique_ptr<Model>> g_models;
+int g_which = 0;
+
+Model* tomo()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_models.empty()) g_models.emplace_back(new Model);
+    return g_models[size_t(g_which) % g_models.size()].get();
+}
+
+// --- per-device streams for the host-pointer entry points -------------------
+struct DevCtx {
+    cudaStream_t compute = nullptr, copy = nullptr;
+    bool ok = false;
+};
+
+DevCtx* dev_ctx()
+{
+    static std::mutex mu;
+    static DevCtx ctx[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    DevCtx& c = ctx[dev];
+    if (!c.ok) {
+        if (cudaStreamCreateWithFlags(&c.compute, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        if (cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        // keep freed blocks in the stream-ordered pool between calls
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        c.ok = true;
+    }
+    return &c;
+}
+
+bool report(const char* what, int rc)
+{
+    if (rc != 0) {
+        fprintf(stderr, "%s failed: %s\n", what, petl_last_error());
+        return false;
+    }
+    return true;
+}
+
+bool cuda_ok(const char* what, cudaError_t e)
+{
+    if (e != cudaSuccess) {
+        fprintf(stderr, "%s failed: %s\n", what, cudaGetErrorString(e));
+        return false;
+    }
+    return true;
+}
+
+// Scoped device allocation from the stream-ordered pool.
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    bool alloc(size_t bytes, cudaStream_t s)
+    {
+        st = s;
+        return cudaMallocAsync(&p, bytes ? bytes : 4, s) == cudaSuccess;
+    }
+    ~DevBuf()
+    {
+        if (p) cudaFreeAsync(p, st);
+    }
+    float* f() const { return static_cast<float*>(p); }
+};
+
+// v1 slabs per pipeline stage so that one stage moves about 64 MB
+int slab_step(const petl_geom& G)
+{
+    const double slab_bytes = double(G.N_v0) * G.N_u1 * G.N_u0 * 4.0;
+    const int s = int(std::max(1.0, std::floor(64.0e6 / std::max(slab_bytes, 1.0))));
+    return std::min(s, G.N_v1);
+}
+
+// ---------------------------------------------------------------------------
+// host elementwise rules (src/data_cube.cpp:97-166), OpenMP as the reference
+// ---------------------------------------------------------------------------
+enum BinOp { MULT, DIV, RDIV };
+
+bool binop(float* x, float* y, size_t n, BinOp op)
+{
+    const long long N = (long long)n;
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < N; i++) {
+        switch (op) {
+        case MULT: x[i] *= y[i]; break;
+        case DIV: x[i] = (y[i] == 0.0f) ? 0.0f : x[i] / y[i]; break;
+        case RDIV: x[i] = (x[i] == 0.0f) ? 0.0f : y[i] / x[i]; break;
+        }
+    }
+    return true;
+}
+
+float inner(const float* x, const float* y, const float* w, size_t slab, size_t nslab)
+{
+    // per-slab double sums, then a double total (src/data_cube.cpp:360-394)
+    std::vector<double> sums(nslab, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long long s = 0; s < (long long)nslab; s++) {
+        double acc = 0.0;
+        const size_t o = size_t(s) * slab;
+        for (size_t k = 0; k < slab; k++)
+            acc += w ? double(x[o + k] * y[o + k] * w[o + k]) : double(x[o + k] * y[o + k]);
+        sums[s] = acc;
+    }
+    double total = 0.0;
+    for (double v : sums) total += v;
+    return float(total);
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// registry
+// ---------------------------------------------------------------------------
+bool set_model(int i)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_which = i;
+    return true;
+}
+
+int create_new_model(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_models.emplace_back(new Model);
+    g_which = int(g_models.size()) - 1;
+    return g_which;
+}
+
+void about(void)
+{
+    printf("***********************************************************\n");
+    printf("       Planogram Emission Tomography Library (PETL)\n");
+    printf("                 version %s (B200 build)\n", kVersion);
+    printf("***********************************************************\n");
+}
+
+bool copy_parameters(int param_id)
+{
+    Model* cur = tomo();
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (0 <= param_id && param_id < int(g_models.size())) {
+        if (g_which != param_id) cur->params = g_models[param_id]->params;
+        return true;
+    }
+    return false;
+}
+
+void clearAll(void) { tomo()->params.clearAll(); }
+
+void print_parameters(void)
+{
+    const Params& P = tomo()->params;
+    auto x0 = [&](int n, float w, float o) { return float((0.0 - 0.5 * (n - 1)) * w + o); };
+    printf("\n======== PET Volume ========\n");
+    printf("number of voxels (x, y, z): %d x %d x %d\n", P.numX, P.numY, P.numZ);
+    printf("voxel size: %f mm x %f mm x %f mm\n", P.voxelWidth, P.voxelWidth, P.voxelHeight);
+    if (P.offsetX != 0.0 || P.offsetY != 0.0 || P.offsetZ != 0.0)
+        printf("volume offset: %f mm, %f mm, %f mm\n", P.offsetX, P.offsetY, P.offsetZ);
+    printf("FOV: [%f, %f] x [%f, %f] x [%f, %f]\n", x0(P.numX, P.voxelWidth, P.offsetX) - 0.5 * P.voxelWidth,
+           (P.numX - 1) * P.voxelWidth + x0(P.numX, P.voxelWidth, P.offsetX) + 0.5 * P.voxelWidth,
+           x0(P.numY, P.voxelWidth, P.offsetY) - 0.5 * P.voxelWidth,
+           (P.numY - 1) * P.voxelWidth + x0(P.numY, P.voxelWidth, P.offsetY) + 0.5 * P.voxelWidth,
+           x0(P.numZ, P.voxelHeight, P.offsetZ) - 0.5 * P.voxelHeight,
+           (P.numZ - 1) * P.voxelHeight + x0(P.numZ, P.voxelHeight, P.offsetZ) + 0.5 * P.voxelHeight);
+    printf("\n======== PET Geometry ========\n");
+    for (size_t i = 0; i < P.plans.size(); i++) {
+        const petl_geom& p = P.plans[i];
+        printf("Planogram %d\n", int(i));
+        printf("  angle = %f deg\n", p.psi * 180.0 / 3.1415926535897932385);
+        printf("  number of samples: %d x %d x %d x %d\n", p.N_v1, p.N_v0, p.N_u1, p.N_u0);
+        printf("  detector size: %f mm x %f mm\n", p.T_u1, p.T_u0);
+        printf("  full detector length: %f mm\n", 2.0 * p.L);
+        printf("  full detector height: %f mm\n", 2.0 * p.H);
+        printf("  distance between panels: %f mm\n", 2.0 * p.R);
+    }
+    int ndev = 0;
+    cudaGetDeviceCount(&ndev);
+    printf("\n======== Settings ========\nGPUs: %d\n%d CPU threads\n\n", ndev, omp_get_num_procs());
+}
+
+bool volume_defined(void) { return tomo()->params.volumeDefined(); }
+bool geometry_defined(void) { return tomo()->params.geometryDefined(); }
+
+int get_numX(void) { return tomo()->params.numX; }
+bool set_numX(int N) { if (N > 0) { tomo()->params.numX = N; return true; } return false; }
+int get_numY(void) { return tomo()->params.numY; }
+bool set_numY(int N) { if (N > 0) { tomo()->params.numY = N; return true; } return false; }
+int get_numZ(void) { return tomo()->params.numZ; }
+bool set_numZ(int N) { if (N > 0) { tomo()->params.numZ = N; return true; } return false; }
+float get_voxelWidth(void) { return tomo()->params.voxelWidth; }
+bool set_voxelWidth(float w) { if (w > 0.0) { tomo()->params.voxelWidth = w; return true; } return false; }
+float get_voxelHeight(void) { return tomo()->params.voxelHeight; }
+bool set_voxelHeight(float h) { if (h > 0.0) { tomo()->params.voxelHeight = h; return true; } return false; }
+// the reference accepts only positive offsets in these setters
+// (src/petl_c_interface.cpp:154-195); set_volume accepts any offset
+float get_offsetX(void) { return tomo()->params.offsetX; }
+bool set_offsetX(float v) { if (v > 0.0) { tomo()->params.offsetX = v; return true; } return false; }
+float get_offsetY(void) { return tomo()->params.offsetY; }
+bool set_offsetY(float v) { if (v > 0.0) { tomo()->params.offsetY = v; return true; } return false; }
+float get_offsetZ(void) { return tomo()->params.offsetZ; }
+bool set_offsetZ(float v) { if (v > 0.0) { tomo()->params.offsetZ = v; return true; } return false; }
+
+int get_numPlanograms(void) { return int(tomo()->params.plans.size()); }
+
+bool get_planogramSize(int which, int* shape)
+{
+    const Params& P = tomo()->params;
+    if (!P.geometryDefined() || which < 0 || which >= int(P.plans.size()) || shape == nullptr) return false;
+    const petl_geom& p = P.plans[which];
+    shape[0] = p.N_v1;
+    shape[1] = p.N_v0;
+    shape[2] = p.N_u1;
+    shape[3] = p.N_u0;
+    return true;
+}
+
+bool add_planogram(float psi, float R, float L, float H, float v_m0, float v_m1, float T)
+{
+    petl_geom g{};
+    if (petl_geom_init(&g, psi, R, L, H, v_m0, v_m1, T) != 0) return false;
+    tomo()->params.plans.push_back(g);
+    return true;
+}
+
+int petl_model_geometry(int which, petl_geom* out)
+{
+    const Params& P = tomo()->params;
+    if (!out || which < 0 || which >= int(P.plans.size())) return -1;
+    *out = P.volumeDefined(false) ? P.full(size_t(which)) : P.plans[size_t(which)];
+    return 0;
+}
+
+bool remove_planogram(int which)
+{
+    auto& v = tomo()->params.plans;
+    if (which >= 0 && which < int(v.size())) {
+        v.erase(v.begin() + which);
+        return true;
+    }
+    return false;
+}
+
+bool keep_only_planogram(int which)
+{
+    auto& v = tomo()->params.plans;
+    if (which >= 0 && which < int(v.size())) {
+        const petl_geom keep = v[which];
+        v.assign(1, keep);
+        return true;
+    }
+    return false;
+}
+
+bool set_default_volume(float scale)
+{
+    // parameters::set_default_volume (src/parameters.cpp:205-248)
+    Params& P = tomo()->params;
+    if (!P.geometryDefined()) return false;
+    P.offsetX = P.offsetY = P.offsetZ = 0.0f;
+    float X = 0, Y = 0, Z = 0;
+    for (size_t i = 0; i < P.plans.size(); i++) {
+        const petl_geom& p = P.plans[i];
+        const float W = p.L, Hh = p.R;
+        const float Xn = float(std::fabs(W * std::cos(double(p.psi))) + std::fabs(Hh * std::sin(double(p.psi))));
+        const float Yn = float(std::fabs(W * std::sin(double(p.psi))) + std::fabs(Hh * std::cos(double(p.psi))));
+        if (i == 0) {
+            P.voxelWidth = p.T_u0;
+            P.voxelHeight = p.T_u1;
+            Z = p.H;
+            X = Xn;
+            Y = Yn;
+        } else {
+            P.voxelWidth = std::min(P.voxelWidth, p.T_u0);
+            P.voxelHeight = std::min(P.voxelHeight, p.T_u1);
+            Z = std::min(Z, p.H);
+            X = std::min(X, Xn);
+            Y = std::min(Y, Yn);
+        }
+    }
+    P.voxelWidth *= scale;
+    P.voxelHeight *= scale;
+    P.numZ = 2 * int(Z / P.voxelHeight);
+    P.numY = 2 * int(Y / P.voxelWidth);
+    P.numX = 2 * int(X / P.voxelWidth);
+    return true;
+}
+
+bool set_volume(int numX, int numY, int numZ, float voxelWidth, float voxelHeight, float offsetX, float offsetY,
+                float offsetZ)
+{
+    if (numX > 0 && numY > 0 && numZ > 0 && voxelWidth > 0.0 && voxelHeight > 0.0) {
+        Params& P = tomo()->params;
+        P.numX = numX;
+        P.numY = numY;
+        P.numZ = numZ;
+        P.voxelWidth = voxelWidth;
+        P.voxelHeight = voxelHeight;
+        P.offsetX = offsetX;
+        P.offsetY = offsetY;
+        P.offsetZ = offsetZ;
+        return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// outside the reconstruction path
+// ---------------------------------------------------------------------------
+static bool not_here(const char* name)
+{
+    fprintf(stderr, "%s: not provided by this build (outside the reconstruction path)\n", name);
+    return false;
+}
+bool bin(float**, char*) { return not_here("bin"); }
+bool simulate_scatter(float**, float*) { return not_here("simulate_scatter"); }
+bool add_object(int, float*, float*, float, float*, float*) { return not_here("add_object"); }
+bool add_module(int, float*, float*, float, float*, float*) { return not_here("add_module"); }
+bool clear_phantom(void) { return true; }
+bool clear_modules(void) { return true; }
+bool scale_phantom(float, float, float) { return not_here("scale_phantom"); }
+bool voxelize(float*, int) { return not_here("voxelize"); }
+bool ray_trace(float**, int) { return not_here("ray_trace"); }
+bool stopping_power(float**, int) { return not_here("stopping_power"); }
+bool set_solid_angle_correction(float**, bool) { return not_here("set_solid_angle_correction"); }
+bool apply_corrections(float**, float**, float) { return not_here("apply_corrections"); }
+
+// ---------------------------------------------------------------------------
+// projectors
+// ---------------------------------------------------------------------------
+bool project(float** g, float* f)
+{
+    const Params P = tomo()->params;
+    if (g == nullptr || f == nullptr || !P.allDefined()) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok("project", cudaErrorNoDevice);
+    DevBuf df;
+    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
+    if (!cuda_ok("project H2D", cudaMemcpyAsync(df.f(), f, P.volElems() * 4, cudaMemcpyHostToDevice, c->compute)))
+        return false;
+    bool ok = true;
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        const petl_geom G = P.full(i);
+        const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0;
+        DevBuf dg;
+        if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
+        const int step = slab_step(G);
+        for (int b = 0; b < G.N_v1 && ok; b += step) {
+            const int e = std::min(G.N_v1, b + step);
+            ok = report("project", petl_project_range_dev(&G, df.f(), dg.f(), b, e, 0, 1, c->compute));
+            cudaEvent_t ev;
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            cudaEventRecord(ev, c->compute);
+            cudaStreamWaitEvent(c->copy, ev, 0);
+            cudaEventDestroy(ev);
+            ok = ok && cuda_ok("project D2H", cudaMemcpyAsync(g[i] + size_t(b) * slab, dg.f() + size_t(b) * slab,
+                                                              size_t(e - b) * slab * 4, cudaMemcpyDeviceToHost,
+                                                              c->copy));
+        }
+        // the buffer is released on the compute stream: order it after the copies
+        cudaEvent_t done;
+        cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+        cudaEventRecord(done, c->copy);
+        cudaStreamWaitEvent(c->compute, done, 0);
+        cudaEventDestroy(done);
+    }
+    ok = cuda_ok("project sync", cudaStreamSynchronize(c->copy)) && ok;
+    ok = cuda_ok("project sync", cudaStreamSynchronize(c->compute)) && ok;
+    return ok;
+}
+
+static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weight_unused)
+{
+    (void)fbp_weight_unused;
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok("backproject", cudaErrorNoDevice);
+    DevBuf df;
+    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("backproject alloc", cudaGetLastError());
+    bool ok = true;
+    bool first = true;
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        const petl_geom G = P.full(i);
+        const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0;
+        DevBuf dg;
+        if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("backproject alloc", cudaGetLastError());
+        // the copy stream may only start once the buffer exists on the compute stream
+        cudaEvent_t ready;
+        cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+        cudaEventRecord(ready, c->compute);
+        cudaStreamWaitEvent(c->copy, ready, 0);
+        cudaEventDestroy(ready);
+        const int step = slab_step(G);
+        for (int b = 0; b < G.N_v1 && ok; b += step) {
+            const int e = std::min(G.N_v1, b + step);
+            ok = cuda_ok("backproject H2D", cudaMemcpyAsync(dg.f() + size_t(b) * slab, g[i] + size_t(b) * slab,
+                                                            size_t(e - b) * slab * 4, cudaMemcpyHostToDevice,
+                                                            c->copy));
+            cudaEvent_t ev;
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            cudaEventRecord(ev, c->copy);
+            cudaStreamWaitEvent(c->compute, ev, 0);
+            cudaEventDestroy(ev);
+            ok = ok && report("backproject", petl_backproject_range_dev(&G, dg.f(), df.f(), PETL_BP_REFERENCE,
+                                                                        first ? 0 : 1, 1.0f, b, e, 0, 1, c->compute));
+            first = false;
+        }
+    }
+    ok = ok && cuda_ok("backproject D2H",
+                       cudaMemcpyAsync(f, df.f(), P.volElems() * 4, cudaMemcpyDeviceToHost, c->compute));
+    ok = cuda_ok("backproject sync", cudaStreamSynchronize(c->compute)) && ok;
+    return ok;
+}
+
+bool backproject(float** g, float* f)
+{
+    const Params P = tomo()->params;
+    if (g == nullptr || f == nullptr || !P.allDefined()) return false;
+    return backproject_impl(P, g, f, false);
+}
+
+bool FBP(float** g, float* f)
+{
+    const Params P = tomo()->params;
+    if (g == nullptr || f == nullptr || !P.allDefined()) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok("FBP", cudaErrorNoDevice);
+    DevBuf df;
+    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("FBP alloc", cudaGetLastError());
+    bool ok = true;
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        const petl_geom G = P.full(i);
+        const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
+        DevBuf dg;
+        if (!dg.alloc(n * 4, c->compute)) return cuda_ok("FBP alloc", cudaGetLastError());
+        ok = cuda_ok("FBP H2D", cudaMemcpyAsync(dg.f(), g[i], n * 4, cudaMemcpyHostToDevice, c->compute));
+        // already-rebinned data is filtered and weighted in the caller's array,
+        // as the reference does (src/petl.cpp:335-349)
+        float* host_back = G.N_v1 == 1 ? g[i] : nullptr;
+        ok = ok && report("FBP", petl::fbp(G, dg.f(), df.f(), i > 0 ? 1 : 0, c->compute, host_back));
+    }
+    ok = ok && cuda_ok("FBP D2H", cudaMemcpyAsync(f, df.f(), P.volElems() * 4, cudaMemcpyDeviceToHost, c->compute));
+    ok = cuda_ok("FBP sync", cudaStreamSynchronize(c->compute)) && ok;
+    return ok;
+}
+
+bool PFDR(float** g, float** g_reb)
+{
+    Model* m = tomo();
+    const Params P = m->params;
+    if (g == nullptr || g_reb == nullptr || !P.geometryDefined()) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok("PFDR", cudaErrorNoDevice);
+    bool ok = true;
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        petl_geom G = P.plans[i];
+        // PFDR needs no volume; give the geometry check a nominal one
+        petl_geom_set_volume(&G, 1, 1, 1, 1.0f, 1.0f, 0.f, 0.f, 0.f);
+        const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
+        const size_t nr = size_t(G.N_v0) * G.N_u1 * G.N_u0;
+        DevBuf dg, dr;
+        if (!dg.alloc(n * 4, c->compute) || !dr.alloc(nr * 4, c->compute))
+            return cuda_ok("PFDR alloc", cudaGetLastError());
+        ok = cuda_ok("PFDR H2D", cudaMemcpyAsync(dg.f(), g[i], n * 4, cudaMemcpyHostToDevice, c->compute));
+        ok = ok && report("PFDR", petl_pfdr_dev(&G, dg.f(), dr.f(), c->compute));
+        ok = ok && cuda_ok("PFDR D2H", cudaMemcpyAsync(g_reb[i], dr.f(), nr * 4, cudaMemcpyDeviceToHost, c->compute));
+        // PETL::doPFDR rewrites the model's planogram (src/petl.cpp:379-380)
+        m->params.plans[i].N_v1 = 1;
+        m->params.plans[i].v1_0 = 0.0f;
+    }
+    ok = cuda_ok("PFDR sync", cudaStreamSynchronize(c->compute)) && ok;
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// elementwise on host arrays (src/petl_c_interface.cpp:313-469)
+// ---------------------------------------------------------------------------
+bool multiply3D(float* x, float* y, int N_1, int N_2, int N_3)
+{
+    if (!x || !y || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) { printf("multiply invalid inputs\n"); return false; }
+    return binop(x, y, size_t(N_1) * N_2 * N_3, MULT);
+}
+bool multiply4D(float* x, float* y, int N_1, int N_2, int N_3, int N_4)
+{
+    if (!x || !y || N_1 <= 0 || N_2 <= 0 || N_3 <= 0 || N_4 <= 0) { printf("multiply invalid inputs\n"); return false; }
+    return binop(x, y, size_t(N_1) * N_2 * N_3 * N_4, MULT);
+}
+bool divide3D(float* x, float* y, int N_1, int N_2, int N_3)
+{
+    if (!x || !y || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) { printf("divide invalid inputs\n"); return false; }
+    return binop(x, y, size_t(N_1) * N_2 * N_3, DIV);
+}
+bool divide4D(float* x, float* y, int N_1, int N_2, int N_3, int N_4)
+{
+    if (!x || !y || N_1 <= 0 || N_2 <= 0 || N_3 <= 0 || N_4 <= 0) { printf("divide invalid inputs\n"); return false; }
+    return binop(x, y, size_t(N_1) * N_2 * N_3 * N_4, DIV);
+}
+bool rdivide3D(float* num, float* denom, int N_1, int N_2, int N_3)
+{
+    if (!num || !denom || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) { printf("rdivide invalid inputs\n"); return false; }
+    return binop(denom, num, size_t(N_1) * N_2 * N_3, RDIV);
+}
+bool rdivide4D(float* num, float* denom, int N_1, int N_2, int N_3, int N_4)
+{
+    if (!num || !denom || N_1 <= 0 || N_2 <= 0 || N_3 <= 0 || N_4 <= 0) { printf("rdivide invalid inputs\n"); return false; }
+    return binop(denom, num, size_t(N_1) * N_2 * N_3 * N_4, RDIV);
+}
+static bool recip(float* x, size_t n, float v)
+{
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)n; i++) x[i] = (x[i] == 0.0f) ? v : float(1.0 / x[i]);
+    return true;
+}
+bool reciprocal3D(float* x, int N_1, int N_2, int N_3, float v)
+{
+    if (!x || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) { printf("rdivide invalid inputs\n"); return false; }
+    return recip(x, size_t(N_1) * N_2 * N_3, v);
+}
+bool reciprocal4D(float* x, int N_1, int N_2, int N_3, int N_4, float v)
+{
+    if (!x || N_1 <= 0 || N_2 <= 0 || N_3 <= 0 || N_4 <= 0) { printf("rdivide invalid inputs\n"); return false; }
+    return recip(x, size_t(N_1) * N_2 * N_3 * N_4, v);
+}
+float inner_product3D(float* x, float* y, float* w, int N_1, int N_2, int N_3)
+{
+    if (!x || !y || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) { printf("inner_product invalid inputs\n"); return 0.0f; }
+    return inner(x, y, w, size_t(N_2) * N_3, size_t(N_1));
+}
+float inner_product4D(float* x, float* y, float* w, int N_1, int N_2, int N_3, int N_4)
+{
+    if (!x || !y || N_1 <= 0 || N_2 <= 0 || N_3 <= 0 || N_4 <= 0) { printf("inner_product invalid inputs\n"); return 0.0f; }
+    // 4D: per 3D block a float result summed in double (src/data_cube.cpp:340-357)
+    double acc = 0.0;
+    const size_t blk = size_t(N_2) * N_3 * N_4;
+    for (int i = 0; i < N_1; i++)
+        acc += double(inner(x + i * blk, y + i * blk, w ? w + i * blk : nullptr, size_t(N_3) * N_4, size_t(N_2)));
+    return float(acc);
+}
+
+// ---------------------------------------------------------------------------
+// regularizers (src/petl_c_interface.cpp:487-531)
+// ---------------------------------------------------------------------------
+namespace {
+struct Staged {
+    // device copies of host arrays (or the caller's device pointers)
+    float* d = nullptr;
+    DevBuf buf;
+    bool stage(float* p, size_t n, bool on_cpu, cudaStream_t st, bool copy_in = true)
+    {
+        if (!on_cpu) {
+            d = p;
+            return true;
+        }
+        if (!buf.alloc(n * 4, st)) return false;
+        d = buf.f();
+        return !copy_in || cudaMemcpyAsync(d, p, n * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    }
+};
+double read_scalar(double* dptr, cudaStream_t st)
+{
+    double h = 0.0;
+    cudaMemcpyAsync(&h, dptr, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return h;
+}
+}  // namespace
+
+float TV_cost(float* f, int N_1, int N_2, int N_3, float delta, float beta, float p, bool data_on_cpu)
+{
+    if (!f) return -1.0f;
+    DevCtx* c = dev_ctx();
+    if (!c) return -1.0f;
+    const size_t n = size_t(N_1) * N_2 * N_3;
+    Staged sf;
+    DevBuf out;
+    if (!sf.stage(f, n, data_on_cpu, c->compute) || !out.alloc(8, c->compute)) return -1.0f;
+    if (!report("TV_cost", petl_tv_cost_dev(sf.d, N_1, N_2, N_3, delta, beta, p, 26, (double*)out.p, c->compute)))
+        return -1.0f;
+    return float(read_scalar((double*)out.p, c->compute));
+}
+
+bool TV_gradient(float* f, float* Df, int N_1, int N_2, int N_3, float delta, float beta, float p, bool data_on_cpu)
+{
+    if (!f || !Df) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return false;
+    const size_t n = size_t(N_1) * N_2 * N_3;
+    Staged sf, sd;
+    if (!sf.stage(f, n, data_on_cpu, c->compute) || !sd.stage(Df, n, data_on_cpu, c->compute, false)) return false;
+    bool ok = report("TV_gradient", petl_tv_gradient_dev(sf.d, sd.d, N_1, N_2, N_3, delta, beta, p, 26, c->compute));
+    if (ok && data_on_cpu) ok = cuda_ok("TV_gradient D2H", cudaMemcpyAsync(Df, sd.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    return cuda_ok("TV_gradient sync", cudaStreamSynchronize(c->compute)) && ok;
+}
+
+float TV_quadForm(float* f, float* d, int N_1, int N_2, int N_3, float delta, float beta, float p, bool data_on_cpu)
+{
+    if (!f || !d) return -1.0f;
+    DevCtx* c = dev_ctx();
+    if (!c) return -1.0f;
+    const size_t n = size_t(N_1) * N_2 * N_3;
+    Staged sf, sd;
+    DevBuf out;
+    if (!sf.stage(f, n, data_on_cpu, c->compute) || !sd.stage(d, n, data_on_cpu, c->compute) || !out.alloc(8, c->compute))
+        return -1.0f;
+    if (!report("TV_quadForm",
+                petl_tv_quadform_dev(sf.d, sd.d, N_1, N_2, N_3, delta, beta, p, 26, (double*)out.p, c->compute)))
+        return -1.0f;
+    return float(read_scalar((double*)out.p, c->compute));
+}
+
+// gradient-descent TV smoothing / denoising (src/total_variation.cu:813-935)
+static bool tv_iterate(float* f, int N_1, int N_2, int N_3, float delta, float beta, float p, int numIter,
+                       bool data_on_cpu, bool denoise)
+{
+    if (!f) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return false;
+    if (delta < 1.0e-8) delta = float(1.0e-8);
+    const size_t n = size_t(N_1) * N_2 * N_3;
+    Staged sf;
+    DevBuf dd, f0, sc;
+    if (!sf.stage(f, n, data_on_cpu, c->compute) || !dd.alloc(n * 4, c->compute) || !sc.alloc(16, c->compute))
+        return false;
+    if (denoise) {
+        if (!f0.alloc(n * 4, c->compute)) return false;
+        cudaMemcpyAsync(f0.p, sf.d, n * 4, cudaMemcpyDeviceToDevice, c->compute);
+    }
+    bool ok = true;
+    for (int it = 0; it < numIter && ok; it++) {
+        ok = report("tv", petl_tv_gradient_dev(sf.d, dd.f(), N_1, N_2, N_3, delta, beta, p, 26, c->compute));
+        ok = ok && report("tv", petl_dot_dev(dd.f(), dd.f(), nullptr, (long long)n, (double*)sc.p, c->compute));
+        ok = ok && report("tv", petl_tv_quadform_dev(sf.d, dd.f(), N_1, N_2, N_3, delta, beta, p, 26,
+                                                     (double*)sc.p + 1, c->compute));
+        if (!ok) break;
+        double h[2];
+        cudaMemcpyAsync(h, sc.p, 16, cudaMemcpyDeviceToHost, c->compute);
+        cudaStreamSynchronize(c->compute);
+        const float num = float(h[0]), den = float(h[1]);
+        if (den <= 1.0e-16) break;
+        const float step = num / den;
+        // f <- f - step*d  (diffuse);  f <- (1-step) f - step (d - f0)  (denoise)
+        if (denoise) {
+            ok = report("tv", petl_axpby_dev(sf.d, dd.f(), 1.0f - step, -step, (long long)n, c->compute));
+            ok = ok && report("tv", petl_axpby_dev(sf.d, f0.f(), 1.0f, step, (long long)n, c->compute));
+        } else {
+            ok = report("tv", petl_axpby_dev(sf.d, dd.f(), 1.0f, -step, (long long)n, c->compute));
+        }
+    }
+    if (ok && data_on_cpu) ok = cuda_ok("tv D2H", cudaMemcpyAsync(f, sf.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    return cuda_ok("tv sync", cudaStreamSynchronize(c->compute)) && ok;
+}
+
+bool diffuse(float* f, int N_1, int N_2, int N_3, float delta, float p, int numIter, bool data_on_cpu)
+{
+    return tv_iterate(f, N_1, N_2, N_3, delta, 1.0f, p, numIter, data_on_cpu, false);
+}
+
+bool TV_denoise(float* f, int N_1, int N_2, int N_3, float delta, float beta, float p, int numIter, bool doMean,
+                bool data_on_cpu)
+{
+    (void)doMean;  // the reference C ABI does not forward it (src/petl_c_interface.cpp:511-515)
+    return tv_iterate(f, N_1, N_2, N_3, delta, beta, p, numIter, data_on_cpu, true);
+}
+
+bool relativeDifferences_gradient(float* f, float* Df, int N_1, int N_2, int N_3, float delta, float beta)
+{
+    if (f == nullptr || Df == nullptr || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return false;
+    const size_t n = size_t(N_1) * N_2 * N_3;
+    Staged sf, sd;
+    if (!sf.stage(f, n, true, c->compute) || !sd.stage(Df, n, true, c->compute, false)) return false;
+    bool ok = report("relativeDifferences_gradient",
+                     petl_rd_gradient_dev(sf.d, sd.d, N_1, N_2, N_3, delta, beta, c->compute));
+    ok = ok && cuda_ok("rd D2H", cudaMemcpyAsync(Df, sd.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    return cuda_ok("rd sync", cudaStreamSynchronize(c->compute)) && ok;
+}
+
+bool gaussian_filter(float* f, int N_1, int N_2, int N_3, float FWHM, int numDims)
+{
+    if (f == nullptr || N_1 <= 0 || N_2 <= 0 || N_3 <= 0) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return false;
+    const size_t n = size_t(N_1) * N_2 * N_3;
+    Staged sf;
+    if (!sf.stage(f, n, true, c->compute)) return false;
+    bool ok = report("gaussian_filter", petl_gaussian_filter_dev(sf.d, N_1, N_2, N_3, FWHM, numDims, c->compute));
+    ok = ok && cuda_ok("gauss D2H", cudaMemcpyAsync(f, sf.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    return cuda_ok("gauss sync", cudaStreamSynchronize(c->compute)) && ok;
+}
+
+}  // extern "C"

@@ -27,9 +27,13 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
         }                                                                                \
     } while (0)
 
-// Checks the launch that was just issued.
+// Counts kernel launches issued by the library (petl_launch_count()).
+void note_launch();
+
+// Checks the launch that was just issued (and counts it).
 #define PETL_LAUNCH_CHECK(name)                                                          \
     do {                                                                                 \
+        ::petl::note_launch();                                                           \
         cudaError_t e_ = cudaGetLastError();                                             \
         if (e_ != cudaSuccess) {                                                         \
             ::petl::set_error(std::string(name) + " launch: " + cudaGetErrorString(e_)); \

@@ -1,0 +1,199 @@
+// Device-pointer entry points (petl_device.h) and kernel dispatch.
+//
+// The projector entry points choose between the shear kernels of
+// projector_shear.cu (axis-aligned planograms whose voxel pitch equals the bin
+// pitch: every benchmark configuration) and the general kernels of
+// projector_general.cu (any orientation and pitch).  Both compute the same
+// operator; the dispatch only changes how fast.
+#include <cmath>
+#include <string>
+
+#include "common.cuh"
+#include "projector.cuh"
+
+namespace petl {
+int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st);
+int ramp(const petl_geom& G, float* g_reb, int apply_weight, cudaStream_t st);
+int launch_gaussian(float* f, int N1, int N2, int N3, float FWHM, int numDims, cudaStream_t st);
+
+// shear fast path (projector_shear.cu)
+bool shear_eligible(const petl_geom& G);
+int launch_project_shear(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                         cudaStream_t st);
+int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                             const ViewRange& vr, cudaStream_t st);
+
+int g_force_general = -1;  // -1: read PETL_FORCE_GENERAL once
+
+bool use_shear(const petl_geom& G)
+{
+    if (g_force_general < 0) {
+        const char* e = getenv("PETL_FORCE_GENERAL");
+        g_force_general = (e && e[0] == '1') ? 1 : 0;
+    }
+    return !g_force_general && shear_eligible(G);
+}
+
+bool range_ok(const petl_geom& G, const ViewRange& vr)
+{
+    return vr.iv1_begin >= 0 && vr.iv1_end <= G.N_v1 && vr.iv1_begin <= vr.iv1_end && vr.iv0_first >= 0 &&
+           vr.iv0_step >= 1;
+}
+
+int project_range(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                  cudaStream_t st)
+{
+    std::string why;
+    PETL_REQUIRE(geom_valid(&G, &why), "project: " + why);
+    PETL_REQUIRE(f && g && range_ok(G, vr), "project: invalid arguments");
+    if (vr.iv1_begin == vr.iv1_end || vr.iv0_first >= G.N_v0) return 0;
+    if (use_shear(G)) return launch_project_shear(G, f, g, vr, meas, st);
+    return launch_project_general(G, f, g, vr, meas, st);
+}
+
+int backproject_range(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                      const ViewRange& vr, cudaStream_t st)
+{
+    std::string why;
+    PETL_REQUIRE(geom_valid(&G, &why), "backproject: " + why);
+    PETL_REQUIRE(f && g && range_ok(G, vr), "backproject: invalid arguments");
+    PETL_REQUIRE(mode == PETL_BP_REFERENCE || mode == PETL_BP_ADJOINT, "backproject: unknown mode");
+    if (use_shear(G)) return launch_backproject_shear(G, g, f, mode, accumulate, scale, vr, st);
+    return launch_backproject_general(G, g, f, mode, accumulate, scale, vr, st);
+}
+
+int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream_t st, float* host_rebinned_out)
+{
+    std::string why;
+    PETL_REQUIRE(geom_valid(&G, &why), "FBP: " + why);
+    petl_geom Gr = G;
+    const size_t nreb = size_t(G.N_v0) * G.N_u1 * G.N_u0;
+    float* reb = nullptr;
+    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&reb), sizeof(float) * nreb, st));
+    int rc = 0;
+    if (G.N_v1 > 1) {
+        // PETL::doFBP -> doPFDR, then the rebinned geometry (src/petl.cpp:379-380)
+        rc = pfdr(G, g, reb, st);
+        Gr.N_v1 = 1;
+        Gr.v1_0 = 0.0f;
+    } else {
+        cudaError_t e = cudaMemcpyAsync(reb, g, sizeof(float) * nreb, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) {
+            set_error(std::string("FBP: ") + cudaGetErrorString(e));
+            rc = int(e);
+        }
+    }
+    if (!rc) rc = ramp(Gr, reb, 1, st);
+    if (!rc && host_rebinned_out) {
+        cudaError_t e = cudaMemcpyAsync(host_rebinned_out, reb, sizeof(float) * nreb, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = int(e);
+    }
+    // FBPweight scale T_v0*T_u0/voxelWidth (src/petl.cpp:254-259), float
+    const float scale = Gr.T_v0 * Gr.T_u0 / Gr.T_x;
+    if (!rc) rc = backproject_range(Gr, reb, f, PETL_BP_REFERENCE, accumulate, scale, ViewRange{0, 1, 0, 1}, st);
+    cudaFreeAsync(reb, st);
+    return rc;
+}
+
+}  // namespace petl
+
+using namespace petl;
+
+extern "C" {
+
+int petl_project_dev(const petl_geom* G, const float* f, float* g, int iv0_first, int iv0_step, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(G, "project: null geometry");
+    return project_range(*G, f, g, ViewRange{0, G->N_v1, iv0_first, iv0_step}, nullptr, as_stream(stream));
+}
+
+int petl_project_range_dev(const petl_geom* G, const float* f, float* g, int iv1_begin, int iv1_end, int iv0_first,
+                           int iv0_step, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(G, "project: null geometry");
+    return project_range(*G, f, g, ViewRange{iv1_begin, iv1_end, iv0_first, iv0_step}, nullptr, as_stream(stream));
+}
+
+int petl_project_ratio_dev(const petl_geom* G, const float* f, const float* meas, float* ratio, int iv1_begin,
+                           int iv1_end, int iv0_first, int iv0_step, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(G && meas, "project_ratio: invalid arguments");
+    return project_range(*G, f, ratio, ViewRange{iv1_begin, iv1_end, iv0_first, iv0_step}, meas, as_stream(stream));
+}
+
+int petl_backproject_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
+                         int iv0_first, int iv0_step, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(G, "backproject: null geometry");
+    return backproject_range(*G, g, f, mode, accumulate, scale, ViewRange{0, G->N_v1, iv0_first, iv0_step},
+                             as_stream(stream));
+}
+
+int petl_backproject_range_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
+                               int iv1_begin, int iv1_end, int iv0_first, int iv0_step, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(G, "backproject: null geometry");
+    return backproject_range(*G, g, f, mode, accumulate, scale, ViewRange{iv1_begin, iv1_end, iv0_first, iv0_step},
+                             as_stream(stream));
+}
+
+int petl_project_nnz_dev(const petl_geom* G, double* nnz_host, void* stream)
+{
+    clear_error();
+    std::string why;
+    PETL_REQUIRE(G && nnz_host && geom_valid(G, &why), "project_nnz: invalid arguments " + why);
+    cudaStream_t st = as_stream(stream);
+    unsigned long long* d = nullptr;
+    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(unsigned long long), st));
+    PETL_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), st));
+    int rc = launch_count_nnz(*G, d, st);
+    unsigned long long h = 0;
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            set_error(std::string("project_nnz: ") + cudaGetErrorString(e));
+            rc = int(e);
+        }
+    }
+    cudaFreeAsync(d, st);
+    *nnz_host = double(h);
+    return rc;
+}
+
+int petl_pfdr_dev(const petl_geom* G, const float* g, float* g_reb, void* stream)
+{
+    clear_error();
+    std::string why;
+    PETL_REQUIRE(G && g && g_reb && geom_valid(G, &why), "PFDR: invalid arguments " + why);
+    return pfdr(*G, g, g_reb, as_stream(stream));
+}
+
+int petl_ramp_dev(const petl_geom* G, float* g_reb, int apply_weight, void* stream)
+{
+    clear_error();
+    std::string why;
+    PETL_REQUIRE(G && g_reb && geom_valid(G, &why), "ramp: invalid arguments " + why);
+    return ramp(*G, g_reb, apply_weight, as_stream(stream));
+}
+
+int petl_fbp_dev(const petl_geom* G, const float* g, float* f, int accumulate, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(G && g && f, "FBP: invalid arguments");
+    return fbp(*G, g, f, accumulate, as_stream(stream), nullptr);
+}
+
+int petl_gaussian_filter_dev(float* f, int N1, int N2, int N3, float FWHM, int numDims, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(f && N1 > 0 && N2 > 0 && N3 > 0, "gaussian_filter: invalid arguments");
+    return launch_gaussian(f, N1, N2, N3, FWHM, numDims, as_stream(stream));
+}
+
+}  // extern "C"

@@ -6,6 +6,7 @@
 // float storage and double intermediates so that the sample counts and
 // start values come out bit-identical.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -18,6 +19,9 @@ namespace {
 thread_local std::string g_last_error;
 }
 
+std::atomic<unsigned long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void set_error(const std::string& msg) { g_last_error = msg; }
 void clear_error() { g_last_error.clear(); }
 
@@ -58,6 +62,8 @@ extern "C" {
 const char* petl_last_error(void) { return petl::g_last_error.c_str(); }
 
 int petl_version(void) { return 100; }
+
+unsigned long long petl_launch_count(void) { return petl::g_launches.load(std::memory_order_relaxed); }
 
 int petl_optimal_fft_size(int N)
 {

@@ -1,0 +1,384 @@
+// PFDR rebinning, ramp filter and FBP.
+//
+// PFDR (reference src/pfdr.cu:43-315).  The reference zero-pads every
+// (v1, u1) slice to NY x NX = optimalFFTsize(N_v0) x optimalFFTsize(N_u0),
+// takes a 2-D R2C transform, accumulates over v1 the spectra whose
+// u0-frequency passes the mask  |v1| <= T_v1/2  or  |U| > |v1|/(4 T_u1 v_m0)
+// (the oblique u1 index of line 107 is u1 itself, so no sample moves),
+// normalises by 1/(NY*NX*count(U)) (count not applied at U = 0), inverts
+// with a 2-D C2R and crops.  The mask and the normalisation depend only on
+// the u0-frequency, so the transform along v0 is applied and then exactly
+// undone; it contributes nothing but a factor NY.  This file therefore runs
+// the same arithmetic with 1-D transforms along u0 only: one pass over the
+// planogram, every row transformed once, spectra accumulated in shared
+// memory, one inverse transform per output row.  Transforms are hand-written
+// mixed radix-4/2/3 Stockham FFTs in shared memory (all optimalFFTsize values
+// are 2^a 3^b).  The masks, counts and per-row weights are computed on the
+// host with the reference's float expressions.
+//
+// Ramp filter (src/ramp_filter.cu:24-76,156-348).  The reference multiplies
+// the zero-padded (N_H >= 2 N_u0) row spectrum by Re(FFT(h))/N_H with
+// h[s] = 1/(T pi (1/4 - s^2)); since h is circularly symmetric and the
+// padding leaves no wrap-around, that is exactly the linear convolution of
+// the row with h.  It is computed here as a direct convolution in shared
+// memory (N_u0^2 FMAs per row, a few microseconds for the whole planogram),
+// fused with the inverse planogram weight that PETL::doFBP applies next
+// (src/planogram.cpp:304-333).
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "projector.cuh"
+
+namespace petl {
+
+namespace {
+
+constexpr int kPfdrRows = 8;     // planogram rows (u1) per CTA, packed two per complex FFT
+constexpr int kPfdrThreads = 128;
+constexpr int kMaxFFT = 2048;
+constexpr int kMaxStages = 12;
+
+struct FFTPlan {
+    int n;
+    int nstages;
+    int radix[kMaxStages];
+};
+
+FFTPlan make_plan(int n)
+{
+    FFTPlan p{};
+    p.n = n;
+    int m = n;
+    while (m % 4 == 0) { p.radix[p.nstages++] = 4; m /= 4; }
+    while (m % 2 == 0) { p.radix[p.nstages++] = 2; m /= 2; }
+    while (m % 3 == 0) { p.radix[p.nstages++] = 3; m /= 3; }
+    p.nstages = m == 1 ? p.nstages : -1;
+    return p;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Batched complex FFTs of length plan.n on nb contiguous sequences in shared
+// memory.  'a' holds the input and receives the output (b is scratch).
+// tw[m] = exp(-2 pi i m / n); sign = -1 forward, +1 inverse (unnormalised).
+__device__ void smem_fft(float2* a, float2* b, const float2* tw, const FFTPlan& plan, int nb, int sign)
+{
+    const int n = plan.n;
+    int Ns = 1;
+    float2* src = a;
+    float2* dst = b;
+    for (int s = 0; s < plan.nstages; s++) {
+        const int R = plan.radix[s];
+        const int nbf = n / R;
+        const int twstep = n / (Ns * R);
+        for (int t = threadIdx.x; t < nb * nbf; t += blockDim.x) {
+            const int seq = t / nbf, j = t - seq * nbf;
+            const float2* in = src + seq * n;
+            float2* out = dst + seq * n;
+            const int k = j % Ns;
+            float2 v[4];
+            for (int r = 0; r < R; r++) {
+                float2 x = in[j + r * nbf];
+                if (r && k) {
+                    float2 w = tw[(r * k * twstep) % n];
+                    w.y *= float(-sign);  // tw is the forward table; conjugate for the inverse
+                    x = cmul(x, w);
+                }
+                v[r] = x;
+            }
+            float2 V[4];
+            if (R == 2) {
+                V[0] = make_float2(v[0].x + v[1].x, v[0].y + v[1].y);
+                V[1] = make_float2(v[0].x - v[1].x, v[0].y - v[1].y);
+            } else if (R == 4) {
+                const float2 s02 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+                const float2 d02 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+                const float2 s13 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+                const float2 d13 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+                // multiply d13 by (sign * i)
+                const float2 jd13 = make_float2(-float(sign) * d13.y, float(sign) * d13.x);
+                V[0] = make_float2(s02.x + s13.x, s02.y + s13.y);
+                V[2] = make_float2(s02.x - s13.x, s02.y - s13.y);
+                V[1] = make_float2(d02.x + jd13.x, d02.y + jd13.y);
+                V[3] = make_float2(d02.x - jd13.x, d02.y - jd13.y);
+            } else {  // R == 3
+                const float c = -0.5f, sn = float(sign) * 0.86602540378443864676f;
+                const float2 s12 = make_float2(v[1].x + v[2].x, v[1].y + v[2].y);
+                const float2 d12 = make_float2(v[1].x - v[2].x, v[1].y - v[2].y);
+                V[0] = make_float2(v[0].x + s12.x, v[0].y + s12.y);
+                const float2 m = make_float2(v[0].x + c * s12.x, v[0].y + c * s12.y);
+                // sn * i * d12
+                const float2 jd = make_float2(-sn * d12.y, sn * d12.x);
+                V[1] = make_float2(m.x + jd.x, m.y + jd.y);
+                V[2] = make_float2(m.x - jd.x, m.y - jd.y);
+            }
+            const int idx = (j / Ns) * Ns * R + k;
+            for (int r = 0; r < R; r++) out[idx + r * Ns] = V[r];
+        }
+        __syncthreads();
+        float2* tmp = src;
+        src = dst;
+        dst = tmp;
+        Ns *= R;
+    }
+    // result must end in 'a'
+    if (src != a) {
+        for (int t = threadIdx.x; t < nb * n; t += blockDim.x) a[t] = src[t];
+        __syncthreads();
+    }
+}
+
+struct PfdrArgs {
+    const float* g;
+    float* g_reb;
+    int N_v1, N_v0, N_u1, N_u0;
+    int NX;
+    const float* row_w;    // [N_v1][N_v0] 1/sqrt(1+v1^2+v0^2)
+    const float* absU;     // [NXH] |U(i)|
+    const float* v1ap;     // [N_v1] |v1| * apertureConstant
+    const unsigned char* central;  // [N_v1] |v1| <= T_v1/2
+    const float* norm;     // [NXH] 1/(NX * count(U)) (count omitted at U = 0)
+    const float* out_w;    // [N_v0] sqrt(1+v0^2)
+    const float2* tw;      // [NX] forward twiddles
+    FFTPlan plan;
+};
+
+__global__ void __launch_bounds__(kPfdrThreads) k_pfdr(const PfdrArgs A)
+{
+    extern __shared__ float2 sm[];
+    const int NX = A.NX, NXH = NX / 2 + 1;
+    constexpr int NB = kPfdrRows / 2;  // complex sequences
+    float2* buf = sm;                  // NB * NX
+    float2* tmp = buf + NB * NX;       // NB * NX
+    float2* acc = tmp + NB * NX;       // kPfdrRows * NXH
+    float2* tw = acc + kPfdrRows * NXH;  // NX
+    float* absU = reinterpret_cast<float*>(tw + NX);  // NXH
+    const int iv0 = blockIdx.x;
+    const int iu1_0 = blockIdx.y * kPfdrRows;
+    const int nrows = min(kPfdrRows, A.N_u1 - iu1_0);
+    for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = A.tw[i];
+    for (int i = threadIdx.x; i < NXH; i += blockDim.x) absU[i] = A.absU[i];
+    for (int i = threadIdx.x; i < kPfdrRows * NXH; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+    __syncthreads();
+    const size_t slab = size_t(A.N_v0) * A.N_u1 * A.N_u0;
+    for (int iv1 = 0; iv1 < A.N_v1; iv1++) {
+        const float w = A.row_w[iv1 * A.N_v0 + iv0];
+        const float* src = A.g + iv1 * slab + (size_t(iv0) * A.N_u1 + iu1_0) * A.N_u0;
+        // rows 2q (real part) and 2q+1 (imaginary part) of sequence q
+        for (int t = threadIdx.x; t < NB * NX; t += blockDim.x) {
+            const int q = t / NX, i = t - q * NX;
+            float re = 0.f, im = 0.f;
+            if (i < A.N_u0) {
+                if (2 * q < nrows) re = __ldg(&src[size_t(2 * q) * A.N_u0 + i]) * w;
+                if (2 * q + 1 < nrows) im = __ldg(&src[size_t(2 * q + 1) * A.N_u0 + i]) * w;
+            }
+            buf[t] = make_float2(re, im);
+        }
+        __syncthreads();
+        smem_fft(buf, tmp, tw, A.plan, NB, -1);
+        // split the two real spectra and accumulate the masked bins
+        const bool cen = A.central[iv1] != 0;
+        const float thr = A.v1ap[iv1];
+        for (int t = threadIdx.x; t < NB * NXH; t += blockDim.x) {
+            const int q = t / NXH, k = t - q * NXH;
+            if (!(cen || absU[k] > thr)) continue;
+            const float2 z = buf[q * NX + k];
+            const float2 zc = buf[q * NX + (k == 0 ? 0 : NX - k)];
+            // X0 = (Z + conj(Zc))/2, X1 = (Z - conj(Zc))/(2i)
+            const float2 x0 = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+            const float2 x1 = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+            float2& a0 = acc[(2 * q) * NXH + k];
+            float2& a1 = acc[(2 * q + 1) * NXH + k];
+            a0.x += x0.x; a0.y += x0.y;
+            a1.x += x1.x; a1.y += x1.y;
+        }
+        __syncthreads();
+    }
+    // normalise and pack pairs of rows into one inverse transform
+    for (int t = threadIdx.x; t < NB * NX; t += blockDim.x) {
+        const int q = t / NX, k = t - q * NX;
+        const int kk = k <= NX / 2 ? k : NX - k;
+        float2 a = acc[(2 * q) * NXH + kk], b = acc[(2 * q + 1) * NXH + kk];
+        const float nr = A.norm[kk];
+        a.x *= nr; a.y *= nr; b.x *= nr; b.y *= nr;
+        if (kk == 0 || 2 * kk == NX) { a.y = 0.f; b.y = 0.f; }  // C2R ignores these
+        if (k > NX / 2) { a.y = -a.y; b.y = -b.y; }             // Hermitian extension
+        buf[t] = make_float2(a.x - b.y, a.y + b.x);             // A + iB
+    }
+    __syncthreads();
+    smem_fft(buf, tmp, tw, A.plan, NB, +1);
+    const float ow = A.out_w[iv0];
+    for (int t = threadIdx.x; t < nrows * A.N_u0; t += blockDim.x) {
+        const int r = t / A.N_u0, i = t - r * A.N_u0;
+        const float2 z = buf[(r >> 1) * NX + i];
+        const float v = (r & 1) ? z.y : z.x;
+        A.g_reb[(size_t(iv0) * A.N_u1 + iu1_0 + r) * A.N_u0 + i] = v * ow;
+    }
+}
+
+// direct convolution of every row with the ramp kernel, times a per-view weight
+constexpr int kRampRows = 8;
+__global__ void __launch_bounds__(256)
+k_ramp(float* __restrict__ g, int nrows, int N, int rows_per_view, const float* __restrict__ h,
+       const float* __restrict__ view_w)
+{
+    extern __shared__ float rs[];
+    float* hs = rs;              // 2N-1 taps, hs[N-1+s] = h(s)
+    float* xs = hs + 2 * N - 1;  // kRampRows * N
+    const int r0 = blockIdx.x * kRampRows;
+    const int nr = min(kRampRows, nrows - r0);
+    for (int i = threadIdx.x; i < 2 * N - 1; i += blockDim.x) hs[i] = h[i];
+    for (int i = threadIdx.x; i < kRampRows * N; i += blockDim.x) {
+        const int r = i / N;
+        xs[i] = r < nr ? g[size_t(r0 + r) * N + (i - r * N)] : 0.0f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        float acc[kRampRows];
+#pragma unroll
+        for (int r = 0; r < kRampRows; r++) acc[r] = 0.f;
+        for (int k = 0; k < N; k++) {
+            const float hv = hs[N - 1 + i - k];
+#pragma unroll
+            for (int r = 0; r < kRampRows; r++) acc[r] = fmaf(xs[r * N + k], hv, acc[r]);
+        }
+        for (int r = 0; r < nr; r++) {
+            const int row = r0 + r;
+            g[size_t(row) * N + i] = acc[r] * view_w[row / rows_per_view];
+        }
+    }
+}
+
+template <class T>
+int upload(const std::vector<T>& v, T** d, cudaStream_t st)
+{
+    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d), sizeof(T) * v.size(), st));
+    PETL_CUDA(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+    return 0;
+}
+
+// host float helpers that must not be contracted into fused multiply-adds
+// (the reference computes these on the host with separate roundings)
+__attribute__((noinline)) float fmul_h(float a, float b) { return a * b; }
+__attribute__((noinline)) float fadd_h(float a, float b) { return a + b; }
+
+}  // namespace
+
+int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
+{
+    const int NX = petl_optimal_fft_size(G.N_u0);
+    const FFTPlan plan = make_plan(NX);
+    PETL_REQUIRE(plan.nstages > 0 && NX <= kMaxFFT, "PFDR: unsupported transform size");
+    const int NXH = NX / 2 + 1;
+    // tables (src/pfdr.cu:16-40, 78-124, 126-142, 144-157)
+    const float T_U = float(1.0 / (NX * G.T_u0));
+    const float aperture = float(1 / (2.0 * G.T_u1 * 2.0 * G.v_m0));
+    std::vector<float> absU(NXH), v1ap(G.N_v1), row_w(size_t(G.N_v1) * G.N_v0), norm(NXH), out_w(G.N_v0);
+    std::vector<unsigned char> central(G.N_v1);
+    std::vector<float2> tw(NX);
+    for (int i = 0; i < NXH; i++) {
+        const float U = i < NX / 2 ? fmul_h(float(i), T_U) : fmul_h(float(i - NX), T_U);
+        absU[i] = std::fabs(U);
+    }
+    std::vector<int> count(NXH, 0);
+    for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
+        const float v1 = fadd_h(fmul_h(float(iv1), G.T_v1), G.v1_0);  // planogram::v1 on the host
+        const float av = std::fabs(v1);
+        central[iv1] = av <= fmul_h(0.5f, G.T_v1);
+        v1ap[iv1] = fmul_h(av, aperture);
+        for (int i = 0; i < NXH; i++)
+            if (central[iv1] || absU[i] > v1ap[iv1]) count[i]++;
+        for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+            const float v0 = std::fmaf(G.T_v0, float(iv0), G.v0_0);  // device expression, contracted
+            row_w[size_t(iv1) * G.N_v0 + iv0] = float(1.0 / std::sqrt(1.0 + double(v1) * v1 + double(v0) * v0));
+        }
+    }
+    for (int i = 0; i < NXH; i++) norm[i] = float(1.0 / (double(NX) * ((i != 0 && count[i] > 0) ? count[i] : 1)));
+    for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+        const float v0 = std::fmaf(G.T_v0, float(iv0), G.v0_0);
+        out_w[iv0] = float(std::sqrt(1.0 + double(v0) * v0));
+    }
+    const double PI = 3.14159265358979323846;
+    for (int m = 0; m < NX; m++) tw[m] = make_float2(float(std::cos(-2.0 * PI * m / NX)), float(std::sin(-2.0 * PI * m / NX)));
+
+    PfdrArgs A{};
+    A.g = g;
+    A.g_reb = g_reb;
+    A.N_v1 = G.N_v1; A.N_v0 = G.N_v0; A.N_u1 = G.N_u1; A.N_u0 = G.N_u0;
+    A.NX = NX;
+    A.plan = plan;
+    float *d_absU = nullptr, *d_v1ap = nullptr, *d_roww = nullptr, *d_norm = nullptr, *d_outw = nullptr;
+    unsigned char* d_central = nullptr;
+    float2* d_tw = nullptr;
+    int rc = 0;
+    if ((rc = upload(absU, &d_absU, st)) || (rc = upload(v1ap, &d_v1ap, st)) || (rc = upload(row_w, &d_roww, st)) ||
+        (rc = upload(norm, &d_norm, st)) || (rc = upload(out_w, &d_outw, st)) || (rc = upload(central, &d_central, st)) ||
+        (rc = upload(tw, &d_tw, st)))
+        return rc;
+    A.absU = d_absU; A.v1ap = d_v1ap; A.row_w = d_roww; A.norm = d_norm; A.out_w = d_outw; A.central = d_central;
+    A.tw = d_tw;
+    const size_t smem = sizeof(float2) * (size_t(2 * (kPfdrRows / 2) * NX) + size_t(kPfdrRows) * NXH + NX) +
+                        sizeof(float) * NXH;
+    cudaError_t e = cudaFuncSetAttribute(k_pfdr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) {
+        dim3 grid(G.N_v0, ceil_div(G.N_u1, kPfdrRows));
+        k_pfdr<<<grid, kPfdrThreads, smem, st>>>(A);
+        e = cudaGetLastError();
+        note_launch();
+    }
+    cudaFreeAsync(d_absU, st); cudaFreeAsync(d_v1ap, st); cudaFreeAsync(d_roww, st); cudaFreeAsync(d_norm, st);
+    cudaFreeAsync(d_outw, st); cudaFreeAsync(d_central, st); cudaFreeAsync(d_tw, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("PFDR: ") + cudaGetErrorString(e));
+        return int(e);
+    }
+    return 0;
+}
+
+int ramp(const petl_geom& G, float* g_reb, int apply_weight, cudaStream_t st)
+{
+    const int N = G.N_u0;
+    PETL_REQUIRE(N > 0 && N <= 4096, "ramp: unsupported row length");
+    // h[s] = 1/(T pi (1/4 - s^2)) stored as float, as rampImpulseResponse
+    std::vector<float> h(2 * N - 1);
+    const double PI = 3.1415926535897932385;
+    const float T = G.T_u0;
+    for (int i = 0; i < 2 * N - 1; i++) {
+        const float s = float(i - (N - 1));
+        h[i] = float(1.0 / (T * PI * (0.25 - s * s)));
+    }
+    // inverse planogram weight per view (apply_planogram_weight(true))
+    std::vector<float> vw(G.N_v0, 1.0f);
+    if (apply_weight) {
+        const float v1 = fadd_h(fmul_h(0.0f, G.T_v1), G.v1_0);
+        for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+            const float v0 = fadd_h(fmul_h(float(iv0), G.T_v0), G.v0_0);
+            const float c = float(1.0 / std::sqrt(1.0 + double(v1) * v1 + double(v0) * v0));
+            vw[iv0] = float(1.0 / c);
+        }
+    }
+    float *d_h = nullptr, *d_vw = nullptr;
+    int rc = 0;
+    if ((rc = upload(h, &d_h, st)) || (rc = upload(vw, &d_vw, st))) return rc;
+    const int nrows = G.N_v0 * G.N_u1;
+    const size_t smem = sizeof(float) * (size_t(2 * N - 1) + size_t(kRampRows) * N);
+    cudaError_t e = cudaFuncSetAttribute(k_ramp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) {
+        k_ramp<<<ceil_div(nrows, kRampRows), 256, smem, st>>>(g_reb, nrows, N, G.N_u1, d_h, d_vw);
+        e = cudaGetLastError();
+        note_launch();
+    }
+    cudaFreeAsync(d_h, st);
+    cudaFreeAsync(d_vw, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("ramp: ") + cudaGetErrorString(e));
+        return int(e);
+    }
+    return 0;
+}
+
+}  // namespace petl

@@ -1,0 +1,252 @@
+"""Device-resident operators on torch CUDA tensors.
+
+Each function calls one entry point of ``libpetl.so`` (include/petl_device.h)
+on the current torch stream; tensors must be contiguous float32 CUDA tensors.
+PyTorch provides only device memory and streams here.  Scalars that the
+library reduces in FP64 come back as float64 0-d CUDA tensors (no host sync).
+"""
+import ctypes
+
+import torch
+
+from ._lib import PetlError, check, lib
+from .geometry import Geometry, as_list
+
+REFERENCE = 0
+ADJOINT = 1
+_MODES = {"reference": REFERENCE, "adjoint": ADJOINT, REFERENCE: REFERENCE, ADJOINT: ADJOINT}
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev(t, name="tensor"):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise PetlError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.float32:
+        raise PetlError(f"{name} must be float32")
+    if not t.is_contiguous():
+        raise PetlError(f"{name} must be contiguous")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _n(t):
+    return ctypes.c_longlong(t.numel())
+
+
+# ----------------------------------------------------------------------------
+# projectors
+# ----------------------------------------------------------------------------
+def project(geom, f, g=None, subset=None, v1_range=None):
+    """g = P f (reference src/projectors.cu:11-238).
+
+    ``subset=(first, step)`` computes only the views iv0 = first + k*step and
+    leaves the others of ``g`` untouched; ``v1_range=(b, e)`` restricts the
+    v1 slices.  ``geom`` may be a list of geometries (one planogram each), in
+    which case ``g`` is a list."""
+    geoms = as_list(geom)
+    if g is None:
+        g = [torch.zeros(G.shape, device=f.device, dtype=torch.float32) for G in geoms]
+    gl = as_list(g)
+    first, step = subset if subset is not None else (0, 1)
+    for G, gi in zip(geoms, gl):
+        b, e = v1_range if v1_range is not None else (0, G.shape[0])
+        check(lib().petl_project_range_dev(G.ptr, _dev(f, "f"), _dev(gi, "g"), b, e, first, step, _stream()),
+              "project")
+    return g if isinstance(geom, (list, tuple)) else gl[0]
+
+
+def project_ratio(geom, f, meas, out=None, subset=None, v1_range=None):
+    """out = meas / (P f) with 0 where P f == 0 (the MLEM data ratio of the
+    reference, src/petl_server.py:1593-1594), computed inside the projector."""
+    geoms = as_list(geom)
+    ml = as_list(meas)
+    if out is None:
+        out = [torch.empty_like(m) for m in ml]
+    ol = as_list(out)
+    first, step = subset if subset is not None else (0, 1)
+    for G, mi, oi in zip(geoms, ml, ol):
+        b, e = v1_range if v1_range is not None else (0, G.shape[0])
+        check(lib().petl_project_ratio_dev(G.ptr, _dev(f, "f"), _dev(mi, "meas"), _dev(oi, "out"), b, e, first, step,
+                                           _stream()), "project_ratio")
+    return out if isinstance(geom, (list, tuple)) else ol[0]
+
+
+def backproject(geom, g, f=None, mode="reference", accumulate=False, scale=1.0, subset=None, v1_range=None):
+    """f = P^T g summed over planograms.
+
+    mode 'reference' follows the reference backprojector's visibility rules
+    (src/projectors.cu:240-377) with exact bilinear weights; mode 'adjoint'
+    is the exact transpose of ``project``."""
+    geoms = as_list(geom)
+    gl = as_list(g)
+    if f is None:
+        f = torch.empty(geoms[0].vol_shape, device=gl[0].device, dtype=torch.float32)
+        accumulate = False
+    first, step = subset if subset is not None else (0, 1)
+    m = _MODES[mode]
+    for i, (G, gi) in enumerate(zip(geoms, gl)):
+        b, e = v1_range if v1_range is not None else (0, G.shape[0])
+        acc = 1 if (accumulate or i > 0) else 0
+        check(lib().petl_backproject_range_dev(G.ptr, _dev(gi, "g"), _dev(f, "f"), m, acc, float(scale), b, e,
+                                               first, step, _stream()), "backproject")
+    return f
+
+
+def nnz(geom):
+    """Exact count of nonzero (ray, voxel) footprint weights of P."""
+    out = ctypes.c_double(0.0)
+    check(lib().petl_project_nnz_dev(geom.ptr, ctypes.byref(out), _stream()), "project_nnz")
+    return out.value
+
+
+# ----------------------------------------------------------------------------
+# PFDR / ramp / FBP
+# ----------------------------------------------------------------------------
+def pfdr(geom, g, g_reb=None):
+    """PFDR rebinning (src/pfdr.cu:159-315) -> [N_v0][N_u1][N_u0]."""
+    if g_reb is None:
+        g_reb = torch.empty(geom.rebinned_shape, device=g.device, dtype=torch.float32)
+    check(lib().petl_pfdr_dev(geom.ptr, _dev(g, "g"), _dev(g_reb, "g_reb"), _stream()), "PFDR")
+    return g_reb
+
+
+def ramp_(geom_reb, g_reb, apply_weight=True):
+    """In-place ramp filter of a rebinned planogram (src/ramp_filter.cu:156-348),
+    followed by the inverse planogram weight when ``apply_weight``."""
+    check(lib().petl_ramp_dev(geom_reb.ptr, _dev(g_reb, "g_reb"), 1 if apply_weight else 0, _stream()), "ramp")
+    return g_reb
+
+
+def fbp(geom, g, f=None, accumulate=False):
+    """FBP of one or more planograms (PETL::doFBP, src/petl.cpp:310-355)."""
+    geoms = as_list(geom)
+    gl = as_list(g)
+    if f is None:
+        f = torch.empty(geoms[0].vol_shape, device=gl[0].device, dtype=torch.float32)
+        accumulate = False
+    for i, (G, gi) in enumerate(zip(geoms, gl)):
+        check(lib().petl_fbp_dev(G.ptr, _dev(gi, "g"), _dev(f, "f"), 1 if (accumulate or i > 0) else 0, _stream()),
+              "FBP")
+    return f
+
+
+# ----------------------------------------------------------------------------
+# regularizers: volumes [N1][N2][N3] (2-D inputs are treated as N1 = 1)
+# ----------------------------------------------------------------------------
+def _dims(f):
+    s = tuple(f.shape)
+    if len(s) == 2:
+        return (1,) + s
+    if len(s) != 3:
+        raise PetlError("regularizers take 2-D or 3-D arrays")
+    return s
+
+
+def _scalar(f):
+    return torch.zeros((), device=f.device, dtype=torch.float64)
+
+
+def rd_gradient(f, delta, beta, out=None):
+    out = torch.empty_like(f) if out is None else out
+    check(lib().petl_rd_gradient_dev(_dev(f, "f"), _dev(out, "Df"), *_dims(f), float(delta), float(beta), _stream()),
+          "rd_gradient")
+    return out
+
+
+def rd_cost(f, delta, beta):
+    out = _scalar(f)
+    check(lib().petl_rd_cost_dev(_dev(f, "f"), *_dims(f), float(delta), float(beta), ctypes.c_void_p(out.data_ptr()),
+                                 _stream()), "rd_cost")
+    return out
+
+
+def tv_gradient(f, delta, beta=0.0, p=1.0, num_neighbors=26, out=None):
+    out = torch.empty_like(f) if out is None else out
+    check(lib().petl_tv_gradient_dev(_dev(f, "f"), _dev(out, "Df"), *_dims(f), float(delta), float(beta), float(p),
+                                     int(num_neighbors), _stream()), "tv_gradient")
+    return out
+
+
+def tv_cost(f, delta, beta=0.0, p=1.0, num_neighbors=26):
+    out = _scalar(f)
+    check(lib().petl_tv_cost_dev(_dev(f, "f"), *_dims(f), float(delta), float(beta), float(p), int(num_neighbors),
+                                 ctypes.c_void_p(out.data_ptr()), _stream()), "tv_cost")
+    return out
+
+
+def tv_quadform(f, d, delta, beta=0.0, p=1.0, num_neighbors=26):
+    out = _scalar(f)
+    check(lib().petl_tv_quadform_dev(_dev(f, "f"), _dev(d, "d"), *_dims(f), float(delta), float(beta), float(p),
+                                     int(num_neighbors), ctypes.c_void_p(out.data_ptr()), _stream()), "tv_quadform")
+    return out
+
+
+def gaussian_filter_(f, fwhm=2.0, num_dims=3):
+    check(lib().petl_gaussian_filter_dev(_dev(f, "f"), *_dims(f), float(fwhm), int(num_dims), _stream()),
+          "gaussian_filter")
+    return f
+
+
+# ----------------------------------------------------------------------------
+# elementwise / reductions
+# ----------------------------------------------------------------------------
+def rdivide_(denom, num):
+    """denom = num / denom, 0 where denom == 0 (reference RDIV)."""
+    check(lib().petl_rdivide_dev(_dev(num, "num"), _dev(denom, "denom"), _n(denom), _stream()), "rdivide")
+    return denom
+
+
+def divide_(x, y):
+    """x = x / y, 0 where y == 0 (reference DIV)."""
+    check(lib().petl_divide_dev(_dev(x, "x"), _dev(y, "y"), _n(x), _stream()), "divide")
+    return x
+
+
+def multiply_(x, y):
+    check(lib().petl_multiply_dev(_dev(x, "x"), _dev(y, "y"), _n(x), _stream()), "multiply")
+    return x
+
+
+def reciprocal_(x, divide_by_zero_value=0.0):
+    check(lib().petl_reciprocal_dev(_dev(x, "x"), _n(x), float(divide_by_zero_value), _stream()), "reciprocal")
+    return x
+
+
+def axpby_(x, y, a, b):
+    check(lib().petl_axpby_dev(_dev(x, "x"), _dev(y, "y"), float(a), float(b), _n(x), _stream()), "axpby")
+    return x
+
+
+def dot(x, y, w=None):
+    """sum(x*y*w) accumulated in FP64 on the device (0-d float64 tensor)."""
+    out = _scalar(x)
+    wp = _dev(w, "w") if w is not None else ctypes.c_void_p(0)
+    check(lib().petl_dot_dev(_dev(x, "x"), _dev(y, "y"), wp, _n(x), ctypes.c_void_p(out.data_ptr()), _stream()),
+          "dot")
+    return out
+
+
+def loglik(g, Pf):
+    """Poisson log-likelihood sum(g log Pf - Pf) over Pf > 0, FP64."""
+    out = _scalar(g)
+    check(lib().petl_loglik_dev(_dev(g, "g"), _dev(Pf, "Pf"), _n(g), ctypes.c_void_p(out.data_ptr()), _stream()),
+          "loglik")
+    return out
+
+
+def mlem_update_(f, d, sens):
+    check(lib().petl_mlem_update_dev(_dev(f, "f"), _dev(d, "d"), _dev(sens, "sens"), _n(f), _stream()), "mlem_update")
+    return f
+
+
+def osl_update_(f, d, sens, Df):
+    check(lib().petl_osl_update_dev(_dev(f, "f"), _dev(d, "d"), _dev(sens, "sens"), _dev(Df, "Df"), _n(f),
+                                    _stream()), "osl_update")
+    return f
+
+
+__all__ = ["Geometry", "project", "project_ratio", "backproject", "nnz", "pfdr", "ramp_", "fbp", "rd_gradient", "rd_cost",
+           "tv_gradient", "tv_cost", "tv_quadform", "gaussian_filter_", "rdivide_", "divide_", "multiply_",
+           "reciprocal_", "axpby_", "dot", "loglik", "mlem_update_", "osl_update_", "REFERENCE", "ADJOINT"]

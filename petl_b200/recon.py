@@ -1,0 +1,169 @@
+"""Device-resident reconstruction drivers: MLEM, OSEM, one-step-late RD MLEM,
+and penalized least squares by preconditioned conjugate gradient.
+
+Every iteration stays on the GPU: the MLEM data ratio is computed inside the
+forward projector (ops.project_ratio), the image update is one fused kernel,
+and the log-likelihood and step-size reductions run in FP64 on the device.
+
+* ``mlem`` follows the reference PETLserver.MLEM loop
+  (src/petl_server.py:1534-1606): f starts at 1 (or is clipped at 0 when
+  given), sensitivity = P^T 1 with zeros replaced by 1, d = P^T (g / P f),
+  f *= d / sens, or with beta > 0 the one-step-late relative-difference
+  update f *= d / max(0.1 sens, sens + grad R(f)).
+* ``osem`` splits the views into S interleaved subsets (subset s holds
+  iv0 = s, s+S, ...); with S = 1 it is ``mlem``.  The reference has no OSEM.
+* ``rwls`` follows PETLserver.RWLS (src/petl_server.py:1691-1877): PCG with
+  an optional SQS preconditioner 1/P^T W P 1, restarts every 50 iterations,
+  step = <d,grad> / (<Pd, W Pd> + TV quadratic form), optional
+  non-negativity.
+"""
+import torch
+
+from . import ops
+from .geometry import as_list
+
+
+def _ones_like_list(gl):
+    return [torch.ones_like(x) for x in gl]
+
+
+def sensitivity(geoms, like, subset=None, mode="reference"):
+    """P^T 1 (src/petl_server.py:1257-1273) with zeros replaced by 1."""
+    geoms = as_list(geoms)
+    ones = _ones_like_list(like)
+    s = ops.backproject(geoms, ones, subset=subset, mode=mode)
+    s[s == 0.0] = 1.0
+    return s
+
+
+def _init_image(geoms, f, device):
+    if f is None:
+        return torch.ones(geoms[0].vol_shape, device=device, dtype=torch.float32)
+    if not torch.any(f):
+        f.fill_(1.0)
+    else:
+        f.clamp_(min=0.0)
+    return f
+
+
+def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, sens=None, loglik_every=0):
+    """MLEM / OSL-RD MLEM; returns (f, loglik history)."""
+    return osem(geoms, g, num_iter, 1, f=f, delta=delta, beta=beta, sens=sens, loglik_every=loglik_every)
+
+
+def osem(geoms, g, num_iter, num_subsets, f=None, delta=2.0, beta=0.0, sens=None, loglik_every=0):
+    """OSEM with interleaved view subsets; returns (f, loglik history).
+
+    ``sens`` may pass precomputed per-subset sensitivities (list of S
+    volumes) so that repeated reconstructions on one geometry reuse them."""
+    single = not isinstance(geoms, (list, tuple))
+    geoms = as_list(geoms)
+    gl = as_list(g)
+    device = gl[0].device
+    f = _init_image(geoms, f, device)
+    S = int(num_subsets)
+    if sens is None:
+        sens = [sensitivity(geoms, gl, subset=(s, S)) for s in range(S)]
+    ratio = [torch.empty_like(x) for x in gl]
+    d = torch.empty_like(f)
+    Df = torch.empty_like(f) if beta > 0.0 else None
+    history = []
+    for it in range(num_iter):
+        for s in range(S):
+            sub = (s, S)
+            ops.project_ratio(geoms, f, gl, out=ratio, subset=sub)
+            ops.backproject(geoms, ratio, f=d, subset=sub)
+            if beta > 0.0:
+                ops.rd_gradient(f, delta, beta, out=Df)
+                ops.osl_update_(f, d, sens[s], Df)
+            else:
+                ops.mlem_update_(f, d, sens[s])
+        if loglik_every and (it + 1) % loglik_every == 0:
+            history.append(loglik(geoms, gl, f))
+    del single
+    return f, history
+
+
+def loglik(geoms, g, f):
+    """Poisson log-likelihood of f (FP64, device)."""
+    geoms = as_list(geoms)
+    gl = as_list(g)
+    Pf = ops.project(geoms, f)
+    Pf = as_list(Pf)
+    total = torch.zeros((), device=gl[0].device, dtype=torch.float64)
+    for gi, pi in zip(gl, Pf):
+        total = total + ops.loglik(gi, pi)
+    return total
+
+
+def rwls(geoms, g, f, num_iter, delta=1.0, beta=0.0, W=None, preconditioner=None, nonnegativity=True, p=1.0,
+         bp_mode="reference"):
+    """Regularized weighted least squares by PCG (PETLserver.RWLS)."""
+    geoms = as_list(geoms)
+    gl = as_list(g)
+    restart = 50
+    if isinstance(W, str) and W == "auto":
+        # W = 1 / max(gaussian(g, 3), 7) (src/petl_server.py:1739-1746)
+        W = []
+        for gi in gl:
+            w = gi.clone()
+            shp = w.shape
+            w2 = w.view(shp[0] * shp[1], shp[2], shp[3])
+            ops.gaussian_filter_(w2, 3.0, 2)
+            w.clamp_(min=7.0)
+            ops.reciprocal_(w, 0.0)
+            W.append(w)
+    Wl = as_list(W) if W is not None else None
+    if torch.any(f):
+        if nonnegativity:
+            f.clamp_(min=0.0)
+        Pf = as_list(ops.project(geoms, f))
+    else:
+        Pf = [torch.zeros_like(x) for x in gl]
+    resid = [p_ - g_ for p_, g_ in zip(Pf, gl)]
+    grad = torch.empty_like(f)
+    d = torch.zeros_like(f)
+    grad_old = torch.zeros_like(f)
+    Pd = [torch.empty_like(x) for x in gl]
+    Q = None
+    if preconditioner in (True, "SQS"):
+        ones = torch.ones_like(f)
+        P1 = as_list(ops.project(geoms, ones))
+        if Wl is not None:
+            P1 = [a * w for a, w in zip(P1, Wl)]
+        Q = ops.backproject(geoms, P1, mode=bp_mode)
+        ops.reciprocal_(Q, 1.0)
+    gog = 0.0
+    for n in range(num_iter):
+        WR = [r * w for r, w in zip(resid, Wl)] if Wl is not None else resid
+        ops.backproject(geoms, WR, f=grad, mode=bp_mode)
+        if beta > 0.0:
+            grad += ops.tv_gradient(f, delta, beta, p)
+        u = grad * Q if Q is not None else grad.clone()
+        if n == 0 or n % restart == 0:
+            d.copy_(u)
+        else:
+            gamma = (float(ops.dot(u, grad)) - float(ops.dot(u, grad_old))) / gog
+            d.mul_(gamma).add_(u)
+            if float(ops.dot(d, grad)) <= 0.0:
+                d.copy_(u)
+        gog = float(ops.dot(u, grad))
+        grad_old.copy_(grad)
+        ops.project(geoms, d, Pd if len(Pd) > 1 else Pd[0])
+        num = float(ops.dot(d, grad))
+        den = 0.0
+        for pd, w in zip(Pd, Wl if Wl is not None else [None] * len(Pd)):
+            den += float(ops.dot(pd, pd, w))
+        if beta > 0.0:
+            den += float(ops.tv_quadform(f, d, delta, beta, p))
+        step = num / den if abs(den) > 1.0e-16 else 0.0
+        if step <= 0.0:
+            break
+        f.add_(d, alpha=-step)
+        if nonnegativity:
+            f.clamp_(min=0.0)
+            Pf = as_list(ops.project(geoms, f))
+            resid = [p_ - g_ for p_, g_ in zip(Pf, gl)]
+        else:
+            resid = [r - step * pd for r, pd in zip(resid, Pd)]
+    return f

@@ -1,0 +1,485 @@
+"""PETLserver: the reference Python operator surface over libpetl.so.
+
+Method names, argument meaning, defaults, return values and error behaviour
+follow the reference class ``PETLserver`` (src/petl_server.py:14-2152):
+geometry setters raise ValueError when the library returns false, projector
+calls raise TypeError, planograms are lists of float32 numpy arrays
+[N_v1][N_v0][N_u1][N_u0], volumes are float32 numpy arrays [z][y][x].
+Numpy inputs go through the reference-compatible C ABI (host pointers);
+torch CUDA tensors (or lists of them) go through the device-resident
+operators in petl_b200.ops without leaving the GPU.
+
+Not provided here (outside the reconstruction path): list-mode binning,
+analytic phantoms and ray tracing, detector response / corrections, scatter
+simulation and the napari display.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from ._lib import c_f, fp, lib
+
+try:  # torch is optional for the host path
+    import torch
+    _has_torch = True
+except Exception:  # pragma: no cover
+    torch = None
+    _has_torch = False
+
+
+def _is_dev(x):
+    if isinstance(x, list):
+        return len(x) > 0 and _is_dev(x[0])
+    return _has_torch and isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def _fp(a):
+    return a.ctypes.data_as(fp)
+
+
+def _pp(arrs):
+    return (fp * len(arrs))(*[_fp(a) for a in arrs])
+
+
+def _check_f32(a, name):
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]):
+        raise TypeError(f"{name} must be a C-contiguous float32 numpy array")
+
+
+class PETLserver:
+    def __init__(self, param_id=None, lib_dir=""):
+        self.libprojectors = lib()
+        if param_id is not None:
+            self.param_id = param_id
+        else:
+            self.param_id = self.libprojectors.create_new_model()
+        self.set_model()
+        self.print_cost = False
+        self.print_warnings = True
+        self.response = None
+        self.include_response_with_projectors = False
+
+    # ------------------------------------------------------------------ model
+    def set_model(self, i=None):
+        if i is not None:
+            self.param_id = i
+        return self.libprojectors.set_model(self.param_id)
+
+    def create_new_model(self):
+        return self.libprojectors.create_new_model()
+
+    def about(self):
+        self.set_model()
+        self.libprojectors.about()
+
+    def copy_parameters(self, param_id):
+        self.set_model()
+        return self.libprojectors.copy_parameters(param_id)
+
+    def clearAll(self):
+        self.set_model()
+        self.libprojectors.clearAll()
+
+    def print_parameters(self):
+        self.set_model()
+        self.libprojectors.print_parameters()
+
+    def all_defined(self):
+        return self.geometry_defined() and self.volume_defined()
+
+    def volume_defined(self):
+        self.set_model()
+        return self.libprojectors.volume_defined()
+
+    def geometry_defined(self):
+        self.set_model()
+        return self.libprojectors.geometry_defined()
+
+    def _getset(self, name, v, setter_type=None):
+        self.set_model()
+        if v is None:
+            return getattr(self.libprojectors, "get_" + name)()
+        if getattr(self.libprojectors, "set_" + name)(v):
+            return getattr(self.libprojectors, "get_" + name)()
+        return None
+
+    def numX(self, N=None):
+        return self._getset("numX", N)
+
+    def numY(self, N=None):
+        return self._getset("numY", N)
+
+    def numZ(self, N=None):
+        return self._getset("numZ", N)
+
+    def voxelWidth(self, w=None):
+        return self._getset("voxelWidth", w)
+
+    def voxelHeight(self, h=None):
+        return self._getset("voxelHeight", h)
+
+    def offsetX(self, x=None):
+        return self._getset("offsetX", x)
+
+    def offsetY(self, y=None):
+        return self._getset("offsetY", y)
+
+    def offsetZ(self, z=None):
+        return self._getset("offsetZ", z)
+
+    def get_numPlanograms(self):
+        self.set_model()
+        return self.libprojectors.get_numPlanograms()
+
+    def get_planogramSize(self, n):
+        if self.geometry_defined():
+            shape = (ctypes.c_int * 4)()
+            self.set_model()
+            self.libprojectors.get_planogramSize(n, shape)
+            return np.array(list(shape), dtype=np.int32)
+        return None
+
+    # -------------------------------------------------------------- geometry
+    def add_planogram(self, psi, D, L, H, T, v_m0=None, v_m1=None):
+        if v_m0 is None:
+            v_m0 = 1.0
+        if v_m1 is None:
+            v_m1 = min(1.0, (H - 1.5 * T) / D)
+        self.set_model()
+        if not self.libprojectors.add_planogram(psi, D, L, H, v_m0, v_m1, T):
+            raise ValueError("Error: add_planogram failed")
+
+    def remove_planogram(self, n):
+        self.set_model()
+        if not self.libprojectors.remove_planogram(n):
+            raise ValueError("Error: remove_planogram failed")
+
+    def keep_only_planogram(self, n):
+        self.set_model()
+        if not self.libprojectors.keep_only_planogram(n):
+            raise ValueError("Error: keep_only_planogram failed")
+
+    def set_default_volume(self, scale=1.0):
+        self.set_model()
+        if not self.libprojectors.set_default_volume(scale):
+            raise ValueError("Error: set_default_volume failed")
+
+    def set_volume(self, numX, numY, numZ, voxelWidth, voxelHeight=0.0, offsetX=0.0, offsetY=0.0, offsetZ=0.0):
+        if voxelHeight == 0.0:
+            voxelHeight = voxelWidth
+        self.set_model()
+        if not self.libprojectors.set_volume(numX, numY, numZ, voxelWidth, voxelHeight, offsetX, offsetY, offsetZ):
+            raise ValueError("Error: set_volume failed")
+
+    # ----------------------------------------------------------- allocation
+    def allocate_projections(self):
+        if self.geometry_defined():
+            return [np.zeros(tuple(self.get_planogramSize(n)), dtype=np.float32)
+                    for n in range(self.get_numPlanograms())]
+        return None
+
+    def allocate_rebinned_projections(self):
+        if self.geometry_defined():
+            return [np.zeros(tuple(self.get_planogramSize(n))[1:], dtype=np.float32)
+                    for n in range(self.get_numPlanograms())]
+        return None
+
+    def allocate_volume(self):
+        if self.volume_defined():
+            return np.zeros((self.numZ(), self.numY(), self.numX()), dtype=np.float32)
+        print("Error: volume is not defined")
+        return None
+
+    def copy_data(self, x):
+        if isinstance(x, list):
+            return [y.clone() if _is_dev(y) else y.copy() for y in x]
+        return x.clone() if _is_dev(x) else x.copy()
+
+    def copyData(self, x):
+        return self.copy_data(x)
+
+    # ------------------------------------------------------------ projectors
+    def project(self, g, f):
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        self.set_model()
+        for a in g:
+            _check_f32(a, "g")
+        _check_f32(f, "f")
+        if not self.libprojectors.project(_pp(g), _fp(f)):
+            raise TypeError("project failed")
+        return g
+
+    def backproject(self, g, f=None):
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        if f is None:
+            f = self.allocate_volume()
+        self.set_model()
+        for a in g:
+            _check_f32(a, "g")
+        _check_f32(f, "f")
+        if not self.libprojectors.backproject(_pp(g), _fp(f)):
+            raise TypeError("backproject failed")
+        return f
+
+    def FBP(self, g, f=None):
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        if f is None:
+            f = self.allocate_volume()
+        self.set_model()
+        if not self.libprojectors.FBP(_pp(g), _fp(f)):
+            raise TypeError("FBP failed")
+        return f
+
+    def PFDR(self, g, g_reb=None):
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        if g_reb is None:
+            g_reb = self.allocate_rebinned_projections()
+        self.set_model()
+        if not self.libprojectors.PFDR(_pp(g), _pp(g_reb)):
+            raise TypeError("PFDR failed")
+        return g_reb
+
+    def sensitivity(self, Pstar1=None):
+        if Pstar1 is None:
+            Pstar1 = self.allocate_volume()
+        ones = self.allocate_projections()
+        for o in ones:
+            o[:] = 1.0
+        self.backproject(ones, Pstar1)
+        return Pstar1
+
+    # ------------------------------------------------------- vector helpers
+    def _binop4(self, name3, name4, x, y):
+        self.set_model()
+        xs = x if isinstance(x, list) else [x]
+        ys = y if isinstance(y, list) else [y]
+        for a, b in zip(xs, ys):
+            if a.ndim == 4:
+                ok = getattr(self.libprojectors, name4)(_fp(a), _fp(b), *a.shape)
+            elif a.ndim == 3:
+                ok = getattr(self.libprojectors, name3)(_fp(a), _fp(b), *a.shape)
+            else:
+                raise ValueError("inputs must be 3D or 4D numpy arrays")
+            if not ok:
+                return None
+        return x
+
+    def multiply(self, x, y):
+        return self._binop4("multiply3D", "multiply4D", x, y)
+
+    def divide(self, num, denom):
+        return self._binop4("divide3D", "divide4D", num, denom)
+
+    def rdivide(self, denom, num):
+        """denom = num / denom (0 where denom == 0)."""
+        self.set_model()
+        ds = denom if isinstance(denom, list) else [denom]
+        ns = num if isinstance(num, list) else [num]
+        for d, n in zip(ds, ns):
+            if d.ndim == 4:
+                ok = self.libprojectors.rdivide4D(_fp(n), _fp(d), *d.shape)
+            else:
+                ok = self.libprojectors.rdivide3D(_fp(n), _fp(d), *d.shape)
+            if not ok:
+                return None
+        return denom
+
+    def reciprocal(self, x, divide_by_zero_value=0.0):
+        self.set_model()
+        xs = x if isinstance(x, list) else [x]
+        for a in xs:
+            if a.ndim == 4:
+                self.libprojectors.reciprocal4D(_fp(a), *a.shape, divide_by_zero_value)
+            else:
+                self.libprojectors.reciprocal3D(_fp(a), *a.shape, divide_by_zero_value)
+        return x
+
+    def inner_product(self, x, y, w=None):
+        if isinstance(x, list):
+            acc = 0.0
+            for n in range(len(x)):
+                if w is None:
+                    acc += self.inner_product(x[n], y[n])
+                elif isinstance(w, (int, float)):
+                    acc += self.inner_product(x[n], y[n]) * w
+                else:
+                    acc += self.inner_product(x[n], y[n], w[n])
+            return acc
+        self.set_model()
+        wp = _fp(w) if w is not None else None
+        if x.ndim == 4:
+            return self.libprojectors.inner_product4D(_fp(x), _fp(y), wp, *x.shape)
+        if x.ndim == 3:
+            return self.libprojectors.inner_product3D(_fp(x), _fp(y), wp, *x.shape)
+        return float(np.sum(x * y * w))
+
+    def innerProd(self, x, y, w=None):
+        return self.inner_product(x, y, w)
+
+    def isAllZeros(self, f):
+        return not np.any(f)
+
+    def setToConstant(self, x, c=0.0):
+        for a in (x if isinstance(x, list) else [x]):
+            a[:] = c
+
+    def setToZero(self, x):
+        self.setToConstant(x, 0.0)
+
+    def setToOne(self, x):
+        self.setToConstant(x, 1.0)
+
+    def clip(self, x, min_val=0.0, max_val=None):
+        for a in (x if isinstance(x, list) else [x]):
+            np.clip(a, min_val, max_val, out=a)
+        return x
+
+    def scale(self, x, c=1.0):
+        for a in (x if isinstance(x, list) else [x]):
+            a[:] *= c
+        return x
+
+    def subtract(self, x, y):
+        for a, b in zip(x if isinstance(x, list) else [x], y if isinstance(y, list) else [y]):
+            a[:] -= b[:]
+        return x
+
+    def scalarAdd(self, x, c, y):
+        for a, b in zip(x if isinstance(x, list) else [x], y if isinstance(y, list) else [y]):
+            a[:] += c * b[:]
+        return x
+
+    def square(self, x):
+        return self.multiply(x, x)
+
+    # --------------------------------------------------------- iterations
+    def MLEM(self, g, f, numIter, delta=2.0, beta=0.0, mask=None):
+        """MLEM / one-step-late RD MLEM (src/petl_server.py:1534-1606).
+
+        Runs device-resident: the planograms are copied to the GPU once, every
+        iteration stays there, and f is copied back at the end."""
+        return self.OSEM(g, f, numIter, 1, delta=delta, beta=beta, mask=mask)
+
+    def OSEM(self, g, f, numIter, numSubsets, delta=2.0, beta=0.0, mask=None):
+        """Ordered-subsets EM with interleaved view subsets (iv0 mod S)."""
+        from . import recon
+        if mask is not None:
+            raise ValueError("mask is not supported by the device-resident MLEM")
+        geoms = self.geometries_from_model()
+        dev = torch.device("cuda")
+        gd = [torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(dev) for x in g]
+        if f is None:
+            f = self.allocate_volume()
+        fd = torch.from_numpy(np.ascontiguousarray(f, np.float32)).to(dev)
+        fd, _ = recon.osem(geoms, gd, numIter, numSubsets, f=fd, delta=delta, beta=beta)
+        f[:] = fd.cpu().numpy()
+        return f
+
+    def geometries_from_model(self):
+        """Geometry objects equal to this model's planograms and volume."""
+        from .geometry import Geometry
+        from ._lib import petl_geom
+        self.set_model()
+        out = []
+        for n in range(self.get_numPlanograms()):
+            G = Geometry.__new__(Geometry)
+            G.args = None
+            G.volume_args = None
+            G.g = petl_geom()
+            if lib().petl_model_geometry(n, ctypes.byref(G.g)) != 0:
+                raise ValueError("model geometry unavailable")
+            out.append(G)
+        return out
+
+    # ------------------------------------------------------- regularizers
+    @staticmethod
+    def _dims(f):
+        if f.ndim == 3:
+            return f.shape
+        return (1,) + tuple(f.shape)
+
+    def TVcost(self, f, delta, beta=0.0, p=1.0):
+        self.set_model()
+        if _is_dev(f):
+            return self.libprojectors.TV_cost(ctypes.c_void_p(f.data_ptr()), *self._dims(f), delta, beta, p, False)
+        return self.libprojectors.TV_cost(f.ctypes.data_as(ctypes.c_void_p), *self._dims(f), delta, beta, p, True)
+
+    def TVgradient(self, f, delta, beta=0.0, p=1.0):
+        self.set_model()
+        if _is_dev(f):
+            Df = f.clone()
+            self.libprojectors.TV_gradient(ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(Df.data_ptr()),
+                                           *self._dims(f), delta, beta, p, False)
+            return Df
+        Df = np.zeros(f.shape, dtype=np.float32)
+        self.libprojectors.TV_gradient(f.ctypes.data_as(ctypes.c_void_p), Df.ctypes.data_as(ctypes.c_void_p),
+                                       *self._dims(f), delta, beta, p, True)
+        return Df
+
+    def TVquadForm(self, f, d, delta, beta=0.0, p=1.0):
+        self.set_model()
+        if _is_dev(f):
+            return self.libprojectors.TV_quadForm(ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(d.data_ptr()),
+                                                  *self._dims(f), delta, beta, p, False)
+        return self.libprojectors.TV_quadForm(f.ctypes.data_as(ctypes.c_void_p), d.ctypes.data_as(ctypes.c_void_p),
+                                              *self._dims(f), delta, beta, p, True)
+
+    def diffuse(self, f, delta, numIter, p=1.0):
+        self.set_model()
+        if _is_dev(f):
+            self.libprojectors.diffuse(ctypes.c_void_p(f.data_ptr()), *self._dims(f), delta, p, numIter, False)
+        else:
+            self.libprojectors.diffuse(f.ctypes.data_as(ctypes.c_void_p), *self._dims(f), delta, p, numIter, True)
+        return f
+
+    def TV_denoise(self, f, delta, beta, numIter, p=1.0, meanOverFirstDim=False):
+        self.set_model()
+        if _is_dev(f):
+            self.libprojectors.TV_denoise(ctypes.c_void_p(f.data_ptr()), *self._dims(f), delta, beta, p, numIter,
+                                          meanOverFirstDim, False)
+        else:
+            self.libprojectors.TV_denoise(f.ctypes.data_as(ctypes.c_void_p), *self._dims(f), delta, beta, p, numIter,
+                                          meanOverFirstDim, True)
+        return f
+
+    def relative_differences_grad(self, f, delta, beta):
+        Df = np.zeros(f.shape, dtype=np.float32)
+        self.set_model()
+        self.libprojectors.relativeDifferences_gradient(_fp(f), _fp(Df), *self._dims(f), delta, beta)
+        return Df
+
+    def gaussian_filter(self, f, FWHM=2.0, numDims=3):
+        if isinstance(f, list):
+            for x in f:
+                self.gaussian_filter(x, FWHM, numDims)
+            return
+        if f.ndim == 4:
+            dims = (f.shape[0] * f.shape[1], f.shape[2], f.shape[3])
+            numDims = 2
+        else:
+            dims = self._dims(f)
+        self.set_model()
+        self.libprojectors.gaussian_filter(_fp(f), *dims, FWHM, numDims)
+
+    # ------------------------------------------------------------- I/O
+    def save_data(self, fileName, x, T=1.0, offset_0=0.0, offset_1=0.0, offset_2=0.0, sequence_offset=0):
+        if fileName.endswith(".npy"):
+            np.save(fileName, x)
+            return True
+        print("Error: only .npy output is supported by this build")
+        return False
+
+    def load_data(self, fileName, x=None, fileRange=None, rowRange=None, colRange=None):
+        if not os.path.isfile(fileName) or not fileName.endswith(".npy"):
+            print("Error: only .npy input is supported by this build")
+            return None
+        y = np.load(fileName)
+        if x is not None:
+            x[:] = y[:]
+            return x
+        return y

@@ -1,0 +1,229 @@
+"""CUDA path against the FP64 oracle and the reference's own outputs.
+
+Tolerances (relative L2 unless stated):
+* forward projector vs oracle FP64 and vs reference: 1e-5;
+* backprojector (reference semantics, exact weights) vs oracle FP64: 1e-5;
+  vs the reference's texture-filtered backprojector: 5e-4;
+* adjoint mode: |<Ax,y> - <x,A^T y>| / |<Ax,y>| < 1e-6;
+* PFDR vs oracle and reference: 1e-5; FBP vs oracle: 1e-5, vs reference 1e-3;
+* RD/TV vs oracle and reference: 1e-5; MLEM vs oracle FP64: 1e-5 per
+  iteration checked, vs reference call sequence: 2e-3 (texture weights).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import load_golden, rel_l2
+from helpers import oracle_geoms, product_geoms
+
+pytestmark = pytest.mark.gpu
+
+PROJ_CASES = ["g0", "g90", "g30", "gpitch", "gpetx", "g0t1"]
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.mark.parametrize("name", PROJ_CASES)
+def test_forward_projection(cuda, name):
+    from petl_b200 import ops
+    z = load_golden(f"proj_{name}.npz")
+    geoms, ogeoms = product_geoms(z), oracle_geoms(z)
+    for key in ("f", "f_noise"):
+        g = ops.project(geoms, _t(z[key], cuda))
+        want = O.project(ogeoms, z[key])
+        for i in range(len(geoms)):
+            assert rel_l2(_np(g[i]), want[i]) < 1e-5
+            ref = z[f"g{i}"] if key == "f" else z[f"gnoise{i}"]
+            assert rel_l2(_np(g[i]), ref) < 1e-5
+
+
+@pytest.mark.parametrize("name", PROJ_CASES)
+def test_backprojection_reference_semantics(cuda, name):
+    from petl_b200 import ops
+    z = load_golden(f"proj_{name}.npz")
+    geoms, ogeoms = product_geoms(z), oracle_geoms(z)
+    ys = [z[f"y{i}"] for i in range(len(geoms))]
+    f = ops.backproject(geoms, [_t(y, cuda) for y in ys])
+    assert rel_l2(_np(f), O.backproject(ogeoms, ys)) < 1e-5
+    assert rel_l2(_np(f), z["b"]) < 5e-4
+    s = ops.backproject(geoms, [_t(np.ones(G.shape), cuda) for G in geoms])
+    assert rel_l2(_np(s), z["sens"]) < 2e-4
+
+
+@pytest.mark.parametrize("name", PROJ_CASES)
+def test_adjoint_mode_is_exact_transpose(cuda, name):
+    import torch
+    from petl_b200 import ops
+    z = load_golden(f"proj_{name}.npz")
+    geoms = product_geoms(z)
+    rng = np.random.default_rng(7)
+    x = _t(rng.random(geoms[0].vol_shape), cuda)
+    ys = [_t(rng.random(G.shape), cuda) for G in geoms]
+    Ax = ops.project(geoms, x)
+    Aty = ops.backproject(geoms, ys, mode="adjoint")
+    lhs = sum(float(torch.sum(a.double() * y.double())) for a, y in zip(Ax, ys))
+    rhs = float(torch.sum(x.double() * Aty.double()))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def test_subsets_and_slabs_compose(cuda):
+    import torch
+    from petl_b200 import ops
+    z = load_golden("proj_g0.npz")
+    G = product_geoms(z)[0]
+    f = _t(z["f"], cuda)
+    full = ops.project(G, f)
+    parts = torch.zeros_like(full)
+    for s in range(3):
+        ops.project(G, f, parts, subset=(s, 3))
+    assert torch.equal(full, parts)
+    slabs = torch.zeros_like(full)
+    ops.project(G, f, slabs, v1_range=(0, 4))
+    ops.project(G, f, slabs, v1_range=(4, G.shape[0]))
+    assert torch.equal(full, slabs)
+    y = _t(z["y0"], cuda)
+    b = ops.backproject(G, y)
+    b2 = ops.backproject(G, y, subset=(0, 2))
+    ops.backproject(G, y, f=b2, subset=(1, 2), accumulate=True)
+    assert rel_l2(_np(b2), _np(b)) < 1e-6
+    b3 = ops.backproject(G, y, v1_range=(0, 3))
+    ops.backproject(G, y, f=b3, v1_range=(3, G.shape[0]), accumulate=True)
+    assert rel_l2(_np(b3), _np(b)) < 1e-6
+
+
+def test_nnz_matches_oracle(cuda):
+    from petl_b200 import ops
+    for name in ("g0", "g30", "gpitch"):
+        z = load_golden(f"proj_{name}.npz")
+        assert ops.nnz(product_geoms(z)[0]) == O.project_nnz(oracle_geoms(z)[0])
+
+
+def test_cabi_host_path_matches_device_path(cuda):
+    from petl_b200 import PETLserver, ops
+    z = load_golden("proj_gpetx.npz")
+    s = PETLserver()
+    for p in z["planograms"]:
+        psi, D, L, H, T, vm0, vm1 = p
+        s.add_planogram(psi, D, L, H, T, vm0, vm1)
+    s.set_volume(*[int(v) if i < 3 else float(v) for i, v in enumerate(z["volume"])])
+    g = s.allocate_projections()
+    s.project(g, z["f"].astype(np.float32))
+    for i in range(2):
+        assert rel_l2(g[i], z[f"g{i}"]) < 1e-5
+    f = s.backproject([z["y0"].copy(), z["y1"].copy()])
+    dev = ops.backproject(s.geometries_from_model(), [_t(z["y0"], cuda), _t(z["y1"], cuda)])
+    assert rel_l2(f, _np(dev)) < 1e-6
+    assert rel_l2(f, z["b"]) < 5e-4
+
+
+@pytest.mark.parametrize("name", ["g0", "g0t1"])
+def test_pfdr_ramp_fbp(cuda, name):
+    from petl_b200 import PETLserver, ops
+    z = load_golden(f"pfdr_{name}.npz")
+    G, Go = product_geoms(z)[0], oracle_geoms(z)[0]
+    g = _t(z["g"], cuda)
+    reb = ops.pfdr(G, g)
+    want = O.pfdr(Go, z["g"])
+    assert rel_l2(_np(reb), want) < 1e-5
+    assert rel_l2(_np(reb), z["g_reb"]) < 1e-5
+    f = ops.fbp(G, g)
+    assert rel_l2(_np(f), O.fbp(Go, z["g"])) < 1e-5
+    assert rel_l2(_np(f), z["fbp"]) < 1e-3
+    # through the reference C ABI: PFDR rewrites the model to N_v1 = 1
+    s = PETLserver()
+    psi, D, L, H, T, vm0, vm1 = z["planograms"][0]
+    s.add_planogram(psi, D, L, H, T, vm0, vm1)
+    s.set_volume(*[int(v) if i < 3 else float(v) for i, v in enumerate(z["volume"])])
+    fb = s.FBP([z["g"].astype(np.float32).copy()])
+    assert rel_l2(fb, z["fbp"]) < 1e-3
+    gr = s.PFDR([z["g"].astype(np.float32).copy()])
+    assert rel_l2(gr[0], z["g_reb"]) < 1e-5
+    assert tuple(s.get_planogramSize(0)) == tuple(z["shape_after"])
+
+
+def test_regularizers(cuda):
+    from petl_b200 import PETLserver, ops
+    r = load_golden("regularizers.npz")
+    s = PETLserver()
+    for tag in ("3d", "2d"):
+        f, d = r[f"f_{tag}"], r[f"d_{tag}"]
+        ft, dt = _t(f, cuda), _t(d, cuda)
+        g = ops.rd_gradient(ft, 2.0, 0.01)
+        assert rel_l2(_np(g), O.rd_gradient(f, 2.0, 0.01)) < 1e-5
+        assert rel_l2(_np(g), r[f"rd_grad_{tag}"]) < 1e-5
+        assert rel_l2(s.relative_differences_grad(f.copy(), 2.0, 0.01), r[f"rd_grad_{tag}"]) < 1e-5
+        for delta, p in ((0.05, 1.0), (0.3, 1.2)):
+            key = f"{tag}_d{delta}_p{p}"
+            tg = ops.tv_gradient(ft, delta, 0.7, p)
+            assert rel_l2(_np(tg), r[f"tv_grad_{key}"]) < 1e-5
+            assert abs(float(ops.tv_cost(ft, delta, 0.7, p)) / r[f"tv_cost_{key}"] - 1) < 1e-5
+            assert abs(float(ops.tv_quadform(ft, dt, delta, 0.7, p)) / r[f"tv_quad_{key}"] - 1) < 1e-5
+            assert abs(s.TVcost(f.copy(), delta, 0.7, p) / r[f"tv_cost_{key}"] - 1) < 1e-5
+        fd = f.copy()
+        s.diffuse(fd, 0.05, 3, 1.0)
+        assert rel_l2(fd, r[f"diffuse_{tag}"]) < 1e-5
+        fn = f.copy()
+        s.TV_denoise(fn, 0.05, 0.5, 3, 1.0)
+        assert rel_l2(fn, r[f"tvdenoise_{tag}"]) < 1e-5
+
+
+def test_mlem_matches_oracle_and_reference(cuda):
+    from petl_b200 import recon
+    z = load_golden("mlem_g0.npz")
+    G, Go = product_geoms(z)[0], oracle_geoms(z)[0]
+    g = _t(z["g"], cuda)
+    for tag, beta in (("plain", 0.0), ("rd", 0.05)):
+        f, _ = recon.mlem(G, g, 4, beta=beta, delta=2.0)
+        assert rel_l2(_np(f), O.mlem(Go, z["g"], 4, beta=beta, delta=2.0)) < 1e-5
+        assert rel_l2(_np(f), z[f"f_{tag}"][3]) < 2e-3
+
+
+def test_osem_one_subset_equals_mlem_and_matches_oracle(cuda):
+    import torch
+    from petl_b200 import recon
+    z = load_golden("mlem_g0.npz")
+    G, Go = product_geoms(z)[0], oracle_geoms(z)[0]
+    g = _t(z["g"], cuda)
+    a, _ = recon.mlem(G, g, 3)
+    b, _ = recon.osem(G, g, 3, 1)
+    assert torch.equal(a, b)
+    c, hist = recon.osem(G, g, 2, 4, loglik_every=1)
+    assert rel_l2(_np(c), O.osem(Go, z["g"], 2, 4)) < 1e-5
+    assert float(hist[1]) > float(hist[0])
+
+
+def test_gaussian_filter_matches_direct_formula(cuda):
+    import torch
+    from petl_b200 import ops
+    rng = np.random.default_rng(3)
+    f = rng.random((6, 9, 11)).astype(np.float32)
+    out = _np(ops.gaussian_filter_(_t(f, cuda), 2.5, 3))
+    # direct 3-D evaluation of the reference kernel (clamped-distance weights)
+    sigma = 2.5 / (2 * np.sqrt(2 * np.log(2)))
+    R = int(np.ceil(np.sqrt(2 * np.log(10)) * sigma))
+    den = 1.0 / (2 * sigma)
+    want = np.zeros_like(f, dtype=np.float64)
+    N = f.shape
+    for i in range(N[0]):
+        for j in range(N[1]):
+            for k in range(N[2]):
+                val = s = 0.0
+                for di in range(-R, R + 1):
+                    ii = min(max(i + di, 0), N[0] - 1)
+                    for dj in range(-R, R + 1):
+                        jj = min(max(j + dj, 0), N[1] - 1)
+                        for dk in range(-R, R + 1):
+                            kk = min(max(k + dk, 0), N[2] - 1)
+                            w = np.exp(-den * ((i - ii) ** 2 + (j - jj) ** 2 + (k - kk) ** 2))
+                            val += w * f[ii, jj, kk]
+                            s += w
+                want[i, j, k] = val / s
+    assert rel_l2(out, want) < 1e-5
+    del torch

@@ -1,0 +1,131 @@
+"""libpetl.so without a GPU: it loads, exports every declared symbol, and its
+host-side logic (geometry, model registry, host elementwise rules) matches
+the reference.  No compute call reaches the device here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ROOT, load_golden
+
+import petl_b200
+from petl_b200 import Geometry
+from petl_b200._lib import API, lib
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    pat = r"\b(?:bool|int|float|void|double|char)\s*\**\s*([A-Za-z_]\w*)\s*\("
+    return {m.group(1) for m in re.finditer(pat, text)}
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(petl_b200.LIB_PATH)
+    declared = _declared("petl.h") | _declared("petl_device.h")
+    assert len(declared) > 90
+    missing = [n for n in sorted(declared) if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding describes every declared function
+    bound = {n for n, _, _ in API}
+    assert declared <= bound, sorted(declared - bound)
+
+
+def test_reference_interface_symbols_present():
+    # every extern "C" function of the reference interface header
+    names = ["set_model", "create_new_model", "about", "copy_parameters", "clearAll", "print_parameters",
+             "volume_defined", "geometry_defined", "get_numX", "set_numX", "get_numY", "set_numY", "get_numZ",
+             "set_numZ", "get_voxelWidth", "set_voxelWidth", "get_voxelHeight", "set_voxelHeight", "get_offsetX",
+             "set_offsetX", "get_offsetY", "set_offsetY", "get_offsetZ", "set_offsetZ", "get_numPlanograms",
+             "get_planogramSize", "add_planogram", "remove_planogram", "keep_only_planogram",
+             "set_default_volume", "set_volume", "bin", "simulate_scatter", "project", "backproject", "FBP",
+             "PFDR", "add_object", "add_module", "clear_phantom", "clear_modules", "scale_phantom", "voxelize",
+             "ray_trace", "stopping_power", "set_solid_angle_correction", "apply_corrections", "multiply3D",
+             "multiply4D", "divide3D", "divide4D", "rdivide3D", "rdivide4D", "reciprocal3D", "reciprocal4D",
+             "inner_product3D", "inner_product4D", "TV_cost", "TV_gradient", "TV_quadForm", "diffuse",
+             "TV_denoise", "relativeDifferences_gradient", "gaussian_filter"]
+    L = lib()
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_geometry_matches_reference_and_oracle():
+    z = load_golden("cpu_rules.npz")
+    for call, shape in zip(z["geom_calls"], z["geom_shapes"]):
+        psi, D, L, H, T, vm0, vm1 = call
+        G = Geometry(psi, D, L, H, T, vm0, vm1, volume=(16, 16, 8, 1.5))
+        assert G.shape == tuple(shape)
+        Go = O.make_geom(psi, D, L, H, T, vm0, vm1, (16, 16, 8, 1.5))
+        for fld in ("T_v1", "T_v0", "T_u1", "T_u0", "v1_0", "v0_0", "u1_0", "u0_0", "cos_psi", "sin_psi",
+                    "R", "L", "H", "v_m1", "x_0", "y_0", "z_0"):
+            ours = getattr(G.g, fld)
+            theirs = getattr(Go, fld)
+            assert ours == theirs, (fld, ours, theirs)
+
+
+def test_optimal_fft_size_matches_oracle():
+    L = lib()
+    for n in range(1, 2100):
+        assert L.petl_optimal_fft_size(n) == O.optimal_fft_size(n)
+
+
+def test_cabi_registry_and_geometry():
+    from petl_b200 import PETLserver
+    s = PETLserver()
+    s.add_planogram(0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25)
+    assert tuple(s.get_planogramSize(0)) == (65, 129, 128, 256)
+    s.set_volume(256, 256, 128, 1.0)
+    assert s.all_defined()
+    assert (s.numX(), s.numY(), s.numZ()) == (256, 256, 128)
+    assert s.voxelHeight() == 1.0
+    # offsets: the setters accept only positive values, as the reference
+    assert s.offsetX(-1.0) is None and s.offsetX(2.0) == 2.0
+    # a second model keeps its own parameters; copy_parameters copies
+    t = PETLserver()
+    assert not t.geometry_defined()
+    assert t.copy_parameters(s.param_id)
+    assert tuple(t.get_planogramSize(0)) == (65, 129, 128, 256)
+    t.keep_only_planogram(0)
+    with pytest.raises(ValueError):
+        t.remove_planogram(3)
+    t.clearAll()
+    assert not t.geometry_defined() and not t.volume_defined()
+    with pytest.raises(ValueError):
+        t.add_planogram(0.0, -1.0, 1.0, 1.0, 1.0)
+
+
+def test_set_default_volume_fills_fov():
+    from petl_b200 import PETLserver
+    s = PETLserver()
+    s.add_planogram(0.0, 256.0, 128.0, 128.0, 2.0, 0.5, 0.25)
+    s.set_default_volume()
+    # X from L, Y from R (half lengths 64 and 128) at the bin pitch
+    assert (s.numX(), s.numY(), s.numZ()) == (64, 128, 64)
+    assert s.voxelWidth() == 2.0
+
+
+def test_host_elementwise_rules_match_reference():
+    z = load_golden("cpu_rules.npz")
+    from petl_b200 import PETLserver
+    s = PETLserver()
+    den = z["rd_den"].copy()
+    s.rdivide(den, z["rd_num"].copy())
+    assert np.array_equal(den, z["rd_out"])
+    x = z["div_x"].copy()
+    s.divide(x, z["div_y"].copy())
+    assert np.array_equal(x, z["div_out"])
+    r = z["recip_in"].copy()
+    s.reciprocal(r, 7.0)
+    assert np.array_equal(r, z["recip_out"])
+    a, b = z["rd_num"][2].copy(), z["rd_den"][2].copy()
+    assert s.inner_product(a, b) == np.float32(z["ip"])
+
+
+def test_unsupported_reference_calls_fail_cleanly():
+    L = lib()
+    assert not L.voxelize(None, 1)
+    assert not L.ray_trace(None, 1)
+    assert L.clear_phantom()

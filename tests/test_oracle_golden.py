@@ -1,0 +1,147 @@
+"""The CPU oracle against golden vectors produced by the reference library.
+
+These pin the oracle before it is trusted as the checker of the CUDA path.
+Tolerances: the reference's forward projector, PFDR and regularizers are
+plain float arithmetic, so the FP64 oracle must agree to ~1e-6 relative L2.
+The reference's backprojector interpolates through texture hardware whose
+linear-filter weights are fixed point (8 fractional bits), which moves its
+output by ~1.5e-4 relative L2 from exact-weight arithmetic; FBP and MLEM end
+in that backprojector.  Those comparisons hold a 1e-3 bound, and the oracle's
+8-bit weight emulation must come closer to the reference than exact weights.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import load_golden, rel_l2
+from helpers import oracle_geoms
+
+PROJ_CASES = ["g0", "g90", "g30", "gpitch", "gpetx", "g0t1"]
+
+
+@pytest.mark.parametrize("name", PROJ_CASES)
+def test_forward_projector_matches_reference(name):
+    z = load_golden(f"proj_{name}.npz")
+    geoms = oracle_geoms(z)
+    g = O.project(geoms, z["f"])
+    gn = O.project(geoms, z["f_noise"])
+    for i in range(len(geoms)):
+        assert rel_l2(g[i], z[f"g{i}"]) < 2e-6
+        assert rel_l2(gn[i], z[f"gnoise{i}"]) < 2e-6
+
+
+@pytest.mark.parametrize("name", PROJ_CASES)
+def test_backprojector_matches_reference_within_texture_error(name):
+    z = load_golden(f"proj_{name}.npz")
+    geoms = oracle_geoms(z)
+    ys = [z[f"y{i}"] for i in range(len(geoms))]
+    exact = O.backproject(geoms, ys, texmode=0)
+    emul = O.backproject(geoms, ys, texmode=1)
+    e_exact, e_emul = rel_l2(exact, z["b"]), rel_l2(emul, z["b"])
+    assert e_exact < 5e-4
+    assert e_emul < e_exact
+    # with unit data only the border taps see the weights: the emulation is exact there
+    sens = O.backproject(geoms, [np.ones(G.shape) for G in geoms], texmode=1)
+    assert rel_l2(sens, z["sens"]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["g0", "g0t1"])
+def test_pfdr_and_fbp_match_reference(name):
+    z = load_golden(f"pfdr_{name}.npz")
+    G = oracle_geoms(z)[0]
+    assert rel_l2(O.pfdr(G, z["g"]), z["g_reb"]) < 1e-6
+    assert tuple(z["shape_after"]) == (1, G.N_v0, G.N_u1, G.N_u0)
+    assert rel_l2(O.fbp(G, z["g"]), z["fbp"]) < 1e-3
+
+
+def test_mlem_matches_reference_call_sequence():
+    z = load_golden("mlem_g0.npz")
+    G = oracle_geoms(z)[0]
+    for tag, beta in (("plain", 0.0), ("rd", 0.05)):
+        for n in (1, 4):
+            f = O.mlem(G, z["g"], n, beta=beta, delta=2.0)
+            assert rel_l2(f, z[f"f_{tag}"][n - 1]) < 1e-3
+
+
+def test_regularizers_match_reference():
+    r = load_golden("regularizers.npz")
+    for tag in ("3d", "2d"):
+        f, d = r[f"f_{tag}"], r[f"d_{tag}"]
+        assert rel_l2(O.rd_gradient(f, 2.0, 0.01), r[f"rd_grad_{tag}"]) < 1e-6
+        for delta, p in ((0.05, 1.0), (0.3, 1.2)):
+            key = f"{tag}_d{delta}_p{p}"
+            assert rel_l2(O.tv_gradient(f, delta, 0.7, p), r[f"tv_grad_{key}"]) < 1e-6
+            assert abs(O.tv_cost(f, delta, 0.7, p) / r[f"tv_cost_{key}"] - 1) < 1e-6
+            assert abs(O.tv_quadform(f, d, delta, 0.7, p) / r[f"tv_quad_{key}"] - 1) < 1e-6
+        assert rel_l2(O.diffuse(f, 0.05, 3, 1.0), r[f"diffuse_{tag}"]) < 1e-6
+        assert rel_l2(O.tv_denoise(f, 0.05, 0.5, 3, 1.0), r[f"tvdenoise_{tag}"]) < 1e-6
+
+
+def test_geometry_shapes_match_reference():
+    z = load_golden("cpu_rules.npz")
+    for call, shape in zip(z["geom_calls"], z["geom_shapes"]):
+        psi, D, L, H, T, vm0, vm1 = call
+        G = O.make_geom(psi, D, L, H, T, vm0, vm1, (8, 8, 8, 1.0))
+        assert G.shape == tuple(shape)
+
+
+def test_optimal_fft_sizes():
+    # smallest 2^(n+1) 3^m >= N, as the reference's search finds it
+    for n, want in [(33, 36), (65, 72), (129, 144), (128, 128), (256, 256), (512, 512), (130, 144), (220, 256)]:
+        assert O.optimal_fft_size(n) == want
+    # the search agrees with brute force everywhere except N = 486 = 2*3^5,
+    # where its loop bound skips the exact fit and returns 512
+    for n in range(3, 1200):
+        bf = min(2 ** (a + 1) * 3 ** b for a in range(12) for b in range(8) if 2 ** (a + 1) * 3 ** b >= n)
+        assert O.optimal_fft_size(n) == (512 if n == 486 else bf)
+
+
+def test_oracle_fft_matches_numpy():
+    rng = np.random.default_rng(0)
+    for n in (2, 6, 72, 128, 144, 256, 432, 512):
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        assert np.abs(O.fft_c2c(x) - np.fft.fft(x)).max() < 1e-11 * n
+
+
+def test_ramp_impulse_response_closed_form():
+    # a unit impulse at u0 = k comes back as h(s) = 1/(T pi (1/4 - s^2))
+    G = O.make_geom(0, 64, 32, 16, 2, 0.5, 0.25, (32, 32, 8, 2.0))
+    Gr = O.rebinned_geom(G)
+    rows = np.zeros((1, G.N_u0))
+    k = 10
+    rows[0, k] = 1.0
+    out = O.ramp(Gr, rows)[0]
+    s = np.arange(G.N_u0) - k
+    h = 1.0 / (G.T_u0 * np.pi * (0.25 - s.astype(np.float64) ** 2))
+    assert np.abs(out - h.astype(np.float32)).max() < 1e-6 * np.abs(h).max()
+
+
+def test_single_voxel_tent_footprint():
+    # psi = 0, voxel pitch = bin pitch: each plane contributes tent weights
+    G = O.make_geom(0, 64, 32, 16, 2, 0.5, 0.25, (32, 32, 8, 2.0))
+    f = np.zeros(G.vol_shape)
+    f[4, 16, 16] = 1.0
+    g = O.project(G, f)[0]
+    iv1, iv0 = G.N_v1 // 2, G.N_v0 // 2    # v1 = 0, v0 = 0: the column maps onto one bin
+    col = g[iv1, iv0]
+    nz = np.argwhere(col > 0)
+    assert len(nz) == 1
+    x = G.x_0 + 16 * G.voxelWidth
+    iu0 = int(round((x - G.u0_0) / G.T_u0))
+    assert tuple(nz[0]) == (4, iu0)
+    assert abs(col[4, iu0] - G.voxelWidth) < 1e-6
+
+
+def test_nnz_counts_taps():
+    G = O.make_geom(0, 64, 32, 16, 2, 0.5, 0.25, (32, 32, 8, 2.0))
+    n = O.project_nnz(G)
+    # at most 4 taps per (ray, plane), at least one plane hit per visible ray
+    assert 0 < n <= 4 * np.prod(G.shape) * G.numY
+
+
+def test_osem_one_subset_is_mlem():
+    z = load_golden("mlem_g0.npz")
+    G = oracle_geoms(z)[0]
+    a = O.mlem(G, z["g"], 2)
+    b = O.osem(G, z["g"], 2, 1)
+    assert rel_l2(a, b) < 1e-12
