@@ -61,6 +61,12 @@ int petl_optimal_fft_size(int N);
  * volume is defined) as set through the petl.h setters. */
 int petl_model_geometry(int which, petl_geom* out);
 
+/* Kernel dispatch for the projectors: 0 (default) uses the shear-warp
+ * kernels for axis-aligned, equal-pitch geometries and the general kernels
+ * otherwise; 1 always uses the general kernels.  Both compute the same
+ * operator. */
+int petl_set_dispatch(int mode);
+
 /* Forward SF projection (src/projectors.cu:11-238).  Computes the views
  * iv0 = iv0_first + k*iv0_step (k = 0.., iv0 < N_v0) of every v1 slice and
  * writes them into the full-size planogram g; other views are untouched.

@@ -484,7 +484,9 @@ void oracle_project_f32(const oracle_geom* G, const float* f, float* g, int n) {
 void oracle_backproject_f64(const oracle_geom* G, const double* g, double* f, int tm, int n) { backproject<double>(*G, g, f, tm, n); }
 void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int tm, int n) { backproject<float>(*G, g, f, tm, n); }
 
-double oracle_project_nnz(const oracle_geom* G, int nthreads)
+double oracle_project_nnz(const oracle_geom* G, int nthreads) { return oracle_project_nnz_t(G, nthreads, 0); }
+
+double oracle_project_nnz_t(const oracle_geom* G, int nthreads, int single)
 {
     set_threads(nthreads);
     const long nview = long(G->N_v1) * G->N_v0;
@@ -495,7 +497,8 @@ double oracle_project_nnz(const oracle_geom* G, int nthreads)
         double c = 0.0;
         for (int iu1 = 0; iu1 < G->N_u1; iu1++)
             for (int iu0 = 0; iu0 < G->N_u0; iu0++)
-                project_ray<double>(*G, (const double*)nullptr, iv1, iv0, iu1, iu0, &c);
+                if (single) project_ray<float>(*G, (const float*)nullptr, iv1, iv0, iu1, iu0, &c);
+                else project_ray<double>(*G, (const double*)nullptr, iv1, iv0, iu1, iu0, &c);
         total += c;
     }
     return total;

@@ -64,6 +64,8 @@ void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int 
 /* Count of (ray, voxel) pairs with a nonzero footprint weight in the forward
  * projector, i.e. nnz(A) for this geometry (the FLOP basis of the roofline). */
 double oracle_project_nnz(const oracle_geom* G, int nthreads);
+/* the same count with the footprint arithmetic in float (single != 0) */
+double oracle_project_nnz_t(const oracle_geom* G, int nthreads, int single);
 
 /* PFDR (src/pfdr.cu:59-315): g[v1][v0][u1][u0] -> g_reb[v0][u1][u0], 2-D
  * transforms done with a mixed radix double FFT. */

@@ -67,6 +67,8 @@ def lib():
         L.oracle_backproject_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int]
         L.oracle_project_nnz.argtypes = [gp, ctypes.c_int]
         L.oracle_project_nnz.restype = ctypes.c_double
+        L.oracle_project_nnz_t.argtypes = [gp, ctypes.c_int, ctypes.c_int]
+        L.oracle_project_nnz_t.restype = ctypes.c_double
         L.oracle_pfdr_f64.argtypes = [gp, dp, dp, ctypes.c_int]
         L.oracle_ramp_f64.argtypes = [gp, dp, ctypes.c_long, ctypes.c_int]
         L.oracle_fft_c2c.argtypes = [dp, ctypes.c_int, ctypes.c_int]
@@ -173,8 +175,8 @@ def backproject(geoms, g, dtype=np.float64, texmode=0, nthreads=0):
     return f
 
 
-def project_nnz(G, nthreads=0):
-    return lib().oracle_project_nnz(ctypes.byref(G), nthreads)
+def project_nnz(G, nthreads=0, single=False):
+    return lib().oracle_project_nnz_t(ctypes.byref(G), nthreads, 1 if single else 0)
 
 
 # ----------------------------------------------------------------------------

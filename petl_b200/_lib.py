@@ -73,6 +73,7 @@ _DEV_API = [
     ("petl_geom_set_volume", c_i, [_G, c_i, c_i, c_i, c_f, c_f, c_f, c_f, c_f]),
     ("petl_optimal_fft_size", c_i, [c_i]),
     ("petl_model_geometry", c_i, [c_i, _G]),
+    ("petl_set_dispatch", c_i, [c_i]),
     ("petl_project_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_vp]),
     ("petl_project_range_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_backproject_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_vp]),

@@ -101,6 +101,14 @@ using namespace petl;
 
 extern "C" {
 
+int petl_set_dispatch(int mode)
+{
+    // 0: choose the shear kernels where eligible, 1: always the general kernels
+    if (mode != 0 && mode != 1) return -1;
+    g_force_general = mode;
+    return 0;
+}
+
 int petl_project_dev(const petl_geom* G, const float* f, float* g, int iv0_first, int iv0_step, void* stream)
 {
     clear_error();
