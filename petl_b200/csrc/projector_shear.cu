@@ -21,7 +21,10 @@
 // arithmetic the reference's float code approximates); ray masks and the
 // reference backprojector's voxel-centre test are evaluated with the same
 // float expressions as the reference (see projector.cuh) and tabulated.
+#include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "projector.cuh"
@@ -457,3 +460,4 @@ int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int m
 }
 
 }  // namespace petl
+
