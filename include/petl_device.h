@@ -79,6 +79,21 @@ int petl_project_dev(const petl_geom* G, const float* f, float* g, int iv0_first
 int petl_backproject_dev(const petl_geom* G, const float* g, float* f, int mode, int accumulate, float scale,
                          int iv0_first, int iv0_step, void* stream);
 
+/* Allocation-free forward projection of every view; no counterpart in the
+ * reference.  For callers that must not allocate device memory while they
+ * run (a real-time acquisition thread that cannot block on the allocator, a
+ * program whose own pool owns the GPU's memory).  It computes the same
+ * projection as petl_project_dev but keeps its scratch tables in a fixed
+ * 4 MiB device array that every GPU loading the library holds until exit,
+ * and calls no cudaMalloc/cudaFree or allocating library routine.  A
+ * geometry whose tables exceed 4 MiB is rejected with an error (nonzero
+ * return, message in petl_last_error()).  All calls on one device share the
+ * array, so calls that overlap on the GPU race; each call rewrites the
+ * tables it reads, so no clearing is needed.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture. */
+int petl_project_noalloc_dev(const petl_geom* G, const float* f, float* g, void* stream);
+
 /* Same as petl_project_dev restricted to the v1 slices [iv1_begin, iv1_end). */
 int petl_project_range_dev(const petl_geom* G, const float* f, float* g, int iv1_begin, int iv1_end, int iv0_first,
                            int iv0_step, void* stream);

@@ -76,6 +76,7 @@ _DEV_API = [
     ("petl_set_dispatch", c_i, [c_i]),
     ("petl_project_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_vp]),
     ("petl_project_range_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
+    ("petl_project_noalloc_dev", c_i, [_G, c_vp, c_vp, c_vp]),
     ("petl_backproject_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_vp]),
     ("petl_backproject_range_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_ratio_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),

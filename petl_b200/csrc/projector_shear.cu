@@ -377,6 +377,51 @@ int make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st)
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free forward projection.
+//
+// Some callers cannot allocate device memory while they run: a real-time
+// acquisition thread that must not block on the allocator, a host program
+// that hands the GPU's whole memory to its own pool, or code that must not
+// change the device's memory state between two measurements.  For them the
+// shear tables of the forward projector live in the fixed array below
+// instead of stream-ordered scratch.  The array is a module global: every
+// GPU that loads this library holds it (4 MiB) until the process exits, and
+// all calls on one device share it, so calls that overlap on the GPU (other
+// streams, other host threads) race on its contents.  Each call rewrites the
+// whole table region it uses before reading it, so nothing needs clearing
+// between calls.
+constexpr size_t kNoAllocTableBytes = size_t(4) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_tables[kNoAllocTableBytes];
+
+size_t table_bytes(const petl_geom& G)
+{
+    const size_t nx = size_t(G.N_v0) * G.numY, nz = size_t(G.N_v1) * G.numY, ns = size_t(G.N_v1) * G.N_v0;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    return al(nx * sizeof(Shift)) + al(nz * sizeof(Shift)) + al(ns * 4) + al(nz * sizeof(int2)) +
+           al(G.N_v0 * sizeof(int2)) + al(G.N_v1 * sizeof(int2));
+}
+
+// Device address of the fixed table array, looked up once per device with
+// that device current (the host-side name of the array is not a device
+// address).
+int noalloc_table_base(void** out)
+{
+    static std::mutex mu;
+    static void* base[64] = {nullptr};
+    int dev = 0;
+    PETL_CUDA(cudaGetDevice(&dev));
+    PETL_REQUIRE(dev >= 0 && dev < 64, "no-alloc projection: device index out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!base[dev]) {
+        void* p = nullptr;
+        PETL_CUDA(cudaGetSymbolAddress(&p, g_noalloc_tables));
+        base[dev] = p;
+    }
+    *out = base[dev];
+    return 0;
+}
+
 }  // namespace
 
 bool shear_eligible(const petl_geom& G)
@@ -461,3 +506,60 @@ int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int m
 
 }  // namespace petl
 
+using namespace petl;
+
+extern "C" int petl_project_noalloc_dev(const petl_geom* G, const float* f, float* g, void* stream)
+{
+    clear_error();
+    std::string why;
+    PETL_REQUIRE(G && f && g && geom_valid(G, &why), "project_noalloc: invalid arguments " + why);
+    cudaStream_t st = as_stream(stream);
+    const ViewRange vr{0, G->N_v1, 0, 1};
+    // geometries outside the shear kernels' domain use the general kernel,
+    // which needs no scratch memory at all
+    if (!shear_eligible(*G)) return launch_project_general(*G, f, g, vr, nullptr, st);
+    const size_t need = table_bytes(*G);
+    if (need > kNoAllocTableBytes) {
+        set_error("project_noalloc: this geometry needs " + std::to_string(need) +
+                  " bytes of table scratch; the allocation-free entry point holds at most " +
+                  std::to_string(kNoAllocTableBytes) + " bytes");
+        return -1;
+    }
+    void* base = nullptr;
+    int rc = noalloc_table_base(&base);
+    if (rc) return rc;
+    // same table layout as the allocating path, placed in the fixed array
+    const size_t nx = size_t(G->N_v0) * G->numY, nz = size_t(G->N_v1) * G->numY, ns = size_t(G->N_v1) * G->N_v0;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    Tables T{};
+    char* p = static_cast<char*>(base);
+    T.xt = reinterpret_cast<Shift*>(p);
+    p += al(nx * sizeof(Shift));
+    T.zt = reinterpret_cast<Shift*>(p);
+    p += al(nz * sizeof(Shift));
+    T.S = reinterpret_cast<float*>(p);
+    p += al(ns * 4);
+    T.zvis = reinterpret_cast<int2*>(p);
+    p += al(nz * sizeof(int2));
+    T.ub0 = reinterpret_cast<int2*>(p);
+    p += al(G->N_v0 * sizeof(int2));
+    T.ub1 = reinterpret_cast<int2*>(p);
+    const size_t n = std::max(std::max(nx, nz), std::max(ns, size_t(std::max(G->N_v0, G->N_v1))));
+    k_shear_tables<<<ceil_div(n, 256), 256, 0, st>>>(*G, T);
+    PETL_LAUNCH_CHECK("shear_tables (no-alloc)");
+    const double ymax =
+        std::max(std::fabs(double(G->y_0)), std::fabs(double(G->y_0) + (G->numY - 1) * double(G->T_x)));
+    const int spread = int(std::ceil(double(F_V1) * double(G->T_v1) * ymax / double(G->T_z))) + 4;
+    FwdArgs A{};
+    A.G = *G;
+    A.vr = vr;
+    A.n_colblk = int(ceil_div(G->N_u0, 32));
+    A.maxr = F_ROWS + spread + 1;
+    A.T = T;
+    const size_t smem = size_t(2) * A.maxr * 32 * sizeof(float);
+    PETL_CUDA(cudaFuncSetAttribute(k_fwd_shear, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    dim3 grid(unsigned(G->N_v0), ceil_div(G->N_v1, F_V1), unsigned(A.n_colblk) * ceil_div(G->N_u1, F_ROWS));
+    k_fwd_shear<<<grid, F_THREADS, smem, st>>>(f, g, nullptr, A);
+    PETL_LAUNCH_CHECK("project_noalloc");
+    return 0;
+}
