@@ -62,10 +62,20 @@ int petl_optimal_fft_size(int N);
 int petl_model_geometry(int which, petl_geom* out);
 
 /* Kernel dispatch for the projectors: 0 (default) uses the shear-warp
- * kernels for axis-aligned, equal-pitch geometries and the general kernels
- * otherwise; 1 always uses the general kernels.  Both compute the same
- * operator. */
+ * kernels for axis-aligned, equal-pitch geometries (TMA-staged where the
+ * layout allows) and the general kernels otherwise; 1 always uses the
+ * general kernels; 2 uses the shear-warp kernels without TMA staging where
+ * the shear path applies.  All compute the same operator. */
 int petl_set_dispatch(int mode);
+/* Which projector kernels the calling thread's last projector call used:
+ * 0 general, 1 shear-warp, 2 TMA-staged shear-warp; -1 before any call. */
+int petl_last_projector_path(void);
+
+/* Error word written by kernels whose waits on asynchronous copies are
+ * bounded: nonzero if a wait gave up (the call's result is then invalid).
+ * Reading it synchronizes the device and clears it.  -1 if it cannot be
+ * read. */
+int petl_device_error_flag(void);
 
 /* Forward SF projection (src/projectors.cu:11-238).  Computes the views
  * iv0 = iv0_first + k*iv0_step (k = 0.., iv0 < N_v0) of every v1 slice and

@@ -74,6 +74,8 @@ _DEV_API = [
     ("petl_optimal_fft_size", c_i, [c_i]),
     ("petl_model_geometry", c_i, [c_i, _G]),
     ("petl_set_dispatch", c_i, [c_i]),
+    ("petl_device_error_flag", c_i, []),
+    ("petl_last_projector_path", c_i, []),
     ("petl_project_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_vp]),
     ("petl_project_range_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_noalloc_dev", c_i, [_G, c_vp, c_vp, c_vp]),

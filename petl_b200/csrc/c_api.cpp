@@ -168,12 +168,13 @@ struct DevBuf {
     float* f() const { return static_cast<float*>(p); }
 };
 
-// v1 slabs per pipeline stage so that one stage moves about 64 MB
+// v1 slices per pipeline stage: a multiple of 16 (the slopes one forward
+// CTA covers, so no stage launches part-empty tiles) moving up to ~256 MB
 int slab_step(const petl_geom& G)
 {
     const double slab_bytes = double(G.N_v0) * G.N_u1 * G.N_u0 * 4.0;
-    const int s = int(std::max(1.0, std::floor(64.0e6 / std::max(slab_bytes, 1.0))));
-    return std::min(s, G.N_v1);
+    const int blocks = int(std::max(1.0, std::floor(256.0e6 / std::max(16.0 * slab_bytes, 1.0))));
+    return std::min(16 * blocks, G.N_v1);
 }
 
 // ---------------------------------------------------------------------------

@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "projector.cuh"
+#include "shear.cuh"
 
 namespace petl {
 int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st);
@@ -23,16 +24,21 @@ int launch_project_shear(const petl_geom& G, const float* f, float* g, const Vie
 int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
                              const ViewRange& vr, cudaStream_t st);
 
-int g_force_general = -1;  // -1: read PETL_FORCE_GENERAL once
+int g_dispatch = -1;  // -1: read PETL_FORCE_GENERAL once
 
-bool use_shear(const petl_geom& G)
+int dispatch_mode()
 {
-    if (g_force_general < 0) {
+    if (g_dispatch < 0) {
         const char* e = getenv("PETL_FORCE_GENERAL");
-        g_force_general = (e && e[0] == '1') ? 1 : 0;
+        g_dispatch = (e && e[0] == '1') ? 1 : 0;
     }
-    return !g_force_general && shear_eligible(G);
+    return g_dispatch;
 }
+
+bool use_shear(const petl_geom& G) { return dispatch_mode() != 1 && shear_eligible(G); }
+
+thread_local int t_last_path = -1;
+void note_path(int path) { t_last_path = path; }
 
 bool range_ok(const petl_geom& G, const ViewRange& vr)
 {
@@ -48,6 +54,7 @@ int project_range(const petl_geom& G, const float* f, float* g, const ViewRange&
     PETL_REQUIRE(f && g && range_ok(G, vr), "project: invalid arguments");
     if (vr.iv1_begin == vr.iv1_end || vr.iv0_first >= G.N_v0) return 0;
     if (use_shear(G)) return launch_project_shear(G, f, g, vr, meas, st);
+    note_path(0);
     return launch_project_general(G, f, g, vr, meas, st);
 }
 
@@ -59,6 +66,7 @@ int backproject_range(const petl_geom& G, const float* g, float* f, int mode, in
     PETL_REQUIRE(f && g && range_ok(G, vr), "backproject: invalid arguments");
     PETL_REQUIRE(mode == PETL_BP_REFERENCE || mode == PETL_BP_ADJOINT, "backproject: unknown mode");
     if (use_shear(G)) return launch_backproject_shear(G, g, f, mode, accumulate, scale, vr, st);
+    note_path(0);
     return launch_backproject_general(G, g, f, mode, accumulate, scale, vr, st);
 }
 
@@ -101,11 +109,14 @@ using namespace petl;
 
 extern "C" {
 
+int petl_last_projector_path(void) { return t_last_path; }
+
 int petl_set_dispatch(int mode)
 {
-    // 0: choose the shear kernels where eligible, 1: always the general kernels
-    if (mode != 0 && mode != 1) return -1;
-    g_force_general = mode;
+    // 0: the fastest kernels that apply; 1: always the general kernels;
+    // 2: shear kernels without TMA staging where the shear path applies
+    if (mode < 0 || mode > 2) return -1;
+    g_dispatch = mode;
     return 0;
 }
 

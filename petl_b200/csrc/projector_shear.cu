@@ -28,24 +28,15 @@
 
 #include "common.cuh"
 #include "projector.cuh"
+#include "shear.cuh"
 
 namespace petl {
 
+using shear::Shift;
+using shear::Tables;
+using shear::TableBuf;
+
 namespace {
-
-struct Shift {
-    int d;    // integer part of the shift
-    float w;  // fractional weight of the second tap
-};
-
-struct Tables {
-    Shift* xt;      // [N_v0][N_y]
-    Shift* zt;      // [N_v1][N_y]
-    float* S;       // [N_v1][N_v0]  l_phi * rsqrt(1 + v0^2 + v1^2)
-    int2* zvis;     // [N_v1][N_y]   voxel-centre visible iz range (reference backprojector)
-    int2* ub0;      // [N_v0]        visible iu0 range of the forward masks
-    int2* ub1;      // [N_v1]        visible iu1 range of the forward masks
-};
 
 // forward tile: 16 v1 x 32 rows x 32 columns, one v0 per CTA
 constexpr int FV = 4;    // v1 slopes per thread
@@ -344,14 +335,9 @@ k_bwd_shear(const float* __restrict__ g, float* __restrict__ f, const BwdArgs A)
     }
 }
 
-// per-call table workspace
-struct TableBuf {
-    void* base = nullptr;
-    Tables T{};
-    size_t bytes = 0;
-};
+}  // namespace
 
-int make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st)
+int shear::make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st)
 {
     const size_t nx = size_t(G.N_v0) * G.numY, nz = size_t(G.N_v1) * G.numY, ns = size_t(G.N_v1) * G.N_v0;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
@@ -376,6 +362,8 @@ int make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st)
     PETL_LAUNCH_CHECK("shear_tables");
     return 0;
 }
+
+namespace {
 
 // ---------------------------------------------------------------------------
 // Allocation-free forward projection.
@@ -442,8 +430,17 @@ int launch_project_shear(const petl_geom& G, const float* f, float* g, const Vie
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (n_v0 <= 0 || nv1 <= 0) return 0;
     TableBuf tb;
-    int rc = make_tables(G, tb, st);
+    int rc = shear::make_tables(G, tb, st);
     if (rc) return rc;
+    if (dispatch_mode() != 2) {
+        rc = shear::project_tma(G, f, g, vr, meas, tb.T, st);
+        if (rc != shear::kNotApplicable) {
+            note_path(2);
+            cudaFreeAsync(tb.base, st);
+            return rc;
+        }
+    }
+    note_path(1);
     // rows of the staged slab: 32 output rows + the spread of 16 slopes + 1
     const double ymax = std::max(std::fabs(double(G.y_0)), std::fabs(double(G.y_0) + (G.numY - 1) * double(G.T_x)));
     const int spread = int(std::ceil(double(F_V1) * double(G.T_v1) * ymax / double(G.T_z))) + 4;
@@ -473,8 +470,17 @@ int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int m
                              const ViewRange& vr, cudaStream_t st)
 {
     TableBuf tb;
-    int rc = make_tables(G, tb, st);
+    int rc = shear::make_tables(G, tb, st);
     if (rc) return rc;
+    if (dispatch_mode() != 2) {
+        rc = shear::backproject_tma(G, g, f, mode, accumulate, scale, vr, tb.T, st);
+        if (rc != shear::kNotApplicable) {
+            note_path(2);
+            cudaFreeAsync(tb.base, st);
+            return rc;
+        }
+    }
+    note_path(1);
     BwdArgs A{};
     A.G = G;
     A.vr = vr;

@@ -1,0 +1,56 @@
+// Shift tables shared by the shear-warp projector kernels (projector_shear.cu,
+// projector_shear_tma.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "projector.cuh"
+
+namespace petl {
+namespace shear {
+
+struct Shift {
+    int d;    // integer part of the shift
+    float w;  // fractional weight of the second tap
+};
+
+struct Tables {
+    Shift* xt;      // [N_v0][N_y]
+    Shift* zt;      // [N_v1][N_y]
+    float* S;       // [N_v1][N_v0]  l_phi * rsqrt(1 + v0^2 + v1^2)
+    int2* zvis;     // [N_v1][N_y]   voxel-centre visible iz range (reference backprojector)
+    int2* ub0;      // [N_v0]        visible iu0 range of the forward masks
+    int2* ub1;      // [N_v1]        visible iu1 range of the forward masks
+};
+
+// per-call table workspace (stream-ordered)
+struct TableBuf {
+    void* base = nullptr;
+    Tables T{};
+    size_t bytes = 0;
+};
+
+int make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st);
+
+// Return value of the TMA launchers when the geometry or the buffers do not
+// fit their layout rules; the caller then uses the first-generation kernels.
+constexpr int kNotApplicable = -2;
+
+// TMA-staged kernels (projector_shear_tma.cu).  They compute the same
+// operator as the first-generation kernels of projector_shear.cu.
+int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                const Tables& T, cudaStream_t st);
+int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                    const ViewRange& vr, const Tables& T, cudaStream_t st);
+
+}  // namespace shear
+
+// Projector kernel choice (petl_set_dispatch): 0 automatic, 1 general kernels
+// only, 2 shear kernels without TMA staging where the shear path applies.
+int dispatch_mode();
+// Records which projector kernels the calling thread used last
+// (petl_last_projector_path): 0 general, 1 shear, 2 TMA-staged shear.
+void note_path(int path);
+
+}  // namespace petl

@@ -1,0 +1,169 @@
+"""The TMA-staged shear-warp kernels against the first-generation shear
+kernels, the general kernels and the FP64 oracle.
+
+Dispatch 0 runs the TMA-staged kernels wherever their layout rules hold
+(volume rows a multiple of 4 floats for the forward copy, N_u0 a multiple of
+4 and at most 256 for the backward); dispatch 2 runs the first-generation
+shear kernels; dispatch 1 the general kernels.  The forward TMA kernel does
+the same float operations in the same order as the first-generation one, so
+the two agree to rounding of the final scale; the backward kernels sum in a
+different order and agree to float accuracy.  Every case also checks that no
+bounded wait gave up (petl_device_error_flag) and which kernels ran.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_l2
+from helpers import ellipsoids
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    # psi, D, L, H, T, v_m0, v_m1 ; volume ; TMA forward, TMA backward expected
+    "t2": ((0.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (64, 64, 16, 2.0), True, True),
+    "t1": ((0.0, 128.0, 64.0, 32.0, 1.0, 0.5, 0.25), (128, 128, 32, 1.0), True, True),
+    # the dual-panel geometry of the 128x128x64 / 2 mm recon: planogram (33, 65, 64, 128)
+    "panel2mm": ((0.0, 256.0, 128.0, 64.0, 2.0, 0.5, 0.25), (128, 128, 64, 2.0), True, True),
+    # ragged sizes, off-centre volume, rows a multiple of 4
+    "rag4": ((0.0, 100.0, 75.0, 27.0, 1.5, 0.45, 0.2), (52, 60, 18, 1.5, 1.5, 3.0, -4.5, 1.5), True, True),
+    # rows not a multiple of 4 floats: falls back to the first-generation kernels
+    "odd": ((0.0, 100.0, 50.0, 26.0, 1.5, 0.45, 0.2), (50, 58, 15, 1.5, 1.5, 3.0, -4.5, 1.5), False, False),
+}
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _setup(name, cuda, seed=0):
+    from petl_b200 import Geometry
+    args, vol, _, _ = CASES[name]
+    G = Geometry(*args, volume=vol)
+    Go = O.make_geom(*args, vol)
+    rng = np.random.default_rng(seed)
+    f = ellipsoids(G.vol_shape, (vol[3], vol[4] if len(vol) > 4 else vol[3]), rng, 8) + \
+        0.1 * rng.random(G.vol_shape).astype(np.float32)
+    return G, Go, f, rng
+
+
+def _under(mode, fn):
+    """fn() under dispatch mode, and the kernel path it took."""
+    import torch
+    from petl_b200 import lib
+    L = lib()
+    assert L.petl_set_dispatch(mode) == 0
+    try:
+        out = fn()
+        torch.cuda.synchronize()
+        path = L.petl_last_projector_path()
+    finally:
+        L.petl_set_dispatch(0)
+    assert L.petl_device_error_flag() == 0
+    return out, path
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_tma_forward(cuda, name):
+    from petl_b200 import ops
+    G, Go, f, _ = _setup(name, cuda)
+    ft = _t(f, cuda)
+    a, pa = _under(0, lambda: _np(ops.project(G, ft)))
+    b, pb = _under(2, lambda: _np(ops.project(G, ft)))
+    c, pc = _under(1, lambda: _np(ops.project(G, ft)))
+    assert (pa, pb, pc) == (2 if CASES[name][2] else 1, 1, 0)
+    assert rel_l2(a, b) < 1e-6
+    assert rel_l2(a, c) < 1e-5
+    if G.shape[0] * G.shape[1] * G.shape[2] * G.shape[3] < 3e6:
+        assert rel_l2(a, O.project(Go, f)[0]) < 1e-5
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("mode", ["reference", "adjoint"])
+def test_tma_backward(cuda, name, mode):
+    from petl_b200 import ops
+    G, Go, f, rng = _setup(name, cuda)
+    y = _t(rng.random(G.shape), cuda)
+    a, pa = _under(0, lambda: _np(ops.backproject(G, y, mode=mode)))
+    b, pb = _under(2, lambda: _np(ops.backproject(G, y, mode=mode)))
+    c, pc = _under(1, lambda: _np(ops.backproject(G, y, mode=mode)))
+    assert (pa, pb, pc) == (2 if CASES[name][3] else 1, 1, 0)
+    assert rel_l2(a, b) < 1e-5
+    assert rel_l2(a, c) < 1e-5
+    if mode == "reference" and G.shape[0] * G.shape[1] * G.shape[2] * G.shape[3] < 3e6:
+        assert rel_l2(a, O.backproject(Go, _np(y))) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["t1", "panel2mm", "rag4"])
+def test_tma_pair_is_exact_adjoint(cuda, name):
+    import torch
+    from petl_b200 import ops
+    G, _, f, rng = _setup(name, cuda)
+    x = _t(rng.random(G.vol_shape), cuda)
+    y = _t(rng.random(G.shape), cuda)
+    (Ax, Aty), path = _under(0, lambda: (ops.project(G, x), ops.backproject(G, y, mode="adjoint")))
+    assert path == 2
+    lhs = float(torch.sum(Ax.double() * y.double()))
+    rhs = float(torch.sum(x.double() * Aty.double()))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def test_tma_subsets_slabs_ratio_accumulate(cuda):
+    import torch
+    from petl_b200 import ops
+    G, _, f, rng = _setup("panel2mm", cuda)
+    ft = _t(f, cuda)
+
+    def run():
+        full = ops.project(G, ft)
+        parts = torch.zeros_like(full)
+        for s in range(4):
+            ops.project(G, ft, parts, subset=(s, 4))
+        slabs = torch.zeros_like(full)
+        ops.project(G, ft, slabs, v1_range=(0, 5))
+        ops.project(G, ft, slabs, v1_range=(5, G.shape[0]))
+        meas = torch.poisson(full * 20.0, generator=torch.Generator(device=full.device).manual_seed(3))
+        ratio = ops.project_ratio(G, ft, meas)
+        y = _t(rng.random(G.shape), cuda)
+        b = ops.backproject(G, y)
+        b2 = ops.backproject(G, y, subset=(0, 3))
+        for s in (1, 2):
+            ops.backproject(G, y, f=b2, subset=(s, 3), accumulate=True)
+        b3 = ops.backproject(G, y, v1_range=(0, 7))
+        ops.backproject(G, y, f=b3, v1_range=(7, G.shape[0]), accumulate=True)
+        b4 = ops.backproject(G, y, scale=2.5)
+        return full, parts, slabs, meas, ratio, b, b2, b3, b4
+
+    (full, parts, slabs, meas, ratio, b, b2, b3, b4), path = _under(0, run)
+    assert path == 2
+    assert torch.equal(full, parts)
+    assert torch.equal(full, slabs)
+    want = torch.where(full == 0, torch.zeros_like(full), meas / full)
+    assert rel_l2(_np(ratio), _np(want)) < 1e-6
+    assert rel_l2(_np(b2), _np(b)) < 1e-6
+    assert rel_l2(_np(b3), _np(b)) < 1e-6
+    assert rel_l2(_np(b4), 2.5 * _np(b)) < 1e-6
+
+
+def test_tma_full_size_against_first_generation(cuda):
+    """The 256x256x128 volume and (65, 129, 128, 256) planogram of the benchmark."""
+    import torch
+    from petl_b200 import Geometry, ops
+    G = Geometry(0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25, volume=(256, 256, 128, 1.0))
+    gen = torch.Generator(device=cuda).manual_seed(5)
+    f = torch.rand(G.vol_shape, device=cuda, generator=gen)
+    a, pa = _under(0, lambda: ops.project(G, f))
+    b, pb = _under(2, lambda: ops.project(G, f))
+    assert (pa, pb) == (2, 1)
+    assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 1e-6
+    del b
+    for mode in ("reference", "adjoint"):
+        x, px = _under(0, lambda: ops.backproject(G, a, mode=mode))
+        z, pz = _under(2, lambda: ops.backproject(G, a, mode=mode))
+        assert (px, pz) == (2, 1)
+        assert float(torch.linalg.vector_norm(x - z) / torch.linalg.vector_norm(z)) < 1e-5
