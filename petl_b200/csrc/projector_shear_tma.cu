@@ -5,22 +5,27 @@
 // the staging and the register blocking differ.
 //
 // Forward, k_fwd_tma: one CTA per (view v0, 16 slopes v1, 32 rows u1, 64
-// columns u0).  For each plane y that reaches the tile, one thread starts a
-// TMA copy of the raw volume rows the tile needs (68 columns x nrb rows of
-// plane y; whatever lies outside the volume arrives as zeros) two planes
-// ahead of use.  The CTA interpolates the rows in x into shared memory once,
-// then each warp applies the z interpolation of its 4 slopes from a single
-// register window of K + 4 rows (the integer shifts of 4 consecutive slopes
-// differ by at most 3 rows), two columns per lane with packed FP32 FMAs.
+// columns u0), 16 warps.  For each plane y that reaches the tile, one thread
+// starts a TMA copy of the raw volume rows the tile needs (68 columns x nrb
+// rows of plane y; whatever lies outside the volume arrives as zeros) up to
+// four planes ahead of use.  The CTA interpolates the rows in x into shared
+// memory once, then each warp applies the z interpolation of its 4 slopes
+// for 8 rows from a single register window of 12 rows (the integer shifts of
+// 4 consecutive slopes differ by at most 3 rows), two columns per lane.
 //
-// Backward, k_bwd_tma<ADJ>: one CTA per (8 planes y, 8 rows z, all columns).
-// For every (view v0, slope v1) whose rows reach the tile, one thread starts a
-// TMA copy of the planogram rows the tile needs (N_u0 columns x brb rows) into
-// a 4-stage ring.  Each thread sums, for its 4 planes and 2 columns, the
-// z-interpolated rows of every slope from one register window (the shifts of
-// 4 consecutive planes differ by at most 2 rows); after each view the x shift
-// goes through shared memory into voxel accumulators held in registers.  Each
-// voxel is owned by one CTA: no atomics, one write at the end.
+// Backward, k_bwd_tma<ADJ>: one CTA per (8 planes y, 8 rows z, all columns),
+// one column per lane, 16 warps.  For every (view v0, slope v1) whose rows
+// reach the tile, one thread starts a TMA copy of the planogram rows the tile
+// needs (N_u0 columns x brb rows) into a ring of up to 6 stages.  Each thread
+// sums, for its 4 planes, the z-interpolated rows of every slope from one
+// register window (the shifts of 4 consecutive planes differ by at most 2
+// rows); after each view the x shift goes through shared memory into voxel
+// accumulators held in registers.  Each voxel is owned by one CTA: no
+// atomics, one write at the end.
+//
+// Both keep two warps' worth of independent FMA chains per scheduler with
+// scalar FFMA: at this register budget (<= 128 per thread, 16 warps per SM)
+// that issues at the full FP32 rate, which the packed f32x2 form does not.
 //
 // Every wait on a copy is bounded; a wait that gives up sets the device error
 // word, and the CTA drains its copies in flight and stops without writing.
@@ -45,6 +50,14 @@ enum : int { kErrLayout = 2 };  // a host-side bound on the shift spread did not
 
 __device__ __forceinline__ float2 dup(float a) { return make_float2(a, a); }
 
+// Two scalar FMAs on a column pair.  Scalar FFMA issues at the full FP32
+// rate with two warps per scheduler; the packed f32x2 form needs about four
+// times the warps to reach the same rate on this part.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem()
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -61,7 +74,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 constexpr int FV = 4;              // slopes per warp
 constexpr int FGV = 4;             // warps along v1
 constexpr int FSL = FV * FGV;      // slopes per CTA
-constexpr int FROWS = 32;          // rows per CTA
+constexpr int FROWS = 16;          // rows per CTA
 constexpr int FCOLS = 64;          // columns per CTA, two per lane
 constexpr int FBOXW = FCOLS + 4;   // staged raw columns: 64 + 1 tap + 3 for 16-byte alignment
 constexpr int FDMAX = 3;           // largest shift difference among a warp's slopes
@@ -71,6 +84,7 @@ struct FwdTmaArgs {
     ViewRange vr;
     int n_colblk;  // ceil(N_u0 / 64)
     int nrb;       // staged rows per plane (32 + CTA shift spread + 1, bounded on the host)
+    int nf;        // raw-row buffers in the copy ring
     int fstride;   // floats per raw buffer
     int xstride;   // floats per interpolated buffer
     Tables T;
@@ -85,14 +99,14 @@ struct FwdPlane {
     float wx;   // x tap weight
 };
 
-// Plane geometry of a forward tile: the z shift is monotone in v1, so the
-// extreme shifts sit at the first and last slope.
-__device__ __forceinline__ FwdPlane fwd_plane(const FwdTmaArgs& A, int iv0, int v1a, int v1b, int col0, int row0,
-                                              int y)
+// Plane geometry of a forward tile from the CTA's shared shift tables (x
+// shifts of its view, z shifts of its slopes).  The z shift is monotone in
+// v1, so the extreme shifts sit at the first and last slope.
+__device__ __forceinline__ FwdPlane fwd_plane(const Shift* s_xt, const Shift* s_zt, int nsl, int NY, int col0,
+                                              int row0, int y)
 {
-    const int NY = A.G.numY;
-    const Shift xs = A.T.xt[size_t(iv0) * NY + y];
-    const int da = A.T.zt[size_t(v1a) * NY + y].d, db = A.T.zt[size_t(v1b) * NY + y].d;
+    const Shift xs = s_xt[y];
+    const int da = s_zt[y].d, db = s_zt[(nsl - 1) * NY + y].d;
     FwdPlane p;
     p.dzmin = min(da, db);
     p.cx = col0 + xs.d;
@@ -102,15 +116,19 @@ __device__ __forceinline__ FwdPlane fwd_plane(const FwdTmaArgs& A, int iv0, int 
     return p;
 }
 
+// z taps of one slope: all first-tap FMAs, then all second-tap FMAs (16
+// independent chains per pass; per element the same order as one fused pass)
 template <int O, int K>
 __device__ __forceinline__ void fwd_taps(float2 (&acc)[K], const float2 (&W)[K + FDMAX + 1], float2 w0, float2 w1)
 {
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] = __ffma2_rn(w1, W[k + O + 1], __ffma2_rn(w0, W[k + O], acc[k]));
+    for (int k = 0; k < K; k++) acc[k] = fma2(w0, W[k + O], acc[k]);
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = fma2(w1, W[k + O + 1], acc[k]);
 }
 
 template <int K>
-__global__ void __launch_bounds__(32 * FGV * (FROWS / K), 1)
+__global__ void __launch_bounds__(32 * FGV * (FROWS / K), 2)
 k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const float* __restrict__ meas,
           const FwdTmaArgs A)
 {
@@ -124,16 +142,20 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
     const int iv0 = A.vr.iv0_first + blockIdx.x * A.vr.iv0_step;
     const int v1a = A.vr.iv1_begin + blockIdx.y * FSL;
     const int v1b = min(v1a + FSL, A.vr.iv1_end) - 1;  // last slope of the CTA
+    const int nsl = v1b - v1a + 1;
     const int rowblk = blockIdx.z / A.n_colblk, colblk = blockIdx.z % A.n_colblk;
     const int cta_row0 = rowblk * FROWS, col0 = colblk * FCOLS;
-    const int v1w = v1a + gv * FV;       // first slope of this warp
+    const int jw = gv * FV;              // first slope of this warp, relative to v1a
     const int row0 = cta_row0 + gr * K;  // first row of this warp
     const int NY = G.numY, NZ = G.numZ, NX = G.numX;
+    const int nf = A.nf;
 
-    float* Fr = reinterpret_cast<float*>(smem);  // [2][nrb][68] raw rows (TMA)
-    float* Xs = Fr + 2 * A.fstride;              // [2][nrb + 3][64] x-interpolated rows
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Xs + 2 * A.xstride);
-    int* s_n = reinterpret_cast<int*>(bar + 2);
+    float* Fr = reinterpret_cast<float*>(smem);                       // [nf][nrb][68] raw rows (TMA)
+    float* Xs = Fr + nf * A.fstride;                                  // [2][nrb + 3][64] x-interpolated rows
+    Shift* s_xt = reinterpret_cast<Shift*>(Xs + 2 * A.xstride);       // [NY] x shifts of view iv0
+    Shift* s_zt = s_xt + NY;                                          // [nsl][NY] z shifts of the slopes
+    uint64_t* bar = reinterpret_cast<uint64_t*>(s_zt + FSL * NY);     // [nf]
+    int* s_n = reinterpret_cast<int*>(bar + nf);
     unsigned short* plist = reinterpret_cast<unsigned short*>(s_n + 2);  // live planes
 
     // a tile outside the visible bins of every slope stays zero
@@ -149,9 +171,8 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
     unsigned wmask = 0;
 #pragma unroll
     for (int j = 0; j < FV; j++) {
-        const int v1 = v1w + j;
-        if (v1 <= v1b) {
-            const int2 u = A.T.ub1[v1];
+        if (jw + j < nsl) {
+            const int2 u = A.T.ub1[v1a + jw + j];
             if (!(row0 > u.y || row0 + K - 1 < u.x)) wmask |= 1u << j;
         }
     }
@@ -163,6 +184,10 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
         for (int k = 0; k < K; k++) acc[j][k] = make_float2(0.0f, 0.0f);
 
     if (live) {  // CTA-uniform
+        // the shift tables this CTA reads, staged once (contiguous rows)
+        for (int e = tid; e < NY; e += NT) s_xt[e] = A.T.xt[size_t(iv0) * NY + e];
+        for (int e = tid; e < nsl * NY; e += NT) s_zt[e] = A.T.zt[size_t(v1a) * NY + e];
+        __syncthreads();
         // planes whose staged window meets the volume, compacted in order
         if (warp == 0) {
             int n = 0;
@@ -170,7 +195,7 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
                 const int y = yb + lane;
                 bool ok = false;
                 if (y < NY) {
-                    const FwdPlane p = fwd_plane(A, iv0, v1a, v1b, col0, cta_row0, y);
+                    const FwdPlane p = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y);
                     ok = !(p.cx + FCOLS < 0 || p.cx >= NX || p.wlo + p.nr - 1 < 0 || p.wlo >= NZ);
                     if (ok && p.nr > A.nrb) {
                         atomicOr(A.err, kErrLayout);
@@ -183,46 +208,48 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
             }
             if (lane == 0) {
                 s_n[0] = n;
-                mbar_init(&bar[0], 1);
-                mbar_init(&bar[1], 1);
+                for (int i = 0; i < nf; i++) mbar_init(&bar[i], 1);
                 fence_barrier_init();
             }
         }
         __syncthreads();
         const int nlive = s_n[0];
         const uint32_t box_bytes = uint32_t(FBOXW) * uint32_t(A.nrb) * 4u;
-        int issued = 0;  // thread 0 only
+        int issued = 0, islot = 0;  // thread 0 only: planes issued, ring slot of the next
         auto issue = [&](int li) {
             const int y = plist[li];
-            const FwdPlane p = fwd_plane(A, iv0, v1a, v1b, col0, cta_row0, y);
-            const int b = li & 1;
-            mbar_arrive_expect_tx(&bar[b], box_bytes);
+            const FwdPlane p = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y);
+            mbar_arrive_expect_tx(&bar[islot], box_bytes);
             // x rounded down to a multiple of 4 floats: TMA needs 16-byte aligned starts
-            tma_load_3d(Fr + b * A.fstride, &fmap, &bar[b], p.cx & ~3, y, p.wlo);
+            tma_load_3d(Fr + islot * A.fstride, &fmap, &bar[islot], p.cx & ~3, y, p.wlo);
+            islot = (islot + 1 == nf) ? 0 : islot + 1;
         };
         if (tid == 0) {
-            for (; issued < 2 && issued < nlive; issued++) issue(issued);
+            for (; issued < nf && issued < nlive; issued++) issue(issued);
         }
 
         bool dead = false;
-        int li = 0;
+        int li = 0, b = 0;  // plane, its ring slot
+        uint32_t phase = 0;  // parity of the slot's current use
         for (; li < nlive; li++) {
-            const int b = li & 1;
+            const int xb = li & 1;
             const int y = plist[li];
-            const FwdPlane p = fwd_plane(A, iv0, v1a, v1b, col0, cta_row0, y);
-            if (!dead) dead = !mbar_wait(&bar[b], uint32_t((li >> 1) & 1), A.err);
-            // stage A: x interpolation of the staged rows (one column per lane)
+            const FwdPlane p = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y);
+            if (!dead) dead = !mbar_wait(&bar[b], phase, A.err);
+            // stage A: x interpolation of the staged rows, a row per warp,
+            // two adjacent columns per lane
             {
-                const float* F = Fr + b * A.fstride + (p.cx - (p.cx & ~3));
-                float* X = Xs + b * A.xstride;
+                const float* F = Fr + b * A.fstride + (p.cx - (p.cx & ~3)) + 2 * lane;
+                float* X = Xs + xb * A.xstride + 2 * lane;
                 const float w1 = p.wx, w0 = 1.0f - p.wx;
-                for (int e = tid; e < p.nr * FCOLS; e += NT) {
-                    const float* fr = F + (e >> 6) * FBOXW + (e & 63);
-                    X[e] = fmaf(w1, fr[1], w0 * fr[0]);
+                for (int r = warp; r < p.nr; r += NT / 32) {
+                    const float* fr = F + r * FBOXW;
+                    const float a = fr[0], c = fr[1], d = fr[2];
+                    *reinterpret_cast<float2*>(X + r * FCOLS) = make_float2(fmaf(w1, c, w0 * a), fmaf(w1, d, w0 * c));
                 }
             }
             if (__syncthreads_or(dead)) break;
-            // every thread is done with raw buffer b: stage plane li + 2 into it
+            // every thread is done with raw buffer b: stage plane li + nf into it
             if (tid == 0 && issued < nlive) {
                 fence_proxy_async_smem();
                 issue(issued);
@@ -236,7 +263,7 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
                 for (int j = 0; j < FV; j++) {
                     zs[j] = Shift{0, 0.0f};
                     if ((wmask >> j) & 1u) {
-                        zs[j] = A.T.zt[size_t(v1w + j) * NY + y];
+                        zs[j] = s_zt[(jw + j) * NY + y];
                         base = min(base, zs[j].d);
                     }
                 }
@@ -245,7 +272,7 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
                 if (base < p.dzmin) {  // the shifts are monotone in v1; never read before the buffer
                     atomicOr(A.err, kErrLayout);
                 } else if (iz0 + WN - 1 >= 0 && iz0 < NZ) {
-                    const float* Xr = Xs + b * A.xstride + xr0 * FCOLS + 2 * lane;
+                    const float* Xr = Xs + xb * A.xstride + xr0 * FCOLS + 2 * lane;
                     float2 W[WN];
 #pragma unroll
                     for (int i = 0; i < WN; i++) W[i] = *reinterpret_cast<const float2*>(Xr + i * FCOLS);
@@ -263,11 +290,15 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
                     }
                 }
             }
+            if (++b == nf) {
+                b = 0;
+                phase ^= 1u;
+            }
         }
         if (li < nlive) {
             // a wait gave up: drain the copies still in flight, write nothing
             if (tid == 0)
-                for (int q = li; q < issued; q++) mbar_wait(&bar[q & 1], uint32_t((q >> 1) & 1), nullptr);
+                for (int q = li; q < issued; q++) mbar_wait(&bar[q % nf], uint32_t((q / nf) & 1), nullptr);
             return;
         }
     }
@@ -277,8 +308,8 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
     const bool pairs = (G.N_u0 & 1) == 0;  // float2 accesses stay 8-byte aligned
 #pragma unroll
     for (int j = 0; j < FV; j++) {
-        const int v1 = v1w + j;
-        if (v1 > v1b) continue;
+        const int v1 = v1a + jw + j;
+        if (jw + j >= nsl) continue;
         const float S = A.T.S[size_t(v1) * G.N_v0 + iv0];
         const int2 u1r = A.T.ub1[v1];
 #pragma unroll
@@ -313,15 +344,29 @@ constexpr int BPG = 2;              // plane groups
 constexpr int BNP = BPT * BPG;      // planes per CTA
 constexpr int BDW = 2;              // largest shift difference among a thread's planes
 constexpr int BWN = BK + BDW + 1;   // register window rows
-constexpr int BNS = 4;              // copy ring stages
+constexpr int BNSMAX = 6;          // copy ring stages at most
 constexpr int BV1CAP = 96;          // slopes held in the per-CTA tables
+
+// Window offsets of a plane group's 4 planes when all are fully visible and
+// their shifts differ by at most one row (monotone in y, the common case):
+// one straight-line block of FMAs per stage.  Any other group takes the
+// per-plane path (kPatGeneric).
+constexpr int kNumPat = 7;
+constexpr int kPatGeneric = 15;
+__host__ __device__ constexpr int pat_offsets(int pid)
+{
+    // o0 | o1 << 2 | o2 << 4 | o3 << 6
+    return pid == 0 ? 0x00 : pid == 1 ? 0x40 : pid == 2 ? 0x50 : pid == 3 ? 0x54
+         : pid == 4 ? 0x01 : pid == 5 ? 0x05 : 0x15;
+}
 
 struct BwdTmaArgs {
     petl_geom G;
     ViewRange vr;
-    int ncw;      // column warps per plane group (64 columns each)
+    int ncw;      // column warps per plane group (32 columns each)
     int brb;      // staged rows per view (>= BWN + CTA shift spread, bounded on the host)
     int sstride;  // floats per ring stage
+    int ns;       // ring stages
     int accumulate;
     float scale;
     Tables T;
@@ -333,24 +378,40 @@ struct BwdTmaArgs {
 // 0/1 factors: vm (window rows that hold visible bins, the adjoint's bin mask)
 // and om (output rows inside the reference backprojector's voxel test).
 template <int O, bool MASK>
-__device__ __forceinline__ void bwd_taps(float2 (&Z)[BK], const float2 (&W)[BWN], float2 w0, float2 w1, uint32_t vm,
+__device__ __forceinline__ void bwd_taps(float (&Z)[BK], const float (&W)[BWN], float w0, float w1, uint32_t vm,
                                          uint32_t om)
 {
+    if (MASK) {
 #pragma unroll
-    for (int k = 0; k < BK; k++) {
-        if (MASK) {
-            const float a = ((vm >> (O + k)) & (om >> k) & 1u) ? 1.0f : 0.0f;
-            const float b = ((vm >> (O + k + 1)) & (om >> k) & 1u) ? 1.0f : 0.0f;
-            Z[k] = __ffma2_rn(make_float2(w1.x * a, w1.y * a), W[O + k],
-                              __ffma2_rn(make_float2(w0.x * b, w0.y * b), W[O + k + 1], Z[k]));
-        } else {
-            Z[k] = __ffma2_rn(w1, W[O + k], __ffma2_rn(w0, W[O + k + 1], Z[k]));
+        for (int k = 0; k < BK; k++) {
+            const float a = ((vm >> (O + k)) & (om >> k) & 1u) ? w1 : 0.0f;
+            const float b = ((vm >> (O + k + 1)) & (om >> k) & 1u) ? w0 : 0.0f;
+            Z[k] = fmaf(a, W[O + k], fmaf(b, W[O + k + 1], Z[k]));
         }
+    } else {
+        // all tap-0 FMAs, then all tap-1 FMAs: independent chains back to back
+#pragma unroll
+        for (int k = 0; k < BK; k++) Z[k] = fmaf(w0, W[O + k + 1], Z[k]);
+#pragma unroll
+        for (int k = 0; k < BK; k++) Z[k] = fmaf(w1, W[O + k], Z[k]);
     }
 }
 
-template <bool ADJ>
-__global__ void __launch_bounds__(256, 1)
+// z taps of a fully visible plane group with compile-time window offsets
+template <int PID>
+__device__ __forceinline__ void bwd_taps4(float (&Z)[BPT][BK], const float (&W)[BWN], float4 wa, float4 wb)
+{
+    constexpr int o = pat_offsets(PID);
+    bwd_taps<(o >> 0) & 3, false>(Z[0], W, wa.x, wa.y, 0u, 0u);
+    bwd_taps<(o >> 2) & 3, false>(Z[1], W, wa.z, wa.w, 0u, 0u);
+    bwd_taps<(o >> 4) & 3, false>(Z[2], W, wb.x, wb.y, 0u, 0u);
+    bwd_taps<(o >> 6) & 3, false>(Z[3], W, wb.z, wb.w, 0u, 0u);
+}
+
+// PITCH > 0: the planogram row pitch N_u0 as a compile-time constant (shared
+// memory offsets become immediates); 0: read it from the geometry.
+template <bool ADJ, int PITCH>
+__global__ void __launch_bounds__(512, 1)
 k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const BwdTmaArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -360,21 +421,25 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
     const int cw = warp % A.ncw, pg = warp / A.ncw;
     const int p0 = blockIdx.x * BNP;  // first plane of the CTA
     const int r0 = blockIdx.y * BK;   // first z row of the CTA
-    const int u = cw * 64 + 2 * lane; // first of this thread's two columns
-    const int NY = G.numY, NX = G.numX, NZ = G.numZ, NU0 = G.N_u0, NU1 = G.N_u1;
+    const int u = cw * 32 + lane;     // this thread's column (planogram u0 and voxel x)
+    const int NY = G.numY, NX = G.numX, NZ = G.numZ, NU1 = G.N_u1;
+    const int NU0 = PITCH > 0 ? PITCH : G.N_u0;
     const int n_v0 = A.vr.n_v0(G.N_v0);
 
-    float* ring = reinterpret_cast<float*>(smem);                         // [BNS][brb][NU0]
-    float* Zs = ring + BNS * A.sstride;                                   // [BNP][BK][NU0]
-    float4* Wt = reinterpret_cast<float4*>(Zs + BNP * BK * NU0);          // [BV1CAP][BNP]
+    const int ns = A.ns;
+    float* ring = reinterpret_cast<float*>(smem);                         // [ns][brb][NU0]
+    float* Zs = ring + ns * A.sstride;                                    // [BNP][BK][NU0]
+    float2* Wt = reinterpret_cast<float2*>(Zs + BNP * BK * NU0);          // [BV1CAP][BNP]
     float* s_w = reinterpret_cast<float*>(Wt + BV1CAP * BNP);             // [BV1CAP][BNP]
     int* s_v1 = reinterpret_cast<int*>(s_w + BV1CAP * BNP);               // [BV1CAP]
     int* s_grow = s_v1 + BV1CAP;                                          // [BV1CAP]
     uint32_t* s_code = reinterpret_cast<uint32_t*>(s_grow + BV1CAP);      // [BV1CAP]
     uint32_t* s_wb = s_code + BV1CAP;                                     // [BV1CAP]
-    uint64_t* full = reinterpret_cast<uint64_t*>(s_wb + BV1CAP);          // [BNS]
-    uint64_t* empty = full + BNS;                                         // [BNS]
-    int* s_n = reinterpret_cast<int*>(empty + BNS);
+    uint32_t* s_mask = s_wb + BV1CAP;                                     // [BV1CAP][BPG]
+    uint32_t* s_pat = s_mask + BV1CAP * BPG;                              // [BV1CAP]
+    uint64_t* full = reinterpret_cast<uint64_t*>(s_pat + BV1CAP);         // [ns]
+    uint64_t* empty = full + BNSMAX;                                      // [ns]
+    int* s_n = reinterpret_cast<int*>(empty + BNSMAX);
 
     // ---- per-CTA slope tables (warp 0): for every slope whose rows reach the
     // tile, the staged g row, per plane the window offset and mode (0 none,
@@ -384,9 +449,12 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
         for (int vb = A.vr.iv1_begin; vb < A.vr.iv1_end; vb += 32) {
             const int v1 = vb + lane;
             bool ok = false;
-            uint32_t code = 0, wbs = 0;
+            uint32_t code = 0, wbs = 0, pats = 0;
+            uint32_t msk[BPG];
             int grow = 0;
             float wz[BNP];
+#pragma unroll
+            for (int q = 0; q < BPG; q++) msk[q] = 0xffffffffu;
             if (v1 < A.vr.iv1_end) {
                 int dz[BNP];
                 int dmin = 1 << 30, dmax = -(1 << 30);
@@ -437,6 +505,43 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
                         ok = true;
                     }
                     wbs |= uint32_t(wb) << (8 * q);
+                    // straight-line pattern of the group, if it has one
+                    int pid = kPatGeneric;
+                    {
+                        bool allfull = true;
+                        int offs = 0;
+#pragma unroll
+                        for (int t = 0; t < BPT; t++) {
+                            const int p = q * BPT + t;
+                            const int o = dmax - dz[p] - wb;
+                            allfull = allfull && mode[p] == 1 && o <= 1;
+                            offs |= (o & 3) << (2 * t);
+                        }
+                        if (allfull)
+                            for (int c = 0; c < kNumPat; c++)
+                                if (pat_offsets(c) == offs) pid = c;
+                    }
+                    pats |= uint32_t(pid) << (4 * q);
+                    // row masks for planes at the edge of the visible range:
+                    // adjoint, window rows holding visible bins of the group;
+                    // reference, per plane the output rows passing the voxel test
+                    if (ADJ) {
+                        uint32_t vm = 0;
+                        for (int i = 0; i < BWN; i++)
+                            if (grow + wb + i >= ub1.x && grow + wb + i <= ub1.y) vm |= 1u << i;
+                        msk[q] = vm;
+                    } else {
+                        uint32_t om = 0;
+#pragma unroll
+                        for (int t = 0; t < BPT; t++) {
+                            const int p = q * BPT + t;
+                            if (mode[p] != 2) continue;
+                            const int2 zv = A.T.zvis[size_t(v1) * NY + p0 + p];
+                            for (int k = 0; k < BK; k++)
+                                if (r0 + k >= zv.x && r0 + k <= zv.y) om |= 1u << (8 * t + k);
+                        }
+                        msk[q] = om;
+                    }
                 }
                 if (ok && bad) {
                     atomicOr(A.err, kErrLayout);
@@ -451,6 +556,9 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
                     s_grow[idx] = grow;
                     s_code[idx] = code;
                     s_wb[idx] = wbs;
+                    s_pat[idx] = pats;
+#pragma unroll
+                    for (int q = 0; q < BPG; q++) s_mask[idx * BPG + q] = msk[q];
 #pragma unroll
                     for (int p = 0; p < BNP; p++) s_w[idx * BNP + p] = wz[p];
                 }
@@ -463,7 +571,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
                 n = BV1CAP;
             }
             s_n[0] = n;
-            for (int s = 0; s < BNS; s++) {
+            for (int s = 0; s < ns; s++) {
                 mbar_init(&full[s], 1);
                 mbar_init(&empty[s], nwarps);
             }
@@ -474,73 +582,114 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
     const int nlive = s_n[0];
     const long long total = (long long)n_v0 * nlive;
 
-    // weights of view v0: (S w0, S w0, S w1, S w1) per live slope and plane
+    // weights of view v0: (S w0, S w1) per live slope and plane
     auto weights = [&](int v0) {
         for (int e = tid; e < nlive * BNP; e += blockDim.x) {
             const int li = e / BNP;
             const float S = A.T.S[size_t(s_v1[li]) * G.N_v0 + v0];
             const float w = s_w[e];
             const float w1 = S * w, w0 = S * (1.0f - w);
-            Wt[e] = make_float4(w0, w0, w1, w1);
+            Wt[e] = make_float2(w0, w1);
         }
     };
     const uint32_t box_bytes = uint32_t(NU0) * uint32_t(A.brb) * 4u;
-    long long issued = 0;  // thread 0 only
+    // producer state (thread 0): stages issued, and the next stage's ring
+    // slot, slope index, view and ring round
+    long long issued = 0;
+    int p_slot = 0, p_li = 0, p_v0 = A.vr.iv0_first, p_round = 0;
     bool dead = false;
-    // start the copy of stage j once every warp has released its ring slot
-    auto issue = [&](long long j) {
-        const int s = int(j % BNS);
-        const int li = int(j % nlive);
-        const int v0 = A.vr.iv0_first + int(j / nlive) * A.vr.iv0_step;
-        if (j >= BNS && !mbar_wait(&empty[s], uint32_t(((j / BNS) - 1) & 1), A.err)) return false;
+    // Start the copy of the next stage into its ring slot once every warp has
+    // released the slot (the consumption of the stage ns earlier).  Without
+    // `block` it only tests once, so thread 0 does not stall its warp on slow
+    // warps while the ring still holds stages ahead.
+    auto issue = [&](bool block) {
+        if (p_round > 0) {
+            const uint32_t par = uint32_t((p_round - 1) & 1);
+            if (block) {
+                if (!mbar_wait(&empty[p_slot], par, A.err)) return -1;
+            } else if (!mbar_test_wait(&empty[p_slot], par)) {
+                return 0;
+            }
+        }
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&full[s], box_bytes);
-        tma_load_4d(ring + s * A.sstride, &gmap, &full[s], 0, s_grow[li], v0, s_v1[li]);
-        return true;
+        mbar_arrive_expect_tx(&full[p_slot], box_bytes);
+        tma_load_4d(ring + p_slot * A.sstride, &gmap, &full[p_slot], 0, s_grow[p_li], p_v0, s_v1[p_li]);
+        if (++p_slot == ns) {
+            p_slot = 0;
+            p_round++;
+        }
+        if (++p_li == nlive) {
+            p_li = 0;
+            p_v0 += A.vr.iv0_step;
+        }
+        issued++;
+        return 1;
     };
     if (tid == 0)
-        for (; issued < BNS - 1 && issued < total; issued++) issue(issued);
+        while (issued < ns && issued < total) issue(true);
     if (n_v0 > 0) weights(A.vr.iv0_first);
     __syncthreads();
 
-    float2 Fv[BPT][BK];  // voxel accumulators (unscaled)
-    float2 Z[BPT][BK];   // z-interpolated sums of the current view
+    float Fv[BPT][BK];  // voxel accumulators (unscaled)
+    float Z[BPT][BK];   // z-interpolated sums of the current view
 #pragma unroll
     for (int q = 0; q < BPT; q++)
 #pragma unroll
         for (int k = 0; k < BK; k++) {
-            Fv[q][k] = make_float2(0.0f, 0.0f);
-            Z[q][k] = make_float2(0.0f, 0.0f);
+            Fv[q][k] = 0.0f;
+            Z[q][k] = 0.0f;
         }
 
     bool aborted = false;
     const bool ucol = u < NU0;
     long long it = 0;
+    int c_slot = 0;         // ring slot of stage it
+    uint32_t c_phase = 0;   // parity of that slot's current use
     for (int iv = 0; iv < n_v0 && !aborted; iv++) {
         const int v0 = A.vr.iv0_first + iv * A.vr.iv0_step;
         for (int li = 0; li < nlive; li++, it++) {
-            if (tid == 0 && issued < total && !dead) {
-                if (issue(issued))
-                    issued++;
-                else
-                    dead = true;
+            if (tid == 0 && !dead) {
+                // keep the ring full; block only when this stage itself is not issued yet
+                while (issued < total && issued < it + ns) {
+                    const int r = issue(issued <= it);
+                    if (r < 0) dead = true;
+                    if (r <= 0) break;
+                }
             }
-            const int s = int(it % BNS);
-            if (!dead) dead = !mbar_wait(&full[s], uint32_t((it / BNS) & 1), A.err);
+            const int s = c_slot;
+            if (!dead) dead = !mbar_wait(&full[s], c_phase, A.err);
             const uint32_t code = s_code[li] >> (16 * pg);  // this group's 4 planes
-            if (ucol && (code & 0x3333u)) {
+            const uint32_t pat = (s_pat[li] >> (4 * pg)) & 15u;
+            if (ucol && pat != uint32_t(kPatGeneric)) {
                 const int wb = (s_wb[li] >> (8 * pg)) & 0xff;
                 const float* Gs = ring + s * A.sstride + wb * NU0 + u;
-                float2 W[BWN];
+                float W[BWN];
 #pragma unroll
-                for (int i = 0; i < BWN; i++) W[i] = *reinterpret_cast<const float2*>(Gs + i * NU0);
-                const float4* Wl = Wt + li * BNP + pg * BPT;
+                for (int i = 0; i < BWN; i++) W[i] = Gs[i * NU0];
+                const float4* W4 = reinterpret_cast<const float4*>(Wt + li * BNP + pg * BPT);
+                const float4 wa = W4[0], wb4 = W4[1];
+                switch (pat) {
+                    case 0: bwd_taps4<0>(Z, W, wa, wb4); break;
+                    case 1: bwd_taps4<1>(Z, W, wa, wb4); break;
+                    case 2: bwd_taps4<2>(Z, W, wa, wb4); break;
+                    case 3: bwd_taps4<3>(Z, W, wa, wb4); break;
+                    case 4: bwd_taps4<4>(Z, W, wa, wb4); break;
+                    case 5: bwd_taps4<5>(Z, W, wa, wb4); break;
+                    default: bwd_taps4<6>(Z, W, wa, wb4); break;
+                }
+            } else if (ucol && (code & 0x3333u)) {
+                const int wb = (s_wb[li] >> (8 * pg)) & 0xff;
+                const float* Gs = ring + s * A.sstride + wb * NU0 + u;
+                float W[BWN];
+#pragma unroll
+                for (int i = 0; i < BWN; i++) W[i] = Gs[i * NU0];
+                const float2* Wl = Wt + li * BNP + pg * BPT;
 #pragma unroll
                 for (int q = 0; q < BPT; q++) {
                     const uint32_t c = (code >> (4 * q)) & 15u;
                     if (!(c & 3u)) continue;
-                    const float4 w = Wl[q];
-                    const float2 w0 = make_float2(w.x, w.y), w1 = make_float2(w.z, w.w);
+                    const float2 w = Wl[q];
+                    const float w0 = w.x, w1 = w.y;
                     const int o = int(c >> 2);
                     if ((c & 3u) == 1u) {
                         switch (o) {
@@ -550,22 +699,9 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
                         }
                     } else {
                         // rows at the edge of the visible range: per-row masks
-                        uint32_t vm = 0xffffffffu, om = 0xffffffffu;
-                        const int v1 = s_v1[li];
-                        if (ADJ) {
-                            const int2 ub1 = A.T.ub1[v1];
-                            const int gr0 = s_grow[li] + wb;  // g row of window row 0
-                            vm = 0;
-#pragma unroll
-                            for (int i = 0; i < BWN; i++)
-                                if (gr0 + i >= ub1.x && gr0 + i <= ub1.y) vm |= 1u << i;
-                        } else {
-                            const int2 zv = A.T.zvis[size_t(v1) * NY + p0 + pg * BPT + q];
-                            om = 0;
-#pragma unroll
-                            for (int k = 0; k < BK; k++)
-                                if (r0 + k >= zv.x && r0 + k <= zv.y) om |= 1u << k;
-                        }
+                        const uint32_t m = s_mask[li * BPG + pg];
+                        const uint32_t vm = ADJ ? m : 0xffffffffu;
+                        const uint32_t om = ADJ ? 0xffffffffu : (m >> (8 * q)) & 0xffu;
                         switch (o) {
                             case 0: bwd_taps<0, true>(Z[q], W, w0, w1, vm, om); break;
                             case 1: bwd_taps<1, true>(Z[q], W, w0, w1, vm, om); break;
@@ -576,6 +712,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
+            if (++c_slot == ns) {
+                c_slot = 0;
+                c_phase ^= 1u;
+            }
         }
         // ---- x shift of view v0 into the voxel accumulators
         {
@@ -586,14 +726,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
 #pragma unroll
                 for (int k = 0; k < BK; k++) {
                     if (ucol) {
-                        float2 z = Z[q][k];
-                        if (ADJ) {
-                            if (u < u0r.x || u > u0r.y) z.x = 0.0f;
-                            if (u + 1 < u0r.x || u + 1 > u0r.y) z.y = 0.0f;
-                        }
-                        *reinterpret_cast<float2*>(Zs + ((pg * BPT + q) * BK + k) * NU0 + u) = z;
+                        const bool vis = !ADJ || (u >= u0r.x && u <= u0r.y);
+                        Zs[((pg * BPT + q) * BK + k) * NU0 + u] = vis ? Z[q][k] : 0.0f;
                     }
-                    Z[q][k] = make_float2(0.0f, 0.0f);
+                    Z[q][k] = 0.0f;
                 }
         }
         if (__syncthreads_or(dead)) {
@@ -612,9 +748,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
                 const float* zr = Zs + ((pg * BPT + q) * BK + k) * NU0;
                 const float zm = (j0 - 1 >= 0 && j0 - 1 < NU0) ? zr[j0 - 1] : 0.0f;
                 const float z0 = (j0 >= 0 && j0 < NU0) ? zr[j0] : 0.0f;
-                const float zp = (j0 + 1 >= 0 && j0 + 1 < NU0) ? zr[j0 + 1] : 0.0f;
-                Fv[q][k].x += fmaf(wx1, zm, wx0 * z0);
-                Fv[q][k].y += fmaf(wx1, z0, wx0 * zp);
+                Fv[q][k] += fmaf(wx1, zm, wx0 * z0);
             }
         }
         if (iv + 1 < n_v0) weights(v0 + A.vr.iv0_step);
@@ -623,8 +757,8 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
     if (aborted) {
         // a wait gave up: drain the copies still in flight, write nothing
         if (tid == 0)
-            for (long long j = std::max(0LL, issued - BNS); j < issued; j++)
-                mbar_wait(&full[j % BNS], uint32_t((j / BNS) & 1), nullptr);
+            for (long long j = std::max(0LL, issued - ns); j < issued; j++)
+                mbar_wait(&full[j % ns], uint32_t((j / ns) & 1), nullptr);
         return;
     }
 
@@ -638,8 +772,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
             const int z = r0 + k;
             if (z >= NZ) break;
             float* fr = f + (size_t(z) * NY + y) * NX;
-            if (u < NX) fr[u] = A.accumulate ? fr[u] + A.scale * Fv[q][k].x : A.scale * Fv[q][k].x;
-            if (u + 1 < NX) fr[u + 1] = A.accumulate ? fr[u + 1] + A.scale * Fv[q][k].y : A.scale * Fv[q][k].y;
+            if (u < NX) fr[u] = A.accumulate ? fr[u] + A.scale * Fv[q][k] : A.scale * Fv[q][k];
         }
     }
 }
@@ -654,7 +787,7 @@ double plane_ymax(const petl_geom& G)
 // at most floor(n * step) + 1 (with a relative margin for the float inputs).
 int shift_spread(int n, double step) { return int(std::floor(double(n) * step * (1.0 + 1e-6))) + 1; }
 
-constexpr int kFwdK = 16;
+constexpr int kFwdK = 8;
 
 }  // namespace
 
@@ -686,8 +819,14 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
     A.xstride = (nrb + FDMAX) * FCOLS;
     A.T = T;
     A.err = err;
-    const size_t smem = size_t(2) * A.fstride * 4 + size_t(2) * A.xstride * 4 + 2 * 8 + 2 * 4 + size_t(G.numY) * 2;
-    if (smem > 227 * 1024) return kNotApplicable;
+    // up to 4 planes in flight, fewer when the staged rows are many
+    size_t smem = 0;
+    for (A.nf = 4; A.nf >= 2; A.nf--) {
+        smem = size_t(A.nf) * A.fstride * 4 + size_t(2) * A.xstride * 4 + size_t(1 + FSL) * G.numY * sizeof(Shift) +
+               size_t(A.nf) * 8 + 2 * 4 + size_t(G.numY) * 2;
+        if (smem <= 227 * 1024) break;
+    }
+    if (A.nf < 2) return kNotApplicable;
     auto kern = k_fwd_tma<kFwdK>;
     PETL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid(unsigned(n_v0), ceil_div(nv1, FSL), unsigned(A.n_colblk) * ceil_div(G.N_u1, FROWS));
@@ -720,25 +859,26 @@ int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int 
     BwdTmaArgs A{};
     A.G = G;
     A.vr = vr;
-    A.ncw = int(ceil_div(std::max(NU0, G.numX), 64));
+    A.ncw = int(ceil_div(std::max(NU0, G.numX), 32));
     A.brb = brb;
     A.sstride = ((brb * NU0 * 4 + 127) & ~127) / 4;
     A.accumulate = accumulate;
     A.scale = scale;
     A.T = T;
     A.err = err;
-    const size_t smem = size_t(BNS) * A.sstride * 4 + size_t(BNP) * BK * NU0 * 4 + size_t(BV1CAP) * BNP * 16 +
-                        size_t(BV1CAP) * BNP * 4 + size_t(BV1CAP) * 4 * 4 + 2 * BNS * 8 + 16;
-    if (smem > 227 * 1024) return kNotApplicable;
+    // as many ring stages as fit (copies from DRAM need several in flight)
+    const size_t fixed = size_t(BNP) * BK * NU0 * 4 + size_t(BV1CAP) * BNP * 8 + size_t(BV1CAP) * BNP * 4 +
+                         size_t(BV1CAP) * 4 * 4 + size_t(BV1CAP) * BPG * 4 + size_t(BV1CAP) * 4 + 2 * BNSMAX * 8 +
+                         16;
+    A.ns = int(std::min<size_t>(BNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / (size_t(A.sstride) * 4)));
+    if (A.ns < 2) return kNotApplicable;
+    const size_t smem = size_t(A.ns) * A.sstride * 4 + fixed;
     const int threads = 32 * A.ncw * BPG;
     dim3 grid(ceil_div(G.numY, BNP), ceil_div(G.numZ, BK));
-    if (mode == PETL_BP_ADJOINT) {
-        PETL_CUDA(cudaFuncSetAttribute(k_bwd_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        k_bwd_tma<true><<<grid, threads, smem, st>>>(map, f, A);
-    } else {
-        PETL_CUDA(cudaFuncSetAttribute(k_bwd_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        k_bwd_tma<false><<<grid, threads, smem, st>>>(map, f, A);
-    }
+    auto kern = mode == PETL_BP_ADJOINT ? (NU0 == 256 ? k_bwd_tma<true, 256> : k_bwd_tma<true, 0>)
+                                        : (NU0 == 256 ? k_bwd_tma<false, 256> : k_bwd_tma<false, 0>);
+    PETL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<grid, threads, smem, st>>>(map, f, A);
     PETL_LAUNCH_CHECK("backproject_tma");
     return 0;
 }
