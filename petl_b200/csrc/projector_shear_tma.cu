@@ -151,8 +151,8 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
     const int nf = A.nf;
 
     float* Fr = reinterpret_cast<float*>(smem);                       // [nf][nrb][68] raw rows (TMA)
-    float* Xs = Fr + nf * A.fstride;                                  // [2][nrb + 3][64] x-interpolated rows
-    Shift* s_xt = reinterpret_cast<Shift*>(Xs + 2 * A.xstride);       // [NY] x shifts of view iv0
+    float* Xs = Fr + nf * A.fstride;                                  // [4][nrb + 3][64] x-interpolated rows
+    Shift* s_xt = reinterpret_cast<Shift*>(Xs + 4 * A.xstride);       // [NY] x shifts of view iv0
     Shift* s_zt = s_xt + NY;                                          // [nsl][NY] z shifts of the slopes
     uint64_t* bar = reinterpret_cast<uint64_t*>(s_zt + FSL * NY);     // [nf]
     int* s_n = reinterpret_cast<int*>(bar + nf);
@@ -228,69 +228,90 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
             for (; issued < nf && issued < nlive; issued++) issue(issued);
         }
 
-        bool dead = false;
-        int li = 0, b = 0;  // plane, its ring slot
-        uint32_t phase = 0;  // parity of the slot's current use
-        for (; li < nlive; li++) {
-            const int xb = li & 1;
-            const int y = plist[li];
-            const FwdPlane p = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y);
-            if (!dead) dead = !mbar_wait(&bar[b], phase, A.err);
-            // stage A: x interpolation of the staged rows, a row per warp,
-            // two adjacent columns per lane
-            {
-                const float* F = Fr + b * A.fstride + (p.cx - (p.cx & ~3)) + 2 * lane;
-                float* X = Xs + xb * A.xstride + 2 * lane;
-                const float w1 = p.wx, w0 = 1.0f - p.wx;
-                for (int r = warp; r < p.nr; r += NT / 32) {
-                    const float* fr = F + r * FBOXW;
-                    const float a = fr[0], c = fr[1], d = fr[2];
-                    *reinterpret_cast<float2*>(X + r * FCOLS) = make_float2(fmaf(w1, c, w0 * a), fmaf(w1, d, w0 * c));
+        // stage A: x interpolation of plane p's staged rows (raw slot rb) into
+        // interpolated buffer xb, a row per warp, two adjacent columns per lane
+        auto stage_a = [&](int rb, int xb, const FwdPlane& p) {
+            const float* F = Fr + rb * A.fstride + (p.cx - (p.cx & ~3)) + 2 * lane;
+            float* X = Xs + xb * A.xstride + 2 * lane;
+            const float w1 = p.wx, w0 = 1.0f - p.wx;
+            for (int r = warp; r < p.nr; r += NT / 32) {
+                const float* fr = F + r * FBOXW;
+                const float a = fr[0], c = fr[1], d = fr[2];
+                *reinterpret_cast<float2*>(X + r * FCOLS) = make_float2(fmaf(w1, c, w0 * a), fmaf(w1, d, w0 * c));
+            }
+        };
+        // stage B: z interpolation of this warp's slopes on plane y from one window
+        auto stage_b = [&](int xb, const FwdPlane& p, int y) {
+            if (!wmask) return;  // warp-uniform
+            Shift zs[FV];
+            int base = 1 << 30;
+#pragma unroll
+            for (int j = 0; j < FV; j++) {
+                zs[j] = Shift{0, 0.0f};
+                if ((wmask >> j) & 1u) {
+                    zs[j] = s_zt[(jw + j) * NY + y];
+                    base = min(base, zs[j].d);
                 }
+            }
+            const int xr0 = row0 - cta_row0 + base - p.dzmin;  // staged row of window row 0
+            const int iz0 = p.wlo + xr0;                        // its volume row
+            if (base < p.dzmin) {  // the shifts are monotone in v1; never read before the buffer
+                atomicOr(A.err, kErrLayout);
+                return;
+            }
+            if (iz0 + WN - 1 < 0 || iz0 >= NZ) return;  // window outside the volume: zeros
+            const float* Xr = Xs + xb * A.xstride + xr0 * FCOLS + 2 * lane;
+            float2 W[WN];
+#pragma unroll
+            for (int i = 0; i < WN; i++) W[i] = *reinterpret_cast<const float2*>(Xr + i * FCOLS);
+#pragma unroll
+            for (int j = 0; j < FV; j++) {
+                if (!((wmask >> j) & 1u)) continue;
+                const float2 w1 = dup(zs[j].w), w0 = dup(1.0f - zs[j].w);
+                switch (zs[j].d - base) {
+                    case 0: fwd_taps<0, K>(acc[j], W, w0, w1); break;
+                    case 1: fwd_taps<1, K>(acc[j], W, w0, w1); break;
+                    case 2: fwd_taps<2, K>(acc[j], W, w0, w1); break;
+                    case 3: fwd_taps<3, K>(acc[j], W, w0, w1); break;
+                    default: atomicOr(A.err, kErrLayout);
+                }
+            }
+        };
+
+        // two planes per CTA barrier: stage A of both, one barrier, stage B of
+        // both; pairs alternate between two pairs of interpolated buffers
+        bool dead = false;
+        int li = 0, b = 0;   // first plane of the pair, its ring slot
+        uint32_t phase = 0;  // parity of that slot's current use
+        for (; li < nlive; li += 2) {
+            const bool two = li + 1 < nlive;
+            const int xq = 2 * ((li >> 1) & 1);
+            int b1 = b + 1;
+            uint32_t phase1 = phase;
+            if (b1 == nf) {
+                b1 = 0;
+                phase1 ^= 1u;
+            }
+            const int y0 = plist[li], y1 = two ? plist[li + 1] : y0;
+            const FwdPlane p0 = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y0);
+            const FwdPlane p1 = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y1);
+            if (!dead) dead = !mbar_wait(&bar[b], phase, A.err);
+            stage_a(b, xq, p0);
+            if (two) {
+                if (!dead) dead = !mbar_wait(&bar[b1], phase1, A.err);
+                stage_a(b1, xq + 1, p1);
             }
             if (__syncthreads_or(dead)) break;
-            // every thread is done with raw buffer b: stage plane li + nf into it
-            if (tid == 0 && issued < nlive) {
+            // every thread is done with the pair's raw slots: stage the planes nf later
+            if (tid == 0) {
                 fence_proxy_async_smem();
-                issue(issued);
-                issued++;
+                for (int n = 0; n < (two ? 2 : 1) && issued < nlive; n++, issued++) issue(issued);
             }
-            // stage B: z interpolation of this warp's slopes from one window
-            if (wmask) {  // warp-uniform
-                Shift zs[FV];
-                int base = 1 << 30;
-#pragma unroll
-                for (int j = 0; j < FV; j++) {
-                    zs[j] = Shift{0, 0.0f};
-                    if ((wmask >> j) & 1u) {
-                        zs[j] = s_zt[(jw + j) * NY + y];
-                        base = min(base, zs[j].d);
-                    }
-                }
-                const int xr0 = row0 - cta_row0 + base - p.dzmin;  // staged row of window row 0
-                const int iz0 = p.wlo + xr0;                        // its volume row
-                if (base < p.dzmin) {  // the shifts are monotone in v1; never read before the buffer
-                    atomicOr(A.err, kErrLayout);
-                } else if (iz0 + WN - 1 >= 0 && iz0 < NZ) {
-                    const float* Xr = Xs + xb * A.xstride + xr0 * FCOLS + 2 * lane;
-                    float2 W[WN];
-#pragma unroll
-                    for (int i = 0; i < WN; i++) W[i] = *reinterpret_cast<const float2*>(Xr + i * FCOLS);
-#pragma unroll
-                    for (int j = 0; j < FV; j++) {
-                        if (!((wmask >> j) & 1u)) continue;
-                        const float2 w1 = dup(zs[j].w), w0 = dup(1.0f - zs[j].w);
-                        switch (zs[j].d - base) {
-                            case 0: fwd_taps<0, K>(acc[j], W, w0, w1); break;
-                            case 1: fwd_taps<1, K>(acc[j], W, w0, w1); break;
-                            case 2: fwd_taps<2, K>(acc[j], W, w0, w1); break;
-                            case 3: fwd_taps<3, K>(acc[j], W, w0, w1); break;
-                            default: atomicOr(A.err, kErrLayout);
-                        }
-                    }
-                }
-            }
-            if (++b == nf) {
+            stage_b(xq, p0, y0);
+            if (two) stage_b(xq + 1, p1, y1);
+            b = b1;
+            phase = phase1;
+            if (two && ++b == nf) {
                 b = 0;
                 phase ^= 1u;
             }
@@ -819,14 +840,19 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
     A.xstride = (nrb + FDMAX) * FCOLS;
     A.T = T;
     A.err = err;
-    // up to 4 planes in flight, fewer when the staged rows are many
-    size_t smem = 0;
-    for (A.nf = 4; A.nf >= 2; A.nf--) {
-        smem = size_t(A.nf) * A.fstride * 4 + size_t(2) * A.xstride * 4 + size_t(1 + FSL) * G.numY * sizeof(Shift) +
-               size_t(A.nf) * 8 + 2 * 4 + size_t(G.numY) * 2;
-        if (smem <= 227 * 1024) break;
-    }
-    if (A.nf < 2) return kNotApplicable;
+    // up to 4 planes in flight; prefer a footprint that leaves room for two
+    // CTAs per SM, else the largest ring that fits one
+    auto bytes = [&](int nf) {
+        return size_t(nf) * A.fstride * 4 + size_t(4) * A.xstride * 4 + size_t(1 + FSL) * G.numY * sizeof(Shift) +
+               size_t(nf) * 8 + 2 * 4 + size_t(G.numY) * 2;
+    };
+    A.nf = 0;
+    for (int nf = 4; nf >= 2 && !A.nf; nf--)
+        if (bytes(nf) <= 113 * 1024) A.nf = nf;
+    for (int nf = 4; nf >= 2 && !A.nf; nf--)
+        if (bytes(nf) <= 227 * 1024) A.nf = nf;
+    if (!A.nf) return kNotApplicable;
+    const size_t smem = bytes(A.nf);
     auto kern = k_fwd_tma<kFwdK>;
     PETL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid(unsigned(n_v0), ceil_div(nv1, FSL), unsigned(A.n_colblk) * ceil_div(G.N_u1, FROWS));
