@@ -171,6 +171,11 @@ int petl_reciprocal_dev(float* x, long long n, float divide_by_zero_value, void*
 int petl_dot_dev(const float* x, const float* y, const float* w, long long n, double* out, void* stream);
 /* *out (device double) = sum over Pf>0 of g*log(Pf) - Pf (Poisson log-likelihood) */
 int petl_loglik_dev(const float* g, const float* Pf, long long n, double* out, void* stream);
+/* Pf = (Pf > 0) ? 1 - g/Pf : 0, in place: the gradient of the Poisson
+ * negative log-likelihood sum(Pf - g log Pf) (over Pf > 0) with respect to
+ * Pf.  No reference counterpart (the reference has no gradient-based
+ * likelihood path); used by the autograd wrappers. */
+int petl_poisson_grad_dev(float* Pf, const float* g, long long n, void* stream);
 /* x = a*x + b*y */
 int petl_axpby_dev(float* x, const float* y, float a, float b, long long n, void* stream);
 /* MLEM image update f *= d / sens with the DIV rule (d/0 -> 0) */

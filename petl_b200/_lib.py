@@ -99,6 +99,7 @@ _DEV_API = [
     ("petl_dot_dev", c_i, [c_vp, c_vp, c_vp, c_ll, c_vp, c_vp]),
     ("petl_loglik_dev", c_i, [c_vp, c_vp, c_ll, c_vp, c_vp]),
     ("petl_axpby_dev", c_i, [c_vp, c_vp, c_f, c_f, c_ll, c_vp]),
+    ("petl_poisson_grad_dev", c_i, [c_vp, c_vp, c_ll, c_vp]),
     ("petl_mlem_update_dev", c_i, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     ("petl_osl_update_dev", c_i, [c_vp, c_vp, c_vp, c_vp, c_ll, c_vp]),
 ]

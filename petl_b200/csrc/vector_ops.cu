@@ -41,6 +41,11 @@ struct OpMul { __device__ float operator()(float a, float b) const { return a * 
 struct OpDiv { __device__ float operator()(float a, float b) const { return b == 0.0f ? 0.0f : a / b; } };
 // out = num / denom with denom stored in the first operand
 struct OpRDiv { __device__ float operator()(float den, float num) const { return den == 0.0f ? 0.0f : num / den; } };
+// d/d(Pf) of the Poisson negative log-likelihood sum(Pf - g log Pf) over
+// Pf > 0 (the bins the log-likelihood sums), Pf stored in the first operand
+struct OpPoissonGrad {
+    __device__ float operator()(float pf, float g) const { return pf > 0.0f ? 1.0f - g / pf : 0.0f; }
+};
 
 __global__ void k_reciprocal(float* __restrict__ x, long long n, float v)
 {
@@ -143,6 +148,11 @@ int petl_divide_dev(float* x, const float* y, long long n, void* stream)
 int petl_rdivide_dev(const float* num, float* denom, long long n, void* stream)
 {
     return map2<OpRDiv>(denom, num, n, stream, "rdivide");
+}
+
+int petl_poisson_grad_dev(float* Pf, const float* g, long long n, void* stream)
+{
+    return map2<OpPoissonGrad>(Pf, g, n, stream, "poisson_grad");
 }
 
 int petl_reciprocal_dev(float* x, long long n, float v, void* stream)

@@ -236,6 +236,13 @@ def loglik(g, Pf):
     return out
 
 
+def poisson_grad_(Pf, g):
+    """Pf = 1 - g/Pf where Pf > 0, else 0, in place: d/d(Pf) of the Poisson
+    negative log-likelihood sum(Pf - g log Pf)."""
+    check(lib().petl_poisson_grad_dev(_dev(Pf, "Pf"), _dev(g, "g"), _n(Pf), _stream()), "poisson_grad")
+    return Pf
+
+
 def mlem_update_(f, d, sens):
     check(lib().petl_mlem_update_dev(_dev(f, "f"), _dev(d, "d"), _dev(sens, "sens"), _n(f), _stream()), "mlem_update")
     return f
@@ -249,4 +256,5 @@ def osl_update_(f, d, sens, Df):
 
 __all__ = ["Geometry", "project", "project_ratio", "backproject", "nnz", "pfdr", "ramp_", "fbp", "rd_gradient", "rd_cost",
            "tv_gradient", "tv_cost", "tv_quadform", "gaussian_filter_", "rdivide_", "divide_", "multiply_",
-           "reciprocal_", "axpby_", "dot", "loglik", "mlem_update_", "osl_update_", "REFERENCE", "ADJOINT"]
+           "reciprocal_", "axpby_", "dot", "loglik", "poisson_grad_", "mlem_update_", "osl_update_", "REFERENCE",
+           "ADJOINT"]
