@@ -138,6 +138,25 @@ int petl_ramp_dev(const petl_geom* G, float* g_reb, int apply_weight, void* stre
  * already rebinned planogram when G->N_v1 == 1. */
 int petl_fbp_dev(const petl_geom* G, const float* g, float* f, int accumulate, void* stream);
 
+/* --- BF16 storage ---------------------------------------------------------
+ * No reference counterpart (the reference stores float32 only).  Volumes and
+ * planograms in bfloat16 (void* = __nv_bfloat16*), footprints accumulated in
+ * FP32, results rounded to bfloat16 once.  These run the TMA-staged
+ * shear-warp kernels only: axis-aligned planograms with bin pitch equal to
+ * the voxel pitch, 16-byte aligned buffers, volume and planogram rows that
+ * are multiples of 8 elements, and N_u0, numX <= 256 for the
+ * backprojection.  Anything else is refused with an error. */
+int petl_project_bf16_dev(const petl_geom* G, const void* f, void* g, int iv1_begin, int iv1_end, int iv0_first,
+                          int iv0_step, void* stream);
+/* ratio = (P f == 0) ? 0 : meas / (P f), all three in bfloat16 */
+int petl_project_ratio_bf16_dev(const petl_geom* G, const void* f, const void* meas, void* ratio, int iv1_begin,
+                                int iv1_end, int iv0_first, int iv0_step, void* stream);
+/* f (float32) = accumulate ? f + scale*P^T g : scale*P^T g with g in bfloat16 */
+int petl_backproject_bf16_dev(const petl_geom* G, const void* g, float* f, int mode, int accumulate, float scale,
+                              int iv1_begin, int iv1_end, int iv0_first, int iv0_step, void* stream);
+/* f (bfloat16) *= d / sens with the DIV rule (d/0 -> 0) */
+int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long long n, void* stream);
+
 /* --- regularizers, volume [N1][N2][N3] ------------------------------------ */
 /* aTV_RelativeDifferencesLoss_gradient (src/relative_differences.cu:481-532) */
 int petl_rd_gradient_dev(const float* f, float* Df, int N1, int N2, int N3, float delta, float beta, void* stream);

@@ -30,6 +30,7 @@
 // Every wait on a copy is bounded; a wait that gives up sets the device error
 // word, and the CTA drains its copies in flight and stops without writing.
 #include <cuda.h>
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -49,6 +50,33 @@ namespace {
 enum : int { kErrLayout = 2 };  // a host-side bound on the shift spread did not hold
 
 __device__ __forceinline__ float2 dup(float a) { return make_float2(a, a); }
+
+// Storage element types: float32, or bfloat16 read into FP32 arithmetic.
+// kAlign is the TMA x-coordinate granule (16 bytes) in elements.
+template <class T>
+struct Store;
+template <>
+struct Store<float> {
+    static constexpr int kAlign = 4;
+    static __device__ __forceinline__ float ld(float x) { return x; }
+    static __device__ __forceinline__ float st(float x) { return x; }
+    static __device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+    static __device__ __forceinline__ void st2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+};
+template <>
+struct Store<__nv_bfloat16> {
+    static constexpr int kAlign = 8;
+    static __device__ __forceinline__ float ld(__nv_bfloat16 x) { return __bfloat162float(x); }
+    static __device__ __forceinline__ __nv_bfloat16 st(float x) { return __float2bfloat16_rn(x); }
+    static __device__ __forceinline__ float2 ld2(const __nv_bfloat16* p)
+    {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+    }
+    static __device__ __forceinline__ void st2(__nv_bfloat16* p, float2 v)
+    {
+        *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
+    }
+};
 
 // Two scalar FMAs on a column pair.  Scalar FFMA issues at the full FP32
 // rate with two warps per scheduler; the packed f32x2 form needs about four
@@ -76,7 +104,9 @@ constexpr int FGV = 4;             // warps along v1
 constexpr int FSL = FV * FGV;      // slopes per CTA
 constexpr int FROWS = 16;          // rows per CTA
 constexpr int FCOLS = 64;          // columns per CTA, two per lane
-constexpr int FBOXW = FCOLS + 4;   // staged raw columns: 64 + 1 tap + 3 for 16-byte alignment
+// staged raw columns: 64 + 1 tap + up to one 16-byte granule for alignment
+template <class TF>
+constexpr int fboxw() { return FCOLS + Store<TF>::kAlign; }
 constexpr int FDMAX = 3;           // largest shift difference among a warp's slopes
 
 struct FwdTmaArgs {
@@ -85,7 +115,7 @@ struct FwdTmaArgs {
     int n_colblk;  // ceil(N_u0 / 64)
     int nrb;       // staged rows per plane (32 + CTA shift spread + 1, bounded on the host)
     int nf;        // raw-row buffers in the copy ring
-    int fstride;   // floats per raw buffer
+    int fstride;   // bytes per raw buffer
     int xstride;   // floats per interpolated buffer
     Tables T;
     int* err;
@@ -127,11 +157,15 @@ __device__ __forceinline__ void fwd_taps(float2 (&acc)[K], const float2 (&W)[K +
     for (int k = 0; k < K; k++) acc[k] = fma2(w1, W[k + O + 1], acc[k]);
 }
 
-template <int K>
+// TF: volume storage, TG: planogram storage (float or bfloat16); the
+// arithmetic is FP32 throughout.
+template <int K, class TF, class TG>
 __global__ void __launch_bounds__(32 * FGV * (FROWS / K), 2)
-k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const float* __restrict__ meas,
+k_fwd_tma(const __grid_constant__ CUtensorMap fmap, TG* __restrict__ g, const TG* __restrict__ meas,
           const FwdTmaArgs A)
 {
+    constexpr int FBOXW = fboxw<TF>();
+    constexpr int AL = Store<TF>::kAlign;
     constexpr int GR = FROWS / K;
     constexpr int NT = 32 * FGV * GR;
     constexpr int WN = K + FDMAX + 1;
@@ -150,8 +184,10 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
     const int NY = G.numY, NZ = G.numZ, NX = G.numX;
     const int nf = A.nf;
 
-    float* Fr = reinterpret_cast<float*>(smem);                       // [nf][nrb][68] raw rows (TMA)
-    float* Xs = Fr + nf * A.fstride;                                  // [4][nrb + 3][64] x-interpolated rows
+    auto Fr = [&](int slot) {  // [nf][nrb][FBOXW] raw rows (TMA)
+        return reinterpret_cast<TF*>(smem + size_t(slot) * A.fstride);
+    };
+    float* Xs = reinterpret_cast<float*>(smem + size_t(nf) * A.fstride);  // [4][nrb + 3][64] x-interpolated rows
     Shift* s_xt = reinterpret_cast<Shift*>(Xs + 4 * A.xstride);       // [NY] x shifts of view iv0
     Shift* s_zt = s_xt + NY;                                          // [nsl][NY] z shifts of the slopes
     uint64_t* bar = reinterpret_cast<uint64_t*>(s_zt + FSL * NY);     // [nf]
@@ -214,14 +250,14 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
         }
         __syncthreads();
         const int nlive = s_n[0];
-        const uint32_t box_bytes = uint32_t(FBOXW) * uint32_t(A.nrb) * 4u;
+        const uint32_t box_bytes = uint32_t(FBOXW) * uint32_t(A.nrb) * uint32_t(sizeof(TF));
         int issued = 0, islot = 0;  // thread 0 only: planes issued, ring slot of the next
         auto issue = [&](int li) {
             const int y = plist[li];
             const FwdPlane p = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y);
             mbar_arrive_expect_tx(&bar[islot], box_bytes);
-            // x rounded down to a multiple of 4 floats: TMA needs 16-byte aligned starts
-            tma_load_3d(Fr + islot * A.fstride, &fmap, &bar[islot], p.cx & ~3, y, p.wlo);
+            // x rounded down to a 16-byte granule: TMA needs 16-byte aligned starts
+            tma_load_3d(Fr(islot), &fmap, &bar[islot], p.cx & ~(AL - 1), y, p.wlo);
             islot = (islot + 1 == nf) ? 0 : islot + 1;
         };
         if (tid == 0) {
@@ -231,12 +267,12 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
         // stage A: x interpolation of plane p's staged rows (raw slot rb) into
         // interpolated buffer xb, a row per warp, two adjacent columns per lane
         auto stage_a = [&](int rb, int xb, const FwdPlane& p) {
-            const float* F = Fr + rb * A.fstride + (p.cx - (p.cx & ~3)) + 2 * lane;
+            const TF* F = Fr(rb) + (p.cx - (p.cx & ~(AL - 1))) + 2 * lane;
             float* X = Xs + xb * A.xstride + 2 * lane;
             const float w1 = p.wx, w0 = 1.0f - p.wx;
             for (int r = warp; r < p.nr; r += NT / 32) {
-                const float* fr = F + r * FBOXW;
-                const float a = fr[0], c = fr[1], d = fr[2];
+                const TF* fr = F + r * FBOXW;
+                const float a = Store<TF>::ld(fr[0]), c = Store<TF>::ld(fr[1]), d = Store<TF>::ld(fr[2]);
                 *reinterpret_cast<float2*>(X + r * FCOLS) = make_float2(fmaf(w1, c, w0 * a), fmaf(w1, d, w0 * c));
             }
         };
@@ -344,13 +380,14 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, float* __restrict__ g, const
             float2 val = make_float2(v0ok ? acc[j][k].x * S : 0.0f, v1ok ? acc[j][k].y * S : 0.0f);
             if (pairs && colA + 1 < G.N_u0) {
                 if (meas) {
-                    const float2 m = __ldg(reinterpret_cast<const float2*>(meas + o));
+                    const float2 m = Store<TG>::ld2(meas + o);
                     val = make_float2(ratio_rule(m.x, val.x), ratio_rule(m.y, val.y));
                 }
-                *reinterpret_cast<float2*>(g + o) = val;
+                Store<TG>::st2(g + o, val);
             } else {
-                if (colA < G.N_u0) g[o] = meas ? ratio_rule(__ldg(meas + o), val.x) : val.x;
-                if (colA + 1 < G.N_u0) g[o + 1] = meas ? ratio_rule(__ldg(meas + o + 1), val.y) : val.y;
+                if (colA < G.N_u0) g[o] = Store<TG>::st(meas ? ratio_rule(Store<TG>::ld(meas[o]), val.x) : val.x);
+                if (colA + 1 < G.N_u0)
+                    g[o + 1] = Store<TG>::st(meas ? ratio_rule(Store<TG>::ld(meas[o + 1]), val.y) : val.y);
             }
         }
     }
@@ -386,7 +423,7 @@ struct BwdTmaArgs {
     ViewRange vr;
     int ncw;      // column warps per plane group (32 columns each)
     int brb;      // staged rows per view (>= BWN + CTA shift spread, bounded on the host)
-    int sstride;  // floats per ring stage
+    int sstride;  // bytes per ring stage
     int ns;       // ring stages
     int accumulate;
     float scale;
@@ -431,9 +468,11 @@ __device__ __forceinline__ void bwd_taps4(float (&Z)[BPT][BK], const float (&W)[
 
 // PITCH > 0: the planogram row pitch N_u0 as a compile-time constant (shared
 // memory offsets become immediates); 0: read it from the geometry.
-template <bool ADJ, int PITCH>
+// TG: planogram storage, TF: volume storage (float or bfloat16); FP32
+// arithmetic throughout.
+template <bool ADJ, int PITCH, class TG, class TF>
 __global__ void __launch_bounds__(512, 1)
-k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const BwdTmaArgs A)
+k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const BwdTmaArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const petl_geom& G = A.G;
@@ -448,8 +487,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
     const int n_v0 = A.vr.n_v0(G.N_v0);
 
     const int ns = A.ns;
-    float* ring = reinterpret_cast<float*>(smem);                         // [ns][brb][NU0]
-    float* Zs = ring + ns * A.sstride;                                    // [BNP][BK][NU0]
+    auto ring = [&](int slot) {  // [ns][brb][NU0] planogram rows (TMA)
+        return reinterpret_cast<TG*>(smem + size_t(slot) * A.sstride);
+    };
+    float* Zs = reinterpret_cast<float*>(smem + size_t(ns) * A.sstride);  // [BNP][BK][NU0]
     float2* Wt = reinterpret_cast<float2*>(Zs + BNP * BK * NU0);          // [BV1CAP][BNP]
     float* s_w = reinterpret_cast<float*>(Wt + BV1CAP * BNP);             // [BV1CAP][BNP]
     int* s_v1 = reinterpret_cast<int*>(s_w + BV1CAP * BNP);               // [BV1CAP]
@@ -613,7 +654,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
             Wt[e] = make_float2(w0, w1);
         }
     };
-    const uint32_t box_bytes = uint32_t(NU0) * uint32_t(A.brb) * 4u;
+    const uint32_t box_bytes = uint32_t(NU0) * uint32_t(A.brb) * uint32_t(sizeof(TG));
     // producer state (thread 0): stages issued, and the next stage's ring
     // slot, slope index, view and ring round
     long long issued = 0;
@@ -634,7 +675,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
         }
         fence_proxy_async_smem();
         mbar_arrive_expect_tx(&full[p_slot], box_bytes);
-        tma_load_4d(ring + p_slot * A.sstride, &gmap, &full[p_slot], 0, s_grow[p_li], p_v0, s_v1[p_li]);
+        tma_load_4d(ring(p_slot), &gmap, &full[p_slot], 0, s_grow[p_li], p_v0, s_v1[p_li]);
         if (++p_slot == ns) {
             p_slot = 0;
             p_round++;
@@ -683,10 +724,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
             const uint32_t pat = (s_pat[li] >> (4 * pg)) & 15u;
             if (ucol && pat != uint32_t(kPatGeneric)) {
                 const int wb = (s_wb[li] >> (8 * pg)) & 0xff;
-                const float* Gs = ring + s * A.sstride + wb * NU0 + u;
+                const TG* Gs = ring(s) + wb * NU0 + u;
                 float W[BWN];
 #pragma unroll
-                for (int i = 0; i < BWN; i++) W[i] = Gs[i * NU0];
+                for (int i = 0; i < BWN; i++) W[i] = Store<TG>::ld(Gs[i * NU0]);
                 const float4* W4 = reinterpret_cast<const float4*>(Wt + li * BNP + pg * BPT);
                 const float4 wa = W4[0], wb4 = W4[1];
                 switch (pat) {
@@ -700,10 +741,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
                 }
             } else if (ucol && (code & 0x3333u)) {
                 const int wb = (s_wb[li] >> (8 * pg)) & 0xff;
-                const float* Gs = ring + s * A.sstride + wb * NU0 + u;
+                const TG* Gs = ring(s) + wb * NU0 + u;
                 float W[BWN];
 #pragma unroll
-                for (int i = 0; i < BWN; i++) W[i] = Gs[i * NU0];
+                for (int i = 0; i < BWN; i++) W[i] = Store<TG>::ld(Gs[i * NU0]);
                 const float2* Wl = Wt + li * BNP + pg * BPT;
 #pragma unroll
                 for (int q = 0; q < BPT; q++) {
@@ -792,8 +833,9 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, float* __restrict__ f, const
         for (int k = 0; k < BK; k++) {
             const int z = r0 + k;
             if (z >= NZ) break;
-            float* fr = f + (size_t(z) * NY + y) * NX;
-            if (u < NX) fr[u] = A.accumulate ? fr[u] + A.scale * Fv[q][k] : A.scale * Fv[q][k];
+            TF* fr = f + (size_t(z) * NY + y) * NX;
+            if (u < NX)
+                fr[u] = Store<TF>::st(A.accumulate ? Store<TF>::ld(fr[u]) + A.scale * Fv[q][k] : A.scale * Fv[q][k]);
         }
     }
 }
@@ -812,13 +854,18 @@ constexpr int kFwdK = 8;
 
 }  // namespace
 
-int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
-                const Tables& T, cudaStream_t st)
+template <class TF, class TG>
+int project_tma_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr, const TG* meas, const Tables& T,
+                  cudaStream_t st)
 {
+    constexpr int FBOXW = fboxw<TF>();
+    constexpr int EB = int(sizeof(TF));
     const int n_v0 = vr.n_v0(G.N_v0);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (n_v0 <= 0 || nv1 <= 0) return 0;
-    if (G.numX % 4 != 0 || (reinterpret_cast<uintptr_t>(f) & 15) != 0 || G.numY > 4096) return kNotApplicable;
+    // volume rows a multiple of 16 bytes (TMA strides), 16-byte aligned base
+    if ((G.numX * EB) % 16 != 0 || (reinterpret_cast<uintptr_t>(f) & 15) != 0 || G.numY > 4096)
+        return kNotApplicable;
     const double step = double(G.T_v1) * plane_ymax(G) / double(G.T_z);  // shift change per slope
     if (shift_spread(FV - 1, step) > FDMAX) return kNotApplicable;
     const int nrb = FROWS + shift_spread(FSL - 1, step) + 1;
@@ -827,23 +874,23 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
     if (!err) return kNotApplicable;
     CUtensorMap map;
     const uint64_t dims[3] = {uint64_t(G.numX), uint64_t(G.numY), uint64_t(G.numZ)};
-    const uint64_t strides[2] = {uint64_t(G.numX) * 4, uint64_t(G.numX) * G.numY * 4};
+    const uint64_t strides[2] = {uint64_t(G.numX) * EB, uint64_t(G.numX) * G.numY * EB};
     const uint32_t box[3] = {uint32_t(FBOXW), 1u, uint32_t(nrb)};
-    if (!encode_tensor_map(&map, f, 3, dims, strides, box)) return kNotApplicable;
+    if (!encode_tensor_map(&map, f, 3, dims, strides, box, EB)) return kNotApplicable;
 
     FwdTmaArgs A{};
     A.G = G;
     A.vr = vr;
     A.n_colblk = int(ceil_div(G.N_u0, FCOLS));
     A.nrb = nrb;
-    A.fstride = ((nrb * FBOXW * 4 + 127) & ~127) / 4;
+    A.fstride = (nrb * FBOXW * EB + 127) & ~127;
     A.xstride = (nrb + FDMAX) * FCOLS;
     A.T = T;
     A.err = err;
     // up to 4 planes in flight; prefer a footprint that leaves room for two
     // CTAs per SM, else the largest ring that fits one
     auto bytes = [&](int nf) {
-        return size_t(nf) * A.fstride * 4 + size_t(4) * A.xstride * 4 + size_t(1 + FSL) * G.numY * sizeof(Shift) +
+        return size_t(nf) * A.fstride + size_t(4) * A.xstride * 4 + size_t(1 + FSL) * G.numY * sizeof(Shift) +
                size_t(nf) * 8 + 2 * 4 + size_t(G.numY) * 2;
     };
     A.nf = 0;
@@ -853,7 +900,7 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
         if (bytes(nf) <= 227 * 1024) A.nf = nf;
     if (!A.nf) return kNotApplicable;
     const size_t smem = bytes(A.nf);
-    auto kern = k_fwd_tma<kFwdK>;
+    auto kern = k_fwd_tma<kFwdK, TF, TG>;
     PETL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid(unsigned(n_v0), ceil_div(nv1, FSL), unsigned(A.n_colblk) * ceil_div(G.N_u1, FROWS));
     kern<<<grid, 32 * FGV * (FROWS / kFwdK), smem, st>>>(map, g, meas, A);
@@ -861,11 +908,13 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
     return 0;
 }
 
-int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
-                    const ViewRange& vr, const Tables& T, cudaStream_t st)
+template <class TG, class TF>
+int backproject_tma_t(const petl_geom& G, const TG* g, TF* f, int mode, int accumulate, float scale,
+                      const ViewRange& vr, const Tables& T, cudaStream_t st)
 {
+    constexpr int EB = int(sizeof(TG));
     const int NU0 = G.N_u0;
-    if (NU0 % 4 != 0 || NU0 > 256 || G.numX > 256 || (reinterpret_cast<uintptr_t>(g) & 15) != 0)
+    if ((NU0 * EB) % 16 != 0 || NU0 > 256 || G.numX > 256 || (reinterpret_cast<uintptr_t>(g) & 15) != 0)
         return kNotApplicable;
     if (vr.iv1_end - vr.iv1_begin > BV1CAP) return kNotApplicable;
     const double step = double(std::max(std::fabs(G.v1_0), std::fabs(G.v1_0 + (G.N_v1 - 1) * G.T_v1))) *
@@ -877,17 +926,17 @@ int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int 
     if (!err) return kNotApplicable;
     CUtensorMap map;
     const uint64_t dims[4] = {uint64_t(NU0), uint64_t(G.N_u1), uint64_t(G.N_v0), uint64_t(G.N_v1)};
-    const uint64_t strides[3] = {uint64_t(NU0) * 4, uint64_t(NU0) * G.N_u1 * 4,
-                                 uint64_t(NU0) * G.N_u1 * G.N_v0 * 4};
+    const uint64_t strides[3] = {uint64_t(NU0) * EB, uint64_t(NU0) * G.N_u1 * EB,
+                                 uint64_t(NU0) * G.N_u1 * G.N_v0 * EB};
     const uint32_t box[4] = {uint32_t(NU0), uint32_t(brb), 1u, 1u};
-    if (!encode_tensor_map(&map, g, 4, dims, strides, box)) return kNotApplicable;
+    if (!encode_tensor_map(&map, g, 4, dims, strides, box, EB)) return kNotApplicable;
 
     BwdTmaArgs A{};
     A.G = G;
     A.vr = vr;
     A.ncw = int(ceil_div(std::max(NU0, G.numX), 32));
     A.brb = brb;
-    A.sstride = ((brb * NU0 * 4 + 127) & ~127) / 4;
+    A.sstride = (brb * NU0 * EB + 127) & ~127;
     A.accumulate = accumulate;
     A.scale = scale;
     A.T = T;
@@ -896,17 +945,42 @@ int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int 
     const size_t fixed = size_t(BNP) * BK * NU0 * 4 + size_t(BV1CAP) * BNP * 8 + size_t(BV1CAP) * BNP * 4 +
                          size_t(BV1CAP) * 4 * 4 + size_t(BV1CAP) * BPG * 4 + size_t(BV1CAP) * 4 + 2 * BNSMAX * 8 +
                          16;
-    A.ns = int(std::min<size_t>(BNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / (size_t(A.sstride) * 4)));
+    A.ns = int(std::min<size_t>(BNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / size_t(A.sstride)));
     if (A.ns < 2) return kNotApplicable;
-    const size_t smem = size_t(A.ns) * A.sstride * 4 + fixed;
+    const size_t smem = size_t(A.ns) * A.sstride + fixed;
     const int threads = 32 * A.ncw * BPG;
     dim3 grid(ceil_div(G.numY, BNP), ceil_div(G.numZ, BK));
-    auto kern = mode == PETL_BP_ADJOINT ? (NU0 == 256 ? k_bwd_tma<true, 256> : k_bwd_tma<true, 0>)
-                                        : (NU0 == 256 ? k_bwd_tma<false, 256> : k_bwd_tma<false, 0>);
+    auto kern = mode == PETL_BP_ADJOINT
+                    ? (NU0 == 256 ? k_bwd_tma<true, 256, TG, TF> : k_bwd_tma<true, 0, TG, TF>)
+                    : (NU0 == 256 ? k_bwd_tma<false, 256, TG, TF> : k_bwd_tma<false, 0, TG, TF>);
     PETL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     kern<<<grid, threads, smem, st>>>(map, f, A);
     PETL_LAUNCH_CHECK("backproject_tma");
     return 0;
+}
+
+int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                const Tables& T, cudaStream_t st)
+{
+    return project_tma_t<float, float>(G, f, g, vr, meas, T, st);
+}
+
+int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                    const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    return backproject_tma_t<float, float>(G, g, f, mode, accumulate, scale, vr, T, st);
+}
+
+int project_tma_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
+                     const __nv_bfloat16* meas, const Tables& T, cudaStream_t st)
+{
+    return project_tma_t<__nv_bfloat16, __nv_bfloat16>(G, f, g, vr, meas, T, st);
+}
+
+int backproject_tma_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate, float scale,
+                         const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    return backproject_tma_t<__nv_bfloat16, float>(G, g, f, mode, accumulate, scale, vr, T, st);
 }
 
 }  // namespace shear

@@ -2,6 +2,7 @@
 // projector_shear_tma.cu).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -43,6 +44,13 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
                 const Tables& T, cudaStream_t st);
 int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
                     const ViewRange& vr, const Tables& T, cudaStream_t st);
+// BF16 storage (volume and planogram in bfloat16, FP32 arithmetic; the
+// backprojection writes an FP32 volume).  Same layout rules with 2-byte
+// elements.
+int project_tma_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
+                     const __nv_bfloat16* meas, const Tables& T, cudaStream_t st);
+int backproject_tma_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate, float scale,
+                         const ViewRange& vr, const Tables& T, cudaStream_t st);
 
 }  // namespace shear
 

@@ -48,14 +48,15 @@ int* device_error_ptr()
 }
 
 bool encode_tensor_map(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
-                       const uint64_t* strides_bytes, const uint32_t* box)
+                       const uint64_t* strides_bytes, const uint32_t* box, int elem_bytes)
 {
     EncodeFn fn = encode_fn();
     if (!fn) return false;
+    if (elem_bytes != 4 && elem_bytes != 2) return false;
     if (reinterpret_cast<uintptr_t>(base) & 15) return false;
     for (int i = 0; i + 1 < rank; i++)
         if (strides_bytes[i] & 15) return false;
-    if ((box[0] * 4) & 15) return false;
+    if ((box[0] * uint32_t(elem_bytes)) & 15) return false;
     cuuint64_t d[5], s[4];
     cuuint32_t b[5], e[5];
     for (int i = 0; i < rank; i++) {
@@ -65,7 +66,8 @@ bool encode_tensor_map(CUtensorMap* map, const void* base, int rank, const uint6
         if (b[i] == 0 || b[i] > 256) return false;
     }
     for (int i = 0; i + 1 < rank; i++) s[i] = strides_bytes[i];
-    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, cuuint32_t(rank), const_cast<void*>(base), d, s, b, e,
+    const CUtensorMapDataType dt = elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const CUresult r = fn(map, dt, cuuint32_t(rank), const_cast<void*>(base), d, s, b, e,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;

@@ -97,10 +97,11 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
-// Host: encode a float32 tiled tensor map (dims/box fastest first).  Returns
-// false when the driver entry point is unavailable or the layout is not
-// TMA-compatible (base 16-byte aligned, strides multiples of 16 bytes).
+// Host: encode a tiled tensor map of float32 (elem_bytes 4) or bfloat16
+// (elem_bytes 2) elements, dims/box fastest first.  Returns false when the
+// driver entry point is unavailable or the layout is not TMA-compatible (base
+// 16-byte aligned, strides and the box's inner extent multiples of 16 bytes).
 bool encode_tensor_map(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
-                       const uint64_t* strides_bytes, const uint32_t* box);
+                       const uint64_t* strides_bytes, const uint32_t* box, int elem_bytes = 4);
 
 }  // namespace petl

@@ -35,6 +35,16 @@ def _n(t):
     return ctypes.c_longlong(t.numel())
 
 
+def _dev16(t, name="tensor"):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise PetlError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.bfloat16:
+        raise PetlError(f"{name} must be bfloat16")
+    if not t.is_contiguous():
+        raise PetlError(f"{name} must be contiguous")
+    return ctypes.c_void_p(t.data_ptr())
+
+
 # ----------------------------------------------------------------------------
 # projectors
 # ----------------------------------------------------------------------------
@@ -91,6 +101,50 @@ def backproject(geom, g, f=None, mode="reference", accumulate=False, scale=1.0, 
         acc = 1 if (accumulate or i > 0) else 0
         check(lib().petl_backproject_range_dev(G.ptr, _dev(gi, "g"), _dev(f, "f"), m, acc, float(scale), b, e,
                                                first, step, _stream()), "backproject")
+    return f
+
+
+# ----------------------------------------------------------------------------
+# BF16 storage: bfloat16 volumes / planograms, FP32 footprint accumulation
+# ----------------------------------------------------------------------------
+def project_bf16(geom, f, g=None, subset=None, v1_range=None):
+    """g = P f with f and g in bfloat16 (one geometry)."""
+    if g is None:
+        g = torch.zeros(geom.shape, device=f.device, dtype=torch.bfloat16)
+    first, step = subset if subset is not None else (0, 1)
+    b, e = v1_range if v1_range is not None else (0, geom.shape[0])
+    check(lib().petl_project_bf16_dev(geom.ptr, _dev16(f, "f"), _dev16(g, "g"), b, e, first, step, _stream()),
+          "project_bf16")
+    return g
+
+
+def project_ratio_bf16(geom, f, meas, out=None, subset=None, v1_range=None):
+    """out = meas / (P f) (0 where P f == 0), all bfloat16."""
+    if out is None:
+        out = torch.empty_like(meas)
+    first, step = subset if subset is not None else (0, 1)
+    b, e = v1_range if v1_range is not None else (0, geom.shape[0])
+    check(lib().petl_project_ratio_bf16_dev(geom.ptr, _dev16(f, "f"), _dev16(meas, "meas"), _dev16(out, "out"), b, e,
+                                            first, step, _stream()), "project_ratio_bf16")
+    return out
+
+
+def backproject_bf16(geom, g, f=None, mode="reference", accumulate=False, scale=1.0, subset=None, v1_range=None):
+    """f (float32) = P^T g with g in bfloat16."""
+    if f is None:
+        f = torch.empty(geom.vol_shape, device=g.device, dtype=torch.float32)
+        accumulate = False
+    first, step = subset if subset is not None else (0, 1)
+    b, e = v1_range if v1_range is not None else (0, geom.shape[0])
+    check(lib().petl_backproject_bf16_dev(geom.ptr, _dev16(g, "g"), _dev(f, "f"), _MODES[mode], 1 if accumulate else 0,
+                                          float(scale), b, e, first, step, _stream()), "backproject_bf16")
+    return f
+
+
+def mlem_update_bf16_(f, d, sens):
+    """f (bfloat16) *= d / sens with d/0 -> 0."""
+    check(lib().petl_mlem_update_bf16_dev(_dev16(f, "f"), _dev(d, "d"), _dev(sens, "sens"), _n(f), _stream()),
+          "mlem_update_bf16")
     return f
 
 
@@ -256,5 +310,5 @@ def osl_update_(f, d, sens, Df):
 
 __all__ = ["Geometry", "project", "project_ratio", "backproject", "nnz", "pfdr", "ramp_", "fbp", "rd_gradient", "rd_cost",
            "tv_gradient", "tv_cost", "tv_quadform", "gaussian_filter_", "rdivide_", "divide_", "multiply_",
-           "reciprocal_", "axpby_", "dot", "loglik", "poisson_grad_", "mlem_update_", "osl_update_", "REFERENCE",
-           "ADJOINT"]
+           "reciprocal_", "axpby_", "dot", "loglik", "poisson_grad_", "mlem_update_", "osl_update_", "project_bf16",
+           "project_ratio_bf16", "backproject_bf16", "mlem_update_bf16_", "REFERENCE", "ADJOINT"]

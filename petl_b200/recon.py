@@ -84,6 +84,36 @@ def osem(geoms, g, num_iter, num_subsets, f=None, delta=2.0, beta=0.0, sens=None
     return f, history
 
 
+def osem_bf16(geom, g, num_iter, num_subsets, f=None, sens=None):
+    """OSEM with the volume, the measured planogram and the data ratio stored
+    in bfloat16 (half the HBM bytes of the planogram-sized arrays); the
+    footprints accumulate in FP32, the backprojection and the sensitivity
+    images are FP32, the update rounds the image to bfloat16 once per
+    subset.  One axis-aligned, equal-pitch geometry (the TMA path).
+    Returns the bfloat16 image."""
+    S = int(num_subsets)
+    device = g.device
+    if g.dtype != torch.bfloat16:
+        raise ValueError("osem_bf16 expects bfloat16 data")
+    if f is None:
+        f = torch.ones(geom.vol_shape, device=device, dtype=torch.bfloat16)
+    if sens is None:
+        ones = torch.ones(geom.shape, device=device, dtype=torch.bfloat16)
+        sens = []
+        for s in range(S):
+            x = ops.backproject_bf16(geom, ones, subset=(s, S))
+            x[x == 0.0] = 1.0
+            sens.append(x)
+    ratio = torch.empty_like(g)
+    d = torch.empty(geom.vol_shape, device=device, dtype=torch.float32)
+    for _ in range(num_iter):
+        for s in range(S):
+            ops.project_ratio_bf16(geom, f, g, out=ratio, subset=(s, S))
+            ops.backproject_bf16(geom, ratio, f=d, subset=(s, S))
+            ops.mlem_update_bf16_(f, d, sens[s])
+    return f
+
+
 def loglik(geoms, g, f):
     """Poisson log-likelihood of f (FP64, device)."""
     geoms = as_list(geoms)
