@@ -157,6 +157,31 @@ int petl_backproject_bf16_dev(const petl_geom* G, const void* g, float* f, int m
 /* f (bfloat16) *= d / sens with the DIV rule (d/0 -> 0) */
 int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long long n, void* stream);
 
+/* --- reconstruction server ------------------------------------------------
+ * No single reference counterpart: the reference serves one call at a time
+ * through petl_server.py (src/petl_server.py:1534-1606).  A worker thread
+ * owns the device and runs OSEM requests (reference-semantics
+ * backprojector, f starting at 1, sensitivity zeros -> 1) with continuous
+ * batching: requests are admitted in arrival order while their device
+ * footprint fits hbm_budget_bytes and fewer than max_active run; every
+ * active request has its own stream with up to `depth` subset steps in
+ * flight, issued round-robin, so requests overlap on the GPU and join while
+ * others run.  Data and images stay resident until the result is copied
+ * out.  A request's result does not depend on what else runs. */
+void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int device);
+/* g_host: the request's planogram, which must stay valid until
+ * petl_server_wait returns for it; *id_out receives the request id. */
+int petl_server_submit(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
+                       long long* id_out);
+/* Blocks until the request finishes; copies the image (numZ*numY*numX
+ * floats) to f_host when non-null; latency = submit to result on the host,
+ * queue = submit to admission, both in seconds. */
+int petl_server_wait(void* server, long long id, float* f_host, double* latency_s, double* queue_s);
+/* out[0..5]: completed, failed, active, pending, HBM bytes reserved now,
+ * peak HBM bytes reserved */
+int petl_server_stats(void* server, double* out);
+void petl_server_destroy(void* server);
+
 /* --- regularizers, volume [N1][N2][N3] ------------------------------------ */
 /* aTV_RelativeDifferencesLoss_gradient (src/relative_differences.cu:481-532) */
 int petl_rd_gradient_dev(const float* f, float* Df, int N1, int N2, int N3, float delta, float beta, void* stream);

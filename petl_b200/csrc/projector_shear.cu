@@ -382,7 +382,7 @@ namespace {
 constexpr size_t kNoAllocTableBytes = size_t(4) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_tables[kNoAllocTableBytes];
 
-size_t table_bytes(const petl_geom& G)
+size_t tables_size(const petl_geom& G)
 {
     const size_t nx = size_t(G.N_v0) * G.numY, nz = size_t(G.N_v1) * G.numY, ns = size_t(G.N_v1) * G.N_v0;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
@@ -423,20 +423,16 @@ bool shear_eligible(const petl_geom& G)
     return true;
 }
 
-int launch_project_shear(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
-                         cudaStream_t st)
+int shear::project_with(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                        const Tables& T, cudaStream_t st)
 {
     const int n_v0 = vr.n_v0(G.N_v0);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (n_v0 <= 0 || nv1 <= 0) return 0;
-    TableBuf tb;
-    int rc = shear::make_tables(G, tb, st);
-    if (rc) return rc;
     if (dispatch_mode() != 2) {
-        rc = shear::project_tma(G, f, g, vr, meas, tb.T, st);
+        const int rc = shear::project_tma(G, f, g, vr, meas, T, st);
         if (rc != shear::kNotApplicable) {
             note_path(2);
-            cudaFreeAsync(tb.base, st);
             return rc;
         }
     }
@@ -449,7 +445,7 @@ int launch_project_shear(const petl_geom& G, const float* f, float* g, const Vie
     A.vr = vr;
     A.n_colblk = int(ceil_div(G.N_u0, 32));
     A.maxr = F_ROWS + spread + 1;
-    A.T = tb.T;
+    A.T = T;
     const size_t smem = size_t(2) * A.maxr * 32 * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k_fwd_shear, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e == cudaSuccess) {
@@ -458,7 +454,6 @@ int launch_project_shear(const petl_geom& G, const float* f, float* g, const Vie
         note_launch();
         e = cudaGetLastError();
     }
-    cudaFreeAsync(tb.base, st);
     if (e != cudaSuccess) {
         set_error(std::string("project_shear: ") + cudaGetErrorString(e));
         return int(e);
@@ -466,17 +461,27 @@ int launch_project_shear(const petl_geom& G, const float* f, float* g, const Vie
     return 0;
 }
 
-int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
-                             const ViewRange& vr, cudaStream_t st)
+size_t shear::table_bytes(const petl_geom& G) { return tables_size(G); }
+
+int launch_project_shear(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                         cudaStream_t st)
 {
+    if (vr.n_v0(G.N_v0) <= 0 || vr.iv1_end <= vr.iv1_begin) return 0;
     TableBuf tb;
     int rc = shear::make_tables(G, tb, st);
     if (rc) return rc;
+    rc = shear::project_with(G, f, g, vr, meas, tb.T, st);
+    cudaFreeAsync(tb.base, st);
+    return rc;
+}
+
+int shear::backproject_with(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                            const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
     if (dispatch_mode() != 2) {
-        rc = shear::backproject_tma(G, g, f, mode, accumulate, scale, vr, tb.T, st);
+        const int rc = shear::backproject_tma(G, g, f, mode, accumulate, scale, vr, T, st);
         if (rc != shear::kNotApplicable) {
             note_path(2);
-            cudaFreeAsync(tb.base, st);
             return rc;
         }
     }
@@ -488,7 +493,7 @@ int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int m
     A.ng = std::max(1, std::min(2, 16 / A.ncw));
     A.accumulate = accumulate;
     A.scale = scale;
-    A.T = tb.T;
+    A.T = T;
     const int threads = A.ncw * 32 * A.ng;
     const size_t smem = size_t(A.ng) * BNP * BK * G.N_u0 * sizeof(float);
     cudaError_t e = cudaSuccess;
@@ -502,12 +507,22 @@ int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int m
     }
     note_launch();
     if (e == cudaSuccess) e = cudaGetLastError();
-    cudaFreeAsync(tb.base, st);
     if (e != cudaSuccess) {
         set_error(std::string("backproject_shear: ") + cudaGetErrorString(e));
         return int(e);
     }
     return 0;
+}
+
+int launch_backproject_shear(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                             const ViewRange& vr, cudaStream_t st)
+{
+    TableBuf tb;
+    int rc = shear::make_tables(G, tb, st);
+    if (rc) return rc;
+    rc = shear::backproject_with(G, g, f, mode, accumulate, scale, vr, tb.T, st);
+    cudaFreeAsync(tb.base, st);
+    return rc;
 }
 
 }  // namespace petl
@@ -524,7 +539,7 @@ extern "C" int petl_project_noalloc_dev(const petl_geom* G, const float* f, floa
     // geometries outside the shear kernels' domain use the general kernel,
     // which needs no scratch memory at all
     if (!shear_eligible(*G)) return launch_project_general(*G, f, g, vr, nullptr, st);
-    const size_t need = table_bytes(*G);
+    const size_t need = tables_size(*G);
     if (need > kNoAllocTableBytes) {
         set_error("project_noalloc: this geometry needs " + std::to_string(need) +
                   " bytes of table scratch; the allocation-free entry point holds at most " +

@@ -1,0 +1,441 @@
+// Reconstruction server: continuous batching of OSEM requests on one GPU.
+//
+// The reference serves reconstructions one call at a time through
+// petl_server.py (src/petl_server.py:1534-1606), moving the planogram over
+// PCIe on every iteration.  Here a worker thread owns the device:
+//
+//  * admission: a submitted request waits until its device footprint (data,
+//    ratio, image, backprojection, one sensitivity image per subset, shift
+//    tables) fits the HBM budget next to the requests already running and a
+//    slot is free; then its data is copied in once and stays resident;
+//  * continuous batching: every active request has its own CUDA stream, and
+//    the worker keeps up to `depth` OSEM subset steps in flight per request,
+//    issuing round-robin, so steps of different requests overlap on the GPU
+//    and new requests join while others run;
+//  * completion: after the last step the image is copied to a pinned host
+//    buffer, the device memory is returned to the stream-ordered pool and
+//    the request's latency (submit to result on the host) is recorded.
+//
+// Each request runs the same kernels in the same order whatever else is
+// running, so its result is bit-identical alone and in a mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "projector.cuh"
+#include "shear.cuh"
+
+namespace petl {
+bool shear_eligible(const petl_geom& G);
+int project_range(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                  cudaStream_t st);
+int backproject_range(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                      const ViewRange& vr, cudaStream_t st);
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+__global__ void k_fill(float* __restrict__ x, long long n, float v)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = v;
+}
+
+// zeros -> 1 (sensitivity normalisation of the reference MLEM)
+__global__ void k_zero_to_one(float* __restrict__ x, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (x[i] == 0.0f) x[i] = 1.0f;
+}
+
+__global__ void k_mlem(float* __restrict__ f, const float* __restrict__ d, const float* __restrict__ s, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float den = s[i];
+        f[i] *= den == 0.0f ? 0.0f : d[i] / den;
+    }
+}
+
+unsigned blocks_for(long long n) { return unsigned(std::min<long long>((n + 255) / 256, 148LL * 8)); }
+
+enum State { kPending = 0, kActive = 1, kDone = 2, kFailed = 3 };
+
+struct Request {
+    long long id = 0;
+    petl_geom G{};
+    const float* g_host = nullptr;
+    int subsets = 1, iters = 1;
+    State state = kPending;
+    std::string error;
+    Clock::time_point t_submit, t_admit, t_done;
+    size_t bytes = 0;
+    // device state
+    cudaStream_t st = nullptr;
+    float *g = nullptr, *ratio = nullptr, *f = nullptr, *d = nullptr, *sens = nullptr;
+    shear::TableBuf tables;
+    bool shear = false;
+    int steps_total = 0, steps_issued = 0;
+    std::deque<cudaEvent_t> inflight;  // one event per issued step
+    cudaEvent_t result_ev = nullptr;
+    float* out_host = nullptr;  // pinned
+    bool result_issued = false;
+};
+
+size_t footprint(const petl_geom& G, int subsets)
+{
+    const size_t ng = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0, nv = size_t(G.numX) * G.numY * G.numZ;
+    return 4 * (2 * ng + (2 + size_t(subsets)) * nv) + shear::table_bytes(G) + (size_t(1) << 20);
+}
+
+}  // namespace
+
+struct Server {
+    int device = 0;
+    double budget = 0;
+    int max_active = 1, depth = 2;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    long long next_id = 1;
+    std::deque<std::shared_ptr<Request>> pending;
+    std::vector<std::shared_ptr<Request>> active;
+    std::map<long long, std::shared_ptr<Request>> all;
+    double in_use = 0, peak = 0;
+    long long completed = 0, failed = 0;
+    std::thread worker;
+
+    void run();
+    bool admit(Request& r);
+    bool issue_step(Request& r);
+    void release(Request& r);
+    void fail(Request& r, const std::string& why);
+};
+
+namespace {
+
+int stream_for(cudaStream_t* st)
+{
+    return cudaStreamCreateWithFlags(st, cudaStreamNonBlocking) == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace
+
+void Server::fail(Request& r, const std::string& why)
+{
+    r.error = why;
+    r.state = kFailed;
+}
+
+bool Server::admit(Request& r)
+{
+    // device buffers and the data copy, all on the request's stream
+    const petl_geom& G = r.G;
+    const long long ng = (long long)G.N_v1 * G.N_v0 * G.N_u1 * G.N_u0;
+    const long long nv = (long long)G.numX * G.numY * G.numZ;
+    if (stream_for(&r.st)) {
+        fail(r, "cannot create a stream");
+        return false;
+    }
+    bool ok = cudaMallocAsync(reinterpret_cast<void**>(&r.g), ng * 4, r.st) == cudaSuccess &&
+              cudaMallocAsync(reinterpret_cast<void**>(&r.ratio), ng * 4, r.st) == cudaSuccess &&
+              cudaMallocAsync(reinterpret_cast<void**>(&r.f), nv * 4, r.st) == cudaSuccess &&
+              cudaMallocAsync(reinterpret_cast<void**>(&r.d), nv * 4, r.st) == cudaSuccess &&
+              cudaMallocAsync(reinterpret_cast<void**>(&r.sens), nv * 4 * r.subsets, r.st) == cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void**>(&r.out_host), nv * 4, cudaHostAllocDefault) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(r.g, r.g_host, ng * 4, cudaMemcpyHostToDevice, r.st) == cudaSuccess;
+    r.shear = shear_eligible(G);
+    if (ok && r.shear) ok = shear::make_tables(G, r.tables, r.st) == 0;
+    if (!ok) {
+        fail(r, "admission failed: " + std::string(cudaGetErrorString(cudaGetLastError())));
+        return false;
+    }
+    // image starts at 1; per-subset sensitivities P_s^T 1 with zeros -> 1
+    k_fill<<<blocks_for(nv), 256, 0, r.st>>>(r.f, nv, 1.0f);
+    k_fill<<<blocks_for(ng), 256, 0, r.st>>>(r.ratio, ng, 1.0f);
+    note_launch();
+    note_launch();
+    for (int s = 0; s < r.subsets && ok; s++) {
+        const ViewRange vr{0, G.N_v1, s, r.subsets};
+        float* sv = r.sens + size_t(s) * nv;
+        const int rc = r.shear ? shear::backproject_with(G, r.ratio, sv, PETL_BP_REFERENCE, 0, 1.0f, vr, r.tables.T, r.st)
+                               : backproject_range(G, r.ratio, sv, PETL_BP_REFERENCE, 0, 1.0f, vr, r.st);
+        ok = rc == 0;
+        k_zero_to_one<<<blocks_for(nv), 256, 0, r.st>>>(sv, nv);
+        note_launch();
+    }
+    if (!ok) {
+        fail(r, "sensitivity failed");
+        return false;
+    }
+    r.steps_total = r.iters * r.subsets;
+    r.state = kActive;
+    r.t_admit = Clock::now();
+    return true;
+}
+
+bool Server::issue_step(Request& r)
+{
+    const petl_geom& G = r.G;
+    const long long nv = (long long)G.numX * G.numY * G.numZ;
+    const int s = r.steps_issued % r.subsets;
+    const ViewRange vr{0, G.N_v1, s, r.subsets};
+    int rc = r.shear ? shear::project_with(G, r.f, r.ratio, vr, r.g, r.tables.T, r.st)
+                     : project_range(G, r.f, r.ratio, vr, r.g, r.st);
+    if (!rc)
+        rc = r.shear ? shear::backproject_with(G, r.ratio, r.d, PETL_BP_REFERENCE, 0, 1.0f, vr, r.tables.T, r.st)
+                     : backproject_range(G, r.ratio, r.d, PETL_BP_REFERENCE, 0, 1.0f, vr, r.st);
+    if (rc) {
+        fail(r, "OSEM step failed");
+        return false;
+    }
+    k_mlem<<<blocks_for(nv), 256, 0, r.st>>>(r.f, r.d, r.sens + size_t(s) * nv, nv);
+    note_launch();
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventRecord(ev, r.st);
+    r.inflight.push_back(ev);
+    r.steps_issued++;
+    return true;
+}
+
+void Server::release(Request& r)
+{
+    for (cudaEvent_t e : r.inflight) cudaEventDestroy(e);
+    r.inflight.clear();
+    if (r.result_ev) cudaEventDestroy(r.result_ev);
+    r.result_ev = nullptr;
+    if (r.st) {
+        if (r.g) cudaFreeAsync(r.g, r.st);
+        if (r.ratio) cudaFreeAsync(r.ratio, r.st);
+        if (r.f) cudaFreeAsync(r.f, r.st);
+        if (r.d) cudaFreeAsync(r.d, r.st);
+        if (r.sens) cudaFreeAsync(r.sens, r.st);
+        if (r.tables.base) cudaFreeAsync(r.tables.base, r.st);
+        cudaStreamSynchronize(r.st);
+        cudaStreamDestroy(r.st);
+    }
+    r.g = r.ratio = r.f = r.d = r.sens = nullptr;
+    r.tables.base = nullptr;
+    r.st = nullptr;
+}
+
+void Server::run()
+{
+    cudaSetDevice(device);
+    while (true) {
+        std::vector<std::shared_ptr<Request>> to_admit;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (stop) break;
+            // admission by HBM budget and free slots, in arrival order
+            while (!pending.empty() && int(active.size() + to_admit.size()) < max_active) {
+                auto& r = pending.front();
+                if (in_use + double(r->bytes) > budget && !(active.empty() && to_admit.empty())) break;
+                in_use += double(r->bytes);
+                peak = std::max(peak, in_use);
+                to_admit.push_back(r);
+                pending.pop_front();
+            }
+        }
+        for (auto& r : to_admit) {
+            if (!admit(*r)) {
+                release(*r);
+                std::lock_guard<std::mutex> lk(mu);
+                in_use -= double(r->bytes);
+                failed++;
+                r->t_done = Clock::now();
+                cv_done.notify_all();
+                continue;
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            active.push_back(r);
+        }
+        bool progressed = !to_admit.empty();
+        // retire finished steps, issue new ones round-robin
+        for (auto& rp : active) {
+            Request& r = *rp;
+            while (!r.inflight.empty() && cudaEventQuery(r.inflight.front()) == cudaSuccess) {
+                cudaEventDestroy(r.inflight.front());
+                r.inflight.pop_front();
+                progressed = true;
+            }
+            if (r.state == kActive && !r.result_issued && r.steps_issued < r.steps_total &&
+                int(r.inflight.size()) < depth) {
+                if (issue_step(r)) progressed = true;
+            }
+            if (r.state == kActive && !r.result_issued && r.steps_issued == r.steps_total) {
+                const long long nv = (long long)r.G.numX * r.G.numY * r.G.numZ;
+                cudaMemcpyAsync(r.out_host, r.f, nv * 4, cudaMemcpyDeviceToHost, r.st);
+                cudaEventCreateWithFlags(&r.result_ev, cudaEventDisableTiming);
+                cudaEventRecord(r.result_ev, r.st);
+                r.result_issued = true;
+                progressed = true;
+            }
+        }
+        // completions
+        std::vector<std::shared_ptr<Request>> finished;
+        for (auto& rp : active) {
+            Request& r = *rp;
+            const bool failed_now = r.state == kFailed;
+            const bool done = r.result_issued && cudaEventQuery(r.result_ev) == cudaSuccess;
+            if (done || failed_now) finished.push_back(rp);
+        }
+        for (auto& rp : finished) {
+            Request& r = *rp;
+            release(r);
+            std::lock_guard<std::mutex> lk(mu);
+            if (r.state != kFailed) {
+                r.state = kDone;
+                completed++;
+            } else {
+                failed++;
+            }
+            r.t_done = Clock::now();
+            in_use -= double(r.bytes);
+            active.erase(std::find(active.begin(), active.end(), rp));
+            cv_done.notify_all();
+            progressed = true;
+        }
+        if (!progressed) {
+            std::unique_lock<std::mutex> lk(mu);
+            if (active.empty() && pending.empty())
+                cv_work.wait(lk, [&] { return stop || !pending.empty(); });
+            else if (!active.empty()) {
+                // wait for the oldest step of some request instead of spinning
+                lk.unlock();
+                for (auto& rp : active)
+                    if (!rp->inflight.empty()) {
+                        cudaEventSynchronize(rp->inflight.front());
+                        break;
+                    }
+            }
+        }
+    }
+    // shutdown: drop whatever is left
+    for (auto& rp : active) release(*rp);
+    for (auto& rp : pending) rp->state = kFailed;
+}
+
+}  // namespace petl
+
+using namespace petl;
+
+extern "C" {
+
+void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int device)
+{
+    clear_error();
+    if (hbm_budget_bytes <= 0 || max_active < 1 || depth < 1) {
+        set_error("server_create: invalid arguments");
+        return nullptr;
+    }
+    Server* s = new Server();
+    s->device = device;
+    s->budget = hbm_budget_bytes;
+    s->max_active = max_active;
+    s->depth = depth;
+    s->worker = std::thread([s] { s->run(); });
+    return s;
+}
+
+int petl_server_submit(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
+                       long long* id_out)
+{
+    clear_error();
+    Server* s = static_cast<Server*>(server);
+    std::string why;
+    PETL_REQUIRE(s && G && g_host && id_out && num_subsets >= 1 && num_iter >= 1 && geom_valid(G, &why),
+                 "server_submit: invalid arguments " + why);
+    PETL_REQUIRE(num_subsets <= G->N_v0, "server_submit: more subsets than views");
+    auto r = std::make_shared<Request>();
+    r->G = *G;
+    r->g_host = g_host;
+    r->subsets = num_subsets;
+    r->iters = num_iter;
+    r->bytes = footprint(*G, num_subsets);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        PETL_REQUIRE(double(r->bytes) <= s->budget, "server_submit: request larger than the HBM budget");
+        r->id = s->next_id++;
+        s->pending.push_back(r);
+        s->all[r->id] = r;
+        *id_out = r->id;
+    }
+    s->cv_work.notify_one();
+    return 0;
+}
+
+int petl_server_wait(void* server, long long id, float* f_host, double* latency_s, double* queue_s)
+{
+    clear_error();
+    Server* s = static_cast<Server*>(server);
+    PETL_REQUIRE(s, "server_wait: null server");
+    std::shared_ptr<Request> r;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->all.find(id);
+        PETL_REQUIRE(it != s->all.end(), "server_wait: unknown request");
+        r = it->second;
+        s->cv_done.wait(lk, [&] { return r->state == kDone || r->state == kFailed; });
+        s->all.erase(it);
+    }
+    const double lat = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+    const double q = r->state == kDone ? std::chrono::duration<double>(r->t_admit - r->t_submit).count() : lat;
+    if (latency_s) *latency_s = lat;
+    if (queue_s) *queue_s = q;
+    int rc = 0;
+    if (r->state == kDone) {
+        if (f_host) std::memcpy(f_host, r->out_host, sizeof(float) * size_t(r->G.numX) * r->G.numY * r->G.numZ);
+    } else {
+        set_error("server request failed: " + r->error);
+        rc = -1;
+    }
+    if (r->out_host) cudaFreeHost(r->out_host);
+    r->out_host = nullptr;
+    return rc;
+}
+
+// out[0..5] = completed, failed, active, pending, HBM bytes in use, peak HBM bytes reserved
+int petl_server_stats(void* server, double* out)
+{
+    Server* s = static_cast<Server*>(server);
+    if (!s || !out) return -1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    out[0] = double(s->completed);
+    out[1] = double(s->failed);
+    out[2] = double(s->active.size());
+    out[3] = double(s->pending.size());
+    out[4] = s->in_use;
+    out[5] = s->peak;
+    return 0;
+}
+
+void petl_server_destroy(void* server)
+{
+    Server* s = static_cast<Server*>(server);
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (auto& kv : s->all)
+        if (kv.second->out_host) cudaFreeHost(kv.second->out_host);
+    delete s;
+}
+
+}  // extern "C"

@@ -33,6 +33,15 @@ struct TableBuf {
 };
 
 int make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st);
+// Bytes of the shift tables of G (make_tables' allocation).
+size_t table_bytes(const petl_geom& G);
+
+// The fastest shear kernels that apply, with caller-held tables (TMA-staged,
+// else first generation).  The geometry must pass shear_eligible.
+int project_with(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                 const Tables& T, cudaStream_t st);
+int backproject_with(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                     const ViewRange& vr, const Tables& T, cudaStream_t st);
 
 // Return value of the TMA launchers when the geometry or the buffers do not
 // fit their layout rules; the caller then uses the first-generation kernels.
