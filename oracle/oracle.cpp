@@ -174,8 +174,9 @@ T project_ray(const oracle_geom& G, const T* f, int iv1, int iv0, int iu1, int i
     return val * (T(1) / std::sqrt(T(1) + v0 * v0 + v1 * v1));
 }
 
+// views iv0 = first, first + step, ...; the other views are set to zero
 template <class T>
-void project(const oracle_geom& G, const T* f, T* g, int nthreads)
+void project(const oracle_geom& G, const T* f, T* g, int nthreads, int first = 0, int step = 1)
 {
     set_threads(nthreads);
     const long nview = long(G.N_v1) * G.N_v0;
@@ -183,9 +184,10 @@ void project(const oracle_geom& G, const T* f, T* g, int nthreads)
     for (long v = 0; v < nview; v++) {
         const int iv1 = int(v / G.N_v0), iv0 = int(v % G.N_v0);
         T* gv = g + size_t(v) * G.N_u1 * G.N_u0;
+        const bool in = iv0 >= first && (iv0 - first) % step == 0;
         for (int iu1 = 0; iu1 < G.N_u1; iu1++)
             for (int iu0 = 0; iu0 < G.N_u0; iu0++)
-                gv[size_t(iu1) * G.N_u0 + iu0] = project_ray<T>(G, f, iv1, iv0, iu1, iu0, nullptr);
+                gv[size_t(iu1) * G.N_u0 + iu0] = in ? project_ray<T>(G, f, iv1, iv0, iu1, iu0, nullptr) : T(0);
     }
 }
 
@@ -216,8 +218,9 @@ inline void texaxis(float x, int mode, int& i, double& a)
     a = frac;
 }
 
+// only the views iv0 = first, first + step, ... contribute
 template <class T>
-void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthreads)
+void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthreads, int first = 0, int step = 1)
 {
     set_threads(nthreads);
     const T cos_psi = T(G.cos_psi), sin_psi = T(G.sin_psi);
@@ -255,7 +258,7 @@ void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthrea
                     const int iu1_max = int(std::floor(iu1_B + T(0.5)));
                     const T xdt_dy = T(0.5) * Tf_y * sin_psi, t_dy = T(0.5) * Tf_y * cos_psi;
                     const T xdt_dx = T(0.5) * Tf_x * cos_psi, t_dx = -T(0.5) * Tf_x * sin_psi;
-                    for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+                    for (int iv0 = first; iv0 < G.N_v0; iv0 += step) {
                         const T v0 = T(iv0) * Tg_x + sg_x;
                         const T width_y = v0 * cos_psi + sin_psi;
                         const T width_x = cos_psi - v0 * sin_psi;
@@ -480,6 +483,14 @@ void oracle_set_volume(oracle_geom* G, int numX, int numY, int numZ, float voxel
 }
 
 void oracle_project_f64(const oracle_geom* G, const double* f, double* g, int n) { project<double>(*G, f, g, n); }
+void oracle_project_sub_f64(const oracle_geom* G, const double* f, double* g, int first, int step, int n)
+{
+    project<double>(*G, f, g, n, first, step);
+}
+void oracle_backproject_sub_f64(const oracle_geom* G, const double* g, double* f, int first, int step, int n)
+{
+    backproject<double>(*G, g, f, 0, n, first, step);
+}
 void oracle_project_f32(const oracle_geom* G, const float* f, float* g, int n) { project<float>(*G, f, g, n); }
 void oracle_backproject_f64(const oracle_geom* G, const double* g, double* f, int tm, int n) { backproject<double>(*G, g, f, tm, n); }
 void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int tm, int n) { backproject<float>(*G, g, f, tm, n); }

@@ -59,6 +59,9 @@ void oracle_project_f32(const oracle_geom* G, const float* f, float* g, int nthr
  * carry 8 fractional bits (texmode 1: round to nearest, 2: truncate).
  * g -> f (overwrites f). */
 void oracle_backproject_f64(const oracle_geom* G, const double* g, double* f, int texmode, int nthreads);
+/* the views iv0 = first + k*step only (ordered subsets); exact weights */
+void oracle_project_sub_f64(const oracle_geom* G, const double* f, double* g, int first, int step, int nthreads);
+void oracle_backproject_sub_f64(const oracle_geom* G, const double* g, double* f, int first, int step, int nthreads);
 void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int texmode, int nthreads);
 
 /* Count of (ray, voxel) pairs with a nonzero footprint weight in the forward

@@ -64,6 +64,8 @@ def lib():
         L.oracle_project_f64.argtypes = [gp, dp, dp, ctypes.c_int]
         L.oracle_project_f32.argtypes = [gp, fp, fp, ctypes.c_int]
         L.oracle_backproject_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int]
+        L.oracle_project_sub_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_backproject_sub_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_backproject_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int]
         L.oracle_project_nnz.argtypes = [gp, ctypes.c_int]
         L.oracle_project_nnz.restype = ctypes.c_double
@@ -363,24 +365,37 @@ def osem(geoms, g, num_iter, num_subsets, f=None, nthreads=0):
         geoms, g = [geoms], [g]
     vol = geoms[0].vol_shape
     f = np.ones(vol, np.float64) if (f is None or not np.any(f)) else np.maximum(_d(f), 0.0)
-    masks = []
-    for s in range(num_subsets):
-        ms = []
+
+    def proj_sub(s):
+        out = []
         for G in geoms:
-            m = np.zeros(G.shape)
-            m[:, s::num_subsets] = 1.0
-            ms.append(m)
-        masks.append(ms)
+            p = np.zeros(G.shape, np.float64)
+            fc = _d(f)
+            lib().oracle_project_sub_f64(ctypes.byref(G), _ptr(fc, ctypes.c_double), _ptr(p, ctypes.c_double), s,
+                                         num_subsets, nthreads)
+            out.append(p)
+        return out
+
+    def back_sub(gl, s):
+        acc = np.zeros(vol, np.float64)
+        for G, gi in zip(geoms, gl):
+            gc = _d(gi)
+            fi = np.zeros(vol, np.float64)
+            lib().oracle_backproject_sub_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(fi, ctypes.c_double), s,
+                                             num_subsets, nthreads)
+            acc += fi
+        return acc
+
     sens = []
     for s in range(num_subsets):
-        ss = backproject(geoms, masks[s], nthreads=nthreads)
+        ss = back_sub([np.ones(G.shape) for G in geoms], s)
         ss[ss == 0.0] = 1.0
         sens.append(ss)
     for _ in range(num_iter):
         for s in range(num_subsets):
-            Pd = project(geoms, f, nthreads=nthreads)
-            ratio = [_rdivide(p, gi) * m for p, gi, m in zip(Pd, g, masks[s])]
-            d = backproject(geoms, ratio, nthreads=nthreads)
+            Pd = proj_sub(s)
+            ratio = [_rdivide(p, gi) for p, gi in zip(Pd, g)]
+            d = back_sub(ratio, s)
             f = f * _divide(d, sens[s])
     return f
 

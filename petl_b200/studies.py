@@ -1,0 +1,256 @@
+"""Reconstruction workloads beyond the fwd+back headline, one JSON line each.
+
+    python -m petl_b200.studies pipeline    # 256x256x128: PFDR, FBP, 8-subset OSEM x 4
+    python -m petl_b200.studies penalized   # 4 x 128x128x64, NLL + RD + TV, 50 steps, FD check
+    python -m petl_b200.studies storage     # 256x256x128 OSEM 10 x 8 subsets, FP32 vs BF16 storage
+    python -m petl_b200.studies serving     # 200 Poisson-arrival OSEM requests, p50/p99
+
+All inputs are synthetic and seeded: ellipsoid phantoms (replace semantics,
+later ellipsoids overwrite earlier ones), forward projected with the
+library's projector and Poisson sampled on the GPU.  Times are CUDA-event
+times on the device except the serving latencies, which are host
+wall-clock from submission to the result on the host.  Accuracy against
+the FP64 oracle is established by the test suite (tests/), not here.
+"""
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import ops, recon
+from .geometry import Geometry
+
+
+def phantom(shape, pitch, rng, n, axes=(5.0, 40.0), vmin=0.1, vmax=1.0, background=0.0, device="cuda"):
+    """Seeded ellipsoids in a [z, y, x] volume of voxel pitch (wx, wz) mm."""
+    nz, ny, nx = shape
+    wx, wz = pitch
+    x = (torch.arange(nx, device=device) - 0.5 * (nx - 1)) * wx
+    y = (torch.arange(ny, device=device) - 0.5 * (ny - 1)) * wx
+    z = (torch.arange(nz, device=device) - 0.5 * (nz - 1)) * wz
+    f = torch.full(shape, float(background), device=device)
+    ext = np.array([nx * wx, ny * wx, nz * wz]) * 0.5
+    for _ in range(n):
+        r = np.minimum(rng.uniform(axes[0], axes[1], 3), ext * 0.95)
+        c = rng.uniform(-1, 1, 3) * np.maximum(ext - r, 0)
+        val = float(rng.uniform(vmin, vmax))
+        inside = (((x - c[0]) / r[0]) ** 2)[None, None, :] + (((y - c[1]) / r[1]) ** 2)[None, :, None] + \
+            (((z - c[2]) / r[2]) ** 2)[:, None, None] <= 1.0
+        f[inside] = val
+    return f
+
+
+def poisson_data(G, f, counts, seed, return_scale=False):
+    y = ops.project(G, f)
+    scale = counts / float(y.sum())
+    y.mul_(scale)
+    y = torch.poisson(y, generator=torch.Generator(device=y.device).manual_seed(seed))
+    return (y, scale) if return_scale else y
+
+
+def _rel(img, ref, scale=1.0):
+    """relative L2 of img / scale against ref (images live on the counts scale)"""
+    return float((img / scale - ref).norm() / ref.norm())
+
+
+class Timer:
+    def __init__(self):
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+
+    def __enter__(self):
+        torch.cuda.synchronize()
+        self.a.record()
+        return self
+
+    def __exit__(self, *exc):
+        self.b.record()
+        torch.cuda.synchronize()
+        self.ms = self.a.elapsed_time(self.b)
+
+
+CFG1 = dict(args=(0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25), volume=(256, 256, 128, 1.0))
+CFG0 = dict(args=(0.0, 256.0, 128.0, 64.0, 2.0, 0.5, 0.25), volume=(128, 128, 64, 2.0))
+
+
+def study_pipeline(seed=0):
+    G = Geometry(*CFG1["args"], volume=CFG1["volume"])
+    rng = np.random.default_rng(seed)
+    f = phantom(G.vol_shape, (1.0, 1.0), rng, 30)
+    f += 0.01 * float(f.max())
+    y, scale = poisson_data(G, f, 5e7, seed, return_scale=True)
+    out = {"study": "pipeline", "workload": "vol 256x256x128 @1mm, planogram (65,129,128,256), 5e7 counts",
+           "geometry": "add_planogram(0, 256, 128, 128, T=1, 0.5, 0.25)"}
+    for _ in range(2):  # warm-up of every stage
+        ops.pfdr(G, y)
+        ops.fbp(G, y)
+    with Timer() as t:
+        reb = ops.pfdr(G, y)
+    out["pfdr_ms"] = t.ms
+    with Timer() as t:
+        img = ops.fbp(G, y)
+    out["fbp_ms"] = t.ms
+    sens = [recon.sensitivity(G, [y], subset=(s, 8)) for s in range(8)]
+    with Timer() as t:
+        fo, _ = recon.osem(G, y, 4, 8, sens=sens)
+    out["osem_4x8_ms"] = t.ms
+    out["osem_ms_per_iteration"] = t.ms / 4
+    # images are on the counts scale: divide by the data scale before comparing
+    out["osem_image_rel_l2_vs_phantom"] = _rel(fo, f, scale)
+    out["fbp_image_rel_l2_vs_phantom"] = _rel(img, f, scale)
+    out["rebinned_shape"] = list(reb.shape)
+    return out
+
+
+def study_penalized(seed=0, steps=50, fd_voxels=64):
+    from . import penalized
+    G = Geometry(*CFG0["args"], volume=CFG0["volume"])
+    rng = np.random.default_rng(seed)
+    vols, data = [], []
+    for b in range(4):
+        f = phantom(G.vol_shape, (2.0, 2.0), np.random.default_rng(seed + b), 12)
+        vols.append(f)
+        data.append(poisson_data(G, f, 1e6, seed + b))
+    yb = torch.stack(data)
+    rd = (2.0, 0.01)                 # gamma, beta (26 neighbours)
+    tv = (1e-4, 0.01, 1.0, 26)       # delta = 1e-4 (eps), beta_tv = 0.01 (chosen), p = 1
+    penalized.reconstruct(G, yb, iters=2, rd=rd, tv=tv)  # warm-up
+    with Timer() as t:
+        fr, hist = penalized.reconstruct(G, yb, iters=steps, rd=rd, tv=tv)
+    f0 = fr[0].contiguous()
+    cand = torch.nonzero(f0.reshape(-1) > 0.05 * float(f0.max())).reshape(-1).cpu().numpy()
+    vox = rng.choice(cand, fd_voxels, replace=False)
+    got, fd = penalized.fd_check(f0, G, yb[0], vox, h=1e-3, rd=rd, tv=tv)
+    got = got.cpu().numpy()
+    fd = fd.numpy()
+    rel = np.abs(got - fd) / np.maximum(np.abs(fd), 1e-12)
+    h = hist.numpy()
+    return {"study": "penalized", "workload": "4 x vol 128x128x64 @2mm, planogram (33,65,64,128), 1e6 counts each",
+            "objective": "Poisson NLL + RD(gamma=2, beta=0.01, 26-nbr) + TV(delta=1e-4, p=1, beta=0.01, 26-nbr)",
+            "steps": steps, "total_ms": t.ms, "ms_per_step_batch4": t.ms / steps,
+            "objective_first": h[0].tolist(), "objective_last": h[-1].tolist(),
+            "monotone_fraction": float((np.diff(h, axis=0) <= 0).mean()),
+            "fd_voxels": fd_voxels, "fd_h": 1e-3, "fd_rel_err_median": float(np.median(rel)),
+            "fd_rel_err_max": float(rel.max())}
+
+
+def study_storage(seed=0, iters=10, subsets=8):
+    G = Geometry(*CFG1["args"], volume=CFG1["volume"])
+    rng = np.random.default_rng(seed)
+    f = phantom(G.vol_shape, (1.0, 1.0), rng, 30)
+    f += 0.01 * float(f.max())
+    y = poisson_data(G, f, 5e7, seed)
+    y16 = y.to(torch.bfloat16)
+    sens = [recon.sensitivity(G, [y], subset=(s, subsets)) for s in range(subsets)]
+    recon.osem(G, y, 1, subsets, sens=sens)
+    with Timer() as t32:
+        f32, _ = recon.osem(G, y, iters, subsets, sens=sens)
+    recon.osem_bf16(G, y16, 1, subsets, sens=sens)
+    with Timer() as t16:
+        f16 = recon.osem_bf16(G, y16, iters, subsets, sens=sens)
+    ng, nv = y.numel(), f.numel()
+    # per subset step: read meas + write ratio (forward), read ratio (backward),
+    # volume traffic: read f (forward), write d, read f, d, sens, write f (update)
+    sub = ng / subsets
+    def traffic(eb):
+        return iters * subsets * (3 * sub * eb + nv * 4 * 4 + nv * eb * 2)
+    p32 = ops.project(G, f32)
+    p16 = ops.project(G, f16.float())
+    return {"study": "storage", "workload": "vol 256x256x128 @1mm, planogram (65,129,128,256), 5e7 counts, "
+            f"OSEM {iters} it x {subsets} subsets",
+            "fp32_ms": t32.ms, "bf16_ms": t16.ms,
+            "fp32_bytes": traffic(4), "bf16_bytes": traffic(2),
+            "fp32_GBps": traffic(4) / (t32.ms * 1e6), "bf16_GBps": traffic(2) / (t16.ms * 1e6),
+            "image_rel_l2_bf16_vs_fp32": float((f16.float() - f32).norm() / f32.norm()),
+            "image_max_abs_bf16_vs_fp32": float((f16.float() - f32).abs().max()),
+            "proj_rel_l2_bf16_vs_fp32": float((p16 - p32).norm() / p32.norm())}
+
+
+def _serving_requests(n, rate, seed, device):
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    reqs = []
+    for i in range(n):
+        N = int(rng.choice([64, 128, 192, 256]))
+        T = float(rng.choice([1.0, 1.5, 2.0]))
+        D = float(rng.choice([200.0, 250.0, 300.0]))
+        counts = float(math.exp(rng.uniform(math.log(1e5), math.log(5e7))))
+        S = int(rng.choice([4, 8]))
+        it = int(rng.integers(2, 7))
+        reqs.append(dict(t=float(t[i]), N=N, T=T, D=D, counts=counts, S=S, it=it))
+    return reqs
+
+
+def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0):
+    from .serving import ReconServer
+    reqs = _serving_requests(n, rate, seed, "cuda")
+    # one data set per geometry class (the work of a request does not depend
+    # on its counts, so requests of a class share one Poisson realisation at
+    # the class's first drawn counts)
+    classes = {}
+    for r in reqs:
+        key = (r["N"], r["T"], r["D"])
+        if key not in classes:
+            N, T, D = key
+            G = Geometry(0.0, D, N * T / 2, N * T / 2, T, 0.5, 0.25, volume=(N, N, N // 2, T))
+            f = phantom(G.vol_shape, (T, T), np.random.default_rng(hash(key) % 2**31), 8)
+            y = poisson_data(G, f, r["counts"], 1)
+            host = torch.empty(y.shape, dtype=torch.float32, pin_memory=True)
+            host.copy_(y.cpu())
+            classes[key] = (G, host)
+            del y, f
+    torch.cuda.synchronize()
+
+    def serve(active):
+        with ReconServer(hbm_budget_gb=budget_gb, max_active=active, depth=2) as srv:
+            # warm-up: one request per class
+            for key, (G, host) in classes.items():
+                srv.wait(srv.submit(G, host, 4, 1))
+            t0 = time.perf_counter()
+            ids = []
+            for r in reqs:
+                now = time.perf_counter() - t0
+                if r["t"] > now:
+                    time.sleep(r["t"] - now)
+                G, host = classes[(r["N"], r["T"], r["D"])]
+                ids.append(srv.submit(G, host, r["S"], r["it"]))
+            lat, queue = [], []
+            for i in ids:
+                _, l, q = srv.wait(i)
+                lat.append(l)
+                queue.append(q)
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        lat = np.array(lat)
+        return {"recons_per_s": n / wall, "wall_s": wall, "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mean_queue_s": float(np.mean(queue)),
+                "hbm_peak_gb": st["hbm_peak_bytes"] / 1e9, "failed": st["failed"]}
+
+    batched = serve(max_active)
+    single = serve(1)
+    return {"study": "serving", "workload": f"{n} OSEM requests, Poisson arrivals {rate}/s (seed {seed}), "
+            "N in {64,128,192,256} (vol NxNxN/2 at pitch T in {1,1.5,2} mm), L=H=N*T/2, D in {200,250,300} mm, "
+            "4 or 8 subsets, 2-6 iterations", "geometry_classes": len(classes), "budget_gb": budget_gb,
+            "continuous_batching": batched, "one_at_a_time": single,
+            "throughput_ratio": batched["recons_per_s"] / single["recons_per_s"]}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--requests", type=int, default=200)
+    a = ap.parse_args(argv)
+    fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage}
+    if a.study == "serving":
+        res = study_serving(n=a.requests, seed=a.seed)
+    else:
+        res = fn[a.study](seed=a.seed)
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
