@@ -154,6 +154,8 @@ int petl_project_ratio_bf16_dev(const petl_geom* G, const void* f, const void* m
 /* f (float32) = accumulate ? f + scale*P^T g : scale*P^T g with g in bfloat16 */
 int petl_backproject_bf16_dev(const petl_geom* G, const void* g, float* f, int mode, int accumulate, float scale,
                               int iv1_begin, int iv1_end, int iv0_first, int iv0_step, void* stream);
+/* y (bfloat16) = x rounded to nearest even */
+int petl_to_bf16_dev(const float* x, void* y, long long n, void* stream);
 /* f (bfloat16) *= d / sens with the DIV rule (d/0 -> 0) */
 int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long long n, void* stream);
 

@@ -87,6 +87,7 @@ _DEV_API = [
     ("petl_project_ratio_bf16_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_backproject_bf16_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_mlem_update_bf16_dev", c_i, [c_vp, c_vp, c_vp, c_ll, c_vp]),
+    ("petl_to_bf16_dev", c_i, [c_vp, c_vp, c_ll, c_vp]),
     ("petl_server_create", c_vp, [c_d, c_i, c_i, c_i]),
     ("petl_server_submit", c_i, [c_vp, _G, c_vp, c_i, c_i, ctypes.POINTER(c_ll)]),
     ("petl_server_wait", c_i, [c_vp, c_ll, c_vp, ctypes.POINTER(c_d), ctypes.POINTER(c_d)]),

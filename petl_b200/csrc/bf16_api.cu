@@ -57,6 +57,13 @@ __global__ void k_mlem_update_bf16(bf16* __restrict__ f, const float* __restrict
     }
 }
 
+__global__ void k_to_bf16(const float* __restrict__ x, bf16* __restrict__ y, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        y[i] = __float2bfloat16_rn(x[i]);
+}
+
 }  // namespace
 }  // namespace petl
 
@@ -106,6 +113,17 @@ int petl_backproject_bf16_dev(const petl_geom* G, const void* g, float* f, int m
     if (rc) return rc;
     rc = shear::backproject_tma_bf16(*G, static_cast<const bf16*>(g), f, mode, accumulate, scale, vr, tb.T, st);
     return bf16_result(rc, "backproject_bf16", tb, st);
+}
+
+int petl_to_bf16_dev(const float* x, void* y, long long n, void* stream)
+{
+    clear_error();
+    PETL_REQUIRE(x && y && n >= 0, "to_bf16: invalid arguments");
+    if (n == 0) return 0;
+    const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_to_bf16<<<unsigned(blocks), 256, 0, as_stream(stream)>>>(x, static_cast<bf16*>(y), n);
+    PETL_LAUNCH_CHECK("to_bf16");
+    return 0;
 }
 
 int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long long n, void* stream)

@@ -141,6 +141,14 @@ def backproject_bf16(geom, g, f=None, mode="reference", accumulate=False, scale=
     return f
 
 
+def to_bf16(x, out=None):
+    """bfloat16 copy of a float32 tensor (round to nearest even)."""
+    if out is None:
+        out = torch.empty(x.shape, device=x.device, dtype=torch.bfloat16)
+    check(lib().petl_to_bf16_dev(_dev(x, "x"), _dev16(out, "out"), _n(x), _stream()), "to_bf16")
+    return out
+
+
 def mlem_update_bf16_(f, d, sens):
     """f (bfloat16) *= d / sens with d/0 -> 0."""
     check(lib().petl_mlem_update_bf16_dev(_dev16(f, "f"), _dev(d, "d"), _dev(sens, "sens"), _n(f), _stream()),
@@ -311,4 +319,4 @@ def osl_update_(f, d, sens, Df):
 __all__ = ["Geometry", "project", "project_ratio", "backproject", "nnz", "pfdr", "ramp_", "fbp", "rd_gradient", "rd_cost",
            "tv_gradient", "tv_cost", "tv_quadform", "gaussian_filter_", "rdivide_", "divide_", "multiply_",
            "reciprocal_", "axpby_", "dot", "loglik", "poisson_grad_", "mlem_update_", "osl_update_", "project_bf16",
-           "project_ratio_bf16", "backproject_bf16", "mlem_update_bf16_", "REFERENCE", "ADJOINT"]
+           "project_ratio_bf16", "backproject_bf16", "mlem_update_bf16_", "to_bf16", "REFERENCE", "ADJOINT"]

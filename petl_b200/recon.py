@@ -84,19 +84,21 @@ def osem(geoms, g, num_iter, num_subsets, f=None, delta=2.0, beta=0.0, sens=None
     return f, history
 
 
-def osem_bf16(geom, g, num_iter, num_subsets, f=None, sens=None):
-    """OSEM with the volume, the measured planogram and the data ratio stored
-    in bfloat16 (half the HBM bytes of the planogram-sized arrays); the
-    footprints accumulate in FP32, the backprojection and the sensitivity
-    images are FP32, the update rounds the image to bfloat16 once per
-    subset.  One axis-aligned, equal-pitch geometry (the TMA path).
-    Returns the bfloat16 image."""
+def osem_bf16(geom, g, num_iter, num_subsets, f=None, sens=None, image="fp32"):
+    """OSEM with the planogram-sized arrays (measured data and data ratio) and
+    the projector's volume input stored in bfloat16, footprints accumulated
+    in FP32.  With image="fp32" (default) the image itself is kept in FP32
+    and rounded to a bfloat16 copy for each forward projection, so bfloat16
+    rounding never compounds through the multiplicative updates; with
+    image="bf16" the image is stored and updated in bfloat16 as well.  One
+    axis-aligned, equal-pitch geometry (the TMA path).  Returns the image
+    (float32 or bfloat16)."""
     S = int(num_subsets)
     device = g.device
     if g.dtype != torch.bfloat16:
         raise ValueError("osem_bf16 expects bfloat16 data")
-    if f is None:
-        f = torch.ones(geom.vol_shape, device=device, dtype=torch.bfloat16)
+    if image not in ("fp32", "bf16"):
+        raise ValueError("image must be 'fp32' or 'bf16'")
     if sens is None:
         ones = torch.ones(geom.shape, device=device, dtype=torch.bfloat16)
         sens = []
@@ -106,11 +108,24 @@ def osem_bf16(geom, g, num_iter, num_subsets, f=None, sens=None):
             sens.append(x)
     ratio = torch.empty_like(g)
     d = torch.empty(geom.vol_shape, device=device, dtype=torch.float32)
+    if image == "bf16":
+        if f is None:
+            f = torch.ones(geom.vol_shape, device=device, dtype=torch.bfloat16)
+        for _ in range(num_iter):
+            for s in range(S):
+                ops.project_ratio_bf16(geom, f, g, out=ratio, subset=(s, S))
+                ops.backproject_bf16(geom, ratio, f=d, subset=(s, S))
+                ops.mlem_update_bf16_(f, d, sens[s])
+        return f
+    if f is None:
+        f = torch.ones(geom.vol_shape, device=device, dtype=torch.float32)
+    f16 = torch.empty(geom.vol_shape, device=device, dtype=torch.bfloat16)
     for _ in range(num_iter):
         for s in range(S):
-            ops.project_ratio_bf16(geom, f, g, out=ratio, subset=(s, S))
+            ops.to_bf16(f, out=f16)
+            ops.project_ratio_bf16(geom, f16, g, out=ratio, subset=(s, S))
             ops.backproject_bf16(geom, ratio, f=d, subset=(s, S))
-            ops.mlem_update_bf16_(f, d, sens[s])
+            ops.mlem_update_(f, d, sens[s])
     return f
 
 

@@ -7,7 +7,8 @@
    to bfloat16, planogram written in bfloat16, FP32 accumulation in both)
    against the FP64 oracle projection of the same (FP32) phantom.
 2. Images at 128x128x64 (planogram (33,65,64,128)): OSEM, 10 iterations x 8
-   subsets, with FP32 storage and with BF16 storage on the GPU against the
+   subsets, with FP32 storage, with BF16 planograms and projector input (FP32
+   image), and with the image stored in BF16 too, on the GPU against the
    same OSEM run by the FP64 oracle, all from one Poisson data set.  The full
    256x256x128 FP64 OSEM would take tens of CPU minutes; the smaller geometry
    has the same slopes and pitch ratio.
@@ -71,9 +72,11 @@ def main():
     out["oracle_osem_s"] = time.time() - t0
     yt = torch.from_numpy(y).to(dev)
     f32, _ = recon.osem(G, yt, 10, 8)
-    f16 = recon.osem_bf16(G, yt.to(torch.bfloat16), 10, 8)
+    f16 = recon.osem_bf16(G, yt.to(torch.bfloat16), 10, 8)                  # FP32 image, BF16 planograms/projector input
+    f16b = recon.osem_bf16(G, yt.to(torch.bfloat16), 10, 8, image="bf16")   # image stored in BF16 too
     out["image_fp32_rel_l2"], out["image_fp32_max_abs"] = rel(f32.cpu().numpy(), f64)
     out["image_bf16_rel_l2"], out["image_bf16_max_abs"] = rel(f16.float().cpu().numpy(), f64)
+    out["image_bf16img_rel_l2"], out["image_bf16img_max_abs"] = rel(f16b.float().cpu().numpy(), f64)
     out["image_scale_max"] = float(np.abs(f64).max())
     print(json.dumps(out))
 

@@ -75,10 +75,14 @@ def test_bf16_osem_tracks_fp32(cuda):
     g = ops.project(G, f16.float())
     meas = torch.poisson(g * (2e6 / float(g.sum())), generator=torch.Generator(device=cuda).manual_seed(5))
     f32, _ = recon.osem(G, meas, 2, 4)
+    # FP32 image, bfloat16 planograms and projector input
     fb = recon.osem_bf16(G, meas.to(torch.bfloat16), 2, 4)
-    # counts above 256 are not exact in bfloat16; the image stays within a
-    # few bfloat16 ulps of the FP32 reconstruction
-    assert rel_l2(fb.float().cpu().numpy(), f32.cpu().numpy()) < 2e-2
+    assert fb.dtype == torch.float32
+    assert rel_l2(fb.cpu().numpy(), f32.cpu().numpy()) < 2e-3
+    # image stored in bfloat16 as well: within a few bfloat16 ulps
+    fbb = recon.osem_bf16(G, meas.to(torch.bfloat16), 2, 4, image="bf16")
+    assert fbb.dtype == torch.bfloat16
+    assert rel_l2(fbb.float().cpu().numpy(), f32.cpu().numpy()) < 2e-2
 
 
 def test_bf16_refuses_non_shear_geometry(cuda):
