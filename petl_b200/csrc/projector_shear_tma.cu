@@ -502,6 +502,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     uint64_t* full = reinterpret_cast<uint64_t*>(s_pat + BV1CAP);         // [ns]
     uint64_t* empty = full + BNSMAX;                                      // [ns]
     int* s_n = reinterpret_cast<int*>(empty + BNSMAX);
+    int* s_round = s_n + 2;                                               // [ns]
 
     // ---- per-CTA slope tables (warp 0): for every slope whose rows reach the
     // tile, the staged g row, per plane the window offset and mode (0 none,
@@ -636,6 +637,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
             for (int s = 0; s < ns; s++) {
                 mbar_init(&full[s], 1);
                 mbar_init(&empty[s], nwarps);
+                s_round[s] = -1;
             }
             fence_barrier_init();
         }
@@ -655,40 +657,30 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
         }
     };
     const uint32_t box_bytes = uint32_t(NU0) * uint32_t(A.brb) * uint32_t(sizeof(TG));
-    // producer state (thread 0): stages issued, and the next stage's ring
-    // slot, slope index, view and ring round
-    long long issued = 0;
-    int p_slot = 0, p_li = 0, p_v0 = A.vr.iv0_first, p_round = 0;
+    // Stage j is started by lane 0 of warp j % nwarps once every warp has
+    // released its ring slot (the consumption of stage j - ns): the producer
+    // work and its waits rotate over the warps instead of slowing one warp,
+    // which would hold every other warp back through the empty barriers.
+    // s_round[slot] records the round of the copy last started in a slot (for
+    // draining after a failed wait).
     bool dead = false;
-    // Start the copy of the next stage into its ring slot once every warp has
-    // released the slot (the consumption of the stage ns earlier).  Without
-    // `block` it only tests once, so thread 0 does not stall its warp on slow
-    // warps while the ring still holds stages ahead.
-    auto issue = [&](bool block) {
-        if (p_round > 0) {
-            const uint32_t par = uint32_t((p_round - 1) & 1);
-            if (block) {
-                if (!mbar_wait(&empty[p_slot], par, A.err)) return -1;
-            } else if (!mbar_test_wait(&empty[p_slot], par)) {
-                return 0;
-            }
-        }
+    const int ntot = int(total);
+    auto issue = [&](int j) {
+        const int slot = j % ns, round = j / ns;
+        const int li = j % nlive;
+        const int v0 = A.vr.iv0_first + (j / nlive) * A.vr.iv0_step;
+        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err)) return false;
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&full[p_slot], box_bytes);
-        tma_load_4d(ring(p_slot), &gmap, &full[p_slot], 0, s_grow[p_li], p_v0, s_v1[p_li]);
-        if (++p_slot == ns) {
-            p_slot = 0;
-            p_round++;
-        }
-        if (++p_li == nlive) {
-            p_li = 0;
-            p_v0 += A.vr.iv0_step;
-        }
-        issued++;
-        return 1;
+        mbar_arrive_expect_tx(&full[slot], box_bytes);
+        tma_load_4d(ring(slot), &gmap, &full[slot], 0, s_grow[li], v0, s_v1[li]);
+        s_round[slot] = round;
+        return true;
     };
     if (tid == 0)
-        while (issued < ns && issued < total) issue(true);
+        for (int j = 0; j < ns - 1 && j < ntot; j++) issue(j);
+    // the next stage this warp starts: the first j >= ns - 1 with j % nwarps == warp
+    int my_next = warp + nwarps * ((ns - 1 - warp + nwarps - 1) / nwarps);
+    if (my_next < ns - 1) my_next += nwarps;
     if (n_v0 > 0) weights(A.vr.iv0_first);
     __syncthreads();
 
@@ -710,13 +702,9 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     for (int iv = 0; iv < n_v0 && !aborted; iv++) {
         const int v0 = A.vr.iv0_first + iv * A.vr.iv0_step;
         for (int li = 0; li < nlive; li++, it++) {
-            if (tid == 0 && !dead) {
-                // keep the ring full; block only when this stage itself is not issued yet
-                while (issued < total && issued < it + ns) {
-                    const int r = issue(issued <= it);
-                    if (r < 0) dead = true;
-                    if (r <= 0) break;
-                }
+            if (it + ns - 1 == my_next) {
+                if (lane == 0 && !dead && my_next < ntot && !issue(my_next)) dead = true;
+                my_next += nwarps;
             }
             const int s = c_slot;
             if (!dead) dead = !mbar_wait(&full[s], c_phase, A.err);
@@ -818,9 +806,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     }
     if (aborted) {
         // a wait gave up: drain the copies still in flight, write nothing
+        __syncthreads();
         if (tid == 0)
-            for (long long j = std::max(0LL, issued - ns); j < issued; j++)
-                mbar_wait(&full[j % ns], uint32_t((j / ns) & 1), nullptr);
+            for (int slot = 0; slot < ns; slot++)
+                if (s_round[slot] >= 0) mbar_wait(&full[slot], uint32_t(s_round[slot] & 1), nullptr);
         return;
     }
 
@@ -944,7 +933,7 @@ int backproject_tma_t(const petl_geom& G, const TG* g, TF* f, int mode, int accu
     // as many ring stages as fit (copies from DRAM need several in flight)
     const size_t fixed = size_t(BNP) * BK * NU0 * 4 + size_t(BV1CAP) * BNP * 8 + size_t(BV1CAP) * BNP * 4 +
                          size_t(BV1CAP) * 4 * 4 + size_t(BV1CAP) * BPG * 4 + size_t(BV1CAP) * 4 + 2 * BNSMAX * 8 +
-                         16;
+                         8 + BNSMAX * 4 + 16;
     A.ns = int(std::min<size_t>(BNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / size_t(A.sstride)));
     if (A.ns < 2) return kNotApplicable;
     const size_t smem = size_t(A.ns) * A.sstride + fixed;
