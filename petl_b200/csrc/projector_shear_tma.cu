@@ -425,6 +425,7 @@ struct BwdTmaArgs {
     int brb;      // staged rows per view (>= BWN + CTA shift spread, bounded on the host)
     int sstride;  // bytes per ring stage
     int ns;       // ring stages
+    int max_views;  // views the x-shift table holds
     int accumulate;
     float scale;
     Tables T;
@@ -493,7 +494,8 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     float* Zs = reinterpret_cast<float*>(smem + size_t(ns) * A.sstride);  // [BNP][BK][NU0]
     float2* Wt = reinterpret_cast<float2*>(Zs + BNP * BK * NU0);          // [BV1CAP][BNP]
     float* s_w = reinterpret_cast<float*>(Wt + BV1CAP * BNP);             // [BV1CAP][BNP]
-    int* s_v1 = reinterpret_cast<int*>(s_w + BV1CAP * BNP);               // [BV1CAP]
+    Shift* s_xs = reinterpret_cast<Shift*>(s_w + BV1CAP * BNP);           // [n_v0][BNP] x shifts of the planes
+    int* s_v1 = reinterpret_cast<int*>(s_xs + A.max_views * BNP);         // [BV1CAP]
     int* s_grow = s_v1 + BV1CAP;                                          // [BV1CAP]
     uint32_t* s_code = reinterpret_cast<uint32_t*>(s_grow + BV1CAP);      // [BV1CAP]
     uint32_t* s_wb = s_code + BV1CAP;                                     // [BV1CAP]
@@ -646,16 +648,35 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     const int nlive = s_n[0];
     const long long total = (long long)n_v0 * nlive;
 
-    // weights of view v0: (S w0, S w1) per live slope and plane
-    auto weights = [&](int v0) {
-        for (int e = tid; e < nlive * BNP; e += blockDim.x) {
-            const int li = e / BNP;
-            const float S = A.T.S[size_t(s_v1[li]) * G.N_v0 + v0];
-            const float w = s_w[e];
-            const float w1 = S * w, w0 = S * (1.0f - w);
-            Wt[e] = make_float2(w0, w1);
+    // weights of view v0: (S w0, S w1) per live slope and plane.  The global
+    // loads of S for the next view are issued at the start of a view
+    // (load_S) and stored after its stages (store_w), so their latency hides
+    // behind the view's work; at most kWPT elements per thread.
+    constexpr int kWPT = (BV1CAP * BNP + 511) / 512;
+    float s_pre[kWPT];
+    auto load_S = [&](int v0) {
+#pragma unroll
+        for (int i = 0; i < kWPT; i++) {
+            const int e = tid + i * int(blockDim.x);
+            s_pre[i] = e < nlive * BNP ? __ldg(&A.T.S[size_t(s_v1[e / BNP]) * G.N_v0 + v0]) : 0.0f;
         }
     };
+    auto store_w = [&]() {
+#pragma unroll
+        for (int i = 0; i < kWPT; i++) {
+            const int e = tid + i * int(blockDim.x);
+            if (e < nlive * BNP) {
+                const float S = s_pre[i], w = s_w[e];
+                Wt[e] = make_float2(S * (1.0f - w), S * w);
+            }
+        }
+    };
+    // x shifts of the CTA's planes for every view, staged once
+    for (int e = tid; e < n_v0 * BNP; e += blockDim.x) {
+        const int iv = e / BNP, p = e % BNP;
+        const int y = min(p0 + p, NY - 1);
+        s_xs[e] = A.T.xt[size_t(A.vr.iv0_first + iv * A.vr.iv0_step) * NY + y];
+    }
     const uint32_t box_bytes = uint32_t(NU0) * uint32_t(A.brb) * uint32_t(sizeof(TG));
     // Stage j is started by lane 0 of warp j % nwarps once every warp has
     // released its ring slot (the consumption of stage j - ns): the producer
@@ -681,7 +702,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     // the next stage this warp starts: the first j >= ns - 1 with j % nwarps == warp
     int my_next = warp + nwarps * ((ns - 1 - warp + nwarps - 1) / nwarps);
     if (my_next < ns - 1) my_next += nwarps;
-    if (n_v0 > 0) weights(A.vr.iv0_first);
+    if (n_v0 > 0) {
+        load_S(A.vr.iv0_first);
+        store_w();
+    }
     __syncthreads();
 
     float Fv[BPT][BK];  // voxel accumulators (unscaled)
@@ -701,6 +725,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     uint32_t c_phase = 0;   // parity of that slot's current use
     for (int iv = 0; iv < n_v0 && !aborted; iv++) {
         const int v0 = A.vr.iv0_first + iv * A.vr.iv0_step;
+        if (iv + 1 < n_v0) load_S(v0 + A.vr.iv0_step);
         for (int li = 0; li < nlive; li++, it++) {
             if (it + ns - 1 == my_next) {
                 if (lane == 0 && !dead && my_next < ntot && !issue(my_next)) dead = true;
@@ -790,7 +815,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
         for (int q = 0; q < BPT; q++) {
             const int y = p0 + pg * BPT + q;
             if (y >= NY) continue;
-            const Shift xs = A.T.xt[size_t(v0) * NY + y];
+            const Shift xs = s_xs[iv * BNP + pg * BPT + q];
             const float wx1 = xs.w, wx0 = 1.0f - xs.w;
             const int j0 = u - xs.d;  // Z column of tap 0 for voxel column u
 #pragma unroll
@@ -801,7 +826,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                 Fv[q][k] += fmaf(wx1, zm, wx0 * z0);
             }
         }
-        if (iv + 1 < n_v0) weights(v0 + A.vr.iv0_step);
+        if (iv + 1 < n_v0) store_w();
         __syncthreads();
     }
     if (aborted) {
@@ -931,7 +956,9 @@ int backproject_tma_t(const petl_geom& G, const TG* g, TF* f, int mode, int accu
     A.T = T;
     A.err = err;
     // as many ring stages as fit (copies from DRAM need several in flight)
+    A.max_views = vr.n_v0(G.N_v0);
     const size_t fixed = size_t(BNP) * BK * NU0 * 4 + size_t(BV1CAP) * BNP * 8 + size_t(BV1CAP) * BNP * 4 +
+                         size_t(A.max_views) * BNP * sizeof(Shift) +
                          size_t(BV1CAP) * 4 * 4 + size_t(BV1CAP) * BPG * 4 + size_t(BV1CAP) * 4 + 2 * BNSMAX * 8 +
                          8 + BNSMAX * 4 + 16;
     A.ns = int(std::min<size_t>(BNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / size_t(A.sstride)));
