@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <string>
 
 #include "common.cuh"
@@ -94,6 +95,17 @@ __device__ __forceinline__ void fence_proxy_async_smem()
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Plain bulk copy global -> this CTA's shared memory (no tensor map, no
+// multicast): both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
 }
 
 // ===========================================================================
@@ -398,8 +410,8 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, TG* __restrict__ g, const TG
 // ===========================================================================
 constexpr int BK = 8;               // z rows per CTA
 constexpr int BPT = 4;              // planes per thread
-constexpr int BPG = 2;              // plane groups
-constexpr int BNP = BPT * BPG;      // planes per CTA
+constexpr int BPG = 2;              // plane groups (at most)
+constexpr int BNP = BPT * BPG;      // planes per CTA (at most)
 constexpr int BDW = 2;              // largest shift difference among a thread's planes
 constexpr int BWN = BK + BDW + 1;   // register window rows
 constexpr int BNSMAX = 6;          // copy ring stages at most
@@ -441,11 +453,14 @@ __device__ __forceinline__ void bwd_taps(float (&Z)[BK], const float (&W)[BWN], 
                                          uint32_t om)
 {
     if (MASK) {
+        // masked taps read zero instead of the window value (rows outside the
+        // view are not copied and may hold any bit pattern, which a zero
+        // weight would not cancel)
 #pragma unroll
         for (int k = 0; k < BK; k++) {
-            const float a = ((vm >> (O + k)) & (om >> k) & 1u) ? w1 : 0.0f;
-            const float b = ((vm >> (O + k + 1)) & (om >> k) & 1u) ? w0 : 0.0f;
-            Z[k] = fmaf(a, W[O + k], fmaf(b, W[O + k + 1], Z[k]));
+            const float b = ((vm >> (O + k + 1)) & (om >> k) & 1u) ? W[O + k + 1] : 0.0f;
+            const float a = ((vm >> (O + k)) & (om >> k) & 1u) ? W[O + k] : 0.0f;
+            Z[k] = fmaf(w1, a, fmaf(w0, b, Z[k]));
         }
     } else {
         // all tap-0 FMAs, then all tap-1 FMAs: independent chains back to back
@@ -471,16 +486,23 @@ __device__ __forceinline__ void bwd_taps4(float (&Z)[BPT][BK], const float (&W)[
 // memory offsets become immediates); 0: read it from the geometry.
 // TG: planogram storage, TF: volume storage (float or bfloat16); FP32
 // arithmetic throughout.
-template <bool ADJ, int PITCH, class TG, class TF>
+// BULK: the planogram rows arrive by plain bulk copies (cp.async.bulk) of
+// whole row pairs instead of a tensor map, which lifts the tensor map's rule
+// that rows be multiples of 16 bytes and its 256-element box (N_u0 need only
+// be even); rows outside the view are not copied and are masked instead.
+// PG: plane groups per CTA (2, or 1 when N_u0 or numX exceeds 256).
+template <bool ADJ, int PITCH, class TG, class TF, bool BULK, int PG>
 __global__ void __launch_bounds__(512, 1)
-k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const BwdTmaArgs A)
+k_bwd_tma(const __grid_constant__ CUtensorMap gmap, const TG* __restrict__ gsrc, TF* __restrict__ f,
+          const BwdTmaArgs A)
 {
+    constexpr int NP = BPT * PG;  // planes per CTA
     extern __shared__ __align__(128) unsigned char smem[];
     const petl_geom& G = A.G;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwarps = blockDim.x >> 5;
     const int cw = warp % A.ncw, pg = warp / A.ncw;
-    const int p0 = blockIdx.x * BNP;  // first plane of the CTA
+    const int p0 = blockIdx.x * NP;  // first plane of the CTA
     const int r0 = blockIdx.y * BK;   // first z row of the CTA
     const int u = cw * 32 + lane;     // this thread's column (planogram u0 and voxel x)
     const int NY = G.numY, NX = G.numX, NZ = G.numZ, NU1 = G.N_u1;
@@ -491,16 +513,17 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     auto ring = [&](int slot) {  // [ns][brb][NU0] planogram rows (TMA)
         return reinterpret_cast<TG*>(smem + size_t(slot) * A.sstride);
     };
-    float* Zs = reinterpret_cast<float*>(smem + size_t(ns) * A.sstride);  // [BNP][BK][NU0]
-    float2* Wt = reinterpret_cast<float2*>(Zs + BNP * BK * NU0);          // [BV1CAP][BNP]
-    float* s_w = reinterpret_cast<float*>(Wt + BV1CAP * BNP);             // [BV1CAP][BNP]
-    Shift* s_xs = reinterpret_cast<Shift*>(s_w + BV1CAP * BNP);           // [n_v0][BNP] x shifts of the planes
-    int* s_v1 = reinterpret_cast<int*>(s_xs + A.max_views * BNP);         // [BV1CAP]
+    float* Zs = reinterpret_cast<float*>(smem + size_t(ns) * A.sstride);  // [NP][BK][NU0]
+    float2* Wt = reinterpret_cast<float2*>(Zs + NP * BK * NU0);          // [BV1CAP][NP]
+    float* s_w = reinterpret_cast<float*>(Wt + BV1CAP * NP);             // [BV1CAP][NP]
+    Shift* s_xs = reinterpret_cast<Shift*>(s_w + BV1CAP * NP);           // [n_v0][NP] x shifts of the planes
+    int* s_v1 = reinterpret_cast<int*>(s_xs + A.max_views * NP);         // [BV1CAP]
     int* s_grow = s_v1 + BV1CAP;                                          // [BV1CAP]
     uint32_t* s_code = reinterpret_cast<uint32_t*>(s_grow + BV1CAP);      // [BV1CAP]
     uint32_t* s_wb = s_code + BV1CAP;                                     // [BV1CAP]
-    uint32_t* s_mask = s_wb + BV1CAP;                                     // [BV1CAP][BPG]
-    uint32_t* s_pat = s_mask + BV1CAP * BPG;                              // [BV1CAP]
+    uint32_t* s_mask = s_wb + BV1CAP;                                     // [BV1CAP][PG]
+    uint32_t* s_vmask = s_mask + BV1CAP * PG;                            // [BV1CAP][PG]
+    uint32_t* s_pat = s_vmask + BV1CAP * PG;                             // [BV1CAP]
     uint64_t* full = reinterpret_cast<uint64_t*>(s_pat + BV1CAP);         // [ns]
     uint64_t* empty = full + BNSMAX;                                      // [ns]
     int* s_n = reinterpret_cast<int*>(empty + BNSMAX);
@@ -515,16 +538,16 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
             const int v1 = vb + lane;
             bool ok = false;
             uint32_t code = 0, wbs = 0, pats = 0;
-            uint32_t msk[BPG];
+            uint32_t msk[PG], vmsk[PG];
             int grow = 0;
-            float wz[BNP];
+            float wz[NP];
 #pragma unroll
-            for (int q = 0; q < BPG; q++) msk[q] = 0xffffffffu;
+            for (int q = 0; q < PG; q++) msk[q] = vmsk[q] = 0xffffffffu;
             if (v1 < A.vr.iv1_end) {
-                int dz[BNP];
+                int dz[NP];
                 int dmin = 1 << 30, dmax = -(1 << 30);
 #pragma unroll
-                for (int p = 0; p < BNP; p++) {
+                for (int p = 0; p < NP; p++) {
                     const int y = min(p0 + p, NY - 1);
                     const Shift zs = A.T.zt[size_t(v1) * NY + y];
                     dz[p] = zs.d;
@@ -536,9 +559,9 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                 }
                 grow = r0 - dmax - 1;
                 const int2 ub1 = A.T.ub1[v1];
-                int mode[BNP];
+                int mode[NP];
 #pragma unroll
-                for (int p = 0; p < BNP; p++) {
+                for (int p = 0; p < NP; p++) {
                     mode[p] = 0;
                     if (p0 + p >= NY) continue;
                     const int lo = r0 - dz[p] - 1, hi = r0 + BK - 1 - dz[p];  // g rows touched
@@ -551,10 +574,12 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                         if (r0 + BK - 1 < zv.x || r0 > zv.y) continue;
                         mode[p] = (r0 >= zv.x && r0 + BK - 1 <= zv.y) ? 1 : 2;
                     }
+                    // bulk copies leave rows outside the view unwritten: mask them
+                    if (BULK && mode[p] == 1 && (lo < 0 || hi >= NU1)) mode[p] = 2;
                 }
                 bool bad = dmax - dmin > A.brb - BWN;
 #pragma unroll
-                for (int q = 0; q < BPG; q++) {
+                for (int q = 0; q < PG; q++) {
                     int wb = 1 << 30;
 #pragma unroll
                     for (int t = 0; t < BPT; t++)
@@ -570,6 +595,12 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                         ok = true;
                     }
                     wbs |= uint32_t(wb) << (8 * q);
+                    if (BULK) {
+                        uint32_t vr = 0;  // window rows inside the view
+                        for (int i = 0; i < BWN; i++)
+                            if (grow + wb + i >= 0 && grow + wb + i < NU1) vr |= 1u << i;
+                        vmsk[q] = vr;
+                    }
                     // straight-line pattern of the group, if it has one
                     int pid = kPatGeneric;
                     {
@@ -594,7 +625,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                         uint32_t vm = 0;
                         for (int i = 0; i < BWN; i++)
                             if (grow + wb + i >= ub1.x && grow + wb + i <= ub1.y) vm |= 1u << i;
-                        msk[q] = vm;
+                        msk[q] = vm & vmsk[q];
                     } else {
                         uint32_t om = 0;
 #pragma unroll
@@ -620,12 +651,15 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                     s_v1[idx] = v1;
                     s_grow[idx] = grow;
                     s_code[idx] = code;
-                    s_wb[idx] = wbs;
+                    // bits 24..: the row of the copied pair block where row grow sits
+                    s_wb[idx] = wbs | (BULK ? uint32_t(grow & 1) << 24 : 0u);
                     s_pat[idx] = pats;
 #pragma unroll
-                    for (int q = 0; q < BPG; q++) s_mask[idx * BPG + q] = msk[q];
+                    for (int q = 0; q < PG; q++) s_vmask[idx * PG + q] = vmsk[q];
 #pragma unroll
-                    for (int p = 0; p < BNP; p++) s_w[idx * BNP + p] = wz[p];
+                    for (int q = 0; q < PG; q++) s_mask[idx * PG + q] = msk[q];
+#pragma unroll
+                    for (int p = 0; p < NP; p++) s_w[idx * NP + p] = wz[p];
                 }
             }
             n += __popc(bal);
@@ -652,28 +686,28 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
     // loads of S for the next view are issued at the start of a view
     // (load_S) and stored after its stages (store_w), so their latency hides
     // behind the view's work; at most kWPT elements per thread.
-    constexpr int kWPT = (BV1CAP * BNP + 511) / 512;
+    constexpr int kWPT = (BV1CAP * NP + 511) / 512;
     float s_pre[kWPT];
     auto load_S = [&](int v0) {
 #pragma unroll
         for (int i = 0; i < kWPT; i++) {
             const int e = tid + i * int(blockDim.x);
-            s_pre[i] = e < nlive * BNP ? __ldg(&A.T.S[size_t(s_v1[e / BNP]) * G.N_v0 + v0]) : 0.0f;
+            s_pre[i] = e < nlive * NP ? __ldg(&A.T.S[size_t(s_v1[e / NP]) * G.N_v0 + v0]) : 0.0f;
         }
     };
     auto store_w = [&]() {
 #pragma unroll
         for (int i = 0; i < kWPT; i++) {
             const int e = tid + i * int(blockDim.x);
-            if (e < nlive * BNP) {
+            if (e < nlive * NP) {
                 const float S = s_pre[i], w = s_w[e];
                 Wt[e] = make_float2(S * (1.0f - w), S * w);
             }
         }
     };
     // x shifts of the CTA's planes for every view, staged once
-    for (int e = tid; e < n_v0 * BNP; e += blockDim.x) {
-        const int iv = e / BNP, p = e % BNP;
+    for (int e = tid; e < n_v0 * NP; e += blockDim.x) {
+        const int iv = e / NP, p = e % NP;
         const int y = min(p0 + p, NY - 1);
         s_xs[e] = A.T.xt[size_t(A.vr.iv0_first + iv * A.vr.iv0_step) * NY + y];
     }
@@ -692,8 +726,22 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
         const int v0 = A.vr.iv0_first + (j / nlive) * A.vr.iv0_step;
         if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err)) return false;
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&full[slot], box_bytes);
-        tma_load_4d(ring(slot), &gmap, &full[slot], 0, s_grow[li], v0, s_v1[li]);
+        if constexpr (BULK) {
+            // row pairs [rp0, rp0 + nrows) of view (v1, v0), the part inside
+            // the view; even rows start 16-byte aligned (N_u0 and N_u1 even)
+            const int gr = s_grow[li], rp0 = gr & ~1;
+            const int nrows = (gr - rp0 + A.brb + 1) & ~1;
+            const int ra = max(rp0, 0), rb = min(rp0 + nrows, NU1);
+            const uint32_t bytes = rb > ra ? uint32_t(rb - ra) * uint32_t(NU0) * uint32_t(sizeof(TG)) : 0u;
+            mbar_arrive_expect_tx(&full[slot], bytes);
+            if (bytes) {
+                const TG* src = gsrc + ((size_t(s_v1[li]) * G.N_v0 + v0) * NU1 + ra) * NU0;
+                bulk_load(ring(slot) + (ra - rp0) * NU0, src, bytes, &full[slot]);
+            }
+        } else {
+            mbar_arrive_expect_tx(&full[slot], box_bytes);
+            tma_load_4d(ring(slot), &gmap, &full[slot], 0, s_grow[li], v0, s_v1[li]);
+        }
         s_round[slot] = round;
         return true;
     };
@@ -736,12 +784,13 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
             const uint32_t code = s_code[li] >> (16 * pg);  // this group's 4 planes
             const uint32_t pat = (s_pat[li] >> (4 * pg)) & 15u;
             if (ucol && pat != uint32_t(kPatGeneric)) {
-                const int wb = (s_wb[li] >> (8 * pg)) & 0xff;
+                const uint32_t wbw = s_wb[li];
+                const int wb = int((wbw >> (8 * pg)) & 0xff) + (BULK ? int(wbw >> 24) : 0);
                 const TG* Gs = ring(s) + wb * NU0 + u;
                 float W[BWN];
 #pragma unroll
                 for (int i = 0; i < BWN; i++) W[i] = Store<TG>::ld(Gs[i * NU0]);
-                const float4* W4 = reinterpret_cast<const float4*>(Wt + li * BNP + pg * BPT);
+                const float4* W4 = reinterpret_cast<const float4*>(Wt + li * NP + pg * BPT);
                 const float4 wa = W4[0], wb4 = W4[1];
                 switch (pat) {
                     case 0: bwd_taps4<0>(Z, W, wa, wb4); break;
@@ -753,12 +802,13 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                     default: bwd_taps4<6>(Z, W, wa, wb4); break;
                 }
             } else if (ucol && (code & 0x3333u)) {
-                const int wb = (s_wb[li] >> (8 * pg)) & 0xff;
+                const uint32_t wbw = s_wb[li];
+                const int wb = int((wbw >> (8 * pg)) & 0xff) + (BULK ? int(wbw >> 24) : 0);
                 const TG* Gs = ring(s) + wb * NU0 + u;
                 float W[BWN];
 #pragma unroll
                 for (int i = 0; i < BWN; i++) W[i] = Store<TG>::ld(Gs[i * NU0]);
-                const float2* Wl = Wt + li * BNP + pg * BPT;
+                const float2* Wl = Wt + li * NP + pg * BPT;
 #pragma unroll
                 for (int q = 0; q < BPT; q++) {
                     const uint32_t c = (code >> (4 * q)) & 15u;
@@ -774,8 +824,8 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
                         }
                     } else {
                         // rows at the edge of the visible range: per-row masks
-                        const uint32_t m = s_mask[li * BPG + pg];
-                        const uint32_t vm = ADJ ? m : 0xffffffffu;
+                        const uint32_t m = s_mask[li * PG + pg];
+                        const uint32_t vm = ADJ ? m : (BULK ? s_vmask[li * PG + pg] : 0xffffffffu);
                         const uint32_t om = ADJ ? 0xffffffffu : (m >> (8 * q)) & 0xffu;
                         switch (o) {
                             case 0: bwd_taps<0, true>(Z[q], W, w0, w1, vm, om); break;
@@ -815,7 +865,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, TF* __restrict__ f, const Bw
         for (int q = 0; q < BPT; q++) {
             const int y = p0 + pg * BPT + q;
             if (y >= NY) continue;
-            const Shift xs = s_xs[iv * BNP + pg * BPT + q];
+            const Shift xs = s_xs[iv * NP + pg * BPT + q];
             const float wx1 = xs.w, wx0 = 1.0f - xs.w;
             const int j0 = u - xs.d;  // Z column of tap 0 for voxel column u
 #pragma unroll
@@ -928,49 +978,64 @@ int backproject_tma_t(const petl_geom& G, const TG* g, TF* f, int mode, int accu
 {
     constexpr int EB = int(sizeof(TG));
     const int NU0 = G.N_u0;
-    if ((NU0 * EB) % 16 != 0 || NU0 > 256 || G.numX > 256 || (reinterpret_cast<uintptr_t>(g) & 15) != 0)
-        return kNotApplicable;
+    if ((reinterpret_cast<uintptr_t>(g) & 15) != 0) return kNotApplicable;
+    // tensor-map staging when the rows are multiples of 16 bytes and fit one
+    // 256-element box; FP32 planograms with even rows otherwise take bulk
+    // copies of row pairs (up to 512 columns)
+    const bool tensor = (NU0 * EB) % 16 == 0 && NU0 <= 256 && G.numX <= 256;
+    const bool bulk = !tensor && EB == 4 && NU0 % 2 == 0 && G.N_u1 % 2 == 0 && NU0 <= 512 && G.numX <= 512;
+    if (!tensor && !bulk) return kNotApplicable;
+    const int pg = std::max(NU0, G.numX) <= 256 ? 2 : 1;
+    const int np = BPT * pg;
     if (vr.iv1_end - vr.iv1_begin > BV1CAP) return kNotApplicable;
     const double step = double(std::max(std::fabs(G.v1_0), std::fabs(G.v1_0 + (G.N_v1 - 1) * G.T_v1))) *
                         double(G.T_x) / double(G.T_z);  // shift change per plane
     if (shift_spread(BPT - 1, step) > BDW) return kNotApplicable;
-    const int brb = BWN + shift_spread(BNP - 1, step);
-    if (brb > 256) return kNotApplicable;
+    const int brb = BWN + shift_spread(np - 1, step);
+    if (brb > 254) return kNotApplicable;
     int* err = device_error_ptr();
     if (!err) return kNotApplicable;
     CUtensorMap map;
-    const uint64_t dims[4] = {uint64_t(NU0), uint64_t(G.N_u1), uint64_t(G.N_v0), uint64_t(G.N_v1)};
-    const uint64_t strides[3] = {uint64_t(NU0) * EB, uint64_t(NU0) * G.N_u1 * EB,
-                                 uint64_t(NU0) * G.N_u1 * G.N_v0 * EB};
-    const uint32_t box[4] = {uint32_t(NU0), uint32_t(brb), 1u, 1u};
-    if (!encode_tensor_map(&map, g, 4, dims, strides, box, EB)) return kNotApplicable;
+    std::memset(&map, 0, sizeof(map));
+    if (tensor) {
+        const uint64_t dims[4] = {uint64_t(NU0), uint64_t(G.N_u1), uint64_t(G.N_v0), uint64_t(G.N_v1)};
+        const uint64_t strides[3] = {uint64_t(NU0) * EB, uint64_t(NU0) * G.N_u1 * EB,
+                                     uint64_t(NU0) * G.N_u1 * G.N_v0 * EB};
+        const uint32_t box[4] = {uint32_t(NU0), uint32_t(brb), 1u, 1u};
+        if (!encode_tensor_map(&map, g, 4, dims, strides, box, EB)) return kNotApplicable;
+    }
 
     BwdTmaArgs A{};
     A.G = G;
     A.vr = vr;
     A.ncw = int(ceil_div(std::max(NU0, G.numX), 32));
     A.brb = brb;
-    A.sstride = (brb * NU0 * EB + 127) & ~127;
+    // bulk copies stage whole row pairs: up to two rows more than the window
+    A.sstride = ((brb + (bulk ? 2 : 0)) * NU0 * EB + 127) & ~127;
     A.accumulate = accumulate;
     A.scale = scale;
     A.T = T;
     A.err = err;
     // as many ring stages as fit (copies from DRAM need several in flight)
     A.max_views = vr.n_v0(G.N_v0);
-    const size_t fixed = size_t(BNP) * BK * NU0 * 4 + size_t(BV1CAP) * BNP * 8 + size_t(BV1CAP) * BNP * 4 +
-                         size_t(A.max_views) * BNP * sizeof(Shift) +
-                         size_t(BV1CAP) * 4 * 4 + size_t(BV1CAP) * BPG * 4 + size_t(BV1CAP) * 4 + 2 * BNSMAX * 8 +
-                         8 + BNSMAX * 4 + 16;
+    const size_t fixed = size_t(np) * BK * NU0 * 4 + size_t(BV1CAP) * np * 8 + size_t(BV1CAP) * np * 4 +
+                         size_t(A.max_views) * np * sizeof(Shift) + size_t(BV1CAP) * 4 * 4 +
+                         size_t(BV1CAP) * pg * 4 * 2 + size_t(BV1CAP) * 4 + 2 * BNSMAX * 8 + 8 + BNSMAX * 4 + 16;
     A.ns = int(std::min<size_t>(BNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / size_t(A.sstride)));
     if (A.ns < 2) return kNotApplicable;
     const size_t smem = size_t(A.ns) * A.sstride + fixed;
-    const int threads = 32 * A.ncw * BPG;
-    dim3 grid(ceil_div(G.numY, BNP), ceil_div(G.numZ, BK));
-    auto kern = mode == PETL_BP_ADJOINT
-                    ? (NU0 == 256 ? k_bwd_tma<true, 256, TG, TF> : k_bwd_tma<true, 0, TG, TF>)
-                    : (NU0 == 256 ? k_bwd_tma<false, 256, TG, TF> : k_bwd_tma<false, 0, TG, TF>);
+    const int threads = 32 * A.ncw * pg;
+    dim3 grid(ceil_div(G.numY, np), ceil_div(G.numZ, BK));
+    const bool adj = mode == PETL_BP_ADJOINT;
+    auto kern = adj ? k_bwd_tma<true, 0, TG, TF, false, 2> : k_bwd_tma<false, 0, TG, TF, false, 2>;
+    if (tensor && NU0 == 256) kern = adj ? k_bwd_tma<true, 256, TG, TF, false, 2> : k_bwd_tma<false, 256, TG, TF, false, 2>;
+    if constexpr (sizeof(TG) == 4) {
+        if (bulk)
+            kern = pg == 2 ? (adj ? k_bwd_tma<true, 0, TG, TF, true, 2> : k_bwd_tma<false, 0, TG, TF, true, 2>)
+                           : (adj ? k_bwd_tma<true, 0, TG, TF, true, 1> : k_bwd_tma<false, 0, TG, TF, true, 1>);
+    }
     PETL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kern<<<grid, threads, smem, st>>>(map, f, A);
+    kern<<<grid, threads, smem, st>>>(map, g, f, A);
     PETL_LAUNCH_CHECK("backproject_tma");
     return 0;
 }

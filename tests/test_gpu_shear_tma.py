@@ -2,8 +2,9 @@
 kernels, the general kernels and the FP64 oracle.
 
 Dispatch 0 runs the TMA-staged kernels wherever their layout rules hold
-(volume rows a multiple of 4 floats for the forward copy, N_u0 a multiple of
-4 and at most 256 for the backward); dispatch 2 runs the first-generation
+(volume rows a multiple of 4 floats for the forward copy; for the backward
+N_u0 a multiple of 4 and at most 256 with a tensor map, else any even N_u0
+up to 512 with bulk copies of row pairs); dispatch 2 runs the first-generation
 shear kernels; dispatch 1 the general kernels.  The forward TMA kernel does
 the same float operations in the same order as the first-generation one, so
 the two agree to rounding of the final scale; the backward kernels sum in a
@@ -27,8 +28,13 @@ CASES = {
     "panel2mm": ((0.0, 256.0, 128.0, 64.0, 2.0, 0.5, 0.25), (128, 128, 64, 2.0), True, True),
     # ragged sizes, off-centre volume, rows a multiple of 4
     "rag4": ((0.0, 100.0, 75.0, 27.0, 1.5, 0.45, 0.2), (52, 60, 18, 1.5, 1.5, 3.0, -4.5, 1.5), True, True),
-    # rows not a multiple of 4 floats: falls back to the first-generation kernels
-    "odd": ((0.0, 100.0, 50.0, 26.0, 1.5, 0.45, 0.2), (50, 58, 15, 1.5, 1.5, 3.0, -4.5, 1.5), False, False),
+    # volume rows not a multiple of 4 floats: first-generation forward; the
+    # backward stages planogram rows (62 columns) by bulk copies of row pairs
+    "odd": ((0.0, 100.0, 50.0, 26.0, 1.5, 0.45, 0.2), (50, 58, 15, 1.5, 1.5, 3.0, -4.5, 1.5), False, True),
+    # N_u0 = 278 (> 256, not a multiple of 4): bulk-copy backward, one plane group
+    "wide": ((0.0, 300.0, 128.0, 32.0, 1.0, 0.5, 0.25), (256, 64, 32, 1.0), True, True),
+    # and numX = 320 > 256
+    "wide2": ((0.0, 300.0, 128.0, 32.0, 1.0, 0.5, 0.25), (320, 48, 16, 1.0), True, True),
 }
 
 
@@ -99,7 +105,7 @@ def test_tma_backward(cuda, name, mode):
         assert rel_l2(a, O.backproject(Go, _np(y))) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["t1", "panel2mm", "rag4"])
+@pytest.mark.parametrize("name", ["t1", "panel2mm", "rag4", "odd", "wide"])
 def test_tma_pair_is_exact_adjoint(cuda, name):
     import torch
     from petl_b200 import ops
