@@ -153,6 +153,25 @@ def cpu_baseline(nslices=2, nthreads=0):
             "seconds_per_step": step_s}
 
 
+def max_over_ranks(x, world, device=None):
+    """The maximum of a per-rank number over all ranks (device timings are
+    reported as the slowest rank's); the number itself for one rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, steps, total_ms):
+    """Whole-job throughput of `world` independent replicas that each ran
+    `steps` steps, timed by the slowest rank's total_ms (weak scaling: the
+    per-GPU work is fixed)."""
+    return world * steps / (total_ms / 1e3)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -242,13 +261,9 @@ def main():
     clk = clocks.stop()
     t_fwd = [a.elapsed_time(b) for a, b, _ in ev]
     t_bwd = [b.elapsed_time(c) for _, b, c in ev]
-    total_ms = float(np.sum(t_fwd) + np.sum(t_bwd))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(np.sum(t_fwd) + np.sum(t_bwd)), world, dev)
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1e3)
+    value = replica_value(world, args.steps, total_ms)
 
     # roofline of the dominant kernel
     hbm, peak_kind, peaks = read_peaks()
@@ -301,11 +316,7 @@ def main():
             s.project([gnp], fnp)
             s.backproject([gnp], bnp)
             ts.append(time.perf_counter() - t0)
-        e2e_s = float(np.mean(ts))
-        if world > 1:
-            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(float(np.mean(ts)), world, dev)
         nb_f, nb_g = 4 * G.n_voxels, 4 * G.n_rays
         line["e2e"] = {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nb_f + nb_g,
                        "d2h_bytes_per_step": nb_g + nb_f, "steps": len(ts),
