@@ -65,7 +65,9 @@ int petl_model_geometry(int which, petl_geom* out);
  * kernels for axis-aligned, equal-pitch geometries (TMA-staged where the
  * layout allows) and the general kernels otherwise; 1 always uses the
  * general kernels; 2 uses the shear-warp kernels without TMA staging where
- * the shear path applies.  All compute the same operator. */
+ * the shear path applies; 3 uses the TMA-staged shear-warp kernels with the
+ * single-kernel forward instead of the split forward (x-shift pass into
+ * scratch + z-tap kernel).  All compute the same operator. */
 int petl_set_dispatch(int mode);
 /* Which projector kernels the calling thread's last projector call used:
  * 0 general, 1 shear-warp, 2 TMA-staged shear-warp; -1 before any call. */

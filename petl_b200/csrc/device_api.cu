@@ -114,8 +114,9 @@ int petl_last_projector_path(void) { return t_last_path; }
 int petl_set_dispatch(int mode)
 {
     // 0: the fastest kernels that apply; 1: always the general kernels;
-    // 2: shear kernels without TMA staging where the shear path applies
-    if (mode < 0 || mode > 2) return -1;
+    // 2: shear kernels without TMA staging where the shear path applies;
+    // 3: TMA-staged shear kernels with the fused (single-kernel) forward
+    if (mode < 0 || mode > 3) return -1;
     g_dispatch = mode;
     return 0;
 }

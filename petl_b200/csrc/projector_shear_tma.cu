@@ -41,72 +41,13 @@
 #include "common.cuh"
 #include "projector.cuh"
 #include "shear.cuh"
+#include "storage.cuh"
 #include "tma.cuh"
 
 namespace petl {
 namespace shear {
 
 namespace {
-
-enum : int { kErrLayout = 2 };  // a host-side bound on the shift spread did not hold
-
-__device__ __forceinline__ float2 dup(float a) { return make_float2(a, a); }
-
-// Storage element types: float32, or bfloat16 read into FP32 arithmetic.
-// kAlign is the TMA x-coordinate granule (16 bytes) in elements.
-template <class T>
-struct Store;
-template <>
-struct Store<float> {
-    static constexpr int kAlign = 4;
-    static __device__ __forceinline__ float ld(float x) { return x; }
-    static __device__ __forceinline__ float st(float x) { return x; }
-    static __device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
-    static __device__ __forceinline__ void st2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
-};
-template <>
-struct Store<__nv_bfloat16> {
-    static constexpr int kAlign = 8;
-    static __device__ __forceinline__ float ld(__nv_bfloat16 x) { return __bfloat162float(x); }
-    static __device__ __forceinline__ __nv_bfloat16 st(float x) { return __float2bfloat16_rn(x); }
-    static __device__ __forceinline__ float2 ld2(const __nv_bfloat16* p)
-    {
-        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
-    }
-    static __device__ __forceinline__ void st2(__nv_bfloat16* p, float2 v)
-    {
-        *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
-    }
-};
-
-// Two scalar FMAs on a column pair.  Scalar FFMA issues at the full FP32
-// rate with two warps per scheduler; the packed f32x2 form needs about four
-// times the warps to reach the same rate on this part.
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
-{
-    return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
-}
-
-__device__ __forceinline__ void fence_proxy_async_smem()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-
-// Plain bulk copy global -> this CTA's shared memory (no tensor map, no
-// multicast): both addresses 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
 
 // ===========================================================================
 // forward
@@ -904,16 +845,6 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, const TG* __restrict__ gsrc,
     }
 }
 
-double plane_ymax(const petl_geom& G)
-{
-    return std::max(std::fabs(double(G.y_0)), std::fabs(double(G.y_0) + (G.numY - 1) * double(G.T_x)));
-}
-
-// Upper bound on the difference of the integer z shifts of slopes (or planes)
-// n steps apart: the exact shifts differ by at most n * step, their floors by
-// at most floor(n * step) + 1 (with a relative margin for the float inputs).
-int shift_spread(int n, double step) { return int(std::floor(double(n) * step * (1.0 + 1e-6))) + 1; }
-
 constexpr int kFwdK = 8;
 
 }  // namespace
@@ -1043,6 +974,12 @@ int backproject_tma_t(const petl_geom& G, const TG* g, TF* f, int mode, int accu
 int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
                 const Tables& T, cudaStream_t st)
 {
+    // the split form (x-shift pass + z-tap kernel) first; dispatch 3 keeps
+    // the fused kernel
+    if (dispatch_mode() != 3) {
+        const int rc = project_split(G, f, g, vr, meas, T, st);
+        if (rc != kNotApplicable) return rc;
+    }
     return project_tma_t<float, float>(G, f, g, vr, meas, T, st);
 }
 
@@ -1055,6 +992,10 @@ int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int 
 int project_tma_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
                      const __nv_bfloat16* meas, const Tables& T, cudaStream_t st)
 {
+    if (dispatch_mode() != 3) {
+        const int rc = project_split_bf16(G, f, g, vr, meas, T, st);
+        if (rc != kNotApplicable) return rc;
+    }
     return project_tma_t<__nv_bfloat16, __nv_bfloat16>(G, f, g, vr, meas, T, st);
 }
 

@@ -5,6 +5,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "common.cuh"
 #include "projector.cuh"
 
@@ -33,6 +35,27 @@ struct TableBuf {
 };
 
 int make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st);
+
+// Largest |y| of the volume's plane centres.
+inline double plane_ymax(const petl_geom& G)
+{
+    return std::fmax(std::fabs(double(G.y_0)), std::fabs(double(G.y_0) + (G.numY - 1) * double(G.T_x)));
+}
+
+// Upper bound on the difference of the integer z shifts of slopes (or planes)
+// n steps apart: the exact shifts differ by at most n * step, their floors by
+// at most floor(n * step) + 1 (with a relative margin for the float inputs).
+inline int shift_spread(int n, double step) { return int(std::floor(double(n) * step * (1.0 + 1e-6))) + 1; }
+
+// Split forward projection (projector_split.cu): an x-shift pass per chunk of
+// views into FP32 scratch, then a z-tap kernel fed by a TMA ring.  Same
+// operator and the same float operations in the same order as project_tma.
+// kNotApplicable when the layout rules or the scratch allocation fail.
+int project_split(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                  const Tables& T, cudaStream_t st);
+int project_split_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
+                       const __nv_bfloat16* meas, const Tables& T, cudaStream_t st);
+
 // Bytes of the shift tables of G (make_tables' allocation).
 size_t table_bytes(const petl_geom& G);
 
@@ -64,7 +87,8 @@ int backproject_tma_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, i
 }  // namespace shear
 
 // Projector kernel choice (petl_set_dispatch): 0 automatic, 1 general kernels
-// only, 2 shear kernels without TMA staging where the shear path applies.
+// only, 2 shear kernels without TMA staging where the shear path applies, 3
+// TMA-staged shear kernels with the fused forward instead of the split one.
 int dispatch_mode();
 // Records which projector kernels the calling thread used last
 // (petl_last_projector_path): 0 general, 1 shear, 2 TMA-staged shear.

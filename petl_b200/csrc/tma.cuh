@@ -14,7 +14,10 @@ namespace petl {
 
 // Device error word (petl_device_error_flag() reads and clears it); kernels
 // receive its device address as an argument (device_error_ptr()).
-enum : int { kErrWaitTimeout = 1 };
+enum : int {
+    kErrWaitTimeout = 1,  // a bounded wait gave up
+    kErrLayout = 2,       // a host-side bound on a kernel's layout (shift spread, table size) did not hold
+};
 int* device_error_ptr();
 
 constexpr unsigned kWaitLimit = 1u << 26;

@@ -4,11 +4,14 @@ kernels, the general kernels and the FP64 oracle.
 Dispatch 0 runs the TMA-staged kernels wherever their layout rules hold
 (volume rows a multiple of 4 floats for the forward copy; for the backward
 N_u0 a multiple of 4 and at most 256 with a tensor map, else any even N_u0
-up to 512 with bulk copies of row pairs); dispatch 2 runs the first-generation
-shear kernels; dispatch 1 the general kernels.  The forward TMA kernel does
-the same float operations in the same order as the first-generation one, so
-the two agree to rounding of the final scale; the backward kernels sum in a
-different order and agree to float accuracy.  Every case also checks that no
+up to 512 with bulk copies of row pairs), with the split forward (x-shift
+pass into scratch, then the z-tap kernel); dispatch 3 the same with the
+single-kernel TMA forward; dispatch 2 runs the first-generation shear
+kernels; dispatch 1 the general kernels.  The split and single-kernel
+forwards do the same float operations in the same order and agree bit for
+bit; the forward TMA kernels and the first-generation one agree to rounding
+of the final scale; the backward kernels sum in a different order and agree
+to float accuracy.  Every case also checks that no
 bounded wait gave up (petl_device_error_flag) and which kernels ran.
 """
 import numpy as np
@@ -21,14 +24,16 @@ from helpers import ellipsoids
 pytestmark = pytest.mark.gpu
 
 CASES = {
-    # psi, D, L, H, T, v_m0, v_m1 ; volume ; TMA forward, TMA backward expected
+    # psi, D, L, H, T, v_m0, v_m1 ; volume ; single-kernel TMA forward, TMA
+    # backward expected (the split forward applies to every case: it stages
+    # its own padded scratch rows, not the volume's)
     "t2": ((0.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (64, 64, 16, 2.0), True, True),
     "t1": ((0.0, 128.0, 64.0, 32.0, 1.0, 0.5, 0.25), (128, 128, 32, 1.0), True, True),
     # the dual-panel geometry of the 128x128x64 / 2 mm recon: planogram (33, 65, 64, 128)
     "panel2mm": ((0.0, 256.0, 128.0, 64.0, 2.0, 0.5, 0.25), (128, 128, 64, 2.0), True, True),
     # ragged sizes, off-centre volume, rows a multiple of 4
     "rag4": ((0.0, 100.0, 75.0, 27.0, 1.5, 0.45, 0.2), (52, 60, 18, 1.5, 1.5, 3.0, -4.5, 1.5), True, True),
-    # volume rows not a multiple of 4 floats: first-generation forward; the
+    # volume rows not a multiple of 4 floats: no single-kernel TMA forward; the
     # backward stages planogram rows (62 columns) by bulk copies of row pairs
     "odd": ((0.0, 100.0, 50.0, 26.0, 1.5, 0.45, 0.2), (50, 58, 15, 1.5, 1.5, 3.0, -4.5, 1.5), False, True),
     # N_u0 = 278 (> 256, not a multiple of 4): bulk-copy backward, one plane group
@@ -82,7 +87,10 @@ def test_tma_forward(cuda, name):
     a, pa = _under(0, lambda: _np(ops.project(G, ft)))
     b, pb = _under(2, lambda: _np(ops.project(G, ft)))
     c, pc = _under(1, lambda: _np(ops.project(G, ft)))
-    assert (pa, pb, pc) == (2 if CASES[name][2] else 1, 1, 0)
+    d, pd = _under(3, lambda: _np(ops.project(G, ft)))
+    assert (pa, pb, pc, pd) == (2, 1, 0, 2 if CASES[name][2] else 1)
+    if CASES[name][2]:
+        assert np.array_equal(a, d)
     assert rel_l2(a, b) < 1e-6
     assert rel_l2(a, c) < 1e-5
     if G.shape[0] * G.shape[1] * G.shape[2] * G.shape[3] < 3e6:
@@ -147,6 +155,10 @@ def test_tma_subsets_slabs_ratio_accumulate(cuda):
 
     (full, parts, slabs, meas, ratio, b, b2, b3, b4), path = _under(0, run)
     assert path == 2
+    (full3, parts3, slabs3, _, ratio3, *_), path3 = _under(3, run)
+    assert path3 == 2
+    assert torch.equal(full, full3) and torch.equal(parts, parts3) and torch.equal(slabs, slabs3)
+    assert torch.equal(ratio, ratio3)
     assert torch.equal(full, parts)
     assert torch.equal(full, slabs)
     want = torch.where(full == 0, torch.zeros_like(full), meas / full)
@@ -165,9 +177,11 @@ def test_tma_full_size_against_first_generation(cuda):
     f = torch.rand(G.vol_shape, device=cuda, generator=gen)
     a, pa = _under(0, lambda: ops.project(G, f))
     b, pb = _under(2, lambda: ops.project(G, f))
-    assert (pa, pb) == (2, 1)
+    c, pc = _under(3, lambda: ops.project(G, f))
+    assert (pa, pb, pc) == (2, 1, 2)
+    assert torch.equal(a, c)
     assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 1e-6
-    del b
+    del b, c
     for mode in ("reference", "adjoint"):
         x, px = _under(0, lambda: ops.backproject(G, a, mode=mode))
         z, pz = _under(2, lambda: ops.backproject(G, a, mode=mode))
