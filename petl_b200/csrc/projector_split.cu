@@ -9,7 +9,8 @@
 // per plane pair.  Here the two stages are separate kernels:
 //
 // * k_xshift writes X for a chunk of views into FP32 scratch, [view][y][z][c]
-//   (memory bound: one write of a volume per view);
+//   (memory bound: one write of a volume per view; each volume row is read
+//   once per chunk);
 // * k_fwd_zsum applies the z taps.  CTA = one view x 16 slopes x 32 rows x 64
 //   columns, 16 warps of 4 slopes x 8 rows x 2 columns per lane.  The staged
 //   rows of each plane arrive by a tiled TMA copy (no multicast) into a ring
@@ -66,35 +67,51 @@ struct XshiftArgs {
     petl_geom G;
     ViewRange vr;
     int vi0;  // first view of the chunk (index in vr)
+    int nvc;  // views in the chunk
     int NXc;  // scratch row pitch (columns, a multiple of 4)
     Tables T;
 };
 
-// X rows of a chunk of views: one float4 of columns per thread.
-// Block (64, 4): 256 columns x 4 rows z; grid (columns, rows, views x planes).
+constexpr int XZB = 8;      // volume rows z per k_xshift block
+constexpr int XMAXNX = 1024;  // longest volume row k_xshift stages
+
+// X rows of a chunk of views.  A block stages rows z0..z0+7 of plane y in
+// shared memory once and writes them shifted for every view of the chunk,
+// one float4 of columns per thread and step.  Grid (ceil(NZ / 8), NY).
 template <class TF>
 __global__ void __launch_bounds__(256) k_xshift(const TF* __restrict__ f, float* __restrict__ X, const XshiftArgs A)
 {
+    __shared__ float rowbuf[XZB * XMAXNX];
     const petl_geom& G = A.G;
     const int NY = G.numY, NX = G.numX, NZ = G.numZ;
-    const int c = (blockIdx.x * 64 + threadIdx.x) * 4;
-    const int z = blockIdx.y * 4 + threadIdx.y;
-    const int vi = blockIdx.z / NY, y = blockIdx.z - vi * NY;
-    if (z >= NZ || c >= A.NXc) return;
-    const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
-    const Shift xs = A.T.xt[size_t(iv0) * NY + y];
-    const float w1 = xs.w, w0 = 1.0f - xs.w;
-    const TF* fr = f + (size_t(z) * NY + y) * NX;
-    float v[5];
-#pragma unroll
-    for (int i = 0; i < 5; i++) {
-        const int ix = c + xs.d + i;
-        v[i] = (ix >= 0 && ix < NX) ? Store<TF>::ld(fr[ix]) : 0.0f;
+    const int y = blockIdx.y, z0 = blockIdx.x * XZB;
+    const int nz = min(XZB, NZ - z0);
+    for (int e = threadIdx.x; e < nz * NX; e += blockDim.x) {
+        const int r = e / NX, x = e - r * NX;
+        rowbuf[r * NX + x] = Store<TF>::ld(f[(size_t(z0 + r) * NY + y) * NX + x]);
     }
-    const float4 o = make_float4(fmaf(w1, v[1], w0 * v[0]), fmaf(w1, v[2], w0 * v[1]), fmaf(w1, v[3], w0 * v[2]),
-                                 fmaf(w1, v[4], w0 * v[3]));
-    // streaming store: the scratch is read once, by the next kernel
-    __stcs(reinterpret_cast<float4*>(X + ((size_t(vi) * NY + y) * NZ + z) * A.NXc + c), o);
+    __syncthreads();
+    const int nq = A.NXc >> 2;  // float4 columns per row
+    for (int vi = 0; vi < A.nvc; vi++) {
+        const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
+        const Shift xs = A.T.xt[size_t(iv0) * NY + y];
+        const float w1 = xs.w, w0 = 1.0f - xs.w;
+        float* Xv = X + (size_t(vi) * NY + y) * NZ * A.NXc;
+        for (int e = threadIdx.x; e < nz * nq; e += blockDim.x) {
+            const int r = e / nq, c = (e - r * nq) * 4;
+            const float* fr = rowbuf + r * NX;
+            float v[5];
+#pragma unroll
+            for (int i = 0; i < 5; i++) {
+                const int ix = c + xs.d + i;
+                v[i] = unsigned(ix) < unsigned(NX) ? fr[ix] : 0.0f;
+            }
+            const float4 o = make_float4(fmaf(w1, v[1], w0 * v[0]), fmaf(w1, v[2], w0 * v[1]),
+                                         fmaf(w1, v[3], w0 * v[2]), fmaf(w1, v[4], w0 * v[3]));
+            // streaming store: the scratch is read once, by the next kernel
+            __stcs(reinterpret_cast<float4*>(Xv + size_t(z0 + r) * A.NXc + c), o);
+        }
+    }
 }
 
 struct ZsumArgs {
@@ -458,8 +475,7 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     const int NXc = (G.N_u0 + 3) & ~3;
     const size_t per_view = size_t(G.numY) * G.numZ * NXc * 4;
     int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), split_scratch_budget() / per_view)));
-    nv = std::min(nv, 65535 / G.numY);  // k_xshift grid.z = views x planes
-    if (nv < 1) return kNotApplicable;
+    if (G.numX > XMAXNX || G.numY > 65535) return kNotApplicable;  // k_xshift row buffer, grid.y
     const int nchunks = (n_v0 + nv - 1) / nv;
     nv = (n_v0 + nchunks - 1) / nchunks;
 
@@ -489,9 +505,8 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     cudaError_t e = cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
-        XshiftArgs XA{G, vr, vi0, NXc, T};
-        const dim3 gx(ceil_div(NXc, 256), ceil_div(G.numZ, 4), unsigned(nvc) * G.numY);
-        k_xshift<TF><<<gx, dim3(64, 4), 0, st>>>(f, X, XA);
+        XshiftArgs XA{G, vr, vi0, nvc, NXc, T};
+        k_xshift<TF><<<dim3(ceil_div(G.numZ, XZB), unsigned(G.numY)), 256, 0, st>>>(f, X, XA);
         note_launch();
         for (int l = 0; l < nl; l++) {
             L[l].A.vi0 = vi0;
