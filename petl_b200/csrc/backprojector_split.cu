@@ -1,0 +1,691 @@
+// Split backprojector (psi = 0, voxel pitch equal to the bin pitch): the
+// transpose of the split forward (projector_split.cu), in the gather form of
+// k_bwd_tma (projector_shear_tma.cu) for the reference semantics of
+// src/projectors.cu:240-377 and for the exact adjoint.
+//
+// The voxel (x, y, z) receives, from view v0 and slope v1 on plane y,
+//   S (1 - wz) g[v1][v0][z - dz][x - dx] + S wz g[v1][v0][z - dz - 1][x - dx]
+// interpolated in x by (1 - wx, wx) over columns x - dx and x - dx - 1.  The
+// two interpolations are separate kernels:
+//
+// * k_bwd_zgather sums the z taps over the slopes of one view into FP32
+//   scratch B[view][y][z][c] (c = planogram column).  CTA = views of a group x
+//   16 planes x 32 rows x 64 columns, 16 warps of 4 planes x 8 rows x 2
+//   columns per lane; per slope the planogram rows the tile needs arrive by a
+//   tiled TMA copy (no multicast) into a ring of two-slope stages with
+//   full/empty mbarriers and a rotating copy issuer; window offsets, modes,
+//   masks and weights are tabulated once per CTA.
+// * k_bwd_xgather applies the x taps and sums the views of a chunk into the
+//   volume (or an FP32 partial sum between chunks).
+//
+// Both do the float operations of k_bwd_tma in the same order (per voxel:
+// z taps over the live slopes in ascending v1, tap 0 then tap 1; x taps over
+// the views in order; the scale last), so the two paths agree bit for bit.
+// Every wait is bounded: a wait that gives up sets the device error word, the
+// CTA drains its copies in flight and returns without writing.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <string>
+
+#include "common.cuh"
+#include "projector.cuh"
+#include "shear.cuh"
+#include "storage.cuh"
+#include "tma.cuh"
+
+namespace petl {
+namespace shear {
+
+namespace {
+
+constexpr int GP = 4;               // planes per warp
+constexpr int GK = 8;               // rows per warp
+constexpr int GPG = 4;              // plane groups per CTA
+constexpr int GRG = 4;              // row groups per CTA
+constexpr int GPL = GP * GPG;       // planes per CTA
+constexpr int GROWS = GK * GRG;     // rows per CTA
+constexpr int GCOLS = 64;           // columns per CTA, two per lane
+constexpr int GWARPS = GPG * GRG;
+constexpr int GNT = 32 * GWARPS;
+constexpr int GDW = 2;              // largest shift difference among a warp's planes
+constexpr int GWN = GK + GDW + 1;   // register window rows
+constexpr int GNSMAX = 8;           // ring stages at most
+constexpr int GV1MAX = 128;         // slopes per call at most
+constexpr int GVG = 4;              // views per CTA at most
+constexpr int kPatGen = 15;         // no straight-line pattern: per-plane taps
+
+// Window offsets of a plane group's 4 planes when all are fully visible and
+// their shifts differ by at most one row: o0 | o1 << 2 | o2 << 4 | o3 << 6.
+constexpr int kNumPat = 7;
+__host__ __device__ constexpr int gpat_offsets(int pid)
+{
+    return pid == 0 ? 0x00 : pid == 1 ? 0x40 : pid == 2 ? 0x50 : pid == 3 ? 0x54
+         : pid == 4 ? 0x01 : pid == 5 ? 0x05 : 0x15;
+}
+
+// Entry of a (slope, warp).  code: plane modes and offsets (4 bits per
+// plane: mode 0 none / 1 full / 2 masked rows, offset << 2), path << 16
+// (0..6: the straight-line pattern of fully visible planes; 8..14: the same
+// pattern with per-plane row intervals; kPatGen: per-plane taps), window row
+// in the stage << 20.  vm: window rows holding visible bins (adjoint).  ivl:
+// per plane the output rows that receive the slope, first | last << 4 (8, 8
+// for none): the rows inside the visible range (adjoint) or passing the
+// voxel test (reference).
+struct __align__(16) GEntry {
+    uint32_t code;
+    uint32_t vm;
+    uint32_t ivl;
+    uint32_t pad;
+};
+constexpr uint32_t kIvlNone = 0x88u;
+
+struct ZgatherArgs {
+    petl_geom G;
+    ViewRange vr;
+    int vi0;       // first view of the chunk (index in vr)
+    int nvc;       // views in the chunk
+    int vg;        // views per CTA
+    int n_colblk;  // ceil(N_u0 / 64)
+    int n_rowblk;  // ceil(numZ / 32)
+    int brb;       // staged planogram rows per slope (33 + CTA shift spread, bounded on the host)
+    int ns;        // ring stages, two slopes each
+    int sstride;   // elements per staged slope (brb + 2 rows of 64; 128-byte multiple)
+    int NUc;       // scratch row pitch (columns)
+    int v1cap;     // slopes the per-CTA tables hold (the call's slope count)
+    Tables T;
+    int* err;
+};
+
+// z taps of one plane (two columns): Z[k] += w0 W[O + k + 1] then w1 W[O + k],
+// with per-row 0/1 masks when MASK (vm: window rows, om: output rows).
+template <int O, bool MASK>
+__device__ __forceinline__ void g_taps(float2 (&Z)[GK], const float2 (&W)[GWN], float w0, float w1, uint32_t vm,
+                                       uint32_t om)
+{
+    if (MASK) {
+#pragma unroll
+        for (int k = 0; k < GK; k++) {
+            const bool kb = (vm >> (O + k + 1)) & (om >> k) & 1u, ka = (vm >> (O + k)) & (om >> k) & 1u;
+            const float2 b = kb ? W[O + k + 1] : make_float2(0.0f, 0.0f);
+            const float2 a = ka ? W[O + k] : make_float2(0.0f, 0.0f);
+            Z[k] = make_float2(fmaf(w1, a.x, fmaf(w0, b.x, Z[k].x)), fmaf(w1, a.y, fmaf(w0, b.y, Z[k].y)));
+        }
+    } else {
+        const float2 a0 = dup(w0), a1 = dup(w1);
+#pragma unroll
+        for (int k = 0; k < GK; k++) Z[k] = fma2(a0, W[O + k + 1], Z[k]);
+#pragma unroll
+        for (int k = 0; k < GK; k++) Z[k] = fma2(a1, W[O + k], Z[k]);
+    }
+}
+
+template <int PID>
+__device__ __forceinline__ void g_taps4(float2 (&Z)[GP][GK], const float2 (&W)[GWN], float4 wa, float4 wb)
+{
+    constexpr int o = gpat_offsets(PID);
+    g_taps<(o >> 0) & 3, false>(Z[0], W, wa.x, wa.y, 0u, 0u);
+    g_taps<(o >> 2) & 3, false>(Z[1], W, wa.z, wa.w, 0u, 0u);
+    g_taps<(o >> 4) & 3, false>(Z[2], W, wb.x, wb.y, 0u, 0u);
+    g_taps<(o >> 6) & 3, false>(Z[3], W, wb.z, wb.w, 0u, 0u);
+}
+
+// z taps of one plane restricted to output rows ka..kb (predicated; rows
+// outside receive nothing, as the masked taps' zero operands give)
+template <int O>
+__device__ __forceinline__ void g_taps_ivl(float2 (&Z)[GK], const float2 (&W)[GWN], float w0, float w1,
+                                           uint32_t ivl)
+{
+    const int ka = int(ivl & 15u);
+    const unsigned span = unsigned(int((ivl >> 4) & 15u) - ka);
+    const float2 a0 = dup(w0), a1 = dup(w1);
+#pragma unroll
+    for (int k = 0; k < GK; k++)
+        if (unsigned(k - ka) <= span) Z[k] = fma2(a0, W[O + k + 1], Z[k]);
+#pragma unroll
+    for (int k = 0; k < GK; k++)
+        if (unsigned(k - ka) <= span) Z[k] = fma2(a1, W[O + k], Z[k]);
+}
+
+template <int PID>
+__device__ __forceinline__ void g_taps4_ivl(float2 (&Z)[GP][GK], const float2 (&W)[GWN], float4 wa, float4 wb,
+                                            uint32_t ivl)
+{
+    constexpr int o = gpat_offsets(PID);
+    g_taps_ivl<(o >> 0) & 3>(Z[0], W, wa.x, wa.y, ivl);
+    g_taps_ivl<(o >> 2) & 3>(Z[1], W, wa.z, wa.w, ivl >> 8);
+    g_taps_ivl<(o >> 4) & 3>(Z[2], W, wb.x, wb.y, ivl >> 16);
+    g_taps_ivl<(o >> 6) & 3>(Z[3], W, wb.z, wb.w, ivl >> 24);
+}
+
+// TG: planogram storage (float or bfloat16); B and the arithmetic are FP32.
+// Warp w: plane group w % 4, row group w / 4.
+template <bool ADJ, class TG>
+__global__ void __launch_bounds__(GNT, 1)
+k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, const ZgatherArgs A)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const petl_geom& G = A.G;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = warp % GPG, r = warp / GPG;
+    int t = blockIdx.x;
+    const int colblk = t % A.n_colblk;
+    t /= A.n_colblk;
+    const int rowblk = t % A.n_rowblk;
+    const int plblk = t / A.n_rowblk;
+    const int p0 = plblk * GPL, r0 = rowblk * GROWS, col0 = colblk * GCOLS;
+    const int z0 = r0 + r * GK;  // first row of this warp
+    const int vfirst = blockIdx.y * A.vg;
+    const int nvw = min(A.vg, A.nvc - vfirst);  // views of this CTA
+    const int NY = G.numY, NZ = G.numZ, NU1 = G.N_u1;
+    const int ns = A.ns;
+
+    TG* ringp = reinterpret_cast<TG*>(smem);                                           // [ns][2][sstride]
+    const int vcap = A.v1cap;
+    GEntry* s_ent = reinterpret_cast<GEntry*>(smem + size_t(ns) * 2 * A.sstride * sizeof(TG));  // [vcap][16]
+    float2* s_wt = reinterpret_cast<float2*>(s_ent + vcap * GWARPS);                    // [vg][vcap][16]
+    int2* s_sl = reinterpret_cast<int2*>(s_wt + size_t(A.vg) * vcap * GPL);             // (v1, first staged row)
+    uint64_t* full = reinterpret_cast<uint64_t*>(s_sl + vcap);                          // [GNSMAX]
+    uint64_t* empty = full + GNSMAX;                                                    // [GNSMAX]
+    int* s_n = reinterpret_cast<int*>(empty + GNSMAX);
+    volatile int* s_abort = s_n + 1;
+    int* s_round = s_n + 2;  // [GNSMAX]
+
+    // ---- slopes whose rows reach the tile (warp 0), compacted in order
+    if (warp == 0) {
+        int n = 0;
+        for (int vb = A.vr.iv1_begin; vb < A.vr.iv1_end; vb += 32) {
+            const int v1 = vb + lane;
+            bool ok = false;
+            int grow = 0;
+            if (v1 < A.vr.iv1_end) {
+                int dmin = 1 << 30, dmax = -(1 << 30);
+                for (int p = 0; p < GPL && p0 + p < NY; p++) {
+                    const int d = A.T.zt[size_t(v1) * NY + p0 + p].d;
+                    dmin = min(dmin, d);
+                    dmax = max(dmax, d);
+                }
+                grow = r0 - dmax - 1;
+                const int2 ub1 = A.T.ub1[v1];
+                for (int p = 0; p < GPL && p0 + p < NY && !ok; p++) {
+                    const int d = A.T.zt[size_t(v1) * NY + p0 + p].d;
+                    // rows of the CTA that can receive this slope on plane p
+                    const int lo = r0 - d - 1, hi = r0 + GROWS - 1 - d;
+                    if (hi < 0 || lo >= NU1) continue;
+                    if (ADJ) {
+                        ok = !(hi < ub1.x || lo > ub1.y);
+                    } else {
+                        const int2 zv = A.T.zvis[size_t(v1) * NY + p0 + p];
+                        ok = !(r0 + GROWS - 1 < zv.x || r0 > zv.y);
+                    }
+                }
+                if (ok && dmax - dmin > A.brb - (GROWS + 1)) {
+                    atomicOr(A.err, kErrLayout);
+                    ok = false;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            const int idx = n + __popc(bal & ((1u << lane) - 1u));
+            if (ok && idx < vcap) s_sl[idx] = make_int2(v1, grow);
+            n += __popc(bal);
+        }
+        if (lane == 0) {
+            if (n > vcap) {  // the host sizes the tables; never index past them
+                atomicOr(A.err, kErrLayout);
+                n = vcap;
+            }
+            s_n[0] = n;
+            *s_abort = 0;
+            for (int s = 0; s < ns; s++) {
+                mbar_init(&full[s], 1);
+                mbar_init(&empty[s], GWARPS);
+                s_round[s] = -1;
+            }
+            fence_barrier_init();
+        }
+    }
+    __syncthreads();
+    const int nlive = s_n[0];
+
+    // ---- per (slope, warp): plane modes, window offsets, pattern, masks
+    for (int e = tid; e < nlive * GWARPS; e += GNT) {
+        const int li = e / GWARPS, w = e - li * GWARPS;
+        const int wq = w % GPG, wr = w / GPG;
+        const int2 sl = s_sl[li];
+        const int v1 = sl.x, grow = sl.y;
+        const int zr = r0 + wr * GK;  // first row of warp w
+        const int2 ub1 = A.T.ub1[v1];
+        int dz[GP], mode[GP];
+        int2 zv[GP];
+        int dmx = -(1 << 30);
+#pragma unroll
+        for (int u = 0; u < GP; u++) {
+            const int y = p0 + wq * GP + u;
+            dz[u] = 0;
+            mode[u] = 0;
+            zv[u] = make_int2(0, -1);
+            if (y >= NY) continue;
+            dz[u] = A.T.zt[size_t(v1) * NY + y].d;
+            const int lo = zr - dz[u] - 1, hi = zr + GK - 1 - dz[u];  // g rows touched
+            if (hi < 0 || lo >= NU1) continue;
+            if (ADJ) {
+                if (hi < ub1.x || lo > ub1.y) continue;
+                mode[u] = (lo >= ub1.x && hi <= ub1.y) ? 1 : 2;
+            } else {
+                zv[u] = A.T.zvis[size_t(v1) * NY + y];
+                if (zr + GK - 1 < zv[u].x || zr > zv[u].y) continue;
+                mode[u] = (zr >= zv[u].x && zr + GK - 1 <= zv[u].y) ? 1 : 2;
+            }
+            dmx = max(dmx, dz[u]);
+        }
+        GEntry en{0u, 0u, 0u, 0u};
+        if (dmx != -(1 << 30)) {
+            const int wfirst = zr - dmx - 1;  // g row of window row 0
+            const int wrow = wfirst - grow;   // its row in the stage
+            bool bad = wrow < 0 || wrow + GWN > A.brb + 2;
+            uint32_t code = 0, ivl = 0, vm = 0;
+            bool allfull = true;
+            int offs = 0, olast = -1;
+            for (int i = 0; i < GWN; i++)
+                if (wfirst + i >= ub1.x && wfirst + i <= ub1.y) vm |= 1u << i;
+#pragma unroll
+            for (int u = 0; u < GP; u++) {
+                const int o = dmx - dz[u];
+                uint32_t iv = kIvlNone;
+                if (mode[u]) {
+                    if (o > GDW) bad = true;
+                    code |= uint32_t(mode[u] | (min(o, 3) << 2)) << (4 * u);
+                    if (ADJ || mode[u] == 1) {
+                        iv = 0x70u;  // rows 0..7 (adjoint: invisible window rows are zeroed instead)
+                    } else {
+                        const int ka = max(zv[u].x - zr, 0), kb = min(zv[u].y - zr, GK - 1);
+                        iv = uint32_t(ka) | uint32_t(kb) << 4;
+                    }
+                }
+                ivl |= iv << (8 * u);
+                allfull = allfull && mode[u] == 1;
+                // planes that receive nothing take a neighbour's offset
+                // (monotone), so that a pattern can cover the group
+                const int oe = mode[u] ? o : (olast >= 0 ? olast : dmx - dz[u]);
+                if (mode[u]) olast = o;
+                offs |= (min(oe, 3) & 3) << (2 * u);
+            }
+            // leading planes without rows: the offset of the first active one
+            if (!mode[0]) {
+                int ofirst = 0;
+                for (int u = GP - 1; u >= 0; u--)
+                    if (mode[u]) ofirst = dmx - dz[u];
+                for (int u = 0; u < GP && !mode[u]; u++) offs = (offs & ~(3 << (2 * u))) | ((ofirst & 3) << (2 * u));
+            }
+            int pid = kPatGen;
+            for (int c = 0; c < kNumPat; c++)
+                if (gpat_offsets(c) == offs) pid = allfull ? c : c + 8;
+            if (bad) {
+                atomicOr(A.err, kErrLayout);
+            } else {
+                en.code = code | uint32_t(pid) << 16 | uint32_t(wrow) << 20;
+                en.vm = vm;
+                en.ivl = ivl;
+            }
+        }
+        s_ent[li * GWARPS + w] = en;
+    }
+    // ---- weights (S (1 - w), S w) per view, slope and plane
+    for (int e = tid; e < nvw * nlive * GPL; e += GNT) {
+        const int k = e / (nlive * GPL), rem = e - k * (nlive * GPL);
+        const int li = rem / GPL, p = rem - li * GPL;
+        const int v1 = s_sl[li].x;
+        const int v0 = A.vr.iv0_first + (A.vi0 + vfirst + k) * A.vr.iv0_step;
+        const int y = min(p0 + p, NY - 1);
+        const float S = A.T.S[size_t(v1) * G.N_v0 + v0];
+        const float w = A.T.zt[size_t(v1) * NY + y].w;
+        s_wt[(k * vcap + li) * GPL + p] = make_float2(S * (1.0f - w), S * w);
+    }
+    __syncthreads();
+
+    // ---- the ring: stage j holds slopes 2p and 2p + 1 (p = j mod nsp) of view j / nsp
+    const int nsp = (nlive + 1) / 2;
+    const int nst = nvw * nsp;
+    const uint32_t box_bytes = uint32_t(GCOLS) * uint32_t(A.brb) * uint32_t(sizeof(TG));
+    bool dead = false;
+    // stage j reuses its slot once every warp has released stage j - ns
+    auto issue = [&](int j) {
+        const int slot = j % ns, round = j / ns;
+        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err)) return false;
+        if (*s_abort) return false;
+        fence_proxy_async_smem();
+        const int k = j / nsp, pr = j - k * nsp;
+        const int v0 = A.vr.iv0_first + (A.vi0 + vfirst + k) * A.vr.iv0_step;
+        const int np = min(2, nlive - 2 * pr);
+        mbar_arrive_expect_tx(&full[slot], box_bytes * uint32_t(np));
+        for (int h = 0; h < np; h++) {
+            const int2 sl = s_sl[2 * pr + h];
+            tma_load_4d(ringp + size_t(2 * slot + h) * A.sstride, &gmap, &full[slot], col0, sl.y, v0, sl.x);
+        }
+        s_round[slot] = round;
+        return true;
+    };
+    if (tid == 0)
+        for (int j = 0; j < ns - 1 && j < nst; j++) issue(j);
+    // the next stage this warp starts: the first j >= ns - 1 with j % 16 == warp
+    int my_next = warp + GWARPS * ((ns - 1 - warp + GWARPS - 1) / GWARPS);
+    if (my_next < ns - 1) my_next += GWARPS;
+
+    float2 Z[GP][GK];
+#pragma unroll
+    for (int u = 0; u < GP; u++)
+#pragma unroll
+        for (int k = 0; k < GK; k++) Z[u][k] = make_float2(0.0f, 0.0f);
+
+    // the z sums of view k go to the scratch (columns outside the view's
+    // visible u0 range zeroed for the adjoint) and restart from zero
+    auto store_view = [&](int k) {
+        const int vi = vfirst + k;
+        const int v0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
+        const int2 u0r = ADJ ? A.T.ub0[v0] : make_int2(0, G.N_u0 - 1);
+        const int c = col0 + 2 * lane;
+        const bool vx = c >= u0r.x && c <= u0r.y, vy = c + 1 >= u0r.x && c + 1 <= u0r.y;
+#pragma unroll
+        for (int u = 0; u < GP; u++) {
+            const int y = p0 + q * GP + u;
+#pragma unroll
+            for (int kk = 0; kk < GK; kk++) {
+                const int z = z0 + kk;
+                if (y < NY && z < NZ && c < G.N_u0) {
+                    float* dst = B + ((size_t(vi) * NY + y) * NZ + z) * A.NUc + c;
+                    const float2 v = make_float2(vx ? Z[u][kk].x : 0.0f, vy ? Z[u][kk].y : 0.0f);
+                    if (c + 1 < G.N_u0)
+                        __stcs(reinterpret_cast<float2*>(dst), v);
+                    else
+                        dst[0] = v.x;
+                }
+                Z[u][kk] = make_float2(0.0f, 0.0f);
+            }
+        }
+    };
+
+    int slot = 0;
+    uint32_t phase = 0;
+    int k = 0, pr = 0;  // view and slope pair of stage j
+    for (int j = 0; j < nst; j++) {
+        if (j + ns - 1 == my_next) {
+            if (lane == 0 && !dead && my_next < nst && !issue(my_next)) dead = true;
+            my_next += GWARPS;
+        }
+        if (!dead) dead = !mbar_wait(&full[slot], phase, A.err);
+        if (dead) *s_abort = 1;  // before this warp releases the slot
+#pragma unroll 1
+        for (int h = 0; h < 2 && !dead; h++) {
+            const int li = 2 * pr + h;
+            if (li >= nlive) break;
+            const GEntry en = s_ent[li * GWARPS + warp];
+            if (!(en.code & 0xffffu)) continue;
+            const TG* Gs = ringp + size_t(2 * slot + h) * A.sstride + (en.code >> 20) * GCOLS + 2 * lane;
+            float2 W[GWN];
+#pragma unroll
+            for (int i = 0; i < GWN; i++) W[i] = Store<TG>::ld2(Gs + i * GCOLS);
+            const float4* W4 = reinterpret_cast<const float4*>(s_wt + (size_t(k) * vcap + li) * GPL + q * GP);
+            const float4 wa = W4[0], wb = W4[1];
+            const uint32_t pid = (en.code >> 16) & 15u;
+            if (pid < 8u) {  // fully visible planes
+                switch (pid) {
+                    case 0: g_taps4<0>(Z, W, wa, wb); break;
+                    case 1: g_taps4<1>(Z, W, wa, wb); break;
+                    case 2: g_taps4<2>(Z, W, wa, wb); break;
+                    case 3: g_taps4<3>(Z, W, wa, wb); break;
+                    case 4: g_taps4<4>(Z, W, wa, wb); break;
+                    case 5: g_taps4<5>(Z, W, wa, wb); break;
+                    default: g_taps4<6>(Z, W, wa, wb); break;
+                }
+            } else if (pid != uint32_t(kPatGen)) {
+                // edge of the visible range: the adjoint zeroes the window
+                // rows outside the view, the reference keeps per-plane rows
+                if (ADJ) {
+#pragma unroll
+                    for (int i = 0; i < GWN; i++)
+                        if (!((en.vm >> i) & 1u)) W[i] = make_float2(0.0f, 0.0f);
+                }
+                switch (pid) {
+                    case 8: g_taps4_ivl<0>(Z, W, wa, wb, en.ivl); break;
+                    case 9: g_taps4_ivl<1>(Z, W, wa, wb, en.ivl); break;
+                    case 10: g_taps4_ivl<2>(Z, W, wa, wb, en.ivl); break;
+                    case 11: g_taps4_ivl<3>(Z, W, wa, wb, en.ivl); break;
+                    case 12: g_taps4_ivl<4>(Z, W, wa, wb, en.ivl); break;
+                    case 13: g_taps4_ivl<5>(Z, W, wa, wb, en.ivl); break;
+                    default: g_taps4_ivl<6>(Z, W, wa, wb, en.ivl); break;
+                }
+            } else {
+                const float w0s[GP] = {wa.x, wa.z, wb.x, wb.z}, w1s[GP] = {wa.y, wa.w, wb.y, wb.w};
+#pragma unroll
+                for (int u = 0; u < GP; u++) {
+                    const uint32_t c = (en.code >> (4 * u)) & 15u;
+                    if (!(c & 3u)) continue;
+                    const int o = int(c >> 2);
+                    if ((c & 3u) == 1u) {
+                        switch (o) {
+                            case 0: g_taps<0, false>(Z[u], W, w0s[u], w1s[u], 0u, 0u); break;
+                            case 1: g_taps<1, false>(Z[u], W, w0s[u], w1s[u], 0u, 0u); break;
+                            default: g_taps<2, false>(Z[u], W, w0s[u], w1s[u], 0u, 0u); break;
+                        }
+                    } else {
+                        // rows at the edge of the visible range: per-row masks
+                        const uint32_t iv = (en.ivl >> (8 * u)) & 0xffu;
+                        const uint32_t ka = iv & 15u, kb = iv >> 4;
+                        const uint32_t rows = kb >= ka && ka < 8u ? (0xffu >> (7u - kb)) & (0xffu << ka) : 0u;
+                        const uint32_t vm = ADJ ? en.vm : 0xffffffffu;
+                        const uint32_t om = ADJ ? 0xffffffffu : rows;
+                        switch (o) {
+                            case 0: g_taps<0, true>(Z[u], W, w0s[u], w1s[u], vm, om); break;
+                            case 1: g_taps<1, true>(Z[u], W, w0s[u], w1s[u], vm, om); break;
+                            default: g_taps<2, true>(Z[u], W, w0s[u], w1s[u], vm, om); break;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        if (++slot == ns) {
+            slot = 0;
+            phase ^= 1u;
+        }
+        if (pr == nsp - 1) {
+            if (!dead) store_view(k);
+            pr = 0;
+            k++;
+        } else {
+            pr++;
+        }
+    }
+    // a tile that no slope reaches still writes its (zero) sums
+    if (nsp == 0)
+        for (int k = 0; k < nvw; k++) store_view(k);
+    if (__syncthreads_or(dead)) {
+        // a wait gave up: drain the copies still in flight
+        if (tid == 0)
+            for (int s = 0; s < ns; s++)
+                if (s_round[s] >= 0) mbar_wait(&full[s], uint32_t(s_round[s] & 1), nullptr);
+    }
+}
+
+struct XgatherArgs {
+    petl_geom G;
+    ViewRange vr;
+    int vi0;         // first view of the chunk (index in vr)
+    int nvc;         // views in the chunk
+    int NUc;         // scratch row pitch
+    int first;       // first chunk: the view sums start at zero, else at the partial sum
+    int last;        // last chunk: write the volume, else the partial sum
+    int accumulate;  // add to the volume instead of overwriting it
+    float scale;
+    Tables T;
+};
+
+constexpr int XR = 4;         // volume rows z per k_bwd_xgather thread
+constexpr int XMAXN = 1024;   // longest scratch / volume row
+
+// x taps of a chunk of views into the volume: thread = column x of rows
+// z0..z0+7 of plane y, reading the two scratch taps of every view straight
+// from global memory (neighbouring threads share them through L1).  Grid
+// (ceil(numX / 256), ceil(numZ / 8), numY).
+__global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B, float* __restrict__ f,
+                                                     float* __restrict__ part, const XgatherArgs A)
+{
+    extern __shared__ Shift s_xs[];  // [nvc] x shifts of plane y
+    const petl_geom& G = A.G;
+    const int NY = G.numY, NZ = G.numZ, NX = G.numX, NU0 = G.N_u0, NUc = A.NUc;
+    const int x = blockIdx.x * 256 + threadIdx.x, z0 = blockIdx.y * XR, y = blockIdx.z;
+    for (int vi = threadIdx.x; vi < A.nvc; vi += 256)
+        s_xs[vi] = A.T.xt[size_t(A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step) * NY + y];
+    __syncthreads();
+    if (x >= NX) return;
+    const int nz = min(XR, NZ - z0);
+    float acc[XR];
+#pragma unroll
+    for (int r = 0; r < XR; r++)
+        acc[r] = (!A.first && r < nz) ? part[(size_t(z0 + r) * NY + y) * NX + x] : 0.0f;
+    const int rlast = nz - 1;
+#pragma unroll 4
+    for (int vi = 0; vi < A.nvc; vi++) {
+        const Shift xs = s_xs[vi];
+        const float wx1 = xs.w, wx0 = 1.0f - xs.w;
+        const int j0 = x - xs.d;  // scratch column of tap 0
+        const bool okm = unsigned(j0 - 1) < unsigned(NU0), ok0 = unsigned(j0) < unsigned(NU0);
+        // in-bounds addresses for every tap; the out-of-range ones are selected away
+        const int jm = min(max(j0 - 1, 0), NU0 - 1), jz = min(max(j0, 0), NU0 - 1);
+        const float* Bv = B + ((size_t(vi) * NY + y) * NZ + z0) * NUc;
+#pragma unroll
+        for (int r = 0; r < XR; r++) {
+            const int rr = min(r, rlast);
+            const float vm = __ldg(Bv + rr * NUc + jm), vz = __ldg(Bv + rr * NUc + jz);
+            acc[r] = acc[r] + fmaf(wx1, okm ? vm : 0.0f, wx0 * (ok0 ? vz : 0.0f));
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < XR; r++) {
+        if (r >= nz) break;
+        const size_t o = (size_t(z0 + r) * NY + y) * NX + x;
+        if (!A.last)
+            part[o] = acc[r];
+        else
+            f[o] = A.accumulate ? f[o] + A.scale * acc[r] : A.scale * acc[r];
+    }
+}
+
+size_t bsplit_scratch_budget()
+{
+    static size_t b = [] {
+        const char* e = std::getenv("PETL_SPLIT_SCRATCH_MB");
+        const long long mb = e ? std::atoll(e) : 0;
+        return mb > 0 ? size_t(mb) << 20 : size_t(1) << 30;
+    }();
+    return b;
+}
+
+}  // namespace
+
+template <class TG>
+int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int accumulate, float scale,
+                        const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    constexpr int EB = int(sizeof(TG));
+    const int n_v0 = vr.n_v0(G.N_v0);
+    const int nv1 = vr.iv1_end - vr.iv1_begin;
+    if (n_v0 <= 0 || nv1 <= 0 || nv1 > GV1MAX) return kNotApplicable;
+    // tensor map rows: a multiple of 16 bytes from a 16-byte aligned base
+    if ((G.N_u0 * EB) % 16 != 0 || (reinterpret_cast<uintptr_t>(g) & 15) != 0) return kNotApplicable;
+    if (G.N_u0 > XMAXN || G.numY > 65535 || G.numZ > 65535 * XR) return kNotApplicable;
+    const double step = double(std::max(std::fabs(G.v1_0), std::fabs(G.v1_0 + (G.N_v1 - 1) * G.T_v1))) *
+                        double(G.T_x) / double(G.T_z);  // shift change per plane
+    if (shift_spread(GP - 1, step) > GDW) return kNotApplicable;
+    const int brb = GROWS + 1 + shift_spread(GPL - 1, step);
+    if (brb > 254) return kNotApplicable;
+    int* err = device_error_ptr();
+    if (!err) return kNotApplicable;
+
+    ZgatherArgs A{};
+    A.G = G;
+    A.vr = vr;
+    A.n_colblk = int(ceil_div(G.N_u0, GCOLS));
+    A.n_rowblk = int(ceil_div(G.numZ, GROWS));
+    A.brb = brb;
+    A.sstride = (brb + 2) * GCOLS;  // a multiple of 64 elements: 128-byte aligned slopes
+    A.NUc = (G.N_u0 + 3) & ~3;
+    A.v1cap = nv1;
+    A.T = T;
+    A.err = err;
+
+    // chunks of views whose scratch fits the budget, balanced in size
+    const size_t per_view = size_t(G.numY) * G.numZ * A.NUc * 4;
+    int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), bsplit_scratch_budget() / per_view)));
+    nv = std::min(nv, 4096);  // k_bwd_xgather stages the chunk's x shifts in shared memory
+    const int nchunks = (n_v0 + nv - 1) / nv;
+    nv = (n_v0 + nchunks - 1) / nchunks;
+    A.vg = std::min(GVG, nv);
+
+    const size_t fixed = size_t(nv1) * GWARPS * sizeof(GEntry) + size_t(A.vg) * nv1 * GPL * 8 + size_t(nv1) * 8 +
+                         2 * GNSMAX * 8 + 8 + GNSMAX * 4;
+    const size_t stage = size_t(2) * A.sstride * EB;
+    A.ns = int(std::min<size_t>(GNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / stage));
+    if (A.ns < 2) return kNotApplicable;
+    const size_t smem = size_t(A.ns) * stage + fixed;
+
+    CUtensorMap map;
+    const uint64_t dims[4] = {uint64_t(G.N_u0), uint64_t(G.N_u1), uint64_t(G.N_v0), uint64_t(G.N_v1)};
+    const uint64_t strides[3] = {uint64_t(G.N_u0) * EB, uint64_t(G.N_u0) * G.N_u1 * EB,
+                                 uint64_t(G.N_u0) * G.N_u1 * G.N_v0 * EB};
+    const uint32_t box[4] = {uint32_t(GCOLS), uint32_t(brb), 1u, 1u};
+    if (!encode_tensor_map(&map, g, 4, dims, strides, box, EB)) return kNotApplicable;
+
+    float* B = nullptr;
+    float* part = nullptr;
+    const size_t nvox = size_t(G.numX) * G.numY * G.numZ;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&B), per_view * nv, st) != cudaSuccess ||
+        (nchunks > 1 && cudaMallocAsync(reinterpret_cast<void**>(&part), nvox * 4, st) != cudaSuccess)) {
+        cudaGetLastError();  // out of memory is not sticky: the caller takes the single-pass kernel
+        if (B) cudaFreeAsync(B, st);
+        return kNotApplicable;
+    }
+    const bool adj = mode == PETL_BP_ADJOINT;
+    auto kz = adj ? k_bwd_zgather<true, TG> : k_bwd_zgather<false, TG>;
+    cudaError_t e = cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const unsigned ntile = unsigned(A.n_colblk) * unsigned(A.n_rowblk) * ceil_div(G.numY, GPL);
+    for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
+        const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
+        A.vi0 = vi0;
+        A.nvc = nvc;
+        kz<<<dim3(ntile, ceil_div(nvc, A.vg)), GNT, smem, st>>>(map, B, A);
+        note_launch();
+        XgatherArgs X{G, vr, vi0, nvc, A.NUc, c == 0, c == nchunks - 1, accumulate, scale, T};
+        k_bwd_xgather<<<dim3(ceil_div(G.numX, 256), ceil_div(G.numZ, XR), unsigned(G.numY)), 256,
+                        size_t(nvc) * sizeof(Shift), st>>>(B, f, part, X);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(B, st);
+    if (part) cudaFreeAsync(part, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("backproject_split: ") + cudaGetErrorString(e));
+        return int(e);
+    }
+    return 0;
+}
+
+int backproject_split(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                      const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    return backproject_split_t<float>(G, g, f, mode, accumulate, scale, vr, T, st);
+}
+
+int backproject_split_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate,
+                           float scale, const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    return backproject_split_t<__nv_bfloat16>(G, g, f, mode, accumulate, scale, vr, T, st);
+}
+
+}  // namespace shear
+}  // namespace petl

@@ -986,6 +986,12 @@ int project_tma(const petl_geom& G, const float* f, float* g, const ViewRange& v
 int backproject_tma(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
                     const ViewRange& vr, const Tables& T, cudaStream_t st)
 {
+    // the split form (z-gather into scratch + x-gather) first; dispatch 3
+    // keeps the single-pass kernel
+    if (dispatch_mode() != 3) {
+        const int rc = backproject_split(G, g, f, mode, accumulate, scale, vr, T, st);
+        if (rc != kNotApplicable) return rc;
+    }
     return backproject_tma_t<float, float>(G, g, f, mode, accumulate, scale, vr, T, st);
 }
 
@@ -1002,6 +1008,10 @@ int project_tma_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* 
 int backproject_tma_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate, float scale,
                          const ViewRange& vr, const Tables& T, cudaStream_t st)
 {
+    if (dispatch_mode() != 3) {
+        const int rc = backproject_split_bf16(G, g, f, mode, accumulate, scale, vr, T, st);
+        if (rc != kNotApplicable) return rc;
+    }
     return backproject_tma_t<__nv_bfloat16, float>(G, g, f, mode, accumulate, scale, vr, T, st);
 }
 

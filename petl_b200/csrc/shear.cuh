@@ -55,6 +55,15 @@ int project_split(const petl_geom& G, const float* f, float* g, const ViewRange&
                   const Tables& T, cudaStream_t st);
 int project_split_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
                        const __nv_bfloat16* meas, const Tables& T, cudaStream_t st);
+// Split backprojection (backprojector_split.cu): a z-gather kernel per chunk
+// of views into FP32 scratch, then an x-gather pass that sums the views into
+// the volume.  Same operator and the same float operations in the same order
+// as backproject_tma; kNotApplicable when the layout rules or the scratch
+// allocation fail.
+int backproject_split(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                      const ViewRange& vr, const Tables& T, cudaStream_t st);
+int backproject_split_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate,
+                           float scale, const ViewRange& vr, const Tables& T, cudaStream_t st);
 
 // Bytes of the shift tables of G (make_tables' allocation).
 size_t table_bytes(const petl_geom& G);

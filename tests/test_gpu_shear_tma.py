@@ -6,10 +6,11 @@ Dispatch 0 runs the TMA-staged kernels wherever their layout rules hold
 N_u0 a multiple of 4 and at most 256 with a tensor map, else any even N_u0
 up to 512 with bulk copies of row pairs), with the split forward (x-shift
 pass into scratch, then the z-tap kernel); dispatch 3 the same with the
-single-kernel TMA forward; dispatch 2 runs the first-generation shear
-kernels; dispatch 1 the general kernels.  The split and single-kernel
-forwards do the same float operations in the same order and agree bit for
-bit; the forward TMA kernels and the first-generation one agree to rounding
+single-kernel TMA forward and single-pass TMA backprojection; dispatch 2
+runs the first-generation shear kernels; dispatch 1 the general kernels.
+The split and single-kernel forms (forward, and backward where the planogram
+rows are multiples of 16 bytes) do the same float operations in the same
+order and agree bit for bit; the forward TMA kernels and the first-generation one agree to rounding
 of the final scale; the backward kernels sum in a different order and agree
 to float accuracy.  Every case also checks that no
 bounded wait gave up (petl_device_error_flag) and which kernels ran.
@@ -106,7 +107,10 @@ def test_tma_backward(cuda, name, mode):
     a, pa = _under(0, lambda: _np(ops.backproject(G, y, mode=mode)))
     b, pb = _under(2, lambda: _np(ops.backproject(G, y, mode=mode)))
     c, pc = _under(1, lambda: _np(ops.backproject(G, y, mode=mode)))
-    assert (pa, pb, pc) == (2 if CASES[name][3] else 1, 1, 0)
+    d, pd = _under(3, lambda: _np(ops.backproject(G, y, mode=mode)))
+    assert (pa, pb, pc, pd) == (2 if CASES[name][3] else 1, 1, 0, pa)
+    # the split backprojection and the single-pass TMA kernel agree bit for bit
+    assert np.array_equal(a, d)
     assert rel_l2(a, b) < 1e-5
     assert rel_l2(a, c) < 1e-5
     if mode == "reference" and G.shape[0] * G.shape[1] * G.shape[2] * G.shape[3] < 3e6:
@@ -132,6 +136,7 @@ def test_tma_subsets_slabs_ratio_accumulate(cuda):
     from petl_b200 import ops
     G, _, f, rng = _setup("panel2mm", cuda)
     ft = _t(f, cuda)
+    y = _t(rng.random(G.shape), cuda)
 
     def run():
         full = ops.project(G, ft)
@@ -143,7 +148,6 @@ def test_tma_subsets_slabs_ratio_accumulate(cuda):
         ops.project(G, ft, slabs, v1_range=(5, G.shape[0]))
         meas = torch.poisson(full * 20.0, generator=torch.Generator(device=full.device).manual_seed(3))
         ratio = ops.project_ratio(G, ft, meas)
-        y = _t(rng.random(G.shape), cuda)
         b = ops.backproject(G, y)
         b2 = ops.backproject(G, y, subset=(0, 3))
         for s in (1, 2):
@@ -155,10 +159,14 @@ def test_tma_subsets_slabs_ratio_accumulate(cuda):
 
     (full, parts, slabs, meas, ratio, b, b2, b3, b4), path = _under(0, run)
     assert path == 2
-    (full3, parts3, slabs3, _, ratio3, *_), path3 = _under(3, run)
+    (full3, parts3, slabs3, _, ratio3, b_3, b2_3, b3_3, b4_3), path3 = _under(3, run)
     assert path3 == 2
     assert torch.equal(full, full3) and torch.equal(parts, parts3) and torch.equal(slabs, slabs3)
     assert torch.equal(ratio, ratio3)
+    assert torch.equal(b, b_3)
+    assert torch.equal(b2, b2_3)
+    assert torch.equal(b3, b3_3)
+    assert torch.equal(b4, b4_3)
     assert torch.equal(full, parts)
     assert torch.equal(full, slabs)
     want = torch.where(full == 0, torch.zeros_like(full), meas / full)
@@ -185,5 +193,7 @@ def test_tma_full_size_against_first_generation(cuda):
     for mode in ("reference", "adjoint"):
         x, px = _under(0, lambda: ops.backproject(G, a, mode=mode))
         z, pz = _under(2, lambda: ops.backproject(G, a, mode=mode))
-        assert (px, pz) == (2, 1)
+        w, pw = _under(3, lambda: ops.backproject(G, a, mode=mode))
+        assert (px, pz, pw) == (2, 1, 2)
+        assert torch.equal(x, w)
         assert float(torch.linalg.vector_norm(x - z) / torch.linalg.vector_norm(z)) < 1e-5
