@@ -576,15 +576,6 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
     }
 }
 
-size_t bsplit_scratch_budget()
-{
-    static size_t b = [] {
-        const char* e = std::getenv("PETL_SPLIT_SCRATCH_MB");
-        const long long mb = e ? std::atoll(e) : 0;
-        return mb > 0 ? size_t(mb) << 20 : size_t(1) << 30;
-    }();
-    return b;
-}
 
 }  // namespace
 
@@ -621,7 +612,7 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
 
     // chunks of views whose scratch fits the budget, balanced in size
     const size_t per_view = size_t(G.numY) * G.numZ * A.NUc * 4;
-    int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), bsplit_scratch_budget() / per_view)));
+    int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), split_scratch_budget() / per_view)));
     nv = std::min(nv, 4096);  // k_bwd_xgather stages the chunk's x shifts in shared memory
     const int nchunks = (n_v0 + nv - 1) / nv;
     nv = (n_v0 + nchunks - 1) / nchunks;
@@ -644,8 +635,8 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     float* B = nullptr;
     float* part = nullptr;
     const size_t nvox = size_t(G.numX) * G.numY * G.numZ;
-    if (cudaMallocAsync(reinterpret_cast<void**>(&B), per_view * nv, st) != cudaSuccess ||
-        (nchunks > 1 && cudaMallocAsync(reinterpret_cast<void**>(&part), nvox * 4, st) != cudaSuccess)) {
+    if (scratch_alloc(reinterpret_cast<void**>(&B), per_view * nv, st) != cudaSuccess ||
+        (nchunks > 1 && scratch_alloc(reinterpret_cast<void**>(&part), nvox * 4, st) != cudaSuccess)) {
         cudaGetLastError();  // out of memory is not sticky: the caller takes the single-pass kernel
         if (B) cudaFreeAsync(B, st);
         return kNotApplicable;

@@ -39,6 +39,7 @@ int petl_gaussian_filter_dev(float* f, int N1, int N2, int N3, float FWHM, int n
 
 namespace petl {
 int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream_t st, float* host_rebinned_out);
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
 }
 
 namespace {
@@ -159,7 +160,7 @@ struct DevBuf {
     bool alloc(size_t bytes, cudaStream_t s)
     {
         st = s;
-        return cudaMallocAsync(&p, bytes ? bytes : 4, s) == cudaSuccess;
+        return petl::scratch_alloc(&p, bytes ? bytes : 4, s) == cudaSuccess;
     }
     ~DevBuf()
     {

@@ -54,6 +54,10 @@ inline unsigned ceil_div(long long a, long long b) { return unsigned((a + b - 1)
 // Number of SMs on the current device (cached per device).
 int sm_count();
 
+// Stream-ordered scratch from the library's own memory pool on the current
+// device, which keeps freed blocks for reuse (free with cudaFreeAsync).
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
+
 // Geometry sanity check shared by the entry points.
 bool geom_valid(const petl_geom* G, std::string* why);
 

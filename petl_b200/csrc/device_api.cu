@@ -77,7 +77,7 @@ int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream
     petl_geom Gr = G;
     const size_t nreb = size_t(G.N_v0) * G.N_u1 * G.N_u0;
     float* reb = nullptr;
-    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&reb), sizeof(float) * nreb, st));
+    PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(&reb), sizeof(float) * nreb, st));
     int rc = 0;
     if (G.N_v1 > 1) {
         // PETL::doFBP -> doPFDR, then the rebinned geometry (src/petl.cpp:379-380)
@@ -169,7 +169,7 @@ int petl_project_nnz_dev(const petl_geom* G, double* nnz_host, void* stream)
     PETL_REQUIRE(G && nnz_host && geom_valid(G, &why), "project_nnz: invalid arguments " + why);
     cudaStream_t st = as_stream(stream);
     unsigned long long* d = nullptr;
-    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(unsigned long long), st));
+    PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(&d), sizeof(unsigned long long), st));
     PETL_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), st));
     int rc = launch_count_nnz(*G, d, st);
     unsigned long long h = 0;

@@ -7,6 +7,7 @@
 // start values come out bit-identical.
 #include <algorithm>
 #include <atomic>
+#include <cstdint>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -36,6 +37,38 @@ int sm_count()
         cached[dev] = n;
     }
     return cached[dev];
+}
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st)
+{
+    // one library pool per device that keeps freed blocks (release threshold
+    // at its maximum): a pool that hands memory back to the system at each
+    // synchronisation would map gigabytes of projector scratch anew per call
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t created = nullptr;
+            e = cudaMemPoolCreate(&created, &props);
+            if (e != cudaSuccess) return e;
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &thr);
+            pools[dev] = created;
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
 }
 
 bool geom_valid(const petl_geom* G, std::string* why)

@@ -344,7 +344,7 @@ int shear::make_tables(const petl_geom& G, TableBuf& tb, cudaStream_t st)
     const size_t b_xt = al(nx * sizeof(Shift)), b_zt = al(nz * sizeof(Shift)), b_S = al(ns * 4),
                  b_zv = al(nz * sizeof(int2)), b_u0 = al(G.N_v0 * sizeof(int2)), b_u1 = al(G.N_v1 * sizeof(int2));
     tb.bytes = b_xt + b_zt + b_S + b_zv + b_u0 + b_u1;
-    PETL_CUDA(cudaMallocAsync(&tb.base, tb.bytes, st));
+    PETL_CUDA(scratch_alloc(&tb.base, tb.bytes, st));
     char* p = static_cast<char*>(tb.base);
     tb.T.xt = reinterpret_cast<Shift*>(p);
     p += b_xt;

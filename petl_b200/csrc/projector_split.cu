@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -404,15 +405,6 @@ k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, TG* __restrict__ g, const T
 
 // Scratch budget of the x-shift pass (bytes of FP32 X per chunk of views);
 // PETL_SPLIT_SCRATCH_MB overrides it.
-size_t split_scratch_budget()
-{
-    static size_t b = [] {
-        const char* e = std::getenv("PETL_SPLIT_SCRATCH_MB");
-        const long long mb = e ? std::atoll(e) : 0;
-        return mb > 0 ? size_t(mb) << 20 : size_t(1) << 30;
-    }();
-    return b;
-}
 
 // Launch layout of k_fwd_zsum for one range of slope blocks.
 struct ZsumLaunch {
@@ -458,6 +450,34 @@ bool zsum_layout(const petl_geom& G, const ViewRange& vr, int v1_first, int v1_e
 
 }  // namespace
 
+size_t split_scratch_budget()
+{
+    static const long long env_mb = [] {
+        const char* e = std::getenv("PETL_SPLIT_SCRATCH_MB");
+        return e ? std::atoll(e) : 0LL;
+    }();
+    if (env_mb > 0) return size_t(env_mb) << 20;
+    // the device's memory size, looked up once per device (a query per call
+    // would cost host time on the launch path)
+    static std::mutex mu;
+    static size_t total[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return size_t(1) << 30;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!total[dev]) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return size_t(1) << 30;
+        }
+        total[dev] = prop.totalGlobalMem;
+    }
+    return std::min(size_t(5) << 30, total[dev] / 8);
+}
+
 template <class TF, class TG>
 int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr, const TG* meas, const Tables& T,
                     cudaStream_t st)
@@ -480,7 +500,7 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     nv = (n_v0 + nchunks - 1) / nchunks;
 
     float* X = nullptr;
-    if (cudaMallocAsync(reinterpret_cast<void**>(&X), per_view * nv, st) != cudaSuccess) {
+    if (scratch_alloc(reinterpret_cast<void**>(&X), per_view * nv, st) != cudaSuccess) {
         cudaGetLastError();  // out of memory is not sticky: the caller takes the fused kernel
         return kNotApplicable;
     }

@@ -256,7 +256,7 @@ k_ramp(float* __restrict__ g, int nrows, int N, int rows_per_view, const float* 
 template <class T>
 int upload(const std::vector<T>& v, T** d, cudaStream_t st)
 {
-    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d), sizeof(T) * v.size(), st));
+    PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(d), sizeof(T) * v.size(), st));
     PETL_CUDA(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
     return 0;
 }

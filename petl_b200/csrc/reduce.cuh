@@ -48,7 +48,7 @@ int reduce_sum(Term term, long long n, double* out, cudaStream_t st, const char*
     const long long want = (n + 255) / 256;
     const int nb = int(want < 1 ? 1 : (want > 4LL * sm_count() ? 4LL * sm_count() : want));
     double* part = nullptr;
-    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * nb, st));
+    PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(&part), sizeof(double) * nb, st));
     k_reduce_partial<<<nb, 256, 0, st>>>(term, n, part);
     note_launch();
     cudaError_t e = cudaGetLastError();

@@ -299,7 +299,7 @@ int launch_gaussian(float* f, int N1, int N2, int N3, float FWHM, int numDims, c
     const float denom = 1.0f / (2.0f * sigma);
     const size_t n = size_t(N1) * N2 * N3;
     float* tmp = nullptr;
-    PETL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp), sizeof(float) * n, st));
+    PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(&tmp), sizeof(float) * n, st));
     dim3 block(32, 8, 1), grid(ceil_div(N3, 32), ceil_div(N2, 8), unsigned(N1));
     int axes[3], na = 0;
     if (numDims == 1) axes[na++] = 0;

@@ -96,7 +96,12 @@ struct Request {
 size_t footprint(const petl_geom& G, int subsets)
 {
     const size_t ng = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0, nv = size_t(G.numX) * G.numY * G.numZ;
-    return 4 * (2 * ng + (2 + size_t(subsets)) * nv) + shear::table_bytes(G) + (size_t(1) << 20);
+    // the split projector's scratch for the views of one subset step (one
+    // volume-sized FP32 array per view, capped by the per-call budget)
+    const size_t views = (size_t(G.N_v0) + size_t(subsets) - 1) / size_t(subsets);
+    const size_t per_view = size_t(G.numY) * G.numZ * ((size_t(G.N_u0) + 3) & ~size_t(3)) * 4;
+    const size_t scratch = std::min(views * per_view, std::max(per_view, shear::split_scratch_budget()));
+    return 4 * (2 * ng + (2 + size_t(subsets)) * nv) + shear::table_bytes(G) + scratch + (size_t(1) << 20);
 }
 
 }  // namespace
@@ -148,11 +153,11 @@ bool Server::admit(Request& r)
         fail(r, "cannot create a stream");
         return false;
     }
-    bool ok = cudaMallocAsync(reinterpret_cast<void**>(&r.g), ng * 4, r.st) == cudaSuccess &&
-              cudaMallocAsync(reinterpret_cast<void**>(&r.ratio), ng * 4, r.st) == cudaSuccess &&
-              cudaMallocAsync(reinterpret_cast<void**>(&r.f), nv * 4, r.st) == cudaSuccess &&
-              cudaMallocAsync(reinterpret_cast<void**>(&r.d), nv * 4, r.st) == cudaSuccess &&
-              cudaMallocAsync(reinterpret_cast<void**>(&r.sens), nv * 4 * r.subsets, r.st) == cudaSuccess &&
+    bool ok = scratch_alloc(reinterpret_cast<void**>(&r.g), ng * 4, r.st) == cudaSuccess &&
+              scratch_alloc(reinterpret_cast<void**>(&r.ratio), ng * 4, r.st) == cudaSuccess &&
+              scratch_alloc(reinterpret_cast<void**>(&r.f), nv * 4, r.st) == cudaSuccess &&
+              scratch_alloc(reinterpret_cast<void**>(&r.d), nv * 4, r.st) == cudaSuccess &&
+              scratch_alloc(reinterpret_cast<void**>(&r.sens), nv * 4 * r.subsets, r.st) == cudaSuccess &&
               cudaHostAlloc(reinterpret_cast<void**>(&r.out_host), nv * 4, cudaHostAllocDefault) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(r.g, r.g_host, ng * 4, cudaMemcpyHostToDevice, r.st) == cudaSuccess;
     r.shear = shear_eligible(G);

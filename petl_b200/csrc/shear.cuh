@@ -47,6 +47,11 @@ inline double plane_ymax(const petl_geom& G)
 // at most floor(n * step) + 1 (with a relative margin for the float inputs).
 inline int shift_spread(int n, double step) { return int(std::floor(double(n) * step * (1.0 + 1e-6))) + 1; }
 
+// Bytes of FP32 scratch one split projection call may hold (its chunk of
+// views): PETL_SPLIT_SCRATCH_MB, else 5 GiB, at most an eighth of the
+// device's memory.
+size_t split_scratch_budget();
+
 // Split forward projection (projector_split.cu): an x-shift pass per chunk of
 // views into FP32 scratch, then a z-tap kernel fed by a TMA ring.  Same
 // operator and the same float operations in the same order as project_tma.
