@@ -127,6 +127,9 @@ struct ZsumArgs {
     int nrb;       // staged rows per plane (rows per CTA + CTA shift spread + 1, bounded on the host)
     int ns;        // ring stages, two planes each
     int pstride;   // floats per staged plane (nrb + ZDMAX rows of 64; a multiple of 32)
+    // shared-memory layout (byte offsets, set by the host): weights, codes,
+    // live planes, barriers
+    unsigned off_w, off_code, off_plane, off_bar;
     Tables T;
     int* err;
 };
@@ -171,12 +174,12 @@ k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, TG* __restrict__ g, const T
     const int NY = G.numY, NZ = G.numZ, NX = G.numX;
     const int ns = A.ns, npl = min(NY, ZMAXPLANES);
 
-    float* ringp = reinterpret_cast<float*>(smem);                                     // [ns][2][pstride]
-    float4* s_w1 = reinterpret_cast<float4*>(smem + size_t(ns) * 2 * A.pstride * 4);    // [npl][4]
-    uint32_t* s_code = reinterpret_cast<uint32_t*>(s_w1 + size_t(npl) * 4);            // [npl][4]
-    int2* s_plane = reinterpret_cast<int2*>(s_code + size_t(npl) * 4);                 // (y, first staged row)
-    uint64_t* full = reinterpret_cast<uint64_t*>(s_plane + npl);                       // [ZNSMAX]
-    uint64_t* empty = full + ZNSMAX;                                                   // [ZNSMAX]
+    float* ringp = reinterpret_cast<float*>(smem);                      // [ns][2][pstride]
+    float4* s_w1 = reinterpret_cast<float4*>(smem + A.off_w);            // [npl][4]
+    uint32_t* s_code = reinterpret_cast<uint32_t*>(smem + A.off_code);   // [npl][4]
+    int2* s_plane = reinterpret_cast<int2*>(smem + A.off_plane);         // [npl] (y, first staged row)
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + A.off_bar);      // [ZNSMAX]
+    uint64_t* empty = full + ZNSMAX;                                     // [ZNSMAX]
     int* s_n = reinterpret_cast<int*>(empty + ZNSMAX);
     volatile int* s_abort = s_n + 1;  // a consumer gave up a wait: start no further copies
     int* s_round = s_n + 2;           // [ZNSMAX] round of the copy last started in a slot
@@ -435,12 +438,22 @@ bool zsum_layout(const petl_geom& G, const ViewRange& vr, int v1_first, int v1_e
     A.pstride = ((nrb + ZDMAX) * ZCOLS + 31) & ~31;  // 128-byte aligned planes
     A.T = T;
     A.err = err;
-    const int np = std::min(G.numY, ZMAXPLANES);
-    const size_t fixed = size_t(np) * 4 * (16 + 4) + size_t(np) * 8 + 2 * ZNSMAX * 8 + 8 + ZNSMAX * 4;
+    // shared memory: the ring, then the per-CTA tables and the barriers
+    const size_t np = size_t(std::min(G.numY, ZMAXPLANES));
+    const size_t b_w = np * 4 * sizeof(float4), b_code = np * 4 * 4, b_plane = np * 8;
+    const size_t b_bar = 2 * ZNSMAX * 8 + (2 + ZNSMAX) * 4;
+    auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+    const size_t fixed = al(b_w) + al(b_code) + al(b_plane) + al(b_bar);
     const size_t stage = size_t(2) * A.pstride * 4;
     A.ns = int(std::min<size_t>(ZNSMAX, (227 * 1024 - std::min<size_t>(fixed, 227 * 1024)) / stage));
     if (A.ns < 2) return false;
-    L.smem = size_t(A.ns) * stage + fixed;
+    const size_t ring = size_t(A.ns) * stage;
+    A.off_w = unsigned(ring);
+    A.off_code = unsigned(A.off_w + al(b_w));
+    A.off_plane = unsigned(A.off_code + al(b_code));
+    A.off_bar = unsigned(A.off_plane + al(b_plane));
+    L.smem = A.off_bar + al(b_bar);
+    if (L.smem > 227 * 1024) return false;
     L.nblk = unsigned(A.n_colblk) * unsigned(A.n_rowblk) * ceil_div(v1_end - v1_first, ZV * sg);
     const uint64_t dims[4] = {uint64_t(NXc), uint64_t(G.numZ), uint64_t(G.numY), uint64_t(nv)};
     const uint64_t strides[3] = {uint64_t(NXc) * 4, uint64_t(NXc) * G.numZ * 4, uint64_t(NXc) * G.numZ * G.numY * 4};

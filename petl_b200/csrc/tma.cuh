@@ -20,7 +20,7 @@ enum : int {
 };
 int* device_error_ptr();
 
-constexpr unsigned kWaitLimit = 1u << 26;
+constexpr unsigned kWaitLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
