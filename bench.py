@@ -13,10 +13,13 @@ the reference publishes no benchmark data set.
   write) between steps, outside the timed events.
 * ``e2e``: the same steps through the reference-compatible C ABI
   (project / backproject on pinned host arrays), host<->device copies inside.
-* ``roofline``: the dominant kernel's algorithmic bytes (volume + planogram,
-  read once and written once) per launch against measured HBM bandwidth;
-  ``fp32`` adds the binding figure, 2*nnz(A) flops per launch against the
-  nominal FP32 rate at the measured clock.
+* ``roofline``: the dominant projection call (forward: x-shift pass +
+  z-tap kernel; backward: z-gather kernel + x-gather pass, one launch each
+  per chunk of views, one chunk at this size): its algorithmic bytes
+  (volume + planogram, read once and written once) per call against
+  measured HBM bandwidth, and the call's DRAM traffic from the committed ncu
+  capture; ``fp32`` adds the binding figure, 2*nnz(A) flops per call against
+  the nominal FP32 rate at the measured clock.
 * ``cpu_baseline``: the FP32 CPU restatement (oracle) on all host cores, on
   a bounded sample (a few v1 slices), scaled to a full step.
 
