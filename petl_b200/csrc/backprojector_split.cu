@@ -581,7 +581,7 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
 
 template <class TG>
 int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int accumulate, float scale,
-                        const ViewRange& vr, const Tables& T, cudaStream_t st)
+                        const ViewRange& vr, const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
     constexpr int EB = int(sizeof(TG));
     const int n_v0 = vr.n_v0(G.N_v0);
@@ -614,6 +614,7 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     const size_t per_view = size_t(G.numY) * G.numZ * A.NUc * 4;
     int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), split_scratch_budget() / per_view)));
     nv = std::min(nv, 4096);  // k_bwd_xgather stages the chunk's x shifts in shared memory
+    if (chunk_cap > 0) nv = std::min(nv, chunk_cap);
     const int nchunks = (n_v0 + nv - 1) / nv;
     nv = (n_v0 + nchunks - 1) / nchunks;
     A.vg = std::min(GVG, nv);
@@ -647,6 +648,7 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     const unsigned ntile = unsigned(A.n_colblk) * unsigned(A.n_rowblk) * ceil_div(G.numY, GPL);
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
+        if (hook && hook->fn) hook->fn(hook->ctx, vi0, nvc);
         A.vi0 = vi0;
         A.nvc = nvc;
         kz<<<dim3(ntile, ceil_div(nvc, A.vg)), GNT, smem, st>>>(map, B, A);
@@ -667,15 +669,15 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
 }
 
 int backproject_split(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
-                      const ViewRange& vr, const Tables& T, cudaStream_t st)
+                      const ViewRange& vr, const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
-    return backproject_split_t<float>(G, g, f, mode, accumulate, scale, vr, T, st);
+    return backproject_split_t<float>(G, g, f, mode, accumulate, scale, vr, T, st, chunk_cap, hook);
 }
 
 int backproject_split_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate,
                            float scale, const ViewRange& vr, const Tables& T, cudaStream_t st)
 {
-    return backproject_split_t<__nv_bfloat16>(G, g, f, mode, accumulate, scale, vr, T, st);
+    return backproject_split_t<__nv_bfloat16>(G, g, f, mode, accumulate, scale, vr, T, st, 0, nullptr);
 }
 
 }  // namespace shear

@@ -40,7 +40,18 @@ int petl_gaussian_filter_dev(float* f, int N1, int N2, int N3, float FWHM, int n
 namespace petl {
 int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream_t st, float* host_rebinned_out);
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
-}
+namespace shear {
+struct ChunkHook {
+    void (*fn)(void* ctx, int vi0, int nvc) = nullptr;
+    void* ctx = nullptr;
+};
+constexpr int kNotApplicable = -2;
+int project_chunked(const petl_geom& G, const float* f, float* g, int chunk_cap, const ChunkHook& hook,
+                    cudaStream_t st);
+int backproject_chunked(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                        int chunk_cap, const ChunkHook& hook, cudaStream_t st);
+}  // namespace shear
+}  // namespace petl
 
 namespace {
 
@@ -169,8 +180,47 @@ struct DevBuf {
     float* f() const { return static_cast<float*>(p); }
 };
 
-// v1 slices per pipeline stage: a multiple of 16 (the slopes one forward
-// CTA covers, so no stage launches part-empty tiles) moving up to ~256 MB
+// Views per pipeline stage of the split projectors: each stage's planogram
+// views move across PCIe while the next stage computes.
+constexpr int kChunkViews = 16;
+
+// Copies views [vi0, vi0 + nvc) of every slope of a planogram between host
+// and device (a strided block: one row of views per slope), on `copy`,
+// ordered after the work enqueued so far on `compute` (device to host) or
+// followed by a wait of `compute` (host to device).
+struct ViewCopy {
+    petl_geom G;
+    float* host;
+    float* dev;
+    cudaStream_t compute, copy;
+    bool to_host;
+    bool ok = true;
+    static void run(void* ctx, int vi0, int nvc)
+    {
+        ViewCopy& c = *static_cast<ViewCopy*>(ctx);
+        const size_t vb = size_t(c.G.N_u1) * c.G.N_u0 * 4, pitch = vb * c.G.N_v0, off = (size_t(vi0) * vb) / 4;
+        cudaEvent_t ev;
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (c.to_host) {
+            cudaEventRecord(ev, c.compute);
+            cudaStreamWaitEvent(c.copy, ev, 0);
+            c.ok = c.ok && cuda_ok("project D2H", cudaMemcpy2DAsync(c.host + off, pitch, c.dev + off, pitch,
+                                                                    vb * nvc, c.G.N_v1, cudaMemcpyDeviceToHost,
+                                                                    c.copy));
+        } else {
+            c.ok = c.ok && cuda_ok("backproject H2D", cudaMemcpy2DAsync(c.dev + off, pitch, c.host + off, pitch,
+                                                                        vb * nvc, c.G.N_v1, cudaMemcpyHostToDevice,
+                                                                        c.copy));
+            cudaEventRecord(ev, c.copy);
+            cudaStreamWaitEvent(c.compute, ev, 0);
+        }
+        cudaEventDestroy(ev);
+    }
+};
+
+// v1 slices per pipeline stage of the other projectors: a multiple of 16
+// (the slopes one forward CTA covers, so no stage launches part-empty
+// tiles) moving up to ~256 MB
 int slab_step(const petl_geom& G)
 {
     const double slab_bytes = double(G.N_v0) * G.N_u1 * G.N_u0 * 4.0;
@@ -453,8 +503,14 @@ bool project(float** g, float* f)
         const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0;
         DevBuf dg;
         if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
+        // split kernels: each chunk of views goes back while the next computes
+        ViewCopy vc{G, g[i], dg.f(), c->compute, c->copy, true};
+        const petl::shear::ChunkHook hook{&ViewCopy::run, &vc};
+        const int rc = petl::shear::project_chunked(G, df.f(), dg.f(), kChunkViews, hook, c->compute);
+        const bool split = rc != petl::shear::kNotApplicable;
+        if (split) ok = report("project", rc) && vc.ok;
         const int step = slab_step(G);
-        for (int b = 0; b < G.N_v1 && ok; b += step) {
+        for (int b = split ? G.N_v1 : 0; b < G.N_v1 && ok; b += step) {
             const int e = std::min(G.N_v1, b + step);
             ok = report("project", petl_project_range_dev(&G, df.f(), dg.f(), b, e, 0, 1, c->compute));
             cudaEvent_t ev;
@@ -498,8 +554,18 @@ static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weig
         cudaEventRecord(ready, c->compute);
         cudaStreamWaitEvent(c->copy, ready, 0);
         cudaEventDestroy(ready);
+        // split kernels: each chunk of views computes while the next comes in
+        ViewCopy vc{G, g[i], dg.f(), c->compute, c->copy, false};
+        const petl::shear::ChunkHook hook{&ViewCopy::run, &vc};
+        const int rc = petl::shear::backproject_chunked(G, dg.f(), df.f(), PETL_BP_REFERENCE, first ? 0 : 1, 1.0f,
+                                                        kChunkViews, hook, c->compute);
+        const bool split = rc != petl::shear::kNotApplicable;
+        if (split) {
+            ok = report("backproject", rc) && vc.ok;
+            first = false;
+        }
         const int step = slab_step(G);
-        for (int b = 0; b < G.N_v1 && ok; b += step) {
+        for (int b = split ? G.N_v1 : 0; b < G.N_v1 && ok; b += step) {
             const int e = std::min(G.N_v1, b + step);
             ok = cuda_ok("backproject H2D", cudaMemcpyAsync(dg.f() + size_t(b) * slab, g[i] + size_t(b) * slab,
                                                             size_t(e - b) * slab * 4, cudaMemcpyHostToDevice,

@@ -475,6 +475,34 @@ int launch_project_shear(const petl_geom& G, const float* f, float* g, const Vie
     return rc;
 }
 
+int shear::project_chunked(const petl_geom& G, const float* f, float* g, int chunk_cap, const ChunkHook& hook,
+                           cudaStream_t st)
+{
+    if (dispatch_mode() != 0 || !shear_eligible(G)) return kNotApplicable;
+    TableBuf tb;
+    int rc = shear::make_tables(G, tb, st);
+    if (rc) return rc;
+    const ViewRange vr{0, G.N_v1, 0, 1};
+    rc = shear::project_split(G, f, g, vr, nullptr, tb.T, st, chunk_cap, &hook);
+    cudaFreeAsync(tb.base, st);
+    if (rc == 0) note_path(2);
+    return rc;
+}
+
+int shear::backproject_chunked(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                               int chunk_cap, const ChunkHook& hook, cudaStream_t st)
+{
+    if (dispatch_mode() != 0 || !shear_eligible(G)) return kNotApplicable;
+    TableBuf tb;
+    int rc = shear::make_tables(G, tb, st);
+    if (rc) return rc;
+    const ViewRange vr{0, G.N_v1, 0, 1};
+    rc = shear::backproject_split(G, g, f, mode, accumulate, scale, vr, tb.T, st, chunk_cap, &hook);
+    cudaFreeAsync(tb.base, st);
+    if (rc == 0) note_path(2);
+    return rc;
+}
+
 int shear::backproject_with(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
                             const ViewRange& vr, const Tables& T, cudaStream_t st)
 {

@@ -493,7 +493,7 @@ size_t split_scratch_budget()
 
 template <class TF, class TG>
 int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr, const TG* meas, const Tables& T,
-                    cudaStream_t st)
+                    cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
     const int n_v0 = vr.n_v0(G.N_v0);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
@@ -509,6 +509,7 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     const size_t per_view = size_t(G.numY) * G.numZ * NXc * 4;
     int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), split_scratch_budget() / per_view)));
     if (G.numX > XMAXNX || G.numY > 65535) return kNotApplicable;  // k_xshift row buffer, grid.y
+    if (chunk_cap > 0) nv = std::min(nv, chunk_cap);
     const int nchunks = (n_v0 + nv - 1) / nv;
     nv = (n_v0 + nchunks - 1) / nchunks;
 
@@ -547,6 +548,7 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
             note_launch();
         }
         e = cudaGetLastError();
+        if (e == cudaSuccess && hook && hook->fn) hook->fn(hook->ctx, vi0, nvc);
     }
     cudaFreeAsync(X, st);
     if (e != cudaSuccess) {
@@ -557,15 +559,15 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
 }
 
 int project_split(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
-                  const Tables& T, cudaStream_t st)
+                  const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
-    return project_split_t<float, float>(G, f, g, vr, meas, T, st);
+    return project_split_t<float, float>(G, f, g, vr, meas, T, st, chunk_cap, hook);
 }
 
 int project_split_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
                        const __nv_bfloat16* meas, const Tables& T, cudaStream_t st)
 {
-    return project_split_t<__nv_bfloat16, __nv_bfloat16>(G, f, g, vr, meas, T, st);
+    return project_split_t<__nv_bfloat16, __nv_bfloat16>(G, f, g, vr, meas, T, st, 0, nullptr);
 }
 
 }  // namespace shear

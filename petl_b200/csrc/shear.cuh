@@ -52,12 +52,23 @@ inline int shift_spread(int n, double step) { return int(std::floor(double(n) * 
 // device's memory.
 size_t split_scratch_budget();
 
+// Called once per chunk of views of a split projection, on the host while
+// the chunk's work is enqueued: after the forward's kernels of the chunk
+// (to start copying its planogram views out) or before the backward's (to
+// make the stream wait for its planogram views).  vi0 is the chunk's first
+// view index in the call's view range, nvc its view count.
+struct ChunkHook {
+    void (*fn)(void* ctx, int vi0, int nvc) = nullptr;
+    void* ctx = nullptr;
+};
+
 // Split forward projection (projector_split.cu): an x-shift pass per chunk of
 // views into FP32 scratch, then a z-tap kernel fed by a TMA ring.  Same
 // operator and the same float operations in the same order as project_tma.
-// kNotApplicable when the layout rules or the scratch allocation fail.
+// chunk_cap > 0 bounds the views per chunk.  kNotApplicable when the layout
+// rules or the scratch allocation fail.
 int project_split(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
-                  const Tables& T, cudaStream_t st);
+                  const Tables& T, cudaStream_t st, int chunk_cap = 0, const ChunkHook* hook = nullptr);
 int project_split_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16* g, const ViewRange& vr,
                        const __nv_bfloat16* meas, const Tables& T, cudaStream_t st);
 // Split backprojection (backprojector_split.cu): a z-gather kernel per chunk
@@ -66,7 +77,8 @@ int project_split_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16
 // as backproject_tma; kNotApplicable when the layout rules or the scratch
 // allocation fail.
 int backproject_split(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
-                      const ViewRange& vr, const Tables& T, cudaStream_t st);
+                      const ViewRange& vr, const Tables& T, cudaStream_t st, int chunk_cap = 0,
+                      const ChunkHook* hook = nullptr);
 int backproject_split_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate,
                            float scale, const ViewRange& vr, const Tables& T, cudaStream_t st);
 
@@ -83,6 +95,15 @@ int backproject_with(const petl_geom& G, const float* g, float* f, int mode, int
 // Return value of the TMA launchers when the geometry or the buffers do not
 // fit their layout rules; the caller then uses the first-generation kernels.
 constexpr int kNotApplicable = -2;
+
+// Projection of all views of G by the split kernels in chunks of at most
+// chunk_cap views, with the shift tables built here and `hook` called per
+// chunk; kNotApplicable when the split kernels do not apply (the caller then
+// projects without chunk hooks).
+int project_chunked(const petl_geom& G, const float* f, float* g, int chunk_cap, const ChunkHook& hook,
+                    cudaStream_t st);
+int backproject_chunked(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                        int chunk_cap, const ChunkHook& hook, cudaStream_t st);
 
 // TMA-staged kernels (projector_shear_tma.cu).  They compute the same
 // operator as the first-generation kernels of projector_shear.cu.
