@@ -16,9 +16,9 @@
  * Error behaviour: bool functions return false (and print a reason to stderr)
  * on invalid input or device failure, the contract the reference binding
  * relies on (it raises on false).  Functions that exist in the reference only
- * for subsystems outside the reconstruction path (list-mode binning, analytic
- * phantoms / ray tracing, detector-response corrections, scatter) are
- * exported so that the binding loads, and return false with a message.
+ * for subsystems outside the reconstruction path (analytic phantoms / ray
+ * tracing, detector-response corrections, scatter) are exported so that the
+ * binding loads, and return false with a message.
  *
  * Device-pointer entry points for the resident path live in petl_device.h.
  */
@@ -62,6 +62,11 @@ bool set_volume(int numX, int numY, int numZ, float voxelWidth, float voxelHeigh
                 float offsetX, float offsetY, float offsetZ);   /* :53 */
 
 /* --- outside the reconstruction path: exported, return false --------------- */
+/* List-mode binning of a coincidence file (.lst records, else the binary
+ * acquisition format) into every planogram, overwriting g: bilinear in
+ * (u1, u0), z from the chest wall, mm -- the reference's defaults
+ * (src/petl.cpp:65-79, src/binning.cpp:558-790).  Parsed on the host in
+ * batches, binned on the GPU. */
 bool bin(float** g, char* file_name);                    /* :55 */
 bool simulate_scatter(float** g, float* mu);             /* :57 */
 bool add_object(int type, float* c, float* r, float val, float* A, float* clip); /* :64 */

@@ -73,6 +73,17 @@ int petl_set_dispatch(int mode);
  * 0 general, 1 shear-warp, 2 TMA-staged shear-warp; -1 before any call. */
 int petl_last_projector_path(void);
 
+/* List-mode binning (src/binning.cpp:614-790 with src/planogram.cpp:113-141):
+ * the coincidences blue[i], pink[i] (xyz in mm, i < n, device arrays of 3n
+ * floats) are added to the planogram g of G.  linear != 0: bilinear weights
+ * in (u1, u0), the reference's binning; else the nearest bin.  chest_wall !=
+ * 0: z is measured from the panels' bottom edge (u1 shifted by -H), the
+ * reference's list-mode origin.  Accumulates into g (zero it first for the
+ * reference's bin, which overwrites).  Deposits are atomic adds, so sums of
+ * fractional weights may differ in the last bits from run to run. */
+int petl_bin_events_dev(const petl_geom* G, const float* blue, const float* pink, long long n, float* g,
+                        int linear, int chest_wall, void* stream);
+
 /* Error word written by kernels whose waits on asynchronous copies are
  * bounded: nonzero if a wait gave up (the call's result is then invalid).
  * Reading it synchronizes the device and clears it.  -1 if it cannot be

@@ -763,4 +763,75 @@ double oracle_tv_quadform_f64(const double* f, const double* d, int N1, int N2, 
     return total;
 }
 
+// List-mode binning, in event order: the coordinate maps of
+// planogram::is_within_acceptable_angle / get_u_coords
+// (src/planogram.cpp:113-141), the chest-wall shift of binning::binAcqdata
+// (src/binning.cpp:630-645) and the deposit of binning::flush_queue
+// (src/binning.cpp:662-790): nearest bin (linear == 0) or bilinear weights
+// in (u1, u0) computed in double and added to the float bin.  The events of
+// one planogram are summed in file order, as the reference's queue flushes
+// do per bin.  Accumulates into g (the caller zeroes it).
+void oracle_bin_events(const oracle_geom* G, const float* blue, const float* pink, long long n, float* g,
+                       int linear, int chest_wall)
+{
+    const size_t proj = size_t(G->N_u1) * G->N_u0, obl = size_t(G->N_v0) * proj;
+    const float cs = G->cos_psi, sn = G->sin_psi;
+    for (long long e = 0; e < n; e++) {
+        const float* b = blue + 3 * e;
+        const float* q = pink + 3 * e;
+        const float r0 = b[0] - q[0], r1 = b[1] - q[1], r2 = b[2] - q[2];
+        const float c = -sn * r0 + cs * r1;
+        if (c == 0.0f) continue;
+        const float v0 = -(cs * r0 + sn * r1) / c;
+        if (std::fabs(v0) > G->v_m0) continue;
+        const float v1 = -r2 / c;
+        if (std::fabs(v1) > G->v_m1) continue;
+        const float t = b[1] * cs - b[0] * sn;
+        float u1 = b[2] + v1 * t;
+        const float u0 = b[0] * cs + b[1] * sn + v0 * t;
+        if (chest_wall) u1 -= G->H;
+        // flush_queue: slope and view by rounding in double (int(x + 0.5))
+        const int iv1 = int(double((v1 - G->v1_0) / G->T_v1) + 0.5);
+        if (iv1 < 0 || iv1 >= G->N_v1) continue;
+        const int iv0 = int(double((v0 - G->v0_0) / G->T_v0) + 0.5);
+        if (iv0 < 0 || iv0 >= G->N_v0) continue;
+        float* P = g + size_t(iv1) * obl + size_t(iv0) * proj;
+        const float w = 1.0f;  // the reference inserts every event with weight 1
+        const float fu1 = (u1 - G->u1_0) / G->T_u1, fu0 = (u0 - G->u0_0) / G->T_u0;
+        if (!linear) {
+            const int a = int(double(fu1) + 0.5), bb = int(double(fu0) + 0.5);
+            if (a >= 0 && a < G->N_u1 && bb >= 0 && bb < G->N_u0) P[size_t(a) * G->N_u0 + bb] += w;
+            continue;
+        }
+        int lo1, hi1, lo0, hi0;
+        float d1, d0;
+        if (fu1 <= 0.0) {
+            lo1 = hi1 = 0;
+            d1 = 0.0f;
+        } else if (fu1 >= G->N_u1 - 1) {
+            lo1 = hi1 = G->N_u1 - 1;
+            d1 = 0.0f;
+        } else {
+            lo1 = int(fu1);
+            hi1 = lo1 + 1;
+            d1 = fu1 - float(lo1);
+        }
+        if (fu0 <= 0.0) {
+            lo0 = hi0 = 0;
+            d0 = 0.0f;
+        } else if (fu0 >= G->N_u0 - 1) {
+            lo0 = hi0 = G->N_u0 - 1;
+            d0 = 0.0f;
+        } else {
+            lo0 = int(fu0);
+            hi0 = lo0 + 1;
+            d0 = fu0 - float(lo0);
+        }
+        P[lo1 * G->N_u0 + lo0] += (1.0 - d1) * (1.0 - d0) * w;
+        P[hi1 * G->N_u0 + lo0] += d1 * (1.0 - d0) * w;
+        P[lo1 * G->N_u0 + hi0] += (1.0 - d1) * d0 * w;
+        P[hi1 * G->N_u0 + hi0] += d1 * d0 * w;
+    }
+}
+
 }  // extern "C"

@@ -45,6 +45,13 @@ void oracle_set_volume(oracle_geom* G, int numX, int numY, int numZ,
                        float voxelWidth, float voxelHeight,
                        float offsetX, float offsetY, float offsetZ);
 
+/* List-mode binning of coincidences (blue[i], pink[i], xyz in mm) into one
+ * planogram, in event order (src/planogram.cpp:113-141, src/binning.cpp:
+ * 614-790): nearest bin (linear == 0) or bilinear deposit in (u1, u0);
+ * chest_wall != 0 shifts u1 by -H.  Accumulates into g (zero it first). */
+void oracle_bin_events(const oracle_geom* G, const float* blue, const float* pink, long long n, float* g,
+                       int linear, int chest_wall);
+
 /* src/vector_ops.cpp:481-505 */
 int oracle_optimal_fft_size(int N);
 

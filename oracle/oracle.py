@@ -58,6 +58,7 @@ def lib():
         gp = P(Geom)
         L.oracle_planogram_init.argtypes = [gp] + [ctypes.c_float] * 7
         L.oracle_planogram_init.restype = ctypes.c_int
+        L.oracle_bin_events.argtypes = [gp, fp, fp, ctypes.c_longlong, fp, ctypes.c_int, ctypes.c_int]
         L.oracle_set_volume.argtypes = [gp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 5
         L.oracle_optimal_fft_size.argtypes = [ctypes.c_int]
         L.oracle_optimal_fft_size.restype = ctypes.c_int
@@ -179,6 +180,22 @@ def backproject(geoms, g, dtype=np.float64, texmode=0, nthreads=0):
 
 def project_nnz(G, nthreads=0, single=False):
     return lib().oracle_project_nnz_t(ctypes.byref(G), nthreads, 1 if single else 0)
+
+
+# ----------------------------------------------------------------------------
+# list-mode binning
+# ----------------------------------------------------------------------------
+def bin_events(geoms, blue, pink, linear=True, chest_wall=True):
+    """Coincidences (blue[i], pink[i], xyz in mm) binned into zeroed float32
+    planograms, one per geometry, in event order (src/binning.cpp:614-790)."""
+    blue, pink = _f(blue).reshape(-1, 3), _f(pink).reshape(-1, 3)
+    out = []
+    for G in (geoms if isinstance(geoms, (list, tuple)) else [geoms]):
+        g = np.zeros(G.shape, np.float32)
+        lib().oracle_bin_events(ctypes.byref(G), _ptr(blue, ctypes.c_float), _ptr(pink, ctypes.c_float),
+                                len(blue), _ptr(g, ctypes.c_float), 1 if linear else 0, 1 if chest_wall else 0)
+        out.append(g)
+    return out
 
 
 # ----------------------------------------------------------------------------

@@ -83,6 +83,7 @@ _DEV_API = [
     ("petl_backproject_range_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_ratio_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_nnz_dev", c_i, [_G, ctypes.POINTER(c_d), c_vp]),
+    ("petl_bin_events_dev", c_i, [_G, c_vp, c_vp, c_ll, c_vp, c_i, c_i, c_vp]),
     ("petl_project_bf16_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_ratio_bf16_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_backproject_bf16_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_i, c_i, c_vp]),

@@ -40,6 +40,8 @@ int petl_gaussian_filter_dev(float* f, int N1, int N2, int N3, float FWHM, int n
 namespace petl {
 int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream_t st, float* host_rebinned_out);
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
+int bin_file(const std::vector<petl_geom>& plans, const std::vector<float*>& dg, const char* path, int linear,
+             int chest_wall, cudaStream_t st, long long* binned_events);
 namespace shear {
 struct ChunkHook {
     void (*fn)(void* ctx, int vi0, int nvc) = nullptr;
@@ -471,7 +473,33 @@ static bool not_here(const char* name)
     fprintf(stderr, "%s: not provided by this build (outside the reconstruction path)\n", name);
     return false;
 }
-bool bin(float**, char*) { return not_here("bin"); }
+bool bin(float** g, char* file_name)
+{
+    // PETL::bin (src/petl.cpp:65-79): the planograms are overwritten with the
+    // file's coincidences, binned with the reference's defaults (bilinear in
+    // (u1, u0), z from the chest wall, mm)
+    const Params P = tomo()->params;
+    if (g == nullptr || file_name == nullptr || file_name[0] == 0 || !P.geometryDefined()) return false;
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok("bin", cudaErrorNoDevice);
+    std::vector<std::unique_ptr<DevBuf>> bufs;
+    std::vector<float*> dg;
+    for (const petl_geom& G : P.plans) {
+        bufs.emplace_back(new DevBuf);
+        const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
+        if (!bufs.back()->alloc(n * 4, c->compute)) return cuda_ok("bin alloc", cudaGetLastError());
+        dg.push_back(bufs.back()->f());
+    }
+    long long events = 0;
+    bool ok = report("bin", petl::bin_file(P.plans, dg, file_name, 1, 1, c->compute, &events));
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        const petl_geom& G = P.plans[i];
+        const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
+        ok = cuda_ok("bin D2H", cudaMemcpyAsync(g[i], dg[i], n * 4, cudaMemcpyDeviceToHost, c->compute));
+    }
+    ok = cuda_ok("bin sync", cudaStreamSynchronize(c->compute)) && ok;
+    return ok;
+}
 bool simulate_scatter(float**, float*) { return not_here("simulate_scatter"); }
 bool add_object(int, float*, float*, float, float*, float*) { return not_here("add_object"); }
 bool add_module(int, float*, float*, float, float*, float*) { return not_here("add_module"); }

@@ -67,6 +67,25 @@ def project(geom, f, g=None, subset=None, v1_range=None):
     return g if isinstance(geom, (list, tuple)) else gl[0]
 
 
+def bin_events(geom, blue, pink, g=None, linear=True, chest_wall=True):
+    """Coincidences blue[i], pink[i] ((n, 3) float32 device tensors, mm)
+    binned into the planogram(s) of ``geom`` (src/binning.cpp:614-790):
+    bilinear in (u1, u0) (the reference's binning) or the nearest bin, z from
+    the chest wall (the reference's origin) or from the centre.  A new,
+    zeroed ``g`` is allocated unless given; a given ``g`` is added to."""
+    geoms = as_list(geom)
+    if g is None:
+        g = [torch.zeros(G.shape, device=blue.device, dtype=torch.float32) for G in geoms]
+    gl = as_list(g)
+    n = int(blue.shape[0]) if blue.dim() > 1 else int(blue.numel()) // 3
+    if int(pink.numel()) != 3 * n or int(blue.numel()) != 3 * n:
+        raise ValueError("bin_events: blue and pink must both hold n xyz triples")
+    for G, gi in zip(geoms, gl):
+        check(lib().petl_bin_events_dev(G.ptr, _dev(blue, "blue"), _dev(pink, "pink"), n, _dev(gi, "g"),
+                                        1 if linear else 0, 1 if chest_wall else 0, _stream()), "bin_events")
+    return g if isinstance(geom, (list, tuple)) else gl[0]
+
+
 def project_ratio(geom, f, meas, out=None, subset=None, v1_range=None):
     """out = meas / (P f) with 0 where P f == 0 (the MLEM data ratio of the
     reference, src/petl_server.py:1593-1594), computed inside the projector."""

@@ -211,6 +211,21 @@ class PETLserver:
             raise TypeError("project failed")
         return g
 
+    def bin(self, file_name, g=None):
+        """Bins a list-mode coincidence file (src/petl_server.py:653-678): the
+        planograms are overwritten with the binned data, as the reference's
+        C++ does (its docstring's "adds to the data" does not hold there)."""
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        if g is None:
+            g = self.allocate_projections()
+        self.set_model()
+        for a in g:
+            _check_f32(a, "g")
+        if not self.libprojectors.bin(_pp(g), bytes(str(file_name), "ascii")):
+            raise TypeError("bin failed")
+        return g
+
     def backproject(self, g, f=None):
         if not self.all_defined():
             raise ValueError("Error: volume and PET geometry must be defined")

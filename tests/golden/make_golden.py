@@ -13,6 +13,9 @@ arguments and the reference outputs.  The committed fixtures in this
 directory were produced by this script; the tests read them, never the
 reference library.
 
+List-mode binning is CPU code in the reference and runs anywhere (it reads
+seeded coincidence files this script writes in the reference's formats).
+
 The MLEM case drives the reference C ABI with the same call sequence as the
 reference ``PETLserver.MLEM`` loop (src/petl_server.py:1534-1606): project,
 rdivide4D, backproject, divide3D, multiply3D, with sensitivity =
@@ -72,6 +75,8 @@ class Ref:
         L.diffuse.restype = c_b
         L.TV_denoise.argtypes = [fp, c_i, c_i, c_i, c_f, c_f, c_f, c_i, c_b, c_b]
         L.TV_denoise.restype = c_b
+        L.bin.argtypes = [ctypes.POINTER(fp), ctypes.c_char_p]
+        L.bin.restype = c_b
         self.L = L
 
     def model(self, planograms, vol):
@@ -292,6 +297,53 @@ def run_cpu(ref, out):
     print("wrote cpu rules", shapes)
 
 
+def run_binning(ref, out):
+    """List-mode binning: CPU reference code (src/binning.cpp).  Events are
+    seeded coincidences on the panels (petl_b200.listmode), written in the
+    reference's two file formats and binned by the reference's bin(); the
+    planograms are pre-filled with 7 to record that bin() overwrites them."""
+    sys.path.insert(0, ROOT)
+    from petl_b200 import listmode
+    import tempfile
+    cases = {
+        # name: (planograms, volume, file format, [(psi of the panels, events)])
+        "bin_g0": ([GEOMS["g0"][0][0]], GEOMS["g0"][1], "acq", [(0.0, 4000)]),
+        "bin_g0t1": ([GEOMS["g0t1"][0][0]], GEOMS["g0t1"][1], "lst", [(0.0, 4000)]),
+        "bin_gpetx": (GEOMS["gpetx"][0], GEOMS["gpetx"][1], "acq", [(0.0, 2000), (90.0, 2000)]),
+    }
+    rec = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (plans, vol, fmt, srcs) in cases.items():
+            rng = np.random.default_rng(sum(map(ord, name)))
+            bl, pk = [], []
+            for psi_p, n in srcs:
+                _, D, L_, H, _, _, _ = plans[0]
+                b, p = listmode.coincidences(n, rng, D / 2, L_ / 2, H / 2, psi_deg=psi_p,
+                                             box=(0.6 * L_ / 2, 0.6 * L_ / 2, 0.6 * H / 2))
+                bl.append(b)
+                pk.append(p)
+            blue, pink = np.concatenate(bl), np.concatenate(pk)
+            path = os.path.join(tmp, name + (".lst" if fmt == "lst" else ".dat"))
+            counts = listmode.interaction_counts(len(blue), rng, 0.2)
+            if fmt == "lst":
+                listmode.write_lst(path, blue, pink)
+            else:
+                listmode.write_acq(path, blue, pink, counts)
+            ref.model(plans, vol)
+            gs = [np.full(sh, 7.0, np.float32) for sh in ref.shapes()]
+            if not ref.L.bin(ref.pp(gs), path.encode()):
+                raise RuntimeError("reference bin failed")
+            rec[f"{name}_planograms"] = np.array(plans)
+            rec[f"{name}_volume"] = np.array(vol)
+            rec[f"{name}_blue"], rec[f"{name}_pink"] = blue, pink
+            rec[f"{name}_format"] = np.array(fmt)
+            rec[f"{name}_nb"], rec[f"{name}_np"] = counts
+            for i, g in enumerate(gs):
+                rec[f"{name}_g{i}"] = g
+    np.savez_compressed(os.path.join(out, "binning.npz"), **rec)
+    print("wrote binning", {k: float(v.sum()) for k, v in rec.items() if k[-3:-1] == "_g"})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
@@ -301,6 +353,7 @@ def main():
     os.makedirs(a.out, exist_ok=True)
     ref = Ref(a.lib)
     run_cpu(ref, a.out)
+    run_binning(ref, a.out)
     if not a.cpu_only:
         run_projectors(ref, a.out)
         run_pfdr_fbp(ref, a.out)
