@@ -4,6 +4,7 @@
     python -m petl_b200.studies penalized   # 4 x 128x128x64, NLL + RD + TV, 50 steps, FD check
     python -m petl_b200.studies storage     # 256x256x128 OSEM 10 x 8 subsets, FP32 vs BF16 storage
     python -m petl_b200.studies serving     # 200 Poisson-arrival OSEM requests, p50/p99
+    python -m petl_b200.studies binning     # list-mode binning, device and C-ABI file rates
 
 All inputs are synthetic and seeded: ellipsoid phantoms (replace semantics,
 later ellipsoids overwrite earlier ones), forward projected with the
@@ -245,13 +246,67 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0):
             "throughput_ratio": batched["recons_per_s"] / single["recons_per_s"]}
 
 
+def study_binning(seed=0, n_events=16_000_000, n_file=8_000_000, tmpdir="/tmp"):
+    """List-mode binning at the 256x256x128 geometry (planogram (65,129,128,
+    256)): device-resident events binned by the kernel (events/s), and a
+    .lst file binned through the reference C ABI (parse + copies + kernel +
+    the planogram back to the host)."""
+    import os
+    from . import listmode
+    from .server import PETLserver
+    args = (0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25)
+    G = Geometry(*args, volume=(256, 256, 128, 1.0))
+    rng = np.random.default_rng(seed)
+    parts_b, parts_p = [], []
+    for k in range(0, n_events, 2_000_000):
+        b, p = listmode.coincidences(min(2_000_000, n_events - k), rng, 128.0, 64.0, 64.0, box=(60.0, 60.0, 50.0))
+        parts_b.append(b)
+        parts_p.append(p)
+    blue_h, pink_h = np.concatenate(parts_b), np.concatenate(parts_p)
+    blue = torch.from_numpy(blue_h).cuda()
+    pink = torch.from_numpy(pink_h).cuda()
+    g = torch.zeros(G.shape, device="cuda")
+    res = {"study": "binning", "workload": f"{n_events} coincidences on the panels of "
+           "add_planogram(0, 256, 128, 128, T=1, 0.5, 0.25), planogram (65,129,128,256), bilinear deposits"}
+    for linear in (True, False):
+        ops.bin_events(G, blue, pink, g=g, linear=linear)
+        ts = []
+        for _ in range(3):
+            g.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ops.bin_events(G, blue, pink, g=g, linear=linear)
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        key = "linear" if linear else "nearest"
+        res[f"device_{key}_ms"] = float(np.median(ts))
+        res[f"device_{key}_events_per_s"] = n_events / (np.median(ts) * 1e-3)
+    res["binned_fraction"] = float(g.sum()) / n_events  # nearest: events landing in a bin
+    path = os.path.join(tmpdir, f"petl_binning_{os.getpid()}.lst")
+    listmode.write_lst(path, blue_h[:n_file], pink_h[:n_file])
+    s = PETLserver()
+    s.add_planogram(*args)
+    s.set_volume(256, 256, 128, 1.0)
+    gh = [np.empty(G.shape, np.float32)]
+    s.bin(path, gh)
+    t0 = time.perf_counter()
+    s.bin(path, gh)
+    t = time.perf_counter() - t0
+    os.remove(path)
+    res.update({"file_events": n_file, "file_bytes": n_file * 48, "cabi_file_s": t,
+                "cabi_file_events_per_s": n_file / t})
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving"])
+    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving", "binning"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--requests", type=int, default=200)
     a = ap.parse_args(argv)
-    fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage}
+    fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
+          "binning": study_binning}
     if a.study == "serving":
         res = study_serving(n=a.requests, seed=a.seed)
     else:
