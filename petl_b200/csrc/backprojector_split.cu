@@ -54,7 +54,9 @@ constexpr int GWARPS = GPG * GRG;
 constexpr int GNT = 32 * GWARPS;
 constexpr int GDW = 2;              // largest shift difference among a warp's planes
 constexpr int GWN = GK + GDW + 1;   // register window rows
-constexpr int GNSMAX = 8;           // ring stages at most
+// ring stages: two (of two slopes each) measured fastest; deeper rings
+// (3-8 stages) ran 3-10 % slower at the 256x256x128 workload
+constexpr int GNSMAX = 2;
 constexpr int GV1MAX = 128;         // slopes per call at most
 constexpr int GVG = 4;              // views per CTA at most
 constexpr int kPatGen = 15;         // no straight-line pattern: per-plane taps

@@ -14,7 +14,7 @@
 // * k_fwd_zsum applies the z taps.  CTA = one view x 16 slopes x 32 rows x 64
 //   columns, 16 warps of 4 slopes x 8 rows x 2 columns per lane.  The staged
 //   rows of each plane arrive by a tiled TMA copy (no multicast) into a ring
-//   of up to 8 stages with full/empty mbarriers; the copy of a stage is
+//   of two stages of two planes with full/empty mbarriers; the copy of a stage is
 //   started by a rotating warp once every warp has released the slot, so no
 //   CTA-wide barrier sits in the plane loop.  The window offset, tap offsets
 //   and weights of every (plane, slope group) are tabulated once per CTA.
@@ -55,7 +55,9 @@ constexpr int ZWARPS = 16;
 constexpr int ZNT = 32 * ZWARPS;
 constexpr int ZDMAX = 3;              // largest shift difference among a warp's slopes
 constexpr int ZWN = ZK + ZDMAX + 1;   // register window rows
-constexpr int ZNSMAX = 8;             // ring stages at most
+// ring stages: two (of two planes each) measured fastest; deeper rings
+// (3-8 stages) ran 1-3 % slower at the 256x256x128 workload
+constexpr int ZNSMAX = 2;
 constexpr int ZMAXPLANES = 1024;      // planes the per-CTA tables hold
 
 // code word of a (plane, slope group): tap offsets (2 bits per slope), the
