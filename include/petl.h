@@ -77,7 +77,15 @@ bool scale_phantom(float, float, float);                 /* :68 */
 bool voxelize(float* f, int oversampling);               /* :69 */
 bool ray_trace(float** g, int oversampling);             /* :70 */
 bool stopping_power(float** g, int oversampling);        /* :71 */
+
+/* --- corrections: implemented (on the GPU, host arrays in and out) --------- */
+/* Every planogram's projection (iv1, iv0) times 2 pi (1 + v0^2 + v1^2)^1.5 /
+ * (T_v1 T_v0), or its inverse (the solid-angle model) for do_inverse
+ * (src/petl.cpp:154-162, src/planogram.cpp:262-302). */
 bool set_solid_angle_correction(float** g, bool do_inverse); /* :72 */
+/* g = g / r, then the bad-pixel median in-fill below threshold * median(r)
+ * per projection, zero outside the field of view (src/petl.cpp:163-192,
+ * src/median_filter.cu). */
 bool apply_corrections(float** g, float** r, float threshold); /* :73 */
 
 /* --- projectors and analytic reconstruction (src/petl_c_interface.h:59-62) -- */

@@ -84,6 +84,20 @@ int petl_last_projector_path(void);
 int petl_bin_events_dev(const petl_geom* G, const float* blue, const float* pink, long long n, float* g,
                         int linear, int chest_wall, void* stream);
 
+/* Solid-angle correction of one planogram on the device
+ * (src/planogram.cpp:262-302): projection (iv1, iv0) is multiplied by
+ * 2 pi (1 + v0^2 + v1^2)^1.5 / (T_v1 T_v0), or by its inverse (the
+ * solid-angle model) when do_inverse != 0.  Needs the planogram only. */
+int petl_solid_angle_dev(const petl_geom* G, float* g, int do_inverse, void* stream);
+
+/* PETL::apply_corrections on one planogram on the device (src/petl.cpp:
+ * 163-192, src/median_filter.cu): g = g / r (0 where r == 0), then per
+ * projection, with t = threshold * median of the projection's r: bins outside
+ * the field of view -> 0; bins with r < t -> the median of the 5x5 window's
+ * divided values above t (edges clamped; 0 if none); other bins keep g / r.
+ * Windows read the divided values before any in-fill. */
+int petl_apply_corrections_dev(const petl_geom* G, float* g, const float* r, float threshold, void* stream);
+
 /* Error word written by kernels whose waits on asynchronous copies are
  * bounded: nonzero if a wait gave up (the call's result is then invalid).
  * Reading it synchronizes the device and clears it.  -1 if it cannot be

@@ -834,4 +834,107 @@ void oracle_bin_events(const oracle_geom* G, const float* blue, const float* pin
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Solid-angle correction (src/planogram.cpp:262-302): projection (iv1, iv0)
+// is scaled by c = 2 pi (1 + v0^2 + v1^2)^1.5 / (T_v1 T_v0), the squares and
+// v = i*T + start in float, the rest in double, c rounded to float; the
+// inverse (the solid-angle model) uses float(1.0 / c).
+// ---------------------------------------------------------------------------
+float oracle_solid_angle_factor(const oracle_geom* G, int iv1, int iv0, int inverse)
+{
+    const float v1 = float(iv1) * G->T_v1 + G->v1_0;
+    const float v0 = float(iv0) * G->T_v0 + G->v0_0;
+    const double s = 1.0 + double(v0 * v0) + double(v1 * v1);
+    float c = float(2.0 * 3.1415926535897932385 * std::pow(s, 1.5) / double(G->T_v1 * G->T_v0));
+    if (inverse) c = float(1.0 / double(c));
+    return c;
+}
+
+void oracle_solid_angle(const oracle_geom* G, float* g, int inverse)
+{
+    const size_t proj = size_t(G->N_u1) * G->N_u0;
+    for (int iv1 = 0; iv1 < G->N_v1; iv1++)
+        for (int iv0 = 0; iv0 < G->N_v0; iv0++) {
+            const float c = oracle_solid_angle_factor(G, iv1, iv0, inverse);
+            float* P = g + (size_t(iv1) * G->N_v0 + iv0) * proj;
+            for (size_t k = 0; k < proj; k++) P[k] *= c;
+        }
+}
+
+// Median of n floats (src/vector_ops.cpp:358-374): the element of rank n/2,
+// and for even n the mean (in float) of the ranks n/2 and n/2 - 1.
+float oracle_median(const float* x, long long n)
+{
+    if (n <= 0) return 0.0f;
+    std::vector<float> t(x, x + n);
+    std::sort(t.begin(), t.end());
+    const size_t mid = size_t(n) / 2;
+    if (n % 2 == 1) return t[mid];
+    return (t[mid] + t[mid - 1]) / 2.0f;
+}
+
+// PETL::apply_corrections (src/petl.cpp:163-192): g = g / r (0 where r == 0,
+// src/data_cube.cpp:144-149), then per projection (iv1, iv0) the bad-pixel
+// in-fill of src/median_filter.cu:11-190 with threshold = rel * median(r of
+// the projection):
+//   outside the field of view (the projector's ray mask)  -> 0
+//   r < threshold -> the median of the window's 5x5 neighbours (indices
+//                    clamped at the projection's edges, so edge pixels
+//                    repeat) whose divided g exceeds the threshold (the
+//                    reference tests g there, not r), averaged for an even
+//                    count, the mean of two for two, the one value for one,
+//                    0 for none
+//   otherwise      -> g / r
+// Every window reads the divided values before any in-fill (the reference
+// kernel rewrites g in place while other threads of the launch read it; the
+// two agree whenever no window holds a pixel that the launch rewrites).
+void oracle_apply_corrections(const oracle_geom* G, float* g, const float* r, float rel, int nthreads)
+{
+    set_threads(nthreads);
+    const int N1 = G->N_u1, N0 = G->N_u0;
+    const size_t proj = size_t(N1) * N0, nproj = size_t(G->N_v1) * G->N_v0;
+#pragma omp parallel for schedule(dynamic)
+    for (long long p = 0; p < (long long)nproj; p++) {
+        const int iv1 = int(p / G->N_v0), iv0 = int(p % G->N_v0);
+        float* P = g + size_t(p) * proj;
+        const float* Q = r + size_t(p) * proj;
+        std::vector<float> d(proj);
+        for (size_t k = 0; k < proj; k++) d[k] = (Q[k] == 0.0f) ? 0.0f : P[k] / Q[k];
+        const float thr = rel * oracle_median(Q, (long long)proj);
+        for (int iu1 = 0; iu1 < N1; iu1++)
+            for (int iu0 = 0; iu0 < N0; iu0++) {
+                const size_t k = size_t(iu1) * N0 + iu0;
+                if (!ray_visible(*G, iv1, iv0, iu1, iu0)) {
+                    P[k] = 0.0f;
+                    continue;
+                }
+                if (!(Q[k] < thr)) {
+                    P[k] = d[k];
+                    continue;
+                }
+                float v[25];
+                int m = 0;
+                for (int dj = -2; dj <= 2; dj++) {
+                    const int j = tmin(tmax(iu1 + dj, 0), N1 - 1);
+                    for (int dk = -2; dk <= 2; dk++) {
+                        const int i = tmin(tmax(iu0 + dk, 0), N0 - 1);
+                        const float x = d[size_t(j) * N0 + i];
+                        if (x > thr) v[m++] = x;
+                    }
+                }
+                if (m == 0) {
+                    P[k] = 0.0f;
+                } else if (m == 1) {
+                    P[k] = v[0];
+                } else if (m == 2) {
+                    P[k] = 0.5f * (v[0] + v[1]);
+                } else {
+                    std::sort(v, v + m);
+                    P[k] = (m % 2) ? v[m / 2] : 0.5f * (v[m / 2] + v[m / 2 - 1]);
+                }
+            }
+    }
+}
+
 }  // extern "C"

@@ -107,6 +107,18 @@ void   oracle_tv_gradient_f64(const double* f, double* Df, int N1, int N2, int N
 double oracle_tv_quadform_f64(const double* f, const double* d, int N1, int N2, int N3,
                               double delta, double beta, double p, int numNeighbors);
 
+/* Solid-angle factor of projection (iv1, iv0) and its application to one
+ * planogram (src/planogram.cpp:262-302); inverse != 0 gives the model. */
+float oracle_solid_angle_factor(const oracle_geom* G, int iv1, int iv0, int inverse);
+void  oracle_solid_angle(const oracle_geom* G, float* g, int inverse);
+
+/* src/vector_ops.cpp:358-374 */
+float oracle_median(const float* x, long long n);
+
+/* PETL::apply_corrections on one planogram: g /= r, then the bad-pixel
+ * median in-fill (src/petl.cpp:163-192, src/median_filter.cu:11-190). */
+void oracle_apply_corrections(const oracle_geom* G, float* g, const float* r, float rel, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,12 @@ def lib():
         L.oracle_planogram_init.argtypes = [gp] + [ctypes.c_float] * 7
         L.oracle_planogram_init.restype = ctypes.c_int
         L.oracle_bin_events.argtypes = [gp, fp, fp, ctypes.c_longlong, fp, ctypes.c_int, ctypes.c_int]
+        L.oracle_solid_angle_factor.argtypes = [gp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_solid_angle_factor.restype = ctypes.c_float
+        L.oracle_solid_angle.argtypes = [gp, fp, ctypes.c_int]
+        L.oracle_median.argtypes = [fp, ctypes.c_longlong]
+        L.oracle_median.restype = ctypes.c_float
+        L.oracle_apply_corrections.argtypes = [gp, fp, fp, ctypes.c_float, ctypes.c_int]
         L.oracle_set_volume.argtypes = [gp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 5
         L.oracle_optimal_fft_size.argtypes = [ctypes.c_int]
         L.oracle_optimal_fft_size.restype = ctypes.c_int
@@ -195,6 +201,40 @@ def bin_events(geoms, blue, pink, linear=True, chest_wall=True):
         lib().oracle_bin_events(ctypes.byref(G), _ptr(blue, ctypes.c_float), _ptr(pink, ctypes.c_float),
                                 len(blue), _ptr(g, ctypes.c_float), 1 if linear else 0, 1 if chest_wall else 0)
         out.append(g)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# corrections
+# ----------------------------------------------------------------------------
+def solid_angle(geoms, g, inverse=False):
+    """Planograms scaled by the solid-angle correction (inverse: the model),
+    src/planogram.cpp:262-302; returns new float32 arrays."""
+    out = []
+    for G, gi in zip(geoms if isinstance(geoms, (list, tuple)) else [geoms], g):
+        a = np.array(gi, np.float32, copy=True, order="C")
+        lib().oracle_solid_angle(ctypes.byref(G), _ptr(a, ctypes.c_float), 1 if inverse else 0)
+        out.append(a)
+    return out
+
+
+def median(x):
+    """src/vector_ops.cpp:358-374 on a float32 array."""
+    a = _f(x).ravel()
+    return float(lib().oracle_median(_ptr(a, ctypes.c_float), a.size))
+
+
+def apply_corrections(geoms, g, r, threshold=0.75, nthreads=0):
+    """PETL::apply_corrections: g / r then the bad-pixel median in-fill
+    (src/petl.cpp:163-192, src/median_filter.cu:11-190); new float32 arrays."""
+    out = []
+    geoms = geoms if isinstance(geoms, (list, tuple)) else [geoms]
+    for G, gi, ri in zip(geoms, g, r):
+        a = np.array(gi, np.float32, copy=True, order="C")
+        b = _f(ri)
+        lib().oracle_apply_corrections(ctypes.byref(G), _ptr(a, ctypes.c_float), _ptr(b, ctypes.c_float),
+                                       threshold, nthreads)
+        out.append(a)
     return out
 
 
@@ -351,20 +391,30 @@ def _divide(x, y):
     return out
 
 
-def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, nthreads=0):
+def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, nthreads=0, response=None):
+    """PETLserver.MLEM (src/petl_server.py:1534-1606).  With a response R the
+    projector includes it (src/petl_server.py:723-747, on during MLEM):
+    P f -> R P f, backprojection of y -> P^T (R y), sensitivity P^T R."""
     if isinstance(geoms, Geom):
         geoms, g = [geoms], [g]
+        if response is not None:
+            response = [response]
     vol = geoms[0].vol_shape
     if f is None or not np.any(f):
         f = np.ones(vol, np.float64)
     else:
         f = np.maximum(_d(f), 0.0)
-    ones = [np.ones(G.shape) for G in geoms]
+    R = [np.asarray(r, np.float64) for r in response] if response is not None else None
+    ones = [np.ones(G.shape) for G in geoms] if R is None else R
     sens = backproject(geoms, ones, nthreads=nthreads)
     sens[sens == 0.0] = 1.0
     for _ in range(num_iter):
         Pd = project(geoms, f, nthreads=nthreads)
+        if R is not None:
+            Pd = [p * r for p, r in zip(Pd, R)]
         ratio = [_rdivide(p, gi) for p, gi in zip(Pd, g)]
+        if R is not None:
+            ratio = [q * r for q, r in zip(ratio, R)]
         d = backproject(geoms, ratio, nthreads=nthreads)
         if beta <= 0.0:
             f = f * _divide(d, sens)

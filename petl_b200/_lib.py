@@ -84,6 +84,8 @@ _DEV_API = [
     ("petl_project_ratio_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_nnz_dev", c_i, [_G, ctypes.POINTER(c_d), c_vp]),
     ("petl_bin_events_dev", c_i, [_G, c_vp, c_vp, c_ll, c_vp, c_i, c_i, c_vp]),
+    ("petl_solid_angle_dev", c_i, [_G, c_vp, c_i, c_vp]),
+    ("petl_apply_corrections_dev", c_i, [_G, c_vp, c_vp, c_f, c_vp]),
     ("petl_project_bf16_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_ratio_bf16_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_backproject_bf16_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_f, c_i, c_i, c_i, c_i, c_vp]),

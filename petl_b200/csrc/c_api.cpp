@@ -42,6 +42,9 @@ int fbp(const petl_geom& G, const float* g, float* f, int accumulate, cudaStream
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
 int bin_file(const std::vector<petl_geom>& plans, const std::vector<float*>& dg, const char* path, int linear,
              int chest_wall, cudaStream_t st, long long* binned_events);
+int solid_angle(const petl_geom& G, float* g, bool inverse, int iv1_b, int iv1_e, cudaStream_t st);
+int apply_corrections(const petl_geom& G, float* g, const float* r, float rel, int iv1_b, int iv1_e,
+                      cudaStream_t st);
 namespace shear {
 struct ChunkHook {
     void (*fn)(void* ctx, int vi0, int nvc) = nullptr;
@@ -265,6 +268,51 @@ float inner(const float* x, const float* y, const float* w, size_t slab, size_t 
     for (double v : sums) total += v;
     return float(total);
 }
+
+// Runs op on each slab of v1 rows of every planogram: the slab's data (and
+// response) go up on the copy stream, op runs on the compute stream once they
+// have arrived, and the slab's result comes back on the compute stream, so
+// uploads of later slabs overlap the downloads of earlier ones.
+template <class Op>
+bool stream_planograms(const Params& P, float** g, float** r, const char* what, Op op)
+{
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok(what, cudaErrorNoDevice);
+    bool ok = true;
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        const petl_geom& G = P.plans[i];
+        const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0, n = slab * G.N_v1;
+        DevBuf dg, dr;
+        if (!dg.alloc(n * 4, c->compute) || (r && !dr.alloc(n * 4, c->compute)))
+            return cuda_ok(what, cudaGetLastError());
+        // the copy stream may only write the buffers once they exist
+        cudaEvent_t ready;
+        cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+        cudaEventRecord(ready, c->compute);
+        cudaStreamWaitEvent(c->copy, ready, 0);
+        cudaEventDestroy(ready);
+        const int step = slab_step(G);
+        for (int b = 0; b < G.N_v1 && ok; b += step) {
+            const int e = std::min(G.N_v1, b + step);
+            const size_t off = size_t(b) * slab, bytes = size_t(e - b) * slab * 4;
+            ok = cuda_ok(what, cudaMemcpyAsync(dg.f() + off, g[i] + off, bytes, cudaMemcpyHostToDevice, c->copy));
+            if (r) ok = ok && cuda_ok(what, cudaMemcpyAsync(dr.f() + off, r[i] + off, bytes, cudaMemcpyHostToDevice,
+                                                            c->copy));
+            cudaEvent_t ev;
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            cudaEventRecord(ev, c->copy);
+            cudaStreamWaitEvent(c->compute, ev, 0);
+            cudaEventDestroy(ev);
+            ok = ok && report(what, op(G, dg.f(), r ? dr.f() : nullptr, b, e, c->compute));
+            ok = ok && cuda_ok(what, cudaMemcpyAsync(g[i] + off, dg.f() + off, bytes, cudaMemcpyDeviceToHost,
+                                                     c->compute));
+        }
+    }
+    ok = cuda_ok(what, cudaStreamSynchronize(c->copy)) && ok;
+    ok = cuda_ok(what, cudaStreamSynchronize(c->compute)) && ok;
+    return ok;
+}
+
 
 }  // namespace
 
@@ -509,8 +557,36 @@ bool scale_phantom(float, float, float) { return not_here("scale_phantom"); }
 bool voxelize(float*, int) { return not_here("voxelize"); }
 bool ray_trace(float**, int) { return not_here("ray_trace"); }
 bool stopping_power(float**, int) { return not_here("stopping_power"); }
-bool set_solid_angle_correction(float**, bool) { return not_here("set_solid_angle_correction"); }
-bool apply_corrections(float**, float**, float) { return not_here("apply_corrections"); }
+
+// PETL::set_solid_angle_correction (src/petl.cpp:154-162)
+bool set_solid_angle_correction(float** g, bool do_inverse)
+{
+    const Params P = tomo()->params;
+    if (g == nullptr) return false;
+    for (size_t i = 0; i < P.plans.size(); i++)
+        if (g[i] == nullptr) {
+            printf("planogram::apply_solid_angle_correction: Error data not set!\n");
+            return false;
+        }
+    return stream_planograms(P, g, nullptr, "set_solid_angle_correction",
+                             [&](const petl_geom& G, float* dg, float*, int b, int e, cudaStream_t st) {
+                                 return petl::solid_angle(G, dg, do_inverse, b, e, st);
+                             });
+}
+
+// PETL::apply_corrections (src/petl.cpp:163-192): g = g / r, then the
+// bad-pixel median in-fill below threshold * median(r) per projection
+bool apply_corrections(float** g, float** r, float threshold)
+{
+    const Params P = tomo()->params;
+    if (g == nullptr || r == nullptr || P.plans.empty()) return false;
+    for (size_t i = 0; i < P.plans.size(); i++)
+        if (g[i] == nullptr || r[i] == nullptr) return false;
+    return stream_planograms(P, g, r, "apply_corrections",
+                             [&](const petl_geom& G, float* dg, float* dr, int b, int e, cudaStream_t st) {
+                                 return petl::apply_corrections(G, dg, dr, threshold, b, e, st);
+                             });
+}
 
 // ---------------------------------------------------------------------------
 // projectors

@@ -86,6 +86,29 @@ def bin_events(geom, blue, pink, g=None, linear=True, chest_wall=True):
     return g if isinstance(geom, (list, tuple)) else gl[0]
 
 
+def solid_angle_(geom, g, inverse=False):
+    """Scales each projection (iv1, iv0) of the planogram(s) g in place by the
+    solid-angle correction 2 pi (1 + v0^2 + v1^2)^1.5 / (T_v1 T_v0), or by
+    its inverse, the solid-angle model (src/planogram.cpp:262-302)."""
+    for G, gi in zip(as_list(geom), as_list(g)):
+        check(lib().petl_solid_angle_dev(G.ptr, _dev(gi, "g"), 1 if inverse else 0, _stream()), "solid_angle")
+    return g
+
+
+def apply_corrections_(geom, g, r, threshold=0.75):
+    """PETL::apply_corrections in place on device planograms: g = g / r, then
+    per projection the bins outside the field of view are zeroed and the bins
+    whose response is below threshold * median(r) get the median of their
+    5x5 window's divided values above that level (src/petl.cpp:163-192,
+    src/median_filter.cu)."""
+    for G, gi, ri in zip(as_list(geom), as_list(g), as_list(r)):
+        if tuple(gi.shape) != tuple(G.shape) or tuple(ri.shape) != tuple(G.shape):
+            raise ValueError("apply_corrections: g and r must have the planogram's shape")
+        check(lib().petl_apply_corrections_dev(G.ptr, _dev(gi, "g"), _dev(ri, "r"), float(threshold), _stream()),
+              "apply_corrections")
+    return g
+
+
 def project_ratio(geom, f, meas, out=None, subset=None, v1_range=None):
     """out = meas / (P f) with 0 where P f == 0 (the MLEM data ratio of the
     reference, src/petl_server.py:1593-1594), computed inside the projector."""

@@ -12,6 +12,8 @@ and the log-likelihood and step-size reductions run in FP64 on the device.
   update f *= d / max(0.1 sens, sens + grad R(f)).
 * ``osem`` splits the views into S interleaved subsets (subset s holds
   iv0 = s, s+S, ...); with S = 1 it is ``mlem``.  The reference has no OSEM.
+  A response R (planograms) makes the system model R P, as in the
+  reference's MLEM once a response is set.
 * ``rwls`` follows PETLserver.RWLS (src/petl_server.py:1691-1877): PCG with
   an optional SQS preconditioner 1/P^T W P 1, restarts every 50 iterations,
   step = <d,grad> / (<Pd, W Pd> + TV quadratic form), optional
@@ -27,13 +29,24 @@ def _ones_like_list(gl):
     return [torch.ones_like(x) for x in gl]
 
 
-def sensitivity(geoms, like, subset=None, mode="reference"):
-    """P^T 1 (src/petl_server.py:1257-1273) with zeros replaced by 1."""
+def sensitivity(geoms, like, subset=None, mode="reference", response=None):
+    """P^T 1 (src/petl_server.py:1257-1273), or P^T R with a response R,
+    with zeros replaced by 1."""
     geoms = as_list(geoms)
-    ones = _ones_like_list(like)
-    s = ops.backproject(geoms, ones, subset=subset, mode=mode)
+    w = _ones_like_list(like) if response is None else as_list(response)
+    s = ops.backproject(geoms, w, subset=subset, mode=mode)
     s[s == 0.0] = 1.0
     return s
+
+
+def _response_masked(gl, response):
+    """The data with zeros where the response is zero.  With a response R the
+    reference's MLEM projects R P f and backprojects R (g / R P f)
+    (src/petl_server.py:723-747 with include_response_with_projectors on
+    during MLEM, src/petl_server.py:1566-1567); R (g / R P f) = g / P f
+    wherever R != 0 and 0 elsewhere, so the iteration keeps the plain data
+    ratio on this masked data and uses P^T R as its sensitivity."""
+    return [torch.where(r != 0, x, torch.zeros_like(x)) for x, r in zip(gl, as_list(response))]
 
 
 def _init_image(geoms, f, device):
@@ -46,24 +59,30 @@ def _init_image(geoms, f, device):
     return f
 
 
-def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, sens=None, loglik_every=0):
+def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, sens=None, loglik_every=0, response=None):
     """MLEM / OSL-RD MLEM; returns (f, loglik history)."""
-    return osem(geoms, g, num_iter, 1, f=f, delta=delta, beta=beta, sens=sens, loglik_every=loglik_every)
+    return osem(geoms, g, num_iter, 1, f=f, delta=delta, beta=beta, sens=sens, loglik_every=loglik_every,
+                response=response)
 
 
-def osem(geoms, g, num_iter, num_subsets, f=None, delta=2.0, beta=0.0, sens=None, loglik_every=0):
+def osem(geoms, g, num_iter, num_subsets, f=None, delta=2.0, beta=0.0, sens=None, loglik_every=0,
+         response=None):
     """OSEM with interleaved view subsets; returns (f, loglik history).
 
     ``sens`` may pass precomputed per-subset sensitivities (list of S
-    volumes) so that repeated reconstructions on one geometry reuse them."""
+    volumes) so that repeated reconstructions on one geometry reuse them.
+    ``response`` (planograms R) makes the system model R P, as the
+    reference's MLEM does when a response is set."""
     single = not isinstance(geoms, (list, tuple))
     geoms = as_list(geoms)
     gl = as_list(g)
     device = gl[0].device
     f = _init_image(geoms, f, device)
     S = int(num_subsets)
+    if response is not None:
+        gl = _response_masked(gl, response)
     if sens is None:
-        sens = [sensitivity(geoms, gl, subset=(s, S)) for s in range(S)]
+        sens = [sensitivity(geoms, gl, subset=(s, S), response=response) for s in range(S)]
     ratio = [torch.empty_like(x) for x in gl]
     d = torch.empty_like(f)
     Df = torch.empty_like(f) if beta > 0.0 else None
@@ -79,7 +98,7 @@ def osem(geoms, g, num_iter, num_subsets, f=None, delta=2.0, beta=0.0, sens=None
             else:
                 ops.mlem_update_(f, d, sens[s])
         if loglik_every and (it + 1) % loglik_every == 0:
-            history.append(loglik(geoms, gl, f))
+            history.append(loglik(geoms, gl, f, response=response))
     del single
     return f, history
 
@@ -129,12 +148,16 @@ def osem_bf16(geom, g, num_iter, num_subsets, f=None, sens=None, image="fp32"):
     return f
 
 
-def loglik(geoms, g, f):
-    """Poisson log-likelihood of f (FP64, device)."""
+def loglik(geoms, g, f, response=None):
+    """Poisson log-likelihood of f (FP64, device), under R P f with a
+    response R."""
     geoms = as_list(geoms)
     gl = as_list(g)
     Pf = ops.project(geoms, f)
     Pf = as_list(Pf)
+    if response is not None:
+        for pi, r in zip(Pf, as_list(response)):
+            ops.multiply_(pi, r)
     total = torch.zeros((), device=gl[0].device, dtype=torch.float64)
     for gi, pi in zip(gl, Pf):
         total = total + ops.loglik(gi, pi)

@@ -9,9 +9,9 @@ Numpy inputs go through the reference-compatible C ABI (host pointers);
 torch CUDA tensors (or lists of them) go through the device-resident
 operators in petl_b200.ops without leaving the GPU.
 
-Not provided here (outside the reconstruction path): list-mode binning,
-analytic phantoms and ray tracing, detector response / corrections, scatter
-simulation and the napari display.
+Not provided here (outside the reconstruction path): analytic phantoms and
+ray tracing, the detector stopping-power response (calc_response therefore
+needs oversampling=0), scatter simulation and the napari display.
 """
 import ctypes
 import os
@@ -209,6 +209,8 @@ class PETLserver:
         _check_f32(f, "f")
         if not self.libprojectors.project(_pp(g), _fp(f)):
             raise TypeError("project failed")
+        if self.response is not None and self.include_response_with_projectors:
+            self.multiply(g, self.response)
         return g
 
     def bin(self, file_name, g=None):
@@ -235,6 +237,8 @@ class PETLserver:
         for a in g:
             _check_f32(a, "g")
         _check_f32(f, "f")
+        if self.response is not None and self.include_response_with_projectors:
+            g = self.multiply(self.copy_data(g), self.response)
         if not self.libprojectors.backproject(_pp(g), _fp(f)):
             raise TypeError("backproject failed")
         return f
@@ -267,6 +271,74 @@ class PETLserver:
             o[:] = 1.0
         self.backproject(ones, Pstar1)
         return Pstar1
+
+    # ------------------------------------------------------ response / corrections
+    def set_response(self, R):
+        """Sets the response map (src/petl_server.py:121-135); with
+        include_response_with_projectors it multiplies the data after project
+        and before backproject, and MLEM/OSEM always include it."""
+        self.response = R
+
+    def clear_response(self):
+        self.response = None
+
+    def calc_response(self, oversampling=1, mu=None):
+        """Response = solid-angle model (times exp(-P mu) when mu is given),
+        src/petl_server.py:578-605.  The detector stopping power
+        (oversampling > 0) is not provided: pass oversampling=0."""
+        if oversampling > 0:
+            raise NotImplementedError("detector stopping power is not provided; use oversampling=0")
+        self.response = self.apply_solid_angle_model(None)
+        if mu is not None:
+            Pmu = self.allocate_projections()
+            self.project(Pmu, mu)
+            for a in Pmu:
+                np.exp(a, out=a)
+            self.divide(self.response, Pmu)
+        return self.response
+
+    def apply_corrections(self, g, oversampling=1, mu=None):
+        """g = g / response with the bad-pixel median in-fill (threshold 0.75
+        of each projection's median response), computing the response first
+        if none is set (src/petl_server.py:607-639).  Device tensors stay on
+        the GPU."""
+        if self.response is None:
+            self.calc_response(oversampling, mu)
+        if self.response is None:
+            return g
+        if _is_dev(g):
+            from . import ops
+            R = self.response if _is_dev(self.response) else \
+                [torch.from_numpy(np.ascontiguousarray(r, np.float32)).to(g[0].device) for r in self.response]
+            ops.apply_corrections_(self.geometries_from_model(), g, R, 0.75)
+            return g
+        self.set_model()
+        for a, r in zip(g, self.response):
+            _check_f32(a, "g")
+            _check_f32(r, "response")
+        if self.libprojectors.apply_corrections(_pp(g), _pp(self.response), 0.75):
+            return g
+        return None
+
+    def apply_solid_angle_correction(self, g=None, do_inverse=False):
+        """Scales every projection by its solid-angle correction, or its
+        inverse (src/petl_server.py:1024-1043); g defaults to ones."""
+        if g is None:
+            g = self.allocate_projections()
+            self.setToOne(g)
+        self.set_model()
+        if _is_dev(g):
+            from . import ops
+            ops.solid_angle_(self.geometries_from_model(), g, do_inverse)
+            return g
+        for a in g:
+            _check_f32(a, "g")
+        if self.libprojectors.set_solid_angle_correction(_pp(g), bool(do_inverse)):
+            return g
+        return None
+
+    def apply_solid_angle_model(self, g=None):
+        return self.apply_solid_angle_correction(g, True)
 
     # ------------------------------------------------------- vector helpers
     def _binop4(self, name3, name4, x, y):
@@ -391,7 +463,11 @@ class PETLserver:
         if f is None:
             f = self.allocate_volume()
         fd = torch.from_numpy(np.ascontiguousarray(f, np.float32)).to(dev)
-        fd, _ = recon.osem(geoms, gd, numIter, numSubsets, f=fd, delta=delta, beta=beta)
+        R = None
+        if self.response is not None:  # MLEM always includes a set response
+            R = [r if _is_dev(r) else torch.from_numpy(np.ascontiguousarray(r, np.float32)).to(dev)
+                 for r in self.response]
+        fd, _ = recon.osem(geoms, gd, numIter, numSubsets, f=fd, delta=delta, beta=beta, response=R)
         f[:] = fd.cpu().numpy()
         return f
 

@@ -6,12 +6,15 @@ PFDR, FBP and regularizers exist only as CUDA, so this script has to run on a
 machine with a GPU; geometry and the dataCube elementwise rules are CPU code
 and run anywhere.
 
-    python tests/golden/make_golden.py --out <dir> [--cpu-only]
+    python tests/golden/make_golden.py --out <dir> [--cpu-only] [--only case ...]
 
 Each case is written as ``<name>.npz`` holding its inputs, the reference
 arguments and the reference outputs.  The committed fixtures in this
 directory were produced by this script; the tests read them, never the
 reference library.
+
+The solid-angle correction is CPU code too; apply_corrections divides on
+the host and in-fills bad pixels with a CUDA kernel, so it needs a GPU.
 
 List-mode binning is CPU code in the reference and runs anywhere (it reads
 seeded coincidence files this script writes in the reference's formats).
@@ -77,6 +80,10 @@ class Ref:
         L.TV_denoise.restype = c_b
         L.bin.argtypes = [ctypes.POINTER(fp), ctypes.c_char_p]
         L.bin.restype = c_b
+        L.set_solid_angle_correction.argtypes = [ctypes.POINTER(fp), c_b]
+        L.set_solid_angle_correction.restype = c_b
+        L.apply_corrections.argtypes = [ctypes.POINTER(fp), ctypes.POINTER(fp), c_f]
+        L.apply_corrections.restype = c_b
         self.L = L
 
     def model(self, planograms, vol):
@@ -344,21 +351,123 @@ def run_binning(ref, out):
     print("wrote binning", {k: float(v.sum()) for k, v in rec.items() if k[-3:-1] == "_g"})
 
 
+def run_solid_angle(ref, out):
+    """Solid-angle correction (CPU code, src/planogram.cpp:262-302) of all-ones
+    planograms: the output is the per-projection factor, recorded as a table
+    (N_v1, N_v0) for the correction and for its inverse (the model)."""
+    cases = {"sa_g0": GEOMS["g0"], "sa_g0t1": GEOMS["g0t1"], "sa_gpetx": GEOMS["gpetx"],
+             "sa_bench": ([(0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25)], (256, 256, 128, 1.0, 1.0, 0.0, 0.0, 0.0))}
+    rec = {}
+    for name, (plans, vol) in cases.items():
+        ref.model(plans, vol)
+        rec[f"{name}_planograms"] = np.array(plans)
+        rec[f"{name}_volume"] = np.array(vol)
+        for inv in (False, True):
+            gs = [np.ones(sh, np.float32) for sh in ref.shapes()]
+            if not ref.L.set_solid_angle_correction(ref.pp(gs), inv):
+                raise RuntimeError("reference set_solid_angle_correction failed")
+            for i, g in enumerate(gs):
+                tab = g[:, :, :1, :1].copy()
+                if not np.array_equal(np.broadcast_to(tab, g.shape), g):
+                    raise RuntimeError("solid-angle output is not one factor per projection")
+                rec[f"{name}_c{int(inv)}_{i}"] = tab[:, :, 0, 0]
+            del gs
+    np.savez_compressed(os.path.join(out, "solid_angle.npz"), **rec)
+    print("wrote solid angle", sorted(k for k in rec if "_c" in k))
+
+
+def _fov_margin(G, eps):
+    """Pixels of planogram G whose field-of-view test (the projector's ray
+    mask, src/median_filter.cu:26-39) holds with margin eps in float64
+    (eps > 0: surely inside, whatever the float rounding)."""
+    v1 = np.arange(G.N_v1) * G.T_v1 + G.v1_0
+    v0 = np.arange(G.N_v0) * G.T_v0 + G.v0_0
+    u1 = np.arange(G.N_u1) * G.T_u1 + G.u1_0
+    u0 = np.arange(G.N_u0) * G.T_u0 + G.u0_0
+    a = (np.abs(u0)[None, None, None, :] - 0.5 * G.T_u0) <= G.L + G.R * np.abs(v0)[None, :, None, None] - eps
+    b = (np.abs(u1)[None, None, :, None] - 0.5 * G.T_u1) <= G.H - G.R * np.abs(v1)[:, None, None, None] - eps
+    return a & b
+
+
+def run_corrections(ref, out):
+    """apply_corrections (src/petl.cpp:163-192): g / r on the host, then the
+    bad-pixel median in-fill, a CUDA kernel (src/median_filter.cu), so this
+    case needs a GPU.  The reference kernel rewrites g in place while other
+    threads read it; the inputs keep every window free of pixels that the
+    launch rewrites to a different value, so its result is the same whatever
+    the thread order: g is 0 wherever a pixel may lie outside the field of
+    view (those are rewritten to 0; bins on the boundary, where rounding
+    decides, included), and the bad pixels (r below the
+    threshold) are at least 3 apart in (u1, u0).  g holds Poisson counts with
+    a rate drawn per projection (many zeros, so windows hold from 0 to 25
+    good values), r quantized values in [1, 1.5] with the bad bins planted
+    below 0.375 (some at 0); the outputs are stored
+    as the entries where they differ from the plain division g / r."""
+    sys.path.insert(0, ROOT)
+    import oracle as O  # geometry values only
+    rec = {}
+    for name in ("g0", "g0t1", "gpetx"):
+        plans, vol = GEOMS[name]
+        rng = np.random.default_rng(sum(map(ord, "corr_" + name)))
+        ref.model(plans, vol)
+        gs, rs = [], []
+        for p, sh in zip(plans, ref.shapes()):
+            G = O.make_geom(*p, vol)
+            inside = _fov_margin(G, 1e-3)
+            lam = rng.uniform(0.05, 3.0, size=sh[:2])[:, :, None, None]
+            g = rng.poisson(lam, size=sh).astype(np.float32)
+            g[~inside] = 0.0
+            # responses in [1, 1.5]: 0.75 of any projection's median stays
+            # below 1, so only the planted bins fall under the threshold
+            r = (rng.integers(64, 97, size=sh) / 64.0).astype(np.float32)
+            bad = np.zeros(sh, bool)
+            for iv1 in range(sh[0]):
+                for iv0 in range(sh[1]):
+                    taken = []
+                    for _ in range(sh[2] * sh[3] // 12):
+                        j, i = int(rng.integers(sh[2])), int(rng.integers(sh[3]))
+                        if all(max(abs(j - a), abs(i - b)) >= 3 for a, b in taken):
+                            taken.append((j, i))
+                            bad[iv1, iv0, j, i] = True
+            kind = rng.integers(0, 3, size=sh)
+            r[bad & (kind == 0)] = 0.0
+            r[bad & (kind != 0)] = (rng.integers(1, 24, size=int((bad & (kind != 0)).sum())) / 64.0).astype(np.float32)
+            thr = 0.75 * np.median(r.reshape(sh[0] * sh[1], -1), axis=1).reshape(sh[:2])[:, :, None, None]
+            if not np.array_equal(r < thr, bad):
+                raise RuntimeError("bins other than the planted ones fall below the threshold")
+            gs.append(g)
+            rs.append(r)
+        g_in = [g.copy() for g in gs]
+        if not ref.L.apply_corrections(ref.pp(gs), ref.pp(rs), 0.75):
+            raise RuntimeError("reference apply_corrections failed")
+        rec[f"{name}_planograms"] = np.array(plans)
+        rec[f"{name}_volume"] = np.array(vol)
+        for i, (g0, r, g1) in enumerate(zip(g_in, rs, gs)):
+            plain = np.where(r == 0, np.float32(0), g0 / np.where(r == 0, np.float32(1), r)).astype(np.float32)
+            idx = np.flatnonzero(g1.ravel() != plain.ravel())
+            rec[f"{name}_g{i}"], rec[f"{name}_r{i}"] = g0, r
+            rec[f"{name}_idx{i}"], rec[f"{name}_val{i}"] = idx.astype(np.int32), g1.ravel()[idx]
+            print("corrections", name, i, "changed", idx.size, "of", g1.size)
+    np.savez_compressed(os.path.join(out, "corrections.npz"), **rec)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--cpu-only", action="store_true")
+    ap.add_argument("--only", nargs="*", default=None,
+                    help="run only these cases (cpu, binning, solid_angle, corrections, projectors, "
+                         "pfdr_fbp, mlem, regularizers)")
     ap.add_argument("--lib", default=REF_LIB)
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = Ref(a.lib)
-    run_cpu(ref, a.out)
-    run_binning(ref, a.out)
-    if not a.cpu_only:
-        run_projectors(ref, a.out)
-        run_pfdr_fbp(ref, a.out)
-        run_mlem(ref, a.out)
-        run_regularizers(ref, a.out)
+    runs = [("cpu", run_cpu, False), ("binning", run_binning, False), ("solid_angle", run_solid_angle, False),
+            ("corrections", run_corrections, True), ("projectors", run_projectors, True),
+            ("pfdr_fbp", run_pfdr_fbp, True), ("mlem", run_mlem, True), ("regularizers", run_regularizers, True)]
+    for name, fn, gpu in runs:
+        if (a.only is None or name in a.only) and not (gpu and a.cpu_only):
+            fn(ref, a.out)
     return 0
 
 

@@ -190,6 +190,30 @@ def test_mlem_matches_oracle_and_reference(cuda):
         assert rel_l2(_np(f), z[f"f_{tag}"][3]) < 2e-3
 
 
+def test_mlem_with_response_matches_oracle(cuda):
+    """A set response R makes MLEM's model R P (the reference's MLEM turns
+    include_response_with_projectors on): device MLEM and OSEM against the
+    oracle's literal restatement of the reference sequence, through
+    recon.mlem and through PETLserver.MLEM after set_response."""
+    from petl_b200 import PETLserver, recon
+    z = load_golden("mlem_g0.npz")
+    G, Go = product_geoms(z)[0], oracle_geoms(z)[0]
+    rng = np.random.default_rng(21)
+    R = O.solid_angle([Go], [rng.uniform(0.5, 1.0, size=Go.shape).astype(np.float32)], inverse=True)[0]
+    R[rng.random(Go.shape) < 0.02] = 0.0
+    want = O.mlem(Go, z["g"], 4, response=R)
+    f, _ = recon.mlem(G, _t(z["g"], cuda), 4, response=[_t(R, cuda)])
+    assert rel_l2(_np(f), want) < 1e-5
+    # the response changes the result
+    assert rel_l2(want, O.mlem(Go, z["g"], 4)) > 1e-3
+    s = PETLserver()
+    s.add_planogram(*z["planograms"][0])
+    s.set_volume(*[int(v) if i < 3 else float(v) for i, v in enumerate(z["volume"][:5])])
+    s.set_response([R])
+    fs = s.MLEM([z["g"].astype(np.float32)], None, 4)
+    assert rel_l2(fs, want) < 1e-5
+
+
 def test_osem_one_subset_equals_mlem_and_matches_oracle(cuda):
     import torch
     from petl_b200 import recon

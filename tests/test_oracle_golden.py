@@ -181,3 +181,72 @@ def test_binning_nearest_conserves_events():
     assert near.sum() <= lin.sum() + 1e-3
     assert near.sum() >= 0.95 * lin.sum()
     assert np.all(near == np.round(near))
+
+
+# ----------------------------------------------------------------------------
+# corrections
+# ----------------------------------------------------------------------------
+SA_CASES = ["sa_g0", "sa_g0t1", "sa_gpetx", "sa_bench"]
+
+
+def solid_angle_case(z, name):
+    vol = tuple(z[f"{name}_volume"])
+    return [O.make_geom(*p, vol) for p in z[f"{name}_planograms"]]
+
+
+@pytest.mark.parametrize("name", SA_CASES)
+def test_solid_angle_factors_match_reference_exactly(name):
+    """set_solid_angle_correction is host code in the reference: every
+    per-projection factor (and its inverse) matches bit for bit."""
+    z = load_golden("solid_angle.npz")
+    for i, G in enumerate(solid_angle_case(z, name)):
+        for inv in (0, 1):
+            ref = z[f"{name}_c{inv}_{i}"]
+            ones = np.ones(G.shape, np.float32)
+            got = O.solid_angle([G], [ones], inverse=bool(inv))[0]
+            assert np.array_equal(got[:, :, 0, 0], ref)
+            assert np.array_equal(got, np.broadcast_to(ref[:, :, None, None], G.shape))
+
+
+def test_median_rule():
+    """src/vector_ops.cpp:358-374: rank n/2; mean of the two middle ranks in
+    float for even n; 0 for an empty input."""
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 3, 10, 11, 1000, 1001):
+        x = rng.standard_normal(n).astype(np.float32)
+        s = np.sort(x)
+        want = s[n // 2] if n % 2 else np.float32((s[n // 2] + s[n // 2 - 1]) / np.float32(2))
+        assert O.median(x) == want
+    assert O.median(np.zeros(0, np.float32)) == 0.0
+    assert O.median(np.array([3, 1, 3, 3], np.float32)) == 3.0
+
+
+CORR_CASES = ["g0", "g0t1", "gpetx"]
+
+
+def corrections_case(z, name):
+    vol = tuple(z[f"{name}_volume"])
+    geoms = [O.make_geom(*p, vol) for p in z[f"{name}_planograms"]]
+    g = [z[f"{name}_g{i}"] for i in range(len(geoms))]
+    r = [z[f"{name}_r{i}"] for i in range(len(geoms))]
+    want = []
+    for i, (gi, ri) in enumerate(zip(g, r)):
+        plain = np.where(ri == 0, np.float32(0), gi / np.where(ri == 0, np.float32(1), ri)).astype(np.float32)
+        out = plain.ravel().copy()
+        out[z[f"{name}_idx{i}"]] = z[f"{name}_val{i}"]
+        want.append(out.reshape(gi.shape))
+    return geoms, g, r, want
+
+
+@pytest.mark.parametrize("name", CORR_CASES)
+def test_apply_corrections_matches_reference_exactly(name):
+    """apply_corrections (host division, then the reference's CUDA bad-pixel
+    kernel on a GPU): the oracle matches the reference's output bit for bit
+    on inputs whose windows the reference kernel does not rewrite."""
+    z = load_golden("corrections.npz")
+    geoms, g, r, want = corrections_case(z, name)
+    got = O.apply_corrections(geoms, g, r, 0.75)
+    for i, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a, b), (name, i, int((a != b).sum()))
+        # the case exercises zeroing, in-fill and untouched bins
+        assert z[f"{name}_idx{i}"].size > 0
