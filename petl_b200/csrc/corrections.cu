@@ -39,7 +39,9 @@ namespace {
 
 constexpr int kCorrThreads = 512;
 constexpr int kCorrWarps = kCorrThreads / 32;
-constexpr int kStageMax = 49152;  // bins of one projection staged in shared memory
+constexpr int kStageMax = 45056;  // bins of one projection staged in shared memory
+constexpr int kDigitBits = 12;    // width of the median search's first histogram
+constexpr int kListMax = 2048;    // keys of the median's buckets resolved from a list
 
 // float -> unsigned key with the same order (negative values reversed)
 __device__ __forceinline__ unsigned ordered_key(float x)
@@ -54,10 +56,11 @@ __device__ __forceinline__ float key_value(unsigned k)
 }
 
 struct SelectSmem {
-    unsigned hist[kCorrWarps * 256];
-    unsigned tot[256];
-    unsigned bcast[2];
+    unsigned hist[1 << kDigitBits];
+    unsigned list[kListMax];
     unsigned red[2 * kCorrWarps];
+    unsigned bcast[8];
+    int box[4];  // visible columns [box0, box1] and rows [box2, box3] of the projection
 };
 
 __device__ __forceinline__ unsigned block_min_max(unsigned lo, unsigned hi, SelectSmem& s, unsigned* hi_out)
@@ -82,88 +85,100 @@ __device__ __forceinline__ unsigned block_min_max(unsigned lo, unsigned hi, Sele
     return lo;
 }
 
-// Key of rank k (0-based, ascending) among the n values x[0..n).  The bits
-// that the smallest and largest keys share are common to all keys; the rest
-// are resolved from the most significant end in digits of up to 8 bits, one
-// pass over x per digit, with per-warp histograms in which same-digit lanes
-// are combined (__match_any_sync) and warps with no candidate lane skip the
-// combine.  *below_equal receives the number of values equal to the result
-// that rank below k.
-__device__ unsigned select_rank(const float* x, int n, unsigned k, SelectSmem& s, unsigned* below_equal)
+// Exclusive prefix sum of v over the block's threads; *total gets the sum.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, SelectSmem& s, unsigned* total)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned lo = 0xffffffffu, hi = 0;
-    for (int i = threadIdx.x; i < n; i += kCorrThreads) {
-        const unsigned key = ordered_key(x[i]);
-        lo = min(lo, key);
-        hi = max(hi, key);
+    unsigned incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
     }
-    lo = block_min_max(lo, hi, s, &hi);
-    if (lo == hi) {
-        *below_equal = k;
-        return lo;
+    __syncthreads();  // s.red may still be read by an earlier call
+    if (lane == 31) s.red[warp] = incl;
+    __syncthreads();
+    unsigned before = 0, tot = 0;
+    for (int w = 0; w < kCorrWarps; w++) {
+        const unsigned t = s.red[w];
+        before += w < warp ? t : 0u;
+        tot += t;
     }
-    const int free_bits = 32 - __clz(lo ^ hi);
-    unsigned prefix = free_bits == 32 ? 0u : (lo & (0xffffffffu << free_bits)), kk = k;
+    *total = tot;
+    return before + incl - v;
+}
+
+// Bins of a histogram holding ranks ka and kb (kb <= ka): bcast[0] = bin of
+// ka, bcast[1] = rank of ka inside it, bcast[2] = bin of kb, bcast[3] =
+// number of keys in the bins below kb's.
+__device__ void locate_ranks(const unsigned* hist, int nbins, unsigned ka, unsigned kb, SelectSmem& s)
+{
+    const int per = (nbins + kCorrThreads - 1) / kCorrThreads, b0 = threadIdx.x * per;
+    unsigned sum = 0;
+    for (int j = 0; j < per; j++)
+        if (b0 + j < nbins) sum += hist[b0 + j];
+    unsigned total;
+    unsigned before = block_exclusive_scan(sum, s, &total);
+    for (int j = 0; j < per && b0 + j < nbins; j++) {
+        const unsigned c = hist[b0 + j];
+        if (ka >= before && ka < before + c) {
+            s.bcast[0] = b0 + j;
+            s.bcast[1] = ka - before;
+        }
+        if (kb >= before && kb < before + c) {
+            s.bcast[2] = b0 + j;
+            s.bcast[3] = before;
+        }
+        before += c;
+    }
+    __syncthreads();
+}
+
+// Key of rank k among the n keys key_at(0..n), all of which share with
+// `prefix` the bits at and above `top`: bits [0, top) are resolved from the
+// most significant end in digits of up to 8 bits, one pass per digit, lanes
+// with the same digit combined (__match_any_sync) and warps without a
+// candidate skipping the combine.  *below_equal receives the number of keys
+// equal to the result that rank below k.
+template <class KeyAt>
+__device__ unsigned radix_rank(KeyAt key_at, int n, unsigned prefix, int top, unsigned k, SelectSmem& s,
+                               unsigned* below_equal)
+{
+    const int lane = threadIdx.x & 31;
     const int nround = (n + kCorrThreads - 1) / kCorrThreads * kCorrThreads;
-    for (int top = free_bits; top > 0; top -= 8) {
+    unsigned kk = k;
+    for (; top > 0; top -= 8) {
         const int shift = max(top - 8, 0);
         const unsigned above = top == 32 ? 0u : (0xffffffffu << top), dmask = (1u << (top - shift)) - 1u;
-        for (int i = threadIdx.x; i < kCorrWarps * 256; i += kCorrThreads) s.hist[i] = 0;
+        __syncthreads();  // the histogram may still be read by an earlier step
+        for (int i = threadIdx.x; i < 256; i += kCorrThreads) s.hist[i] = 0;
         __syncthreads();
-        unsigned* wh = s.hist + warp * 256;
         for (int i = threadIdx.x; i < nround; i += kCorrThreads) {
             unsigned d = 256;
             if (i < n) {
-                const unsigned key = ordered_key(x[i]);
+                const unsigned key = key_at(i);
                 if ((key & above) == prefix) d = (key >> shift) & dmask;
             }
             if (__any_sync(0xffffffffu, d < 256)) {
                 const unsigned peers = __match_any_sync(0xffffffffu, d);
-                if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&wh[d], unsigned(__popc(peers)));
+                if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&s.hist[d], unsigned(__popc(peers)));
             }
         }
         __syncthreads();
-        if (threadIdx.x < 256) {
-            unsigned t = 0;
-            for (int w = 0; w < kCorrWarps; w++) t += s.hist[w * 256 + threadIdx.x];
-            s.tot[threadIdx.x] = t;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            unsigned c[8], sum = 0;
-            for (int j = 0; j < 8; j++) {
-                c[j] = s.tot[lane * 8 + j];
-                sum += c[j];
-            }
-            unsigned incl = sum;
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            unsigned before = incl - sum;
-            for (int j = 0; j < 8; j++) {
-                if (kk >= before && kk < before + c[j]) {
-                    s.bcast[0] = prefix | (unsigned(lane * 8 + j) << shift);
-                    s.bcast[1] = kk - before;
-                }
-                before += c[j];
-            }
-        }
-        __syncthreads();
-        prefix = s.bcast[0];
+        locate_ranks(s.hist, 256, kk, kk, s);
+        prefix |= s.bcast[0] << shift;
         kk = s.bcast[1];
     }
     *below_equal = kk;
     return prefix;
 }
 
-// Largest key below `bound` among x[0..n) (0 if none).
-__device__ unsigned max_key_below(const float* x, int n, unsigned bound, SelectSmem& s)
+// Largest key below `bound` among key_at(0..n) (0 if none).
+template <class KeyAt>
+__device__ unsigned max_key_below(KeyAt key_at, int n, unsigned bound, SelectSmem& s)
 {
     unsigned m = 0;
     for (int i = threadIdx.x; i < n; i += kCorrThreads) {
-        const unsigned key = ordered_key(x[i]);
+        const unsigned key = key_at(i);
         if (key < bound && key > m) m = key;
     }
     unsigned mx;
@@ -171,18 +186,73 @@ __device__ unsigned max_key_below(const float* x, int n, unsigned bound, SelectS
     return mx;
 }
 
-// Median of x[0..n) as src/vector_ops.cpp:358-374 defines it: rank n/2, and
-// for even n the float mean of ranks n/2 and n/2 - 1.
-__device__ float block_median(const float* x, int n, SelectSmem& s)
+__device__ __forceinline__ float mean2(unsigned a, unsigned b)
+{
+    return __fdiv_rn(__fadd_rn(key_value(a), key_value(b)), 2.0f);
+}
+
+// Median of the n floats val(0..n) as src/vector_ops.cpp:358-374 defines
+// it (rank n/2; for even n the float mean of ranks n/2 and n/2 - 1), given
+// the smallest and largest of their keys.  One histogram pass over the top
+// kDigitBits bits that the keys do not all share finds the buckets of the
+// two ranks; a second pass lists the keys of those buckets, and the ranks
+// are resolved on the list (on all keys if the list overflows).
+template <class ValAt>
+__device__ float block_median(ValAt val, int n, unsigned lo, unsigned hi, SelectSmem& s)
 {
     const unsigned mid = unsigned(n) / 2;
-    unsigned eq_below = 0;
-    const unsigned up = select_rank(x, n, mid, s, &eq_below);
-    const float upper = key_value(up);
-    if (n & 1) return upper;
-    // rank mid - 1 equals rank mid when a copy of it ranks below mid
-    const float lower = eq_below > 0 ? upper : key_value(max_key_below(x, n, up, s));
-    return __fdiv_rn(__fadd_rn(upper, lower), 2.0f);
+    const bool even = (n & 1) == 0;
+    if (lo == hi) return even ? mean2(lo, lo) : key_value(lo);
+    const int lane = threadIdx.x & 31;
+    const int free_bits = 32 - __clz(lo ^ hi);
+    const unsigned common = free_bits == 32 ? 0u : (lo & (0xffffffffu << free_bits));
+    const int dbits = min(kDigitBits, free_bits), shift = free_bits - dbits;
+    const unsigned dmask = (1u << dbits) - 1u;
+    const int nround = (n + kCorrThreads - 1) / kCorrThreads * kCorrThreads;
+    for (int i = threadIdx.x; i < (1 << dbits); i += kCorrThreads) s.hist[i] = 0;
+    if (threadIdx.x == 0) s.bcast[4] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nround; i += kCorrThreads) {
+        const unsigned d = i < n ? (ordered_key(val(i)) >> shift) & dmask : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (i < n && lane == __ffs(peers) - 1) atomicAdd(&s.hist[d], unsigned(__popc(peers)));
+    }
+    __syncthreads();
+    locate_ranks(s.hist, 1 << dbits, mid, even ? mid - 1 : mid, s);
+    const unsigned b_up = s.bcast[0], b_lo = s.bcast[2], base = s.bcast[3];
+    for (int i = threadIdx.x; i < nround; i += kCorrThreads) {
+        unsigned key = 0;
+        bool take = false;
+        if (i < n) {
+            key = ordered_key(val(i));
+            const unsigned d = (key >> shift) & dmask;
+            take = d >= b_lo && d <= b_up;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, take);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned pos0 = 0;
+            if (lane == leader) pos0 = atomicAdd(&s.bcast[4], unsigned(__popc(m)));
+            pos0 = __shfl_sync(0xffffffffu, pos0, leader);
+            const unsigned pos = pos0 + __popc(m & ((1u << lane) - 1u));
+            if (take && pos < kListMax) s.list[pos] = key;
+        }
+    }
+    __syncthreads();
+    const unsigned cnt = s.bcast[4];
+    unsigned eq_below, up, low;
+    if (cnt <= kListMax) {
+        auto listed = [&](int i) { return s.list[i]; };
+        up = radix_rank(listed, int(cnt), common, free_bits, mid - base, s, &eq_below);
+        if (!even) return key_value(up);
+        low = eq_below > 0 ? up : max_key_below(listed, int(cnt), up, s);
+    } else {
+        auto keyed = [&](int i) { return ordered_key(val(i)); };
+        up = radix_rank(keyed, n, common, free_bits, mid, s, &eq_below);
+        if (!even) return key_value(up);
+        low = eq_below > 0 ? up : max_key_below(keyed, n, up, s);
+    }
+    return mean2(up, low);
 }
 
 // Sorts 32 values held in registers (bitonic network, fully unrolled so that
@@ -256,15 +326,20 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes)
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ float divided(float g, float r) { return (r == 0.0f) ? 0.0f : __fdiv_rn(g, r); }
+
 // Persistent CTAs, one per SM, each correcting projections view0 + b,
-// view0 + b + gridDim.x, ...  STAGE: the projection's response, then its
-// divided values, live in shared memory next to a bitmask of the bins below
-// the threshold; the bins are written in one pass (zero outside the field of
-// view, g / r elsewhere) and the bins below the threshold are then
-// overwritten with their window medians, spread evenly over the threads by
-// their rank in the bitmask.  Otherwise (projections too large to stage) the
-// divided values go to scratch + blockIdx.x * n and every bin is written
-// once, in-filled where its response is below the threshold.
+// view0 + b + gridDim.x, ... while the next one is prefetched into L2.
+// Per projection: the visible columns and rows (two intervals), the
+// response's key range, its median, then
+//   STAGE: the response is staged in shared memory and replaced by the
+//   divided values while a bitmask records the bins below the threshold;
+//   every bin is written once (zero outside the field of view, g / r
+//   inside) and the visible bins below the threshold are then overwritten
+//   with their window medians, spread evenly over the threads by their rank
+//   in the bitmask;
+//   otherwise (projections too large to stage): the divided values go to
+//   scratch + blockIdx.x * n and every bin is written once.
 template <bool STAGE>
 __global__ void __launch_bounds__(kCorrThreads, 1) k_apply_corrections(const CorrArgs a)
 {
@@ -272,139 +347,187 @@ __global__ void __launch_bounds__(kCorrThreads, 1) k_apply_corrections(const Cor
     const petl_geom& G = a.G;
     const int N1 = G.N_u1, N0 = G.N_u0, n = N1 * N0;
     const int n4 = (n + 3) & ~3, nw = (n + 31) / 32;
+    const int lane = threadIdx.x & 31;
     float* d = reinterpret_cast<float*>(smem_raw);
     unsigned* bad = reinterpret_cast<unsigned*>(d + n4);
     unsigned* rank = bad + nw + 1;
     SelectSmem& s = *reinterpret_cast<SelectSmem*>(STAGE ? reinterpret_cast<unsigned char*>(rank + nw + 1)
                                                          : smem_raw);
-    // float4 paths need every projection 16-byte aligned
-    const bool vec = (n & 3) == 0 && ((reinterpret_cast<uintptr_t>(a.g) | reinterpret_cast<uintptr_t>(a.r)) & 15) == 0;
-    const size_t bytes = size_t(n) * 4;
+    // float4 paths: rows of whole float4s, every projection 16-byte aligned
+    const bool vec =
+        (N0 & 3) == 0 && ((reinterpret_cast<uintptr_t>(a.g) | reinterpret_cast<uintptr_t>(a.r)) & 15) == 0;
+    const uint32_t bytes = uint32_t(n) * 4u;
     if (threadIdx.x == 0 && vec && blockIdx.x < a.nviews) {
         const size_t v = size_t(a.view0) + blockIdx.x;
-        prefetch_l2(a.r + v * n, uint32_t(bytes));
-        prefetch_l2(a.g + v * n, uint32_t(bytes));
+        prefetch_l2(a.r + v * n, bytes);
+        prefetch_l2(a.g + v * n, bytes);
     }
     for (int vi = blockIdx.x; vi < a.nviews; vi += gridDim.x) {
         const int view = a.view0 + vi;
         const int iv1 = view / G.N_v0, iv0 = view % G.N_v0;
         float* gv = a.g + size_t(view) * n;
         const float* rv = a.r + size_t(view) * n;
-        if (threadIdx.x == 0 && vec && vi + gridDim.x < a.nviews) {
-            const size_t nx = size_t(view) + gridDim.x;
-            prefetch_l2(a.r + nx * n, uint32_t(bytes));
-            prefetch_l2(a.g + nx * n, uint32_t(bytes));
-        }
-        float* dd = STAGE ? d : a.scratch + size_t(blockIdx.x) * n;
-        if (STAGE) {
-            if (vec) {
-                const float4* r4 = reinterpret_cast<const float4*>(rv);
-                float4* d4 = reinterpret_cast<float4*>(d);
-#pragma unroll 8
-                for (int i = threadIdx.x; i < n / 4; i += kCorrThreads) d4[i] = __ldcs(r4 + i);
-            } else {
-                for (int i = threadIdx.x; i < n; i += kCorrThreads) d[i] = __ldcs(rv + i);
+        if (threadIdx.x == 0) {
+            if (vec && vi + gridDim.x < a.nviews) {
+                const size_t nx = size_t(view) + gridDim.x;
+                prefetch_l2(a.r + nx * n, bytes);
+                prefetch_l2(a.g + nx * n, bytes);
             }
-            __syncthreads();
+            s.box[0] = N0;
+            s.box[1] = -1;
+            s.box[2] = N1;
+            s.box[3] = -1;
         }
-        const float thr = __fmul_rn(a.rel, block_median(STAGE ? d : rv, n, s));
-        if (STAGE) {
-            // bins below the threshold, one bit each
-            const int nround = nw * 32;
-            for (int i = threadIdx.x; i < ((nround + kCorrThreads - 1) / kCorrThreads) * kCorrThreads;
-                 i += kCorrThreads) {
-                const unsigned w = __ballot_sync(0xffffffffu, i < n && d[i] < thr);
-                if ((threadIdx.x & 31) == 0 && i < nround) bad[i >> 5] = w;
-            }
-        }
-        // divided values (src/data_cube.cpp:144-149)
+        // the response (staged) and its key range
+        unsigned lo = 0xffffffffu, hi = 0;
         if (STAGE && vec) {
-            const float4* g4 = reinterpret_cast<const float4*>(gv);
+            const float4* r4 = reinterpret_cast<const float4*>(rv);
             float4* d4 = reinterpret_cast<float4*>(d);
 #pragma unroll 4
             for (int i = threadIdx.x; i < n / 4; i += kCorrThreads) {
-                const float4 x = __ldcs(g4 + i);
-                float4 r = d4[i];
-                r.x = (r.x == 0.0f) ? 0.0f : __fdiv_rn(x.x, r.x);
-                r.y = (r.y == 0.0f) ? 0.0f : __fdiv_rn(x.y, r.y);
-                r.z = (r.z == 0.0f) ? 0.0f : __fdiv_rn(x.z, r.z);
-                r.w = (r.w == 0.0f) ? 0.0f : __fdiv_rn(x.w, r.w);
-                d4[i] = r;
+                const float4 x = __ldcs(r4 + i);
+                d4[i] = x;
+                const unsigned k0 = ordered_key(x.x), k1 = ordered_key(x.y), k2 = ordered_key(x.z),
+                               k3 = ordered_key(x.w);
+                lo = min(min(lo, min(k0, k1)), min(k2, k3));
+                hi = max(max(hi, max(k0, k1)), max(k2, k3));
             }
         } else {
             for (int i = threadIdx.x; i < n; i += kCorrThreads) {
-                const float r = STAGE ? d[i] : rv[i];
-                dd[i] = (r == 0.0f) ? 0.0f : __fdiv_rn(__ldcs(gv + i), r);
+                const float x = __ldcs(rv + i);
+                if (STAGE) d[i] = x;
+                lo = min(lo, ordered_key(x));
+                hi = max(hi, ordered_key(x));
             }
         }
-        __syncthreads();
+        lo = block_min_max(lo, hi, s, &hi);  // (its barriers also publish the stage and the box reset)
+        for (int c = threadIdx.x; c < N0; c += kCorrThreads)
+            if (u0_visible(G, iv0, c)) {
+                atomicMin(&s.box[0], c);
+                atomicMax(&s.box[1], c);
+            }
+        for (int r = threadIdx.x; r < N1; r += kCorrThreads)
+            if (u1_visible(G, iv1, r)) {
+                atomicMin(&s.box[2], r);
+                atomicMax(&s.box[3], r);
+            }
+        __syncthreads();  // the box is read below (the median may take no barrier)
+        float med;
+        if (STAGE)
+            med = block_median([&](int i) { return d[i]; }, n, lo, hi, s);
+        else
+            med = block_median([&](int i) { return rv[i]; }, n, lo, hi, s);
+        const float thr = __fmul_rn(a.rel, med);
+        const int c0 = s.box[0], c1 = s.box[1], r0 = s.box[2], r1 = s.box[3];
+        auto visible = [&](int row, int col) { return col >= c0 && col <= c1 && row >= r0 && row <= r1; };
+
         if (!STAGE) {
+            float* dd = a.scratch + size_t(blockIdx.x) * n;
+            for (int i = threadIdx.x; i < n; i += kCorrThreads) dd[i] = divided(__ldcs(gv + i), rv[i]);
+            __syncthreads();
             for (int i = threadIdx.x; i < n; i += kCorrThreads) {
-                const int iu1 = i / N0, iu0 = i - iu1 * N0;
-                float out;
-                if (!ray_visible(G, iv1, iv0, iu1, iu0))
-                    out = 0.0f;
-                else
-                    out = rv[i] < thr ? window_fill(dd, N1, N0, iu1, iu0, thr) : dd[i];
+                const int row = i / N0, col = i - row * N0;
+                float out = 0.0f;
+                if (visible(row, col)) out = rv[i] < thr ? window_fill(dd, N1, N0, row, col, thr) : dd[i];
                 __stcs(gv + i, out);
             }
             __syncthreads();  // the scratch slice is rewritten for the next projection
             continue;
         }
-        // every bin: zero outside the field of view, else g / r
+        // divided values in place of the response, and the bitmask of the
+        // bins below the threshold (src/data_cube.cpp:144-149)
         if (vec) {
+            const float4* g4 = reinterpret_cast<const float4*>(gv);
+            float4* d4 = reinterpret_cast<float4*>(d);
+            const int q4 = n / 4, qround = (q4 + kCorrThreads - 1) / kCorrThreads * kCorrThreads;
+#pragma unroll 2
+            for (int i4 = threadIdx.x; i4 < qround; i4 += kCorrThreads) {
+                unsigned nib = 0;
+                if (i4 < q4) {
+                    const float4 x = __ldcs(g4 + i4);
+                    float4 r = d4[i4];
+                    nib = unsigned(r.x < thr) | unsigned(r.y < thr) << 1 | unsigned(r.z < thr) << 2 |
+                          unsigned(r.w < thr) << 3;
+                    r.x = divided(x.x, r.x);
+                    r.y = divided(x.y, r.y);
+                    r.z = divided(x.z, r.z);
+                    r.w = divided(x.w, r.w);
+                    d4[i4] = r;
+                }
+                // lanes 8j..8j+7 hold the 32 bins of one bitmask word
+                unsigned w = nib << (4 * (lane & 7));
+                w |= __shfl_xor_sync(0xffffffffu, w, 1);
+                w |= __shfl_xor_sync(0xffffffffu, w, 2);
+                w |= __shfl_xor_sync(0xffffffffu, w, 4);
+                if ((lane & 7) == 0 && i4 < q4) bad[i4 >> 3] = w;
+            }
+        } else {
+            const int nround = nw * 32, iround = (nround + kCorrThreads - 1) / kCorrThreads * kCorrThreads;
+            for (int i = threadIdx.x; i < iround; i += kCorrThreads) {
+                const bool b = i < n && d[i] < thr;
+                if (i < n) d[i] = divided(__ldcs(gv + i), d[i]);
+                const unsigned w = __ballot_sync(0xffffffffu, b);
+                if (lane == 0 && i < nround) bad[i >> 5] = w;
+            }
+        }
+        __syncthreads();
+        // every bin: zero outside the field of view, g / r inside
+        if (vec) {
+            const float4* d4 = reinterpret_cast<const float4*>(d);
             float4* o4 = reinterpret_cast<float4*>(gv);
+            const int step = 4 * kCorrThreads, drow = step / N0, dcol = step - drow * N0;
+            int row = (4 * threadIdx.x) / N0, col = 4 * threadIdx.x - row * N0;
             for (int i4 = threadIdx.x; i4 < n / 4; i4 += kCorrThreads) {
-                float4 x = reinterpret_cast<const float4*>(d)[i4];
-                int iu1 = (4 * i4) / N0, iu0 = 4 * i4 - iu1 * N0;
-                auto mask = [&](float& c) {
-                    if (!ray_visible(G, iv1, iv0, iu1, iu0)) c = 0.0f;
-                    if (++iu0 == N0) {
-                        iu0 = 0;
-                        iu1++;
-                    }
-                };
-                mask(x.x);
-                mask(x.y);
-                mask(x.z);
-                mask(x.w);
+                float4 x = d4[i4];
+                if (!(row >= r0 && row <= r1)) {
+                    x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                } else {
+                    x.x = (col >= c0 && col <= c1) ? x.x : 0.0f;
+                    x.y = (col + 1 >= c0 && col + 1 <= c1) ? x.y : 0.0f;
+                    x.z = (col + 2 >= c0 && col + 2 <= c1) ? x.z : 0.0f;
+                    x.w = (col + 3 >= c0 && col + 3 <= c1) ? x.w : 0.0f;
+                }
                 __stcs(o4 + i4, x);
+                row += drow;
+                col += dcol;
+                if (col >= N0) {
+                    col -= N0;
+                    row++;
+                }
             }
         } else {
             for (int i = threadIdx.x; i < n; i += kCorrThreads) {
-                const int iu1 = i / N0, iu0 = i - iu1 * N0;
-                __stcs(gv + i, ray_visible(G, iv1, iv0, iu1, iu0) ? d[i] : 0.0f);
+                const int row = i / N0, col = i - row * N0;
+                __stcs(gv + i, visible(row, col) ? d[i] : 0.0f);
             }
         }
-        // rank of the first bad bin of each bitmask word (exclusive scan)
-        if (threadIdx.x < 32) {
-            unsigned carry = 0;
-            for (int w0 = 0; w0 < nw; w0 += 32) {
-                const int w = w0 + threadIdx.x;
-                const unsigned c = w < nw ? __popc(bad[w]) : 0u;
-                unsigned incl = c;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (threadIdx.x >= o) incl += y;
-                }
-                if (w < nw) rank[w] = carry + incl - c;
-                carry += __shfl_sync(0xffffffffu, incl, 31);
+        // rank of the first bin below the threshold in each bitmask word
+        const int per = (nw + kCorrThreads - 1) / kCorrThreads, w0 = threadIdx.x * per;
+        unsigned cnt = 0;
+        for (int j = 0; j < per; j++)
+            if (w0 + j < nw) cnt += __popc(bad[w0 + j]);
+        unsigned nbad;
+        unsigned before = block_exclusive_scan(cnt, s, &nbad);
+        for (int j = 0; j < per; j++)
+            if (w0 + j < nw) {
+                rank[w0 + j] = before;
+                before += __popc(bad[w0 + j]);
             }
-            if (threadIdx.x == 0) rank[nw] = carry;
-        }
-        __syncthreads();  // orders the bulk writes above before the in-fill overwrites
-        const unsigned nbad = rank[nw];
+        __syncthreads();  // (also orders the bulk writes above before the in-fill overwrites)
         for (unsigned q = threadIdx.x; q < nbad; q += kCorrThreads) {
-            int lo = 0, hi = nw - 1;  // last word whose first rank is <= q
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (rank[mid] <= q) lo = mid; else hi = mid - 1;
+            int wlo = 0, whi = nw - 1;  // last word whose first rank is <= q
+            while (wlo < whi) {
+                const int m = (wlo + whi + 1) >> 1;
+                if (rank[m] <= q)
+                    wlo = m;
+                else
+                    whi = m - 1;
             }
-            const unsigned bit = __fns(bad[lo], 0, int(q - rank[lo]) + 1);
-            const int i = lo * 32 + int(bit);
-            if (bit >= 32 || i >= n) continue;  // not reached: q ranks a set bit of word lo
-            const int iu1 = i / N0, iu0 = i - iu1 * N0;
-            if (ray_visible(G, iv1, iv0, iu1, iu0)) __stcs(gv + i, window_fill(d, N1, N0, iu1, iu0, thr));
+            const unsigned bit = __fns(bad[wlo], 0, int(q - rank[wlo]) + 1);
+            const int i = wlo * 32 + int(bit);
+            if (bit >= 32 || i >= n) continue;  // not reached: q ranks a set bit of word wlo
+            const int row = i / N0, col = i - row * N0;
+            if (visible(row, col)) __stcs(gv + i, window_fill(d, N1, N0, row, col, thr));
         }
         __syncthreads();  // shared memory is restaged for the next projection
     }

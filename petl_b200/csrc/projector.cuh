@@ -14,16 +14,27 @@
 namespace petl {
 
 // The ray masks of the reference's forward kernel, evaluated in float with
-// fused multiply-adds as the reference's compiled kernel evaluates them.
-__device__ __forceinline__ bool ray_visible(const petl_geom& G, int iv1, int iv0, int iu1, int iu0)
+// fused multiply-adds as the reference's compiled kernel evaluates them:
+// the u0 test depends on (iv0, iu0) only, the u1 test on (iv1, iu1) only.
+// Each holds on an interval of its bin index (the tests are monotone in
+// |u0| and |u1|).
+__device__ __forceinline__ bool u0_visible(const petl_geom& G, int iv0, int iu0)
+{
+    const float v0 = ffma(float(iv0), G.T_v0, G.v0_0);
+    const float u0 = ffma(float(iu0), G.T_u0, G.u0_0);
+    return !(fsub(fabsf(u0), fmul(0.5f, G.T_u0)) > ffma(G.R, fabsf(v0), G.L));
+}
+
+__device__ __forceinline__ bool u1_visible(const petl_geom& G, int iv1, int iu1)
 {
     const float v1 = ffma(float(iv1), G.T_v1, G.v1_0);
-    const float v0 = ffma(float(iv0), G.T_v0, G.v0_0);
     const float u1 = ffma(float(iu1), G.T_u1, G.u1_0);
-    const float u0 = ffma(float(iu0), G.T_u0, G.u0_0);
-    if (fsub(fabsf(u0), fmul(0.5f, G.T_u0)) > ffma(G.R, fabsf(v0), G.L)) return false;
-    if (fsub(fabsf(u1), fmul(0.5f, G.T_u1)) > ffma(-G.R, fabsf(v1), G.H)) return false;
-    return true;
+    return !(fsub(fabsf(u1), fmul(0.5f, G.T_u1)) > ffma(-G.R, fabsf(v1), G.H));
+}
+
+__device__ __forceinline__ bool ray_visible(const petl_geom& G, int iv1, int iv0, int iu1, int iu0)
+{
+    return u0_visible(G, iv0, iu0) && u1_visible(G, iv1, iu1);
 }
 
 struct RayGeom {

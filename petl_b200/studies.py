@@ -5,6 +5,7 @@
     python -m petl_b200.studies storage     # 256x256x128 OSEM 10 x 8 subsets, FP32 vs BF16 storage
     python -m petl_b200.studies serving     # 200 Poisson-arrival OSEM requests, p50/p99
     python -m petl_b200.studies binning     # list-mode binning, device and C-ABI file rates
+    python -m petl_b200.studies corrections # solid angle and apply_corrections, device and C ABI
 
 All inputs are synthetic and seeded: ellipsoid phantoms (replace semantics,
 later ellipsoids overwrite earlier ones), forward projected with the
@@ -299,14 +300,82 @@ def study_binning(seed=0, n_events=16_000_000, n_file=8_000_000, tmpdir="/tmp"):
     return res
 
 
+def study_corrections(seed=0, reps=5):
+    """Planogram corrections on the 256x256x128 geometry's planogram
+    (65,129,128,256), device-resident: the solid-angle scaling (8 bytes of
+    HBM traffic per bin) and apply_corrections (12 bytes per bin) with two
+    responses: detector gaps (responses in [0.9, 1.1], 2 % of the bins at a
+    tenth of that: 2 % of the bins in-filled) and a stress case (responses
+    in [0.5, 1.5]: a quarter of the bins in-filled).  Then both through the
+    reference C ABI on pinned host arrays."""
+    from .server import PETLserver
+    args = (0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25)
+    G = Geometry(*args, volume=(256, 256, 128, 1.0))
+    rng = np.random.default_rng(seed)
+    sh = G.shape
+    nbins = int(np.prod(sh))
+    g_h = rng.poisson(1.0, size=sh).astype(np.float32)
+    g = torch.from_numpy(g_h).cuda()
+    work = torch.empty_like(g)
+    flush = torch.empty(64 << 20, device="cuda", dtype=torch.float32)  # 256 MB > L2
+    res = {"study": "corrections", "workload": "planogram (65,129,128,256) of add_planogram(0, 256, 128, 128, "
+           "T=1, 0.5, 0.25), Poisson(1) data; L2 flushed before each timed call", "bins": nbins}
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            work.copy_(g)
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    t = timed(lambda: ops.solid_angle_(G, work))
+    res.update({"solid_angle_ms": t, "solid_angle_gbs": 8.0 * nbins / (t * 1e6)})
+    responses = {}
+    r = rng.uniform(0.9, 1.1, size=sh).astype(np.float32)
+    r[rng.random(sh) < 0.02] *= np.float32(0.1)
+    responses["gaps"] = r
+    responses["stress"] = rng.uniform(0.5, 1.5, size=sh).astype(np.float32)
+    for key, r_h in responses.items():
+        r = torch.from_numpy(r_h).cuda()
+        t = timed(lambda: ops.apply_corrections_(G, work, r, 0.75))
+        res.update({f"corrections_{key}_ms": t, f"corrections_{key}_gbs": 12.0 * nbins / (t * 1e6)})
+    del r
+    s = PETLserver()
+    s.add_planogram(*args)
+    gp = [torch.from_numpy(g_h).pin_memory().numpy()]
+    rp = [torch.from_numpy(responses["gaps"]).pin_memory().numpy()]
+    s.set_response(rp)
+    ts = []
+    for _ in range(3):
+        gp[0][:] = g_h
+        t0 = time.perf_counter()
+        s.apply_corrections(gp)
+        ts.append(time.perf_counter() - t0)
+    res["cabi_corrections_gaps_ms"] = 1e3 * min(ts)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        s.apply_solid_angle_correction(gp)
+        ts.append(time.perf_counter() - t0)
+    res["cabi_solid_angle_ms"] = 1e3 * min(ts)
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving", "binning"])
+    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving", "binning", "corrections"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--requests", type=int, default=200)
     a = ap.parse_args(argv)
     fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
-          "binning": study_binning}
+          "binning": study_binning, "corrections": study_corrections}
     if a.study == "serving":
         res = study_serving(n=a.requests, seed=a.seed)
     else:

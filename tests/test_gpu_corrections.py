@@ -62,7 +62,10 @@ def test_cabi_solid_angle_matches_reference(cuda):
 def _random_case(shape, rng, bad_frac=0.05, distinct=False, zero_frac=0.01):
     lam = rng.uniform(0.05, 3.0, size=shape[:2])[:, :, None, None]
     g = rng.poisson(lam, size=shape).astype(np.float32)
-    if distinct:
+    if distinct == "few":
+        # three response values: the median's bucket outgrows the kernel's list
+        r = rng.choice(np.array([1.0, 1.25, 1.5], np.float32), size=shape)
+    elif distinct:
         r = rng.uniform(0.5, 1.5, size=shape).astype(np.float32)
     else:
         r = (rng.integers(48, 97, size=shape) / 64.0).astype(np.float32)
@@ -83,6 +86,10 @@ def _random_case(shape, rng, bad_frac=0.05, distinct=False, zero_frac=0.01):
     ((90.0, 48.0, 24.0, 16.0, 1.0, 0.5, 0.25), False),
     # 256 x 266 bins per projection: more than the shared-memory stage holds
     ((0.0, 128.0, 64.0, 64.0, 0.25, 0.02, 0.01), True),
+    # 30 bins per row: rows are not whole float4s (the scalar staging path)
+    ((0.0, 64.0, 30.0, 16.0, 2.0, 0.5, 0.25), True),
+    # 128 x 140 bins with three response values
+    ((0.0, 256.0, 128.0, 128.0, 1.0, 0.05, 0.02), "few"),
 ])
 def test_device_apply_corrections_matches_oracle(cuda, args, distinct):
     from petl_b200 import Geometry, ops, lib
