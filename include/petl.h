@@ -61,20 +61,32 @@ bool set_default_volume(float scale);                    /* :52 */
 bool set_volume(int numX, int numY, int numZ, float voxelWidth, float voxelHeight,
                 float offsetX, float offsetY, float offsetZ);   /* :53 */
 
-/* --- outside the reconstruction path: exported, return false --------------- */
+/* --- list-mode binning, phantoms, detector modules, scatter ---------------- */
 /* List-mode binning of a coincidence file (.lst records, else the binary
  * acquisition format) into every planogram, overwriting g: bilinear in
  * (u1, u0), z from the chest wall, mm -- the reference's defaults
  * (src/petl.cpp:65-79, src/binning.cpp:558-790).  Parsed on the host in
  * batches, binned on the GPU. */
 bool bin(float** g, char* file_name);                    /* :55 */
+/* Scatter simulation: as the reference's, true for valid inputs and a
+ * defined model, and g is left as it is (src/petl.cpp:194-202). */
 bool simulate_scatter(float** g, float* mu);             /* :57 */
+/* Analytic solids (type 0 ellipsoid, 1 parallelepiped, 2-4 cylinder x/y/z,
+ * 5-7 cone x/y/z; A a 3x3 rotation or null; clip per axis or null) appended
+ * to the model's phantom or to its detector-module model
+ * (src/phantom.cpp:79-93, 535-640). */
 bool add_object(int type, float* c, float* r, float val, float* A, float* clip); /* :64 */
 bool add_module(int type, float* c, float* r, float val, float* A, float* clip); /* :65 */
 bool clear_phantom(void);                                /* :66 */
 bool clear_modules(void);                                /* :67 */
-bool scale_phantom(float, float, float);                 /* :68 */
+bool scale_phantom(float, float, float);                 /* :68 src/phantom.cpp:1120-1141 */
+/* The phantom's solids written into f in order (values outside every solid
+ * kept), 1..5 sub-samples per axis (src/phantom.cpp:105-335); on the GPU. */
 bool voxelize(float* f, int oversampling);               /* :69 */
+/* Analytic line integrals of every planogram through the phantom, and the
+ * detector stopping power through the module model (1 everywhere without
+ * modules); oversampling odd 1..11 lines per bin and axis
+ * (src/analytic_ray_tracing_gpu.cu:693-994); on the GPU. */
 bool ray_trace(float** g, int oversampling);             /* :70 */
 bool stopping_power(float** g, int oversampling);        /* :71 */
 

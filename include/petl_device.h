@@ -98,6 +98,51 @@ int petl_solid_angle_dev(const petl_geom* G, float* g, int do_inverse, void* str
  * Windows read the divided values before any in-fill. */
 int petl_apply_corrections_dev(const petl_geom* G, float* g, const float* r, float threshold, void* stream);
 
+/* One analytic solid of a phantom or of the detector-module model
+ * (src/phantom.h:23-57, src/analytic_ray_tracing_gpu.cuh:27-39).  type:
+ * 0 ellipsoid, 1 parallelepiped, 2/3/4 cylinder along x/y/z, 5/6/7 cone
+ * along x/y/z.  centers/radii are the ray tracer's form (cones rewritten to
+ * a unit-slope cone and its axial clip range clip_cone, src/phantom.cpp:
+ * 594-638); given_c/given_r keep the values as given (the voxelizer
+ * rebuilds cones from them, src/phantom.cpp:118-121).  clip planes are
+ * (n, d) with n . x >= d kept. */
+typedef struct petl_solid {
+    int type;
+    float centers[3], radii[3];
+    float val;
+    float A[9];
+    float clip[6][4];
+    int rotated, num_clip;
+    float clip_cone[2];
+    float given_c[3], given_r[3];
+} petl_solid;
+
+/* geometricObject::init (src/phantom.cpp:535-640): 0, or -1 for a bad type
+ * or a null c / r.  A and clip may be null. */
+int petl_solid_init(petl_solid* s, int type, const float* c, const float* r, float val, const float* A,
+                    const float* clip);
+
+/* phantom::scale_phantom on n solids (src/phantom.cpp:1120-1141). */
+void petl_solids_scale(petl_solid* s, int n, float sx, float sy, float sz);
+
+/* phantom::voxelize (src/phantom.cpp:105-335) on the device: the solids in
+ * order, each one replacing the voxel values inside it (oversampling 1) or
+ * blending toward its value by the fraction of 1..5^3 sub-samples inside.
+ * f is [numZ][numY][numX]; x_0/y_0/z_0 are the coordinates of voxel 0. */
+int petl_voxelize_dev(const petl_solid* solids, int n, float* f, int numX, int numY, int numZ, float voxelWidth,
+                      float voxelHeight, float x_0, float y_0, float z_0, int oversampling, void* stream);
+
+/* Analytic ray tracing of a planogram through n solids
+ * (src/analytic_ray_tracing_gpu.cu:693-846, rayTrace_gpu): per bin the
+ * sum of value x length of the intervals of the bin's line that each solid
+ * (the last one covering an interval) occupies, in the reference's
+ * parameterisation (lengths over 1 + v0^2 + v1^2), averaged over an
+ * oversampling^2 grid of lines (oversampling odd, 1..11); stopping_power != 0
+ * gives (1 - exp(-forward)) (1 - exp(-backward)) of the two half-lines
+ * instead.  Bins outside the field of view are 0. */
+int petl_ray_trace_dev(const petl_geom* G, const petl_solid* solids, int n, float* g, int oversampling,
+                       int stopping_power, void* stream);
+
 /* Error word written by kernels whose waits on asynchronous copies are
  * bounded: nonzero if a wait gave up (the call's result is then invalid).
  * Reading it synchronizes the device and clears it.  -1 if it cannot be

@@ -937,4 +937,452 @@ void oracle_apply_corrections(const oracle_geom* G, float* g, const float* r, fl
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Analytic solids, voxelization and ray tracing (src/phantom.cpp,
+// src/analytic_ray_tracing_gpu.cu).
+// ---------------------------------------------------------------------------
+
+// geometricObject::init (src/phantom.cpp:535-640)
+int oracle_solid_init(oracle_solid* s, int type, const float* c, const float* r, float val, const float* A,
+                      const float* clip)
+{
+    std::memset(s, 0, sizeof(*s));
+    s->type = -1;
+    if (!c || !r || type < 0 || type > 7) return 0;
+    s->type = type;
+    for (int i = 0; i < 3; i++) {
+        s->centers[i] = s->given_c[i] = c[i];
+        s->radii[i] = s->given_r[i] = r[i];
+    }
+    if (clip) {
+        for (int i = 0; i < 3; i++)
+            if (clip[i] != 0.0) {
+                s->clip[s->num_clip][i] = -1.0f;
+                s->clip[s->num_clip][3] = -clip[i];
+                s->num_clip += 1;
+            }
+    }
+    s->val = val;
+    if (A) {
+        for (int i = 0; i < 9; i++) {
+            s->A[i] = A[i];
+            if (i == 0 || i == 4 || i == 8) {
+                if (std::fabs(A[i] - 1.0) > 1.0e-8) s->rotated = 1;
+            } else if (std::fabs(A[i]) > 1.0e-8) {
+                s->rotated = 1;
+            }
+        }
+    }
+    auto cone = [&](int axis, int a, int b, float* cc, float* rr, float* clip_cone) {
+        // axis length l and end radii r_1 (index a), r_2 (index b)
+        const double l = rr[axis], r_1 = rr[a], r_2 = rr[b];
+        rr[a] = float(std::fabs(r_2 - r_1) / (2.0 * l));
+        rr[b] = rr[a];
+        rr[axis] = 1.0f;
+        cc[axis] = float(cc[axis] - l * (r_2 + r_1) / (r_2 - r_1));
+        clip_cone[0] = float(-l + l * (r_2 + r_1) / (r_2 - r_1));
+        clip_cone[1] = float(l + l * (r_2 + r_1) / (r_2 - r_1));
+    };
+    if (type == 5) cone(0, 1, 2, s->centers, s->radii, s->clip_cone);
+    if (type == 6) cone(1, 0, 2, s->centers, s->radii, s->clip_cone);
+    if (type == 7) cone(2, 0, 1, s->centers, s->radii, s->clip_cone);
+    return 1;
+}
+
+namespace {
+
+// phantom::isInside (src/phantom.cpp:337-387)
+bool vox_is_inside(float x, float y, float z, int type, const float* clip, const float* cone)
+{
+    bool in = false;
+    switch (type) {
+    case 0: in = x * x + y * y + z * z <= 1.0; break;
+    case 1: in = std::fabs(x) <= 1.0 && std::fabs(y) <= 1.0 && std::fabs(z) <= 1.0; break;
+    case 2: in = std::fabs(x) <= 1.0 && y * y + z * z <= 1.0; break;
+    case 3: in = std::fabs(y) <= 1.0 && x * x + z * z <= 1.0; break;
+    case 4: in = std::fabs(z) <= 1.0 && x * x + y * y <= 1.0; break;
+    case 5: in = y * y + z * z <= x * x && cone[0] <= x && x <= cone[1]; break;
+    case 6: in = x * x + z * z <= y * y && cone[0] <= y && y <= cone[1]; break;
+    case 7: in = x * x + y * y <= z * z && cone[0] <= z && z <= cone[1]; break;
+    default: break;
+    }
+    if (clip) {
+        if (clip[0] * x > 0.0) in = false;
+        if (clip[1] * y > 0.0) in = false;
+        if (clip[2] * z > 0.0) in = false;
+    }
+    return in;
+}
+
+// phantom::addObject(f, ...) for one solid (src/phantom.cpp:141-335),
+// with c and r as the voxelizer passes them
+void vox_add(float* f, int numX, int numY, int numZ, float T_x, float T_z, float x_0, float y_0, float z_0, int type,
+             float* c, float* r, float val, const float* A, const float* clip, int os)
+{
+    const float T_y = T_x;
+    auto xi = [&](float v) { return (v - x_0) / T_x; };
+    auto yi = [&](float v) { return (v - y_0) / T_y; };
+    auto zi = [&](float v) { return (v - z_0) / T_z; };
+    int minX = int(std::floor(xi(c[0] - r[0] - T_x))), maxX = int(std::ceil(xi(c[0] + r[0] + T_x)));
+    int minY = int(std::floor(yi(c[1] - r[1] - T_y))), maxY = int(std::ceil(yi(c[1] + r[1] + T_y)));
+    int minZ = int(std::floor(zi(c[2] - r[2] - T_z))), maxZ = int(std::ceil(zi(c[2] + r[2] + T_z)));
+    const bool rotated = A && (A[0] != 1.0 || A[4] != 1.0 || A[8] != 1.0);
+    if (rotated || (type >= 5 && type <= 7)) {
+        const float r_max = std::sqrt(3.0) * std::max(r[0], std::max(r[1], r[2]));
+        minX = int(std::floor(xi(c[0] - r_max - T_x)));
+        maxX = int(std::ceil(xi(c[0] + r_max + T_x)));
+        minY = int(std::floor(yi(c[1] - r_max - T_y)));
+        maxY = int(std::ceil(yi(c[1] + r_max + T_y)));
+        minZ = int(std::floor(zi(c[2] - r_max - T_z)));
+        maxZ = int(std::ceil(zi(c[2] + r_max + T_z)));
+    }
+    float cone[2] = {0.0f, 0.0f};
+    auto conify = [&](int axis, int a, int b) {
+        const double l = r[axis], r_1 = r[a], r_2 = r[b];
+        r[a] = std::fabs(r_2 - r_1) / (2.0 * l);
+        r[b] = r[a];
+        r[axis] = 1.0;
+        c[axis] = c[axis] - l * (r_2 + r_1) / (r_2 - r_1);
+        cone[0] = -l + l * (r_2 + r_1) / (r_2 - r_1);
+        cone[1] = l + l * (r_2 + r_1) / (r_2 - r_1);
+    };
+    if (type == 5) conify(0, 1, 2);
+    if (type == 6) conify(1, 0, 2);
+    if (type == 7) conify(2, 0, 1);
+    auto clampi = [](int v, int n) { return std::max(0, std::min(n - 1, v)); };
+    minX = clampi(minX, numX), maxX = clampi(maxX, numX);
+    minY = clampi(minY, numY), maxY = clampi(maxY, numY);
+    minZ = clampi(minZ, numZ), maxZ = clampi(maxZ, numZ);
+    os = std::max(1, std::min(os, 5));
+    auto inside = [&](float x, float y, float z) {
+        if (rotated) {
+            const float xr = (A[0] * (x - c[0]) + A[1] * (y - c[1]) + A[2] * (z - c[2])) / r[0];
+            const float yr = (A[3] * (x - c[0]) + A[4] * (y - c[1]) + A[5] * (z - c[2])) / r[1];
+            const float zr = (A[6] * (x - c[0]) + A[7] * (y - c[1]) + A[8] * (z - c[2])) / r[2];
+            return vox_is_inside(xr, yr, zr, type, clip, cone);
+        }
+        return vox_is_inside((x - c[0]) / r[0], (y - c[1]) / r[1], (z - c[2]) / r[2], type, clip, cone);
+    };
+#pragma omp parallel for
+    for (int iz = minZ; iz <= maxZ; iz++) {
+        const float z = iz * T_z + z_0;
+        for (int iy = minY; iy <= maxY; iy++) {
+            const float y = iy * T_y + y_0;
+            float* line = f + (size_t(iz) * numY + iy) * numX;
+            for (int ix = minX; ix <= maxX; ix++) {
+                const float x = ix * T_x + x_0;
+                if (os == 1) {
+                    if (inside(x, y, z)) line[ix] = val;
+                    continue;
+                }
+                const double frac = 1.0 / float(os * os * os);
+                const float cur = line[ix];
+                float acc = 0.0;
+                for (int kz = 0; kz < os; kz++) {
+                    const float zs = z + T_z / float(os + 1) * (float(kz) - 0.5 * float(os - 1));
+                    for (int ky = 0; ky < os; ky++) {
+                        const float ys = y + T_y / float(os + 1) * (float(ky) - 0.5 * float(os - 1));
+                        for (int kx = 0; kx < os; kx++) {
+                            const float xs = x + T_x / float(os + 1) * (float(kx) - 0.5 * float(os - 1));
+                            if (inside(xs, ys, zs)) acc += (val - cur) * frac;
+                        }
+                    }
+                }
+                line[ix] = acc + cur;
+            }
+        }
+    }
+}
+
+const float kOOB = 1.0e12f;  // src/analytic_ray_tracing_gpu.cu:21
+
+// src/analytic_ray_tracing_gpu.cu:84-114
+bool rt_slab(float* ts, float p, float r)
+{
+    if (std::fabs(r) < 1e-12f) {
+        if (std::fabs(p) < 1.0f) {
+            ts[0] = -kOOB;
+            ts[1] = kOOB;
+            return true;
+        }
+        return false;
+    }
+    if (r > 0.0f) {
+        ts[0] = (-1.0f - p) / r;
+        ts[1] = (1.0f - p) / r;
+    } else {
+        ts[1] = (-1.0f - p) / r;
+        ts[0] = (1.0f - p) / r;
+    }
+    return true;
+}
+
+// src/analytic_ray_tracing_gpu.cu:150-463
+bool rt_normalized(const double* p, const double* r, float* ts, const oracle_solid& sd)
+{
+    ts[0] = ts[1] = -kOOB;
+    const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const double pr = r[0] * p[0] + r[1] * p[1] + r[2] * p[2];
+    auto quad2 = [&](double b, double a, double c, float* t) {  // b^2 - a c > 0 -> roots
+        double disc = b * b - a * c;
+        if (!(disc > 0.0)) return false;
+        disc = std::sqrt(disc);
+        t[0] = float((-b - disc) / a);
+        t[1] = float((-b + disc) / a);
+        return true;
+    };
+    float tz[2], t[2];
+    switch (sd.type) {
+    case 0: {
+        double disc = pr * pr + rr * (1.0 - (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]));
+        if (!(disc > 0.0)) return false;
+        disc = std::sqrt(disc);
+        ts[0] = float((-pr - disc) / rr);
+        ts[1] = float((-pr + disc) / rr);
+        break;
+    }
+    case 1: {
+        float tx[2], ty[2];
+        if (!rt_slab(tx, float(p[0]), float(r[0])) || !rt_slab(ty, float(p[1]), float(r[1])) ||
+            !rt_slab(tz, float(p[2]), float(r[2])))
+            return false;
+        ts[0] = std::max(std::max(tx[0], ty[0]), tz[0]);
+        ts[1] = std::min(std::min(tx[1], ty[1]), tz[1]);
+        break;
+    }
+    case 4: case 2: case 3: {
+        int k, i, j;
+        double b, c;
+        const double a = sd.type == 4 ? rr - r[2] * r[2] : sd.type == 2 ? rr - r[0] * r[0] : rr - r[1] * r[1];
+        if (sd.type == 4) {
+            k = 2, i = 0, j = 1;
+            b = pr - p[2] * r[2];
+            c = p[0] * p[0] + p[1] * p[1] - 1.0;
+        } else if (sd.type == 2) {
+            k = 0, i = 1, j = 2;
+            b = p[2] * r[2] + p[1] * r[1];
+            c = p[2] * p[2] + p[1] * p[1] - 1.0;
+        } else {
+            k = 1, i = 0, j = 2;
+            b = p[0] * r[0] + p[2] * r[2];
+            c = p[0] * p[0] + p[2] * p[2] - 1.0;
+        }
+        if (quad2(b, a, c, t)) {
+            if (!rt_slab(tz, float(p[k]), float(r[k]))) return false;
+            ts[0] = std::max(t[0], tz[0]);
+            ts[1] = std::min(t[1], tz[1]);
+        } else if (r[i] == 0.0 && r[j] == 0.0 && p[i] * p[i] + p[j] * p[j] <= 1.0) {
+            if (!rt_slab(ts, float(p[k]), float(r[k]))) return false;
+        } else {
+            return false;
+        }
+        break;
+    }
+    case 7: case 5: {
+        const int k = sd.type == 7 ? 2 : 0, i = sd.type == 7 ? 0 : 2, j = 1;
+        const double a = r[i] * r[i] + r[j] * r[j] - r[k] * r[k];
+        const double b = p[i] * r[i] + p[j] * r[j] - p[k] * r[k];
+        const double c = p[i] * p[i] + p[j] * p[j] - p[k] * p[k];
+        if (!quad2(b, a, c, t)) return false;
+        if (t[0] > t[1]) std::swap(t[0], t[1]);
+        const double shift = 0.5 * (sd.clip_cone[1] + sd.clip_cone[0]);
+        const double scale = 0.5 * (sd.clip_cone[1] - sd.clip_cone[0]);
+        if (!rt_slab(tz, float((p[k] - shift) / scale), float(r[k] / scale))) return false;
+        ts[0] = std::max(t[0], tz[0]);
+        ts[1] = std::min(t[1], tz[1]);
+        break;
+    }
+    case 6: {
+        const double a = r[0] * r[0] + r[2] * r[2] - r[1] * r[1];
+        const double b = p[0] * r[0] + p[2] * r[2] - p[1] * r[1];
+        const double c = p[0] * p[0] + p[2] * p[2] - p[1] * p[1];
+        double disc = b * b - a * c;
+        if (!(disc > 0.0)) break;
+        disc = std::sqrt(disc);
+        double tmin = (-b - disc) / a, tmax = (-b + disc) / a;
+        if (tmin > tmax) std::swap(tmin, tmax);
+        const double shift = 0.5 * (sd.clip_cone[1] + sd.clip_cone[0]);
+        const double scale = 0.5 * (sd.clip_cone[1] - sd.clip_cone[0]);
+        if (!rt_slab(tz, float((p[1] - shift) / scale), float(r[1] / scale))) break;
+        if (!(std::fabs(r[1]) > 1.0e-12f)) {
+            ts[0] = float(tmin);
+            ts[1] = float(tmax);
+            break;
+        }
+        auto in_at = [&](float tt) {
+            double x = p[0] + tt * r[0], y = p[1] + tt * r[1], z = p[2] + tt * r[2];
+            return x * x + z * z <= y * y;
+        };
+        const bool in0 = in_at(tz[0]), in1 = in_at(tz[1]);
+        if (in0 && in1) {
+            ts[0] = tz[0];
+            ts[1] = tz[1];
+        } else if (in0) {
+            ts[0] = tz[0];
+            ts[1] = float((tz[0] <= tmin && tmin <= tz[1]) ? tmin : tmax);
+        } else if (in1) {
+            ts[0] = float((tz[0] <= tmin && tmin <= tz[1]) ? tmin : tmax);
+            ts[1] = tz[1];
+        } else if (tz[0] <= tmin && tmax <= tz[1]) {
+            ts[0] = float(tmin);
+            ts[1] = float(tmax);
+        } else {
+            ts[0] = ts[1] = -kOOB;
+            return false;
+        }
+        break;
+    }
+    default:
+        return false;
+    }
+    if (ts[0] >= ts[1]) {
+        ts[0] = ts[1] = -kOOB;
+        return false;
+    }
+    return true;
+}
+
+// src/analytic_ray_tracing_gpu.cu:465-518 (with the clipping planes,
+// 116-148)
+bool rt_hit(const float* p, const float* r, float* ts, const oracle_solid& sd)
+{
+    double q[3], m[3];
+    if (!sd.rotated) {
+        for (int k = 0; k < 3; k++) {
+            q[k] = (p[k] - sd.centers[k]) / sd.radii[k];
+            m[k] = r[k] / sd.radii[k];
+        }
+    } else {
+        const double d[3] = {p[0] - sd.centers[0], p[1] - sd.centers[1], p[2] - sd.centers[2]};
+        for (int k = 0; k < 3; k++) {
+            q[k] = (d[0] * sd.A[3 * k] + d[1] * sd.A[3 * k + 1] + d[2] * sd.A[3 * k + 2]) / sd.radii[k];
+            m[k] = (r[0] * sd.A[3 * k] + r[1] * sd.A[3 * k + 1] + r[2] * sd.A[3 * k + 2]) / sd.radii[k];
+        }
+    }
+    if (!rt_normalized(q, m, ts, sd)) return false;
+    for (int i = 0; i < sd.num_clip; i++) {
+        const float* n = sd.clip[i];
+        const float pn = n[0] * p[0] + n[1] * p[1] + n[2] * p[2];
+        const float rn = n[0] * r[0] + n[1] * r[1] + n[2] * r[2];
+        if (std::fabs(rn) < 1.0e-12f) {
+            if (pn < n[3]) return false;
+        } else if (rn > 0.0f) {
+            const float t = (n[3] - pn) / rn;
+            if (ts[1] < t) return false;
+            if (t > ts[0]) ts[0] = t;
+        } else {
+            const float t = (n[3] - pn) / rn;
+            if (ts[0] > t) return false;
+            if (ts[1] > t) ts[1] = t;
+        }
+    }
+    return ts[1] > ts[0];
+}
+
+// src/analytic_ray_tracing_gpu.cu:536-691: line integral (split == 0) or
+// the two half-lines (*fwd, *bwd)
+void rt_line(const oracle_solid* sd, int n, const float* p, const float* r, int split, float* fwd, float* bwd)
+{
+    std::vector<float> ends, t0(n), t1(n);
+    std::vector<int> idx;
+    for (int i = 0; i < n; i++) {
+        float ts[2];
+        if (rt_hit(p, r, ts, sd[i])) {
+            ends.push_back(ts[0]);
+            ends.push_back(ts[1]);
+            t0[i] = ts[0];
+            t1[i] = ts[1];
+            idx.push_back(i);
+        }
+    }
+    *fwd = *bwd = 0.0f;
+    std::sort(ends.begin(), ends.end());
+    for (int i = 0; i + 1 < int(ends.size()); i++) {
+        const float mid = (ends[i + 1] + ends[i]) * 0.5f;
+        for (int h = int(idx.size()) - 1; h >= 0; h--) {
+            const int j = idx[h];
+            if (t0[j] <= mid && mid <= t1[j]) {
+                const float v = sd[j].val * (ends[i + 1] - ends[i]);
+                if (!split || mid >= 0.0f)
+                    *fwd += v;
+                else
+                    *bwd += v;
+                break;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// phantom::voxelize (src/phantom.cpp:105-139): every solid in order
+void oracle_voxelize(const oracle_solid* sd, int n, float* f, int numX, int numY, int numZ, float T_x, float T_z,
+                     float x_0, float y_0, float z_0, int os)
+{
+    for (int k = 0; k < n; k++) {
+        float c[3], r[3], clip[4];
+        const bool cone = sd[k].type >= 5 && sd[k].type <= 7;
+        for (int i = 0; i < 3; i++) {
+            c[i] = cone ? sd[k].given_c[i] : sd[k].centers[i];
+            r[i] = cone ? sd[k].given_r[i] : sd[k].radii[i];
+        }
+        for (int i = 0; i < 4; i++) clip[i] = -sd[k].clip[0][i];
+        const float* cp = (!cone && sd[k].num_clip > 0) ? clip : nullptr;
+        vox_add(f, numX, numY, numZ, T_x, T_z, x_0, y_0, z_0, sd[k].type, c, r, sd[k].val, sd[k].A, cp, os);
+    }
+}
+
+// rayTracingKernel / stoppingPowerKernel (src/analytic_ray_tracing_gpu.cu:
+// 693-846) for one planogram, with the direction and field-of-view rules of
+// the kernels (cos/sin of the float psi in float)
+void oracle_ray_trace(const oracle_geom* G, const oracle_solid* sd, int n, float* g, int oversampling, int stopping,
+                      int nthreads)
+{
+    set_threads(nthreads);
+    int os = std::max(1, std::min(oversampling, 11));
+    if (os % 2 == 0) os += 1;
+    os = std::max(1, std::min(os, 11));
+    const float cs = std::cos(G->psi), sn = std::sin(G->psi);
+    const long long total = (long long)G->N_v1 * G->N_v0 * G->N_u1 * G->N_u0;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (long long id = 0; id < total; id++) {
+        long long t = id;
+        const int iu0 = int(t % G->N_u0);
+        t /= G->N_u0;
+        const int iu1 = int(t % G->N_u1);
+        t /= G->N_u1;
+        const int iv0 = int(t % G->N_v0), iv1 = int(t / G->N_v0);
+        const float v1 = std::fma(float(iv1), G->T_v1, G->v1_0);
+        const float v0 = std::fma(float(iv0), G->T_v0, G->v0_0);
+        const float u1 = std::fma(float(iu1), G->T_u1, G->u1_0);
+        const float u0 = std::fma(float(iu0), G->T_u0, G->u0_0);
+        if (std::fabs(u1) - 0.5f * G->T_u1 > std::fma(-G->R, std::fabs(v1), G->H) ||
+            std::fabs(u0) - 0.5f * G->T_v0 > std::fma(G->R, std::fabs(v0), G->L)) {
+            g[id] = 0.0f;
+            continue;
+        }
+        float r[3] = {-(v0 * cs + sn), -(v0 * sn - cs), -v1};
+        const float mag = 1.0f / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        for (int k = 0; k < 3; k++) r[k] = r[k] / mag;
+        auto value = [&](float du1, float du0) {
+            const float w = u0 + du0;
+            const float p[3] = {w * cs, w * sn, u1 + du1};
+            float fwd, bwd;
+            rt_line(sd, n, p, r, stopping, &fwd, &bwd);
+            return stopping ? (1.0f - std::exp(-fwd)) * (1.0f - std::exp(-bwd)) : fwd;
+        };
+        if (os <= 1) {
+            g[id] = value(0.0f, 0.0f);
+        } else {
+            const float d1 = G->T_u1 / float(os + 1), d0 = G->T_u0 / float(os + 1);
+            const int rad = (os - 1) / 2;
+            float acc = 0.0f;
+            for (int j = -rad; j <= rad; j++)
+                for (int k = -rad; k <= rad; k++) acc += value(j * d1, k * d0);
+            g[id] = acc / float(os * os);
+        }
+    }
+}
+
 }  // extern "C"

@@ -119,6 +119,30 @@ float oracle_median(const float* x, long long n);
  * median in-fill (src/petl.cpp:163-192, src/median_filter.cu:11-190). */
 void oracle_apply_corrections(const oracle_geom* G, float* g, const float* r, float rel, int nthreads);
 
+/* An analytic solid (src/phantom.h:23-57): type 0 ellipsoid, 1
+ * parallelepiped, 2-4 cylinder x/y/z, 5-7 cone x/y/z. */
+typedef struct oracle_solid {
+    int type;
+    float centers[3], radii[3];
+    float val;
+    float A[9];
+    float clip[6][4];
+    int rotated, num_clip;
+    float clip_cone[2];
+    float given_c[3], given_r[3];
+} oracle_solid;
+
+/* geometricObject::init (src/phantom.cpp:535-640); 0 on invalid input. */
+int oracle_solid_init(oracle_solid* s, int type, const float* c, const float* r, float val, const float* A,
+                      const float* clip);
+/* phantom::voxelize (src/phantom.cpp:105-335), into f [z][y][x]. */
+void oracle_voxelize(const oracle_solid* s, int n, float* f, int numX, int numY, int numZ, float T_x, float T_z,
+                     float x_0, float y_0, float z_0, int oversampling);
+/* rayTracingKernel / stoppingPowerKernel of one planogram
+ * (src/analytic_ray_tracing_gpu.cu:693-846). */
+void oracle_ray_trace(const oracle_geom* G, const oracle_solid* s, int n, float* g, int oversampling, int stopping,
+                      int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,14 @@ class Geom(ctypes.Structure):
         return g
 
 
+class Solid(ctypes.Structure):
+    """oracle_solid (oracle.h)."""
+    _fields_ = [("type", ctypes.c_int), ("centers", ctypes.c_float * 3), ("radii", ctypes.c_float * 3),
+                ("val", ctypes.c_float), ("A", ctypes.c_float * 9), ("clip", (ctypes.c_float * 4) * 6),
+                ("rotated", ctypes.c_int), ("num_clip", ctypes.c_int), ("clip_cone", ctypes.c_float * 2),
+                ("given_c", ctypes.c_float * 3), ("given_r", ctypes.c_float * 3)]
+
+
 def lib():
     global _LIB
     if _LIB is None:
@@ -59,6 +67,11 @@ def lib():
         L.oracle_planogram_init.argtypes = [gp] + [ctypes.c_float] * 7
         L.oracle_planogram_init.restype = ctypes.c_int
         L.oracle_bin_events.argtypes = [gp, fp, fp, ctypes.c_longlong, fp, ctypes.c_int, ctypes.c_int]
+        sp = ctypes.POINTER(Solid)
+        L.oracle_solid_init.argtypes = [sp, ctypes.c_int, fp, fp, ctypes.c_float, fp, fp]
+        L.oracle_voxelize.argtypes = [sp, ctypes.c_int, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + \
+            [ctypes.c_float] * 5 + [ctypes.c_int]
+        L.oracle_ray_trace.argtypes = [gp, sp, ctypes.c_int, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_solid_angle_factor.argtypes = [gp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_solid_angle_factor.restype = ctypes.c_float
         L.oracle_solid_angle.argtypes = [gp, fp, ctypes.c_int]
@@ -202,6 +215,61 @@ def bin_events(geoms, blue, pink, linear=True, chest_wall=True):
                                 len(blue), _ptr(g, ctypes.c_float), 1 if linear else 0, 1 if chest_wall else 0)
         out.append(g)
     return out
+
+
+# ----------------------------------------------------------------------------
+# analytic phantoms
+# ----------------------------------------------------------------------------
+def make_solid(kind, c, r, val, A=None, clip=None):
+    """geometricObject::init (src/phantom.cpp:535-640) with the Python
+    defaults of PETLserver.add_object (identity A, no clipping)."""
+    c = _f(np.broadcast_to(np.asarray(c, np.float32), (3,)))
+    r = _f(np.broadcast_to(np.asarray(r, np.float32), (3,)))
+    A = np.eye(3, dtype=np.float32) if A is None else _f(A)
+    clip = np.zeros(3, np.float32) if clip is None else _f(clip)
+    s = Solid()
+    if not lib().oracle_solid_init(ctypes.byref(s), int(kind), _ptr(c, ctypes.c_float), _ptr(r, ctypes.c_float),
+                                   float(val), _ptr(A, ctypes.c_float), _ptr(clip, ctypes.c_float)):
+        raise ValueError("invalid solid")
+    return s
+
+
+def scale_solids(solids, sx, sy, sz):
+    """phantom::scale_phantom (src/phantom.cpp:1120-1141): centres and radii
+    per axis; clipping planes' y, z normals by sy, sz and offsets by sx."""
+    for s in solids:
+        for k, f in enumerate((sx, sy, sz)):
+            s.centers[k] = np.float32(np.float32(s.centers[k]) * np.float32(f))
+            s.radii[k] = np.float32(np.float32(s.radii[k]) * np.float32(f))
+        for i in range(s.num_clip):
+            s.clip[i][1] = np.float32(np.float32(s.clip[i][1]) * np.float32(sy))
+            s.clip[i][2] = np.float32(np.float32(s.clip[i][2]) * np.float32(sz))
+            s.clip[i][3] = np.float32(np.float32(s.clip[i][3]) * np.float32(sx))
+    return solids
+
+
+def _solids(solids):
+    return (Solid * max(1, len(solids)))(*solids), len(solids)
+
+
+def voxelize(solids, f, voxel_width, voxel_height, x_0, y_0, z_0, oversampling=1):
+    """phantom::voxelize into a copy of f [z][y][x] (src/phantom.cpp:105-335)."""
+    out = np.array(f, np.float32, copy=True, order="C")
+    nz, ny, nx = out.shape
+    arr, n = _solids(solids)
+    lib().oracle_voxelize(arr, n, _ptr(out, ctypes.c_float), nx, ny, nz, voxel_width, voxel_height, x_0, y_0, z_0,
+                          int(oversampling))
+    return out
+
+
+def ray_trace(G, solids, oversampling=1, stopping_power=False, nthreads=0):
+    """rayTracingKernel / stoppingPowerKernel on one planogram
+    (src/analytic_ray_tracing_gpu.cu:693-846)."""
+    g = np.zeros(G.shape, np.float32)
+    arr, n = _solids(solids)
+    lib().oracle_ray_trace(ctypes.byref(G), arr, n, _ptr(g, ctypes.c_float), int(oversampling),
+                           1 if stopping_power else 0, nthreads)
+    return g
 
 
 # ----------------------------------------------------------------------------

@@ -27,6 +27,13 @@ class petl_geom(ctypes.Structure):
                [(n, c_f) for n in ("T_x", "T_z", "x_0", "y_0", "z_0")]
 
 
+class petl_solid(ctypes.Structure):
+    """Mirror of ``petl_solid`` (include/petl_device.h)."""
+    _fields_ = [("type", c_i), ("centers", c_f * 3), ("radii", c_f * 3), ("val", c_f), ("A", c_f * 9),
+                ("clip", (c_f * 4) * 6), ("rotated", c_i), ("num_clip", c_i), ("clip_cone", c_f * 2),
+                ("given_c", c_f * 3), ("given_r", c_f * 3)]
+
+
 # (name, restype, argtypes) of every exported function
 _REF_API = [
     ("set_model", c_b, [c_i]), ("create_new_model", c_i, []), ("about", None, []),
@@ -85,6 +92,11 @@ _DEV_API = [
     ("petl_project_nnz_dev", c_i, [_G, ctypes.POINTER(c_d), c_vp]),
     ("petl_bin_events_dev", c_i, [_G, c_vp, c_vp, c_ll, c_vp, c_i, c_i, c_vp]),
     ("petl_solid_angle_dev", c_i, [_G, c_vp, c_i, c_vp]),
+    ("petl_solid_init", c_i, [ctypes.POINTER(petl_solid), c_i, fp, fp, c_f, fp, fp]),
+    ("petl_solids_scale", None, [ctypes.POINTER(petl_solid), c_i, c_f, c_f, c_f]),
+    ("petl_voxelize_dev", c_i, [ctypes.POINTER(petl_solid), c_i, c_vp, c_i, c_i, c_i, c_f, c_f, c_f, c_f, c_f,
+                                c_i, c_vp]),
+    ("petl_ray_trace_dev", c_i, [_G, ctypes.POINTER(petl_solid), c_i, c_vp, c_i, c_i, c_vp]),
     ("petl_apply_corrections_dev", c_i, [_G, c_vp, c_vp, c_f, c_vp]),
     ("petl_project_bf16_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
     ("petl_project_ratio_bf16_dev", c_i, [_G, c_vp, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),

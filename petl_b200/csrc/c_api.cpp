@@ -110,6 +110,7 @@ struct Params {
 
 struct Model {
     Params params;
+    std::vector<petl_solid> phantom, modules;  // analytic solids (src/petl.h:140-141)
 };
 
 std::mutex g_mu;
@@ -514,13 +515,8 @@ bool set_volume(int numX, int numY, int numZ, float voxelWidth, float voxelHeigh
 }
 
 // ---------------------------------------------------------------------------
-// outside the reconstruction path
+// list-mode binning
 // ---------------------------------------------------------------------------
-static bool not_here(const char* name)
-{
-    fprintf(stderr, "%s: not provided by this build (outside the reconstruction path)\n", name);
-    return false;
-}
 bool bin(float** g, char* file_name)
 {
     // PETL::bin (src/petl.cpp:65-79): the planograms are overwritten with the
@@ -548,15 +544,104 @@ bool bin(float** g, char* file_name)
     ok = cuda_ok("bin sync", cudaStreamSynchronize(c->compute)) && ok;
     return ok;
 }
-bool simulate_scatter(float**, float*) { return not_here("simulate_scatter"); }
-bool add_object(int, float*, float*, float, float*, float*) { return not_here("add_object"); }
-bool add_module(int, float*, float*, float, float*, float*) { return not_here("add_module"); }
-bool clear_phantom(void) { return true; }
-bool clear_modules(void) { return true; }
-bool scale_phantom(float, float, float) { return not_here("scale_phantom"); }
-bool voxelize(float*, int) { return not_here("voxelize"); }
-bool ray_trace(float**, int) { return not_here("ray_trace"); }
-bool stopping_power(float**, int) { return not_here("stopping_power"); }
+// the reference's scatter simulation validates its inputs and computes
+// nothing (src/petl.cpp:194-202)
+bool simulate_scatter(float** g, float* mu) { return g != nullptr && mu != nullptr && tomo()->params.allDefined(); }
+
+// ---------------------------------------------------------------------------
+// analytic phantoms and detector modules (src/petl_c_interface.cpp:271-301,
+// src/petl.cpp:81-152)
+// ---------------------------------------------------------------------------
+static bool add_solid(std::vector<petl_solid>& list, int type, float* c, float* r, float val, float* A, float* clip)
+{
+    petl_solid sd;
+    if (petl_solid_init(&sd, type, c, r, val, A, clip) != 0) return false;
+    list.push_back(sd);
+    return true;
+}
+bool add_object(int type, float* c, float* r, float val, float* A, float* clip)
+{
+    return add_solid(tomo()->phantom, type, c, r, val, A, clip);
+}
+bool add_module(int type, float* c, float* r, float val, float* A, float* clip)
+{
+    return add_solid(tomo()->modules, type, c, r, val, A, clip);
+}
+bool clear_phantom(void)
+{
+    tomo()->phantom.clear();
+    return true;
+}
+bool clear_modules(void)
+{
+    tomo()->modules.clear();
+    return true;
+}
+bool scale_phantom(float sx, float sy, float sz)
+{
+    Model* m = tomo();
+    petl_solids_scale(m->phantom.data(), int(m->phantom.size()), sx, sy, sz);
+    return true;
+}
+
+// phantom::voxelize into the host volume f (values outside every solid are
+// kept), on the GPU
+bool voxelize(float* f, int oversampling)
+{
+    Model* m = tomo();
+    const Params P = m->params;
+    if (f == nullptr || !P.volumeDefined()) return false;
+    const std::vector<petl_solid> solids = m->phantom;
+    if (solids.empty()) return true;
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok("voxelize", cudaErrorNoDevice);
+    petl_geom Gv{};
+    petl_geom_set_volume(&Gv, P.numX, P.numY, P.numZ, P.voxelWidth, P.voxelHeight, P.offsetX, P.offsetY,
+                         P.offsetZ);
+    const size_t n = P.volElems();
+    DevBuf df;
+    if (!df.alloc(n * 4, c->compute)) return cuda_ok("voxelize alloc", cudaGetLastError());
+    bool ok = cuda_ok("voxelize H2D", cudaMemcpyAsync(df.f(), f, n * 4, cudaMemcpyHostToDevice, c->compute));
+    ok = ok && report("voxelize", petl_voxelize_dev(solids.data(), int(solids.size()), df.f(), P.numX, P.numY,
+                                                    P.numZ, P.voxelWidth, P.voxelHeight, Gv.x_0, Gv.y_0, Gv.z_0,
+                                                    oversampling, c->compute));
+    ok = ok && cuda_ok("voxelize D2H", cudaMemcpyAsync(f, df.f(), n * 4, cudaMemcpyDeviceToHost, c->compute));
+    return cuda_ok("voxelize sync", cudaStreamSynchronize(c->compute)) && ok;
+}
+
+static bool trace_planograms(float** g, int oversampling, bool stopping, const char* what)
+{
+    Model* m = tomo();
+    const Params P = m->params;
+    if (g == nullptr || !P.geometryDefined()) return false;
+    const std::vector<petl_solid> solids = stopping ? m->modules : m->phantom;
+    if (stopping && solids.empty()) {
+        // no module model: unit stopping power (src/petl.cpp:139-147)
+        for (size_t i = 0; i < P.plans.size(); i++) {
+            const petl_geom& G = P.plans[i];
+            std::fill(g[i], g[i] + size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0, 1.0f);
+        }
+        return true;
+    }
+    DevCtx* c = dev_ctx();
+    if (!c) return cuda_ok(what, cudaErrorNoDevice);
+    bool ok = true;
+    for (size_t i = 0; i < P.plans.size() && ok; i++) {
+        const petl_geom& G = P.plans[i];
+        const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
+        DevBuf dg;
+        if (!dg.alloc(n * 4, c->compute)) return cuda_ok(what, cudaGetLastError());
+        ok = report(what, petl_ray_trace_dev(&G, solids.data(), int(solids.size()), dg.f(), oversampling,
+                                             stopping ? 1 : 0, c->compute));
+        ok = ok && cuda_ok(what, cudaMemcpyAsync(g[i], dg.f(), n * 4, cudaMemcpyDeviceToHost, c->compute));
+    }
+    return cuda_ok(what, cudaStreamSynchronize(c->compute)) && ok;
+}
+bool ray_trace(float** g, int oversampling) { return trace_planograms(g, oversampling, false, "ray_trace"); }
+bool stopping_power(float** g, int oversampling)
+{
+    return trace_planograms(g, oversampling, true, "stopping_power");
+}
 
 // PETL::set_solid_angle_correction (src/petl.cpp:154-162)
 bool set_solid_angle_correction(float** g, bool do_inverse)

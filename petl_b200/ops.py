@@ -7,6 +7,7 @@ library reduces in FP64 come back as float64 0-d CUDA tensors (no host sync).
 """
 import ctypes
 
+import numpy as np
 import torch
 
 from ._lib import PetlError, check, lib
@@ -83,6 +84,67 @@ def bin_events(geom, blue, pink, g=None, linear=True, chest_wall=True):
     for G, gi in zip(geoms, gl):
         check(lib().petl_bin_events_dev(G.ptr, _dev(blue, "blue"), _dev(pink, "pink"), n, _dev(gi, "g"),
                                         1 if linear else 0, 1 if chest_wall else 0, _stream()), "bin_events")
+    return g if isinstance(geom, (list, tuple)) else gl[0]
+
+
+# ----------------------------------------------------------------------------
+# analytic phantoms
+# ----------------------------------------------------------------------------
+SOLID_TYPES = {"ellipsoid": 0, "ball": 0, "sphere": 0, "parallelepiped": 1, "box": 1, "can_x": 2, "can_y": 3,
+               "can_z": 4, "can": 4, "cone_x": 5, "cone_y": 6, "cone_z": 7, "cone": 7}
+
+
+def make_solid(kind, c, r, val, A=None, clip=None):
+    """One analytic solid (geometricObject::init, src/phantom.cpp:535-640):
+    kind is a type number 0..7 or a name (ellipsoid, box, can_x/y/z, cone_x/y/z);
+    A a 3x3 rotation (default identity), clip per-axis clipping (default none)."""
+    from ._lib import petl_solid
+    t = SOLID_TYPES[kind.lower()] if isinstance(kind, str) else int(kind)
+    c = np.ascontiguousarray(np.broadcast_to(np.asarray(c, np.float32), (3,)))
+    r = np.ascontiguousarray(np.broadcast_to(np.asarray(r, np.float32), (3,)))
+    A = np.eye(3, dtype=np.float32) if A is None else np.ascontiguousarray(A, np.float32)
+    clip = np.zeros(3, np.float32) if clip is None else np.ascontiguousarray(clip, np.float32)
+    s = petl_solid()
+    fptr = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))  # noqa: E731
+    if lib().petl_solid_init(ctypes.byref(s), t, fptr(c), fptr(r), float(val), fptr(A), fptr(clip)) != 0:
+        raise ValueError("invalid solid")
+    return s
+
+
+def _solid_array(solids):
+    from ._lib import petl_solid
+    arr = (petl_solid * max(1, len(solids)))(*solids)
+    return arr, len(solids)
+
+
+def voxelize_(f, solids, voxel_width, voxel_height=None, x_0=None, y_0=None, z_0=None, oversampling=1):
+    """Writes the solids, in order, into the device volume f [z][y][x]
+    (phantom::voxelize, src/phantom.cpp:105-335); x_0/y_0/z_0 default to a
+    volume centred on the origin."""
+    nz, ny, nx = f.shape
+    vh = voxel_width if voxel_height is None else voxel_height
+    x_0 = float(np.float32(-0.5 * (nx - 1) * voxel_width)) if x_0 is None else x_0
+    y_0 = float(np.float32(-0.5 * (ny - 1) * voxel_width)) if y_0 is None else y_0
+    z_0 = float(np.float32(-0.5 * (nz - 1) * vh)) if z_0 is None else z_0
+    arr, n = _solid_array(solids)
+    check(lib().petl_voxelize_dev(arr, n, _dev(f, "f"), nx, ny, nz, float(voxel_width), float(vh), float(x_0),
+                                  float(y_0), float(z_0), int(oversampling), _stream()), "voxelize")
+    return f
+
+
+def ray_trace(geom, solids, g=None, oversampling=1, stopping_power=False):
+    """Analytic ray tracing of the planogram(s) through the solids
+    (src/analytic_ray_tracing_gpu.cu:693-994): line integrals, or with
+    stopping_power the product of the two half-lines' absorption
+    probabilities."""
+    geoms = as_list(geom)
+    if g is None:
+        g = [torch.empty(G.shape, device="cuda", dtype=torch.float32) for G in geoms]
+    gl = as_list(g)
+    arr, n = _solid_array(solids)
+    for G, gi in zip(geoms, gl):
+        check(lib().petl_ray_trace_dev(G.ptr, arr, n, _dev(gi, "g"), int(oversampling), 1 if stopping_power else 0,
+                                       _stream()), "ray_trace")
     return g if isinstance(geom, (list, tuple)) else gl[0]
 
 

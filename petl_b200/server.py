@@ -9,9 +9,8 @@ Numpy inputs go through the reference-compatible C ABI (host pointers);
 torch CUDA tensors (or lists of them) go through the device-resident
 operators in petl_b200.ops without leaving the GPU.
 
-Not provided here (outside the reconstruction path): analytic phantoms and
-ray tracing, the detector stopping-power response (calc_response therefore
-needs oversampling=0), scatter simulation and the napari display.
+Not provided here: scatter simulation (the reference's computes nothing
+either) and the napari display.
 """
 import ctypes
 import os
@@ -272,6 +271,99 @@ class PETLserver:
         self.backproject(ones, Pstar1)
         return Pstar1
 
+    # ----------------------------------------------- phantoms and modules
+    def add_object(self, typeOfObject, c, r, val, A=None, clip=None):
+        """Appends an analytic solid to the phantom (src/petl_server.py:813-875):
+        type 0..7 or a name (ball/sphere/ellipsoid, box/parallelepiped,
+        can_x, can_y, can_z/can, cone_x, cone_y, cone_z/cone)."""
+        from .ops import SOLID_TYPES
+        if A is None:
+            A = np.eye(3, dtype=np.float32)
+        if clip is None:
+            clip = np.zeros(3, dtype=np.float32)
+        if isinstance(c, (int, float)):
+            c = [c, c, c]
+        if isinstance(r, (int, float)):
+            r = [r, r, r]
+        if isinstance(typeOfObject, str):
+            if typeOfObject.lower() not in SOLID_TYPES:
+                print("Error: unknown object type")
+                return False
+            typeOfObject = SOLID_TYPES[typeOfObject.lower()]
+        c, r = np.ascontiguousarray(c, np.float32), np.ascontiguousarray(r, np.float32)
+        A, clip = np.ascontiguousarray(A, np.float32), np.ascontiguousarray(clip, np.float32)
+        self.set_model()
+        return self.libprojectors.add_object(int(typeOfObject), _fp(c), _fp(r), float(val), _fp(A), _fp(clip))
+
+    def add_module(self, c, r, val=0.0815, A=None):
+        """Appends a detector module (a parallelepiped of attenuation val,
+        mm^-1) to the stopping-power model (src/petl_server.py:877-910)."""
+        if A is None:
+            A = np.eye(3, dtype=np.float32)
+        if isinstance(c, (int, float)):
+            c = [c, c, c]
+        if isinstance(r, (int, float)):
+            r = [r, r, r]
+        c, r = np.ascontiguousarray(c, np.float32), np.ascontiguousarray(r, np.float32)
+        A, clip = np.ascontiguousarray(A, np.float32), np.zeros(3, np.float32)
+        self.set_model()
+        return self.libprojectors.add_module(1, _fp(c), _fp(r), float(val), _fp(A), _fp(clip))
+
+    def clear_phantom(self):
+        self.set_model()
+        self.libprojectors.clear_phantom()
+
+    def clear_modules(self):
+        self.set_model()
+        self.libprojectors.clear_modules()
+
+    def scale_phantom(self, c):
+        if isinstance(c, (int, float)):
+            cx = cy = cz = c
+        elif isinstance(c, np.ndarray) and c.size == 3:
+            cx, cy, cz = (float(v) for v in c)
+        else:
+            return False
+        self.set_model()
+        return self.libprojectors.scale_phantom(cx, cy, cz)
+
+    def voxelize(self, f=None, oversampling=1):
+        """Writes the phantom's solids into f (src/petl_server.py:946-965)."""
+        if not self.volume_defined():
+            raise ValueError("Error: volume parameters not specified")
+        if f is None:
+            f = self.allocate_volume()
+        _check_f32(f, "f")
+        self.set_model()
+        return f if self.libprojectors.voxelize(_fp(f), int(oversampling)) else None
+
+    def ray_trace(self, g=None, oversampling=1):
+        """Analytic line integrals of the phantom (src/petl_server.py:967-993)."""
+        if not self.geometry_defined():
+            raise ValueError("Error: PET scanner not specified")
+        if g is None:
+            g = self.allocate_projections()
+        for a in g:
+            _check_f32(a, "g")
+        self.set_model()
+        return g if self.libprojectors.ray_trace(_pp(g), int(oversampling)) else None
+
+    def stopping_power(self, g=None, oversampling=1):
+        """Detector stopping power of every coincidence line through the
+        module model, smoothed by a 0.6571-bin Gaussian as the reference does
+        (src/petl_server.py:995-1022)."""
+        if not self.geometry_defined():
+            raise ValueError("Error: PET scanner not specified")
+        if g is None:
+            g = self.allocate_projections()
+        for a in g:
+            _check_f32(a, "g")
+        self.set_model()
+        if self.libprojectors.stopping_power(_pp(g), int(oversampling)):
+            self.gaussian_filter(g, 0.6571)
+            return g
+        return None
+
     # ------------------------------------------------------ response / corrections
     def set_response(self, R):
         """Sets the response map (src/petl_server.py:121-135); with
@@ -283,12 +375,14 @@ class PETLserver:
         self.response = None
 
     def calc_response(self, oversampling=1, mu=None):
-        """Response = solid-angle model (times exp(-P mu) when mu is given),
-        src/petl_server.py:578-605.  The detector stopping power
-        (oversampling > 0) is not provided: pass oversampling=0."""
+        """Response = detector stopping power (oversampling > 0) times the
+        solid-angle model, divided by exp(P mu) when mu is given
+        (src/petl_server.py:578-605)."""
         if oversampling > 0:
-            raise NotImplementedError("detector stopping power is not provided; use oversampling=0")
-        self.response = self.apply_solid_angle_model(None)
+            self.response = self.stopping_power(self.response, oversampling=oversampling)
+        else:
+            self.response = None
+        self.response = self.apply_solid_angle_model(self.response)
         if mu is not None:
             Pmu = self.allocate_projections()
             self.project(Pmu, mu)

@@ -80,6 +80,18 @@ class Ref:
         L.TV_denoise.restype = c_b
         L.bin.argtypes = [ctypes.POINTER(fp), ctypes.c_char_p]
         L.bin.restype = c_b
+        for n in ("add_object", "add_module"):
+            getattr(L, n).argtypes = [c_i, fp, fp, c_f, fp, fp]
+            getattr(L, n).restype = c_b
+        L.clear_phantom.restype = c_b
+        L.clear_modules.restype = c_b
+        L.scale_phantom.argtypes = [c_f, c_f, c_f]
+        L.scale_phantom.restype = c_b
+        L.voxelize.argtypes = [fp, c_i]
+        L.voxelize.restype = c_b
+        for n in ("ray_trace", "stopping_power"):
+            getattr(L, n).argtypes = [ctypes.POINTER(fp), c_i]
+            getattr(L, n).restype = c_b
         L.set_solid_angle_correction.argtypes = [ctypes.POINTER(fp), c_b]
         L.set_solid_angle_correction.restype = c_b
         L.apply_corrections.argtypes = [ctypes.POINTER(fp), ctypes.POINTER(fp), c_f]
@@ -351,6 +363,97 @@ def run_binning(ref, out):
     print("wrote binning", {k: float(v.sum()) for k, v in rec.items() if k[-3:-1] == "_g"})
 
 
+# Solids of the phantom cases: (type, centre, radii, value, rotation, clip)
+# (types: 0 ellipsoid, 1 box, 2/3/4 cylinder x/y/z, 5/6/7 cone x/y/z; cones
+# take (l, r_1, r_2) in the reference's per-axis order)
+_C30 = float(np.cos(np.pi / 6)), float(np.sin(np.pi / 6))
+PHANTOM = [
+    (0, (2.0, -3.0, 1.0), (10.0, 7.0, 4.0), 1.0, None, None),
+    (1, (-5.0, 4.0, 0.0), (4.0, 3.0, 2.0), 2.0, None, None),
+    (4, (6.0, 6.0, 0.0), (3.0, 3.0, 5.0), 0.5, None, None),
+    (2, (0.0, -8.0, 2.0), (8.0, 2.0, 2.0), 1.5, None, None),
+    (3, (-8.0, 0.0, -2.0), (2.0, 9.0, 2.0), 0.7, None, None),
+    (7, (0.0, 0.0, 0.0), (2.0, 4.0, 5.0), 0.3, None, None),
+    (5, (5.0, -5.0, -2.0), (4.0, 1.0, 3.0), 0.9, None, None),
+    (6, (-4.0, -6.0, 1.0), (1.0, 5.0, 3.0), 1.2, None, None),
+    (0, (10.0, -10.0, 0.0), (6.0, 2.0, 3.0), 0.8,
+     ((_C30[0], -_C30[1], 0.0), (_C30[1], _C30[0], 0.0), (0.0, 0.0, 1.0)), None),
+    (1, (-10.0, -12.0, 0.0), (5.0, 5.0, 3.0), 1.1, None, (1.0, 0.0, 0.0)),
+]
+
+
+def _add_solids(fn, solids):
+    for t, c, r, v, A, clip in solids:
+        c = np.array(c, np.float32)
+        r = np.array(r, np.float32)
+        A = np.eye(3, dtype=np.float32) if A is None else np.array(A, np.float32)
+        clip = np.zeros(3, np.float32) if clip is None else np.array(clip, np.float32)
+        if not fn(t, ptr(c), ptr(r), v, ptr(A), ptr(clip)):
+            raise RuntimeError("reference rejected a solid")
+
+
+def _modules(D, L_, H):
+    """Four detector slabs around a planogram pair's field of view, as the
+    reference's simple PET/X module model (src/petx_server.py:22-27)."""
+    return [(1, (0.0, 0.5 * D + 10.0, 0.0), (0.5 * L_, 10.0, 0.5 * H), 0.0815, None, None),
+            (1, (0.0, -0.5 * D - 10.0, 0.0), (0.5 * L_, 10.0, 0.5 * H), 0.0815, None, None),
+            (1, (0.5 * L_ + 10.0, 0.0, 0.0), (10.0, 0.5 * D + 20.0, 0.5 * H), 0.0815, None, None),
+            (1, (-0.5 * L_ - 10.0, 0.0, 0.0), (10.0, 0.5 * D + 20.0, 0.5 * H), 0.0815, None, None)]
+
+
+def run_voxelize(ref, out):
+    """phantom::voxelize (CPU code, src/phantom.cpp:105-335) of the PHANTOM
+    solids into a volume pre-filled with 0.25 (values outside every solid are
+    kept), with 1 and 3 sub-samples per axis, and after scale_phantom."""
+    rec = {}
+    vol = (32, 32, 8, 2.0, 2.0, 0.0, 0.0, 0.0)
+    ref.model([GEOMS["g0"][0][0]], vol)
+    ref.L.clear_phantom()
+    _add_solids(ref.L.add_object, PHANTOM)
+    for os_ in (1, 3):
+        f = np.full((vol[2], vol[1], vol[0]), 0.25, np.float32)
+        if not ref.L.voxelize(ptr(f), os_):
+            raise RuntimeError("reference voxelize failed")
+        rec[f"f_os{os_}"] = f
+    ref.L.scale_phantom(1.25, 0.8, 1.1)
+    f = np.full((vol[2], vol[1], vol[0]), 0.25, np.float32)
+    ref.L.voxelize(ptr(f), 1)
+    rec["f_scaled"] = f
+    rec["volume"] = np.array(vol)
+    np.savez_compressed(os.path.join(out, "voxelize.npz"), **rec)
+    print("wrote voxelize", {k: float(v.sum()) for k, v in rec.items() if k.startswith("f_")})
+
+
+def run_raytrace(ref, out):
+    """Analytic ray tracing (rayTracingKernel) of the PHANTOM solids and the
+    stopping power (stoppingPowerKernel) of a four-slab module model, CUDA
+    code in the reference, so this case needs a GPU."""
+    rec = {}
+    for name in ("g0", "g30", "gpetx"):
+        plans, vol = GEOMS[name]
+        ref.model(plans, vol)
+        ref.L.clear_phantom()
+        ref.L.clear_modules()
+        _add_solids(ref.L.add_object, PHANTOM)
+        _, D, L_, H, _, _, _ = plans[0]
+        _add_solids(ref.L.add_module, _modules(D, L_, H))
+        for os_ in (1, 3):
+            gs = [np.full(sh, 7.0, np.float32) for sh in ref.shapes()]
+            if not ref.L.ray_trace(ref.pp(gs), os_):
+                raise RuntimeError("reference ray_trace failed")
+            for i, g in enumerate(gs):
+                rec[f"{name}_rt{os_}_{i}"] = g
+        gs = [np.full(sh, 7.0, np.float32) for sh in ref.shapes()]
+        if not ref.L.stopping_power(ref.pp(gs), 1):
+            raise RuntimeError("reference stopping_power failed")
+        for i, g in enumerate(gs):
+            rec[f"{name}_sp_{i}"] = g
+        rec[f"{name}_planograms"] = np.array(plans)
+        rec[f"{name}_volume"] = np.array(vol)
+    np.savez_compressed(os.path.join(out, "raytrace.npz"), **rec)
+    print("wrote raytrace", {k: float(v.sum()) for k, v in rec.items() if "_rt" in k or "_sp" in k})
+
+
 def run_solid_angle(ref, out):
     """Solid-angle correction (CPU code, src/planogram.cpp:262-302) of all-ones
     planograms: the output is the per-projection factor, recorded as a table
@@ -456,14 +559,15 @@ def main():
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--cpu-only", action="store_true")
     ap.add_argument("--only", nargs="*", default=None,
-                    help="run only these cases (cpu, binning, solid_angle, corrections, projectors, "
-                         "pfdr_fbp, mlem, regularizers)")
+                    help="run only these cases (cpu, binning, solid_angle, voxelize, corrections, raytrace, "
+                         "projectors, pfdr_fbp, mlem, regularizers)")
     ap.add_argument("--lib", default=REF_LIB)
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = Ref(a.lib)
     runs = [("cpu", run_cpu, False), ("binning", run_binning, False), ("solid_angle", run_solid_angle, False),
-            ("corrections", run_corrections, True), ("projectors", run_projectors, True),
+            ("voxelize", run_voxelize, False), ("corrections", run_corrections, True),
+            ("raytrace", run_raytrace, True), ("projectors", run_projectors, True),
             ("pfdr_fbp", run_pfdr_fbp, True), ("mlem", run_mlem, True), ("regularizers", run_regularizers, True)]
     for name, fn, gpu in runs:
         if (a.only is None or name in a.only) and not (gpu and a.cpu_only):
