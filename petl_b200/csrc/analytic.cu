@@ -16,9 +16,11 @@
 // are found in the solid's normalised frame; the end points are sorted and
 // each interval between consecutive end points is credited to the last solid
 // (in insertion order) that covers its midpoint.  The solids are staged in
-// shared memory; the hits of a line are kept per thread (up to kMaxHits, a
-// line with more is resolved by rescanning the solids per interval, which
-// gives the same sum).  The reference's line parameterisation is kept: its
+// shared memory with a bounding sphere each, and a line runs the exact
+// intersection only for the solids whose sphere it meets (a conservative
+// test: the result is unchanged).  The hits of a line are kept per thread
+// (up to kMaxHits; a line with more is resolved by rescanning the solids per
+// interval, which gives the same sum).  The reference's line parameterisation is kept: its
 // direction is the unnormalised direction times its own length (the
 // reference divides by rsqrt of the squared length), so lengths come out
 // divided by 1 + v0^2 + v1^2; and its field-of-view test for u0 uses half
@@ -37,7 +39,7 @@ enum SolidType { kEllipsoid = 0, kBox = 1, kCylX = 2, kCylY = 3, kCylZ = 4, kCon
 constexpr float kFar = 1.0e12f;  // parameter of an unbounded side
 constexpr int kMaxHits = 32;     // hits of one line kept per thread
 constexpr int kRayThreads = 128;
-constexpr int kSmemSolids = 160;  // solids staged in shared memory (~23 KB)
+constexpr int kSmemSolids = 200;  // solids (and bounds) staged in shared memory (<= 44 KB)
 
 // ---------------------------------------------------------------------------
 // intersections (device)
@@ -258,6 +260,23 @@ __device__ bool solid_hit(const petl_solid& s, float3 p, float3 r, float& t0, fl
     return t1 > t0;
 }
 
+// Bounding sphere of a solid for culling (r2 < 0: always tested).
+struct Bound {
+    float cx, cy, cz, r2;
+};
+
+// Whether the line p + t r may meet the solid: its distance to the sphere's
+// centre against the radius, with margins (relative to the radius and to the
+// float cancellation in |w|^2 - (w.r)^2/|r|^2) that keep every line the exact
+// test accepts.
+__device__ __forceinline__ bool may_hit(const Bound& b, float3 p, float3 r, float rr)
+{
+    if (b.r2 < 0.0f) return true;
+    const float wx = b.cx - p.x, wy = b.cy - p.y, wz = b.cz - p.z;
+    const float ww = wx * wx + wy * wy + wz * wz, wr = wx * r.x + wy * r.y + wz * r.z;
+    return ww - wr * wr / rr <= b.r2 + 1.0e-5f * ww;
+}
+
 struct LineSums {
     float fwd, bwd;  // value x length with the interval midpoint at t >= 0 / t < 0
 };
@@ -267,15 +286,16 @@ struct LineSums {
 // (src/analytic_ray_tracing_gpu.cu:536-691).  SPLIT: the two half-lines
 // apart (stopping power); otherwise every interval into fwd, in order.
 template <bool SPLIT>
-__device__ LineSums line_sums(const petl_solid* solids, int n, float3 p, float3 r)
+__device__ LineSums line_sums(const petl_solid* solids, const Bound* bounds, int n, float3 p, float3 r)
 {
     float h0[kMaxHits], h1[kMaxHits], e[2 * kMaxHits];
     int hid[kMaxHits];
     int count = 0;
     bool overflow = false;
+    const float rr = r.x * r.x + r.y * r.y + r.z * r.z;
     for (int j = 0; j < n; j++) {
         float t0, t1;
-        if (!solid_hit(solids[j], p, r, t0, t1)) continue;
+        if (!may_hit(bounds[j], p, r, rr) || !solid_hit(solids[j], p, r, t0, t1)) continue;
         if (count == kMaxHits) {
             overflow = true;
             break;
@@ -349,6 +369,7 @@ __device__ LineSums line_sums(const petl_solid* solids, int n, float3 p, float3 
 struct RayArgs {
     petl_geom G;
     const petl_solid* solids;
+    const Bound* bounds;
     int n;
     float* g;
     int os;
@@ -360,16 +381,21 @@ template <bool STOP>
 __global__ void __launch_bounds__(kRayThreads) k_ray_trace(const RayArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    petl_solid* ss = reinterpret_cast<petl_solid*>(smem_raw);
+    Bound* sb = reinterpret_cast<Bound*>(smem_raw);
+    petl_solid* ss = reinterpret_cast<petl_solid*>(sb + (a.n <= kSmemSolids ? a.n : 0));
     const bool staged = a.n <= kSmemSolids;
     if (staged) {
-        const int words = a.n * int(sizeof(petl_solid) / 4);
+        const int words = a.n * int(sizeof(petl_solid) / 4), bwords = a.n * 4;
         const int* src = reinterpret_cast<const int*>(a.solids);
         int* dst = reinterpret_cast<int*>(ss);
         for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+        const int* bsrc = reinterpret_cast<const int*>(a.bounds);
+        int* bdst = reinterpret_cast<int*>(sb);
+        for (int i = threadIdx.x; i < bwords; i += blockDim.x) bdst[i] = bsrc[i];
         __syncthreads();
     }
     const petl_solid* solids = staged ? ss : a.solids;
+    const Bound* bounds = staged ? sb : a.bounds;
     const petl_geom& G = a.G;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.total;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -397,7 +423,7 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_trace(const RayArgs a)
         auto value = [&](float du1, float du0) {
             const float w = u0 + du0;
             const LineSums s =
-                line_sums<STOP>(solids, a.n, make_float3(w * a.cos_psi, w * a.sin_psi, u1 + du1), r);
+                line_sums<STOP>(solids, bounds, a.n, make_float3(w * a.cos_psi, w * a.sin_psi, u1 + du1), r);
             return STOP ? (1.0f - expf(-s.fwd)) * (1.0f - expf(-s.bwd)) : s.fwd;
         };
         float out;
@@ -605,6 +631,26 @@ int voxelize(const petl_solid* solids, int n, float* f, int numX, int numY, int 
     return 0;
 }
 
+// Bounding sphere of a solid in world coordinates: centre, and the radius of
+// its unrotated, unclipped extent (rotations and clipping keep it inside);
+// cones are always tested.
+Bound solid_bound(const petl_solid& s)
+{
+    const float* c = s.centers;
+    const float* r = s.radii;
+    double rad;
+    switch (s.type) {
+    case kEllipsoid: rad = std::max(r[0], std::max(r[1], r[2])); break;
+    case kBox: rad = std::sqrt(double(r[0]) * r[0] + double(r[1]) * r[1] + double(r[2]) * r[2]); break;
+    case kCylX: rad = std::sqrt(double(r[0]) * r[0] + std::pow(std::max(r[1], r[2]), 2.0)); break;
+    case kCylY: rad = std::sqrt(double(r[1]) * r[1] + std::pow(std::max(r[0], r[2]), 2.0)); break;
+    case kCylZ: rad = std::sqrt(double(r[2]) * r[2] + std::pow(std::max(r[0], r[1]), 2.0)); break;
+    default: return Bound{0.0f, 0.0f, 0.0f, -1.0f};
+    }
+    rad = std::fabs(rad) * (1.0 + 1.0e-4) + 1.0e-3;
+    return Bound{c[0], c[1], c[2], float(rad * rad)};
+}
+
 int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int oversampling, bool stopping,
               cudaStream_t st)
 {
@@ -616,10 +662,17 @@ int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int
     os = std::max(1, std::min(os, 11));
     petl_solid* ds = nullptr;
     if (int rc = upload(solids, size_t(n), &ds, st)) return rc;
+    std::vector<Bound> hb;
+    for (int j = 0; j < n; j++) hb.push_back(solid_bound(solids[j]));
+    Bound* db = nullptr;
+    if (int rc = upload(hb.data(), hb.size(), &db, st)) {
+        cudaFreeAsync(ds, st);
+        return rc;
+    }
     // the reference's constants: cos/sin of the float psi in float
-    RayArgs a{G, ds, n, g, os, std::cos(G.psi), std::sin(G.psi),
+    RayArgs a{G, ds, db, n, g, os, std::cos(G.psi), std::sin(G.psi),
               (long long)G.N_v1 * G.N_v0 * G.N_u1 * G.N_u0};
-    const size_t smem = n <= kSmemSolids ? size_t(n) * sizeof(petl_solid) : 0;
+    const size_t smem = n <= kSmemSolids ? size_t(n) * (sizeof(petl_solid) + sizeof(Bound)) : 0;
     const int grid = int(std::min<long long>((a.total + kRayThreads - 1) / kRayThreads, 64LL * sm_count()));
     if (stopping)
         k_ray_trace<true><<<grid, kRayThreads, smem, st>>>(a);
@@ -628,6 +681,7 @@ int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int
     note_launch();
     const cudaError_t e = cudaGetLastError();
     cudaFreeAsync(ds, st);
+    cudaFreeAsync(db, st);
     if (e != cudaSuccess) {
         set_error(std::string("ray_trace launch: ") + cudaGetErrorString(e));
         return int(e);
