@@ -535,6 +535,86 @@ def osem(geoms, g, num_iter, num_subsets, f=None, nthreads=0):
     return f
 
 
+def rwls(geoms, g, f, num_iter, delta=1.0, beta=0.0, W=None, sqs=False, nonnegativity=True, response=None,
+         p=1.0, nthreads=0):
+    """PETLserver.RWLS in FP64 (src/petl_server.py:1691-1877): PCG with a
+    restart every 50 iterations, the SQS preconditioner 1 / P^T W P 1 (zeros
+    -> 1), step <d, grad> / (<Pd, W Pd> + TV quadratic form); W planograms or
+    None; a response R puts R in the projectors (project then multiply by R,
+    multiply by R then backproject)."""
+    if isinstance(geoms, Geom):
+        geoms, g = [geoms], [g]
+        W = [W] if W is not None else None
+        response = [response] if response is not None else None
+    R = [_d(r) for r in response] if response is not None else None
+
+    def P(x):
+        out = project(geoms, x, nthreads=nthreads)
+        return [o * r for o, r in zip(out, R)] if R is not None else out
+
+    def PT(ys):
+        ys = [y * r for y, r in zip(ys, R)] if R is not None else ys
+        return backproject(geoms, ys, nthreads=nthreads)
+
+    def dot(a, b, w=None):
+        if isinstance(a, list):
+            return sum(dot(x, y, None if w is None else wi) for x, y, wi in zip(a, b, w or [None] * len(a)))
+        return float(np.sum(a * b * w)) if w is not None else float(np.sum(a * b))
+
+    g = [_d(x) for x in g]
+    W = [_d(w) for w in W] if W is not None else None
+    f = _d(f).copy()
+    if np.any(f):
+        if nonnegativity:
+            f = np.maximum(f, 0.0)
+        Pf = P(f)
+    else:
+        Pf = [np.zeros_like(x) for x in g]
+    resid = [a - b for a, b in zip(Pf, g)]
+    Q = None
+    if sqs:
+        P1 = P(np.ones_like(f))
+        if W is not None:
+            P1 = [a * w for a, w in zip(P1, W)]
+        Q = PT(P1)
+        nz = Q != 0.0
+        Q[nz] = 1.0 / Q[nz]
+        Q[~nz] = 1.0
+    d = np.zeros_like(f)
+    grad_old = np.zeros_like(f)
+    gog = 0.0
+    for n in range(num_iter):
+        grad = PT([r * w for r, w in zip(resid, W)] if W is not None else resid)
+        if beta > 0.0:
+            grad = grad + tv_gradient(f, delta, beta, p).reshape(f.shape)
+        u = grad * Q if Q is not None else grad.copy()
+        if n % 50 == 0:
+            d = u.copy()
+        else:
+            gamma = (dot(u, grad) - dot(u, grad_old)) / gog
+            d = u + gamma * d
+            if dot(d, grad) <= 0.0:
+                d = u.copy()
+        gog = dot(u, grad)
+        grad_old = grad.copy()
+        Pd = P(d)
+        num = dot(d, grad)
+        den = dot(Pd, Pd, W)
+        if beta > 0.0:
+            den += tv_quadform(f, d, delta, beta, p)
+        step = num / den if abs(den) > 1.0e-16 else 0.0
+        if step <= 0.0:
+            break
+        f = f - step * d
+        if nonnegativity:
+            f = np.maximum(f, 0.0)
+            Pf = P(f)
+            resid = [a - b for a, b in zip(Pf, g)]
+        else:
+            resid = [r - step * pd for r, pd in zip(resid, Pd)]
+    return f
+
+
 def poisson_loglik(g, Pf):
     """sum(g*log(Pf) - Pf) over bins with Pf > 0 (the MLEM objective)."""
     total = 0.0

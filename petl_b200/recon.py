@@ -164,28 +164,52 @@ def loglik(geoms, g, f, response=None):
     return total
 
 
+def auto_weights(gl):
+    """The reference RWLS default weights 1 / max(gaussian(g, 3 bins), 7),
+    per planogram, the Gaussian over (u1, u0) (src/petl_server.py:1739-1746)."""
+    out = []
+    for gi in as_list(gl):
+        w = gi.clone()
+        ops.gaussian_filter_(w.view(w.shape[0] * w.shape[1], w.shape[2], w.shape[3]), 3.0, 2)
+        w.clamp_(min=7.0)
+        ops.reciprocal_(w, 0.0)
+        out.append(w)
+    return out
+
+
 def rwls(geoms, g, f, num_iter, delta=1.0, beta=0.0, W=None, preconditioner=None, nonnegativity=True, p=1.0,
-         bp_mode="reference"):
-    """Regularized weighted least squares by PCG (PETLserver.RWLS)."""
+         bp_mode="reference", response=None):
+    """Regularized weighted least squares by PCG (PETLserver.RWLS,
+    src/petl_server.py:1691-1877): restarts every 50 iterations, optional
+    SQS preconditioner 1 / P^T W P 1, step <d, grad> / (<Pd, W Pd> + TV
+    quadratic form), optional non-negativity.  W: planograms, "auto" for
+    1 / max(gaussian(g, 3), 7) (src/petl_server.py:1739-1746), or None.
+    ``response`` (planograms R) makes the model R P, as the reference's
+    projectors with include_response_with_projectors."""
     geoms = as_list(geoms)
     gl = as_list(g)
+    Rl = as_list(response) if response is not None else None
     restart = 50
     if isinstance(W, str) and W == "auto":
-        # W = 1 / max(gaussian(g, 3), 7) (src/petl_server.py:1739-1746)
-        W = []
-        for gi in gl:
-            w = gi.clone()
-            shp = w.shape
-            w2 = w.view(shp[0] * shp[1], shp[2], shp[3])
-            ops.gaussian_filter_(w2, 3.0, 2)
-            w.clamp_(min=7.0)
-            ops.reciprocal_(w, 0.0)
-            W.append(w)
+        W = auto_weights(gl)
     Wl = as_list(W) if W is not None else None
+
+    def fwd(x, out=None):
+        y = as_list(ops.project(geoms, x, out if out is None or len(out) > 1 else out[0]))
+        if Rl is not None:
+            for yi, r in zip(y, Rl):
+                ops.multiply_(yi, r)
+        return y
+
+    def bwd(ys, out=None):
+        if Rl is not None:
+            ys = [y * r for y, r in zip(ys, Rl)]
+        return ops.backproject(geoms, ys, f=out, mode=bp_mode)
+
     if torch.any(f):
         if nonnegativity:
             f.clamp_(min=0.0)
-        Pf = as_list(ops.project(geoms, f))
+        Pf = fwd(f)
     else:
         Pf = [torch.zeros_like(x) for x in gl]
     resid = [p_ - g_ for p_, g_ in zip(Pf, gl)]
@@ -195,16 +219,15 @@ def rwls(geoms, g, f, num_iter, delta=1.0, beta=0.0, W=None, preconditioner=None
     Pd = [torch.empty_like(x) for x in gl]
     Q = None
     if preconditioner in (True, "SQS"):
-        ones = torch.ones_like(f)
-        P1 = as_list(ops.project(geoms, ones))
+        P1 = fwd(torch.ones_like(f))
         if Wl is not None:
             P1 = [a * w for a, w in zip(P1, Wl)]
-        Q = ops.backproject(geoms, P1, mode=bp_mode)
+        Q = bwd(P1)
         ops.reciprocal_(Q, 1.0)
     gog = 0.0
     for n in range(num_iter):
         WR = [r * w for r, w in zip(resid, Wl)] if Wl is not None else resid
-        ops.backproject(geoms, WR, f=grad, mode=bp_mode)
+        bwd(WR, out=grad)
         if beta > 0.0:
             grad += ops.tv_gradient(f, delta, beta, p)
         u = grad * Q if Q is not None else grad.clone()
@@ -217,7 +240,7 @@ def rwls(geoms, g, f, num_iter, delta=1.0, beta=0.0, W=None, preconditioner=None
                 d.copy_(u)
         gog = float(ops.dot(u, grad))
         grad_old.copy_(grad)
-        ops.project(geoms, d, Pd if len(Pd) > 1 else Pd[0])
+        Pd = fwd(d, Pd)
         num = float(ops.dot(d, grad))
         den = 0.0
         for pd, w in zip(Pd, Wl if Wl is not None else [None] * len(Pd)):
@@ -230,7 +253,7 @@ def rwls(geoms, g, f, num_iter, delta=1.0, beta=0.0, W=None, preconditioner=None
         f.add_(d, alpha=-step)
         if nonnegativity:
             f.clamp_(min=0.0)
-            Pf = as_list(ops.project(geoms, f))
+            Pf = fwd(f)
             resid = [p_ - g_ for p_, g_ in zip(Pf, gl)]
         else:
             resid = [r - step * pd for r, pd in zip(resid, Pd)]

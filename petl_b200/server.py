@@ -565,6 +565,82 @@ class PETLserver:
         f[:] = fd.cpu().numpy()
         return f
 
+    def LS(self, g, f, numIter, preconditioner=None, nonnegativityConstraint=True):
+        """Least squares by PCG (src/petl_server.py:1608-1634)."""
+        return self.RWLS(g, f, numIter, 1.0, 0.0, 1.0, preconditioner, nonnegativityConstraint)
+
+    def WLS(self, g, f, numIter, W=None, preconditioner=None, nonnegativityConstraint=True):
+        """Weighted least squares by PCG (src/petl_server.py:1636-1662)."""
+        return self.RWLS(g, f, numIter, 1.0, 0.0, W, preconditioner, nonnegativityConstraint)
+
+    def RLS(self, g, f, numIter, delta=1.0, beta=0.0, preconditioner=None, nonnegativityConstraint=True):
+        """Regularized (Huber-TV) least squares by PCG (src/petl_server.py:
+        1664-1689)."""
+        return self.RWLS(g, f, numIter, delta, beta, 1.0, preconditioner, nonnegativityConstraint)
+
+    def RWLS(self, g, f, numIter, delta=1.0, beta=0.0, W=None, preconditioner=None, nonnegativityConstraint=True,
+             include_response_with_projectors=False):
+        """Regularized weighted least squares by preconditioned conjugate
+        gradient (src/petl_server.py:1691-1845), device-resident.  W None:
+        1 / max(gaussian(g, 3), 7), times the response squared when a
+        response is set and not in the projectors; a number: no weights; else
+        planograms.  preconditioner True or 'SQS': 1 / P^T W P 1.  With a set
+        response: in the projectors (include_response_with_projectors), or
+        else g is corrected in place first and multiplied by the response at
+        the end, as the reference does."""
+        from . import recon
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        dev = torch.device("cuda")
+        to_dev = lambda a: a if _is_dev(a) else torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)  # noqa
+        R = [to_dev(r) for r in self.response] if self.response is not None else None
+        if W is None:
+            Wd = recon.auto_weights([to_dev(x) for x in g])
+            if R is not None and not include_response_with_projectors:
+                Wd = [w * r * r for w, r in zip(Wd, R)]
+        elif isinstance(W, list):
+            Wd = [to_dev(w) for w in W]
+        else:
+            Wd = None
+        corrected = R is not None and not include_response_with_projectors
+        if corrected:
+            self.apply_corrections(g)
+        gd = [to_dev(x) for x in g]
+        if f is None:
+            f = self.allocate_volume()
+        fd = to_dev(f)
+        pre = "SQS" if preconditioner in (True, "SQS") else None
+        fd = recon.rwls(self.geometries_from_model(), gd, fd, numIter, delta=delta, beta=beta, W=Wd,
+                        preconditioner=pre, nonnegativity=nonnegativityConstraint,
+                        response=R if include_response_with_projectors else None)
+        if corrected:
+            self.multiply(g, self.response)
+        if not _is_dev(f):
+            f[:] = fd.cpu().numpy()
+        return f
+
+    def RWLSstepSize(self, f, grad, d, Pd, W, delta, beta, num=None):
+        """<d, grad> / (<Pd, W Pd> + TV quadratic form), 0 if the denominator
+        vanishes (src/petl_server.py:1847-1877)."""
+        if num is None:
+            num = self.innerProd(d, grad)
+        denom = self.innerProd(Pd, Pd, W) if W is not None else self.innerProd(Pd, Pd)
+        if beta > 0.0:
+            denom += self.TVquadForm(f, d, delta, beta)
+        return num / denom if np.abs(denom) > 1.0e-16 else 0.0
+
+    def simulate_scatter(self, g, mu):
+        """As the reference's: validates the model and returns g unchanged
+        (src/petl_server.py:679-701)."""
+        if not self.all_defined():
+            raise ValueError("Error: volume and PET geometry must be defined")
+        if g is None:
+            g = self.allocate_projections()
+        self.set_model()
+        if not self.libprojectors.simulate_scatter(_pp(g), _fp(mu)):
+            raise TypeError("simulate_scatter failed")
+        return g
+
     def geometries_from_model(self):
         """Geometry objects equal to this model's planograms and volume."""
         from .geometry import Geometry
