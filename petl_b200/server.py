@@ -641,6 +641,31 @@ class PETLserver:
             raise TypeError("simulate_scatter failed")
         return g
 
+    # ------------------------------------------------ helpers of the reference
+    def floatstarstar(self, g):
+        """float** of a list of float32 arrays (src/petl_server.py:641-651)."""
+        return _pp(g)
+
+    def as_float_ptr(self, arr):
+        if arr is None:
+            return None
+        arr = np.asarray(arr, dtype=np.float32, order="C")
+        return arr.ctypes.data_as(fp)
+
+    def inner_product_helper(self, x, y, w=None):
+        return self.inner_product(x, y, w)
+
+    def display(self, x):
+        """Shows 3D data with napari when it is installed
+        (src/petl_server.py:1118-1134)."""
+        try:
+            import napari
+            napari.view_image(np.squeeze(x) if min(x.shape) == 1 else x, rgb=False)
+            napari.run()
+        except Exception:
+            print("Cannot load napari, to install run this command:")
+            print("pip install napari[all]")
+
     def geometries_from_model(self):
         """Geometry objects equal to this model's planograms and volume."""
         from .geometry import Geometry
@@ -744,3 +769,41 @@ class PETLserver:
             x[:] = y[:]
             return x
         return y
+
+
+class PETXserver(PETLserver):
+    """The PET/X scanner preset (src/petx_server.py:4-42): two planograms
+    (psi 0 and 90 degrees, 1.6 mm pixels), the default volume, and the
+    crystal-block module model used for the stopping power: 8 x 5 blocks on
+    each psi-0 panel and 4 x 5 on each psi-90 panel, 30.32 mm blocks with
+    1.28 mm gaps, 20 mm deep (use_simple_geometry: four slabs instead)."""
+
+    def __init__(self, param_id=None, lib_dir="", use_simple_geometry=False):
+        super().__init__(param_id, lib_dir)
+        pitch = 1.6
+        self.add_planogram(psi=0.0, D=101.0, L=251.52, H=156.72, T=pitch)
+        self.add_planogram(psi=90.0, D=266.6, L=125.12, H=156.72, T=pitch)
+        self.set_default_volume()
+        block, gap, depth = 30.32, 1.28, 20.0
+        if use_simple_geometry:
+            self.add_module([0.0, 0.5 * 101.0 + 10.0, 0.0], [0.5 * 251.52, 10.0, 0.5 * 156.72])
+            self.add_module([0.0, -0.5 * 101.0 - 10.0, 0.0], [0.5 * 251.52, 10.0, 0.5 * 156.72])
+            self.add_module([0.5 * 251.52 + 10.0, 0.0, 0.0], [10.0, 0.5 * 101.0 + 20.0, 0.5 * 156.72])
+            self.add_module([-0.5 * 251.52 - 10.0, 0.0, 0.0], [10.0, 0.5 * 101.0 + 20.0, 0.5 * 156.72])
+            return
+        c_y = 101.0 * 0.5
+        for m in range(5):
+            c_z = (m - 2) * (block + gap)
+            for n in range(8):
+                c_x = (n - 3.5) * (block + gap)
+                half = [0.5 * block, 0.5 * depth, 0.5 * block]
+                self.add_module([c_x, c_y + 0.5 * depth, c_z], half)
+                self.add_module([c_x, -c_y - 0.5 * depth, c_z], half)
+        c_x = 266.6 * 0.5
+        for m in range(5):
+            c_z = (m - 2) * (block + gap)
+            for n in range(4):
+                c_y = (n - 1.5) * (block + gap)
+                half = [0.5 * depth, 0.5 * block, 0.5 * block]
+                self.add_module([c_x + 0.5 * depth, c_y, c_z], half)
+                self.add_module([-c_x - 0.5 * depth, c_y, c_z], half)

@@ -129,3 +129,35 @@ def test_unsupported_reference_calls_fail_cleanly():
     assert not L.voxelize(None, 1)
     assert not L.ray_trace(None, 1)
     assert L.clear_phantom()
+
+
+def test_server_exposes_the_reference_methods():
+    """Every public method of the reference PETLserver (src/petl_server.py)
+    exists on the mirror class."""
+    from petl_b200.server import PETLserver
+    names = """about set_response clear_response create_new_model set_model volume_defined geometry_defined
+    all_defined print_parameters numX numY numZ voxelWidth voxelHeight offsetX offsetY offsetZ get_numPlanograms
+    get_planogramSize allocate_projections allocate_rebinned_projections copy_data copyData allocate_volume
+    clearAll add_planogram remove_planogram keep_only_planogram set_default_volume set_volume calc_response
+    apply_corrections floatstarstar bin simulate_scatter project backproject FBP PFDR add_object add_module
+    clear_phantom clear_modules scale_phantom voxelize ray_trace stopping_power apply_solid_angle_correction
+    apply_solid_angle_model save_data load_data display as_float_ptr inner_product_helper inner_product innerProd
+    isAllZeros setToConstant setToZero setToOne sensitivity clip scale square subtract scalarAdd multiply divide
+    rdivide reciprocal MLEM LS WLS RLS RWLS RWLSstepSize TVcost TVgradient TVquadForm diffuse TV_denoise
+    relative_differences_grad gaussian_filter""".split()
+    missing = [n for n in names if not callable(getattr(PETLserver, n, None))]
+    assert not missing, missing
+
+
+def test_petx_preset_model():
+    """The PET/X preset (src/petx_server.py:4-42): two planograms with the
+    reference's shapes, the default volume, 120 crystal blocks."""
+    from petl_b200 import PETXserver
+    s = PETXserver()
+    assert s.get_numPlanograms() == 2
+    assert [tuple(int(v) for v in s.get_planogramSize(i)) for i in range(2)] == [(63, 63, 96, 220),
+                                                                                 (97, 167, 96, 244)]
+    assert s.volume_defined()
+    # solids are checked on the host: a bad one is refused, good ones accepted
+    assert not s.add_object(9, [0, 0, 0], [1, 1, 1], 1.0)
+    assert s.add_object("cone_y", [0, 0, 0], [1, 5, 3], 1.0)
