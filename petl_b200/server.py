@@ -771,12 +771,41 @@ class PETLserver:
         return y
 
 
+def petx_modules(use_simple_geometry=False):
+    """The PET/X crystal blocks as (centre, half sizes) in mm
+    (src/petx_server.py:13-42): 8 x 5 blocks on each psi-0 panel and 4 x 5 on
+    each psi-90 panel, 30.32 mm blocks with 1.28 mm gaps, 20 mm deep; or four
+    slabs (use_simple_geometry)."""
+    if use_simple_geometry:
+        return [([0.0, 0.5 * 101.0 + 10.0, 0.0], [0.5 * 251.52, 10.0, 0.5 * 156.72]),
+                ([0.0, -0.5 * 101.0 - 10.0, 0.0], [0.5 * 251.52, 10.0, 0.5 * 156.72]),
+                ([0.5 * 251.52 + 10.0, 0.0, 0.0], [10.0, 0.5 * 101.0 + 20.0, 0.5 * 156.72]),
+                ([-0.5 * 251.52 - 10.0, 0.0, 0.0], [10.0, 0.5 * 101.0 + 20.0, 0.5 * 156.72])]
+    block, gap, depth = 30.32, 1.28, 20.0
+    out = []
+    c_y = 101.0 * 0.5
+    for m in range(5):
+        c_z = (m - 2) * (block + gap)
+        for n in range(8):
+            c_x = (n - 3.5) * (block + gap)
+            half = [0.5 * block, 0.5 * depth, 0.5 * block]
+            out.append(([c_x, c_y + 0.5 * depth, c_z], half))
+            out.append(([c_x, -c_y - 0.5 * depth, c_z], half))
+    c_x = 266.6 * 0.5
+    for m in range(5):
+        c_z = (m - 2) * (block + gap)
+        for n in range(4):
+            c_y = (n - 1.5) * (block + gap)
+            half = [0.5 * depth, 0.5 * block, 0.5 * block]
+            out.append(([c_x + 0.5 * depth, c_y, c_z], half))
+            out.append(([-c_x - 0.5 * depth, c_y, c_z], half))
+    return out
+
+
 class PETXserver(PETLserver):
     """The PET/X scanner preset (src/petx_server.py:4-42): two planograms
     (psi 0 and 90 degrees, 1.6 mm pixels), the default volume, and the
-    crystal-block module model used for the stopping power: 8 x 5 blocks on
-    each psi-0 panel and 4 x 5 on each psi-90 panel, 30.32 mm blocks with
-    1.28 mm gaps, 20 mm deep (use_simple_geometry: four slabs instead)."""
+    crystal-block module model (petx_modules) for the stopping power."""
 
     def __init__(self, param_id=None, lib_dir="", use_simple_geometry=False):
         super().__init__(param_id, lib_dir)
@@ -784,26 +813,5 @@ class PETXserver(PETLserver):
         self.add_planogram(psi=0.0, D=101.0, L=251.52, H=156.72, T=pitch)
         self.add_planogram(psi=90.0, D=266.6, L=125.12, H=156.72, T=pitch)
         self.set_default_volume()
-        block, gap, depth = 30.32, 1.28, 20.0
-        if use_simple_geometry:
-            self.add_module([0.0, 0.5 * 101.0 + 10.0, 0.0], [0.5 * 251.52, 10.0, 0.5 * 156.72])
-            self.add_module([0.0, -0.5 * 101.0 - 10.0, 0.0], [0.5 * 251.52, 10.0, 0.5 * 156.72])
-            self.add_module([0.5 * 251.52 + 10.0, 0.0, 0.0], [10.0, 0.5 * 101.0 + 20.0, 0.5 * 156.72])
-            self.add_module([-0.5 * 251.52 - 10.0, 0.0, 0.0], [10.0, 0.5 * 101.0 + 20.0, 0.5 * 156.72])
-            return
-        c_y = 101.0 * 0.5
-        for m in range(5):
-            c_z = (m - 2) * (block + gap)
-            for n in range(8):
-                c_x = (n - 3.5) * (block + gap)
-                half = [0.5 * block, 0.5 * depth, 0.5 * block]
-                self.add_module([c_x, c_y + 0.5 * depth, c_z], half)
-                self.add_module([c_x, -c_y - 0.5 * depth, c_z], half)
-        c_x = 266.6 * 0.5
-        for m in range(5):
-            c_z = (m - 2) * (block + gap)
-            for n in range(4):
-                c_y = (n - 1.5) * (block + gap)
-                half = [0.5 * depth, 0.5 * block, 0.5 * block]
-                self.add_module([c_x + 0.5 * depth, c_y, c_z], half)
-                self.add_module([-c_x - 0.5 * depth, c_y, c_z], half)
+        for c, r in petx_modules(use_simple_geometry):
+            self.add_module(c, r)

@@ -6,6 +6,7 @@
     python -m petl_b200.studies serving     # 200 Poisson-arrival OSEM requests, p50/p99
     python -m petl_b200.studies binning     # list-mode binning, device and C-ABI file rates
     python -m petl_b200.studies corrections # solid angle and apply_corrections, device and C ABI
+    python -m petl_b200.studies response    # PET/X stopping power (120 blocks) and calc_response
 
 All inputs are synthetic and seeded: ellipsoid phantoms (replace semantics,
 later ellipsoids overwrite earlier ones), forward projected with the
@@ -368,14 +369,46 @@ def study_corrections(seed=0, reps=5):
     return res
 
 
+def study_response(seed=0, reps=3):
+    """The PET/X detector response: the stopping power of its 120 crystal
+    blocks over both planograms (463 M coincidence lines), device-resident
+    (CUDA events), then PETLserver.calc_response (stopping power through the
+    C ABI, the 0.6571-bin Gaussian, the solid-angle model) on host arrays."""
+    from .server import PETXserver, petx_modules
+    s = PETXserver()
+    geoms = s.geometries_from_model()
+    solids = [ops.make_solid(1, c, r, 0.0815) for c, r in petx_modules()]
+    out = [torch.empty(G.shape, device="cuda") for G in geoms]
+    lines = sum(int(np.prod(G.shape)) for G in geoms)
+    ops.ray_trace(geoms, solids, g=out, stopping_power=True)
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ops.ray_trace(geoms, solids, g=out, stopping_power=True)
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    res = {"study": "response", "workload": "PET/X preset, planograms (63,63,96,220) and (97,167,96,244), "
+           "120 crystal blocks", "lines": lines, "stopping_power_device_ms": float(np.median(ts)),
+           "lines_per_s": lines / (np.median(ts) * 1e-3)}
+    del out
+    t0 = time.perf_counter()
+    R = s.calc_response(oversampling=1)
+    res["calc_response_s"] = time.perf_counter() - t0
+    res["response_mean"] = [float(r.mean()) for r in R]
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving", "binning", "corrections"])
+    ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving", "binning", "corrections",
+                                      "response"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--requests", type=int, default=200)
     a = ap.parse_args(argv)
     fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
-          "binning": study_binning, "corrections": study_corrections}
+          "binning": study_binning, "corrections": study_corrections, "response": study_response}
     if a.study == "serving":
         res = study_serving(n=a.requests, seed=a.seed)
     else:

@@ -29,27 +29,6 @@ PITCH = 1.6
 PLANOGRAMS = [(0.0, 101.0, 251.52, 156.72, PITCH), (90.0, 266.6, 125.12, 156.72, PITCH)]
 
 
-def petx_modules():
-    """The crystal blocks of src/petx_server.py:28-42: (centre, half sizes)."""
-    block, gap, depth = 30.32, 1.28, 20.0
-    out = []
-    c_y = 101.0 * 0.5
-    for m in range(5):
-        c_z = (m - 2) * (block + gap)
-        for n in range(8):
-            c_x = (n - 3.5) * (block + gap)
-            out.append(([c_x, c_y + 0.5 * depth, c_z], [0.5 * block, 0.5 * depth, 0.5 * block]))
-            out.append(([c_x, -c_y - 0.5 * depth, c_z], [0.5 * block, 0.5 * depth, 0.5 * block]))
-    c_x = 266.6 * 0.5
-    for m in range(5):
-        c_z = (m - 2) * (block + gap)
-        for n in range(4):
-            c_y = (n - 1.5) * (block + gap)
-            out.append(([c_x + 0.5 * depth, c_y, c_z], [0.5 * depth, 0.5 * block, 0.5 * block]))
-            out.append(([-c_x - 0.5 * depth, c_y, c_z], [0.5 * depth, 0.5 * block, 0.5 * block]))
-    return out
-
-
 def v_m1(D, H, T):
     return min(1.0, (H - 1.5 * T) / D)  # src/petl_server.py:498-501
 
@@ -57,7 +36,7 @@ def v_m1(D, H, T):
 def main():
     import torch
     from petl_b200 import PETLserver, ops
-    from petl_b200.server import _pp
+    from petl_b200.server import _pp, petx_modules
     mods = petx_modules()
     res = {"workload": "PET/X preset: planograms psi 0 (D 101, L 251.52, H 156.72) and psi 90 (D 266.6, "
                        "L 125.12, H 156.72), T 1.6 mm, v_m0 1; 120 crystal blocks (0.0815 / mm)",
