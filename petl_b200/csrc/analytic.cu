@@ -397,15 +397,20 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_trace(const RayArgs a)
     const petl_solid* solids = staged ? ss : a.solids;
     const Bound* bounds = staged ? sb : a.bounds;
     const petl_geom& G = a.G;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        long long t = idx;
-        const int iu0 = int(t % G.N_u0);
-        t /= G.N_u0;
-        const int iu1 = int(t % G.N_u1);
-        t /= G.N_u1;
-        const int iv0 = int(t % G.N_v0);
-        const int iv1 = int(t / G.N_v0);
+    // a warp traces a 4 x 8 (u1 x u0) tile of bins of one view: neighbouring
+    // parallel lines, which meet mostly the same solids
+    const int tiles_x = (G.N_u0 + 7) / 8, tiles_view = tiles_x * ((G.N_u1 + 3) / 4);
+    const long long items = (long long)G.N_v1 * G.N_v0 * tiles_view * 32;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int lane = int(it & 31);
+        const long long tile = it >> 5;
+        const long long view = tile / tiles_view;
+        const int tv = int(tile - view * tiles_view);
+        const int iu1 = (tv / tiles_x) * 4 + (lane >> 3), iu0 = (tv % tiles_x) * 8 + (lane & 7);
+        if (iu1 >= G.N_u1 || iu0 >= G.N_u0) continue;
+        const int iv0 = int(view % G.N_v0), iv1 = int(view / G.N_v0);
+        const long long idx = (view * G.N_u1 + iu1) * G.N_u0 + iu0;
         const float v1 = float(iv1) * G.T_v1 + G.v1_0;
         const float v0 = float(iv0) * G.T_v0 + G.v0_0;
         const float u1 = float(iu1) * G.T_u1 + G.u1_0;
