@@ -493,6 +493,24 @@ def mlem(geoms, g, num_iter, f=None, delta=2.0, beta=0.0, nthreads=0, response=N
     return f
 
 
+def project_sub(G, f, first, step, nthreads=0):
+    """P f on the views iv0 = first + k step of one planogram (FP64)."""
+    p = np.zeros(G.shape, np.float64)
+    fc = _d(f)
+    lib().oracle_project_sub_f64(ctypes.byref(G), _ptr(fc, ctypes.c_double), _ptr(p, ctypes.c_double), first, step,
+                                 nthreads)
+    return p
+
+
+def backproject_sub(G, g, first, step, nthreads=0):
+    """P^T g of one planogram using only the views iv0 = first + k step (FP64)."""
+    gc = _d(g)
+    out = np.zeros(G.vol_shape, np.float64)
+    lib().oracle_backproject_sub_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(out, ctypes.c_double), first,
+                                     step, nthreads)
+    return out
+
+
 def osem(geoms, g, num_iter, num_subsets, f=None, nthreads=0):
     """Ordered-subsets EM with interleaved subsets over iv0 (subset s holds the
     views iv0 with iv0 % S == s).  With S = 1 it is exactly ``mlem``."""
