@@ -16,8 +16,8 @@
 // are found in the solid's normalised frame; the end points are sorted and
 // each interval between consecutive end points is credited to the last solid
 // (in insertion order) that covers its midpoint.  The solids are staged in
-// shared memory with a bounding sphere each, and a line runs the exact
-// intersection only for the solids whose sphere it meets (a conservative
+// shared memory with a padded axis-aligned box each, and a line runs the
+// exact intersection only for the solids whose box it meets (a conservative
 // test: the result is unchanged).  The hits of a line are kept per thread
 // (up to kMaxHits; a line with more is resolved by rescanning the solids per
 // interval, which gives the same sum).  The reference's line parameterisation is kept: its
@@ -39,7 +39,7 @@ enum SolidType { kEllipsoid = 0, kBox = 1, kCylX = 2, kCylY = 3, kCylZ = 4, kCon
 constexpr float kFar = 1.0e12f;  // parameter of an unbounded side
 constexpr int kMaxHits = 32;     // hits of one line kept per thread
 constexpr int kRayThreads = 128;
-constexpr int kSmemSolids = 200;  // solids (and bounds) staged in shared memory (<= 44 KB)
+constexpr int kSmemSolids = 192;  // solids (and bounds) staged in shared memory (<= 46 KB)
 
 // ---------------------------------------------------------------------------
 // intersections (device)
@@ -260,21 +260,26 @@ __device__ bool solid_hit(const petl_solid& s, float3 p, float3 r, float& t0, fl
     return t1 > t0;
 }
 
-// Bounding sphere of a solid for culling (r2 < 0: always tested).
+// Axis-aligned box around a solid for culling, padded (always != 0: the
+// solid is always tested).
 struct Bound {
-    float cx, cy, cz, r2;
+    float lo[3], hi[3];
+    int always, pad;
 };
 
-// Whether the line p + t r may meet the solid: its distance to the sphere's
-// centre against the radius, with margins (relative to the radius and to the
-// float cancellation in |w|^2 - (w.r)^2/|r|^2) that keep every line the exact
-// test accepts.
-__device__ __forceinline__ bool may_hit(const Bound& b, float3 p, float3 r, float rr)
+// Whether the line p + t r may meet the solid: the line against the padded
+// box by slabs (inv = 1 / r per axis, infinite for a zero component).  The
+// padding (1e-4 of the extent plus 1e-3) exceeds the float error of the
+// slab parameters, so every line the exact test accepts passes.
+__device__ __forceinline__ bool may_hit(const Bound& b, float3 p, float3 inv)
 {
-    if (b.r2 < 0.0f) return true;
-    const float wx = b.cx - p.x, wy = b.cy - p.y, wz = b.cz - p.z;
-    const float ww = wx * wx + wy * wy + wz * wz, wr = wx * r.x + wy * r.y + wz * r.z;
-    return ww - wr * wr / rr <= b.r2 + 1.0e-5f * ww;
+    if (b.always) return true;
+    const float ax = (b.lo[0] - p.x) * inv.x, bx = (b.hi[0] - p.x) * inv.x;
+    const float ay = (b.lo[1] - p.y) * inv.y, by = (b.hi[1] - p.y) * inv.y;
+    const float az = (b.lo[2] - p.z) * inv.z, bz = (b.hi[2] - p.z) * inv.z;
+    const float tmin = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    const float tmax = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    return tmin <= tmax;
 }
 
 struct LineSums {
@@ -292,10 +297,10 @@ __device__ LineSums line_sums(const petl_solid* solids, const Bound* bounds, int
     int hid[kMaxHits];
     int count = 0;
     bool overflow = false;
-    const float rr = r.x * r.x + r.y * r.y + r.z * r.z;
+    const float3 inv = make_float3(1.0f / r.x, 1.0f / r.y, 1.0f / r.z);
     for (int j = 0; j < n; j++) {
         float t0, t1;
-        if (!may_hit(bounds[j], p, r, rr) || !solid_hit(solids[j], p, r, t0, t1)) continue;
+        if (!may_hit(bounds[j], p, inv) || !solid_hit(solids[j], p, r, t0, t1)) continue;
         if (count == kMaxHits) {
             overflow = true;
             break;
@@ -385,7 +390,7 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_trace(const RayArgs a)
     petl_solid* ss = reinterpret_cast<petl_solid*>(sb + (a.n <= kSmemSolids ? a.n : 0));
     const bool staged = a.n <= kSmemSolids;
     if (staged) {
-        const int words = a.n * int(sizeof(petl_solid) / 4), bwords = a.n * 4;
+        const int words = a.n * int(sizeof(petl_solid) / 4), bwords = a.n * int(sizeof(Bound) / 4);
         const int* src = reinterpret_cast<const int*>(a.solids);
         int* dst = reinterpret_cast<int*>(ss);
         for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
@@ -636,24 +641,36 @@ int voxelize(const petl_solid* solids, int n, float* f, int numX, int numY, int 
     return 0;
 }
 
-// Bounding sphere of a solid in world coordinates: centre, and the radius of
-// its unrotated, unclipped extent (rotations and clipping keep it inside);
-// cones are always tested.
+// Padded axis-aligned box around a solid in world coordinates: the solid's
+// extents when it is not rotated, else the box of its bounding sphere
+// (clipping only removes parts); cones are always tested.
 Bound solid_bound(const petl_solid& s)
 {
+    Bound b{};
     const float* c = s.centers;
     const float* r = s.radii;
-    double rad;
-    switch (s.type) {
-    case kEllipsoid: rad = std::max(r[0], std::max(r[1], r[2])); break;
-    case kBox: rad = std::sqrt(double(r[0]) * r[0] + double(r[1]) * r[1] + double(r[2]) * r[2]); break;
-    case kCylX: rad = std::sqrt(double(r[0]) * r[0] + std::pow(std::max(r[1], r[2]), 2.0)); break;
-    case kCylY: rad = std::sqrt(double(r[1]) * r[1] + std::pow(std::max(r[0], r[2]), 2.0)); break;
-    case kCylZ: rad = std::sqrt(double(r[2]) * r[2] + std::pow(std::max(r[0], r[1]), 2.0)); break;
-    default: return Bound{0.0f, 0.0f, 0.0f, -1.0f};
+    double ext[3] = {std::fabs(double(r[0])), std::fabs(double(r[1])), std::fabs(double(r[2]))};
+    if (s.type >= kConeX || s.type < kEllipsoid) {
+        b.always = 1;
+        return b;
     }
-    rad = std::fabs(rad) * (1.0 + 1.0e-4) + 1.0e-3;
-    return Bound{c[0], c[1], c[2], float(rad * rad)};
+    if (s.rotated) {
+        double rad;
+        switch (s.type) {
+        case kEllipsoid: rad = std::max(ext[0], std::max(ext[1], ext[2])); break;
+        case kBox: rad = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]); break;
+        case kCylX: rad = std::sqrt(ext[0] * ext[0] + std::pow(std::max(ext[1], ext[2]), 2.0)); break;
+        case kCylY: rad = std::sqrt(ext[1] * ext[1] + std::pow(std::max(ext[0], ext[2]), 2.0)); break;
+        default: rad = std::sqrt(ext[2] * ext[2] + std::pow(std::max(ext[0], ext[1]), 2.0)); break;
+        }
+        ext[0] = ext[1] = ext[2] = rad;
+    }
+    for (int k = 0; k < 3; k++) {
+        const double e = ext[k] * (1.0 + 1.0e-4) + 1.0e-3;
+        b.lo[k] = float(double(c[k]) - e);
+        b.hi[k] = float(double(c[k]) + e);
+    }
+    return b;
 }
 
 int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int oversampling, bool stopping,
