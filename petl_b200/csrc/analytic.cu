@@ -16,15 +16,18 @@
 // are found in the solid's normalised frame; the end points are sorted and
 // each interval between consecutive end points is credited to the last solid
 // (in insertion order) that covers its midpoint.  The solids are staged in
-// shared memory with a padded axis-aligned box each, and a line runs the
-// exact intersection only for the solids whose box it meets (a conservative
-// test: the result is unchanged).  The hits of a line are kept per thread
+// shared memory with a padded axis-aligned box each, grouped into clusters of
+// up to 8 nearby solids with a box around each cluster; a line tests a
+// cluster's box, then the boxes of its members, and runs the exact
+// intersection only for the solids whose box it meets (conservative tests:
+// the result is unchanged).  The hits of a line are kept per thread
 // (up to kMaxHits; a line with more is resolved by rescanning the solids per
 // interval, which gives the same sum).  The reference's line parameterisation is kept: its
 // direction is the unnormalised direction times its own length (the
 // reference divides by rsqrt of the squared length), so lengths come out
 // divided by 1 + v0^2 + v1^2; and its field-of-view test for u0 uses half
 // of T_v0 (src/analytic_ray_tracing_gpu.cu:721).
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -39,7 +42,7 @@ enum SolidType { kEllipsoid = 0, kBox = 1, kCylX = 2, kCylY = 3, kCylZ = 4, kCon
 constexpr float kFar = 1.0e12f;  // parameter of an unbounded side
 constexpr int kMaxHits = 32;     // hits of one line kept per thread
 constexpr int kRayThreads = 128;
-constexpr int kSmemSolids = 192;  // solids (and bounds) staged in shared memory (<= 46 KB)
+constexpr int kSmemSolids = 176;  // solids, boxes, clusters staged in shared memory (<= 45 KB)
 
 // ---------------------------------------------------------------------------
 // intersections (device)
@@ -282,6 +285,15 @@ __device__ __forceinline__ bool may_hit(const Bound& b, float3 p, float3 inv)
     return tmin <= tmax;
 }
 
+// A group of up to kClusterSize solids that lie close together: the padded
+// box around all of them, and their indices order[first .. first + count).
+struct Cluster {
+    Bound box;
+    int first, count, pad0, pad1;
+};
+
+constexpr int kClusterSize = 8;
+
 struct LineSums {
     float fwd, bwd;  // value x length with the interval midpoint at t >= 0 / t < 0
 };
@@ -291,26 +303,40 @@ struct LineSums {
 // (src/analytic_ray_tracing_gpu.cu:536-691).  SPLIT: the two half-lines
 // apart (stopping power); otherwise every interval into fwd, in order.
 template <bool SPLIT>
-__device__ LineSums line_sums(const petl_solid* solids, const Bound* bounds, int n, float3 p, float3 r)
+__device__ LineSums line_sums(const petl_solid* solids, const Bound* bounds, const Cluster* clusters, int ncl,
+                              const int* order, int n, float3 p, float3 r)
 {
     float h0[kMaxHits], h1[kMaxHits], e[2 * kMaxHits];
     int hid[kMaxHits];
     int count = 0;
     bool overflow = false;
     const float3 inv = make_float3(1.0f / r.x, 1.0f / r.y, 1.0f / r.z);
-    for (int j = 0; j < n; j++) {
-        float t0, t1;
-        if (!may_hit(bounds[j], p, inv) || !solid_hit(solids[j], p, r, t0, t1)) continue;
-        if (count == kMaxHits) {
-            overflow = true;
-            break;
+    // clusters, then their members; the hits are kept in solid order
+    for (int c = 0; c < ncl && !overflow; c++) {
+        const Cluster& cl = clusters[c];
+        if (!may_hit(cl.box, p, inv)) continue;
+        for (int k = cl.first; k < cl.first + cl.count; k++) {
+            const int j = order[k];
+            float t0, t1;
+            if (!may_hit(bounds[j], p, inv) || !solid_hit(solids[j], p, r, t0, t1)) continue;
+            if (count == kMaxHits) {
+                overflow = true;
+                break;
+            }
+            int pos = count;
+            while (pos > 0 && hid[pos - 1] > j) {
+                h0[pos] = h0[pos - 1];
+                h1[pos] = h1[pos - 1];
+                hid[pos] = hid[pos - 1];
+                pos--;
+            }
+            h0[pos] = t0;
+            h1[pos] = t1;
+            hid[pos] = j;
+            e[2 * count] = t0;
+            e[2 * count + 1] = t1;
+            count++;
         }
-        h0[count] = t0;
-        h1[count] = t1;
-        hid[count] = j;
-        e[2 * count] = t0;
-        e[2 * count + 1] = t1;
-        count++;
     }
     LineSums acc{0.0f, 0.0f};
     if (!overflow) {
@@ -375,6 +401,9 @@ struct RayArgs {
     petl_geom G;
     const petl_solid* solids;
     const Bound* bounds;
+    const Cluster* clusters;
+    const int* order;
+    int ncl;
     int n;
     float* g;
     int os;
@@ -386,21 +415,26 @@ template <bool STOP>
 __global__ void __launch_bounds__(kRayThreads) k_ray_trace(const RayArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Bound* sb = reinterpret_cast<Bound*>(smem_raw);
-    petl_solid* ss = reinterpret_cast<petl_solid*>(sb + (a.n <= kSmemSolids ? a.n : 0));
     const bool staged = a.n <= kSmemSolids;
+    Cluster* sc = reinterpret_cast<Cluster*>(smem_raw);
+    Bound* sb = reinterpret_cast<Bound*>(sc + (staged ? a.ncl : 0));
+    petl_solid* ss = reinterpret_cast<petl_solid*>(sb + (staged ? a.n : 0));
+    int* so = reinterpret_cast<int*>(ss + (staged ? a.n : 0));
     if (staged) {
-        const int words = a.n * int(sizeof(petl_solid) / 4), bwords = a.n * int(sizeof(Bound) / 4);
-        const int* src = reinterpret_cast<const int*>(a.solids);
-        int* dst = reinterpret_cast<int*>(ss);
-        for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
-        const int* bsrc = reinterpret_cast<const int*>(a.bounds);
-        int* bdst = reinterpret_cast<int*>(sb);
-        for (int i = threadIdx.x; i < bwords; i += blockDim.x) bdst[i] = bsrc[i];
+        auto copy = [&](void* dst, const void* src, int words) {
+            for (int i = threadIdx.x; i < words; i += blockDim.x)
+                static_cast<int*>(dst)[i] = static_cast<const int*>(src)[i];
+        };
+        copy(sc, a.clusters, a.ncl * int(sizeof(Cluster) / 4));
+        copy(sb, a.bounds, a.n * int(sizeof(Bound) / 4));
+        copy(ss, a.solids, a.n * int(sizeof(petl_solid) / 4));
+        copy(so, a.order, a.n);
         __syncthreads();
     }
     const petl_solid* solids = staged ? ss : a.solids;
     const Bound* bounds = staged ? sb : a.bounds;
+    const Cluster* clusters = staged ? sc : a.clusters;
+    const int* order = staged ? so : a.order;
     const petl_geom& G = a.G;
     // a warp traces a 4 x 8 (u1 x u0) tile of bins of one view: neighbouring
     // parallel lines, which meet mostly the same solids
@@ -433,7 +467,8 @@ __global__ void __launch_bounds__(kRayThreads) k_ray_trace(const RayArgs a)
         auto value = [&](float du1, float du0) {
             const float w = u0 + du0;
             const LineSums s =
-                line_sums<STOP>(solids, bounds, a.n, make_float3(w * a.cos_psi, w * a.sin_psi, u1 + du1), r);
+                line_sums<STOP>(solids, bounds, clusters, a.ncl, order, a.n,
+                                make_float3(w * a.cos_psi, w * a.sin_psi, u1 + du1), r);
             return STOP ? (1.0f - expf(-s.fwd)) * (1.0f - expf(-s.bwd)) : s.fwd;
         };
         float out;
@@ -609,6 +644,7 @@ int upload(const T* host, size_t count, T** dev, cudaStream_t st)
     const cudaError_t e = cudaMemcpyAsync(*dev, host, count * sizeof(T), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
         cudaFreeAsync(*dev, st);
+        *dev = nullptr;
         set_error(std::string("analytic: upload: ") + cudaGetErrorString(e));
         return int(e);
     }
@@ -673,6 +709,59 @@ Bound solid_bound(const petl_solid& s)
     return b;
 }
 
+// Groups the solids into clusters of up to kClusterSize that lie close
+// together: solids always tested in clusters of their own, the others by
+// median splits of their box centres along the longest axis.
+void make_clusters(const std::vector<Bound>& b, std::vector<Cluster>& cl, std::vector<int>& order)
+{
+    std::vector<int> boxed, always;
+    for (int j = 0; j < int(b.size()); j++) (b[j].always ? always : boxed).push_back(j);
+    auto emit = [&](const int* idx, int cnt, bool all) {
+        Cluster c{};
+        c.first = int(order.size());
+        c.count = cnt;
+        c.box.always = all ? 1 : 0;
+        for (int k = 0; k < 3; k++) {
+            c.box.lo[k] = 3.0e38f;
+            c.box.hi[k] = -3.0e38f;
+        }
+        for (int i = 0; i < cnt; i++) {
+            order.push_back(idx[i]);
+            for (int k = 0; k < 3 && !all; k++) {
+                c.box.lo[k] = std::min(c.box.lo[k], b[idx[i]].lo[k]);
+                c.box.hi[k] = std::max(c.box.hi[k], b[idx[i]].hi[k]);
+            }
+        }
+        cl.push_back(c);
+    };
+    for (size_t i = 0; i < always.size(); i += kClusterSize)
+        emit(always.data() + i, int(std::min<size_t>(kClusterSize, always.size() - i)), true);
+    auto centre = [&](int j, int k) { return 0.5f * (b[j].lo[k] + b[j].hi[k]); };
+    std::vector<std::pair<int, int>> todo{{0, int(boxed.size())}};
+    while (!todo.empty()) {
+        const auto [lo, hi] = todo.back();
+        todo.pop_back();
+        if (hi - lo <= kClusterSize) {
+            if (hi > lo) emit(boxed.data() + lo, hi - lo, false);
+            continue;
+        }
+        float mn[3] = {3.0e38f, 3.0e38f, 3.0e38f}, mx[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
+        for (int i = lo; i < hi; i++)
+            for (int k = 0; k < 3; k++) {
+                mn[k] = std::min(mn[k], centre(boxed[i], k));
+                mx[k] = std::max(mx[k], centre(boxed[i], k));
+            }
+        int ax = 0;
+        for (int k = 1; k < 3; k++)
+            if (mx[k] - mn[k] > mx[ax] - mn[ax]) ax = k;
+        const int mid = (lo + hi) / 2;
+        std::nth_element(boxed.begin() + lo, boxed.begin() + mid, boxed.begin() + hi,
+                         [&](int x, int y) { return centre(x, ax) < centre(y, ax); });
+        todo.push_back({mid, hi});
+        todo.push_back({lo, mid});
+    }
+}
+
 int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int oversampling, bool stopping,
               cudaStream_t st)
 {
@@ -686,15 +775,25 @@ int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int
     if (int rc = upload(solids, size_t(n), &ds, st)) return rc;
     std::vector<Bound> hb;
     for (int j = 0; j < n; j++) hb.push_back(solid_bound(solids[j]));
+    std::vector<Cluster> hc;
+    std::vector<int> ho;
+    make_clusters(hb, hc, ho);
     Bound* db = nullptr;
-    if (int rc = upload(hb.data(), hb.size(), &db, st)) {
-        cudaFreeAsync(ds, st);
+    Cluster* dc = nullptr;
+    int* dord = nullptr;
+    int rc = upload(hb.data(), hb.size(), &db, st);
+    if (!rc) rc = upload(hc.data(), hc.size(), &dc, st);
+    if (!rc) rc = upload(ho.data(), ho.size(), &dord, st);
+    if (rc) {
+        for (void* q : {static_cast<void*>(ds), static_cast<void*>(db), static_cast<void*>(dc)})
+            if (q) cudaFreeAsync(q, st);
         return rc;
     }
     // the reference's constants: cos/sin of the float psi in float
-    RayArgs a{G, ds, db, n, g, os, std::cos(G.psi), std::sin(G.psi),
+    RayArgs a{G, ds, db, dc, dord, int(hc.size()), n, g, os, std::cos(G.psi), std::sin(G.psi),
               (long long)G.N_v1 * G.N_v0 * G.N_u1 * G.N_u0};
-    const size_t smem = n <= kSmemSolids ? size_t(n) * (sizeof(petl_solid) + sizeof(Bound)) : 0;
+    const size_t smem =
+        n <= kSmemSolids ? hc.size() * sizeof(Cluster) + size_t(n) * (sizeof(petl_solid) + sizeof(Bound) + 4) : 0;
     const int grid = int(std::min<long long>((a.total + kRayThreads - 1) / kRayThreads, 64LL * sm_count()));
     if (stopping)
         k_ray_trace<true><<<grid, kRayThreads, smem, st>>>(a);
@@ -704,6 +803,8 @@ int ray_trace(const petl_geom& G, const petl_solid* solids, int n, float* g, int
     const cudaError_t e = cudaGetLastError();
     cudaFreeAsync(ds, st);
     cudaFreeAsync(db, st);
+    cudaFreeAsync(dc, st);
+    cudaFreeAsync(dord, st);
     if (e != cudaSuccess) {
         set_error(std::string("ray_trace launch: ") + cudaGetErrorString(e));
         return int(e);
