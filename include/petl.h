@@ -15,10 +15,11 @@
  *
  * Error behaviour: bool functions return false (and print a reason to stderr)
  * on invalid input or device failure, the contract the reference binding
- * relies on (it raises on false).  Functions that exist in the reference only
- * for subsystems outside the reconstruction path (analytic phantoms / ray
- * tracing, detector-response corrections, scatter) are exported so that the
- * binding loads, and return false with a message.
+ * relies on (it raises on false).  Setters keep the reference's rules, e.g.
+ * an offset must be positive to be accepted (src/petl_c_interface.cpp:
+ * 154-200).  Every function of the reference interface computes what the
+ * reference's does, on the GPU; the scatter simulation, which computes
+ * nothing in the reference, validates its inputs as the reference's does.
  *
  * Device-pointer entry points for the resident path live in petl_device.h.
  */
