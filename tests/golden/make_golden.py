@@ -382,6 +382,30 @@ PHANTOM = [
 ]
 
 
+def _rot(axis, deg):
+    """Rotation by deg degrees about x (0), y (1) or z (2), as a 3x3 tuple."""
+    c, s_ = float(np.cos(np.radians(deg))), float(np.sin(np.radians(deg)))
+    R = np.eye(3)
+    i, j = [(1, 2), (0, 2), (0, 1)][axis]
+    R[i, i], R[i, j], R[j, i], R[j, j] = c, -s_, s_, c
+    return tuple(map(tuple, R))
+
+
+# Rotated cylinders, cones and boxes, clipping on y and z, a negative value
+# and overlaps.
+PHANTOM2 = [
+    (1, (0.0, 0.0, 0.0), (20.0, 18.0, 6.0), 0.2, None, None),
+    (4, (-6.0, 4.0, 0.0), (4.0, 3.0, 5.0), 1.3, _rot(0, 40.0), None),
+    (5, (8.0, 6.0, 1.0), (6.0, 1.5, 3.5), 0.7, _rot(2, 20.0), None),
+    (7, (-8.0, -8.0, -1.0), (1.0, 3.0, 4.0), 0.6, _rot(1, 15.0), None),
+    (0, (6.0, -6.0, 0.0), (7.0, 5.0, 4.0), 1.8, None, (0.0, 1.0, 0.0)),
+    (2, (0.0, 10.0, 1.0), (9.0, 2.5, 2.5), 0.9, None, (0.0, 0.0, 2.0)),
+    (1, (12.0, -12.0, 0.0), (3.0, 4.0, 3.0), -0.5, _rot(1, 30.0), None),
+    (3, (-12.0, 0.0, 2.0), (2.0, 8.0, 2.0), 1.1, _rot(2, -25.0), None),
+    (6, (0.0, -14.0, 0.0), (2.0, 4.0, 1.0), 0.4, None, None),
+]
+
+
 def _add_solids(fn, solids):
     for t, c, r, v, A, clip in solids:
         c = np.array(c, np.float32)
@@ -419,6 +443,12 @@ def run_voxelize(ref, out):
     f = np.full((vol[2], vol[1], vol[0]), 0.25, np.float32)
     ref.L.voxelize(ptr(f), 1)
     rec["f_scaled"] = f
+    ref.L.clear_phantom()
+    _add_solids(ref.L.add_object, PHANTOM2)
+    for os_ in (1, 5):
+        f = np.zeros((vol[2], vol[1], vol[0]), np.float32)
+        ref.L.voxelize(ptr(f), os_)
+        rec[f"f2_os{os_}"] = f
     rec["volume"] = np.array(vol)
     np.savez_compressed(os.path.join(out, "voxelize.npz"), **rec)
     print("wrote voxelize", {k: float(v.sum()) for k, v in rec.items() if k.startswith("f_")})
@@ -443,6 +473,13 @@ def run_raytrace(ref, out):
                 raise RuntimeError("reference ray_trace failed")
             for i, g in enumerate(gs):
                 rec[f"{name}_rt{os_}_{i}"] = g
+        ref.L.clear_phantom()
+        _add_solids(ref.L.add_object, PHANTOM2)
+        gs = [np.full(sh, 7.0, np.float32) for sh in ref.shapes()]
+        if not ref.L.ray_trace(ref.pp(gs), 1):
+            raise RuntimeError("reference ray_trace failed")
+        for i, g in enumerate(gs):
+            rec[f"{name}_rt2_{i}"] = g
         gs = [np.full(sh, 7.0, np.float32) for sh in ref.shapes()]
         if not ref.L.stopping_power(ref.pp(gs), 1):
             raise RuntimeError("reference stopping_power failed")

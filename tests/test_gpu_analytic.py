@@ -21,7 +21,7 @@ from conftest import load_golden, rel_l2
 pytestmark = pytest.mark.gpu
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
-from make_golden import PHANTOM, _modules  # noqa: E402
+from make_golden import PHANTOM, PHANTOM2, _modules  # noqa: E402
 
 RT_CASES = ["g0", "g30", "gpetx"]
 
@@ -63,6 +63,11 @@ def test_device_voxelize_matches_reference(cuda):
     f = _t(np.full((nz, ny, nx), 0.25, np.float32), cuda)
     ops.voxelize_(f, list(arr), vw, vh, x0, y0, z0)
     assert np.array_equal(f.cpu().numpy(), z["f_scaled"])
+    solids2 = _product_solids(PHANTOM2)
+    for os_ in (1, 5):
+        f = _t(np.zeros((nz, ny, nx), np.float32), cuda)
+        ops.voxelize_(f, solids2, vw, vh, x0, y0, z0, oversampling=os_)
+        assert np.array_equal(f.cpu().numpy(), z[f"f2_os{os_}"])
 
 
 def test_cabi_voxelize_matches_reference(cuda):
@@ -105,6 +110,9 @@ def test_device_ray_trace_matches_oracle_and_reference(cuda, name):
             got = ops.ray_trace(G, solids, oversampling=os_).cpu().numpy()
             assert rel_l2(got, O.ray_trace(Go, osolids, os_)) < 1e-5
             assert rel_l2(got, z[f"{name}_rt{os_}_{i}"]) < 1e-5
+        got2 = ops.ray_trace(G, _product_solids(PHANTOM2)).cpu().numpy()
+        assert rel_l2(got2, O.ray_trace(Go, _oracle_solids(PHANTOM2), 1)) < 1e-5
+        assert rel_l2(got2, z[f"{name}_rt2_{i}"]) < 1e-5
         sp = ops.ray_trace(G, mods, stopping_power=True).cpu().numpy()
         assert rel_l2(sp, O.ray_trace(Go, omods, 1, stopping_power=True)) < 1e-5
         assert rel_l2(sp, z[f"{name}_sp_{i}"]) < 1e-5

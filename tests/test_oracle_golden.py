@@ -284,6 +284,12 @@ def test_voxelize_matches_reference_exactly():
     O.scale_solids(solids, 1.25, 0.8, 1.1)
     f = O.voxelize(solids, np.full((nz, ny, nx), 0.25, np.float32), vw, vh, x0, y0, z0, 1)
     assert np.array_equal(f, z["f_scaled"])
+    # rotated cylinders, cones and boxes, clipping on y and z, 5 sub-samples
+    from make_golden import PHANTOM2
+    solids2 = [O.make_solid(*p) for p in PHANTOM2]
+    for os_ in (1, 5):
+        f = O.voxelize(solids2, np.zeros((nz, ny, nx), np.float32), vw, vh, x0, y0, z0, os_)
+        assert np.array_equal(f, z[f"f2_os{os_}"])
     # every solid type leaves a mark
     assert len(np.unique(z["f_os1"])) >= 10
 
@@ -306,3 +312,7 @@ def test_ray_trace_matches_reference(name):
         for os_ in (1, 3):
             assert rel_l2(O.ray_trace(G, solids, os_), z[f"{name}_rt{os_}_{i}"]) < 1e-6
         assert rel_l2(O.ray_trace(G, mods, 1, stopping_power=True), z[f"{name}_sp_{i}"]) < 1e-6
+        # rotated cylinders, cones and boxes, clipped solids
+        from make_golden import PHANTOM2
+        solids2 = [O.make_solid(*q) for q in PHANTOM2]
+        assert rel_l2(O.ray_trace(G, solids2, 1), z[f"{name}_rt2_{i}"]) < 1e-6
