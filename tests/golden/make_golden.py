@@ -491,6 +491,41 @@ def run_raytrace(ref, out):
     print("wrote raytrace", {k: float(v.sum()) for k, v in rec.items() if "_rt" in k or "_sp" in k})
 
 
+def run_demo(ref, out):
+    """The reference's geometry demo (demo/d01_set_geometry.py): six
+    planograms at psi = 0, 30, ..., 150 degrees (D 180, L 192, H 144, T 2,
+    v_m0 = v_m1 = tan 15 degrees), the default volume, two ellipsoids traced
+    analytically and reconstructed by FBP.  CUDA code in the reference, so
+    this case needs a GPU; the FBP volume is recorded."""
+    t15 = float(np.tan(np.radians(15.0)))
+    plans = [(n * 30.0, 180.0, 192.0, 144.0, 2.0, t15, t15) for n in range(6)]
+    m = ref.L.create_new_model()
+    ref.L.set_model(m)
+    for psi, D, L_, H, T, vm0, vm1 in plans:
+        if not ref.L.add_planogram(psi, D, L_, H, vm0, vm1, T):
+            raise RuntimeError("add_planogram failed")
+    ref.L.set_default_volume.argtypes = [ctypes.c_float]
+    ref.L.set_default_volume.restype = ctypes.c_bool
+    ref.L.set_default_volume(1.0)
+    for n in ("get_numX", "get_numY", "get_numZ"):
+        getattr(ref.L, n).restype = ctypes.c_int
+    ref.L.get_voxelWidth.restype = ctypes.c_float
+    ref.L.get_voxelHeight.restype = ctypes.c_float
+    vol = (ref.L.get_numX(), ref.L.get_numY(), ref.L.get_numZ(), ref.L.get_voxelWidth(), ref.L.get_voxelHeight())
+    ref.L.clear_phantom()
+    _add_solids(ref.L.add_object, [(0, (0.0, 0.0, 0.0), (90.0, 80.0, 70.0), 100.0, None, None),
+                                   (0, (0.0, 0.0, 0.0), (5.0, 5.0, 5.0), 1000.0, None, None)])
+    gs = [np.zeros(sh, np.float32) for sh in ref.shapes()]
+    if not ref.L.ray_trace(ref.pp(gs), 1):
+        raise RuntimeError("reference ray_trace failed")
+    f = np.zeros((vol[2], vol[1], vol[0]), np.float32)
+    if not ref.L.FBP(ref.pp(gs), ptr(f)):
+        raise RuntimeError("reference FBP failed")
+    np.savez_compressed(os.path.join(out, "demo_d01.npz"), planograms=np.array(plans), volume=np.array(vol), f=f,
+                        g_sums=np.array([g.sum(dtype=np.float64) for g in gs]))
+    print("wrote demo", vol, float(f.sum()))
+
+
 def run_solid_angle(ref, out):
     """Solid-angle correction (CPU code, src/planogram.cpp:262-302) of all-ones
     planograms: the output is the per-projection factor, recorded as a table
@@ -596,7 +631,7 @@ def main():
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--cpu-only", action="store_true")
     ap.add_argument("--only", nargs="*", default=None,
-                    help="run only these cases (cpu, binning, solid_angle, voxelize, corrections, raytrace, "
+                    help="run only these cases (cpu, binning, solid_angle, voxelize, corrections, raytrace, demo, "
                          "projectors, pfdr_fbp, mlem, regularizers)")
     ap.add_argument("--lib", default=REF_LIB)
     a = ap.parse_args()
@@ -604,7 +639,7 @@ def main():
     ref = Ref(a.lib)
     runs = [("cpu", run_cpu, False), ("binning", run_binning, False), ("solid_angle", run_solid_angle, False),
             ("voxelize", run_voxelize, False), ("corrections", run_corrections, True),
-            ("raytrace", run_raytrace, True), ("projectors", run_projectors, True),
+            ("raytrace", run_raytrace, True), ("demo", run_demo, True), ("projectors", run_projectors, True),
             ("pfdr_fbp", run_pfdr_fbp, True), ("mlem", run_mlem, True), ("regularizers", run_regularizers, True)]
     for name, fn, gpu in runs:
         if (a.only is None or name in a.only) and not (gpu and a.cpu_only):
