@@ -60,6 +60,11 @@ int petl_optimal_fft_size(int N);
 /* The currently selected model's planogram `which` (and its volume, when the
  * volume is defined) as set through the petl.h setters. */
 int petl_model_geometry(int which, petl_geom* out);
+/* The solids of the selected model's phantom (modules == 0) or detector-module
+ * model (modules != 0): copies up to capacity of them into out (may be null)
+ * and returns how many there are.  The struct is declared below. */
+struct petl_solid;
+int petl_model_solids(int modules, struct petl_solid* out, int capacity);
 
 /* Kernel dispatch for the projectors: 0 (default) uses the shear-warp
  * kernels for axis-aligned, equal-pitch geometries (TMA-staged where the

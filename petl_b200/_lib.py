@@ -80,6 +80,7 @@ _DEV_API = [
     ("petl_geom_set_volume", c_i, [_G, c_i, c_i, c_i, c_f, c_f, c_f, c_f, c_f]),
     ("petl_optimal_fft_size", c_i, [c_i]),
     ("petl_model_geometry", c_i, [c_i, _G]),
+    ("petl_model_solids", c_i, [c_i, ctypes.POINTER(petl_solid), c_i]),
     ("petl_set_dispatch", c_i, [c_i]),
     ("petl_device_error_flag", c_i, []),
     ("petl_last_projector_path", c_i, []),

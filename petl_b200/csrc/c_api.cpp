@@ -441,6 +441,14 @@ int petl_model_geometry(int which, petl_geom* out)
     return 0;
 }
 
+int petl_model_solids(int modules, petl_solid* out, int capacity)
+{
+    const Model* m = tomo();
+    const std::vector<petl_solid>& v = modules ? m->modules : m->phantom;
+    for (int i = 0; out && i < capacity && i < int(v.size()); i++) out[i] = v[size_t(i)];
+    return int(v.size());
+}
+
 bool remove_planogram(int which)
 {
     auto& v = tomo()->params.plans;

@@ -379,10 +379,9 @@ class PETLserver:
         solid-angle model, divided by exp(P mu) when mu is given
         (src/petl_server.py:578-605)."""
         if oversampling > 0:
-            self.response = self.stopping_power(self.response, oversampling=oversampling)
+            self.response = self._device_response(oversampling)
         else:
-            self.response = None
-        self.response = self.apply_solid_angle_model(self.response)
+            self.response = self.apply_solid_angle_model(None)
         if mu is not None:
             Pmu = self.allocate_projections()
             self.project(Pmu, mu)
@@ -390,6 +389,26 @@ class PETLserver:
                 np.exp(a, out=a)
             self.divide(self.response, Pmu)
         return self.response
+
+    def _device_response(self, oversampling):
+        """The stopping power of the module model (1 without modules), the
+        0.6571-bin Gaussian and the solid-angle model, composed on the GPU
+        with the same kernels as the host-array calls and copied back once."""
+        from . import ops
+        from ._lib import petl_solid
+        self.set_model()
+        geoms = self.geometries_from_model()
+        n = lib().petl_model_solids(1, None, 0)
+        if n > 0:
+            arr = (petl_solid * n)()
+            lib().petl_model_solids(1, arr, n)
+            R = ops.ray_trace(geoms, list(arr), oversampling=oversampling, stopping_power=True)
+        else:
+            R = [torch.ones(G.shape, device="cuda", dtype=torch.float32) for G in geoms]
+        for r in R:
+            ops.gaussian_filter_(r.view(r.shape[0] * r.shape[1], r.shape[2], r.shape[3]), 0.6571, 2)
+        ops.solid_angle_(geoms, R, inverse=True)
+        return [r.cpu().numpy() for r in R]
 
     def apply_corrections(self, g, oversampling=1, mu=None):
         """g = g / response with the bad-pixel median in-fill (threshold 0.75

@@ -189,3 +189,27 @@ def test_reference_geometry_demo_end_to_end(cuda):
     f = s.allocate_volume()
     s.FBP(g, f)
     assert rel_l2(f, z["f"]) < 5e-4
+
+
+def test_calc_response_device_composition_equals_host_calls(cuda):
+    """calc_response composes the stopping power, the Gaussian and the
+    solid-angle model on the GPU; it must equal the same three steps through
+    the C ABI on host arrays bit for bit, with and without modules."""
+    from petl_b200 import PETLserver
+    from petl_b200.server import _pp
+    z, plans, vol, _, _ = _case("gpetx")
+    s = PETLserver()
+    for p in plans:
+        s.add_planogram(*p)
+    for with_modules in (False, True):
+        if with_modules:
+            _, D, L_, H, _, _, _ = plans[0]
+            for _, c, r, v, _, _ in _modules(D, L_, H):
+                s.add_module(c, r, v)
+        R = s.calc_response(oversampling=3)
+        g = s.allocate_projections()
+        assert s.libprojectors.stopping_power(_pp(g), 3)
+        s.gaussian_filter(g, 0.6571)
+        s.apply_solid_angle_model(g)
+        for a, b in zip(R, g):
+            assert np.array_equal(a, b)
