@@ -170,6 +170,216 @@ bool cuda_ok(const char* what, cudaError_t e)
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Host <-> device copies of caller arrays.  Pinned (page-locked) host memory
+// is copied directly and asynchronously.  Pageable memory -- a plain numpy
+// array, what the reference binding passes -- moves through a ring of four
+// 32 MB pinned buffers per device: the DMA of one buffer overlaps the
+// multi-threaded host copy of another (the driver's own pageable copies run
+// at 11-20 GB/s on this class of machine; page-locking the caller's array for
+// one call costs more than it saves).  Staged copies return once the host
+// side is done: device to host, the data is in the caller's array; host to
+// device, the caller's array has been read and the DMAs are queued on the
+// stream.
+// ---------------------------------------------------------------------------
+constexpr int kRingSlots = 4;
+constexpr size_t kRingBytes = size_t(32) << 20;
+
+struct Ring {
+    std::mutex mu;
+    char* buf[kRingSlots] = {};
+    cudaEvent_t ev[kRingSlots] = {};
+    int next = 0;
+    bool ready = false;
+};
+
+Ring* ring_for_device()
+{
+    static Ring rings[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    return &rings[dev];
+}
+
+bool ring_init(Ring& r)
+{
+    if (r.ready) return true;
+    for (int k = 0; k < kRingSlots; k++) {
+        if (cudaHostAlloc(reinterpret_cast<void**>(&r.buf[k]), kRingBytes, cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&r.ev[k], cudaEventDisableTiming) != cudaSuccess)
+            return false;
+    }
+    r.ready = true;
+    return true;
+}
+
+bool host_pinned(const void* p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // an unknown pointer: pageable
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
+// Many host copies at once: one parallel region over blocks of up to 1 MB of
+// all of them.
+struct CopyJob {
+    char* dst;
+    const char* src;
+    size_t bytes;
+};
+
+void par_memcpy(const std::vector<CopyJob>& jobs)
+{
+    const size_t block = size_t(1) << 20;
+    std::vector<CopyJob> blocks;
+    for (const CopyJob& j : jobs)
+        for (size_t o = 0; o < j.bytes; o += block) blocks.push_back({j.dst + o, j.src + o, std::min(block, j.bytes - o)});
+    const long long nb = (long long)blocks.size();
+#pragma omp parallel for schedule(static)
+    for (long long b = 0; b < nb; b++) std::memcpy(blocks[size_t(b)].dst, blocks[size_t(b)].src, blocks[size_t(b)].bytes);
+}
+
+// A strided block: rows of `width` bytes, `height` of them, at pitches
+// hpitch (host) and dpitch (device).
+struct Block {
+    char* host;
+    char* dev;
+    size_t hpitch, dpitch, width, height;
+};
+
+// Pieces of the block that fit in ring slots, in order: (row, offset, bytes).
+template <class F>
+void for_pieces(const Block& b, F f)
+{
+    for (size_t y = 0; y < b.height; y++)
+        for (size_t o = 0; o < b.width; o += kRingBytes) f(y, o, std::min(kRingBytes, b.width - o));
+}
+
+cudaError_t staged_d2h(const Block& b, cudaStream_t st)
+{
+    Ring* r = ring_for_device();
+    if (!r) return cudaErrorNoDevice;
+    std::lock_guard<std::mutex> lk(r->mu);
+    if (!ring_init(*r)) return cudaErrorMemoryAllocation;
+    struct Piece {
+        char* host;
+        size_t off, bytes;
+    };
+    std::vector<Piece> batch[kRingSlots];
+    std::vector<int> queue;  // slots with copies in flight, oldest first
+    size_t fill = 0;
+    int slot = r->next;
+    auto consume = [&](int k) -> cudaError_t {
+        const cudaError_t e = cudaEventSynchronize(r->ev[k]);
+        if (e != cudaSuccess) return e;
+        std::vector<CopyJob> jobs;
+        for (const Piece& pc : batch[k]) jobs.push_back({pc.host, r->buf[k] + pc.off, pc.bytes});
+        par_memcpy(jobs);
+        batch[k].clear();
+        return cudaSuccess;
+    };
+    auto close = [&]() -> cudaError_t {
+        if (batch[slot].empty()) return cudaSuccess;
+        cudaError_t e = cudaEventRecord(r->ev[slot], st);
+        if (e != cudaSuccess) return e;
+        queue.push_back(slot);
+        slot = (slot + 1) % kRingSlots;
+        fill = 0;
+        if (int(queue.size()) == kRingSlots) {  // the next slot is the oldest: empty it
+            e = consume(queue.front());
+            queue.erase(queue.begin());
+        }
+        return e;
+    };
+    cudaError_t e = cudaSuccess;
+    for_pieces(b, [&](size_t y, size_t o, size_t n) {
+        if (e != cudaSuccess) return;
+        if (fill + n > kRingBytes) e = close();
+        if (e != cudaSuccess) return;
+        e = cudaMemcpyAsync(r->buf[slot] + fill, b.dev + y * b.dpitch + o, n, cudaMemcpyDeviceToHost, st);
+        batch[slot].push_back({b.host + y * b.hpitch + o, fill, n});
+        fill += n;
+    });
+    if (e == cudaSuccess) e = close();
+    for (int k : queue) {
+        const cudaError_t e2 = consume(k);
+        if (e == cudaSuccess) e = e2;
+    }
+    r->next = slot;
+    return e;
+}
+
+cudaError_t staged_h2d(const Block& b, cudaStream_t st)
+{
+    Ring* r = ring_for_device();
+    if (!r) return cudaErrorNoDevice;
+    std::lock_guard<std::mutex> lk(r->mu);
+    if (!ring_init(*r)) return cudaErrorMemoryAllocation;
+    struct Piece {
+        const char* host;
+        char* dev;
+        size_t off, bytes;
+    };
+    std::vector<Piece> batch;
+    size_t fill = 0;
+    int slot = r->next;
+    cudaError_t e = cudaSuccess;
+    auto flush = [&]() {
+        if (batch.empty() || e != cudaSuccess) return;
+        // the slot's previous copies have left it
+        e = cudaEventSynchronize(r->ev[slot]);
+        std::vector<CopyJob> jobs;
+        for (const Piece& pc : batch) jobs.push_back({r->buf[slot] + pc.off, pc.host, pc.bytes});
+        par_memcpy(jobs);
+        for (const Piece& pc : batch)
+            if (e == cudaSuccess) e = cudaMemcpyAsync(pc.dev, r->buf[slot] + pc.off, pc.bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaEventRecord(r->ev[slot], st);
+        batch.clear();
+        fill = 0;
+        slot = (slot + 1) % kRingSlots;
+    };
+    for_pieces(b, [&](size_t y, size_t o, size_t n) {
+        if (fill + n > kRingBytes) flush();
+        batch.push_back({b.host + y * b.hpitch + o, b.dev + y * b.dpitch + o, fill, n});
+        fill += n;
+    });
+    flush();
+    r->next = slot;
+    return e;
+}
+
+// cudaMemcpy2DAsync / cudaMemcpyAsync between a caller's host array and the
+// device, staged when the host array is pageable.
+cudaError_t copy_d2h_2d(void* host, size_t hpitch, const void* dev, size_t dpitch, size_t width, size_t height,
+                        cudaStream_t st)
+{
+    if (host_pinned(host))
+        return cudaMemcpy2DAsync(host, hpitch, dev, dpitch, width, height, cudaMemcpyDeviceToHost, st);
+    return staged_d2h(Block{static_cast<char*>(host), const_cast<char*>(static_cast<const char*>(dev)), hpitch,
+                            dpitch, width, height},
+                      st);
+}
+cudaError_t copy_h2d_2d(void* dev, size_t dpitch, const void* host, size_t hpitch, size_t width, size_t height,
+                        cudaStream_t st)
+{
+    if (host_pinned(host))
+        return cudaMemcpy2DAsync(dev, dpitch, host, hpitch, width, height, cudaMemcpyHostToDevice, st);
+    return staged_h2d(Block{const_cast<char*>(static_cast<const char*>(host)), static_cast<char*>(dev), hpitch,
+                            dpitch, width, height},
+                      st);
+}
+cudaError_t copy_d2h(void* host, const void* dev, size_t bytes, cudaStream_t st)
+{
+    return copy_d2h_2d(host, bytes, dev, bytes, bytes, 1, st);
+}
+cudaError_t copy_h2d(void* dev, const void* host, size_t bytes, cudaStream_t st)
+{
+    return copy_h2d_2d(dev, bytes, host, bytes, bytes, 1, st);
+}
+
 // Scoped device allocation from the stream-ordered pool.
 struct DevBuf {
     void* p = nullptr;
@@ -194,6 +404,9 @@ constexpr int kChunkViews = 16;
 // and device (a strided block: one row of views per slope), on `copy`,
 // ordered after the work enqueued so far on `compute` (device to host) or
 // followed by a wait of `compute` (host to device).
+// A pageable destination is copied one chunk late (staged copies block the
+// host until the data is in place, so the chunk after it must already be
+// queued on the device); flush() copies what is left.
 struct ViewCopy {
     petl_geom G;
     float* host;
@@ -201,6 +414,18 @@ struct ViewCopy {
     cudaStream_t compute, copy;
     bool to_host;
     bool ok = true;
+    bool pinned = true;
+    std::vector<std::pair<int, int>> pending;  // chunks (vi0, nvc) not yet copied to a pageable host array
+    void d2h(int vi0, int nvc)
+    {
+        const size_t vb = size_t(G.N_u1) * G.N_u0 * 4, pitch = vb * G.N_v0, off = (size_t(vi0) * vb) / 4;
+        ok = ok && cuda_ok("project D2H", copy_d2h_2d(host + off, pitch, dev + off, pitch, vb * nvc, G.N_v1, copy));
+    }
+    void flush()
+    {
+        for (const auto& pc : pending) d2h(pc.first, pc.second);
+        pending.clear();
+    }
     static void run(void* ctx, int vi0, int nvc)
     {
         ViewCopy& c = *static_cast<ViewCopy*>(ctx);
@@ -208,15 +433,18 @@ struct ViewCopy {
         cudaEvent_t ev;
         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (c.to_host) {
+            // the previous chunk first: the copy stream already follows its
+            // compute, and not yet this chunk's
+            if (!c.pinned) c.flush();
             cudaEventRecord(ev, c.compute);
             cudaStreamWaitEvent(c.copy, ev, 0);
-            c.ok = c.ok && cuda_ok("project D2H", cudaMemcpy2DAsync(c.host + off, pitch, c.dev + off, pitch,
-                                                                    vb * nvc, c.G.N_v1, cudaMemcpyDeviceToHost,
-                                                                    c.copy));
+            if (c.pinned)
+                c.d2h(vi0, nvc);
+            else
+                c.pending.push_back({vi0, nvc});
         } else {
-            c.ok = c.ok && cuda_ok("backproject H2D", cudaMemcpy2DAsync(c.dev + off, pitch, c.host + off, pitch,
-                                                                        vb * nvc, c.G.N_v1, cudaMemcpyHostToDevice,
-                                                                        c.copy));
+            c.ok = c.ok && cuda_ok("backproject H2D", copy_h2d_2d(c.dev + off, pitch, c.host + off, pitch, vb * nvc,
+                                                                  c.G.N_v1, c.copy));
             cudaEventRecord(ev, c.copy);
             cudaStreamWaitEvent(c.compute, ev, 0);
         }
@@ -296,17 +524,15 @@ bool stream_planograms(const Params& P, float** g, float** r, const char* what, 
         for (int b = 0; b < G.N_v1 && ok; b += step) {
             const int e = std::min(G.N_v1, b + step);
             const size_t off = size_t(b) * slab, bytes = size_t(e - b) * slab * 4;
-            ok = cuda_ok(what, cudaMemcpyAsync(dg.f() + off, g[i] + off, bytes, cudaMemcpyHostToDevice, c->copy));
-            if (r) ok = ok && cuda_ok(what, cudaMemcpyAsync(dr.f() + off, r[i] + off, bytes, cudaMemcpyHostToDevice,
-                                                            c->copy));
+            ok = cuda_ok(what, copy_h2d(dg.f() + off, g[i] + off, bytes, c->copy));
+            if (r) ok = ok && cuda_ok(what, copy_h2d(dr.f() + off, r[i] + off, bytes, c->copy));
             cudaEvent_t ev;
             cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
             cudaEventRecord(ev, c->copy);
             cudaStreamWaitEvent(c->compute, ev, 0);
             cudaEventDestroy(ev);
             ok = ok && report(what, op(G, dg.f(), r ? dr.f() : nullptr, b, e, c->compute));
-            ok = ok && cuda_ok(what, cudaMemcpyAsync(g[i] + off, dg.f() + off, bytes, cudaMemcpyDeviceToHost,
-                                                     c->compute));
+            ok = ok && cuda_ok(what, copy_d2h(g[i] + off, dg.f() + off, bytes, c->compute));
         }
     }
     ok = cuda_ok(what, cudaStreamSynchronize(c->copy)) && ok;
@@ -547,7 +773,7 @@ bool bin(float** g, char* file_name)
     for (size_t i = 0; i < P.plans.size() && ok; i++) {
         const petl_geom& G = P.plans[i];
         const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
-        ok = cuda_ok("bin D2H", cudaMemcpyAsync(g[i], dg[i], n * 4, cudaMemcpyDeviceToHost, c->compute));
+        ok = cuda_ok("bin D2H", copy_d2h(g[i], dg[i], n * 4, c->compute));
     }
     ok = cuda_ok("bin sync", cudaStreamSynchronize(c->compute)) && ok;
     return ok;
@@ -609,11 +835,11 @@ bool voxelize(float* f, int oversampling)
     const size_t n = P.volElems();
     DevBuf df;
     if (!df.alloc(n * 4, c->compute)) return cuda_ok("voxelize alloc", cudaGetLastError());
-    bool ok = cuda_ok("voxelize H2D", cudaMemcpyAsync(df.f(), f, n * 4, cudaMemcpyHostToDevice, c->compute));
+    bool ok = cuda_ok("voxelize H2D", copy_h2d(df.f(), f, n * 4, c->compute));
     ok = ok && report("voxelize", petl_voxelize_dev(solids.data(), int(solids.size()), df.f(), P.numX, P.numY,
                                                     P.numZ, P.voxelWidth, P.voxelHeight, Gv.x_0, Gv.y_0, Gv.z_0,
                                                     oversampling, c->compute));
-    ok = ok && cuda_ok("voxelize D2H", cudaMemcpyAsync(f, df.f(), n * 4, cudaMemcpyDeviceToHost, c->compute));
+    ok = ok && cuda_ok("voxelize D2H", copy_d2h(f, df.f(), n * 4, c->compute));
     return cuda_ok("voxelize sync", cudaStreamSynchronize(c->compute)) && ok;
 }
 
@@ -641,7 +867,7 @@ static bool trace_planograms(float** g, int oversampling, bool stopping, const c
         if (!dg.alloc(n * 4, c->compute)) return cuda_ok(what, cudaGetLastError());
         ok = report(what, petl_ray_trace_dev(&G, solids.data(), int(solids.size()), dg.f(), oversampling,
                                              stopping ? 1 : 0, c->compute));
-        ok = ok && cuda_ok(what, cudaMemcpyAsync(g[i], dg.f(), n * 4, cudaMemcpyDeviceToHost, c->compute));
+        ok = ok && cuda_ok(what, copy_d2h(g[i], dg.f(), n * 4, c->compute));
     }
     return cuda_ok(what, cudaStreamSynchronize(c->compute)) && ok;
 }
@@ -692,7 +918,7 @@ bool project(float** g, float* f)
     if (!c) return cuda_ok("project", cudaErrorNoDevice);
     DevBuf df;
     if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
-    if (!cuda_ok("project H2D", cudaMemcpyAsync(df.f(), f, P.volElems() * 4, cudaMemcpyHostToDevice, c->compute)))
+    if (!cuda_ok("project H2D", copy_h2d(df.f(), f, P.volElems() * 4, c->compute)))
         return false;
     bool ok = true;
     for (size_t i = 0; i < P.plans.size() && ok; i++) {
@@ -702,8 +928,10 @@ bool project(float** g, float* f)
         if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
         // split kernels: each chunk of views goes back while the next computes
         ViewCopy vc{G, g[i], dg.f(), c->compute, c->copy, true};
+        vc.pinned = host_pinned(g[i]);
         const petl::shear::ChunkHook hook{&ViewCopy::run, &vc};
         const int rc = petl::shear::project_chunked(G, df.f(), dg.f(), kChunkViews, hook, c->compute);
+        vc.flush();
         const bool split = rc != petl::shear::kNotApplicable;
         if (split) ok = report("project", rc) && vc.ok;
         const int step = slab_step(G);
@@ -715,9 +943,8 @@ bool project(float** g, float* f)
             cudaEventRecord(ev, c->compute);
             cudaStreamWaitEvent(c->copy, ev, 0);
             cudaEventDestroy(ev);
-            ok = ok && cuda_ok("project D2H", cudaMemcpyAsync(g[i] + size_t(b) * slab, dg.f() + size_t(b) * slab,
-                                                              size_t(e - b) * slab * 4, cudaMemcpyDeviceToHost,
-                                                              c->copy));
+            ok = ok && cuda_ok("project D2H", copy_d2h(g[i] + size_t(b) * slab, dg.f() + size_t(b) * slab,
+                                                       size_t(e - b) * slab * 4, c->copy));
         }
         // the buffer is released on the compute stream: order it after the copies
         cudaEvent_t done;
@@ -764,8 +991,8 @@ static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weig
         const int step = slab_step(G);
         for (int b = split ? G.N_v1 : 0; b < G.N_v1 && ok; b += step) {
             const int e = std::min(G.N_v1, b + step);
-            ok = cuda_ok("backproject H2D", cudaMemcpyAsync(dg.f() + size_t(b) * slab, g[i] + size_t(b) * slab,
-                                                            size_t(e - b) * slab * 4, cudaMemcpyHostToDevice,
+            ok = cuda_ok("backproject H2D", copy_h2d(dg.f() + size_t(b) * slab, g[i] + size_t(b) * slab,
+                                                     size_t(e - b) * slab * 4,
                                                             c->copy));
             cudaEvent_t ev;
             cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -778,7 +1005,7 @@ static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weig
         }
     }
     ok = ok && cuda_ok("backproject D2H",
-                       cudaMemcpyAsync(f, df.f(), P.volElems() * 4, cudaMemcpyDeviceToHost, c->compute));
+                       copy_d2h(f, df.f(), P.volElems() * 4, c->compute));
     ok = cuda_ok("backproject sync", cudaStreamSynchronize(c->compute)) && ok;
     return ok;
 }
@@ -804,13 +1031,13 @@ bool FBP(float** g, float* f)
         const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
         DevBuf dg;
         if (!dg.alloc(n * 4, c->compute)) return cuda_ok("FBP alloc", cudaGetLastError());
-        ok = cuda_ok("FBP H2D", cudaMemcpyAsync(dg.f(), g[i], n * 4, cudaMemcpyHostToDevice, c->compute));
+        ok = cuda_ok("FBP H2D", copy_h2d(dg.f(), g[i], n * 4, c->compute));
         // already-rebinned data is filtered and weighted in the caller's array,
         // as the reference does (src/petl.cpp:335-349)
         float* host_back = G.N_v1 == 1 ? g[i] : nullptr;
         ok = ok && report("FBP", petl::fbp(G, dg.f(), df.f(), i > 0 ? 1 : 0, c->compute, host_back));
     }
-    ok = ok && cuda_ok("FBP D2H", cudaMemcpyAsync(f, df.f(), P.volElems() * 4, cudaMemcpyDeviceToHost, c->compute));
+    ok = ok && cuda_ok("FBP D2H", copy_d2h(f, df.f(), P.volElems() * 4, c->compute));
     ok = cuda_ok("FBP sync", cudaStreamSynchronize(c->compute)) && ok;
     return ok;
 }
@@ -832,9 +1059,9 @@ bool PFDR(float** g, float** g_reb)
         DevBuf dg, dr;
         if (!dg.alloc(n * 4, c->compute) || !dr.alloc(nr * 4, c->compute))
             return cuda_ok("PFDR alloc", cudaGetLastError());
-        ok = cuda_ok("PFDR H2D", cudaMemcpyAsync(dg.f(), g[i], n * 4, cudaMemcpyHostToDevice, c->compute));
+        ok = cuda_ok("PFDR H2D", copy_h2d(dg.f(), g[i], n * 4, c->compute));
         ok = ok && report("PFDR", petl_pfdr_dev(&G, dg.f(), dr.f(), c->compute));
-        ok = ok && cuda_ok("PFDR D2H", cudaMemcpyAsync(g_reb[i], dr.f(), nr * 4, cudaMemcpyDeviceToHost, c->compute));
+        ok = ok && cuda_ok("PFDR D2H", copy_d2h(g_reb[i], dr.f(), nr * 4, c->compute));
         // PETL::doPFDR rewrites the model's planogram (src/petl.cpp:379-380)
         m->params.plans[i].N_v1 = 1;
         m->params.plans[i].v1_0 = 0.0f;
@@ -924,7 +1151,7 @@ struct Staged {
         }
         if (!buf.alloc(n * 4, st)) return false;
         d = buf.f();
-        return !copy_in || cudaMemcpyAsync(d, p, n * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
+        return !copy_in || copy_h2d(d, p, n * 4, st) == cudaSuccess;
     }
 };
 double read_scalar(double* dptr, cudaStream_t st)
@@ -959,7 +1186,7 @@ bool TV_gradient(float* f, float* Df, int N_1, int N_2, int N_3, float delta, fl
     Staged sf, sd;
     if (!sf.stage(f, n, data_on_cpu, c->compute) || !sd.stage(Df, n, data_on_cpu, c->compute, false)) return false;
     bool ok = report("TV_gradient", petl_tv_gradient_dev(sf.d, sd.d, N_1, N_2, N_3, delta, beta, p, 26, c->compute));
-    if (ok && data_on_cpu) ok = cuda_ok("TV_gradient D2H", cudaMemcpyAsync(Df, sd.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    if (ok && data_on_cpu) ok = cuda_ok("TV_gradient D2H", copy_d2h(Df, sd.d, n * 4, c->compute));
     return cuda_ok("TV_gradient sync", cudaStreamSynchronize(c->compute)) && ok;
 }
 
@@ -1017,7 +1244,7 @@ static bool tv_iterate(float* f, int N_1, int N_2, int N_3, float delta, float b
             ok = report("tv", petl_axpby_dev(sf.d, dd.f(), 1.0f, -step, (long long)n, c->compute));
         }
     }
-    if (ok && data_on_cpu) ok = cuda_ok("tv D2H", cudaMemcpyAsync(f, sf.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    if (ok && data_on_cpu) ok = cuda_ok("tv D2H", copy_d2h(f, sf.d, n * 4, c->compute));
     return cuda_ok("tv sync", cudaStreamSynchronize(c->compute)) && ok;
 }
 
@@ -1043,7 +1270,7 @@ bool relativeDifferences_gradient(float* f, float* Df, int N_1, int N_2, int N_3
     if (!sf.stage(f, n, true, c->compute) || !sd.stage(Df, n, true, c->compute, false)) return false;
     bool ok = report("relativeDifferences_gradient",
                      petl_rd_gradient_dev(sf.d, sd.d, N_1, N_2, N_3, delta, beta, c->compute));
-    ok = ok && cuda_ok("rd D2H", cudaMemcpyAsync(Df, sd.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    ok = ok && cuda_ok("rd D2H", copy_d2h(Df, sd.d, n * 4, c->compute));
     return cuda_ok("rd sync", cudaStreamSynchronize(c->compute)) && ok;
 }
 
@@ -1056,7 +1283,7 @@ bool gaussian_filter(float* f, int N_1, int N_2, int N_3, float FWHM, int numDim
     Staged sf;
     if (!sf.stage(f, n, true, c->compute)) return false;
     bool ok = report("gaussian_filter", petl_gaussian_filter_dev(sf.d, N_1, N_2, N_3, FWHM, numDims, c->compute));
-    ok = ok && cuda_ok("gauss D2H", cudaMemcpyAsync(f, sf.d, n * 4, cudaMemcpyDeviceToHost, c->compute));
+    ok = ok && cuda_ok("gauss D2H", copy_d2h(f, sf.d, n * 4, c->compute));
     return cuda_ok("gauss sync", cudaStreamSynchronize(c->compute)) && ok;
 }
 
