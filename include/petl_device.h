@@ -60,6 +60,13 @@ int petl_optimal_fft_size(int N);
 /* The currently selected model's planogram `which` (and its volume, when the
  * volume is defined) as set through the petl.h setters. */
 int petl_model_geometry(int which, petl_geom* out);
+/* Copies between a host array and device memory on `stream`, returning once
+ * the copy is complete; pageable host arrays are staged through the
+ * library's pinned buffers (much faster than the driver's own pageable
+ * copies), pinned ones copied directly.  0 on success. */
+int petl_copy_to_host(void* host, const void* dev, long long bytes, void* stream);
+int petl_copy_to_device(void* dev, const void* host, long long bytes, void* stream);
+
 /* The solids of the selected model's phantom (modules == 0) or detector-module
  * model (modules != 0): copies up to capacity of them into out (may be null)
  * and returns how many there are.  The struct is declared below. */

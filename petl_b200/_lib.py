@@ -81,6 +81,7 @@ _DEV_API = [
     ("petl_optimal_fft_size", c_i, [c_i]),
     ("petl_model_geometry", c_i, [c_i, _G]),
     ("petl_model_solids", c_i, [c_i, ctypes.POINTER(petl_solid), c_i]),
+    ("petl_copy_to_host", c_i, [c_vp, c_vp, c_ll, c_vp]), ("petl_copy_to_device", c_i, [c_vp, c_vp, c_ll, c_vp]),
     ("petl_set_dispatch", c_i, [c_i]),
     ("petl_device_error_flag", c_i, []),
     ("petl_last_projector_path", c_i, []),

@@ -667,6 +667,24 @@ int petl_model_geometry(int which, petl_geom* out)
     return 0;
 }
 
+int petl_copy_to_host(void* host, const void* dev, long long bytes, void* stream)
+{
+    if (!host || !dev || bytes < 0) return -1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = copy_d2h(host, dev, size_t(bytes), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? 0 : int(e);
+}
+
+int petl_copy_to_device(void* dev, const void* host, long long bytes, void* stream)
+{
+    if (!host || !dev || bytes < 0) return -1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = copy_h2d(dev, host, size_t(bytes), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? 0 : int(e);
+}
+
 int petl_model_solids(int modules, petl_solid* out, int capacity)
 {
     const Model* m = tomo();

@@ -408,7 +408,15 @@ class PETLserver:
         for r in R:
             ops.gaussian_filter_(r.view(r.shape[0] * r.shape[1], r.shape[2], r.shape[3]), 0.6571, 2)
         ops.solid_angle_(geoms, R, inverse=True)
-        return [r.cpu().numpy() for r in R]
+        out = []
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for r in R:
+            h = np.empty(tuple(r.shape), np.float32)
+            if lib().petl_copy_to_host(ctypes.c_void_p(h.ctypes.data), ctypes.c_void_p(r.data_ptr()), h.nbytes,
+                                       st) != 0:
+                raise TypeError("calc_response: copy to the host failed")
+            out.append(h)
+        return out
 
     def apply_corrections(self, g, oversampling=1, mu=None):
         """g = g / response with the bad-pixel median in-fill (threshold 0.75
