@@ -41,6 +41,38 @@ def _pp(arrs):
     return (fp * len(arrs))(*[_fp(a) for a in arrs])
 
 
+def _to_device(a, device="cuda"):
+    """A float32 CUDA tensor with the contents of the host array a (or a
+    itself when it already is one), copied through the library's staged
+    host copies."""
+    if _is_dev(a):
+        return a
+    a = np.ascontiguousarray(a, np.float32)
+    t = torch.empty(a.shape, dtype=torch.float32, device=device)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if a.nbytes and lib().petl_copy_to_device(ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(a.ctypes.data),
+                                              a.nbytes, st) != 0:
+        raise TypeError("copy to the device failed")
+    return t
+
+
+def _to_host_(out, t):
+    """Copies the CUDA tensor t into the host array out (float32, C order)."""
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if out.nbytes and lib().petl_copy_to_host(ctypes.c_void_p(out.ctypes.data), ctypes.c_void_p(t.data_ptr()),
+                                              out.nbytes, st) != 0:
+        raise TypeError("copy to the host failed")
+    return out
+
+
+def _copy_back(f, fd):
+    """The device result fd into the caller's host array f."""
+    if isinstance(f, np.ndarray) and f.dtype == np.float32 and f.flags["C_CONTIGUOUS"]:
+        _to_host_(f, fd.contiguous())
+    else:
+        f[...] = fd.cpu().numpy()
+
+
 def _check_f32(a, name):
     if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]):
         raise TypeError(f"{name} must be a C-contiguous float32 numpy array")
@@ -430,7 +462,7 @@ class PETLserver:
         if _is_dev(g):
             from . import ops
             R = self.response if _is_dev(self.response) else \
-                [torch.from_numpy(np.ascontiguousarray(r, np.float32)).to(g[0].device) for r in self.response]
+                [_to_device(r, g[0].device) for r in self.response]
             ops.apply_corrections_(self.geometries_from_model(), g, R, 0.75)
             return g
         self.set_model()
@@ -580,16 +612,15 @@ class PETLserver:
             raise ValueError("mask is not supported by the device-resident MLEM")
         geoms = self.geometries_from_model()
         dev = torch.device("cuda")
-        gd = [torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(dev) for x in g]
+        gd = [_to_device(x, dev) for x in g]
         if f is None:
             f = self.allocate_volume()
-        fd = torch.from_numpy(np.ascontiguousarray(f, np.float32)).to(dev)
+        fd = _to_device(f, dev)
         R = None
         if self.response is not None:  # MLEM always includes a set response
-            R = [r if _is_dev(r) else torch.from_numpy(np.ascontiguousarray(r, np.float32)).to(dev)
-                 for r in self.response]
+            R = [_to_device(r, dev) for r in self.response]
         fd, _ = recon.osem(geoms, gd, numIter, numSubsets, f=fd, delta=delta, beta=beta, response=R)
-        f[:] = fd.cpu().numpy()
+        _copy_back(f, fd)
         return f
 
     def LS(self, g, f, numIter, preconditioner=None, nonnegativityConstraint=True):
@@ -619,7 +650,7 @@ class PETLserver:
         if not self.all_defined():
             raise ValueError("Error: volume and PET geometry must be defined")
         dev = torch.device("cuda")
-        to_dev = lambda a: a if _is_dev(a) else torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)  # noqa
+        to_dev = lambda a: _to_device(a, dev)  # noqa: E731
         R = [to_dev(r) for r in self.response] if self.response is not None else None
         if W is None:
             Wd = recon.auto_weights([to_dev(x) for x in g])
@@ -643,7 +674,7 @@ class PETLserver:
         if corrected:
             self.multiply(g, self.response)
         if not _is_dev(f):
-            f[:] = fd.cpu().numpy()
+            _copy_back(f, fd)
         return f
 
     def RWLSstepSize(self, f, grad, d, Pd, W, delta, beta, num=None):
