@@ -161,3 +161,42 @@ def test_petx_preset_model():
     # solids are checked on the host: a bad one is refused, good ones accepted
     assert not s.add_object(9, [0, 0, 0], [1, 1, 1], 1.0)
     assert s.add_object("cone_y", [0, 0, 0], [1, 5, 3], 1.0)
+
+
+def test_host_logic_of_the_response_and_phantom_calls():
+    """Behaviour the reference's C ABI defines before any device work: null
+    arguments are refused, the stopping power without a module model is 1
+    everywhere (src/petl.cpp:139-147), solids are validated as
+    geometricObject::init does, simulate_scatter validates and computes
+    nothing (src/petl.cpp:194-202)."""
+    import numpy as np
+    from petl_b200.server import PETLserver, _pp
+    s = PETLserver()
+    L = s.libprojectors
+    assert not L.set_solid_angle_correction(None, False)
+    assert not L.apply_corrections(None, None, 0.75)
+    assert not L.voxelize(None, 1)
+    assert not L.ray_trace(None, 1)
+    s.add_planogram(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)
+    g = s.allocate_projections()
+    for a in g:
+        a[:] = 7.0
+    assert L.stopping_power(_pp(g), 1)
+    assert all(np.all(a == 1.0) for a in g)
+    # the volume is not set: voxelize refuses, scatter refuses
+    f = np.zeros((4, 4, 4), np.float32)
+    assert not L.voxelize(f.ctypes.data_as(type(_pp([f])[0])), 1)
+    c = np.zeros(3, np.float32)
+    assert not s.add_object(8, c, c + 1, 1.0)
+    assert s.add_object(0, c, c + 1, 1.0) and s.scale_phantom(2.0)
+    assert not s.scale_phantom("x")
+    try:
+        s.simulate_scatter(g, f)
+        raised = False
+    except ValueError:
+        raised = True
+    assert raised
+    s.set_volume(4, 4, 4, 1.0)
+    assert s.simulate_scatter(g, f) is g
+    s.clear_phantom()
+    s.clear_modules()
