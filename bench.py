@@ -32,6 +32,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -83,8 +84,8 @@ class Clocks:
 
     def __init__(self, index=0):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_{os.getpid()}.csv"
+        fd, self.path = tempfile.mkstemp(prefix="petl_clocks_", suffix=".csv")
+        os.close(fd)
         self.index = index
 
     def start(self):
@@ -117,6 +118,10 @@ class Clocks:
                     rows.append((float(p[1]), float(p[2]), p[5:9]))
                 except ValueError:
                     pass
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         if not rows:
             return None
         sm = sorted(r[0] for r in rows)

@@ -185,7 +185,13 @@ int petl_backproject_dev(const petl_geom* G, const float* g, float* f, int mode,
  * array, so calls that overlap on the GPU race; each call rewrites the
  * tables it reads, so no clearing is needed.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make that first call before any stream capture. */
+ * device current; make that first call before any stream capture.  With
+ * CUDA's lazy module loading (the default), the first call of this library
+ * on a device -- this one or any other -- loads the library's device code
+ * on that device, which allocates device memory (the 4 MiB array among it):
+ * make one call during set-up, before the code that must not allocate runs.
+ * petl_set_dispatch(1) makes it run the general kernel, which needs no
+ * tables. */
 int petl_project_noalloc_dev(const petl_geom* G, const float* f, float* g, void* stream);
 
 /* Same as petl_project_dev restricted to the v1 slices [iv1_begin, iv1_end). */

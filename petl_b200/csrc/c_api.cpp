@@ -299,6 +299,10 @@ cudaError_t staged_d2h(const Block& b, cudaStream_t st)
         if (e != cudaSuccess) return;
         if (fill + n > kRingBytes) e = close();
         if (e != cudaSuccess) return;
+        // the slot's last user may be an upload on another stream whose DMA
+        // out of the slot is still queued: this stream waits for it
+        if (fill == 0) e = cudaStreamWaitEvent(st, r->ev[slot], 0);
+        if (e != cudaSuccess) return;
         e = cudaMemcpyAsync(r->buf[slot] + fill, b.dev + y * b.dpitch + o, n, cudaMemcpyDeviceToHost, st);
         batch[slot].push_back({b.host + y * b.hpitch + o, fill, n});
         fill += n;

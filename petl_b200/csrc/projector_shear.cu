@@ -564,9 +564,12 @@ extern "C" int petl_project_noalloc_dev(const petl_geom* G, const float* f, floa
     PETL_REQUIRE(G && f && g && geom_valid(G, &why), "project_noalloc: invalid arguments " + why);
     cudaStream_t st = as_stream(stream);
     const ViewRange vr{0, G->N_v1, 0, 1};
-    // geometries outside the shear kernels' domain use the general kernel,
-    // which needs no scratch memory at all
-    if (!shear_eligible(*G)) return launch_project_general(*G, f, g, vr, nullptr, st);
+    // geometries outside the shear kernels' domain (or a forced general
+    // dispatch) use the general kernel, which needs no scratch memory at all
+    if (dispatch_mode() == 1 || !shear_eligible(*G)) {
+        note_path(0);
+        return launch_project_general(*G, f, g, vr, nullptr, st);
+    }
     const size_t need = tables_size(*G);
     if (need > kNoAllocTableBytes) {
         set_error("project_noalloc: this geometry needs " + std::to_string(need) +
@@ -610,5 +613,6 @@ extern "C" int petl_project_noalloc_dev(const petl_geom* G, const float* f, floa
     dim3 grid(unsigned(G->N_v0), ceil_div(G->N_v1, F_V1), unsigned(A.n_colblk) * ceil_div(G->N_u1, F_ROWS));
     k_fwd_shear<<<grid, F_THREADS, smem, st>>>(f, g, nullptr, A);
     PETL_LAUNCH_CHECK("project_noalloc");
+    note_path(1);
     return 0;
 }

@@ -44,8 +44,29 @@ def test_noalloc_projection_matches_allocating_entry_point(cuda):
         got = torch.full(G.shape, -2.0, device=cuda)
         assert L.petl_project_dev(G.ptr, _vp(f), _vp(want), 0, 1, _stream()) == 0
         assert L.petl_project_noalloc_dev(G.ptr, _vp(f), _vp(got), _stream()) == 0, L.petl_last_error()
+        # the shear kernel ran, so its tables went through the fixed array
+        assert L.petl_last_projector_path() == 1
         torch.cuda.synchronize()
         assert rel_l2(got.cpu().numpy(), want.cpu().numpy()) < 1e-5
+
+
+def test_noalloc_projection_follows_forced_general_dispatch(cuda):
+    import torch
+    from petl_b200 import Geometry, lib
+    L = lib()
+    G = Geometry(0.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25, volume=(64, 64, 16, 2.0))
+    f = torch.from_numpy(np.random.default_rng(12).random(G.vol_shape).astype(np.float32)).to(cuda)
+    want = torch.zeros(G.shape, device=cuda)
+    got = torch.zeros(G.shape, device=cuda)
+    assert L.petl_project_dev(G.ptr, _vp(f), _vp(want), 0, 1, _stream()) == 0
+    assert L.petl_set_dispatch(1) == 0
+    try:
+        assert L.petl_project_noalloc_dev(G.ptr, _vp(f), _vp(got), _stream()) == 0, L.petl_last_error()
+        assert L.petl_last_projector_path() == 0
+    finally:
+        L.petl_set_dispatch(0)
+    torch.cuda.synchronize()
+    assert rel_l2(got.cpu().numpy(), want.cpu().numpy()) < 1e-5
 
 
 def test_noalloc_projection_refuses_oversized_tables(cuda):
