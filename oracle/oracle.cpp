@@ -176,13 +176,16 @@ T project_ray(const oracle_geom& G, const T* f, int iv1, int iv0, int iu1, int i
 
 // views iv0 = first, first + step, ...; the other views are set to zero
 template <class T>
-void project(const oracle_geom& G, const T* f, T* g, int nthreads, int first = 0, int step = 1)
+void project(const oracle_geom& G, const T* f, T* g, int nthreads, int first = 0, int step = 1, int v1b = 0,
+             int v1e = -1)
 {
+    // g holds the v1 slices [v1b, v1e) only (all of them by default)
     set_threads(nthreads);
-    const long nview = long(G.N_v1) * G.N_v0;
+    if (v1e < 0) v1e = G.N_v1;
+    const long nview = long(v1e - v1b) * G.N_v0;
 #pragma omp parallel for schedule(dynamic)
     for (long v = 0; v < nview; v++) {
-        const int iv1 = int(v / G.N_v0), iv0 = int(v % G.N_v0);
+        const int iv1 = v1b + int(v / G.N_v0), iv0 = int(v % G.N_v0);
         T* gv = g + size_t(v) * G.N_u1 * G.N_u0;
         const bool in = iv0 >= first && (iv0 - first) % step == 0;
         for (int iu1 = 0; iu1 < G.N_u1; iu1++)
@@ -220,9 +223,13 @@ inline void texaxis(float x, int mode, int& i, double& a)
 
 // only the views iv0 = first, first + step, ... contribute
 template <class T>
-void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthreads, int first = 0, int step = 1)
+void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthreads, int first = 0, int step = 1,
+                 int v1b = 0, int v1e = -1)
 {
+    // g holds the v1 slices [v1b, v1e) only (all of them by default); only
+    // those slices are summed
     set_threads(nthreads);
+    if (v1e < 0) v1e = G.N_v1;
     const T cos_psi = T(G.cos_psi), sin_psi = T(G.sin_psi);
     const T R = T(G.R), H = T(G.H);
     const T Tg_w = T(G.T_v1), Tg_x = T(G.T_v0), Tg_y = T(G.T_u1), Tg_z = T(G.T_u0);
@@ -237,8 +244,8 @@ void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthrea
         for (int ix = 0; ix < G.numX; ix++) {
             const T x = T(ix) * Tf_x + sf_x, y = T(iy) * Tf_y + sf_y, z = T(iz) * Tf_z + sf_z;
             T acc = T(0);
-            for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
-                const T* gs = g + size_t(iv1) * plan_sz;
+            for (int iv1 = v1b; iv1 < v1e; iv1++) {
+                const T* gs = g + size_t(iv1 - v1b) * plan_sz;
                 const T v1 = T(iv1) * Tg_w + sg_w;
                 const T t = y * cos_psi - x * sin_psi;
                 const T u1 = z + v1 * t;
@@ -492,6 +499,14 @@ void oracle_backproject_sub_f64(const oracle_geom* G, const double* g, double* f
     backproject<double>(*G, g, f, 0, n, first, step);
 }
 void oracle_project_f32(const oracle_geom* G, const float* f, float* g, int n) { project<float>(*G, f, g, n); }
+void oracle_project_band_f64(const oracle_geom* G, const double* f, double* g, int v1b, int v1e, int n)
+{
+    project<double>(*G, f, g, n, 0, 1, v1b, v1e);
+}
+void oracle_backproject_band_f64(const oracle_geom* G, const double* g, double* f, int v1b, int v1e, int n)
+{
+    backproject<double>(*G, g, f, 0, n, 0, 1, v1b, v1e);
+}
 void oracle_backproject_f64(const oracle_geom* G, const double* g, double* f, int tm, int n) { backproject<double>(*G, g, f, tm, n); }
 void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int tm, int n) { backproject<float>(*G, g, f, tm, n); }
 

@@ -86,6 +86,8 @@ def lib():
         L.oracle_backproject_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int]
         L.oracle_project_sub_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_backproject_sub_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_project_band_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_backproject_band_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_backproject_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int]
         L.oracle_project_nnz.argtypes = [gp, ctypes.c_int]
         L.oracle_project_nnz.restype = ctypes.c_double
@@ -194,6 +196,27 @@ def backproject(geoms, g, dtype=np.float64, texmode=0, nthreads=0):
             lib().oracle_backproject_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(fi, ctypes.c_double),
                                          int(texmode), nthreads)
         f = fi if f is None else f + fi
+    return f
+
+
+def project_band(G, f, v1_begin, v1_end, nthreads=0):
+    """The v1 slices [v1_begin, v1_end) of P f (FP64): the same rays as
+    ``project`` computes for those slices (src/projectors.cu:11-238)."""
+    fc = _d(f)
+    g = np.zeros((v1_end - v1_begin,) + tuple(G.shape[1:]), np.float64)
+    lib().oracle_project_band_f64(ctypes.byref(G), _ptr(fc, ctypes.c_double), _ptr(g, ctypes.c_double),
+                                  int(v1_begin), int(v1_end), nthreads)
+    return g
+
+
+def backproject_band(G, g_band, v1_begin, v1_end, nthreads=0):
+    """Backprojection of the v1 slices [v1_begin, v1_end) only; g_band holds
+    just those slices (FP64, src/projectors.cu:240-377 summed over the band)."""
+    gc = _d(g_band)
+    assert gc.shape[0] == v1_end - v1_begin
+    f = np.zeros(G.vol_shape, np.float64)
+    lib().oracle_backproject_band_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(f, ctypes.c_double),
+                                      int(v1_begin), int(v1_end), nthreads)
     return f
 
 
@@ -374,6 +397,36 @@ def _shape3(f):
     if f.ndim == 2:
         return (1,) + f.shape
     return f.shape
+
+
+def gaussian_filter(f, fwhm, num_dims=3):
+    """gaussian_filter (src/relative_differences.cu:314-411): for every voxel,
+    the weighted mean over the (2r+1)^d window with indices clamped at the
+    borders and weights exp(-(squared distance to the clamped index)/(2 sigma))
+    (the reference divides by 2 sigma, not 2 sigma^2); sigma = FWHM / (2
+    sqrt(2 ln 2)), r = ceil(sqrt(2 ln 10) sigma) in float.  num_dims 1 filters
+    along the first axis, 2 along the last two, 3 along all three.  FP64."""
+    f = np.asarray(f, np.float64)
+    sigma = np.float32(fwhm) / (np.float32(2.0) * np.sqrt(np.float32(2.0) * np.log(np.float32(2.0))))
+    r = int(np.ceil(np.sqrt(np.float32(2.0) * np.log(np.float32(10.0))) * sigma))
+    denom = 1.0 / (2.0 * float(sigma))
+    axes = {1: (0,), 2: (1, 2)}.get(num_dims, (0, 1, 2))
+    n = f.shape
+    grids = np.meshgrid(*[np.arange(m) for m in n], indexing="ij")
+    val = np.zeros_like(f)
+    wsum = np.zeros_like(f)
+    import itertools
+    for offs in itertools.product(range(-r, r + 1), repeat=len(axes)):
+        idx = list(grids)
+        dist = np.zeros_like(f)
+        for a, d in zip(axes, offs):
+            sh = np.clip(grids[a] + d, 0, n[a] - 1)
+            idx[a] = sh
+            dist += (grids[a] - sh).astype(np.float64) ** 2
+        w = np.exp(-denom * dist)
+        val += w * f[tuple(idx)]
+        wsum += w
+    return val / wsum
 
 
 def rd_gradient(f, delta, beta, nthreads=0):

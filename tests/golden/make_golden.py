@@ -78,6 +78,8 @@ class Ref:
         L.diffuse.restype = c_b
         L.TV_denoise.argtypes = [fp, c_i, c_i, c_i, c_f, c_f, c_f, c_i, c_b, c_b]
         L.TV_denoise.restype = c_b
+        L.gaussian_filter.argtypes = [fp, c_i, c_i, c_i, c_f, c_i]
+        L.gaussian_filter.restype = c_b
         L.bin.argtypes = [ctypes.POINTER(fp), ctypes.c_char_p]
         L.bin.restype = c_b
         for n in ("add_object", "add_module"):
@@ -119,16 +121,34 @@ class Ref:
 
     @staticmethod
     def pp(arrs):
+        """float** over the arrays; the returned object keeps them alive (a
+        pointer taken from a temporary array would dangle once the array is
+        freed, and large arrays are unmapped when freed)."""
+        arrs = list(arrs)
         a = (fp * len(arrs))(*[x.ctypes.data_as(fp) for x in arrs])
+        a._keep = arrs
         return a
+
+    @staticmethod
+    def check_device(what):
+        """Stop at the first reference call that left the device in error:
+        the reference prints a failure and carries on (its copies' return
+        values are not checked), so a later call would run on bad pointers."""
+        rt = ctypes.CDLL(os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64", "libcudart.so"))
+        e = rt.cudaDeviceSynchronize()
+        if e == 0:
+            e = rt.cudaGetLastError()
+        if e != 0:
+            raise RuntimeError(f"reference call {what} left CUDA error {e}")
 
 
 def ptr(a):
     return a.ctypes.data_as(fp)
 
 
-def ellipsoids(shape, vox, rng, n, vmin=0.1, vmax=1.0, background=0.0):
-    """Seeded ellipsoid phantom (replace semantics, insertion order)."""
+def ellipsoids(shape, vox, rng, n, vmin=0.1, vmax=1.0, background=0.0, axes=None):
+    """Seeded ellipsoid phantom (replace semantics, insertion order); semi-axes
+    a fraction of the volume, or uniform in `axes` (mm) when given."""
     nz, ny, nx = shape
     wx, wz = vox
     x = (np.arange(nx) - 0.5 * (nx - 1)) * wx
@@ -138,7 +158,10 @@ def ellipsoids(shape, vox, rng, n, vmin=0.1, vmax=1.0, background=0.0):
     f = np.full(shape, background, np.float32)
     ext = np.array([nx * wx, ny * wx, nz * wz]) * 0.5
     for _ in range(n):
-        r = rng.uniform(0.08, 0.3, 3) * ext
+        if axes is None:
+            r = rng.uniform(0.08, 0.3, 3) * ext
+        else:
+            r = np.minimum(rng.uniform(axes[0], axes[1], 3), ext * 0.95)
         c = rng.uniform(-1, 1, 3) * np.maximum(ext - r, 0)
         val = rng.uniform(vmin, vmax)
         inside = ((X - c[0]) / r[0]) ** 2 + ((Y - c[1]) / r[1]) ** 2 + ((Z - c[2]) / r[2]) ** 2 <= 1.0
@@ -626,13 +649,156 @@ def run_corrections(ref, out):
     np.savez_compressed(os.path.join(out, "corrections.npz"), **rec)
 
 
+# The two workloads at their stated sizes: the dual-panel geometry at 2 mm
+# (planogram (33, 65, 64, 128), volume 128x128x64) and at 1 mm (planogram
+# (65, 129, 128, 256), volume 256x256x128).  Outputs are stored for a few
+# views / planes only, so that the fixtures stay small; the inputs are
+# stored whole (piecewise-constant phantoms compress well) or regenerated
+# from seeds and checked by checksum.
+CFG0 = ((0.0, 256.0, 128.0, 128.0, 2.0, 0.5, 0.25), (128, 128, 64, 2.0, 2.0, 0.0, 0.0, 0.0))
+CFG1 = ((0.0, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25), (256, 256, 128, 1.0, 1.0, 0.0, 0.0, 0.0))
+CFG0_VIEWS = ((0, 0), (0, 32), (8, 20), (16, 32), (16, 64), (24, 45), (32, 32), (32, 64))  # (iv1, iv0)
+CFG0_PLANES = (5, 20, 32, 44, 60)
+CFG1_VIEWS = ((0, 64), (20, 10), (32, 64), (64, 128))
+CFG1_PLANES = (20, 64)
+CFG1_REB = (0, 40, 64, 128)
+
+
+def config_phantom(which):
+    """The seeded ellipsoid phantoms of the two workloads: semi-axes 2.5-20 mm
+    (axes 5-40 mm), activities 0.1-1.0; twelve ellipsoids at 2 mm, thirty
+    plus a uniform background of 1 % of the maximum at 1 mm."""
+    plans, vol = (CFG0, CFG1)[which]
+    vshape = (vol[2], vol[1], vol[0])
+    if which == 0:
+        return ellipsoids(vshape, (vol[3], vol[4]), np.random.default_rng(20260), 12, axes=(2.5, 20.0))
+    f = ellipsoids(vshape, (vol[3], vol[4]), np.random.default_rng(20261), 30, axes=(2.5, 20.0))
+    return f + np.float32(0.01) * f.max()
+
+
+def config0_counts(f):
+    """Poisson data of the 2 mm workload: 5e6 expected counts on the FP64
+    oracle projection of the phantom (seeded), float32 counts."""
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    plans, vol = CFG0
+    Go = O.make_geom(*plans, vol)
+    return config0_counts_from(O.project(Go, f)[0])
+
+
+def config0_counts_from(lam):
+    lam = lam * (5e6 / lam.sum())
+    return np.random.default_rng(20262).poisson(lam).astype(np.float32)
+
+
+def counts_crc(g):
+    import zlib
+    return np.int64(zlib.crc32(np.ascontiguousarray(g, np.float32).tobytes()))
+
+
+def run_config0(ref, out):
+    plans, vol = CFG0
+    ref.model([plans], vol)
+    shape = ref.shapes()[0]
+    vshape = (vol[2], vol[1], vol[0])
+    f = config_phantom(0)
+    g = [np.zeros(shape, np.float32)]
+    if not ref.L.project(ref.pp(g), ptr(f)):
+        raise RuntimeError("project failed")
+    ref.check_device("project")
+    counts = config0_counts(f)
+    b = np.zeros(vshape, np.float32)
+    if not ref.L.backproject(ref.pp([counts]), ptr(b)):
+        raise RuntimeError("backproject failed")
+    ref.check_device("backproject")
+    ones = np.ones(shape, np.float32)
+    sens = np.zeros(vshape, np.float32)
+    ref.L.backproject(ref.pp([ones]), ptr(sens))
+    ref.check_device("backproject (sensitivity)")
+    sens[sens == 0.0] = 1.0
+    # PETLserver.MLEM's call sequence (src/petl_server.py:1534-1606), 20 iterations from f = 1
+    x = np.ones(vshape, np.float32)
+    Pd = [np.zeros(shape, np.float32)]
+    d = np.zeros(vshape, np.float32)
+    keep = {}
+    for n in range(20):
+        ref.L.project(ref.pp(Pd), ptr(x))
+        ref.L.rdivide4D(ptr(counts), ptr(Pd[0]), *shape)
+        ref.L.backproject(ref.pp(Pd), ptr(d))
+        ref.L.divide3D(ptr(d), ptr(sens), *vshape)
+        ref.L.multiply3D(ptr(x), ptr(d), *vshape)
+        ref.check_device(f"MLEM iteration {n + 1}")
+        if n + 1 in (1, 20):
+            keep[n + 1] = x[list(CFG0_PLANES)].copy()
+    views = np.array(CFG0_VIEWS)
+    planes = np.array(CFG0_PLANES)
+    np.savez_compressed(os.path.join(out, "config0.npz"), planograms=np.array([plans], np.float64),
+                        volume=np.array(vol, np.float64), shape=np.array(shape), f=f, views=views,
+                        g_views=g[0][views[:, 0], views[:, 1]], counts_sum=np.float64(counts.sum()),
+                        counts_crc=counts_crc(counts), planes=planes, b_planes=b[planes],
+                        sens_planes=sens[planes], mlem1_planes=keep[1], mlem20_planes=keep[20])
+    print("wrote config0", shape)
+
+
+def run_config1(ref, out):
+    plans, vol = CFG1
+    ref.model([plans], vol)
+    shape = ref.shapes()[0]
+    vshape = (vol[2], vol[1], vol[0])
+    f = config_phantom(1)
+    g = [np.zeros(shape, np.float32)]
+    if not ref.L.project(ref.pp(g), ptr(f)):
+        raise RuntimeError("project failed")
+    ref.check_device("project")
+    b = np.zeros(vshape, np.float32)
+    ref.L.backproject(ref.pp(g), ptr(b))
+    ref.check_device("backproject")
+    fbp = np.zeros(vshape, np.float32)
+    if not ref.L.FBP(ref.pp(g), ptr(fbp)):
+        raise RuntimeError("FBP failed")
+    ref.check_device("FBP")
+    greb = [np.zeros(shape[1:], np.float32)]
+    if not ref.L.PFDR(ref.pp(g), ref.pp(greb)):  # rewrites the model to N_v1 = 1: last
+        raise RuntimeError("PFDR failed")
+    ref.check_device("PFDR")
+    views = np.array(CFG1_VIEWS)
+    planes = np.array(CFG1_PLANES)
+    reb = np.array(CFG1_REB)
+    np.savez_compressed(os.path.join(out, "config1.npz"), planograms=np.array([plans], np.float64),
+                        volume=np.array(vol, np.float64), shape=np.array(shape), views=views,
+                        g_views=g[0][views[:, 0], views[:, 1]], planes=planes, b_planes=b[planes],
+                        fbp_planes=fbp[planes], reb_views=reb, greb_views=greb[0][reb])
+    print("wrote config1", shape)
+
+
+def run_gaussian(ref, out):
+    """gaussian_filter (src/relative_differences.cu:314-411,753-800) along 1, 2
+    and 3 dimensions, and the RWLS weight width (FWHM 3) and the response
+    smoothing width (FWHM 0.6571) of the reference's Python layer."""
+    ref.model([GEOMS["g0"][0][0]], GEOMS["g0"][1])
+    rng = np.random.default_rng(5151)
+    rec = {}
+    shape = (9, 14, 23)
+    for numDims in (1, 2, 3):
+        for fwhm in (0.6571, 2.0, 3.0):
+            f = (rng.random(shape) * 3.0).astype(np.float32)
+            out_f = f.copy()
+            if not ref.L.gaussian_filter(ptr(out_f), *shape, fwhm, numDims):
+                raise RuntimeError("gaussian_filter failed")
+            ref.check_device("gaussian_filter")
+            rec[f"in_{numDims}_{fwhm}"] = f
+            rec[f"out_{numDims}_{fwhm}"] = out_f
+    np.savez_compressed(os.path.join(out, "gaussian.npz"), shape=np.array(shape), **rec)
+    print("wrote gaussian")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--cpu-only", action="store_true")
     ap.add_argument("--only", nargs="*", default=None,
                     help="run only these cases (cpu, binning, solid_angle, voxelize, corrections, raytrace, demo, "
-                         "projectors, pfdr_fbp, mlem, regularizers)")
+                         "projectors, pfdr_fbp, mlem, regularizers, config0, config1, gaussian)")
     ap.add_argument("--lib", default=REF_LIB)
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
@@ -640,7 +806,8 @@ def main():
     runs = [("cpu", run_cpu, False), ("binning", run_binning, False), ("solid_angle", run_solid_angle, False),
             ("voxelize", run_voxelize, False), ("corrections", run_corrections, True),
             ("raytrace", run_raytrace, True), ("demo", run_demo, True), ("projectors", run_projectors, True),
-            ("pfdr_fbp", run_pfdr_fbp, True), ("mlem", run_mlem, True), ("regularizers", run_regularizers, True)]
+            ("pfdr_fbp", run_pfdr_fbp, True), ("mlem", run_mlem, True), ("regularizers", run_regularizers, True),
+            ("config0", run_config0, True), ("config1", run_config1, True), ("gaussian", run_gaussian, True)]
     for name, fn, gpu in runs:
         if (a.only is None or name in a.only) and not (gpu and a.cpu_only):
             fn(ref, a.out)

@@ -1,0 +1,259 @@
+"""Parity at the stated workload sizes.
+
+* The dual-panel geometry at 2 mm: planogram (33, 65, 64, 128), volume
+  128x128x64, a 12-ellipsoid phantom, 5e6 Poisson counts.  Forward and
+  backprojection, the adjoint pair, 20 MLEM iterations and 8-subset OSEM are
+  held to the FP64 oracle on the whole problem, and to the reference
+  library's own outputs (golden views and planes from
+  tests/golden/make_golden.py, run against the reference build).
+* The same geometry at 1 mm: planogram (65, 129, 128, 256), volume
+  256x256x128, 30 ellipsoids plus a 1 % background.  The FP64 oracle is
+  too slow for whole projections here, so forward and backprojection are
+  held to it on bands of v1 slices (ends and centre of the slope range) and
+  the full-size results through linearity (the sum of band backprojections
+  is the full backprojection); PFDR and FBP are held to the oracle whole.
+  OSEM (8 subsets, 4 iterations) is held to the oracle on the three central
+  slopes of the same geometry (volume and detector size unchanged), and at
+  full size through its invariants.
+
+Tolerances: 1e-5 relative L2 against the FP64 oracle; against the reference
+5e-4 for backprojection (its texture unit interpolates with 8-bit weights),
+1e-3 for FBP and 2e-3 for MLEM (the same weights, compounded).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import load_golden, rel_l2
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+import make_golden as MG  # noqa: E402  (seeds and phantoms of the golden cases)
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _geoms(cfg):
+    from petl_b200 import Geometry
+    plans, vol = cfg
+    return Geometry(*plans, volume=vol), O.make_geom(*plans, vol)
+
+
+def _no_device_error():
+    from petl_b200 import lib
+    assert lib().petl_device_error_flag() == 0
+
+
+# ----------------------------------------------------------------------------
+# 2 mm workload, whole problem
+# ----------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def cfg0(cuda):
+    z = load_golden("config0.npz")
+    G, Go = _geoms(MG.CFG0)
+    assert tuple(G.shape) == (33, 65, 64, 128) == tuple(z["shape"])
+    f = z["f"]
+    assert np.array_equal(f, MG.config_phantom(0))
+    lam = O.project(Go, f)[0]
+    counts = MG.config0_counts_from(lam)
+    assert MG.counts_crc(counts) == int(z["counts_crc"])
+    return dict(z=z, G=G, Go=Go, f=f, lam=lam, counts=counts)
+
+
+def test_config0_forward(cuda, cfg0):
+    from petl_b200 import lib, ops
+    G, z = cfg0["G"], cfg0["z"]
+    g = _np(ops.project(G, _t(cfg0["f"], cuda)))
+    assert lib().petl_last_projector_path() == 2
+    _no_device_error()
+    assert rel_l2(g, cfg0["lam"]) < 1e-5
+    v = z["views"]
+    assert rel_l2(g[v[:, 0], v[:, 1]], z["g_views"]) < 1e-5
+    for k, (a, b) in enumerate(v):  # view by view, the edge slopes included
+        assert rel_l2(g[a, b], z["g_views"][k]) < 1e-5
+
+
+def test_config0_backprojection(cuda, cfg0):
+    from petl_b200 import lib, ops, recon
+    G, Go, z = cfg0["G"], cfg0["Go"], cfg0["z"]
+    y = _t(cfg0["counts"], cuda)
+    b = _np(ops.backproject(G, y))
+    assert lib().petl_last_projector_path() == 2
+    _no_device_error()
+    assert rel_l2(b, O.backproject(Go, cfg0["counts"])) < 1e-5
+    p = z["planes"]
+    assert rel_l2(b[p], z["b_planes"]) < 5e-4
+    sens = _np(recon.sensitivity(G, [y]))
+    assert rel_l2(sens[p], z["sens_planes"]) < 5e-4
+
+
+def test_config0_adjoint_pair(cuda, cfg0):
+    import torch
+    from petl_b200 import ops
+    G = cfg0["G"]
+    gen = torch.Generator(device=cuda).manual_seed(9)
+    x = torch.rand(G.vol_shape, device=cuda, generator=gen)
+    y = torch.rand(G.shape, device=cuda, generator=gen)
+    lhs = float(torch.sum(ops.project(G, x).double() * y.double()))
+    rhs = float(torch.sum(x.double() * ops.backproject(G, y, mode="adjoint").double()))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def test_config0_mlem_20_iterations(cuda, cfg0):
+    from petl_b200 import recon
+    G, Go, z = cfg0["G"], cfg0["Go"], cfg0["z"]
+    y = _t(cfg0["counts"], cuda)
+    f1, _ = recon.mlem(G, y, 1)
+    p = z["planes"]
+    assert rel_l2(_np(f1)[p], z["mlem1_planes"]) < 5e-4
+    f20, _ = recon.mlem(G, y, 20)
+    _no_device_error()
+    f20 = _np(f20)
+    want = O.mlem(Go, cfg0["counts"], 20)
+    assert rel_l2(f20, want) < 1e-5
+    assert rel_l2(f20[p], z["mlem20_planes"]) < 2e-3
+
+
+def test_config0_osem(cuda, cfg0):
+    from petl_b200 import recon
+    G, Go = cfg0["G"], cfg0["Go"]
+    f, _ = recon.osem(G, _t(cfg0["counts"], cuda), 4, 8)
+    assert rel_l2(_np(f), O.osem(Go, cfg0["counts"], 4, 8)) < 1e-5
+
+
+# ----------------------------------------------------------------------------
+# 1 mm workload: bands of slices against the oracle, the whole through
+# linearity
+# ----------------------------------------------------------------------------
+BANDS = ((0, 2), (31, 34), (63, 65))
+
+
+@pytest.fixture(scope="module")
+def cfg1(cuda):
+    from petl_b200 import ops
+    z = load_golden("config1.npz")
+    G, Go = _geoms(MG.CFG1)
+    assert tuple(G.shape) == (65, 129, 128, 256) == tuple(z["shape"])
+    f = MG.config_phantom(1)
+    ft = _t(f, cuda)
+    g = ops.project(G, ft)
+    return dict(z=z, G=G, Go=Go, f=f, ft=ft, g=g)
+
+
+def test_config1_forward_bands(cuda, cfg1):
+    G, Go, z, g = cfg1["G"], cfg1["Go"], cfg1["z"], cfg1["g"]
+    _no_device_error()
+    for a, b in BANDS:
+        want = O.project_band(Go, cfg1["f"], a, b)
+        assert rel_l2(_np(g[a:b]), want) < 1e-5, (a, b)
+    v = z["views"]
+    got = _np(g[v[:, 0], v[:, 1]])
+    for k in range(len(v)):
+        assert rel_l2(got[k], z["g_views"][k]) < 1e-5
+
+
+def test_config1_backprojection_bands_and_linearity(cuda, cfg1):
+    import torch
+    from petl_b200 import ops
+    G, Go, z, g = cfg1["G"], cfg1["Go"], cfg1["z"], cfg1["g"]
+    full = ops.backproject(G, g)
+    _no_device_error()
+    assert rel_l2(_np(full)[z["planes"]], z["b_planes"]) < 5e-4
+    for a, b in BANDS:
+        part = ops.backproject(G, g, v1_range=(a, b))
+        want = O.backproject_band(Go, _np(g[a:b]), a, b)
+        assert rel_l2(_np(part), want) < 1e-5, (a, b)
+    # the whole as a sum over slabs of slices
+    acc = torch.zeros_like(full)
+    edges = (0, 2, 17, 31, 34, 50, 63, 65)
+    for a, b in zip(edges[:-1], edges[1:]):
+        ops.backproject(G, g, f=acc, v1_range=(a, b), accumulate=True)
+    assert rel_l2(_np(acc), _np(full)) < 1e-6
+    # the adjoint pair at full size
+    gen = torch.Generator(device=cuda).manual_seed(10)
+    y = torch.rand(G.shape, device=cuda, generator=gen)
+    lhs = float(torch.sum(g.double() * y.double()))
+    rhs = float(torch.sum(cfg1["ft"].double() * ops.backproject(G, y, mode="adjoint").double()))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def test_config1_pfdr_fbp(cuda, cfg1):
+    from petl_b200 import ops
+    G, Go, z, g = cfg1["G"], cfg1["Go"], cfg1["z"], cfg1["g"]
+    g_host = _np(g)
+    reb = _np(ops.pfdr(G, g))
+    want = O.pfdr(Go, g_host)
+    assert rel_l2(reb, want) < 1e-5
+    r = z["reb_views"]
+    assert rel_l2(reb[r], z["greb_views"]) < 1e-5
+    f = _np(ops.fbp(G, g))
+    _no_device_error()
+    Gr = O.rebinned_geom(Go)
+    assert rel_l2(f, O.fbp(Gr, want)) < 1e-5
+    assert rel_l2(f[z["planes"]], z["fbp_planes"]) < 1e-3
+
+
+def test_config1_osem_central_slopes(cuda, cfg1):
+    """OSEM 8 x 4 on the three central axial slopes of the 1 mm geometry
+    (volume 256x256x128, planogram (3, 129, 128, 256)) against the oracle."""
+    import torch
+    from petl_b200 import Geometry, ops, recon
+    plans, vol = MG.CFG1
+    sub = plans[:6] + (1.0 / 128.0,)
+    G = Geometry(*sub, volume=vol)
+    Go = O.make_geom(*sub, vol)
+    assert tuple(G.shape) == (3, 129, 128, 256)
+    g = ops.project(G, cfg1["ft"])
+    g *= 2e6 / float(g.sum())
+    counts = torch.poisson(g, generator=torch.Generator(device=cuda).manual_seed(11))
+    f, _ = recon.osem(G, counts, 4, 8)
+    _no_device_error()
+    assert rel_l2(_np(f), O.osem(Go, _np(counts), 4, 8)) < 1e-5
+
+
+def test_config1_pfdr_fbp_osem_chain(cuda, cfg1):
+    """The full 1 mm chain on 5e7 counts: PFDR, FBP, then OSEM 8 x 4 from
+    the (clipped) FBP image.  Every OSEM sub-iteration maps the image
+    through f <- f P_s^T(y / P_s f) / P_s^T 1, so with the exact-adjoint
+    pair, sum_j (P_s^T 1)_j f_j after the last subset step equals the data
+    counted where P_s f > 0 -- checked here on the subset the iteration
+    ended with, together with a log-likelihood that rises each iteration."""
+    import torch
+    from petl_b200 import ops, recon
+    G, g = cfg1["G"], cfg1["g"]
+    lam = g * (5e7 / float(g.sum()))
+    y = torch.poisson(lam, generator=torch.Generator(device=cuda).manual_seed(12))
+    f0 = ops.fbp(G, y).clamp_(min=0.0)
+    assert float(f0.sum()) > 0
+    S = 8
+    sens = [recon.sensitivity(G, [y], subset=(s, S), mode="adjoint") for s in range(S)]
+    f = f0.clone()
+    ll = [recon.loglik(G, y, f)]
+    ratio = torch.empty_like(y)
+    d = torch.empty_like(f)
+    Pf = torch.zeros_like(y)
+    for _ in range(4):
+        for s in range(S):
+            if s == S - 1:  # the data this step sees: its views, where P_s f > 0
+                ops.project(G, f, Pf, subset=(s, S))
+                seen = float(torch.sum(torch.where(Pf[:, s::S] > 0, y[:, s::S], 0.0), dtype=torch.float64))
+            ops.project_ratio(G, f, y, out=ratio, subset=(s, S))
+            ops.backproject(G, ratio, f=d, subset=(s, S), mode="adjoint")
+            ops.mlem_update_(f, d, sens[s])
+        ll.append(recon.loglik(G, y, f))
+        got = float(torch.sum(sens[S - 1].double() * f.double()))
+        assert abs(got - seen) / seen < 1e-4
+    _no_device_error()
+    assert all(b > a for a, b in zip(ll[:-1], ll[1:])), ll
+    assert torch.isfinite(f).all() and float(f.min()) >= 0.0

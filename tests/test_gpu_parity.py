@@ -317,3 +317,22 @@ def test_server_least_squares_family(cuda):
     assert np.array_equal(gg[0], _np(gc) * R)
     want = O.rwls(Go, _np(gc), f0, 3, W=_np(Wd) * R * R)
     assert rel_l2(got, want) < 1e-4
+
+
+@pytest.mark.parametrize("num_dims", [1, 2, 3])
+def test_gaussian_filter_against_reference(cuda, num_dims):
+    """gaussian_filter (src/relative_differences.cu:314-411,753-800) along 1, 2
+    and 3 dimensions at the widths the reference's Python layer uses, on the
+    device path and through the C ABI."""
+    from petl_b200 import PETLserver, ops
+    z = load_golden("gaussian.npz")
+    s = PETLserver()
+    s.add_planogram(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25)
+    for fwhm in (0.6571, 2.0, 3.0):
+        f = z[f"in_{num_dims}_{fwhm}"]
+        want = z[f"out_{num_dims}_{fwhm}"]
+        got = _np(ops.gaussian_filter_(_t(f, cuda), fwhm, num_dims))
+        assert rel_l2(got, want) < 1e-5, fwhm
+        h = f.copy()
+        s.gaussian_filter(h, fwhm, num_dims)
+        assert rel_l2(h, want) < 1e-5, fwhm

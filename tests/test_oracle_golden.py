@@ -333,3 +333,65 @@ def test_geometry_demo_matches_reference():
     for gi, want in zip(g, z["g_sums"]):
         assert abs(gi.sum(dtype=np.float64) / want - 1.0) < 1e-6
     assert rel_l2(O.fbp(geoms, g), z["f"]) < 5e-4
+
+
+def test_gaussian_filter_matches_reference():
+    z = load_golden("gaussian.npz")
+    for nd in (1, 2, 3):
+        for fwhm in (0.6571, 2.0, 3.0):
+            got = O.gaussian_filter(z[f"in_{nd}_{fwhm}"], fwhm, nd)
+            assert rel_l2(got, z[f"out_{nd}_{fwhm}"]) < 1e-6, (nd, fwhm)
+
+
+def _config(name):
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden as MG
+    return MG, load_golden(f"config{name}.npz")
+
+
+def test_config0_oracle_matches_reference():
+    """The 2 mm dual-panel workload at its stated size: planogram
+    (33, 65, 64, 128), volume 128x128x64 (the reference's outputs are stored
+    for a few views and planes)."""
+    MG, z = _config(0)
+    Go = O.make_geom(*MG.CFG0[0], MG.CFG0[1])
+    assert tuple(Go.shape) == tuple(z["shape"]) == (33, 65, 64, 128)
+    f = MG.config_phantom(0)
+    assert np.array_equal(f, z["f"])
+    lam = O.project(Go, f)[0]
+    v = z["views"]
+    assert rel_l2(lam[v[:, 0], v[:, 1]], z["g_views"]) < 2e-6
+    counts = MG.config0_counts_from(lam)
+    assert MG.counts_crc(counts) == int(z["counts_crc"]) and counts.sum() == z["counts_sum"]
+    p = z["planes"]
+    b = O.backproject(Go, counts)
+    assert rel_l2(b[p], z["b_planes"]) < 5e-4
+    f1 = O.mlem(Go, counts, 1)
+    assert rel_l2(f1[p], z["mlem1_planes"]) < 1e-3
+
+
+def test_config1_oracle_matches_reference_on_views():
+    """The 1 mm workload (planogram (65, 129, 128, 256)): the oracle's v1
+    slices of the stored reference views."""
+    MG, z = _config(1)
+    Go = O.make_geom(*MG.CFG1[0], MG.CFG1[1])
+    assert tuple(Go.shape) == tuple(z["shape"]) == (65, 129, 128, 256)
+    f = MG.config_phantom(1)
+    for k, (a, b) in enumerate(z["views"]):
+        g = O.project_band(Go, f, int(a), int(a) + 1)
+        assert rel_l2(g[0, b], z["g_views"][k]) < 1e-5  # FP32 sums over 256 planes in the reference
+
+
+def test_band_projections_are_slices_of_the_whole():
+    Go = O.make_geom(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25, (32, 32, 8, 2.0))
+    rng = np.random.default_rng(3)
+    f = rng.random(Go.vol_shape)
+    g = O.project(Go, f)[0]
+    assert np.array_equal(O.project_band(Go, f, 3, 7), g[3:7])
+    y = rng.random(Go.shape)
+    y2 = y.copy()
+    y2[:3] = 0.0
+    y2[7:] = 0.0
+    assert np.allclose(O.backproject_band(Go, y[3:7], 3, 7), O.backproject(Go, y2), rtol=0, atol=1e-12)
