@@ -21,7 +21,10 @@ the reference publishes no benchmark data set.
   capture; ``fp32`` adds the binding figure, 2*nnz(A) flops per call against
   the nominal FP32 rate at the measured clock.
 * ``cpu_baseline``: the FP32 CPU restatement (oracle) on all host cores, on
-  a bounded sample (a few v1 slices), scaled to a full step.
+  a bounded sample (two v1 slices), extrapolated to a full step.
+* ``reference_gpu``: the reference's own GPU build (its sources compiled
+  for sm_100a) through its C ABI on numpy host arrays, with this library on
+  the same calls beside it (single-GPU runs).
 
 ``--impl reference`` times the reference path's CPU implementation (the
 oracle restatement: the reference has no CPU projector) instead.
@@ -135,30 +138,91 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_baseline(nslices=2, nthreads=0):
-    """FP32 CPU restatement of fwd+back on `nslices` v1 slices, scaled to a step."""
+SAMPLE_SLICES = (16, 48)   # v1 slices timed by the CPU sample (a quarter and three quarters of the range)
+_SAMPLE_PHANTOM = {}
+
+
+def cpu_sample(slices=SAMPLE_SLICES, nthreads=0):
+    """FP32 CPU restatement (oracle) of fwd+back on the given v1 slices of the
+    workload: each slice projected, then backprojected.  Returns the seconds
+    taken and the fraction of one fwd+back pair that the slices are."""
     import oracle as O
     G = O.make_geom(*GEOM_ARGS[:5], GEOM_ARGS[5], GEOM_ARGS[6], VOLUME)
-    full_nv1 = G.N_v1
-    sub = G.copy()
-    # a representative band of v1 slices away from the centre
-    b = full_nv1 // 4
-    sub.N_v1 = nslices
-    sub.v1_0 = float(np.float32(np.float32(G.v1_0) + np.float32(b) * np.float32(G.T_v1)))
-    rng = np.random.default_rng(0)
-    f = phantom(rng)
-    t0 = time.perf_counter()
-    g = O.project(sub, f, dtype=np.float32, nthreads=nthreads)[0]
-    t1 = time.perf_counter()
-    O.backproject(sub, g, dtype=np.float32, nthreads=nthreads)
-    t2 = time.perf_counter()
-    scale = full_nv1 / nslices
-    step_s = (t2 - t0) * scale
+    if "f" not in _SAMPLE_PHANTOM:
+        _SAMPLE_PHANTOM["f"] = phantom(np.random.default_rng(0))
+    f = _SAMPLE_PHANTOM["f"]
+    t_f = t_b = 0.0
+    for a in slices:
+        t0 = time.perf_counter()
+        g = O.project_band(G, f, a, a + 1, nthreads=nthreads, dtype=np.float32)
+        t1 = time.perf_counter()
+        O.backproject_band(G, g, a, a + 1, nthreads=nthreads, dtype=np.float32)
+        t2 = time.perf_counter()
+        t_f += t1 - t0
+        t_b += t2 - t1
+    frac = len(slices) / G.N_v1
     cores = nthreads if nthreads > 0 else (os.cpu_count() or 1)
-    return {"value": 1.0 / step_s, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{nslices} of {full_nv1} v1 slices (fwd {t1 - t0:.2f} s + back {t2 - t1:.2f} s), "
-                      f"scaled x{scale:.1f}; FP32 C++/OpenMP restatement of the reference kernels",
-            "seconds_per_step": step_s}
+    return {"seconds": t_f + t_b, "pairs": frac, "cores": cores,
+            "sample": f"v1 slices {list(slices)} of {G.N_v1} (fwd {t_f:.2f} s + back {t_b:.2f} s) = "
+                      f"{len(slices)}/{G.N_v1} of a fwd+back pair, throughput extrapolated by "
+                      f"x{1 / frac:.1f}; FP32 C++/OpenMP restatement of the reference kernels"}
+
+
+def cpu_baseline(nthreads=0):
+    r = cpu_sample(nthreads=nthreads)
+    return {"value": r["pairs"] / r["seconds"], "unit": UNIT, "cores": r["cores"], "kind": "port",
+            "sample": r["sample"]}
+
+
+def reference_gpu_baseline(f_host, steps=2):
+    """The reference library's own GPU projector and backprojector (its
+    unmodified sources compiled for sm_100a into oracle/_ref/libpetl_ref.so),
+    timed like a reference user calls them: its C ABI on numpy (pageable)
+    host arrays, host<->device copies inside, wall clock per pair after one
+    warm-up pair.  This library's libpetl.so is timed on the same calls and
+    arrays for comparison.  A reported baseline; None without the build."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libpetl_ref.so")
+    if not os.path.exists(path):
+        return None
+    fp = ctypes.POINTER(ctypes.c_float)
+
+    def bind(libpath):
+        L = ctypes.CDLL(libpath)
+        L.create_new_model.restype = ctypes.c_int
+        L.set_model.argtypes = [ctypes.c_int]
+        L.add_planogram.argtypes = [ctypes.c_float] * 7
+        L.add_planogram.restype = ctypes.c_bool
+        L.set_volume.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 5
+        L.set_volume.restype = ctypes.c_bool
+        for n in ("project", "backproject"):
+            getattr(L, n).argtypes = [ctypes.POINTER(fp), fp]
+            getattr(L, n).restype = ctypes.c_bool
+        return L
+
+    psi, D, Lp, H, T, vm0, vm1 = GEOM_ARGS
+    g = np.zeros((65, 129, 128, 256), np.float32)
+    b = np.zeros_like(f_host)
+    gp = (fp * 1)(g.ctypes.data_as(fp))
+    out = {}
+    for name, libpath in (("reference", path), ("petl_b200", os.path.join(ROOT, "petl_b200", "libpetl.so"))):
+        L = bind(libpath)
+        L.set_model(L.create_new_model())
+        if not (L.add_planogram(psi, D, Lp, H, vm0, vm1, T) and L.set_volume(*VOLUME, 1.0, 0.0, 0.0, 0.0)):
+            return None
+        ts = []
+        for k in range(steps + 1):
+            t0 = time.perf_counter()
+            ok = L.project(gp, f_host.ctypes.data_as(fp)) and L.backproject(gp, b.ctypes.data_as(fp))
+            if not ok:
+                return None
+            if k:
+                ts.append(time.perf_counter() - t0)
+        out[name] = {"value": 1.0 / float(np.mean(ts)), "unit": UNIT, "steps": steps}
+    return {"value": out["reference"]["value"], "unit": UNIT, "steps": steps,
+            "host_arrays": "numpy (pageable), as the reference binding passes them",
+            "build": "reference sources unmodified, nvcc -arch=sm_100a --use_fast_math (oracle/Makefile)",
+            "this_library_same_calls": out["petl_b200"]["value"]}
 
 
 def max_over_ranks(x, world, device=None):
@@ -183,19 +247,22 @@ def replica_value(world, steps, total_ms):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
+    # one step = the sampled v1 slices of one fwd+back pair (a bounded sample
+    # of the workload); throughput = pairs sampled / seconds
     t_all = []
     base = None
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(nslices=1)
+        r = cpu_sample()
         if i >= args.warmup:
-            t_all.append(r["seconds_per_step"])
+            t_all.append(r["seconds"])
             base = r
     step = float(np.mean(t_all))
-    val = 1.0 / step
+    val = base["pairs"] / step
     line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "path": "reference CPU restatement (oracle), all host cores"},
+            "config": {"workload": WORKLOAD, "path": "reference CPU restatement (oracle), all host cores",
+                       "step": f"{base['pairs']:.4f} of a fwd+back pair (the sampled v1 slices)"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": base["cores"], "kind": "port",
                              "sample": base["sample"]},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -330,7 +397,9 @@ def main():
                        "d2h_bytes_per_step": nb_g + nb_f, "steps": len(ts),
                        "path": "PETLserver.project + backproject (reference C ABI, pinned host arrays)"}
     if rank == 0 and not args.no_cpu:
-        line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds_per_step"}
+        line["cpu_baseline"] = cpu_baseline()
+        if world == 1:
+            line["reference_gpu"] = reference_gpu_baseline(f_host)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

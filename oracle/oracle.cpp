@@ -507,6 +507,14 @@ void oracle_backproject_band_f64(const oracle_geom* G, const double* g, double* 
 {
     backproject<double>(*G, g, f, 0, n, 0, 1, v1b, v1e);
 }
+void oracle_project_band_f32(const oracle_geom* G, const float* f, float* g, int v1b, int v1e, int n)
+{
+    project<float>(*G, f, g, n, 0, 1, v1b, v1e);
+}
+void oracle_backproject_band_f32(const oracle_geom* G, const float* g, float* f, int v1b, int v1e, int n)
+{
+    backproject<float>(*G, g, f, 0, n, 0, 1, v1b, v1e);
+}
 void oracle_backproject_f64(const oracle_geom* G, const double* g, double* f, int tm, int n) { backproject<double>(*G, g, f, tm, n); }
 void oracle_backproject_f32(const oracle_geom* G, const float* g, float* f, int tm, int n) { backproject<float>(*G, g, f, tm, n); }
 

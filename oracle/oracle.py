@@ -88,6 +88,8 @@ def lib():
         L.oracle_backproject_sub_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_project_band_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_backproject_band_f64.argtypes = [gp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_project_band_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_backproject_band_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_backproject_f32.argtypes = [gp, fp, fp, ctypes.c_int, ctypes.c_int]
         L.oracle_project_nnz.argtypes = [gp, ctypes.c_int]
         L.oracle_project_nnz.restype = ctypes.c_double
@@ -199,21 +201,36 @@ def backproject(geoms, g, dtype=np.float64, texmode=0, nthreads=0):
     return f
 
 
-def project_band(G, f, v1_begin, v1_end, nthreads=0):
-    """The v1 slices [v1_begin, v1_end) of P f (FP64): the same rays as
-    ``project`` computes for those slices (src/projectors.cu:11-238)."""
+def project_band(G, f, v1_begin, v1_end, nthreads=0, dtype=np.float64):
+    """The v1 slices [v1_begin, v1_end) of P f (FP64, or FP32 for timing): the
+    same rays as ``project`` computes for those slices
+    (src/projectors.cu:11-238)."""
+    shape = (v1_end - v1_begin,) + tuple(G.shape[1:])
+    if dtype == np.float32:
+        fc = _f(f)
+        g = np.zeros(shape, np.float32)
+        lib().oracle_project_band_f32(ctypes.byref(G), _ptr(fc, ctypes.c_float), _ptr(g, ctypes.c_float),
+                                      int(v1_begin), int(v1_end), nthreads)
+        return g
     fc = _d(f)
-    g = np.zeros((v1_end - v1_begin,) + tuple(G.shape[1:]), np.float64)
+    g = np.zeros(shape, np.float64)
     lib().oracle_project_band_f64(ctypes.byref(G), _ptr(fc, ctypes.c_double), _ptr(g, ctypes.c_double),
                                   int(v1_begin), int(v1_end), nthreads)
     return g
 
 
-def backproject_band(G, g_band, v1_begin, v1_end, nthreads=0):
+def backproject_band(G, g_band, v1_begin, v1_end, nthreads=0, dtype=np.float64):
     """Backprojection of the v1 slices [v1_begin, v1_end) only; g_band holds
-    just those slices (FP64, src/projectors.cu:240-377 summed over the band)."""
+    just those slices (FP64, or FP32 for timing; src/projectors.cu:240-377
+    summed over the band)."""
+    assert np.shape(g_band)[0] == v1_end - v1_begin
+    if dtype == np.float32:
+        gc = _f(g_band)
+        f = np.zeros(G.vol_shape, np.float32)
+        lib().oracle_backproject_band_f32(ctypes.byref(G), _ptr(gc, ctypes.c_float), _ptr(f, ctypes.c_float),
+                                          int(v1_begin), int(v1_end), nthreads)
+        return f
     gc = _d(g_band)
-    assert gc.shape[0] == v1_end - v1_begin
     f = np.zeros(G.vol_shape, np.float64)
     lib().oracle_backproject_band_f64(ctypes.byref(G), _ptr(gc, ctypes.c_double), _ptr(f, ctypes.c_double),
                                       int(v1_begin), int(v1_end), nthreads)
