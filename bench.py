@@ -25,6 +25,10 @@ the reference publishes no benchmark data set.
 * ``reference_gpu``: the reference's own GPU build (its sources compiled
   for sm_100a) through its C ABI on numpy host arrays, with this library on
   the same calls beside it (single-GPU runs).
+* ``serving``: the served-reconstruction workload (200 OSEM requests of
+  four volume sizes; petl_b200.studies.study_serving): p50 / p99 latency and
+  recons/s of the continuous-batching server and of the one-at-a-time device
+  path, at 20 arrivals/s and at saturation (single-GPU runs).
 
 ``--impl reference`` times the reference path's CPU implementation (the
 oracle restatement: the reference has no CPU projector) instead.
@@ -279,6 +283,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -400,6 +405,12 @@ def main():
         line["cpu_baseline"] = cpu_baseline()
         if world == 1:
             line["reference_gpu"] = reference_gpu_baseline(f_host)
+    if world == 1 and not args.no_serving:
+        # the metric's second half: served reconstructions, p50 / p99
+        del g, fb, flush
+        torch.cuda.empty_cache()
+        from petl_b200.studies import study_serving
+        line["serving"] = study_serving()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -158,8 +158,33 @@ int petl_ray_trace_dev(const petl_geom* G, const petl_solid* solids, int n, floa
 /* Error word written by kernels whose waits on asynchronous copies are
  * bounded: nonzero if a wait gave up (the call's result is then invalid).
  * Reading it synchronizes the device and clears it.  -1 if it cannot be
- * read. */
+ * read.  The reference-compatible calls (project, backproject, FBP) read it
+ * after their own synchronisation and return false when it is set; callers
+ * of the stream-ordered entry points here read it themselves. */
 int petl_device_error_flag(void);
+
+/* Failure-path hook; no counterpart in the reference.  The projector
+ * kernels' waits on staged data give up after 2^22 polls: they set the error
+ * word, drain their copies in flight (with the full bound) and return
+ * without writing.  With on != 0 every such wait of the kernels launched
+ * afterwards gives up before polling, which drives that path without a
+ * fault or a hang; on == 0 restores the bound.  Process-wide, read when a
+ * launch is built. */
+int petl_force_wait_timeout(int on);
+
+/* Allocation failure injection; no counterpart in the reference (whose
+ * calls leak their device buffers when a cudaMalloc fails).  Every scratch
+ * allocation of this library (device buffers of the reference-compatible
+ * calls, projector tables and scratch, reductions) comes from one stream-
+ * ordered pool per device.  petl_inject_alloc_failure(n) makes the n-th
+ * allocation from now fail once as out of memory (n <= 0 disarms);
+ * petl_scratch_alloc_count() counts the allocations made so far;
+ * petl_scratch_in_use() gives the bytes of the current device's pool held by
+ * live allocations (after a synchronisation: 0 when no call is running), -1
+ * if it cannot be read. */
+int petl_inject_alloc_failure(long long n);
+long long petl_scratch_alloc_count(void);
+long long petl_scratch_in_use(void);
 
 /* Forward SF projection (src/projectors.cu:11-238).  Computes the views
  * iv0 = iv0_first + k*iv0_step (k = 0.., iv0 < N_v0) of every v1 slice and
@@ -265,6 +290,16 @@ void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int
  * petl_server_wait returns for it; *id_out receives the request id. */
 int petl_server_submit(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
                        long long* id_out);
+/* The same with a deadline, deadline_s seconds after submission (< 0: none).
+ * A request still pending at its deadline fails without being admitted; an
+ * active one issues no further steps, lets its steps in flight finish,
+ * releases its memory and fails.  Its waiter gets a nonzero return and
+ * "deadline exceeded" in petl_last_error(). */
+int petl_server_submit_deadline(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
+                                double deadline_s, long long* id_out);
+/* Cancels a request that has not been waited for: it ends as a deadline
+ * does, with "cancelled".  A request that already finished is unaffected. */
+int petl_server_cancel(void* server, long long id);
 /* Blocks until the request finishes; copies the image (numZ*numY*numX
  * floats) to f_host when non-null; latency = submit to result on the host,
  * queue = submit to admission, both in seconds. */

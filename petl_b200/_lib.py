@@ -84,6 +84,10 @@ _DEV_API = [
     ("petl_copy_to_host", c_i, [c_vp, c_vp, c_ll, c_vp]), ("petl_copy_to_device", c_i, [c_vp, c_vp, c_ll, c_vp]),
     ("petl_set_dispatch", c_i, [c_i]),
     ("petl_device_error_flag", c_i, []),
+    ("petl_force_wait_timeout", c_i, [c_i]),
+    ("petl_inject_alloc_failure", c_i, [ctypes.c_longlong]),
+    ("petl_scratch_alloc_count", ctypes.c_longlong, []),
+    ("petl_scratch_in_use", ctypes.c_longlong, []),
     ("petl_last_projector_path", c_i, []),
     ("petl_project_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_vp]),
     ("petl_project_range_dev", c_i, [_G, c_vp, c_vp, c_i, c_i, c_i, c_i, c_vp]),
@@ -107,6 +111,8 @@ _DEV_API = [
     ("petl_to_bf16_dev", c_i, [c_vp, c_vp, c_ll, c_vp]),
     ("petl_server_create", c_vp, [c_d, c_i, c_i, c_i]),
     ("petl_server_submit", c_i, [c_vp, _G, c_vp, c_i, c_i, ctypes.POINTER(c_ll)]),
+    ("petl_server_submit_deadline", c_i, [c_vp, _G, c_vp, c_i, c_i, c_d, ctypes.POINTER(c_ll)]),
+    ("petl_server_cancel", c_i, [c_vp, c_ll]),
     ("petl_server_wait", c_i, [c_vp, c_ll, c_vp, ctypes.POINTER(c_d), ctypes.POINTER(c_d)]),
     ("petl_server_stats", c_i, [c_vp, ctypes.POINTER(c_d)]),
     ("petl_server_destroy", None, [c_vp]),

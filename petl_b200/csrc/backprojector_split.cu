@@ -101,6 +101,7 @@ struct ZgatherArgs {
     int v1cap;     // slopes the per-CTA tables hold (the call's slope count)
     Tables T;
     int* err;
+    unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
 };
 
 // z taps of one plane (two columns): Z[k] += w0 W[O + k + 1] then w1 W[O + k],
@@ -357,7 +358,7 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
     // stage j reuses its slot once every warp has released stage j - ns
     auto issue = [&](int j) {
         const int slot = j % ns, round = j / ns;
-        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err)) return false;
+        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err, A.wait_limit)) return false;
         if (*s_abort) return false;
         fence_proxy_async_smem();
         const int k = j / nsp, pr = j - k * nsp;
@@ -418,7 +419,7 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
             if (lane == 0 && !dead && my_next < nst && !issue(my_next)) dead = true;
             my_next += GWARPS;
         }
-        if (!dead) dead = !mbar_wait(&full[slot], phase, A.err);
+        if (!dead) dead = !mbar_wait(&full[slot], phase, A.err, A.wait_limit);
         if (dead) *s_abort = 1;  // before this warp releases the slot
 #pragma unroll 1
         for (int h = 0; h < 2 && !dead; h++) {
@@ -611,6 +612,7 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     A.v1cap = nv1;
     A.T = T;
     A.err = err;
+    A.wait_limit = wait_limit();
 
     // chunks of views whose scratch fits the budget, balanced in size
     const size_t per_view = size_t(G.numY) * G.numZ * A.NUc * 4;

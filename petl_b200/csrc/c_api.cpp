@@ -161,6 +161,21 @@ bool report(const char* what, int rc)
     return true;
 }
 
+// The kernels' bounded waits record a give-up (and a failed host-side layout
+// bound) in the device error word instead of hanging; a call whose kernels
+// did so has incomplete outputs and fails.  Read after the call's final
+// synchronisation (reading clears the word).
+bool device_ok(const char* what)
+{
+    const int flag = petl_device_error_flag();
+    if (flag > 0) {
+        fprintf(stderr, "%s failed: device error word %d (1: a bounded wait gave up, 2: a layout bound)\n", what,
+                flag);
+        return false;
+    }
+    return true;
+}
+
 bool cuda_ok(const char* what, cudaError_t e)
 {
     if (e != cudaSuccess) {
@@ -388,10 +403,16 @@ cudaError_t copy_h2d(void* dev, const void* host, size_t bytes, cudaStream_t st)
 struct DevBuf {
     void* p = nullptr;
     cudaStream_t st = nullptr;
+    cudaError_t err = cudaSuccess;  // of the last alloc()
     bool alloc(size_t bytes, cudaStream_t s)
     {
         st = s;
-        return petl::scratch_alloc(&p, bytes ? bytes : 4, s) == cudaSuccess;
+        err = petl::scratch_alloc(&p, bytes ? bytes : 4, s);
+        if (err != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();  // an allocation failure is not sticky: clear it
+        }
+        return err == cudaSuccess;
     }
     ~DevBuf()
     {
@@ -517,7 +538,7 @@ bool stream_planograms(const Params& P, float** g, float** r, const char* what, 
         const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0, n = slab * G.N_v1;
         DevBuf dg, dr;
         if (!dg.alloc(n * 4, c->compute) || (r && !dr.alloc(n * 4, c->compute)))
-            return cuda_ok(what, cudaGetLastError());
+            return cuda_ok(what, dg.err != cudaSuccess ? dg.err : dr.err);
         // the copy stream may only write the buffers once they exist
         cudaEvent_t ready;
         cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
@@ -787,7 +808,7 @@ bool bin(float** g, char* file_name)
     for (const petl_geom& G : P.plans) {
         bufs.emplace_back(new DevBuf);
         const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
-        if (!bufs.back()->alloc(n * 4, c->compute)) return cuda_ok("bin alloc", cudaGetLastError());
+        if (!bufs.back()->alloc(n * 4, c->compute)) return cuda_ok("bin alloc", bufs.back()->err);
         dg.push_back(bufs.back()->f());
     }
     long long events = 0;
@@ -856,7 +877,7 @@ bool voxelize(float* f, int oversampling)
                          P.offsetZ);
     const size_t n = P.volElems();
     DevBuf df;
-    if (!df.alloc(n * 4, c->compute)) return cuda_ok("voxelize alloc", cudaGetLastError());
+    if (!df.alloc(n * 4, c->compute)) return cuda_ok("voxelize alloc", df.err);
     bool ok = cuda_ok("voxelize H2D", copy_h2d(df.f(), f, n * 4, c->compute));
     ok = ok && report("voxelize", petl_voxelize_dev(solids.data(), int(solids.size()), df.f(), P.numX, P.numY,
                                                     P.numZ, P.voxelWidth, P.voxelHeight, Gv.x_0, Gv.y_0, Gv.z_0,
@@ -886,7 +907,7 @@ static bool trace_planograms(float** g, int oversampling, bool stopping, const c
         const petl_geom& G = P.plans[i];
         const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
         DevBuf dg;
-        if (!dg.alloc(n * 4, c->compute)) return cuda_ok(what, cudaGetLastError());
+        if (!dg.alloc(n * 4, c->compute)) return cuda_ok(what, dg.err);
         ok = report(what, petl_ray_trace_dev(&G, solids.data(), int(solids.size()), dg.f(), oversampling,
                                              stopping ? 1 : 0, c->compute));
         ok = ok && cuda_ok(what, copy_d2h(g[i], dg.f(), n * 4, c->compute));
@@ -939,7 +960,7 @@ bool project(float** g, float* f)
     DevCtx* c = dev_ctx();
     if (!c) return cuda_ok("project", cudaErrorNoDevice);
     DevBuf df;
-    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
+    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("project alloc", df.err);
     if (!cuda_ok("project H2D", copy_h2d(df.f(), f, P.volElems() * 4, c->compute)))
         return false;
     bool ok = true;
@@ -947,7 +968,7 @@ bool project(float** g, float* f)
         const petl_geom G = P.full(i);
         const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0;
         DevBuf dg;
-        if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("project alloc", cudaGetLastError());
+        if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("project alloc", dg.err);
         // split kernels: each chunk of views goes back while the next computes
         ViewCopy vc{G, g[i], dg.f(), c->compute, c->copy, true};
         vc.pinned = host_pinned(g[i]);
@@ -977,7 +998,7 @@ bool project(float** g, float* f)
     }
     ok = cuda_ok("project sync", cudaStreamSynchronize(c->copy)) && ok;
     ok = cuda_ok("project sync", cudaStreamSynchronize(c->compute)) && ok;
-    return ok;
+    return device_ok("project") && ok;
 }
 
 static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weight_unused)
@@ -986,14 +1007,14 @@ static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weig
     DevCtx* c = dev_ctx();
     if (!c) return cuda_ok("backproject", cudaErrorNoDevice);
     DevBuf df;
-    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("backproject alloc", cudaGetLastError());
+    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("backproject alloc", df.err);
     bool ok = true;
     bool first = true;
     for (size_t i = 0; i < P.plans.size() && ok; i++) {
         const petl_geom G = P.full(i);
         const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0;
         DevBuf dg;
-        if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("backproject alloc", cudaGetLastError());
+        if (!dg.alloc(slab * G.N_v1 * 4, c->compute)) return cuda_ok("backproject alloc", dg.err);
         // the copy stream may only start once the buffer exists on the compute stream
         cudaEvent_t ready;
         cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
@@ -1029,7 +1050,7 @@ static bool backproject_impl(const Params& P, float** g, float* f, bool fbp_weig
     ok = ok && cuda_ok("backproject D2H",
                        copy_d2h(f, df.f(), P.volElems() * 4, c->compute));
     ok = cuda_ok("backproject sync", cudaStreamSynchronize(c->compute)) && ok;
-    return ok;
+    return device_ok("backproject") && ok;
 }
 
 bool backproject(float** g, float* f)
@@ -1046,13 +1067,13 @@ bool FBP(float** g, float* f)
     DevCtx* c = dev_ctx();
     if (!c) return cuda_ok("FBP", cudaErrorNoDevice);
     DevBuf df;
-    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("FBP alloc", cudaGetLastError());
+    if (!df.alloc(P.volElems() * 4, c->compute)) return cuda_ok("FBP alloc", df.err);
     bool ok = true;
     for (size_t i = 0; i < P.plans.size() && ok; i++) {
         const petl_geom G = P.full(i);
         const size_t n = size_t(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0;
         DevBuf dg;
-        if (!dg.alloc(n * 4, c->compute)) return cuda_ok("FBP alloc", cudaGetLastError());
+        if (!dg.alloc(n * 4, c->compute)) return cuda_ok("FBP alloc", dg.err);
         ok = cuda_ok("FBP H2D", copy_h2d(dg.f(), g[i], n * 4, c->compute));
         // already-rebinned data is filtered and weighted in the caller's array,
         // as the reference does (src/petl.cpp:335-349)
@@ -1061,7 +1082,7 @@ bool FBP(float** g, float* f)
     }
     ok = ok && cuda_ok("FBP D2H", copy_d2h(f, df.f(), P.volElems() * 4, c->compute));
     ok = cuda_ok("FBP sync", cudaStreamSynchronize(c->compute)) && ok;
-    return ok;
+    return device_ok("FBP") && ok;
 }
 
 bool PFDR(float** g, float** g_reb)
@@ -1080,7 +1101,7 @@ bool PFDR(float** g, float** g_reb)
         const size_t nr = size_t(G.N_v0) * G.N_u1 * G.N_u0;
         DevBuf dg, dr;
         if (!dg.alloc(n * 4, c->compute) || !dr.alloc(nr * 4, c->compute))
-            return cuda_ok("PFDR alloc", cudaGetLastError());
+            return cuda_ok("PFDR alloc", dg.err != cudaSuccess ? dg.err : dr.err);
         ok = cuda_ok("PFDR H2D", copy_h2d(dg.f(), g[i], n * 4, c->compute));
         ok = ok && report("PFDR", petl_pfdr_dev(&G, dg.f(), dr.f(), c->compute));
         ok = ok && cuda_ok("PFDR D2H", copy_d2h(g_reb[i], dr.f(), nr * 4, c->compute));

@@ -39,20 +39,32 @@ int sm_count()
     return cached[dev];
 }
 
+namespace {
+std::atomic<long long> g_alloc_countdown{0};  // > 0: the allocation that brings it to 0 fails
+std::atomic<long long> g_alloc_count{0};
+cudaMemPool_t g_pools[64] = {nullptr};
+std::mutex g_pool_mu;
+}  // namespace
+
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st)
 {
+    g_alloc_count.fetch_add(1, std::memory_order_relaxed);
+    if (g_alloc_countdown.load(std::memory_order_relaxed) > 0 &&
+        g_alloc_countdown.fetch_sub(1, std::memory_order_relaxed) == 1) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;  // injected (petl_inject_alloc_failure)
+    }
     // one library pool per device that keeps freed blocks (release threshold
     // at its maximum): a pool that hands memory back to the system at each
     // synchronisation would map gigabytes of projector scratch anew per call
-    static std::mutex mu;
-    static cudaMemPool_t pools[64] = {nullptr};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     cudaMemPool_t pool = nullptr;
     {
-        std::lock_guard<std::mutex> lk(mu);
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        cudaMemPool_t* pools = g_pools;
         if (!pools[dev]) {
             cudaMemPoolProps props{};
             props.allocType = cudaMemAllocationTypePinned;
@@ -68,7 +80,9 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st)
         }
         pool = pools[dev];
     }
-    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+    e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+    if (e != cudaSuccess) cudaGetLastError();  // out of memory is not sticky: leave no error behind
+    return e;
 }
 
 bool geom_valid(const petl_geom* G, std::string* why)
@@ -97,6 +111,29 @@ const char* petl_last_error(void) { return petl::g_last_error.c_str(); }
 int petl_version(void) { return 100; }
 
 unsigned long long petl_launch_count(void) { return petl::g_launches.load(std::memory_order_relaxed); }
+
+int petl_inject_alloc_failure(long long n)
+{
+    petl::g_alloc_countdown.store(n > 0 ? n : 0, std::memory_order_relaxed);
+    return 0;
+}
+
+long long petl_scratch_alloc_count(void) { return petl::g_alloc_count.load(std::memory_order_relaxed); }
+
+long long petl_scratch_in_use(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(petl::g_pool_mu);
+        pool = petl::g_pools[dev];
+    }
+    if (!pool) return 0;
+    uint64_t used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) return -1;
+    return (long long)used;
+}
 
 int petl_optimal_fft_size(int N)
 {

@@ -72,6 +72,7 @@ struct FwdTmaArgs {
     int xstride;   // floats per interpolated buffer
     Tables T;
     int* err;
+    unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
 };
 
 struct FwdPlane {
@@ -284,10 +285,10 @@ k_fwd_tma(const __grid_constant__ CUtensorMap fmap, TG* __restrict__ g, const TG
             const int y0 = plist[li], y1 = two ? plist[li + 1] : y0;
             const FwdPlane p0 = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y0);
             const FwdPlane p1 = fwd_plane(s_xt, s_zt, nsl, NY, col0, cta_row0, y1);
-            if (!dead) dead = !mbar_wait(&bar[b], phase, A.err);
+            if (!dead) dead = !mbar_wait(&bar[b], phase, A.err, A.wait_limit);
             stage_a(b, xq, p0);
             if (two) {
-                if (!dead) dead = !mbar_wait(&bar[b1], phase1, A.err);
+                if (!dead) dead = !mbar_wait(&bar[b1], phase1, A.err, A.wait_limit);
                 stage_a(b1, xq + 1, p1);
             }
             if (__syncthreads_or(dead)) break;
@@ -383,6 +384,7 @@ struct BwdTmaArgs {
     float scale;
     Tables T;
     int* err;
+    unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
 };
 
 // z taps of one plane: Z[k] += w1 g[row k of tap 1] + w0 g[row k of tap 0],
@@ -468,6 +470,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, const TG* __restrict__ gsrc,
     uint64_t* full = reinterpret_cast<uint64_t*>(s_pat + BV1CAP);         // [ns]
     uint64_t* empty = full + BNSMAX;                                      // [ns]
     int* s_n = reinterpret_cast<int*>(empty + BNSMAX);
+    volatile int* s_abort = s_n + 1;  // a consumer gave up a wait: start no further copies
     int* s_round = s_n + 2;                                               // [ns]
 
     // ---- per-CTA slope tables (warp 0): for every slope whose rows reach the
@@ -611,6 +614,7 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, const TG* __restrict__ gsrc,
                 n = BV1CAP;
             }
             s_n[0] = n;
+            *s_abort = 0;
             for (int s = 0; s < ns; s++) {
                 mbar_init(&full[s], 1);
                 mbar_init(&empty[s], nwarps);
@@ -665,7 +669,10 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, const TG* __restrict__ gsrc,
         const int slot = j % ns, round = j / ns;
         const int li = j % nlive;
         const int v0 = A.vr.iv0_first + (j / nlive) * A.vr.iv0_step;
-        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err)) return false;
+        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err, A.wait_limit)) return false;
+        // a warp that gave up released its slot without its copy confirmed:
+        // no copy may start into a slot after that
+        if (*s_abort) return false;
         fence_proxy_async_smem();
         if constexpr (BULK) {
             // row pairs [rp0, rp0 + nrows) of view (v1, v0), the part inside
@@ -721,10 +728,13 @@ k_bwd_tma(const __grid_constant__ CUtensorMap gmap, const TG* __restrict__ gsrc,
                 my_next += nwarps;
             }
             const int s = c_slot;
-            if (!dead) dead = !mbar_wait(&full[s], c_phase, A.err);
+            if (!dead) dead = !mbar_wait(&full[s], c_phase, A.err, A.wait_limit);
+            if (dead) *s_abort = 1;  // before this warp releases the slot
             const uint32_t code = s_code[li] >> (16 * pg);  // this group's 4 planes
             const uint32_t pat = (s_pat[li] >> (4 * pg)) & 15u;
-            if (ucol && pat != uint32_t(kPatGeneric)) {
+            if (dead) {
+                // the slot's data may not have arrived: nothing is read
+            } else if (ucol && pat != uint32_t(kPatGeneric)) {
                 const uint32_t wbw = s_wb[li];
                 const int wb = int((wbw >> (8 * pg)) & 0xff) + (BULK ? int(wbw >> 24) : 0);
                 const TG* Gs = ring(s) + wb * NU0 + u;
@@ -882,6 +892,7 @@ int project_tma_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr, c
     A.xstride = (nrb + FDMAX) * FCOLS;
     A.T = T;
     A.err = err;
+    A.wait_limit = wait_limit();
     // up to 4 planes in flight; prefer a footprint that leaves room for two
     // CTAs per SM, else the largest ring that fits one
     auto bytes = [&](int nf) {
@@ -947,6 +958,7 @@ int backproject_tma_t(const petl_geom& G, const TG* g, TF* f, int mode, int accu
     A.scale = scale;
     A.T = T;
     A.err = err;
+    A.wait_limit = wait_limit();
     // as many ring stages as fit (copies from DRAM need several in flight)
     A.max_views = vr.n_v0(G.N_v0);
     const size_t fixed = size_t(np) * BK * NU0 * 4 + size_t(BV1CAP) * np * 8 + size_t(BV1CAP) * np * 4 +

@@ -134,6 +134,7 @@ struct ZsumArgs {
     unsigned off_w, off_code, off_plane, off_bar;
     Tables T;
     int* err;
+    unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
 };
 
 // z taps of one slope: all first-tap FMAs, then all second-tap FMAs (16
@@ -308,7 +309,7 @@ k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, TG* __restrict__ g, const T
         // warp has released stage j - ns
         auto issue = [&](int j) {
             const int slot = j % ns, round = j / ns;
-            if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err)) return false;
+            if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err, A.wait_limit)) return false;
             if (*s_abort) return false;
             fence_proxy_async_smem();
             const int np = min(2, nlive - 2 * j);
@@ -332,7 +333,7 @@ k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, TG* __restrict__ g, const T
                 if (lane == 0 && !dead && my_next < nst && !issue(my_next)) dead = true;
                 my_next += ZWARPS;
             }
-            if (!dead) dead = !mbar_wait(&full[slot], phase, A.err);
+            if (!dead) dead = !mbar_wait(&full[slot], phase, A.err, A.wait_limit);
             if (dead) *s_abort = 1;  // before this warp releases the slot
 #pragma unroll 1
             for (int h = 0; h < 2 && !dead; h++) {
@@ -440,6 +441,7 @@ bool zsum_layout(const petl_geom& G, const ViewRange& vr, int v1_first, int v1_e
     A.pstride = ((nrb + ZDMAX) * ZCOLS + 31) & ~31;  // 128-byte aligned planes
     A.T = T;
     A.err = err;
+    A.wait_limit = wait_limit();
     // shared memory: the ring, then the per-CTA tables and the barriers
     const size_t np = size_t(std::min(G.numY, ZMAXPLANES));
     const size_t b_w = np * 4 * sizeof(float4), b_code = np * 4 * 4, b_plane = np * 8;

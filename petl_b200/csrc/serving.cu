@@ -14,7 +14,11 @@
 //    and new requests join while others run;
 //  * completion: after the last step the image is copied to a pinned host
 //    buffer, the device memory is returned to the stream-ordered pool and
-//    the request's latency (submit to result on the host) is recorded.
+//    the request's latency (submit to result on the host) is recorded;
+//  * deadlines and cancellation: a request may carry a deadline (seconds
+//    after submission) and may be cancelled; a pending one is dropped before
+//    admission, an active one issues no further steps, its steps in flight
+//    finish, its memory is released and its waiter gets an error.
 //
 // Each request runs the same kernels in the same order whatever else is
 // running, so its result is bit-identical alone and in a mix.
@@ -80,6 +84,9 @@ struct Request {
     State state = kPending;
     std::string error;
     Clock::time_point t_submit, t_admit, t_done;
+    bool has_deadline = false;
+    Clock::time_point deadline;
+    bool cancelled = false;  // set by petl_server_cancel under the server mutex
     size_t bytes = 0;
     // device state
     cudaStream_t st = nullptr;
@@ -122,6 +129,7 @@ struct Server {
     std::thread worker;
 
     void run();
+    void drop_expired_pending();
     bool admit(Request& r);
     bool issue_step(Request& r);
     void release(Request& r);
@@ -141,6 +149,33 @@ void Server::fail(Request& r, const std::string& why)
 {
     r.error = why;
     r.state = kFailed;
+}
+
+// A request's reason to stop, or nullptr: cancelled, or past its deadline.
+const char* stop_reason(const Request& r, Clock::time_point now)
+{
+    if (r.cancelled) return "cancelled";
+    if (r.has_deadline && now >= r.deadline) return "deadline exceeded";
+    return nullptr;
+}
+
+// Pending requests that were cancelled or whose deadline passed fail
+// without being admitted (caller holds the mutex).
+void Server::drop_expired_pending()
+{
+    const Clock::time_point now = Clock::now();
+    for (auto it = pending.begin(); it != pending.end();) {
+        Request& r = **it;
+        if (const char* why = stop_reason(r, now)) {
+            fail(r, std::string(why) + " before admission");
+            r.t_done = now;
+            failed++;
+            it = pending.erase(it);
+            cv_done.notify_all();
+        } else {
+            ++it;
+        }
+    }
 }
 
 bool Server::admit(Request& r)
@@ -244,6 +279,7 @@ void Server::run()
         {
             std::unique_lock<std::mutex> lk(mu);
             if (stop) break;
+            drop_expired_pending();
             // admission by HBM budget and free slots, in arrival order
             while (!pending.empty() && int(active.size() + to_admit.size()) < max_active) {
                 auto& r = pending.front();
@@ -269,12 +305,25 @@ void Server::run()
         }
         bool progressed = !to_admit.empty();
         // retire finished steps, issue new ones round-robin
+        const Clock::time_point now = Clock::now();
         for (auto& rp : active) {
             Request& r = *rp;
             while (!r.inflight.empty() && cudaEventQuery(r.inflight.front()) == cudaSuccess) {
                 cudaEventDestroy(r.inflight.front());
                 r.inflight.pop_front();
                 progressed = true;
+            }
+            if (r.state == kActive && !r.result_issued) {
+                const char* why = nullptr;
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    why = stop_reason(r, now);
+                }
+                if (why) {  // no further steps; release() waits for those in flight
+                    fail(r, why);
+                    progressed = true;
+                    continue;
+                }
             }
             if (r.state == kActive && !r.result_issued && r.steps_issued < r.steps_total &&
                 int(r.inflight.size()) < depth) {
@@ -317,6 +366,10 @@ void Server::run()
             std::unique_lock<std::mutex> lk(mu);
             if (active.empty() && pending.empty())
                 cv_work.wait(lk, [&] { return stop || !pending.empty(); });
+            else if (active.empty())
+                // pending requests that do not fit yet cannot exist with no
+                // request active; wake up for deadlines and cancellations
+                cv_work.wait_for(lk, std::chrono::milliseconds(5));
             else if (!active.empty()) {
                 // wait for the oldest step of some request instead of spinning
                 lk.unlock();
@@ -355,8 +408,17 @@ void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int
     return s;
 }
 
+int petl_server_submit_deadline(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
+                                double deadline_s, long long* id_out);
+
 int petl_server_submit(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
                        long long* id_out)
+{
+    return petl_server_submit_deadline(server, G, g_host, num_subsets, num_iter, -1.0, id_out);
+}
+
+int petl_server_submit_deadline(void* server, const petl_geom* G, const float* g_host, int num_subsets, int num_iter,
+                                double deadline_s, long long* id_out)
 {
     clear_error();
     Server* s = static_cast<Server*>(server);
@@ -371,6 +433,10 @@ int petl_server_submit(void* server, const petl_geom* G, const float* g_host, in
     r->iters = num_iter;
     r->bytes = footprint(*G, num_subsets);
     r->t_submit = Clock::now();
+    if (deadline_s >= 0.0) {
+        r->has_deadline = true;
+        r->deadline = r->t_submit + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(deadline_s));
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         PETL_REQUIRE(double(r->bytes) <= s->budget, "server_submit: request larger than the HBM budget");
@@ -411,6 +477,21 @@ int petl_server_wait(void* server, long long id, float* f_host, double* latency_
     if (r->out_host) cudaFreeHost(r->out_host);
     r->out_host = nullptr;
     return rc;
+}
+
+int petl_server_cancel(void* server, long long id)
+{
+    clear_error();
+    Server* s = static_cast<Server*>(server);
+    PETL_REQUIRE(s, "server_cancel: null server");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->all.find(id);
+        PETL_REQUIRE(it != s->all.end(), "server_cancel: unknown request");
+        it->second->cancelled = true;
+    }
+    s->cv_work.notify_one();
+    return 0;
 }
 
 // out[0..5] = completed, failed, active, pending, HBM bytes in use, peak HBM bytes reserved

@@ -3,6 +3,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -31,6 +33,12 @@ EncodeFn encode_fn()
     return fn;
 }
 }  // namespace
+
+namespace {
+std::atomic<int> g_force_timeout{0};
+}
+
+unsigned wait_limit() { return g_force_timeout.load(std::memory_order_relaxed) ? 0u : kWaitLimit; }
 
 int* device_error_ptr()
 {
@@ -86,4 +94,10 @@ extern "C" int petl_device_error_flag(void)
         cudaMemcpy(p, &z, sizeof(int), cudaMemcpyHostToDevice);
     }
     return h;
+}
+
+extern "C" int petl_force_wait_timeout(int on)
+{
+    petl::g_force_timeout.store(on ? 1 : 0, std::memory_order_relaxed);
+    return 0;
 }

@@ -24,9 +24,12 @@ class ReconServer:
         self._keep = {}
         self._shapes = {}
 
-    def submit(self, geom, g, num_subsets, num_iter):
+    def submit(self, geom, g, num_subsets, num_iter, deadline_s=None):
         """Queue OSEM of planogram ``g`` (float32, host numpy array or CPU
-        tensor, contiguous, shape geom.shape); returns the request id."""
+        tensor, contiguous, shape geom.shape); returns the request id.  With
+        ``deadline_s`` the request fails ("deadline exceeded") if it has not
+        finished that many seconds after submission: dropped before
+        admission, or stopped between subset steps."""
         if hasattr(g, "data_ptr"):
             ptr = g.data_ptr()
             assert g.dtype.__str__() == "torch.float32" and g.is_contiguous() and not g.is_cuda
@@ -35,8 +38,9 @@ class ReconServer:
             ptr = g.ctypes.data
         assert tuple(g.shape) == tuple(geom.shape), (g.shape, geom.shape)
         rid = ctypes.c_longlong(0)
-        check(lib().petl_server_submit(self._s, geom.ptr, ctypes.c_void_p(ptr), int(num_subsets), int(num_iter),
-                                       ctypes.byref(rid)), "server_submit")
+        dl = -1.0 if deadline_s is None else float(deadline_s)
+        check(lib().petl_server_submit_deadline(self._s, geom.ptr, ctypes.c_void_p(ptr), int(num_subsets),
+                                                int(num_iter), dl, ctypes.byref(rid)), "server_submit")
         self._keep[rid.value] = (g, geom)
         self._shapes[rid.value] = tuple(geom.vol_shape)
         return rid.value
@@ -51,6 +55,10 @@ class ReconServer:
         self._shapes.pop(rid, None)
         check(rc, "server_wait")
         return out, lat.value, q.value
+
+    def cancel(self, rid):
+        """Cancel a request (its wait() then raises with "cancelled")."""
+        check(lib().petl_server_cancel(self._s, ctypes.c_longlong(rid)), "server_cancel")
 
     def stats(self):
         buf = (ctypes.c_double * 6)()

@@ -194,12 +194,23 @@ def _serving_requests(n, rate, seed, device):
     return reqs
 
 
-def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0):
+def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, modes=("arrivals", "saturation")):
+    """The serving workload: n OSEM requests with seeded Poisson arrivals at
+    `rate`/s (mode "arrivals") or all submitted at t = 0 ("saturation"),
+    served (a) by the continuous-batching server and (b) one request at a
+    time by the plain device path (host data to the device, recon.osem, the
+    image back to the host, in arrival order).  Latency is host wall clock
+    from a request's arrival to its image on the host; recons/s is n over
+    the time from the first arrival to the last result."""
     from .serving import ReconServer
     reqs = _serving_requests(n, rate, seed, "cuda")
-    # one data set per geometry class (the work of a request does not depend
-    # on its counts, so requests of a class share one Poisson realisation at
-    # the class's first drawn counts)
+    # geometry classes: N in {64,128,192,256}, T in {1,1.5,2} mm, D in
+    # {200,250,300} mm (the workload draws T and D from [1,2] and [200,300];
+    # a request's work depends on them only through its planogram shape and
+    # slopes, which the grid spans, and one pinned planogram per distinct
+    # geometry would need up to 1.1 GB of page-locked host memory each).
+    # Requests of a class share one Poisson realisation at the class's first
+    # drawn counts: the work does not depend on the counts.
     classes = {}
     for r in reqs:
         key = (r["N"], r["T"], r["D"])
@@ -214,38 +225,82 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0):
             del y, f
     torch.cuda.synchronize()
 
-    def serve(active):
-        with ReconServer(hbm_budget_gb=budget_gb, max_active=active, depth=2) as srv:
-            # warm-up: one request per class
-            for key, (G, host) in classes.items():
+    def arrivals(mode):
+        return [r["t"] if mode == "arrivals" else 0.0 for r in reqs]
+
+    def summary(lat, wall, extra=None):
+        lat = np.array(lat)
+        out = {"recons_per_s": n / wall, "wall_s": wall, "p50_s": float(np.percentile(lat, 50)),
+               "p99_s": float(np.percentile(lat, 99)), "max_s": float(lat.max())}
+        out.update(extra or {})
+        return out
+
+    def serve_server(mode):
+        at = arrivals(mode)
+        with ReconServer(hbm_budget_gb=budget_gb, max_active=max_active, depth=2) as srv:
+            for key, (G, host) in classes.items():  # warm-up: one request per class
                 srv.wait(srv.submit(G, host, 4, 1))
             t0 = time.perf_counter()
             ids = []
-            for r in reqs:
+            for r, a in zip(reqs, at):
                 now = time.perf_counter() - t0
-                if r["t"] > now:
-                    time.sleep(r["t"] - now)
+                if a > now:
+                    time.sleep(a - now)
                 G, host = classes[(r["N"], r["T"], r["D"])]
                 ids.append(srv.submit(G, host, r["S"], r["it"]))
-            lat, queue = [], []
-            for i in ids:
-                _, l, q = srv.wait(i)
-                lat.append(l)
-                queue.append(q)
+            lat = []
+            for i, a in zip(ids, at):
+                srv.wait(i)
+                lat.append(time.perf_counter() - t0 - a)
             wall = time.perf_counter() - t0
             st = srv.stats()
-        lat = np.array(lat)
-        return {"recons_per_s": n / wall, "wall_s": wall, "p50_s": float(np.percentile(lat, 50)),
-                "p99_s": float(np.percentile(lat, 99)), "mean_queue_s": float(np.mean(queue)),
-                "hbm_peak_gb": st["hbm_peak_bytes"] / 1e9, "failed": st["failed"]}
+        return summary(lat, wall, {"hbm_peak_gb": st["hbm_peak_bytes"] / 1e9, "failed": st["failed"],
+                                   "max_active": max_active})
 
-    batched = serve(max_active)
-    single = serve(1)
-    return {"study": "serving", "workload": f"{n} OSEM requests, Poisson arrivals {rate}/s (seed {seed}), "
-            "N in {64,128,192,256} (vol NxNxN/2 at pitch T in {1,1.5,2} mm), L=H=N*T/2, D in {200,250,300} mm, "
-            "4 or 8 subsets, 2-6 iterations", "geometry_classes": len(classes), "budget_gb": budget_gb,
-            "continuous_batching": batched, "one_at_a_time": single,
-            "throughput_ratio": batched["recons_per_s"] / single["recons_per_s"]}
+    def serve_sequential(mode):
+        at = arrivals(mode)
+        for key, (G, host) in classes.items():  # warm-up
+            recon.osem(G, host.to("cuda", non_blocking=True), 1, 4)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lat = []
+        for r, a in zip(reqs, at):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            G, host = classes[(r["N"], r["T"], r["D"])]
+            f, _ = recon.osem(G, host.to("cuda", non_blocking=True), r["it"], r["S"])
+            f.cpu()
+            lat.append(time.perf_counter() - t0 - a)
+        wall = time.perf_counter() - t0
+        return summary(lat, wall)
+
+    # GPU-seconds of the mix: every request alone on the device, back to back
+    gpu_s = 0.0
+    for r in reqs:
+        G, host = classes[(r["N"], r["T"], r["D"])]
+        g = host.to("cuda")
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        recon.osem(G, g, r["it"], r["S"])
+        b.record()
+        torch.cuda.synchronize()
+        gpu_s += a.elapsed_time(b) / 1e3
+    out = {"study": "serving", "workload": f"{n} OSEM requests, Poisson arrivals {rate}/s (seed {seed}), "
+           "N in {64,128,192,256} (vol NxNxN/2 at pitch T in {1,1.5,2} mm), L=H=N*T/2, D in {200,250,300} mm, "
+           "4 or 8 subsets, 2-6 iterations", "geometry_classes": len(classes), "budget_gb": budget_gb,
+           "gpu_seconds_per_request": gpu_s / n,
+           "bound_recons_per_s": n / gpu_s,
+           "bound_note": "device time of the requests run alone back to back: no schedule of them on one GPU "
+                         "serves more than n / that many per second unless requests share launches"}
+    for mode in modes:
+        srv = serve_server(mode)
+        seq = serve_sequential(mode)
+        out[mode] = {"server": srv, "one_at_a_time": seq,
+                     "throughput_ratio": srv["recons_per_s"] / seq["recons_per_s"],
+                     "p99_ratio": srv["p99_s"] / seq["p99_s"]}
+    return out
 
 
 def study_binning(seed=0, n_events=16_000_000, n_file=8_000_000, tmpdir="/tmp"):

@@ -200,3 +200,20 @@ def test_host_logic_of_the_response_and_phantom_calls():
     assert s.simulate_scatter(g, f) is g
     s.clear_phantom()
     s.clear_modules()
+
+
+def test_server_drops_a_request_past_its_deadline_before_admission():
+    """Deadlines are host logic: a request whose deadline has passed when the
+    worker looks at it fails without being admitted (no device work), and
+    unknown requests cannot be cancelled."""
+    from petl_b200 import PetlError
+    from petl_b200.serving import ReconServer
+    G = Geometry(0.0, 64.0, 32.0, 16.0, 2.0, 0.5, 0.25, volume=(32, 32, 8, 2.0))
+    g = np.zeros(G.shape, np.float32)
+    with ReconServer(hbm_budget_gb=1, max_active=1) as srv:
+        rid = srv.submit(G, g, 2, 1, deadline_s=0.0)
+        with pytest.raises(PetlError, match="deadline exceeded before admission"):
+            srv.wait(rid)
+        with pytest.raises(PetlError, match="unknown request"):
+            srv.cancel(12345)
+        assert srv.stats()["failed"] == 1
