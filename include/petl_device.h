@@ -280,11 +280,15 @@ int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long l
  * owns the device and runs OSEM requests (reference-semantics
  * backprojector, f starting at 1, sensitivity zeros -> 1) with continuous
  * batching: requests are admitted in arrival order while their device
- * footprint fits hbm_budget_bytes and fewer than max_active run; every
- * active request has its own stream with up to `depth` subset steps in
- * flight, issued round-robin, so requests overlap on the GPU and join while
- * others run.  Data and images stay resident until the result is copied
- * out.  A request's result does not depend on what else runs. */
+ * footprint fits hbm_budget_bytes and fewer than max_active run; requests
+ * of like geometry (and subset count) share one copy of its sensitivity
+ * images and projector tables, computed once and cached within the budget
+ * (idle entries evicted least recently used first); every active request
+ * has its own stream with up to `depth` subset steps in flight, issued
+ * oldest request first while the work in flight stays under about two
+ * full-size steps, so small requests overlap with large ones and new ones
+ * join while others run.  Data and images stay resident until the result
+ * is copied out.  A request's result does not depend on what else runs. */
 void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int device);
 /* g_host: the request's planogram, which must stay valid until
  * petl_server_wait returns for it; *id_out receives the request id. */

@@ -29,8 +29,12 @@
 
 #include "common.cuh"
 #include "projector.cuh"
+#include "storage.cuh"
+#include "tma.cuh"
 
 namespace petl {
+
+int dispatch_mode();
 
 namespace {
 
@@ -220,6 +224,228 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr(const PfdrArgs A)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Streamed PFDR for power-of-two transform sizes and rows of a multiple of 4
+// floats (the workload sizes: N_u0 = 128 / 256 -> NX = 128 / 256).  Same
+// arithmetic as k_pfdr, organised for bandwidth:
+//  * a CTA owns kPfdrRows planogram rows (u1) of one view v0 and walks the
+//    v1 slices; each slice's rows are one contiguous block of the planogram,
+//    fetched by a bulk copy (cp.async.bulk, no tensor map, no multicast) into
+//    a ring of kPfdrStages slots two slices ahead of the computation;
+//  * every warp transforms its own pair of rows (one complex sequence) with a
+//    warp-synchronous radix-4/2 Stockham FFT whose sizes are compile-time
+//    constants, and keeps the masked spectrum sums of its rows in registers;
+//  * one CTA barrier per slice releases the slot to the next copy.
+// Waits on the ring are bounded: a wait that gives up sets the device error
+// word; the CTA then drains its copies in flight and returns without writing.
+// ---------------------------------------------------------------------------
+constexpr int kPfdrStages = 3;
+constexpr int kPfdrWarps = kPfdrRows / 2;
+
+template <int N>
+__device__ __forceinline__ void warp_fft(float2* a, float2* b, const float2* __restrict__ tw, float sign, int lane)
+{
+    // Stockham radix-4 stages, then one radix-2 stage when log2(N) is odd;
+    // tw[m] = exp(-2 pi i m / N).  Result in a.
+    float2* src = a;
+    float2* dst = b;
+    int Ns = 1;
+#pragma unroll
+    for (int s = 0; (1 << (2 * s + 2)) <= N; s++) {
+        constexpr int nbf = N / 4;
+        const int twstep = N / (Ns * 4);
+#pragma unroll
+        for (int j = lane; j < nbf; j += 32) {
+            const int k = j & (Ns - 1);
+            float2 v[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                float2 x = src[j + r * nbf];
+                if (r && k) {
+                    float2 w = tw[(r * k * twstep) & (N - 1)];
+                    w.y *= -sign;
+                    x = cmul(x, w);
+                }
+                v[r] = x;
+            }
+            const float2 s02 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+            const float2 d02 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+            const float2 s13 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+            const float2 d13 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+            const float2 jd13 = make_float2(-sign * d13.y, sign * d13.x);
+            const int idx = (j - k) * 4 + k;
+            dst[idx] = make_float2(s02.x + s13.x, s02.y + s13.y);
+            dst[idx + Ns] = make_float2(d02.x + jd13.x, d02.y + jd13.y);
+            dst[idx + 2 * Ns] = make_float2(s02.x - s13.x, s02.y - s13.y);
+            dst[idx + 3 * Ns] = make_float2(d02.x - jd13.x, d02.y - jd13.y);
+        }
+        __syncwarp();
+        float2* t = src;
+        src = dst;
+        dst = t;
+        Ns *= 4;
+    }
+    if (Ns < N) {  // radix-2 stage
+        constexpr int nbf = N / 2;
+        const int twstep = N / (Ns * 2);
+#pragma unroll
+        for (int j = lane; j < nbf; j += 32) {
+            const int k = j & (Ns - 1);
+            float2 x0 = src[j], x1 = src[j + nbf];
+            if (k) {
+                float2 w = tw[(k * twstep) & (N - 1)];
+                w.y *= -sign;
+                x1 = cmul(x1, w);
+            }
+            const int idx = (j - k) * 2 + k;
+            dst[idx] = make_float2(x0.x + x1.x, x0.y + x1.y);
+            dst[idx + Ns] = make_float2(x0.x - x1.x, x0.y - x1.y);
+        }
+        __syncwarp();
+        float2* t = src;
+        src = dst;
+        dst = t;
+    }
+    if (src != a) {
+        for (int i = lane; i < N; i += 32) a[i] = src[i];
+        __syncwarp();
+    }
+}
+
+template <int NX>
+__global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, int* err)
+{
+    constexpr int NXH = NX / 2 + 1;
+    constexpr int KPL = (NXH + 31) / 32;  // spectrum bins per lane
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int N_u0 = A.N_u0;
+    const int stage_floats = kPfdrRows * N_u0;
+    float* stage = reinterpret_cast<float*>(smraw);                                   // [S][rows][N_u0]
+    float2* wbuf = reinterpret_cast<float2*>(stage + kPfdrStages * stage_floats);     // [warps][2][NX]
+    float2* tw = wbuf + kPfdrWarps * 2 * NX;                                          // [NX]
+    uint64_t* full = reinterpret_cast<uint64_t*>(tw + NX);                           // [S]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int iv0 = blockIdx.x;
+    const int iu1_0 = blockIdx.y * kPfdrRows;
+    const int nrows = min(kPfdrRows, A.N_u1 - iu1_0);
+    const uint32_t bytes = uint32_t(nrows) * uint32_t(N_u0) * 4u;
+    const size_t slab = size_t(A.N_v0) * A.N_u1 * N_u0;
+    const float* base = A.g + (size_t(iv0) * A.N_u1 + iu1_0) * N_u0;
+    for (int i = tid; i < NX; i += blockDim.x) tw[i] = A.tw[i];
+    if (tid == 0) {
+        for (int q = 0; q < kPfdrStages; q++) mbar_init(&full[q], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int j = 0; j < kPfdrStages && j < A.N_v1; j++) {
+            mbar_arrive_expect_tx(&full[j], bytes);
+            bulk_load(stage + j * stage_floats, base + size_t(j) * slab, bytes, &full[j]);
+        }
+    float2* a = wbuf + warp * 2 * NX;
+    float2* b = a + NX;
+    const int r0 = 2 * warp, r1 = 2 * warp + 1;  // rows of this warp's sequence
+    float absU[KPL];
+    float2 acc0[KPL], acc1[KPL];
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+        const int k = lane + 32 * m;
+        absU[m] = k < NXH ? A.absU[k] : 0.0f;
+        acc0[m] = make_float2(0.f, 0.f);
+        acc1[m] = make_float2(0.f, 0.f);
+    }
+    bool dead = false;
+    int j = 0;
+    for (; j < A.N_v1; j++) {
+        const int slot = j % kPfdrStages;
+        if (!dead) dead = !mbar_wait(&full[slot], uint32_t((j / kPfdrStages) & 1), err);
+        if (!dead) {
+            const float w = A.row_w[j * A.N_v0 + iv0];
+            const float* s = stage + slot * stage_floats;
+            for (int i = lane; i < NX; i += 32) {
+                float re = 0.f, im = 0.f;
+                if (i < N_u0) {
+                    if (r0 < nrows) re = s[r0 * N_u0 + i] * w;
+                    if (r1 < nrows) im = s[r1 * N_u0 + i] * w;
+                }
+                a[i] = make_float2(re, im);
+            }
+        }
+        // the slot has been read: the copy of slice j + S may start
+        if (__syncthreads_or(dead)) break;
+        if (tid == 0 && j + kPfdrStages < A.N_v1) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&full[slot], bytes);
+            bulk_load(stage + slot * stage_floats, base + size_t(j + kPfdrStages) * slab, bytes, &full[slot]);
+        }
+        __syncwarp();
+        warp_fft<NX>(a, b, tw, -1.0f, lane);
+        // split the two real spectra and accumulate the masked bins
+        const bool cen = A.central[j] != 0;
+        const float thr = A.v1ap[j];
+#pragma unroll
+        for (int m = 0; m < KPL; m++) {
+            const int k = lane + 32 * m;
+            if (k < NXH && (cen || absU[m] > thr)) {
+                const float2 z = a[k];
+                const float2 zc = a[k == 0 ? 0 : NX - k];
+                acc0[m].x += 0.5f * (z.x + zc.x);
+                acc0[m].y += 0.5f * (z.y - zc.y);
+                acc1[m].x += 0.5f * (z.y + zc.y);
+                acc1[m].y += -0.5f * (z.x - zc.x);
+            }
+        }
+        __syncwarp();
+    }
+    if (j < A.N_v1) {
+        // a wait gave up: drain the copies in flight (slices j .. j + S - 1), write nothing
+        if (tid == 0)
+            for (int q = j; q < j + kPfdrStages && q < A.N_v1; q++)
+                mbar_wait(&full[q % kPfdrStages], uint32_t((q / kPfdrStages) & 1), nullptr);
+        return;
+    }
+    // normalise and pack the two rows into one inverse transform, A + iB:
+    // the lane holding bin k writes bin k and its Hermitian image NX - k
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+        const int k = lane + 32 * m;
+        if (k < NXH) {
+            const float nr = A.norm[k];
+            float2 x = make_float2(acc0[m].x * nr, acc0[m].y * nr), y = make_float2(acc1[m].x * nr, acc1[m].y * nr);
+            const bool edge = k == 0 || 2 * k == NX;
+            if (edge) {  // C2R ignores these imaginary parts
+                x.y = 0.f;
+                y.y = 0.f;
+            }
+            a[k] = make_float2(x.x - y.y, x.y + y.x);
+            if (!edge) a[NX - k] = make_float2(x.x - (-y.y), (-x.y) + y.x);  // conjugates of both spectra
+        }
+    }
+    __syncwarp();
+    warp_fft<NX>(a, b, tw, 1.0f, lane);
+    const float ow = A.out_w[iv0];
+    for (int i = lane; i < N_u0; i += 32) {
+        const float2 z = a[i];
+        if (r0 < nrows) A.g_reb[(size_t(iv0) * A.N_u1 + iu1_0 + r0) * N_u0 + i] = z.x * ow;
+        if (r1 < nrows) A.g_reb[(size_t(iv0) * A.N_u1 + iu1_0 + r1) * N_u0 + i] = z.y * ow;
+    }
+}
+
+template <int NX>
+cudaError_t launch_pfdr_stream(const PfdrArgs& A, cudaStream_t st)
+{
+    int* err = device_error_ptr();
+    if (!err) return cudaErrorUnknown;
+    const size_t smem = size_t(kPfdrStages) * kPfdrRows * A.N_u0 * 4 + sizeof(float2) * (size_t(kPfdrWarps) * 2 * NX + NX) +
+                        sizeof(uint64_t) * kPfdrStages;
+    cudaError_t e = cudaFuncSetAttribute(k_pfdr_stream<NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    dim3 grid(A.N_v0, ceil_div(A.N_u1, kPfdrRows));
+    k_pfdr_stream<NX><<<grid, kPfdrThreads, smem, st>>>(A, err);
+    note_launch();
+    return cudaGetLastError();
+}
+
 // direct convolution of every row with the ramp kernel, times a per-view weight
 constexpr int kRampRows = 8;
 __global__ void __launch_bounds__(256)
@@ -321,14 +547,24 @@ int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
         return rc;
     A.absU = d_absU; A.v1ap = d_v1ap; A.row_w = d_roww; A.norm = d_norm; A.out_w = d_outw; A.central = d_central;
     A.tw = d_tw;
-    const size_t smem = sizeof(float2) * (size_t(2 * (kPfdrRows / 2) * NX) + size_t(kPfdrRows) * NXH + NX) +
-                        sizeof(float) * NXH;
-    cudaError_t e = cudaFuncSetAttribute(k_pfdr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) {
-        dim3 grid(G.N_v0, ceil_div(G.N_u1, kPfdrRows));
-        k_pfdr<<<grid, kPfdrThreads, smem, st>>>(A);
-        e = cudaGetLastError();
-        note_launch();
+    // the streamed kernel: bulk copies need 16-byte aligned rows of slices
+    const bool rows_ok = (G.N_u0 % 4) == 0 && (reinterpret_cast<uintptr_t>(g) & 15) == 0 && G.N_u0 <= NX &&
+                         dispatch_mode() != 2;  // dispatch 2: the first-generation kernel
+    cudaError_t e = cudaErrorNotSupported;
+    if (rows_ok && NX == 128) e = launch_pfdr_stream<128>(A, st);
+    else if (rows_ok && NX == 256) e = launch_pfdr_stream<256>(A, st);
+    else if (rows_ok && NX == 512) e = launch_pfdr_stream<512>(A, st);
+    else if (rows_ok && NX == 1024) e = launch_pfdr_stream<1024>(A, st);
+    else {
+        const size_t smem = sizeof(float2) * (size_t(2 * (kPfdrRows / 2) * NX) + size_t(kPfdrRows) * NXH + NX) +
+                            sizeof(float) * NXH;
+        e = cudaFuncSetAttribute(k_pfdr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e == cudaSuccess) {
+            dim3 grid(G.N_v0, ceil_div(G.N_u1, kPfdrRows));
+            k_pfdr<<<grid, kPfdrThreads, smem, st>>>(A);
+            e = cudaGetLastError();
+            note_launch();
+        }
     }
     cudaFreeAsync(d_absU, st); cudaFreeAsync(d_v1ap, st); cudaFreeAsync(d_roww, st); cudaFreeAsync(d_norm, st);
     cudaFreeAsync(d_outw, st); cudaFreeAsync(d_central, st); cudaFreeAsync(d_tw, st);

@@ -5,13 +5,20 @@
 // PCIe on every iteration.  Here a worker thread owns the device:
 //
 //  * admission: a submitted request waits until its device footprint (data,
-//    ratio, image, backprojection, one sensitivity image per subset, shift
-//    tables) fits the HBM budget next to the requests already running and a
-//    slot is free; then its data is copied in once and stays resident;
+//    ratio, image, backprojection, projector scratch) fits the HBM budget next
+//    to the requests already running and a slot is free; then its data is
+//    copied in once and stays resident;
+//  * requests of like geometry share their geometry's state: the per-subset
+//    sensitivity images P_s^T 1 and the projector shift tables are computed
+//    once per (geometry, subset count), kept in a cache that counts against
+//    the budget (idle entries are evicted oldest first when memory is
+//    needed), and reused by every later request of that geometry;
 //  * continuous batching: every active request has its own CUDA stream, and
 //    the worker keeps up to `depth` OSEM subset steps in flight per request,
-//    issuing round-robin, so steps of different requests overlap on the GPU
-//    and new requests join while others run;
+//    issued oldest request first while the work in flight is under a cap of
+//    about two full-size steps: large requests run nearly in arrival order
+//    (the GPU is full with one of them), small ones overlap with them and
+//    with each other, and new requests join while others run;
 //  * completion: after the last step the image is copied to a pinned host
 //    buffer, the device memory is returned to the stream-ordered pool and
 //    the request's latency (submit to result on the host) is recorded;
@@ -76,6 +83,37 @@ unsigned blocks_for(long long n) { return unsigned(std::min<long long>((n + 255)
 
 enum State { kPending = 0, kActive = 1, kDone = 2, kFailed = 3 };
 
+// Geometry state shared by the requests of one (geometry, subset count).
+struct GeomState {
+    std::string key;
+    float* sens = nullptr;  // [subsets][numZ][numY][numX], zeros -> 1
+    shear::TableBuf tables;
+    bool shear = false;
+    cudaEvent_t ready = nullptr;  // recorded after the state was computed
+    size_t bytes = 0;
+    int users = 0;
+    unsigned long long last_use = 0;
+};
+
+std::string geom_key(const petl_geom& G, int subsets)
+{
+    std::string k(reinterpret_cast<const char*>(&G), sizeof(petl_geom));
+    k.append(reinterpret_cast<const char*>(&subsets), sizeof(int));
+    return k;
+}
+
+size_t state_bytes(const petl_geom& G, int subsets)
+{
+    const size_t nv = size_t(G.numX) * G.numY * G.numZ;
+    return 4 * nv * size_t(subsets) + shear::table_bytes(G) + 4096;
+}
+
+// work of one subset step: rays x planes
+double step_work(const petl_geom& G, int subsets)
+{
+    return double(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0 * double(G.numY) / double(subsets);
+}
+
 struct Request {
     long long id = 0;
     petl_geom G{};
@@ -90,9 +128,9 @@ struct Request {
     size_t bytes = 0;
     // device state
     cudaStream_t st = nullptr;
-    float *g = nullptr, *ratio = nullptr, *f = nullptr, *d = nullptr, *sens = nullptr;
-    shear::TableBuf tables;
-    bool shear = false;
+    float *g = nullptr, *ratio = nullptr, *f = nullptr, *d = nullptr;
+    std::shared_ptr<GeomState> gs;  // sensitivities and tables of the geometry
+    double work = 0;                // of one subset step
     int steps_total = 0, steps_issued = 0;
     std::deque<cudaEvent_t> inflight;  // one event per issued step
     cudaEvent_t result_ev = nullptr;
@@ -108,7 +146,7 @@ size_t footprint(const petl_geom& G, int subsets)
     const size_t views = (size_t(G.N_v0) + size_t(subsets) - 1) / size_t(subsets);
     const size_t per_view = size_t(G.numY) * G.numZ * ((size_t(G.N_u0) + 3) & ~size_t(3)) * 4;
     const size_t scratch = std::min(views * per_view, std::max(per_view, shear::split_scratch_budget()));
-    return 4 * (2 * ng + (2 + size_t(subsets)) * nv) + shear::table_bytes(G) + scratch + (size_t(1) << 20);
+    return 4 * (2 * ng + 2 * nv) + scratch + (size_t(1) << 20);
 }
 
 }  // namespace
@@ -127,9 +165,51 @@ struct Server {
     double in_use = 0, peak = 0;
     long long completed = 0, failed = 0;
     std::thread worker;
+    // geometry states (worker thread only; their bytes count in in_use)
+    std::map<std::string, std::shared_ptr<GeomState>> states;
+    unsigned long long use_clock = 0;
+    cudaStream_t aux = nullptr;  // frees evicted states
+    double work_cap = 0;
+    // reused per-request resources: streams (worker thread only) and pinned
+    // result buffers by size (worker and waiters, under pool_mu); creating
+    // a stream and page-locking a result per request cost milliseconds of
+    // the worker's time each
+    std::vector<cudaStream_t> free_streams;
+    std::mutex pool_mu;
+    std::multimap<size_t, float*> free_host;
+    size_t free_host_bytes = 0;
+
+    float* take_host(size_t bytes)
+    {
+        {
+            std::lock_guard<std::mutex> lk(pool_mu);
+            auto it = free_host.find(bytes);
+            if (it != free_host.end()) {
+                float* p = it->second;
+                free_host.erase(it);
+                free_host_bytes -= bytes;
+                return p;
+            }
+        }
+        float* p = nullptr;
+        return cudaHostAlloc(reinterpret_cast<void**>(&p), bytes, cudaHostAllocDefault) == cudaSuccess ? p : nullptr;
+    }
+    void give_host(float* p, size_t bytes)
+    {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(pool_mu);
+        if (free_host_bytes + bytes > (size_t(4) << 30)) {  // keep at most 4 GB page-locked
+            cudaFreeHost(p);
+            return;
+        }
+        free_host.emplace(bytes, p);
+        free_host_bytes += bytes;
+    }
 
     void run();
     void drop_expired_pending();
+    bool evict_idle_states(double need);
+    bool build_state(Request& r, GeomState& e);
     bool admit(Request& r);
     bool issue_step(Request& r);
     void release(Request& r);
@@ -178,47 +258,112 @@ void Server::drop_expired_pending()
     }
 }
 
+// Frees idle geometry states, least recently used first, until `need` more
+// bytes fit the budget; false if they cannot be made to fit.
+bool Server::evict_idle_states(double need)
+{
+    while (in_use + need > budget) {
+        std::shared_ptr<GeomState> victim;
+        for (auto& kv : states)
+            if (kv.second->users == 0 && (!victim || kv.second->last_use < victim->last_use)) victim = kv.second;
+        if (!victim) return false;
+        // its users have finished (their streams were synchronised): free it
+        if (victim->sens) cudaFreeAsync(victim->sens, aux);
+        if (victim->tables.base) cudaFreeAsync(victim->tables.base, aux);
+        if (victim->ready) cudaEventDestroy(victim->ready);
+        in_use -= double(victim->bytes);
+        states.erase(victim->key);
+    }
+    return true;
+}
+
+// Sensitivities P_s^T 1 (zeros -> 1) and tables of a geometry, on the
+// stream of the request that first needs them.
+bool Server::build_state(Request& r, GeomState& e)
+{
+    const petl_geom& G = r.G;
+    const long long ng = (long long)G.N_v1 * G.N_v0 * G.N_u1 * G.N_u0;
+    const long long nv = (long long)G.numX * G.numY * G.numZ;
+    bool ok = scratch_alloc(reinterpret_cast<void**>(&e.sens), nv * 4 * r.subsets, r.st) == cudaSuccess;
+    e.shear = shear_eligible(G);
+    if (ok && e.shear) ok = shear::make_tables(G, e.tables, r.st) == 0;
+    if (!ok) return false;
+    k_fill<<<blocks_for(ng), 256, 0, r.st>>>(r.ratio, ng, 1.0f);
+    note_launch();
+    for (int s = 0; s < r.subsets && ok; s++) {
+        const ViewRange vr{0, G.N_v1, s, r.subsets};
+        float* sv = e.sens + size_t(s) * nv;
+        const int rc = e.shear ? shear::backproject_with(G, r.ratio, sv, PETL_BP_REFERENCE, 0, 1.0f, vr, e.tables.T, r.st)
+                               : backproject_range(G, r.ratio, sv, PETL_BP_REFERENCE, 0, 1.0f, vr, r.st);
+        ok = rc == 0;
+        k_zero_to_one<<<blocks_for(nv), 256, 0, r.st>>>(sv, nv);
+        note_launch();
+    }
+    return ok && cudaEventCreateWithFlags(&e.ready, cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventRecord(e.ready, r.st) == cudaSuccess;
+}
+
 bool Server::admit(Request& r)
 {
     // device buffers and the data copy, all on the request's stream
     const petl_geom& G = r.G;
     const long long ng = (long long)G.N_v1 * G.N_v0 * G.N_u1 * G.N_u0;
     const long long nv = (long long)G.numX * G.numY * G.numZ;
-    if (stream_for(&r.st)) {
+    if (!free_streams.empty()) {
+        r.st = free_streams.back();
+        free_streams.pop_back();
+    } else if (stream_for(&r.st)) {
         fail(r, "cannot create a stream");
         return false;
     }
+    r.out_host = take_host(size_t(nv) * 4);
     bool ok = scratch_alloc(reinterpret_cast<void**>(&r.g), ng * 4, r.st) == cudaSuccess &&
               scratch_alloc(reinterpret_cast<void**>(&r.ratio), ng * 4, r.st) == cudaSuccess &&
               scratch_alloc(reinterpret_cast<void**>(&r.f), nv * 4, r.st) == cudaSuccess &&
-              scratch_alloc(reinterpret_cast<void**>(&r.d), nv * 4, r.st) == cudaSuccess &&
-              scratch_alloc(reinterpret_cast<void**>(&r.sens), nv * 4 * r.subsets, r.st) == cudaSuccess &&
-              cudaHostAlloc(reinterpret_cast<void**>(&r.out_host), nv * 4, cudaHostAllocDefault) == cudaSuccess;
+              scratch_alloc(reinterpret_cast<void**>(&r.d), nv * 4, r.st) == cudaSuccess && r.out_host != nullptr;
+    if (!ok) {
+        cudaGetLastError();
+        fail(r, "admission failed: out of memory");
+        return false;
+    }
+    // the geometry's shared state: reuse it, or build it here
+    const std::string key = geom_key(G, r.subsets);
+    auto it = states.find(key);
+    if (it != states.end()) {
+        r.gs = it->second;
+        r.gs->users++;  // released in release()
+        ok = cudaStreamWaitEvent(r.st, r.gs->ready, 0) == cudaSuccess;
+    } else {
+        auto e = std::make_shared<GeomState>();
+        e->key = key;
+        e->bytes = state_bytes(G, r.subsets);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            in_use += double(e->bytes);
+        }
+        ok = build_state(r, *e);
+        if (ok) {
+            states[key] = e;
+            r.gs = e;
+            r.gs->users++;  // released in release()
+        } else {
+            if (e->sens) cudaFreeAsync(e->sens, r.st);
+            if (e->tables.base) cudaFreeAsync(e->tables.base, r.st);
+            if (e->ready) cudaEventDestroy(e->ready);
+            std::lock_guard<std::mutex> lk(mu);
+            in_use -= double(e->bytes);
+        }
+    }
     ok = ok && cudaMemcpyAsync(r.g, r.g_host, ng * 4, cudaMemcpyHostToDevice, r.st) == cudaSuccess;
-    r.shear = shear_eligible(G);
-    if (ok && r.shear) ok = shear::make_tables(G, r.tables, r.st) == 0;
     if (!ok) {
         fail(r, "admission failed: " + std::string(cudaGetErrorString(cudaGetLastError())));
         return false;
     }
-    // image starts at 1; per-subset sensitivities P_s^T 1 with zeros -> 1
+    r.gs->last_use = ++use_clock;
+    // image starts at 1
     k_fill<<<blocks_for(nv), 256, 0, r.st>>>(r.f, nv, 1.0f);
-    k_fill<<<blocks_for(ng), 256, 0, r.st>>>(r.ratio, ng, 1.0f);
     note_launch();
-    note_launch();
-    for (int s = 0; s < r.subsets && ok; s++) {
-        const ViewRange vr{0, G.N_v1, s, r.subsets};
-        float* sv = r.sens + size_t(s) * nv;
-        const int rc = r.shear ? shear::backproject_with(G, r.ratio, sv, PETL_BP_REFERENCE, 0, 1.0f, vr, r.tables.T, r.st)
-                               : backproject_range(G, r.ratio, sv, PETL_BP_REFERENCE, 0, 1.0f, vr, r.st);
-        ok = rc == 0;
-        k_zero_to_one<<<blocks_for(nv), 256, 0, r.st>>>(sv, nv);
-        note_launch();
-    }
-    if (!ok) {
-        fail(r, "sensitivity failed");
-        return false;
-    }
+    r.work = step_work(G, r.subsets);
     r.steps_total = r.iters * r.subsets;
     r.state = kActive;
     r.t_admit = Clock::now();
@@ -231,16 +376,17 @@ bool Server::issue_step(Request& r)
     const long long nv = (long long)G.numX * G.numY * G.numZ;
     const int s = r.steps_issued % r.subsets;
     const ViewRange vr{0, G.N_v1, s, r.subsets};
-    int rc = r.shear ? shear::project_with(G, r.f, r.ratio, vr, r.g, r.tables.T, r.st)
+    const GeomState& e = *r.gs;
+    int rc = e.shear ? shear::project_with(G, r.f, r.ratio, vr, r.g, e.tables.T, r.st)
                      : project_range(G, r.f, r.ratio, vr, r.g, r.st);
     if (!rc)
-        rc = r.shear ? shear::backproject_with(G, r.ratio, r.d, PETL_BP_REFERENCE, 0, 1.0f, vr, r.tables.T, r.st)
+        rc = e.shear ? shear::backproject_with(G, r.ratio, r.d, PETL_BP_REFERENCE, 0, 1.0f, vr, e.tables.T, r.st)
                      : backproject_range(G, r.ratio, r.d, PETL_BP_REFERENCE, 0, 1.0f, vr, r.st);
     if (rc) {
         fail(r, "OSEM step failed");
         return false;
     }
-    k_mlem<<<blocks_for(nv), 256, 0, r.st>>>(r.f, r.d, r.sens + size_t(s) * nv, nv);
+    k_mlem<<<blocks_for(nv), 256, 0, r.st>>>(r.f, r.d, e.sens + size_t(s) * nv, nv);
     note_launch();
     cudaEvent_t ev;
     cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -261,31 +407,37 @@ void Server::release(Request& r)
         if (r.ratio) cudaFreeAsync(r.ratio, r.st);
         if (r.f) cudaFreeAsync(r.f, r.st);
         if (r.d) cudaFreeAsync(r.d, r.st);
-        if (r.sens) cudaFreeAsync(r.sens, r.st);
-        if (r.tables.base) cudaFreeAsync(r.tables.base, r.st);
         cudaStreamSynchronize(r.st);
-        cudaStreamDestroy(r.st);
+        free_streams.push_back(r.st);
     }
-    r.g = r.ratio = r.f = r.d = r.sens = nullptr;
-    r.tables.base = nullptr;
+    if (r.gs) r.gs->users--;  // the use taken in admit()
+    r.gs = nullptr;
+    r.g = r.ratio = r.f = r.d = nullptr;
     r.st = nullptr;
 }
 
 void Server::run()
 {
     cudaSetDevice(device);
+    cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking);
     while (true) {
         std::vector<std::shared_ptr<Request>> to_admit;
         {
             std::unique_lock<std::mutex> lk(mu);
             if (stop) break;
             drop_expired_pending();
-            // admission by HBM budget and free slots, in arrival order
+            // admission by HBM budget and free slots, in arrival order; a
+            // geometry seen before needs no new state
             while (!pending.empty() && int(active.size() + to_admit.size()) < max_active) {
                 auto& r = pending.front();
-                if (in_use + double(r->bytes) > budget && !(active.empty() && to_admit.empty())) break;
+                bool known = states.count(geom_key(r->G, r->subsets)) != 0;
+                for (auto& q : to_admit) known = known || (q->G.N_v0 == r->G.N_v0 &&
+                                                            geom_key(q->G, q->subsets) == geom_key(r->G, r->subsets));
+                const double need = double(r->bytes) + (known ? 0.0 : double(state_bytes(r->G, r->subsets)));
+                const bool alone = active.empty() && to_admit.empty();
+                if (in_use + need > budget && !evict_idle_states(need) && !alone) break;
                 in_use += double(r->bytes);
-                peak = std::max(peak, in_use);
+                peak = std::max(peak, in_use + (known ? 0.0 : double(state_bytes(r->G, r->subsets))));
                 to_admit.push_back(r);
                 pending.pop_front();
             }
@@ -304,8 +456,7 @@ void Server::run()
             active.push_back(r);
         }
         bool progressed = !to_admit.empty();
-        // retire finished steps, issue new ones round-robin
-        const Clock::time_point now = Clock::now();
+        // retire finished steps
         for (auto& rp : active) {
             Request& r = *rp;
             while (!r.inflight.empty() && cudaEventQuery(r.inflight.front()) == cudaSuccess) {
@@ -313,6 +464,20 @@ void Server::run()
                 r.inflight.pop_front();
                 progressed = true;
             }
+        }
+        // issue new steps, oldest request first, while the work in flight is
+        // under the cap (the oldest request may always keep `depth` steps)
+        double inflight_work = 0;
+        double biggest = 0;
+        for (auto& rp : active) {
+            inflight_work += double(rp->inflight.size()) * rp->work;
+            biggest = std::max(biggest, rp->work);
+        }
+        const double cap = std::max(work_cap, 2.0 * biggest);
+        const Clock::time_point now = Clock::now();
+        bool oldest = true;
+        for (auto& rp : active) {
+            Request& r = *rp;
             if (r.state == kActive && !r.result_issued) {
                 const char* why = nullptr;
                 {
@@ -325,10 +490,13 @@ void Server::run()
                     continue;
                 }
             }
-            if (r.state == kActive && !r.result_issued && r.steps_issued < r.steps_total &&
-                int(r.inflight.size()) < depth) {
-                if (issue_step(r)) progressed = true;
+            while (r.state == kActive && !r.result_issued && r.steps_issued < r.steps_total &&
+                   int(r.inflight.size()) < depth && (oldest || inflight_work + r.work <= cap)) {
+                if (!issue_step(r)) break;
+                inflight_work += r.work;
+                progressed = true;
             }
+            if (r.state == kActive) oldest = false;
             if (r.state == kActive && !r.result_issued && r.steps_issued == r.steps_total) {
                 const long long nv = (long long)r.G.numX * r.G.numY * r.G.numZ;
                 cudaMemcpyAsync(r.out_host, r.f, nv * 4, cudaMemcpyDeviceToHost, r.st);
@@ -384,6 +552,18 @@ void Server::run()
     // shutdown: drop whatever is left
     for (auto& rp : active) release(*rp);
     for (auto& rp : pending) rp->state = kFailed;
+    for (auto& kv : states) {
+        if (kv.second->sens) cudaFreeAsync(kv.second->sens, aux);
+        if (kv.second->tables.base) cudaFreeAsync(kv.second->tables.base, aux);
+        if (kv.second->ready) cudaEventDestroy(kv.second->ready);
+    }
+    states.clear();
+    if (aux) {
+        cudaStreamSynchronize(aux);
+        cudaStreamDestroy(aux);
+    }
+    for (cudaStream_t st : free_streams) cudaStreamDestroy(st);
+    free_streams.clear();
 }
 
 }  // namespace petl
@@ -439,7 +619,8 @@ int petl_server_submit_deadline(void* server, const petl_geom* G, const float* g
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        PETL_REQUIRE(double(r->bytes) <= s->budget, "server_submit: request larger than the HBM budget");
+        PETL_REQUIRE(double(r->bytes + state_bytes(*G, num_subsets)) <= s->budget,
+                     "server_submit: request larger than the HBM budget");
         r->id = s->next_id++;
         s->pending.push_back(r);
         s->all[r->id] = r;
@@ -474,7 +655,7 @@ int petl_server_wait(void* server, long long id, float* f_host, double* latency_
         set_error("server request failed: " + r->error);
         rc = -1;
     }
-    if (r->out_host) cudaFreeHost(r->out_host);
+    s->give_host(r->out_host, sizeof(float) * size_t(r->G.numX) * r->G.numY * r->G.numZ);
     r->out_host = nullptr;
     return rc;
 }
@@ -521,6 +702,7 @@ void petl_server_destroy(void* server)
     if (s->worker.joinable()) s->worker.join();
     for (auto& kv : s->all)
         if (kv.second->out_host) cudaFreeHost(kv.second->out_host);
+    for (auto& kv : s->free_host) cudaFreeHost(kv.second);
     delete s;
 }
 

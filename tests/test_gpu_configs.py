@@ -193,6 +193,15 @@ def test_config1_pfdr_fbp(cuda, cfg1):
     G, Go, z, g = cfg1["G"], cfg1["Go"], cfg1["z"], cfg1["g"]
     g_host = _np(g)
     reb = _np(ops.pfdr(G, g))
+    # the streamed kernel (default) and the first-generation one (dispatch 2)
+    # evaluate the same expressions (contracted into FMAs differently)
+    from petl_b200 import lib
+    assert lib().petl_set_dispatch(2) == 0
+    try:
+        reb2 = _np(ops.pfdr(G, g))
+    finally:
+        lib().petl_set_dispatch(0)
+    assert rel_l2(reb, reb2) < 1e-6
     want = O.pfdr(Go, g_host)
     assert rel_l2(reb, want) < 1e-5
     r = z["reb_views"]
