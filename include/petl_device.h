@@ -163,8 +163,8 @@ int petl_ray_trace_dev(const petl_geom* G, const petl_solid* solids, int n, floa
  * of the stream-ordered entry points here read it themselves. */
 int petl_device_error_flag(void);
 
-/* Failure-path hook; no counterpart in the reference.  The projector
- * kernels' waits on staged data give up after 2^22 polls: they set the error
+/* Failure-path hook; no counterpart in the reference.  The projector and
+ * PFDR kernels' waits on staged data give up after 2^22 polls: they set the error
  * word, drain their copies in flight (with the full bound) and return
  * without writing.  With on != 0 every such wait of the kernels launched
  * afterwards gives up before polling, which drives that path without a

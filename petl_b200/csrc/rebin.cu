@@ -25,6 +25,7 @@
 // fused with the inverse planogram weight that PETL::doFBP applies next
 // (src/planogram.cpp:304-333).
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -149,6 +150,13 @@ struct PfdrArgs {
     const float* out_w;    // [N_v0] sqrt(1+v0^2)
     const float2* tw;      // [NX] forward twiddles
     FFTPlan plan;
+    // streamed kernel: slices in processing order and the groups of one or
+    // two slices transformed together (slopes +v1 and -v1 share the mask and
+    // the normalisation, so their weighted rows are added before one
+    // transform: the transform is linear)
+    const int* order;      // [N_v1] slice of each load position
+    const int* gfirst;     // [ngroups + 1] first load position of each group
+    int ngroups;
 };
 
 __global__ void __launch_bounds__(kPfdrThreads) k_pfdr(const PfdrArgs A)
@@ -313,7 +321,7 @@ __device__ __forceinline__ void warp_fft(float2* a, float2* b, const float2* __r
 }
 
 template <int NX>
-__global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, int* err)
+__global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, int* err, unsigned wlim)
 {
     constexpr int NXH = NX / 2 + 1;
     constexpr int KPL = (NXH + 31) / 32;  // spectrum bins per lane
@@ -331,16 +339,19 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, 
     const uint32_t bytes = uint32_t(nrows) * uint32_t(N_u0) * 4u;
     const size_t slab = size_t(A.N_v0) * A.N_u1 * N_u0;
     const float* base = A.g + (size_t(iv0) * A.N_u1 + iu1_0) * N_u0;
+    const int nsl = A.N_v1;
     for (int i = tid; i < NX; i += blockDim.x) tw[i] = A.tw[i];
     if (tid == 0) {
         for (int q = 0; q < kPfdrStages; q++) mbar_init(&full[q], 1);
         fence_barrier_init();
     }
     __syncthreads();
+    // load position q (the q-th slice in processing order) goes to slot q % S
+    int issued = 0;  // meaningful in thread 0
     if (tid == 0)
-        for (int j = 0; j < kPfdrStages && j < A.N_v1; j++) {
-            mbar_arrive_expect_tx(&full[j], bytes);
-            bulk_load(stage + j * stage_floats, base + size_t(j) * slab, bytes, &full[j]);
+        for (; issued < kPfdrStages && issued < nsl; issued++) {
+            mbar_arrive_expect_tx(&full[issued], bytes);
+            bulk_load(stage + issued * stage_floats, base + size_t(A.order[issued]) * slab, bytes, &full[issued]);
         }
     float2* a = wbuf + warp * 2 * NX;
     float2* b = a + NX;
@@ -355,34 +366,43 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, 
         acc1[m] = make_float2(0.f, 0.f);
     }
     bool dead = false;
-    int j = 0;
-    for (; j < A.N_v1; j++) {
-        const int slot = j % kPfdrStages;
-        if (!dead) dead = !mbar_wait(&full[slot], uint32_t((j / kPfdrStages) & 1), err);
+    int gi = 0, q0 = 0;
+    for (; gi < A.ngroups; gi++) {
+        q0 = A.gfirst[gi];
+        const int q1 = A.gfirst[gi + 1];
+        for (int q = q0; q < q1 && !dead; q++)
+            dead = !mbar_wait(&full[q % kPfdrStages], uint32_t((q / kPfdrStages) & 1), err, wlim);
         if (!dead) {
-            const float w = A.row_w[j * A.N_v0 + iv0];
-            const float* s = stage + slot * stage_floats;
             for (int i = lane; i < NX; i += 32) {
                 float re = 0.f, im = 0.f;
                 if (i < N_u0) {
-                    if (r0 < nrows) re = s[r0 * N_u0 + i] * w;
-                    if (r1 < nrows) im = s[r1 * N_u0 + i] * w;
+                    for (int q = q0; q < q1; q++) {
+                        const float w = A.row_w[A.order[q] * A.N_v0 + iv0];
+                        const float* st = stage + (q % kPfdrStages) * stage_floats;
+                        if (r0 < nrows) re += st[r0 * N_u0 + i] * w;
+                        if (r1 < nrows) im += st[r1 * N_u0 + i] * w;
+                    }
                 }
                 a[i] = make_float2(re, im);
             }
         }
-        // the slot has been read: the copy of slice j + S may start
+        // the group's slots have been read: later slices may be copied in
         if (__syncthreads_or(dead)) break;
-        if (tid == 0 && j + kPfdrStages < A.N_v1) {
+        if (tid == 0) {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&full[slot], bytes);
-            bulk_load(stage + slot * stage_floats, base + size_t(j + kPfdrStages) * slab, bytes, &full[slot]);
+            for (; issued < nsl && issued < q1 + kPfdrStages; issued++) {
+                const int slot = issued % kPfdrStages;
+                mbar_arrive_expect_tx(&full[slot], bytes);
+                bulk_load(stage + slot * stage_floats, base + size_t(A.order[issued]) * slab, bytes, &full[slot]);
+            }
         }
         __syncwarp();
         warp_fft<NX>(a, b, tw, -1.0f, lane);
-        // split the two real spectra and accumulate the masked bins
-        const bool cen = A.central[j] != 0;
-        const float thr = A.v1ap[j];
+        // split the two real spectra and accumulate the masked bins (the
+        // group's slices share the mask)
+        const int sl = A.order[q0];
+        const bool cen = A.central[sl] != 0;
+        const float thr = A.v1ap[sl];
 #pragma unroll
         for (int m = 0; m < KPL; m++) {
             const int k = lane + 32 * m;
@@ -397,11 +417,12 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, 
         }
         __syncwarp();
     }
-    if (j < A.N_v1) {
-        // a wait gave up: drain the copies in flight (slices j .. j + S - 1), write nothing
+    if (gi < A.ngroups) {
+        // a wait gave up: drain the copies in flight (load positions q0 ..
+        // issued - 1, at most S of them; thread 0 tracks `issued`), write
+        // nothing
         if (tid == 0)
-            for (int q = j; q < j + kPfdrStages && q < A.N_v1; q++)
-                mbar_wait(&full[q % kPfdrStages], uint32_t((q / kPfdrStages) & 1), nullptr);
+            for (int q = q0; q < issued; q++) mbar_wait(&full[q % kPfdrStages], uint32_t((q / kPfdrStages) & 1), nullptr);
         return;
     }
     // normalise and pack the two rows into one inverse transform, A + iB:
@@ -441,7 +462,7 @@ cudaError_t launch_pfdr_stream(const PfdrArgs& A, cudaStream_t st)
     cudaError_t e = cudaFuncSetAttribute(k_pfdr_stream<NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     dim3 grid(A.N_v0, ceil_div(A.N_u1, kPfdrRows));
-    k_pfdr_stream<NX><<<grid, kPfdrThreads, smem, st>>>(A, err);
+    k_pfdr_stream<NX><<<grid, kPfdrThreads, smem, st>>>(A, err, wait_limit());
     note_launch();
     return cudaGetLastError();
 }
@@ -547,6 +568,32 @@ int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
         return rc;
     A.absU = d_absU; A.v1ap = d_v1ap; A.row_w = d_roww; A.norm = d_norm; A.out_w = d_outw; A.central = d_central;
     A.tw = d_tw;
+    // processing order for the streamed kernel: slope iv1 with its mirror
+    // N_v1 - 1 - iv1 when both have bit-identical masks (central flag and
+    // threshold), else alone
+    std::vector<int> order, gfirst;
+    {
+        std::vector<char> done(G.N_v1, 0);
+        for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
+            if (done[iv1]) continue;
+            gfirst.push_back(int(order.size()));
+            order.push_back(iv1);
+            done[iv1] = 1;
+            const int m = G.N_v1 - 1 - iv1;
+            if (m != iv1 && !done[m] && central[m] == central[iv1] &&
+                std::memcmp(&v1ap[m], &v1ap[iv1], sizeof(float)) == 0) {
+                order.push_back(m);
+                done[m] = 1;
+            }
+        }
+        gfirst.push_back(int(order.size()));
+    }
+    int* d_order = nullptr;
+    int* d_gfirst = nullptr;
+    if ((rc = upload(order, &d_order, st)) || (rc = upload(gfirst, &d_gfirst, st))) return rc;
+    A.order = d_order;
+    A.gfirst = d_gfirst;
+    A.ngroups = int(gfirst.size()) - 1;
     // the streamed kernel: bulk copies need 16-byte aligned rows of slices
     const bool rows_ok = (G.N_u0 % 4) == 0 && (reinterpret_cast<uintptr_t>(g) & 15) == 0 && G.N_u0 <= NX &&
                          dispatch_mode() != 2;  // dispatch 2: the first-generation kernel
@@ -568,6 +615,7 @@ int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
     }
     cudaFreeAsync(d_absU, st); cudaFreeAsync(d_v1ap, st); cudaFreeAsync(d_roww, st); cudaFreeAsync(d_norm, st);
     cudaFreeAsync(d_outw, st); cudaFreeAsync(d_central, st); cudaFreeAsync(d_tw, st);
+    cudaFreeAsync(d_order, st); cudaFreeAsync(d_gfirst, st);
     if (e != cudaSuccess) {
         set_error(std::string("PFDR: ") + cudaGetErrorString(e));
         return int(e);

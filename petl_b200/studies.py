@@ -7,6 +7,7 @@
     python -m petl_b200.studies binning     # list-mode binning, device and C-ABI file rates
     python -m petl_b200.studies corrections # solid angle and apply_corrections, device and C ABI
     python -m petl_b200.studies response    # PET/X stopping power (120 blocks) and calc_response
+    python -m petl_b200.studies kernels     # PFDR, ramp, FBP, RD/TV stencils: device time, HBM fraction
 
 All inputs are synthetic and seeded: ellipsoid phantoms (replace semantics,
 later ellipsoids overwrite earlier ones), forward projected with the
@@ -109,6 +110,68 @@ def study_pipeline(seed=0):
     out["fbp_image_rel_l2_vs_phantom_fov_fitted_scale"] = _rel(img[fov] * a, f[fov])
     out["fbp_fitted_scale_over_data_scale"] = 1.0 / (a * scale)
     out["rebinned_shape"] = list(reb.shape)
+    return out
+
+
+def _peak_hbm_gbs():
+    import os
+    try:
+        with open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                               "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def study_kernels(seed=0, reps=10):
+    """Device time of the rebinning and regularizer kernels (CUDA events,
+    median of `reps`, the L2 flushed before each) with their algorithmic
+    bytes and the fraction of the measured HBM bandwidth: PFDR (reads the
+    planogram once, writes the rebinned one), the ramp filter (reads and
+    writes the rebinned planogram), FBP (PFDR + ramp + the N_v1 = 1
+    backprojection), and the RD / TV gradients (read the volume, write the
+    gradient) at 128x128x64 and 256x256x128."""
+    peak, kind = _peak_hbm_gbs()
+    flush = torch.empty(64 * 1024 * 1024, device="cuda")
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            with Timer() as t:
+                fn()
+            ts.append(t.ms)
+        return float(np.median(ts))
+
+    out = {"study": "kernels", "hbm_peak_gbs": peak, "hbm_peak_kind": kind}
+    for name, cfg in (("256x256x128", CFG1), ("128x128x64", CFG0)):
+        G = Geometry(*cfg["args"], volume=cfg["volume"])
+        rng = np.random.default_rng(seed)
+        f = phantom(G.vol_shape, (cfg["volume"][3],) * 2, rng, 12) + 0.01
+        y = ops.project(G, f)
+        Gr = G.rebinned()
+        reb = ops.pfdr(G, y)
+        nb_g, nb_r, nb_f = 4 * y.numel(), 4 * reb.numel(), 4 * f.numel()
+        r = {}
+        t = timed(lambda: ops.pfdr(G, y, reb))
+        r["pfdr_ms"], r["pfdr_hbm_frac"] = t, (nb_g + nb_r) / (t * 1e6) / peak
+        work = reb.clone()
+        t = timed(lambda: ops.ramp_(Gr, work))
+        r["ramp_ms"], r["ramp_hbm_frac"] = t, 2 * nb_r / (t * 1e6) / peak
+        t = timed(lambda: ops.fbp(G, y))
+        r["fbp_ms"] = t
+        Df = torch.empty_like(f)
+        t = timed(lambda: ops.rd_gradient(f, 2.0, 0.01, out=Df))
+        r["rd_gradient_ms"], r["rd_gradient_hbm_frac"] = t, 2 * nb_f / (t * 1e6) / peak
+        t = timed(lambda: ops.tv_gradient(f, 1e-4, 0.01, 1.0, out=Df))
+        r["tv_gradient_ms"], r["tv_gradient_hbm_frac"] = t, 2 * nb_f / (t * 1e6) / peak
+        t = timed(lambda: ops.tv_cost(f, 1e-4, 0.01, 1.0))
+        r["tv_cost_ms"], r["tv_cost_hbm_frac"] = t, nb_f / (t * 1e6) / peak
+        t = timed(lambda: ops.rd_cost(f, 2.0, 0.01))
+        r["rd_cost_ms"], r["rd_cost_hbm_frac"] = t, nb_f / (t * 1e6) / peak
+        r["planogram"], r["rebinned"], r["volume"] = list(G.shape), list(reb.shape), list(f.shape)
+        out[name] = r
     return out
 
 
@@ -457,12 +520,13 @@ def study_response(seed=0, reps=3):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("study", choices=["pipeline", "penalized", "storage", "serving", "binning", "corrections",
-                                      "response"])
+                                      "response", "kernels"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--requests", type=int, default=200)
     a = ap.parse_args(argv)
     fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
-          "binning": study_binning, "corrections": study_corrections, "response": study_response}
+          "binning": study_binning, "corrections": study_corrections, "response": study_response,
+          "kernels": study_kernels}
     if a.study == "serving":
         res = study_serving(n=a.requests, seed=a.seed)
     else:

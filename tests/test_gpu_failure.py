@@ -83,6 +83,19 @@ def test_bounded_waits_give_up_and_the_device_stays_usable(cuda, dispatch):
         L.petl_set_dispatch(0)
 
 
+def test_pfdr_wait_gives_up_and_recovers(cuda):
+    import torch
+    from petl_b200 import Geometry, lib, ops
+    G = Geometry(0.0, 256.0, 128.0, 128.0, 2.0, 0.5, 0.25, volume=(128, 128, 64, 2.0))
+    y = torch.rand(G.shape, device=cuda, generator=torch.Generator(device=cuda).manual_seed(3))
+    want = ops.pfdr(G, y)
+    torch.cuda.synchronize()
+    assert lib().petl_device_error_flag() == 0
+    _, flag = _timing_out(lambda: ops.pfdr(G, y))
+    assert flag == 1
+    assert torch.equal(ops.pfdr(G, y), want)
+
+
 def test_reference_calls_report_a_wait_that_gave_up(cuda):
     from petl_b200 import PETLserver, lib
     L = lib()
