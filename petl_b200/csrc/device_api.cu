@@ -46,6 +46,92 @@ bool range_ok(const petl_geom& G, const ViewRange& vr)
            vr.iv0_step >= 1;
 }
 
+// ---------------------------------------------------------------------------
+// psi = 90 degrees (the second planogram of PET/X, src/petx_server.py:9-10).
+// The reference takes its x-driven branch there (src/projectors.cu:77-130):
+// the ray through bin (u0, u1) of view (v0, v1) crosses the plane at x in
+// y = u0 + v0 x, z = u1 + v1 x, which is the psi = 0 (y-driven) ray of
+// plane t = -x on a volume whose axes are exchanged: x' = y, y' = -x.  The
+// projection is therefore the shear-warp projection of the transposed,
+// flipped volume f'[z][nx-1-ix][iy] = f[z][iy][ix] under the psi = 0
+// geometry with those axes (equal pitch in x and y, which the volume has),
+// and the backprojection is the flip of the shear-warp backprojection.  The
+// reference evaluates cos(pi/2) in float (-4.4e-8, not 0), which moves its
+// ray coordinates by parts in 1e8: the two agree to rounding.
+// ---------------------------------------------------------------------------
+namespace {
+
+bool psi90(const petl_geom& G)
+{
+    return std::fabs(G.cos_psi) < 1e-6f && G.sin_psi == 1.0f;
+}
+
+petl_geom transposed(const petl_geom& G)
+{
+    petl_geom T = G;
+    T.cos_psi = 1.0f;
+    T.sin_psi = 0.0f;
+    T.numX = G.numY;
+    T.numY = G.numX;
+    T.x_0 = G.y_0;
+    T.y_0 = -(G.x_0 + float(G.numX - 1) * G.T_x);
+    return T;
+}
+
+// dir 0: out[z][nx-1-ix][iy] = in[z][iy][ix] (in: nz x ny x nx)
+// dir 1: out[z][iy][ix] (+)= in[z][nx-1-ix][iy] (in: nz x nx x ny)
+__global__ void __launch_bounds__(256)
+k_flip_transpose(const float* __restrict__ in, float* __restrict__ out, int nx, int ny, int dir, int accumulate)
+{
+    __shared__ float tile[32][33];
+    const int z = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    if (dir == 0) {
+        const int ix0 = blockIdx.x * 32, iy0 = blockIdx.y * 32;
+        for (int r = ty; r < 32; r += 8) {
+            const int iy = iy0 + r, ix = ix0 + tx;
+            if (iy < ny && ix < nx) tile[r][tx] = in[(size_t(z) * ny + iy) * nx + ix];
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int ix = ix0 + r, iy = iy0 + tx;  // out row nx-1-ix, column iy
+            if (iy < ny && ix < nx) out[(size_t(z) * nx + (nx - 1 - ix)) * ny + iy] = tile[tx][r];
+        }
+    } else {
+        const int iy0 = blockIdx.x * 32, r0 = blockIdx.y * 32;  // in: rows r = nx-1-ix, columns iy
+        for (int r = ty; r < 32; r += 8) {
+            const int row = r0 + r, iy = iy0 + tx;
+            if (row < nx && iy < ny) tile[r][tx] = in[(size_t(z) * nx + row) * ny + iy];
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int iy = iy0 + r, row = r0 + tx, ix = nx - 1 - row;
+            if (row < nx && iy < ny) {
+                const size_t o = (size_t(z) * ny + iy) * nx + ix;
+                const float v = tile[tx][r];
+                out[o] = accumulate ? out[o] + v : v;
+            }
+        }
+    }
+}
+
+int flip_transpose(const float* in, float* out, const petl_geom& G, int dir, int accumulate, cudaStream_t st)
+{
+    const dim3 block(32, 8);
+    const dim3 grid = dir == 0 ? dim3(ceil_div(G.numX, 32), ceil_div(G.numY, 32), unsigned(G.numZ))
+                               : dim3(ceil_div(G.numY, 32), ceil_div(G.numX, 32), unsigned(G.numZ));
+    k_flip_transpose<<<grid, block, 0, st>>>(in, out, G.numX, G.numY, dir, accumulate);
+    PETL_LAUNCH_CHECK("flip_transpose");
+    return 0;
+}
+
+bool use_psi90_shear(const petl_geom& G)
+{
+    return dispatch_mode() != 1 && psi90(G) && G.T_x == G.T_u0 && G.numZ <= 65535 && shear_eligible(transposed(G));
+}
+
+}  // namespace
+
 int project_range(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
                   cudaStream_t st)
 {
@@ -54,6 +140,15 @@ int project_range(const petl_geom& G, const float* f, float* g, const ViewRange&
     PETL_REQUIRE(f && g && range_ok(G, vr), "project: invalid arguments");
     if (vr.iv1_begin == vr.iv1_end || vr.iv0_first >= G.N_v0) return 0;
     if (use_shear(G)) return launch_project_shear(G, f, g, vr, meas, st);
+    if (use_psi90_shear(G)) {
+        const petl_geom T = transposed(G);
+        float* ft = nullptr;
+        PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(&ft), sizeof(float) * size_t(G.numX) * G.numY * G.numZ, st));
+        int rc = flip_transpose(f, ft, G, 0, 0, st);
+        if (!rc) rc = launch_project_shear(T, ft, g, vr, meas, st);
+        cudaFreeAsync(ft, st);
+        return rc;
+    }
     note_path(0);
     return launch_project_general(G, f, g, vr, meas, st);
 }
@@ -66,6 +161,15 @@ int backproject_range(const petl_geom& G, const float* g, float* f, int mode, in
     PETL_REQUIRE(f && g && range_ok(G, vr), "backproject: invalid arguments");
     PETL_REQUIRE(mode == PETL_BP_REFERENCE || mode == PETL_BP_ADJOINT, "backproject: unknown mode");
     if (use_shear(G)) return launch_backproject_shear(G, g, f, mode, accumulate, scale, vr, st);
+    if (use_psi90_shear(G)) {
+        const petl_geom T = transposed(G);
+        float* bt = nullptr;
+        PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(&bt), sizeof(float) * size_t(G.numX) * G.numY * G.numZ, st));
+        int rc = launch_backproject_shear(T, g, bt, mode, 0, scale, vr, st);
+        if (!rc) rc = flip_transpose(bt, f, G, 1, accumulate, st);
+        cudaFreeAsync(bt, st);
+        return rc;
+    }
     note_path(0);
     return launch_backproject_general(G, g, f, mode, accumulate, scale, vr, st);
 }

@@ -373,14 +373,22 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, 
         for (int q = q0; q < q1 && !dead; q++)
             dead = !mbar_wait(&full[q % kPfdrStages], uint32_t((q / kPfdrStages) & 1), err, wlim);
         if (!dead) {
+            // one or two slices: weights and staged rows hoisted out of the row loop
+            const bool two = q1 - q0 > 1;
+            const float w0 = A.row_w[A.order[q0] * A.N_v0 + iv0];
+            const float w1 = two ? A.row_w[A.order[q0 + 1] * A.N_v0 + iv0] : 0.0f;
+            const float* s0 = stage + (q0 % kPfdrStages) * stage_floats;
+            const float* s1 = stage + ((q0 + 1) % kPfdrStages) * stage_floats;
+            const int o0 = min(r0, nrows - 1) * N_u0, o1 = min(r1, nrows - 1) * N_u0;
+            const bool v0 = r0 < nrows, v1 = r1 < nrows;
             for (int i = lane; i < NX; i += 32) {
                 float re = 0.f, im = 0.f;
                 if (i < N_u0) {
-                    for (int q = q0; q < q1; q++) {
-                        const float w = A.row_w[A.order[q] * A.N_v0 + iv0];
-                        const float* st = stage + (q % kPfdrStages) * stage_floats;
-                        if (r0 < nrows) re += st[r0 * N_u0 + i] * w;
-                        if (r1 < nrows) im += st[r1 * N_u0 + i] * w;
+                    if (v0) re = s0[o0 + i] * w0;
+                    if (v1) im = s0[o1 + i] * w0;
+                    if (two) {
+                        if (v0) re += s1[o0 + i] * w1;
+                        if (v1) im += s1[o1 + i] * w1;
                     }
                 }
                 a[i] = make_float2(re, im);

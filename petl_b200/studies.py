@@ -172,6 +172,36 @@ def study_kernels(seed=0, reps=10):
         r["rd_cost_ms"], r["rd_cost_hbm_frac"] = t, nb_f / (t * 1e6) / peak
         r["planogram"], r["rebinned"], r["volume"] = list(G.shape), list(reb.shape), list(f.shape)
         out[name] = r
+    # projectors by planogram orientation at 256x256x128 (1 mm): psi = 0 and
+    # 90 run the shear-warp kernels (90 on the volume with x and y
+    # exchanged), psi = 30 the general kernels; FP32 fraction of 2 nnz(A)
+    # flops per call at the nominal rate (148 SM x 128 FMA/clk at 1965 MHz)
+    fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
+    from . import lib
+    for psi in (0.0, 90.0, 30.0):
+        G = Geometry(psi, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25, volume=(256, 256, 128, 1.0))
+        f = phantom(G.vol_shape, (1.0, 1.0), np.random.default_rng(seed), 12) + 0.01
+        g = torch.empty(G.shape, device="cuda")
+        b = torch.empty_like(f)
+        nnz = ops.nnz(G)
+        reps_p = reps if psi != 30.0 else 2
+        ops.project(G, f, g)
+        path = lib().petl_last_projector_path()
+        ts_f, ts_b = [], []
+        for _ in range(reps_p):
+            flush.zero_()
+            with Timer() as t:
+                ops.project(G, f, g)
+            ts_f.append(t.ms)
+            flush.zero_()
+            with Timer() as t:
+                ops.backproject(G, g, b)
+            ts_b.append(t.ms)
+        tf, tb = float(np.median(ts_f)), float(np.median(ts_b))
+        out[f"project_psi{int(psi)}"] = {"planogram": list(G.shape), "path": path, "forward_ms": tf,
+                                         "backward_ms": tb, "nnz": nnz,
+                                         "forward_fp32_frac": 2 * nnz / (tf * 1e-3) / 1e12 / fp32_peak,
+                                         "backward_fp32_frac": 2 * nnz / (tb * 1e-3) / 1e12 / fp32_peak}
     return out
 
 

@@ -41,6 +41,10 @@ CASES = {
     "wide": ((0.0, 300.0, 128.0, 32.0, 1.0, 0.5, 0.25), (256, 64, 32, 1.0), True, True),
     # and numX = 320 > 256
     "wide2": ((0.0, 300.0, 128.0, 32.0, 1.0, 0.5, 0.25), (320, 48, 16, 1.0), True, True),
+    # psi = 90 degrees (x-driven rays): the same kernels on the volume with x and
+    # y exchanged (y' = -x); square, and ragged with offsets (numX != numY)
+    "p90": ((90.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (64, 64, 16, 2.0), True, True),
+    "p90rag": ((90.0, 100.0, 75.0, 27.0, 1.5, 0.45, 0.2), (52, 60, 18, 1.5, 1.5, 3.0, -4.5, 1.5), True, True),
 }
 
 
@@ -116,7 +120,7 @@ def test_tma_backward(cuda, name, mode):
         assert rel_l2(a, O.backproject(Go, _np(y))) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["t1", "panel2mm", "rag4", "odd", "wide"])
+@pytest.mark.parametrize("name", ["t1", "panel2mm", "rag4", "odd", "wide", "p90", "p90rag"])
 def test_tma_pair_is_exact_adjoint(cuda, name):
     import torch
     from petl_b200 import ops
