@@ -20,7 +20,7 @@ namespace petl {
 // forward projection, one thread per ray
 // ---------------------------------------------------------------------------
 template <bool COUNT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl_geom G, const ViewRange vr,
                   int n_v0, unsigned long long* __restrict__ nnz, const float* __restrict__ meas)
 {
@@ -35,38 +35,49 @@ k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl
     if (inside && ray_visible(G, iv1, iv0, iu1, iu0)) {
         const RayGeom rg = ray_geom(G, iv1, iv0, iu1, iu0);
         const int Nx = G.numX, Ny = G.numY;
+        // per plane: the z weights of the (at most kZT) slices in range are
+        // computed once and reused for every in-plane tap; the taps, their
+        // order and their float operations are those of the tap-by-tap form
+        // (which remains for footprints spanning more slices)
+        constexpr int kZT = 4;
+        auto plane = [&](const PlaneTaps& pt, int plane_idx, bool xdr) {
+            const int nz = pt.z_max - pt.z_min + 1;
+            if (nz <= 0) return;
+            if (nz <= kZT) {
+                float wz[kZT];
+#pragma unroll
+                for (int q = 0; q < kZT; q++) wz[q] = q < nz ? tap_w1(G, rg, pt.t, pt.z_min + q, iu1) : 0.0f;
+                for (int a = pt.a_min; a <= pt.a_max; a++) {
+                    const float w0 = xdr ? tap_w0_x(G, rg, pt.t, a, iu0) : tap_w0_y(G, rg, pt.t, a, iu0);
+                    if (!(w0 > 0.0f)) continue;
+                    const int ix = xdr ? plane_idx : a, iy = xdr ? a : plane_idx;
+#pragma unroll
+                    for (int q = 0; q < kZT; q++) {
+                        if (q < nz && wz[q] > 0.0f) {
+                            if (COUNT) cnt++;
+                            else val = ffma(__ldg(&f[(size_t(pt.z_min + q) * Ny + iy) * Nx + ix]), fmul(w0, wz[q]), val);
+                        }
+                    }
+                }
+            } else {
+                for (int a = pt.a_min; a <= pt.a_max; a++) {
+                    const float w0 = xdr ? tap_w0_x(G, rg, pt.t, a, iu0) : tap_w0_y(G, rg, pt.t, a, iu0);
+                    if (!(w0 > 0.0f)) continue;
+                    const int ix = xdr ? plane_idx : a, iy = xdr ? a : plane_idx;
+                    for (int iz = pt.z_min; iz <= pt.z_max; iz++) {
+                        const float w1 = tap_w1(G, rg, pt.t, iz, iu1);
+                        if (w1 > 0.0f) {
+                            if (COUNT) cnt++;
+                            else val = ffma(__ldg(&f[(size_t(iz) * Ny + iy) * Nx + ix]), fmul(w0, w1), val);
+                        }
+                    }
+                }
+            }
+        };
         if (rg.xdriven) {
-            for (int ix = 0; ix < Nx; ix++) {
-                const PlaneTaps pt = plane_taps_x(G, rg, ix);
-                for (int iy = pt.a_min; iy <= pt.a_max; iy++) {
-                    const float w0 = tap_w0_x(G, rg, pt.t, iy, iu0);
-                    if (w0 > 0.0f) {
-                        for (int iz = pt.z_min; iz <= pt.z_max; iz++) {
-                            const float w1 = tap_w1(G, rg, pt.t, iz, iu1);
-                            if (w1 > 0.0f) {
-                                if (COUNT) cnt++;
-                                else val = ffma(__ldg(&f[(size_t(iz) * Ny + iy) * Nx + ix]), fmul(w0, w1), val);
-                            }
-                        }
-                    }
-                }
-            }
+            for (int ix = 0; ix < Nx; ix++) plane(plane_taps_x(G, rg, ix), ix, true);
         } else {
-            for (int iy = 0; iy < Ny; iy++) {
-                const PlaneTaps pt = plane_taps_y(G, rg, iy);
-                for (int ix = pt.a_min; ix <= pt.a_max; ix++) {
-                    const float w0 = tap_w0_y(G, rg, pt.t, ix, iu0);
-                    if (w0 > 0.0f) {
-                        for (int iz = pt.z_min; iz <= pt.z_max; iz++) {
-                            const float w1 = tap_w1(G, rg, pt.t, iz, iu1);
-                            if (w1 > 0.0f) {
-                                if (COUNT) cnt++;
-                                else val = ffma(__ldg(&f[(size_t(iz) * Ny + iy) * Nx + ix]), fmul(w0, w1), val);
-                            }
-                        }
-                    }
-                }
-            }
+            for (int iy = 0; iy < Ny; iy++) plane(plane_taps_y(G, rg, iy), iy, false);
         }
         val = fmul(fmul(val, rg.l_phi), rg.rs);
     }
@@ -87,7 +98,7 @@ k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl
 // src/projectors.cu:240-377: voxel-centre u1 visibility test, no u0 test,
 // border bins read as zero; f = sum_v1 T_x * sum_v0 ...
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 k_backproject_ref_general(const float* __restrict__ g, float* __restrict__ f, const petl_geom G, const ViewRange vr,
                           int accumulate, float scale)
 {
@@ -116,6 +127,16 @@ k_backproject_ref_general(const float* __restrict__ g, float* __restrict__ f, co
         const int iu1_min = int(ceilf(iu1_A - 0.5f));
         const int iu1_max = int(floorf(iu1_B + 0.5f));
         const float* gs = g + size_t(iv1) * slab;
+        // u1 weights of this slope's rows, the same for every view
+        constexpr int kUT = 4;
+        const int ua = max(iu1_min, 0), ub = min(iu1_max, G.N_u1 - 1);
+        const bool fewu = ub - ua + 1 <= kUT;
+        float w1s[kUT];
+#pragma unroll
+        for (int q = 0; q < kUT; q++) {
+            const int iu1 = ua + q;
+            w1s[q] = fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B) - fmaxf(float(iu1) - 0.5f, iu1_A));
+        }
         float val = 0.0f;
         for (int iv0 = vr.iv0_first; iv0 < G.N_v0; iv0 += vr.iv0_step) {
             const float v0 = fmaf(float(iv0), G.T_v0, G.v0_0);
@@ -138,15 +159,29 @@ k_backproject_ref_general(const float* __restrict__ g, float* __restrict__ f, co
             const int iu0_max = min(int(floorf(B + 0.5f)), G.N_u0 - 1);
             const float* gv = gs + size_t(iv0) * G.N_u1 * G.N_u0;
             float sv = 0.0f;
-            for (int iu1 = max(iu1_min, 0); iu1 <= min(iu1_max, G.N_u1 - 1); iu1++) {
-                const float w1 = fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B) - fmaxf(float(iu1) - 0.5f, iu1_A));
-                if (!(w1 > 0.0f)) continue;
-                float s0 = 0.0f;
-                for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
-                    const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
-                    s0 = fmaf(w0, __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]), s0);
+            if (fewu) {
+#pragma unroll
+                for (int q = 0; q < kUT; q++) {
+                    const int iu1 = ua + q;
+                    if (iu1 > ub || !(w1s[q] > 0.0f)) continue;
+                    float s0 = 0.0f;
+                    for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
+                        const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
+                        s0 = fmaf(w0, __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]), s0);
+                    }
+                    sv = fmaf(w1s[q], s0, sv);
                 }
-                sv = fmaf(w1, s0, sv);
+            } else {
+                for (int iu1 = ua; iu1 <= ub; iu1++) {
+                    const float w1 = fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B) - fmaxf(float(iu1) - 0.5f, iu1_A));
+                    if (!(w1 > 0.0f)) continue;
+                    float s0 = 0.0f;
+                    for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
+                        const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
+                        s0 = fmaf(w0, __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]), s0);
+                    }
+                    sv = fmaf(w1, s0, sv);
+                }
             }
             val = fmaf(sv, l_phi, val);
         }
@@ -163,7 +198,7 @@ k_backproject_ref_general(const float* __restrict__ g, float* __restrict__ f, co
 // enumerated and the forward projector's own tap test and weights are
 // evaluated for them (same device functions, bit-identical weights).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 k_backproject_adj_general(const float* __restrict__ g, float* __restrict__ f, const petl_geom G, const ViewRange vr,
                           int accumulate, float scale)
 {
