@@ -20,7 +20,7 @@ namespace petl {
 // forward projection, one thread per ray
 // ---------------------------------------------------------------------------
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128)
 k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl_geom G, const ViewRange vr,
                   int n_v0, unsigned long long* __restrict__ nnz, const float* __restrict__ meas)
 {
@@ -35,49 +35,38 @@ k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl
     if (inside && ray_visible(G, iv1, iv0, iu1, iu0)) {
         const RayGeom rg = ray_geom(G, iv1, iv0, iu1, iu0);
         const int Nx = G.numX, Ny = G.numY;
-        // per plane: the z weights of the (at most kZT) slices in range are
-        // computed once and reused for every in-plane tap; the taps, their
-        // order and their float operations are those of the tap-by-tap form
-        // (which remains for footprints spanning more slices)
-        constexpr int kZT = 4;
-        auto plane = [&](const PlaneTaps& pt, int plane_idx, bool xdr) {
-            const int nz = pt.z_max - pt.z_min + 1;
-            if (nz <= 0) return;
-            if (nz <= kZT) {
-                float wz[kZT];
-#pragma unroll
-                for (int q = 0; q < kZT; q++) wz[q] = q < nz ? tap_w1(G, rg, pt.t, pt.z_min + q, iu1) : 0.0f;
-                for (int a = pt.a_min; a <= pt.a_max; a++) {
-                    const float w0 = xdr ? tap_w0_x(G, rg, pt.t, a, iu0) : tap_w0_y(G, rg, pt.t, a, iu0);
-                    if (!(w0 > 0.0f)) continue;
-                    const int ix = xdr ? plane_idx : a, iy = xdr ? a : plane_idx;
-#pragma unroll
-                    for (int q = 0; q < kZT; q++) {
-                        if (q < nz && wz[q] > 0.0f) {
-                            if (COUNT) cnt++;
-                            else val = ffma(__ldg(&f[(size_t(pt.z_min + q) * Ny + iy) * Nx + ix]), fmul(w0, wz[q]), val);
-                        }
-                    }
-                }
-            } else {
-                for (int a = pt.a_min; a <= pt.a_max; a++) {
-                    const float w0 = xdr ? tap_w0_x(G, rg, pt.t, a, iu0) : tap_w0_y(G, rg, pt.t, a, iu0);
-                    if (!(w0 > 0.0f)) continue;
-                    const int ix = xdr ? plane_idx : a, iy = xdr ? a : plane_idx;
-                    for (int iz = pt.z_min; iz <= pt.z_max; iz++) {
-                        const float w1 = tap_w1(G, rg, pt.t, iz, iu1);
-                        if (w1 > 0.0f) {
-                            if (COUNT) cnt++;
-                            else val = ffma(__ldg(&f[(size_t(iz) * Ny + iy) * Nx + ix]), fmul(w0, w1), val);
+        if (rg.xdriven) {
+            for (int ix = 0; ix < Nx; ix++) {
+                const PlaneTaps pt = plane_taps_x(G, rg, ix);
+                for (int iy = pt.a_min; iy <= pt.a_max; iy++) {
+                    const float w0 = tap_w0_x(G, rg, pt.t, iy, iu0);
+                    if (w0 > 0.0f) {
+                        for (int iz = pt.z_min; iz <= pt.z_max; iz++) {
+                            const float w1 = tap_w1(G, rg, pt.t, iz, iu1);
+                            if (w1 > 0.0f) {
+                                if (COUNT) cnt++;
+                                else val = ffma(__ldg(&f[(size_t(iz) * Ny + iy) * Nx + ix]), fmul(w0, w1), val);
+                            }
                         }
                     }
                 }
             }
-        };
-        if (rg.xdriven) {
-            for (int ix = 0; ix < Nx; ix++) plane(plane_taps_x(G, rg, ix), ix, true);
         } else {
-            for (int iy = 0; iy < Ny; iy++) plane(plane_taps_y(G, rg, iy), iy, false);
+            for (int iy = 0; iy < Ny; iy++) {
+                const PlaneTaps pt = plane_taps_y(G, rg, iy);
+                for (int ix = pt.a_min; ix <= pt.a_max; ix++) {
+                    const float w0 = tap_w0_y(G, rg, pt.t, ix, iu0);
+                    if (w0 > 0.0f) {
+                        for (int iz = pt.z_min; iz <= pt.z_max; iz++) {
+                            const float w1 = tap_w1(G, rg, pt.t, iz, iu1);
+                            if (w1 > 0.0f) {
+                                if (COUNT) cnt++;
+                                else val = ffma(__ldg(&f[(size_t(iz) * Ny + iy) * Nx + ix]), fmul(w0, w1), val);
+                            }
+                        }
+                    }
+                }
+            }
         }
         val = fmul(fmul(val, rg.l_phi), rg.rs);
     }
@@ -94,102 +83,167 @@ k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl
 }
 
 // ---------------------------------------------------------------------------
-// reference-semantics backprojection, one thread per voxel (gather)
-// src/projectors.cu:240-377: voxel-centre u1 visibility test, no u0 test,
-// border bins read as zero; f = sum_v1 T_x * sum_v0 ...
+// reference-semantics backprojection, KZ voxels (z .. z+KZ-1) per thread: the
+// voxels of a column share, per view, the u0 footprint (A, B), its range and
+// l_phi, and their u1 rows overlap, so every planogram row of the column's
+// union is summed over u0 once and combined per voxel with its own u1
+// weights, in the order (ascending u1) and with the float operations of
+// k_backproject_ref_general.  Columns whose union spans more than kRows
+// rows take the per-voxel form.
 // ---------------------------------------------------------------------------
+template <int KZ>
 __global__ void __launch_bounds__(128, 4)
-k_backproject_ref_general(const float* __restrict__ g, float* __restrict__ f, const petl_geom G, const ViewRange vr,
-                          int accumulate, float scale)
+k_backproject_ref_general_multi(const float* __restrict__ g, float* __restrict__ f, const petl_geom G,
+                                const ViewRange vr, int accumulate, float scale)
 {
+    constexpr int kRows = 8;
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * 4 + threadIdx.y;
-    const int iz = blockIdx.z;
+    const int iz0 = blockIdx.z * KZ;
     if (ix >= G.numX || iy >= G.numY) return;
     const float cs = G.cos_psi, sn = G.sin_psi;
     const float x = fmaf(float(ix), G.T_x, G.x_0);
     const float y = fmaf(float(iy), G.T_x, G.y_0);
-    const float z = fmaf(float(iz), G.T_z, G.z_0);
+    float z[KZ];
+#pragma unroll
+    for (int k = 0; k < KZ; k++) z[k] = fmaf(float(iz0 + k), G.T_z, G.z_0);
     const float t = fmaf(y, cs, -(x * sn));
     const float x_dot_theta = fmaf(x, cs, y * sn);
     const float Tu1_inv = 1.0f / G.T_u1, Tu0_inv = 1.0f / G.T_u0;
     const float xdt_dy = 0.5f * G.T_x * sn, t_dy = 0.5f * G.T_x * cs;
     const float xdt_dx = 0.5f * G.T_x * cs, t_dx = -0.5f * G.T_x * sn;
     const size_t slab = size_t(G.N_v0) * G.N_u1 * G.N_u0;
-    float acc = 0.0f;
+    float acc[KZ];
+#pragma unroll
+    for (int k = 0; k < KZ; k++) acc[k] = 0.0f;
     for (int iv1 = vr.iv1_begin; iv1 < vr.iv1_end; iv1++) {
         const float v1 = fmaf(float(iv1), G.T_v1, G.v1_0);
-        const float u1 = fmaf(v1, t, z);
-        if (!(fabsf(u1) - 0.5f * G.T_u1 <= fmaf(-G.R, fabsf(v1), G.H))) continue;
-        const float iu1_mid = (u1 - G.u1_0) * Tu1_inv;
-        const float iu1_A = iu1_mid - 0.5f * G.T_z * Tu1_inv;
-        const float iu1_B = iu1_mid + 0.5f * G.T_z * Tu1_inv;
-        const int iu1_min = int(ceilf(iu1_A - 0.5f));
-        const int iu1_max = int(floorf(iu1_B + 0.5f));
+        bool vis[KZ];
+        float iu1_A[KZ], iu1_B[KZ];
+        int ua[KZ], ub[KZ];
+        int lo = 1 << 30, hi = -(1 << 30);
+        bool anyv = false;
+#pragma unroll
+        for (int k = 0; k < KZ; k++) {
+            const float u1 = fmaf(v1, t, z[k]);
+            vis[k] = iz0 + k < G.numZ && (fabsf(u1) - 0.5f * G.T_u1 <= fmaf(-G.R, fabsf(v1), G.H));
+            const float iu1_mid = (u1 - G.u1_0) * Tu1_inv;
+            iu1_A[k] = iu1_mid - 0.5f * G.T_z * Tu1_inv;
+            iu1_B[k] = iu1_mid + 0.5f * G.T_z * Tu1_inv;
+            ua[k] = max(int(ceilf(iu1_A[k] - 0.5f)), 0);
+            ub[k] = min(int(floorf(iu1_B[k] + 0.5f)), G.N_u1 - 1);
+            if (vis[k] && ua[k] <= ub[k]) {
+                lo = min(lo, ua[k]);
+                hi = max(hi, ub[k]);
+            }
+            anyv = anyv || vis[k];
+        }
+        if (!anyv) continue;
         const float* gs = g + size_t(iv1) * slab;
-        // u1 weights of this slope's rows, the same for every view
-        constexpr int kUT = 4;
-        const int ua = max(iu1_min, 0), ub = min(iu1_max, G.N_u1 - 1);
-        const bool fewu = ub - ua + 1 <= kUT;
-        float w1s[kUT];
+        float val[KZ];
 #pragma unroll
-        for (int q = 0; q < kUT; q++) {
-            const int iu1 = ua + q;
-            w1s[q] = fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B) - fmaxf(float(iu1) - 0.5f, iu1_A));
-        }
-        float val = 0.0f;
-        for (int iv0 = vr.iv0_first; iv0 < G.N_v0; iv0 += vr.iv0_step) {
-            const float v0 = fmaf(float(iv0), G.T_v0, G.v0_0);
-            const float wy = fmaf(v0, cs, sn);
-            const float wx = fmaf(-v0, sn, cs);
-            const float l_phi = 1.0f / fmaxf(fabsf(wy), fabsf(wx)) * rsqrtf(1.0f + v0 * v0 + v1 * v1);
-            float A, B;
-            if (fabsf(wy) > fabsf(wx)) {
-                const float lo = (x_dot_theta - xdt_dy + v0 * (t - t_dy) - G.u0_0) * Tu0_inv;
-                const float hi = (x_dot_theta + xdt_dy + v0 * (t + t_dy) - G.u0_0) * Tu0_inv;
-                A = wy >= 0.0f ? lo : hi;
-                B = wy >= 0.0f ? hi : lo;
-            } else {
-                const float lo = (x_dot_theta - xdt_dx + v0 * (t - t_dx) - G.u0_0) * Tu0_inv;
-                const float hi = (x_dot_theta + xdt_dx + v0 * (t + t_dx) - G.u0_0) * Tu0_inv;
-                A = wx >= 0.0f ? lo : hi;
-                B = wx >= 0.0f ? hi : lo;
-            }
-            const int iu0_min = max(int(ceilf(A - 0.5f)), 0);
-            const int iu0_max = min(int(floorf(B + 0.5f)), G.N_u0 - 1);
-            const float* gv = gs + size_t(iv0) * G.N_u1 * G.N_u0;
-            float sv = 0.0f;
-            if (fewu) {
+        for (int k = 0; k < KZ; k++) val[k] = 0.0f;
+        if (hi - lo + 1 <= kRows) {
+            // u1 weight of union row r for voxel k (0 outside its rows)
+            float w1r[KZ][kRows];
 #pragma unroll
-                for (int q = 0; q < kUT; q++) {
-                    const int iu1 = ua + q;
-                    if (iu1 > ub || !(w1s[q] > 0.0f)) continue;
-                    float s0 = 0.0f;
+            for (int k = 0; k < KZ; k++)
+#pragma unroll
+                for (int r = 0; r < kRows; r++) {
+                    const int iu1 = lo + r;
+                    w1r[k][r] = (vis[k] && iu1 >= ua[k] && iu1 <= ub[k])
+                                    ? fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B[k]) - fmaxf(float(iu1) - 0.5f, iu1_A[k]))
+                                    : 0.0f;
+                }
+            for (int iv0 = vr.iv0_first; iv0 < G.N_v0; iv0 += vr.iv0_step) {
+                const float v0 = fmaf(float(iv0), G.T_v0, G.v0_0);
+                const float wy = fmaf(v0, cs, sn);
+                const float wx = fmaf(-v0, sn, cs);
+                const float l_phi = 1.0f / fmaxf(fabsf(wy), fabsf(wx)) * rsqrtf(1.0f + v0 * v0 + v1 * v1);
+                float A, B;
+                if (fabsf(wy) > fabsf(wx)) {
+                    const float lo_ = (x_dot_theta - xdt_dy + v0 * (t - t_dy) - G.u0_0) * Tu0_inv;
+                    const float hi_ = (x_dot_theta + xdt_dy + v0 * (t + t_dy) - G.u0_0) * Tu0_inv;
+                    A = wy >= 0.0f ? lo_ : hi_;
+                    B = wy >= 0.0f ? hi_ : lo_;
+                } else {
+                    const float lo_ = (x_dot_theta - xdt_dx + v0 * (t - t_dx) - G.u0_0) * Tu0_inv;
+                    const float hi_ = (x_dot_theta + xdt_dx + v0 * (t + t_dx) - G.u0_0) * Tu0_inv;
+                    A = wx >= 0.0f ? lo_ : hi_;
+                    B = wx >= 0.0f ? hi_ : lo_;
+                }
+                const int iu0_min = max(int(ceilf(A - 0.5f)), 0);
+                const int iu0_max = min(int(floorf(B + 0.5f)), G.N_u0 - 1);
+                const float* gv = gs + size_t(iv0) * G.N_u1 * G.N_u0;
+                float s0[kRows];
+#pragma unroll
+                for (int r = 0; r < kRows; r++) {
+                    s0[r] = 0.0f;
+                    if (lo + r > hi) continue;
                     for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
                         const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
-                        s0 = fmaf(w0, __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]), s0);
+                        s0[r] = fmaf(w0, __ldg(&gv[size_t(lo + r) * G.N_u0 + iu0]), s0[r]);
                     }
-                    sv = fmaf(w1s[q], s0, sv);
                 }
-            } else {
-                for (int iu1 = ua; iu1 <= ub; iu1++) {
-                    const float w1 = fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B) - fmaxf(float(iu1) - 0.5f, iu1_A));
-                    if (!(w1 > 0.0f)) continue;
-                    float s0 = 0.0f;
-                    for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
-                        const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
-                        s0 = fmaf(w0, __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]), s0);
-                    }
-                    sv = fmaf(w1, s0, sv);
+#pragma unroll
+                for (int k = 0; k < KZ; k++) {
+                    float sv = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < kRows; r++)
+                        if (w1r[k][r] > 0.0f) sv = fmaf(w1r[k][r], s0[r], sv);
+                    val[k] = fmaf(sv, l_phi, val[k]);
                 }
             }
-            val = fmaf(sv, l_phi, val);
+        } else {
+            for (int iv0 = vr.iv0_first; iv0 < G.N_v0; iv0 += vr.iv0_step) {
+                const float v0 = fmaf(float(iv0), G.T_v0, G.v0_0);
+                const float wy = fmaf(v0, cs, sn);
+                const float wx = fmaf(-v0, sn, cs);
+                const float l_phi = 1.0f / fmaxf(fabsf(wy), fabsf(wx)) * rsqrtf(1.0f + v0 * v0 + v1 * v1);
+                float A, B;
+                if (fabsf(wy) > fabsf(wx)) {
+                    const float lo_ = (x_dot_theta - xdt_dy + v0 * (t - t_dy) - G.u0_0) * Tu0_inv;
+                    const float hi_ = (x_dot_theta + xdt_dy + v0 * (t + t_dy) - G.u0_0) * Tu0_inv;
+                    A = wy >= 0.0f ? lo_ : hi_;
+                    B = wy >= 0.0f ? hi_ : lo_;
+                } else {
+                    const float lo_ = (x_dot_theta - xdt_dx + v0 * (t - t_dx) - G.u0_0) * Tu0_inv;
+                    const float hi_ = (x_dot_theta + xdt_dx + v0 * (t + t_dx) - G.u0_0) * Tu0_inv;
+                    A = wx >= 0.0f ? lo_ : hi_;
+                    B = wx >= 0.0f ? hi_ : lo_;
+                }
+                const int iu0_min = max(int(ceilf(A - 0.5f)), 0);
+                const int iu0_max = min(int(floorf(B + 0.5f)), G.N_u0 - 1);
+                const float* gv = gs + size_t(iv0) * G.N_u1 * G.N_u0;
+#pragma unroll
+                for (int k = 0; k < KZ; k++) {
+                    if (!vis[k]) continue;
+                    float sv = 0.0f;
+                    for (int iu1 = ua[k]; iu1 <= ub[k]; iu1++) {
+                        const float w1 = fmaxf(0.0f, fminf(float(iu1) + 0.5f, iu1_B[k]) - fmaxf(float(iu1) - 0.5f, iu1_A[k]));
+                        if (!(w1 > 0.0f)) continue;
+                        float s0 = 0.0f;
+                        for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
+                            const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
+                            s0 = fmaf(w0, __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]), s0);
+                        }
+                        sv = fmaf(w1, s0, sv);
+                    }
+                    val[k] = fmaf(sv, l_phi, val[k]);
+                }
+            }
         }
-        acc = fmaf(val, G.T_x, acc);
+#pragma unroll
+        for (int k = 0; k < KZ; k++)
+            if (vis[k]) acc[k] = fmaf(val[k], G.T_x, acc[k]);
     }
-    const size_t o = (size_t(iz) * G.numY + iy) * G.numX + ix;
-    const float r = acc * scale;
-    f[o] = accumulate ? f[o] + r : r;
+#pragma unroll
+    for (int k = 0; k < KZ; k++) {
+        if (iz0 + k >= G.numZ) break;
+        const size_t o = (size_t(iz0 + k) * G.numY + iy) * G.numX + ix;
+        const float r = acc[k] * scale;
+        f[o] = accumulate ? f[o] + r : r;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -295,10 +349,13 @@ int launch_backproject_general(const petl_geom& G, const float* g, float* f, int
     PETL_REQUIRE(G.numZ <= 65535, "numZ exceeds grid limit");
     dim3 block(32, 4, 1);
     dim3 grid(ceil_div(G.numX, 32), ceil_div(G.numY, 4), unsigned(G.numZ));
-    if (mode == PETL_BP_ADJOINT)
+    constexpr int KZ = 4;
+    if (mode == PETL_BP_ADJOINT) {
         k_backproject_adj_general<<<grid, block, 0, st>>>(g, f, G, vr, accumulate, scale);
-    else
-        k_backproject_ref_general<<<grid, block, 0, st>>>(g, f, G, vr, accumulate, scale);
+    } else {
+        grid.z = ceil_div(G.numZ, KZ);
+        k_backproject_ref_general_multi<KZ><<<grid, block, 0, st>>>(g, f, G, vr, accumulate, scale);
+    }
     PETL_LAUNCH_CHECK("backproject_general");
     return 0;
 }
