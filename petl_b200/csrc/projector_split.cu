@@ -18,6 +18,10 @@
 //   started by a rotating warp once every warp has released the slot, so no
 //   CTA-wide barrier sits in the plane loop.  The window offset, tap offsets
 //   and weights of every (plane, slope group) are tabulated once per CTA.
+//   The tap offsets of a warp's four consecutive slopes move by at most one
+//   row from slope to slope, so they form one of 15 monotone patterns: one
+//   dispatch per plane selects a fully unrolled form (four per-slope
+//   dispatches measured 10 % slower); other groups take the per-slope form.
 //
 // Both kernels do the float operations of project_tma in the same order (x
 // taps fmaf(w1, b, w0 * a); per ray, the z taps of the live planes in
@@ -146,6 +150,17 @@ __device__ __forceinline__ void zsum_taps(float2 (&acc)[ZK], const float2 (&W)[Z
     for (int k = 0; k < ZK; k++) acc[k] = fma2(w0, W[k + O], acc[k]);
 #pragma unroll
     for (int k = 0; k < ZK; k++) acc[k] = fma2(w1, W[k + O + 1], acc[k]);
+}
+
+// z taps of the four slopes of a warp with compile-time tap offsets
+// (PC: 2 bits per slope), each slope's FMAs as zsum_taps orders them.
+template <int PC>
+__device__ __forceinline__ void zsum4(float2 (&acc)[ZV][ZK], const float2 (&W)[ZWN], const float (&wj)[ZV])
+{
+    zsum_taps<(PC >> 0) & 3>(acc[0], W, dup(1.0f - wj[0]), dup(wj[0]));
+    zsum_taps<(PC >> 2) & 3>(acc[1], W, dup(1.0f - wj[1]), dup(wj[1]));
+    zsum_taps<(PC >> 4) & 3>(acc[2], W, dup(1.0f - wj[2]), dup(wj[2]));
+    zsum_taps<(PC >> 6) & 3>(acc[3], W, dup(1.0f - wj[3]), dup(wj[3]));
 }
 
 // TG: planogram storage (float or bfloat16); X and the arithmetic are FP32.
@@ -348,15 +363,40 @@ k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, TG* __restrict__ g, const T
                 float2 W[ZWN];
 #pragma unroll
                 for (int i = 0; i < ZWN; i++) W[i] = *reinterpret_cast<const float2*>(Xr + i * ZCOLS);
+                // the offsets of four consecutive slopes move by at most one
+                // row per slope: one dispatch over the 15 monotone patterns
+                bool done = wmask == 0xFu;
+                if (done) {
+                    switch (code & 0xffu) {
+                        case 0x00: zsum4<0x00>(acc, W, wj); break;
+                        case 0x40: zsum4<0x40>(acc, W, wj); break;
+                        case 0x50: zsum4<0x50>(acc, W, wj); break;
+                        case 0x90: zsum4<0x90>(acc, W, wj); break;
+                        case 0x54: zsum4<0x54>(acc, W, wj); break;
+                        case 0x94: zsum4<0x94>(acc, W, wj); break;
+                        case 0xA4: zsum4<0xA4>(acc, W, wj); break;
+                        case 0xE4: zsum4<0xE4>(acc, W, wj); break;
+                        case 0x01: zsum4<0x01>(acc, W, wj); break;
+                        case 0x05: zsum4<0x05>(acc, W, wj); break;
+                        case 0x15: zsum4<0x15>(acc, W, wj); break;
+                        case 0x06: zsum4<0x06>(acc, W, wj); break;
+                        case 0x16: zsum4<0x16>(acc, W, wj); break;
+                        case 0x1A: zsum4<0x1A>(acc, W, wj); break;
+                        case 0x1B: zsum4<0x1B>(acc, W, wj); break;
+                        default: done = false;
+                    }
+                }
+                if (!done) {
 #pragma unroll
-                for (int jj = 0; jj < ZV; jj++) {
-                    if (!((wmask >> jj) & 1u)) continue;
-                    const float2 a1 = dup(wj[jj]), a0 = dup(1.0f - wj[jj]);
-                    switch ((code >> (2 * jj)) & 3u) {
-                        case 0: zsum_taps<0>(acc[jj], W, a0, a1); break;
-                        case 1: zsum_taps<1>(acc[jj], W, a0, a1); break;
-                        case 2: zsum_taps<2>(acc[jj], W, a0, a1); break;
-                        default: zsum_taps<3>(acc[jj], W, a0, a1); break;
+                    for (int jj = 0; jj < ZV; jj++) {
+                        if (!((wmask >> jj) & 1u)) continue;
+                        const float2 a1 = dup(wj[jj]), a0 = dup(1.0f - wj[jj]);
+                        switch ((code >> (2 * jj)) & 3u) {
+                            case 0: zsum_taps<0>(acc[jj], W, a0, a1); break;
+                            case 1: zsum_taps<1>(acc[jj], W, a0, a1); break;
+                            case 2: zsum_taps<2>(acc[jj], W, a0, a1); break;
+                            default: zsum_taps<3>(acc[jj], W, a0, a1); break;
+                        }
                     }
                 }
             }
