@@ -593,6 +593,10 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     const int n_v0 = vr.n_v0(G.N_v0);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (n_v0 <= 0 || nv1 <= 0 || nv1 > GV1MAX) return kNotApplicable;
+    // the scratch holds a volume per view whatever the slope count: below
+    // about ten slopes (the 2-D backprojection of FBP has one) the
+    // single-pass kernel is cheaper than that round trip
+    if (nv1 < kSplitMinSlopes) return kNotApplicable;
     // tensor map rows: a multiple of 16 bytes from a 16-byte aligned base
     if ((G.N_u0 * EB) % 16 != 0 || (reinterpret_cast<uintptr_t>(g) & 15) != 0) return kNotApplicable;
     if (G.N_u0 > XMAXN || G.numY > 65535 || G.numZ > 65535 * XR) return kNotApplicable;

@@ -542,6 +542,9 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     const int n_v0 = vr.n_v0(G.N_v0);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (n_v0 <= 0 || nv1 <= 0) return 0;
+    // the x pass writes a volume per view whatever the slope count: below
+    // about ten slopes the single-pass kernel is cheaper than that round trip
+    if (nv1 < kSplitMinSlopes) return kNotApplicable;
     if (G.numY > ZMAXPLANES || G.numZ > 65535 * 4) return kNotApplicable;
     const double step = double(G.T_v1) * plane_ymax(G) / double(G.T_z);  // shift change per slope
     if (shift_spread(ZV - 1, step) > ZDMAX) return kNotApplicable;

@@ -27,6 +27,11 @@ struct Tables {
     int2* ub1;      // [N_v1]        visible iu1 range of the forward masks
 };
 
+// The split kernels (projector_split.cu, backprojector_split.cu) move a
+// volume-sized scratch array per view; with fewer slopes than this a call
+// takes the single-pass kernels instead.
+constexpr int kSplitMinSlopes = 10;
+
 // per-call table workspace (stream-ordered)
 struct TableBuf {
     void* base = nullptr;
