@@ -287,8 +287,13 @@ int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long l
  * has its own stream with up to `depth` subset steps in flight, issued
  * oldest request first while the work in flight stays under about two
  * full-size steps, so small requests overlap with large ones and new ones
- * join while others run.  Data and images stay resident until the result
- * is copied out.  A request's result does not depend on what else runs. */
+ * join while others run.  Batched launches: when a request whose subset
+ * steps are too small to fill the device (under two waves of CTAs) issues a
+ * step, up to seven younger requests of its geometry and subset count with
+ * no step in flight join it (each at its own subset), and one launch of
+ * each split projector kernel and of the image update serves them all.  Data
+ * and images stay resident until the result is copied out.  A request's
+ * result does not depend on what else runs, batched or not. */
 void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int device);
 /* g_host: the request's planogram, which must stay valid until
  * petl_server_wait returns for it; *id_out receives the request id. */
@@ -311,6 +316,12 @@ int petl_server_wait(void* server, long long id, float* f_host, double* latency_
 /* out[0..5]: completed, failed, active, pending, HBM bytes reserved now,
  * peak HBM bytes reserved */
 int petl_server_stats(void* server, double* out);
+/* Members of a batched step at most, 1 (no batched launches) to 8 (the
+ * default). */
+int petl_server_set_batching(void* server, int max_members);
+/* out[0]: batched steps issued (two or more members), out[1]: member steps
+ * they served */
+int petl_server_batch_stats(void* server, double* out);
 void petl_server_destroy(void* server);
 
 /* --- regularizers, volume [N1][N2][N3] ------------------------------------ */

@@ -115,6 +115,8 @@ _DEV_API = [
     ("petl_server_cancel", c_i, [c_vp, c_ll]),
     ("petl_server_wait", c_i, [c_vp, c_ll, c_vp, ctypes.POINTER(c_d), ctypes.POINTER(c_d)]),
     ("petl_server_stats", c_i, [c_vp, ctypes.POINTER(c_d)]),
+    ("petl_server_set_batching", c_i, [c_vp, c_i]),
+    ("petl_server_batch_stats", c_i, [c_vp, ctypes.POINTER(c_d)]),
     ("petl_server_destroy", None, [c_vp]),
     ("petl_pfdr_dev", c_i, [_G, c_vp, c_vp, c_vp]),
     ("petl_ramp_dev", c_i, [_G, c_vp, c_i, c_vp]),

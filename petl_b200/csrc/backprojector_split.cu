@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 
 #include "common.cuh"
@@ -88,10 +89,9 @@ constexpr uint32_t kIvlNone = 0x88u;
 
 struct ZgatherArgs {
     petl_geom G;
-    ViewRange vr;
-    int vi0;       // first view of the chunk (index in vr)
-    int nvc;       // views in the chunk
+    ViewRange vr;  // slopes and view step (the members hold their views)
     int vg;        // views per CTA
+    int gpm;       // CTAs along y per member: ceil(view slots per member / vg)
     int n_colblk;  // ceil(N_u0 / 64)
     int n_rowblk;  // ceil(numZ / 32)
     int brb;       // staged planogram rows per slope (33 + CTA shift spread, bounded on the host)
@@ -102,6 +102,13 @@ struct ZgatherArgs {
     Tables T;
     int* err;
     unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
+    Members M;  // views of the chunk per member (the planograms are the tensor maps)
+};
+
+// tensor maps of the members' planograms
+template <int NM>
+struct GMaps {
+    CUtensorMap m[NM];
 };
 
 // z taps of one plane (two columns): Z[k] += w0 W[O + k + 1] then w1 W[O + k],
@@ -167,9 +174,9 @@ __device__ __forceinline__ void g_taps4_ivl(float2 (&Z)[GP][GK], const float2 (&
 
 // TG: planogram storage (float or bfloat16); B and the arithmetic are FP32.
 // Warp w: plane group w % 4, row group w / 4.
-template <bool ADJ, class TG>
+template <bool ADJ, class TG, int NM>
 __global__ void __launch_bounds__(GNT, 1)
-k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, const ZgatherArgs A)
+k_bwd_zgather(const __grid_constant__ GMaps<NM> gmaps, float* __restrict__ B, const ZgatherArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const petl_geom& G = A.G;
@@ -182,8 +189,16 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
     const int plblk = t / A.n_rowblk;
     const int p0 = plblk * GPL, r0 = rowblk * GROWS, col0 = colblk * GCOLS;
     const int z0 = r0 + r * GK;  // first row of this warp
-    const int vfirst = blockIdx.y * A.vg;
-    const int nvw = min(A.vg, A.nvc - vfirst);  // views of this CTA
+    const int mb = NM == 1 ? 0 : blockIdx.y / A.gpm;  // member
+    const int vfirst = (blockIdx.y - mb * A.gpm) * A.vg;  // first view of this CTA in the member's chunk
+    const int nvw = min(A.vg, member_pick<NM>(A.M.nv, mb) - vfirst);  // views of this CTA
+    if (nvw <= 0) return;  // a member with fewer views than the slots
+    const int vbase = member_pick<NM>(A.M.first, mb) + vfirst * A.vr.iv0_step;  // view of k = 0
+    const int sbase = mb * A.M.nvm + vfirst;                                // its scratch slot
+    const CUtensorMap* gmap = &gmaps.m[0];
+#pragma unroll
+    for (int i = 1; i < NM; i++)
+        if (mb == i) gmap = &gmaps.m[i];
     const int NY = G.numY, NZ = G.numZ, NU1 = G.N_u1;
     const int ns = A.ns;
 
@@ -342,7 +357,7 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
         const int k = e / (nlive * GPL), rem = e - k * (nlive * GPL);
         const int li = rem / GPL, p = rem - li * GPL;
         const int v1 = s_sl[li].x;
-        const int v0 = A.vr.iv0_first + (A.vi0 + vfirst + k) * A.vr.iv0_step;
+        const int v0 = vbase + k * A.vr.iv0_step;
         const int y = min(p0 + p, NY - 1);
         const float S = A.T.S[size_t(v1) * G.N_v0 + v0];
         const float w = A.T.zt[size_t(v1) * NY + y].w;
@@ -362,12 +377,12 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
         if (*s_abort) return false;
         fence_proxy_async_smem();
         const int k = j / nsp, pr = j - k * nsp;
-        const int v0 = A.vr.iv0_first + (A.vi0 + vfirst + k) * A.vr.iv0_step;
+        const int v0 = vbase + k * A.vr.iv0_step;
         const int np = min(2, nlive - 2 * pr);
         mbar_arrive_expect_tx(&full[slot], box_bytes * uint32_t(np));
         for (int h = 0; h < np; h++) {
             const int2 sl = s_sl[2 * pr + h];
-            tma_load_4d(ringp + size_t(2 * slot + h) * A.sstride, &gmap, &full[slot], col0, sl.y, v0, sl.x);
+            tma_load_4d(ringp + size_t(2 * slot + h) * A.sstride, gmap, &full[slot], col0, sl.y, v0, sl.x);
         }
         s_round[slot] = round;
         return true;
@@ -387,8 +402,8 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
     // the z sums of view k go to the scratch (columns outside the view's
     // visible u0 range zeroed for the adjoint) and restart from zero
     auto store_view = [&](int k) {
-        const int vi = vfirst + k;
-        const int v0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
+        const int vi = sbase + k;  // scratch slot
+        const int v0 = vbase + k * A.vr.iv0_step;
         const int2 u0r = ADJ ? A.T.ub0[v0] : make_int2(0, G.N_u0 - 1);
         const int c = col0 + 2 * lane;
         const bool vx = c >= u0r.x && c <= u0r.y, vy = c + 1 >= u0r.x && c + 1 <= u0r.y;
@@ -421,8 +436,9 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
         }
         // the hot wait keeps the compile-time bound (a run-time bound here
         // measured 1 % slower); the forced give-up reaches this kernel through
-        // the slot waits of issue()
-        if (!dead) dead = !mbar_wait(&full[slot], phase, A.err);
+        // the slot waits of issue(), and the warps waiting here for a copy
+        // that was then never started leave on the abort flag
+        if (!dead) dead = !mbar_wait_abortable(&full[slot], phase, A.err, s_abort);
         if (dead) *s_abort = 1;  // before this warp releases the slot
 #pragma unroll 1
         for (int h = 0; h < 2 && !dead; h++) {
@@ -520,33 +536,36 @@ k_bwd_zgather(const __grid_constant__ CUtensorMap gmap, float* __restrict__ B, c
 
 struct XgatherArgs {
     petl_geom G;
-    ViewRange vr;
-    int vi0;         // first view of the chunk (index in vr)
-    int nvc;         // views in the chunk
+    int step;        // view step of the members' view ranges
     int NUc;         // scratch row pitch
     int first;       // first chunk: the view sums start at zero, else at the partial sum
     int last;        // last chunk: write the volume, else the partial sum
     int accumulate;  // add to the volume instead of overwriting it
     float scale;
     Tables T;
+    Members M;       // volumes (out) and views of the chunk
 };
 
 constexpr int XR = 4;         // volume rows z per k_bwd_xgather thread
 constexpr int XMAXN = 1024;   // longest scratch / volume row
 
 // x taps of a chunk of views into the volume: thread = column x of rows
-// z0..z0+7 of plane y, reading the two scratch taps of every view straight
-// from global memory (neighbouring threads share them through L1).  Grid
-// (ceil(numX / 256), ceil(numZ / 8), numY).
-__global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B, float* __restrict__ f,
-                                                     float* __restrict__ part, const XgatherArgs A)
+// z0..z0+3 of plane y of one member, reading the two scratch taps of every
+// view of that member straight from global memory (neighbouring threads
+// share them through L1).  Grid (ceil(numX / 256), ceil(numZ / 4), numY x
+// members).
+template <int NM>
+__global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B, float* __restrict__ part,
+                                                     const XgatherArgs A)
 {
-    extern __shared__ Shift s_xs[];  // [nvc] x shifts of plane y
+    extern __shared__ Shift s_xs[];  // [views of the member] x shifts of plane y
     const petl_geom& G = A.G;
     const int NY = G.numY, NZ = G.numZ, NX = G.numX, NU0 = G.N_u0, NUc = A.NUc;
-    const int x = blockIdx.x * 256 + threadIdx.x, z0 = blockIdx.y * XR, y = blockIdx.z;
-    for (int vi = threadIdx.x; vi < A.nvc; vi += 256)
-        s_xs[vi] = A.T.xt[size_t(A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step) * NY + y];
+    const int mb = NM == 1 ? 0 : blockIdx.z / NY, y = blockIdx.z - mb * NY;
+    const int x = blockIdx.x * 256 + threadIdx.x, z0 = blockIdx.y * XR;
+    const int first = member_pick<NM>(A.M.first, mb), nvb = member_pick<NM>(A.M.nv, mb);
+    float* __restrict__ f = static_cast<float*>(member_pick<NM>(A.M.out, mb));
+    for (int vi = threadIdx.x; vi < nvb; vi += 256) s_xs[vi] = A.T.xt[size_t(first + vi * A.step) * NY + y];
     __syncthreads();
     if (x >= NX) return;
     const int nz = min(XR, NZ - z0);
@@ -555,15 +574,16 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
     for (int r = 0; r < XR; r++)
         acc[r] = (!A.first && r < nz) ? part[(size_t(z0 + r) * NY + y) * NX + x] : 0.0f;
     const int rlast = nz - 1;
+    const float* Bm = B + size_t(mb) * A.M.nvm * NY * NZ * NUc;
 #pragma unroll 4
-    for (int vi = 0; vi < A.nvc; vi++) {
+    for (int vi = 0; vi < nvb; vi++) {
         const Shift xs = s_xs[vi];
         const float wx1 = xs.w, wx0 = 1.0f - xs.w;
         const int j0 = x - xs.d;  // scratch column of tap 0
         const bool okm = unsigned(j0 - 1) < unsigned(NU0), ok0 = unsigned(j0) < unsigned(NU0);
         // in-bounds addresses for every tap; the out-of-range ones are selected away
         const int jm = min(max(j0 - 1, 0), NU0 - 1), jz = min(max(j0, 0), NU0 - 1);
-        const float* Bv = B + ((size_t(vi) * NY + y) * NZ + z0) * NUc;
+        const float* Bv = Bm + ((size_t(vi) * NY + y) * NZ + z0) * NUc;
 #pragma unroll
         for (int r = 0; r < XR; r++) {
             const int rr = min(r, rlast);
@@ -582,24 +602,33 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
     }
 }
 
-
 }  // namespace
 
+// Backprojection of the members' views.  One member: its views in chunks of
+// at most the scratch budget (and chunk_cap); several: one chunk, else
+// kNotApplicable.  Member b reads planogram M0.in[b] and writes (or adds to)
+// volume M0.out[b].
 template <class TG>
-int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int accumulate, float scale,
+int backproject_split_m(const petl_geom& G, const Members& M0, int mode, int accumulate, float scale,
                         const ViewRange& vr, const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
     constexpr int EB = int(sizeof(TG));
-    const int n_v0 = vr.n_v0(G.N_v0);
+    const int nb = M0.nb;
+    if (nb < 1 || nb > kMaxMembers) return kNotApplicable;
+    int nvmax = 0;
+    for (int b = 0; b < nb; b++) nvmax = std::max(nvmax, M0.nv[b]);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
-    if (n_v0 <= 0 || nv1 <= 0 || nv1 > GV1MAX) return kNotApplicable;
+    if (nvmax <= 0 || nv1 <= 0 || nv1 > GV1MAX) return kNotApplicable;
     // the scratch holds a volume per view whatever the slope count: below
     // about ten slopes (the 2-D backprojection of FBP has one) the
     // single-pass kernel is cheaper than that round trip
     if (nv1 < kSplitMinSlopes) return kNotApplicable;
     // tensor map rows: a multiple of 16 bytes from a 16-byte aligned base
-    if ((G.N_u0 * EB) % 16 != 0 || (reinterpret_cast<uintptr_t>(g) & 15) != 0) return kNotApplicable;
+    if ((G.N_u0 * EB) % 16 != 0) return kNotApplicable;
+    for (int b = 0; b < nb; b++)
+        if ((reinterpret_cast<uintptr_t>(M0.in[b]) & 15) != 0) return kNotApplicable;
     if (G.N_u0 > XMAXN || G.numY > 65535 || G.numZ > 65535 * XR) return kNotApplicable;
+    if (size_t(G.numY) * nb > 65535) return kNotApplicable;  // k_bwd_xgather grid.z
     const double step = double(std::max(std::fabs(G.v1_0), std::fabs(G.v1_0 + (G.N_v1 - 1) * G.T_v1))) *
                         double(G.T_x) / double(G.T_z);  // shift change per plane
     if (shift_spread(GP - 1, step) > GDW) return kNotApplicable;
@@ -623,12 +652,21 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
 
     // chunks of views whose scratch fits the budget, balanced in size
     const size_t per_view = size_t(G.numY) * G.numZ * A.NUc * 4;
-    int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), split_scratch_budget() / per_view)));
-    nv = std::min(nv, 4096);  // k_bwd_xgather stages the chunk's x shifts in shared memory
-    if (chunk_cap > 0) nv = std::min(nv, chunk_cap);
-    const int nchunks = (n_v0 + nv - 1) / nv;
-    nv = (n_v0 + nchunks - 1) / nchunks;
+    const size_t fit = std::max<size_t>(1, split_scratch_budget() / per_view);
+    int nv, nchunks;
+    if (nb == 1) {
+        nv = int(std::min<size_t>(size_t(nvmax), fit));
+        nv = std::min(nv, 4096);  // k_bwd_xgather stages the chunk's x shifts in shared memory
+        if (chunk_cap > 0) nv = std::min(nv, chunk_cap);
+        nchunks = (nvmax + nv - 1) / nv;
+        nv = (nvmax + nchunks - 1) / nchunks;
+    } else {
+        if (size_t(nb) * nvmax > fit || nvmax > 4096 || chunk_cap > 0) return kNotApplicable;
+        nv = nvmax;
+        nchunks = 1;
+    }
     A.vg = std::min(GVG, nv);
+    if (size_t(ceil_div(nv, A.vg)) * nb > 65535) return kNotApplicable;  // grid.y
 
     const size_t fixed = size_t(nv1) * GWARPS * sizeof(GEntry) + size_t(A.vg) * nv1 * GPL * 8 + size_t(nv1) * 8 +
                          2 * GNSMAX * 8 + 8 + GNSMAX * 4;
@@ -637,36 +675,55 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     if (A.ns < 2) return kNotApplicable;
     const size_t smem = size_t(A.ns) * stage + fixed;
 
-    CUtensorMap map;
+    GMaps<kMaxMembers> maps;
+    std::memset(&maps, 0, sizeof(maps));
     const uint64_t dims[4] = {uint64_t(G.N_u0), uint64_t(G.N_u1), uint64_t(G.N_v0), uint64_t(G.N_v1)};
     const uint64_t strides[3] = {uint64_t(G.N_u0) * EB, uint64_t(G.N_u0) * G.N_u1 * EB,
                                  uint64_t(G.N_u0) * G.N_u1 * G.N_v0 * EB};
     const uint32_t box[4] = {uint32_t(GCOLS), uint32_t(brb), 1u, 1u};
-    if (!encode_tensor_map(&map, g, 4, dims, strides, box, EB)) return kNotApplicable;
+    for (int b = 0; b < nb; b++)
+        if (!encode_tensor_map(&maps.m[b], M0.in[b], 4, dims, strides, box, EB)) return kNotApplicable;
 
     float* B = nullptr;
     float* part = nullptr;
     const size_t nvox = size_t(G.numX) * G.numY * G.numZ;
-    if (scratch_alloc(reinterpret_cast<void**>(&B), per_view * nv, st) != cudaSuccess ||
+    if (scratch_alloc(reinterpret_cast<void**>(&B), per_view * nv * nb, st) != cudaSuccess ||
         (nchunks > 1 && scratch_alloc(reinterpret_cast<void**>(&part), nvox * 4, st) != cudaSuccess)) {
         cudaGetLastError();  // out of memory is not sticky: the caller takes the single-pass kernel
         if (B) cudaFreeAsync(B, st);
         return kNotApplicable;
     }
     const bool adj = mode == PETL_BP_ADJOINT;
-    auto kz = adj ? k_bwd_zgather<true, TG> : k_bwd_zgather<false, TG>;
-    cudaError_t e = cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    // kernels compiled for one member where there is one
+    GMaps<1> map1;
+    map1.m[0] = maps.m[0];
+    auto kz1 = adj ? k_bwd_zgather<true, TG, 1> : k_bwd_zgather<false, TG, 1>;
+    auto kzm = adj ? k_bwd_zgather<true, TG, kMaxMembers> : k_bwd_zgather<false, TG, kMaxMembers>;
+    auto kx = nb == 1 ? k_bwd_xgather<1> : k_bwd_xgather<kMaxMembers>;
+    cudaError_t e = nb == 1 ? cudaFuncSetAttribute(kz1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))
+                            : cudaFuncSetAttribute(kzm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     const unsigned ntile = unsigned(A.n_colblk) * unsigned(A.n_rowblk) * ceil_div(G.numY, GPL);
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
-        const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
+        Members M = M0;
+        const int vi0 = c * nv;
+        int nvc = nv;
+        if (nb == 1) {
+            nvc = std::min(nv, nvmax - vi0);
+            M.first[0] = M0.first[0] + vi0 * vr.iv0_step;
+            M.nv[0] = nvc;
+        }
+        M.nvm = nvc;
         if (hook && hook->fn) hook->fn(hook->ctx, vi0, nvc);
-        A.vi0 = vi0;
-        A.nvc = nvc;
-        kz<<<dim3(ntile, ceil_div(nvc, A.vg)), GNT, smem, st>>>(map, B, A);
+        A.M = M;
+        A.gpm = int(ceil_div(nvc, A.vg));
+        if (nb == 1)
+            kz1<<<dim3(ntile, unsigned(A.gpm)), GNT, smem, st>>>(map1, B, A);
+        else
+            kzm<<<dim3(ntile, unsigned(A.gpm) * unsigned(nb)), GNT, smem, st>>>(maps, B, A);
         note_launch();
-        XgatherArgs X{G, vr, vi0, nvc, A.NUc, c == 0, c == nchunks - 1, accumulate, scale, T};
-        k_bwd_xgather<<<dim3(ceil_div(G.numX, 256), ceil_div(G.numZ, XR), unsigned(G.numY)), 256,
-                        size_t(nvc) * sizeof(Shift), st>>>(B, f, part, X);
+        XgatherArgs X{G, vr.iv0_step, A.NUc, c == 0, c == nchunks - 1, accumulate, scale, T, M};
+        kx<<<dim3(ceil_div(G.numX, 256), ceil_div(G.numZ, XR), unsigned(G.numY) * unsigned(nb)), 256,
+                        size_t(nvc) * sizeof(Shift), st>>>(B, part, X);
         note_launch();
         e = cudaGetLastError();
     }
@@ -679,6 +736,19 @@ int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int
     return 0;
 }
 
+template <class TG>
+int backproject_split_t(const petl_geom& G, const TG* g, float* f, int mode, int accumulate, float scale,
+                        const ViewRange& vr, const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
+{
+    Members M;
+    M.nb = 1;
+    M.first[0] = vr.iv0_first;
+    M.nv[0] = vr.n_v0(G.N_v0);
+    M.in[0] = g;
+    M.out[0] = f;
+    return backproject_split_m<TG>(G, M, mode, accumulate, scale, vr, T, st, chunk_cap, hook);
+}
+
 int backproject_split(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
                       const ViewRange& vr, const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
@@ -689,6 +759,12 @@ int backproject_split_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f,
                            float scale, const ViewRange& vr, const Tables& T, cudaStream_t st)
 {
     return backproject_split_t<__nv_bfloat16>(G, g, f, mode, accumulate, scale, vr, T, st, 0, nullptr);
+}
+
+int backproject_split_members(const petl_geom& G, const Members& M, int mode, int accumulate, float scale,
+                              const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    return backproject_split_m<float>(G, M, mode, accumulate, scale, vr, T, st, 0, nullptr);
 }
 
 }  // namespace shear

@@ -72,59 +72,62 @@ constexpr int kCodeSkipShift = 16;
 
 struct XshiftArgs {
     petl_geom G;
-    ViewRange vr;
-    int vi0;  // first view of the chunk (index in vr)
-    int nvc;  // views in the chunk
-    int NXc;  // scratch row pitch (columns, a multiple of 4)
+    int step;  // view step of the members' view ranges
+    int NXc;   // scratch row pitch (columns, a multiple of 4)
     Tables T;
+    Members M;  // volumes (in) and views of the chunk
 };
 
 constexpr int XZB = 8;      // volume rows z per k_xshift block
 constexpr int XMAXNX = 1024;  // longest volume row k_xshift stages
 
-// X rows of a chunk of views.  A block stages rows z0..z0+7 of plane y in
-// shared memory once and writes them shifted for every view of the chunk,
-// one float4 of columns per thread and step.  Grid (ceil(NZ / 8), NY).
-template <class TF>
-__global__ void __launch_bounds__(256) k_xshift(const TF* __restrict__ f, float* __restrict__ X, const XshiftArgs A)
+// X rows of a chunk of views.  A block stages rows z0..z0+7 of plane y of
+// each member's volume in shared memory once and writes them shifted for
+// every view of that member in the chunk, one float4 of columns per thread
+// and step.  Grid (ceil(NZ / 8), NY).
+template <class TF, int NM>
+__global__ void __launch_bounds__(256) k_xshift(float* __restrict__ X, const XshiftArgs A)
 {
     __shared__ float rowbuf[XZB * XMAXNX];
     const petl_geom& G = A.G;
     const int NY = G.numY, NX = G.numX, NZ = G.numZ;
     const int y = blockIdx.y, z0 = blockIdx.x * XZB;
     const int nz = min(XZB, NZ - z0);
-    for (int e = threadIdx.x; e < nz * NX; e += blockDim.x) {
-        const int r = e / NX, x = e - r * NX;
-        rowbuf[r * NX + x] = Store<TF>::ld(f[(size_t(z0 + r) * NY + y) * NX + x]);
-    }
-    __syncthreads();
     const int nq = A.NXc >> 2;  // float4 columns per row
-    for (int vi = 0; vi < A.nvc; vi++) {
-        const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
-        const Shift xs = A.T.xt[size_t(iv0) * NY + y];
-        const float w1 = xs.w, w0 = 1.0f - xs.w;
-        float* Xv = X + (size_t(vi) * NY + y) * NZ * A.NXc;
-        for (int e = threadIdx.x; e < nz * nq; e += blockDim.x) {
-            const int r = e / nq, c = (e - r * nq) * 4;
-            const float* fr = rowbuf + r * NX;
-            float v[5];
+    for (int b = 0; b < (NM == 1 ? 1 : A.M.nb); b++) {
+        const TF* __restrict__ f = static_cast<const TF*>(member_pick<NM>(A.M.in, b));
+        if (b) __syncthreads();  // the previous member's rows are read
+        for (int e = threadIdx.x; e < nz * NX; e += blockDim.x) {
+            const int r = e / NX, x = e - r * NX;
+            rowbuf[r * NX + x] = Store<TF>::ld(f[(size_t(z0 + r) * NY + y) * NX + x]);
+        }
+        __syncthreads();
+        const int first = member_pick<NM>(A.M.first, b), nvb = member_pick<NM>(A.M.nv, b);
+        for (int iv = 0; iv < nvb; iv++) {
+            const Shift xs = A.T.xt[size_t(first + iv * A.step) * NY + y];
+            const float w1 = xs.w, w0 = 1.0f - xs.w;
+            float* Xv = X + (size_t(b * A.M.nvm + iv) * NY + y) * NZ * A.NXc;
+            for (int e = threadIdx.x; e < nz * nq; e += blockDim.x) {
+                const int r = e / nq, c = (e - r * nq) * 4;
+                const float* fr = rowbuf + r * NX;
+                float v[5];
 #pragma unroll
-            for (int i = 0; i < 5; i++) {
-                const int ix = c + xs.d + i;
-                v[i] = unsigned(ix) < unsigned(NX) ? fr[ix] : 0.0f;
+                for (int i = 0; i < 5; i++) {
+                    const int ix = c + xs.d + i;
+                    v[i] = unsigned(ix) < unsigned(NX) ? fr[ix] : 0.0f;
+                }
+                const float4 o = make_float4(fmaf(w1, v[1], w0 * v[0]), fmaf(w1, v[2], w0 * v[1]),
+                                             fmaf(w1, v[3], w0 * v[2]), fmaf(w1, v[4], w0 * v[3]));
+                // streaming store: the scratch is read once, by the next kernel
+                __stcs(reinterpret_cast<float4*>(Xv + size_t(z0 + r) * A.NXc + c), o);
             }
-            const float4 o = make_float4(fmaf(w1, v[1], w0 * v[0]), fmaf(w1, v[2], w0 * v[1]),
-                                         fmaf(w1, v[3], w0 * v[2]), fmaf(w1, v[4], w0 * v[3]));
-            // streaming store: the scratch is read once, by the next kernel
-            __stcs(reinterpret_cast<float4*>(Xv + size_t(z0 + r) * A.NXc + c), o);
         }
     }
 }
 
 struct ZsumArgs {
     petl_geom G;
-    ViewRange vr;
-    int vi0;       // first view of the chunk (index in vr)
+    int step;      // view step of the members' view ranges
     int v1_first;  // first slope of the launch's slope blocks
     int v1_end;    // one past its last slope
     int sg;        // slope groups per CTA (4; 1 or 2 for a tail block of at most 8 slopes)
@@ -139,6 +142,7 @@ struct ZsumArgs {
     Tables T;
     int* err;
     unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
+    Members M;  // planograms (out), measured planograms (meas) and views of the chunk
 };
 
 // z taps of one slope: all first-tap FMAs, then all second-tap FMAs (16
@@ -166,18 +170,21 @@ __device__ __forceinline__ void zsum4(float2 (&acc)[ZV][ZK], const float2 (&W)[Z
 // TG: planogram storage (float or bfloat16); X and the arithmetic are FP32.
 // Warp w: slope group w % sg, row group w / sg.  The copy of stage j is
 // started by lane 0 of warp j % 16 once every warp has released the slot.
-template <class TG>
+template <class TG, int NM>
 __global__ void __launch_bounds__(ZNT, 1)
-k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, TG* __restrict__ g, const TG* __restrict__ meas,
-           const ZsumArgs A)
+k_fwd_zsum(const __grid_constant__ CUtensorMap xmap, const ZsumArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const petl_geom& G = A.G;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int sg = A.sg, rows = ZK * (ZWARPS / sg);
     const int gv = warp % sg, gr = warp / sg;
-    const int vi = blockIdx.y;  // view within the chunk
-    const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
+    const int vi = blockIdx.y;  // view slot within the chunk
+    const int mb = NM == 1 ? 0 : vi / A.M.nvm, mv = vi - mb * A.M.nvm;
+    if (mv >= member_pick<NM>(A.M.nv, mb)) return;  // a member with fewer views than the slots
+    const int iv0 = member_pick<NM>(A.M.first, mb) + mv * A.step;
+    TG* __restrict__ g = static_cast<TG*>(member_pick<NM>(A.M.out, mb));
+    const TG* __restrict__ meas = static_cast<const TG*>(member_pick<NM>(A.M.meas, mb));
     int t = blockIdx.x;
     const int colblk = t % A.n_colblk;
     t /= A.n_colblk;
@@ -471,7 +478,7 @@ bool zsum_layout(const petl_geom& G, const ViewRange& vr, int v1_first, int v1_e
     ZsumArgs& A = L.A;
     A = ZsumArgs{};
     A.G = G;
-    A.vr = vr;
+    A.step = vr.iv0_step;
     A.v1_first = v1_first;
     A.v1_end = v1_end;
     A.sg = sg;
@@ -535,13 +542,19 @@ size_t split_scratch_budget()
     return std::min(size_t(5) << 30, total[dev] / 8);
 }
 
+// Forward projection of the members' views.  One member: its views in
+// chunks of at most the scratch budget (and chunk_cap); several: one chunk,
+// else kNotApplicable.
 template <class TF, class TG>
-int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr, const TG* meas, const Tables& T,
-                    cudaStream_t st, int chunk_cap, const ChunkHook* hook)
+int project_split_m(const petl_geom& G, const Members& M0, const ViewRange& vr, const Tables& T, cudaStream_t st,
+                    int chunk_cap, const ChunkHook* hook)
 {
-    const int n_v0 = vr.n_v0(G.N_v0);
+    const int nb = M0.nb;
+    if (nb < 1 || nb > kMaxMembers) return kNotApplicable;
+    int nvmax = 0;
+    for (int b = 0; b < nb; b++) nvmax = std::max(nvmax, M0.nv[b]);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
-    if (n_v0 <= 0 || nv1 <= 0) return 0;
+    if (nvmax <= 0 || nv1 <= 0) return 0;
     // the x pass writes a volume per view whatever the slope count: below
     // about ten slopes the single-pass kernel is cheaper than that round trip
     if (nv1 < kSplitMinSlopes) return kNotApplicable;
@@ -554,14 +567,22 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     // chunks of views whose X fits the scratch budget, balanced in size
     const int NXc = (G.N_u0 + 3) & ~3;
     const size_t per_view = size_t(G.numY) * G.numZ * NXc * 4;
-    int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), split_scratch_budget() / per_view)));
     if (G.numX > XMAXNX || G.numY > 65535) return kNotApplicable;  // k_xshift row buffer, grid.y
-    if (chunk_cap > 0) nv = std::min(nv, chunk_cap);
-    const int nchunks = (n_v0 + nv - 1) / nv;
-    nv = (n_v0 + nchunks - 1) / nchunks;
+    const size_t fit = std::max<size_t>(1, split_scratch_budget() / per_view);
+    int nv, nchunks;
+    if (nb == 1) {
+        nv = int(std::min<size_t>(size_t(nvmax), fit));
+        if (chunk_cap > 0) nv = std::min(nv, chunk_cap);
+        nchunks = (nvmax + nv - 1) / nv;
+        nv = (nvmax + nchunks - 1) / nchunks;
+    } else {
+        if (size_t(nb) * nvmax > fit || size_t(nb) * nvmax > 65535 || chunk_cap > 0) return kNotApplicable;
+        nv = nvmax;
+        nchunks = 1;
+    }
 
     float* X = nullptr;
-    if (scratch_alloc(reinterpret_cast<void**>(&X), per_view * nv, st) != cudaSuccess) {
+    if (scratch_alloc(reinterpret_cast<void**>(&X), per_view * nv * nb, st) != cudaSuccess) {
         cudaGetLastError();  // out of memory is not sticky: the caller takes the fused kernel
         return kNotApplicable;
     }
@@ -574,24 +595,34 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     int nl = 0;
     bool ok = true;
     if (v1_split > vr.iv1_begin)
-        ok = zsum_layout(G, vr, vr.iv1_begin, v1_split, ZSG, step, X, NXc, nv, T, err, L[nl++]);
-    if (ok && tail_sg) ok = zsum_layout(G, vr, v1_split, vr.iv1_end, tail_sg, step, X, NXc, nv, T, err, L[nl++]);
+        ok = zsum_layout(G, vr, vr.iv1_begin, v1_split, ZSG, step, X, NXc, nv * nb, T, err, L[nl++]);
+    if (ok && tail_sg) ok = zsum_layout(G, vr, v1_split, vr.iv1_end, tail_sg, step, X, NXc, nv * nb, T, err, L[nl++]);
     if (!ok) {
         cudaFreeAsync(X, st);
         return kNotApplicable;
     }
-    auto kz = k_fwd_zsum<TG>;
+    // kernels compiled for one member where there is one
+    auto kz = nb == 1 ? k_fwd_zsum<TG, 1> : k_fwd_zsum<TG, kMaxMembers>;
+    auto kx = nb == 1 ? k_xshift<TF, 1> : k_xshift<TF, kMaxMembers>;
     size_t smem_max = 0;
     for (int l = 0; l < nl; l++) smem_max = std::max(smem_max, L[l].smem);
     cudaError_t e = cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
-        const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
-        XshiftArgs XA{G, vr, vi0, nvc, NXc, T};
-        k_xshift<TF><<<dim3(ceil_div(G.numZ, XZB), unsigned(G.numY)), 256, 0, st>>>(f, X, XA);
+        Members M = M0;
+        const int vi0 = c * nv;
+        int nvc = nv;
+        if (nb == 1) {
+            nvc = std::min(nv, nvmax - vi0);
+            M.first[0] = M0.first[0] + vi0 * vr.iv0_step;
+            M.nv[0] = nvc;
+        }
+        M.nvm = nvc;
+        XshiftArgs XA{G, vr.iv0_step, NXc, T, M};
+        kx<<<dim3(ceil_div(G.numZ, XZB), unsigned(G.numY)), 256, 0, st>>>(X, XA);
         note_launch();
         for (int l = 0; l < nl; l++) {
-            L[l].A.vi0 = vi0;
-            kz<<<dim3(L[l].nblk, unsigned(nvc)), ZNT, L[l].smem, st>>>(L[l].map, g, meas, L[l].A);
+            L[l].A.M = M;
+            kz<<<dim3(L[l].nblk, unsigned(nvc * nb)), ZNT, L[l].smem, st>>>(L[l].map, L[l].A);
             note_launch();
         }
         e = cudaGetLastError();
@@ -605,6 +636,21 @@ int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr,
     return 0;
 }
 
+template <class TF, class TG>
+int project_split_t(const petl_geom& G, const TF* f, TG* g, const ViewRange& vr, const TG* meas, const Tables& T,
+                    cudaStream_t st, int chunk_cap, const ChunkHook* hook)
+{
+    Members M;
+    M.nb = 1;
+    M.first[0] = vr.iv0_first;
+    M.nv[0] = vr.n_v0(G.N_v0);
+    M.in[0] = f;
+    M.out[0] = g;
+    M.meas[0] = meas;
+    if (M.nv[0] <= 0 || vr.iv1_end <= vr.iv1_begin) return 0;
+    return project_split_m<TF, TG>(G, M, vr, T, st, chunk_cap, hook);
+}
+
 int project_split(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
                   const Tables& T, cudaStream_t st, int chunk_cap, const ChunkHook* hook)
 {
@@ -615,6 +661,12 @@ int project_split_bf16(const petl_geom& G, const __nv_bfloat16* f, __nv_bfloat16
                        const __nv_bfloat16* meas, const Tables& T, cudaStream_t st)
 {
     return project_split_t<__nv_bfloat16, __nv_bfloat16>(G, f, g, vr, meas, T, st, 0, nullptr);
+}
+
+int project_split_members(const petl_geom& G, const Members& M, const ViewRange& vr, const Tables& T,
+                          cudaStream_t st)
+{
+    return project_split_m<float, float>(G, M, vr, T, st, 0, nullptr);
 }
 
 }  // namespace shear

@@ -19,6 +19,12 @@
 //    about two full-size steps: large requests run nearly in arrival order
 //    (the GPU is full with one of them), small ones overlap with them and
 //    with each other, and new requests join while others run;
+//  * batched launches: when a request of a geometry whose subset steps are
+//    too small to fill the device issues a step, up to seven younger active
+//    requests of its geometry and subset count with no step in flight join
+//    it, each at its own subset: one launch of each projector kernel (and of
+//    the image update) serves them all, on the first one's stream, ordered
+//    after and before each member's own stream by events;
 //  * completion: after the last step the image is copied to a pinned host
 //    buffer, the device memory is returned to the stream-ordered pool and
 //    the request's latency (submit to result on the host) is recorded;
@@ -30,6 +36,7 @@
 // Each request runs the same kernels in the same order whatever else is
 // running, so its result is bit-identical alone and in a mix.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -70,13 +77,32 @@ __global__ void k_zero_to_one(float* __restrict__ x, long long n)
         if (x[i] == 0.0f) x[i] = 1.0f;
 }
 
-__global__ void k_mlem(float* __restrict__ f, const float* __restrict__ d, const float* __restrict__ s, long long n)
+__device__ __forceinline__ void mlem_update(float* __restrict__ f, const float* __restrict__ d,
+                                            const float* __restrict__ s, long long n)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float den = s[i];
         f[i] *= den == 0.0f ? 0.0f : d[i] / den;
     }
+}
+
+__global__ void k_mlem(float* __restrict__ f, const float* __restrict__ d, const float* __restrict__ s, long long n)
+{
+    mlem_update(f, d, s, n);
+}
+
+// the image updates of a batched step: member blockIdx.y
+struct MlemMembers {
+    float* f[shear::kMaxMembers];
+    const float* d[shear::kMaxMembers];
+    const float* s[shear::kMaxMembers];
+};
+
+__global__ void k_mlem_members(const MlemMembers P, long long n)
+{
+    const int b = blockIdx.y;
+    mlem_update(shear::member_pick(P.f, b), shear::member_pick(P.d, b), shear::member_pick(P.s, b), n);
 }
 
 unsigned blocks_for(long long n) { return unsigned(std::min<long long>((n + 255) / 256, 148LL * 8)); }
@@ -89,6 +115,7 @@ struct GeomState {
     float* sens = nullptr;  // [subsets][numZ][numY][numX], zeros -> 1
     shear::TableBuf tables;
     bool shear = false;
+    bool batch = false;  // split projector and small steps: requests share launches
     cudaEvent_t ready = nullptr;  // recorded after the state was computed
     size_t bytes = 0;
     int users = 0;
@@ -112,6 +139,17 @@ size_t state_bytes(const petl_geom& G, int subsets)
 double step_work(const petl_geom& G, int subsets)
 {
     return double(G.N_v1) * G.N_v0 * G.N_u1 * G.N_u0 * double(G.numY) / double(subsets);
+}
+
+// A subset step whose forward z-tap launch has fewer CTAs than two waves of
+// the SMs leaves most of the device idle: requests of its geometry share
+// launches.  Larger steps fill the device alone, and batching them would
+// only tie the requests' progress together.
+bool small_step(const petl_geom& G, int subsets, int sms)
+{
+    const long long views = (G.N_v0 + subsets - 1) / subsets;
+    const long long ctas = ((G.N_u0 + 63) / 64) * ((G.N_u1 + 31) / 32) * ((G.N_v1 + 15) / 16) * views;
+    return ctas < 2LL * sms;
 }
 
 struct Request {
@@ -212,7 +250,12 @@ struct Server {
     bool build_state(Request& r, GeomState& e);
     bool admit(Request& r);
     bool issue_step(Request& r);
+    bool issue_batch(std::vector<Request*>& ms);
     void release(Request& r);
+    // batched launches: members per step at most (1: none), and counts
+    std::atomic<int> batch_max{shear::kMaxMembers};
+    int sms = 148;  // multiprocessors of the device
+    std::atomic<long long> batched_steps{0}, batched_members{0};
     void fail(Request& r, const std::string& why);
 };
 
@@ -286,6 +329,7 @@ bool Server::build_state(Request& r, GeomState& e)
     const long long nv = (long long)G.numX * G.numY * G.numZ;
     bool ok = scratch_alloc(reinterpret_cast<void**>(&e.sens), nv * 4 * r.subsets, r.st) == cudaSuccess;
     e.shear = shear_eligible(G);
+    e.batch = e.shear && small_step(G, r.subsets, sms);
     if (ok && e.shear) ok = shear::make_tables(G, e.tables, r.st) == 0;
     if (!ok) return false;
     k_fill<<<blocks_for(ng), 256, 0, r.st>>>(r.ratio, ng, 1.0f);
@@ -396,6 +440,90 @@ bool Server::issue_step(Request& r)
     return true;
 }
 
+// One OSEM subset step for each of ms (same geometry state, split
+// projector): the members' steps share one launch of each kernel on the
+// first member's stream.  Each member's own stream is ordered before the
+// batch (an event per member) and after it (its step event).  Where the
+// batched kernels do not apply (scratch for all members' views), the
+// members' steps are issued one by one on the same stream; every member's
+// floats are those of its own step either way.
+bool Server::issue_batch(std::vector<Request*>& ms)
+{
+    if (ms.size() == 1) return issue_step(*ms[0]);
+    Request& L = *ms[0];
+    const petl_geom& G = L.G;
+    const GeomState& e = *L.gs;
+    const int S = L.subsets;
+    const long long nv = (long long)G.numX * G.numY * G.numZ;
+    const int nb = int(ms.size());
+    bool ok = true;
+    for (int b = 1; b < nb && ok; b++) {
+        cudaEvent_t ev;
+        ok = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) break;
+        ok = cudaEventRecord(ev, ms[b]->st) == cudaSuccess && cudaStreamWaitEvent(L.st, ev, 0) == cudaSuccess;
+        cudaEventDestroy(ev);
+    }
+    shear::Members F, B;
+    F.nb = B.nb = nb;
+    MlemMembers U{};
+    for (int b = 0; b < nb; b++) {
+        Request& q = *ms[b];
+        const int s = q.steps_issued % S;
+        F.first[b] = B.first[b] = s;
+        F.nv[b] = B.nv[b] = ViewRange{0, G.N_v1, s, S}.n_v0(G.N_v0);
+        F.in[b] = q.f;
+        F.out[b] = q.ratio;
+        F.meas[b] = q.g;
+        B.in[b] = q.ratio;
+        B.out[b] = q.d;
+        U.f[b] = q.f;
+        U.d[b] = q.d;
+        U.s[b] = e.sens + size_t(s) * nv;
+    }
+    const ViewRange vr{0, G.N_v1, 0, S};
+    // the split kernels where a step of its own would take them (dispatch 2
+    // and 3 force other kernel families)
+    const bool split = dispatch_mode() != 2 && dispatch_mode() != 3;
+    int rc = !ok ? -1 : split ? shear::project_split_members(G, F, vr, e.tables.T, L.st) : shear::kNotApplicable;
+    if (rc == shear::kNotApplicable)
+        for (int b = 0; b < nb && (rc == 0 || rc == shear::kNotApplicable); b++) {
+            const ViewRange vb{0, G.N_v1, F.first[b], S};
+            rc = shear::project_with(G, ms[b]->f, ms[b]->ratio, vb, ms[b]->g, e.tables.T, L.st);
+        }
+    if (rc == 0)
+        rc = split ? shear::backproject_split_members(G, B, PETL_BP_REFERENCE, 0, 1.0f, vr, e.tables.T, L.st)
+                   : shear::kNotApplicable;
+    if (rc == shear::kNotApplicable)
+        for (int b = 0; b < nb && (rc == 0 || rc == shear::kNotApplicable); b++) {
+            const ViewRange vb{0, G.N_v1, B.first[b], S};
+            rc = shear::backproject_with(G, ms[b]->ratio, ms[b]->d, PETL_BP_REFERENCE, 0, 1.0f, vb, e.tables.T,
+                                         L.st);
+        }
+    if (rc) {
+        for (Request* q : ms) fail(*q, "OSEM step failed");
+        return false;
+    }
+    k_mlem_members<<<dim3(blocks_for(nv), unsigned(nb)), 256, 0, L.st>>>(U, nv);
+    note_launch();
+    cudaEvent_t done;
+    cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+    cudaEventRecord(done, L.st);
+    L.inflight.push_back(done);
+    for (int b = 1; b < nb; b++) {
+        Request& q = *ms[b];
+        cudaStreamWaitEvent(q.st, done, 0);
+        cudaEvent_t ev;
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        cudaEventRecord(ev, q.st);
+        q.inflight.push_back(ev);
+    }
+    for (Request* q : ms) q->steps_issued++;
+    batched_steps++;
+    batched_members += nb;
+    return true;
+}
+
 void Server::release(Request& r)
 {
     for (cudaEvent_t e : r.inflight) cudaEventDestroy(e);
@@ -420,6 +548,10 @@ void Server::run()
 {
     cudaSetDevice(device);
     cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
     while (true) {
         std::vector<std::shared_ptr<Request>> to_admit;
         {
@@ -476,8 +608,12 @@ void Server::run()
         const double cap = std::max(work_cap, 2.0 * biggest);
         const Clock::time_point now = Clock::now();
         bool oldest = true;
-        for (auto& rp : active) {
-            Request& r = *rp;
+        auto can_step = [&](const Request& q) {
+            return q.state == kActive && !q.result_issued && q.steps_issued < q.steps_total &&
+                   int(q.inflight.size()) < depth;
+        };
+        for (size_t ai = 0; ai < active.size(); ai++) {
+            Request& r = *active[ai];
             if (r.state == kActive && !r.result_issued) {
                 const char* why = nullptr;
                 {
@@ -490,10 +626,28 @@ void Server::run()
                     continue;
                 }
             }
-            while (r.state == kActive && !r.result_issued && r.steps_issued < r.steps_total &&
-                   int(r.inflight.size()) < depth && (oldest || inflight_work + r.work <= cap)) {
-                if (!issue_step(r)) break;
-                inflight_work += r.work;
+            while (can_step(r) && (oldest || inflight_work + r.work <= cap)) {
+                // younger requests of the same geometry state with no step in
+                // flight join this one's launches (small steps of the split
+                // projector only)
+                std::vector<Request*> ms{&r};
+                double w = r.work;
+                if (batch_max > 1 && r.gs && r.gs->batch)
+                    for (size_t aj = ai + 1; aj < active.size() && int(ms.size()) < batch_max; aj++) {
+                        Request& q = *active[aj];
+                        if (q.gs != r.gs || !can_step(q) || !q.inflight.empty() || inflight_work + w + q.work > cap)
+                            continue;
+                        bool stopping = false;
+                        {
+                            std::lock_guard<std::mutex> lk(mu);
+                            stopping = stop_reason(q, now) != nullptr;
+                        }
+                        if (stopping) continue;  // failed when the loop reaches it
+                        ms.push_back(&q);
+                        w += q.work;
+                    }
+                if (!issue_batch(ms)) break;
+                inflight_work += w;
                 progressed = true;
             }
             if (r.state == kActive) oldest = false;
@@ -676,6 +830,26 @@ int petl_server_cancel(void* server, long long id)
 }
 
 // out[0..5] = completed, failed, active, pending, HBM bytes in use, peak HBM bytes reserved
+int petl_server_set_batching(void* server, int max_members)
+{
+    Server* s = static_cast<Server*>(server);
+    if (!s || max_members < 1 || max_members > shear::kMaxMembers) {
+        set_error("server_set_batching: invalid arguments");
+        return -1;
+    }
+    s->batch_max = max_members;
+    return 0;
+}
+
+int petl_server_batch_stats(void* server, double* out)
+{
+    Server* s = static_cast<Server*>(server);
+    if (!s || !out) return -1;
+    out[0] = double(s->batched_steps.load());
+    out[1] = double(s->batched_members.load());
+    return 0;
+}
+
 int petl_server_stats(void* server, double* out)
 {
     Server* s = static_cast<Server*>(server);

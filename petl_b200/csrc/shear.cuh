@@ -32,6 +32,36 @@ struct Tables {
 // takes the single-pass kernels instead.
 constexpr int kSplitMinSlopes = 10;
 
+// The volumes (or planograms) one launch of a split kernel serves: a plain
+// call has one member; a batched call has up to kMaxMembers requests of the
+// same geometry, each with its own buffers and its own view subset (first
+// view, the common view step).  Member b's views v = 0 .. nv[b] - 1 are view
+// iv0 = first[b] + v * step of the geometry and occupy the scratch view
+// slots b * nvm + v.
+constexpr int kMaxMembers = 8;
+struct Members {
+    int nb = 1;                         // members
+    int nvm = 0;                        // view slots per member (the largest nv)
+    int first[kMaxMembers] = {};        // first view of each member in this launch
+    int nv[kMaxMembers] = {};           // views of each member in this launch
+    const void* in[kMaxMembers] = {};   // volume (forward) or planogram (backward)
+    void* out[kMaxMembers] = {};        // planogram (forward) or volume (backward)
+    const void* meas[kMaxMembers] = {}; // measured planogram of the forward's MLEM ratio, or null
+};
+
+// member b's entry of a per-member parameter array, by selects (a dynamic
+// index would copy the kernel's parameter block to local memory); kernels
+// compiled for one member (NM = 1) read entry 0
+template <int NM = kMaxMembers, class T>
+__device__ __forceinline__ T member_pick(const T (&a)[kMaxMembers], int b)
+{
+    T v = a[0];
+#pragma unroll
+    for (int i = 1; i < NM; i++)
+        if (b == i) v = a[i];
+    return v;
+}
+
 // per-call table workspace (stream-ordered)
 struct TableBuf {
     void* base = nullptr;
@@ -86,6 +116,15 @@ int backproject_split(const petl_geom& G, const float* g, float* f, int mode, in
                       const ChunkHook* hook = nullptr);
 int backproject_split_bf16(const petl_geom& G, const __nv_bfloat16* g, float* f, int mode, int accumulate,
                            float scale, const ViewRange& vr, const Tables& T, cudaStream_t st);
+// The same for the members of M (FP32): one launch of each split kernel
+// serves all of them, every member's result equal bit for bit to its own
+// call.  vr gives the slopes and the view step; the members' first views and
+// view counts are in M.  kNotApplicable when the split kernels do not apply
+// or the members' views do not fit one chunk of scratch.
+int project_split_members(const petl_geom& G, const Members& M, const ViewRange& vr, const Tables& T,
+                          cudaStream_t st);
+int backproject_split_members(const petl_geom& G, const Members& M, int mode, int accumulate, float scale,
+                              const ViewRange& vr, const Tables& T, cudaStream_t st);
 
 // Bytes of the shift tables of G (make_tables' allocation).
 size_t table_bytes(const petl_geom& G);

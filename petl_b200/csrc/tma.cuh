@@ -91,6 +91,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
     return false;
 }
 
+// Bounded wait that also ends when *abort is nonzero: another warp of the
+// CTA gave up a wait, and the copy awaited here may never be started.  The
+// flag is read only after an unsuccessful poll.  false on either; the error
+// word is set on a timeout only (the warp that gave up has set it).
+__device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, uint32_t parity, int* err, const volatile int* abort)
+{
+    for (unsigned i = 0; i < kWaitLimit; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*abort) return false;
+    }
+    if (err) atomicOr(err, kErrWaitTimeout);
+    return false;
+}
+
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2)
 {
     asm volatile(

@@ -2,7 +2,8 @@
 
 ``ReconServer`` wraps the C++ server of libpetl.so (include/petl_device.h,
 petl_server_*): requests are OSEM reconstructions of one planogram each,
-admitted by HBM budget and run concurrently on their own CUDA streams.  The
+admitted by HBM budget and run concurrently on their own CUDA streams, and
+like-geometry requests share kernel launches (batched steps).  The
 planogram of a request must stay alive until its result is collected; the
 front end keeps a reference for that.  Use pinned host tensors
 (``torch.empty(..., pin_memory=True)``) for the data so that the copy in is
@@ -16,13 +17,17 @@ from ._lib import check, lib
 
 
 class ReconServer:
-    def __init__(self, hbm_budget_gb=150.0, max_active=16, depth=2, device=0):
+    def __init__(self, hbm_budget_gb=150.0, max_active=16, depth=2, device=0, batch=8):
+        """batch: members of a batched step at most (1: every request
+        launches its own kernels; up to 8 like-geometry requests share
+        launches by default)."""
         L = lib()
         self._s = L.petl_server_create(float(hbm_budget_gb) * 1e9, int(max_active), int(depth), int(device))
         if not self._s:
             raise RuntimeError(L.petl_last_error().decode())
         self._keep = {}
         self._shapes = {}
+        check(L.petl_server_set_batching(self._s, int(batch)), "server_set_batching")
 
     def submit(self, geom, g, num_subsets, num_iter, deadline_s=None):
         """Queue OSEM of planogram ``g`` (float32, host numpy array or CPU
@@ -65,6 +70,12 @@ class ReconServer:
         lib().petl_server_stats(self._s, buf)
         keys = ("completed", "failed", "active", "pending", "hbm_bytes", "hbm_peak_bytes")
         return dict(zip(keys, list(buf)))
+
+    def batch_stats(self):
+        """Batched steps issued so far and the member steps they served."""
+        buf = (ctypes.c_double * 2)()
+        lib().petl_server_batch_stats(self._s, buf)
+        return {"batched_steps": int(buf[0]), "member_steps": int(buf[1])}
 
     def close(self):
         if self._s:

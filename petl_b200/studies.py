@@ -290,7 +290,8 @@ def _serving_requests(n, rate, seed, device):
 def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, modes=("arrivals", "saturation")):
     """The serving workload: n OSEM requests with seeded Poisson arrivals at
     `rate`/s (mode "arrivals") or all submitted at t = 0 ("saturation"),
-    served (a) by the continuous-batching server and (b) one request at a
+    served (a) by the continuous-batching server (like-geometry requests in
+    batched launches, and again with batching off) and (b) one request at a
     time by the plain device path (host data to the device, recon.osem, the
     image back to the host, in arrival order).  Latency is host wall clock
     from a request's arrival to its image on the host; recons/s is n over
@@ -328,9 +329,9 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, mode
         out.update(extra or {})
         return out
 
-    def serve_server(mode):
+    def serve_server(mode, batch=8):
         at = arrivals(mode)
-        with ReconServer(hbm_budget_gb=budget_gb, max_active=max_active, depth=2) as srv:
+        with ReconServer(hbm_budget_gb=budget_gb, max_active=max_active, depth=2, batch=batch) as srv:
             for key, (G, host) in classes.items():  # warm-up: one request per class
                 srv.wait(srv.submit(G, host, 4, 1))
             t0 = time.perf_counter()
@@ -346,8 +347,9 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, mode
                 lat.append(srv.wait(i)[1])
             wall = time.perf_counter() - t0
             st = srv.stats()
+            bs = srv.batch_stats()
         return summary(lat, wall, {"hbm_peak_gb": st["hbm_peak_bytes"] / 1e9, "failed": st["failed"],
-                                   "max_active": max_active})
+                                   "max_active": max_active, "batch_max": batch, **bs})
 
     def serve_sequential(mode):
         at = arrivals(mode)
@@ -388,10 +390,12 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, mode
                          "serves more than n / that many per second unless requests share launches"}
     for mode in modes:
         srv = serve_server(mode)
+        unb = serve_server(mode, batch=1)
         seq = serve_sequential(mode)
-        out[mode] = {"server": srv, "one_at_a_time": seq,
+        out[mode] = {"server": srv, "server_unbatched": unb, "one_at_a_time": seq,
                      "throughput_ratio": srv["recons_per_s"] / seq["recons_per_s"],
-                     "p99_ratio": srv["p99_s"] / seq["p99_s"]}
+                     "p99_ratio": srv["p99_s"] / seq["p99_s"],
+                     "batching_throughput_ratio": srv["recons_per_s"] / unb["recons_per_s"]}
     return out
 
 

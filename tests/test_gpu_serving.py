@@ -73,3 +73,51 @@ def test_admission_respects_budget(cuda):
     assert all(np.array_equal(res[0][0], r[0]) for r in res)
     # the later requests queued behind the budget
     assert res[2][2] > 0.0
+
+
+def test_batched_launches_equal_alone(cuda):
+    """Requests of one geometry and subset count share kernel launches, each
+    at its own subset (subsets of unequal view counts included); every image
+    equals the request run alone, bit for bit, and the batched server issued
+    batched steps."""
+    import time
+
+    import torch
+    from petl_b200 import Geometry, ops
+    from petl_b200.serving import ReconServer
+    args, vol = (0.0, 256.0, 128.0, 64.0, 2.0, 0.5, 0.25), (128, 128, 64, 2.0)
+    G = Geometry(*args, volume=vol)
+    S = 4
+    assert G.shape[1] % S != 0  # subsets of unequal view counts
+    rng = np.random.default_rng(11)
+    data = []
+    for k in range(6):
+        f = ellipsoids(G.vol_shape, (2.0, 2.0), rng, 6) + 0.05
+        y = ops.project(G, torch.from_numpy(f.astype(np.float32)).to(cuda))
+        y = torch.poisson(y * (1e5 / float(y.sum())), generator=torch.Generator(device=cuda).manual_seed(k))
+        host = torch.empty(y.shape, dtype=torch.float32, pin_memory=True)
+        host.copy_(y.cpu())
+        data.append((host, 1 + k % 3))
+    with ReconServer(hbm_budget_gb=60, max_active=1) as srv:
+        alone = [srv.wait(srv.submit(G, g, S, it))[0] for g, it in data]
+        assert srv.batch_stats()["batched_steps"] == 0
+    # all at once: like-geometry steps batched from the first step on
+    with ReconServer(hbm_budget_gb=60, max_active=8, depth=2) as srv:
+        ids = [srv.submit(G, g, S, it) for g, it in data]
+        together = [srv.wait(i)[0] for i in ids]
+        bs = srv.batch_stats()
+    assert bs["batched_steps"] > 0 and bs["member_steps"] >= 2 * bs["batched_steps"]
+    # staggered: later requests join while the first ones are at other subsets
+    with ReconServer(hbm_budget_gb=60, max_active=8, depth=1) as srv:
+        ids = []
+        for g, it in data:
+            ids.append(srv.submit(G, g, S, it))
+            time.sleep(0.002)
+        staggered = [srv.wait(i)[0] for i in ids]
+    # batching off: the same
+    with ReconServer(hbm_budget_gb=60, max_active=8, batch=1) as srv:
+        ids = [srv.submit(G, g, S, it) for g, it in data]
+        unbatched = [srv.wait(i)[0] for i in ids]
+        assert srv.batch_stats()["batched_steps"] == 0
+    for a, b, c, d in zip(alone, together, staggered, unbatched):
+        assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
