@@ -289,9 +289,10 @@ int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long l
  * full-size steps, so small requests overlap with large ones and new ones
  * join while others run.  Batched launches: when a request whose subset
  * steps are too small to fill the device (under two waves of CTAs) issues a
- * step, up to seven younger requests of its geometry and subset count with
- * no step in flight join it (each at its own subset), and one launch of
- * each split projector kernel and of the image update serves them all.  Data
+ * step with none in flight, up to seven younger requests of its geometry
+ * and subset count with no step in flight join it (each at its own
+ * subset), and one launch of each split projector kernel and of the image
+ * update serves them all.  Data
  * and images stay resident until the result is copied out.  A request's
  * result does not depend on what else runs, batched or not. */
 void* petl_server_create(double hbm_budget_bytes, int max_active, int depth, int device);

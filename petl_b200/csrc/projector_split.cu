@@ -82,9 +82,9 @@ constexpr int XZB = 8;      // volume rows z per k_xshift block
 constexpr int XMAXNX = 1024;  // longest volume row k_xshift stages
 
 // X rows of a chunk of views.  A block stages rows z0..z0+7 of plane y of
-// each member's volume in shared memory once and writes them shifted for
+// one member's volume in shared memory once and writes them shifted for
 // every view of that member in the chunk, one float4 of columns per thread
-// and step.  Grid (ceil(NZ / 8), NY).
+// and step.  Grid (ceil(NZ / 8), NY, members).
 template <class TF, int NM>
 __global__ void __launch_bounds__(256) k_xshift(float* __restrict__ X, const XshiftArgs A)
 {
@@ -92,35 +92,33 @@ __global__ void __launch_bounds__(256) k_xshift(float* __restrict__ X, const Xsh
     const petl_geom& G = A.G;
     const int NY = G.numY, NX = G.numX, NZ = G.numZ;
     const int y = blockIdx.y, z0 = blockIdx.x * XZB;
+    const int b = NM == 1 ? 0 : int(blockIdx.z);
     const int nz = min(XZB, NZ - z0);
     const int nq = A.NXc >> 2;  // float4 columns per row
-    for (int b = 0; b < (NM == 1 ? 1 : A.M.nb); b++) {
-        const TF* __restrict__ f = static_cast<const TF*>(member_pick<NM>(A.M.in, b));
-        if (b) __syncthreads();  // the previous member's rows are read
-        for (int e = threadIdx.x; e < nz * NX; e += blockDim.x) {
-            const int r = e / NX, x = e - r * NX;
-            rowbuf[r * NX + x] = Store<TF>::ld(f[(size_t(z0 + r) * NY + y) * NX + x]);
-        }
-        __syncthreads();
-        const int first = member_pick<NM>(A.M.first, b), nvb = member_pick<NM>(A.M.nv, b);
-        for (int iv = 0; iv < nvb; iv++) {
-            const Shift xs = A.T.xt[size_t(first + iv * A.step) * NY + y];
-            const float w1 = xs.w, w0 = 1.0f - xs.w;
-            float* Xv = X + (size_t(b * A.M.nvm + iv) * NY + y) * NZ * A.NXc;
-            for (int e = threadIdx.x; e < nz * nq; e += blockDim.x) {
-                const int r = e / nq, c = (e - r * nq) * 4;
-                const float* fr = rowbuf + r * NX;
-                float v[5];
+    const TF* __restrict__ f = static_cast<const TF*>(member_pick<NM>(A.M.in, b));
+    for (int e = threadIdx.x; e < nz * NX; e += blockDim.x) {
+        const int r = e / NX, x = e - r * NX;
+        rowbuf[r * NX + x] = Store<TF>::ld(f[(size_t(z0 + r) * NY + y) * NX + x]);
+    }
+    __syncthreads();
+    const int first = member_pick<NM>(A.M.first, b), nvb = member_pick<NM>(A.M.nv, b);
+    for (int iv = 0; iv < nvb; iv++) {
+        const Shift xs = A.T.xt[size_t(first + iv * A.step) * NY + y];
+        const float w1 = xs.w, w0 = 1.0f - xs.w;
+        float* Xv = X + (size_t(b * A.M.nvm + iv) * NY + y) * NZ * A.NXc;
+        for (int e = threadIdx.x; e < nz * nq; e += blockDim.x) {
+            const int r = e / nq, c = (e - r * nq) * 4;
+            const float* fr = rowbuf + r * NX;
+            float v[5];
 #pragma unroll
-                for (int i = 0; i < 5; i++) {
-                    const int ix = c + xs.d + i;
-                    v[i] = unsigned(ix) < unsigned(NX) ? fr[ix] : 0.0f;
-                }
-                const float4 o = make_float4(fmaf(w1, v[1], w0 * v[0]), fmaf(w1, v[2], w0 * v[1]),
-                                             fmaf(w1, v[3], w0 * v[2]), fmaf(w1, v[4], w0 * v[3]));
-                // streaming store: the scratch is read once, by the next kernel
-                __stcs(reinterpret_cast<float4*>(Xv + size_t(z0 + r) * A.NXc + c), o);
+            for (int i = 0; i < 5; i++) {
+                const int ix = c + xs.d + i;
+                v[i] = unsigned(ix) < unsigned(NX) ? fr[ix] : 0.0f;
             }
+            const float4 o = make_float4(fmaf(w1, v[1], w0 * v[0]), fmaf(w1, v[2], w0 * v[1]),
+                                         fmaf(w1, v[3], w0 * v[2]), fmaf(w1, v[4], w0 * v[3]));
+            // streaming store: the scratch is read once, by the next kernel
+            __stcs(reinterpret_cast<float4*>(Xv + size_t(z0 + r) * A.NXc + c), o);
         }
     }
 }
@@ -618,7 +616,7 @@ int project_split_m(const petl_geom& G, const Members& M0, const ViewRange& vr, 
         }
         M.nvm = nvc;
         XshiftArgs XA{G, vr.iv0_step, NXc, T, M};
-        kx<<<dim3(ceil_div(G.numZ, XZB), unsigned(G.numY)), 256, 0, st>>>(X, XA);
+        kx<<<dim3(ceil_div(G.numZ, XZB), unsigned(G.numY), unsigned(nb)), 256, 0, st>>>(X, XA);
         note_launch();
         for (int l = 0; l < nl; l++) {
             L[l].A.M = M;

@@ -250,27 +250,61 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr(const PfdrArgs A)
 constexpr int kPfdrStages = 3;
 constexpr int kPfdrWarps = kPfdrRows / 2;
 
+// Work-buffer index of element i inside the FFT: bits 0-3 are XORed with 5
+// times bits 4-5 (an involution on every block of 16).  The butterfly stores
+// of the first two radix-4 stages go to indices 4j + c and 16 (j / 4) +
+// 4c + j % 4; with the permutation each half warp's 16 stores (and every
+// contiguous run of 16) hit 16 distinct bank pairs instead of 4.
+__device__ __forceinline__ int fsw(int i) { return i ^ (((i >> 4) & 3) * 5); }
+
+// Twiddles of the warp FFT in stage order: radix-4 stage s (Ns = 4^s) holds
+// entries [k][r - 1] = tw[(r k N / (4 Ns)) mod N] at offset 4^s - 1, the
+// radix-2 stage (when log2 N is odd) entries [k] = tw[k N / (2 Ns)] after
+// them; fewer than N entries in all.  A half warp reads consecutive k, 24 or
+// 8 bytes apart: distinct bank pairs.
 template <int N>
-__device__ __forceinline__ void warp_fft(float2* a, float2* b, const float2* __restrict__ tw, float sign, int lane)
+__device__ void fill_stage_twiddles(float2* tws, const float2* __restrict__ tw, int tid, int nthreads)
+{
+    int off = 0, Ns = 1;
+    for (; Ns * 4 <= N; off += 3 * Ns, Ns *= 4) {
+        const int twstep = N / (Ns * 4);
+        for (int e = tid; e < 3 * Ns; e += nthreads) {
+            const int k = e / 3, r = e - 3 * k + 1;
+            tws[off + e] = tw[(r * k * twstep) & (N - 1)];
+        }
+    }
+    if (Ns < N) {
+        const int twstep = N / (Ns * 2);
+        for (int k = tid; k < Ns; k += nthreads) tws[off + k] = tw[(k * twstep) & (N - 1)];
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void warp_fft(float2* a, float2* b, const float2* __restrict__ tws, float sign, int lane)
 {
     // Stockham radix-4 stages, then one radix-2 stage when log2(N) is odd;
-    // tw[m] = exp(-2 pi i m / N).  Result in a.
+    // twiddles from fill_stage_twiddles (forward table, conjugated for the
+    // inverse).  Input and result in a in natural order; the buffers
+    // between stages are in fsw order.
+    constexpr int n4 = []() { int n = 0; for (int m = 1; m * 4 <= N; m *= 4) n++; return n; }();
+    constexpr bool has2 = (1 << (2 * n4)) < N;
     float2* src = a;
     float2* dst = b;
-    int Ns = 1;
+    int Ns = 1, off = 0;
 #pragma unroll
-    for (int s = 0; (1 << (2 * s + 2)) <= N; s++) {
+    for (int s = 0; s < n4; s++) {
         constexpr int nbf = N / 4;
-        const int twstep = N / (Ns * 4);
+        const bool rsw = s > 0, wsw = has2 || s < n4 - 1;  // natural order at the ends
 #pragma unroll
         for (int j = lane; j < nbf; j += 32) {
             const int k = j & (Ns - 1);
             float2 v[4];
 #pragma unroll
             for (int r = 0; r < 4; r++) {
-                float2 x = src[j + r * nbf];
+                const int si = j + r * nbf;
+                float2 x = src[rsw ? fsw(si) : si];
                 if (r && k) {
-                    float2 w = tw[(r * k * twstep) & (N - 1)];
+                    float2 w = tws[off + 3 * k + r - 1];
                     w.y *= -sign;
                     x = cmul(x, w);
                 }
@@ -282,26 +316,29 @@ __device__ __forceinline__ void warp_fft(float2* a, float2* b, const float2* __r
             const float2 d13 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
             const float2 jd13 = make_float2(-sign * d13.y, sign * d13.x);
             const int idx = (j - k) * 4 + k;
-            dst[idx] = make_float2(s02.x + s13.x, s02.y + s13.y);
-            dst[idx + Ns] = make_float2(d02.x + jd13.x, d02.y + jd13.y);
-            dst[idx + 2 * Ns] = make_float2(s02.x - s13.x, s02.y - s13.y);
-            dst[idx + 3 * Ns] = make_float2(d02.x - jd13.x, d02.y - jd13.y);
+            const float2 o[4] = {make_float2(s02.x + s13.x, s02.y + s13.y), make_float2(d02.x + jd13.x, d02.y + jd13.y),
+                                 make_float2(s02.x - s13.x, s02.y - s13.y), make_float2(d02.x - jd13.x, d02.y - jd13.y)};
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int di = idx + c * Ns;
+                dst[wsw ? fsw(di) : di] = o[c];
+            }
         }
         __syncwarp();
         float2* t = src;
         src = dst;
         dst = t;
+        off += 3 * Ns;
         Ns *= 4;
     }
-    if (Ns < N) {  // radix-2 stage
+    if (has2) {  // radix-2 stage: reads fsw order, writes natural order
         constexpr int nbf = N / 2;
-        const int twstep = N / (Ns * 2);
 #pragma unroll
         for (int j = lane; j < nbf; j += 32) {
             const int k = j & (Ns - 1);
-            float2 x0 = src[j], x1 = src[j + nbf];
+            float2 x0 = src[fsw(j)], x1 = src[fsw(j + nbf)];
             if (k) {
-                float2 w = tw[(k * twstep) & (N - 1)];
+                float2 w = tws[off + k];
                 w.y *= -sign;
                 x1 = cmul(x1, w);
             }
@@ -340,7 +377,7 @@ __global__ void __launch_bounds__(kPfdrThreads) k_pfdr_stream(const PfdrArgs A, 
     const size_t slab = size_t(A.N_v0) * A.N_u1 * N_u0;
     const float* base = A.g + (size_t(iv0) * A.N_u1 + iu1_0) * N_u0;
     const int nsl = A.N_v1;
-    for (int i = tid; i < NX; i += blockDim.x) tw[i] = A.tw[i];
+    fill_stage_twiddles<NX>(tw, A.tw, tid, blockDim.x);
     if (tid == 0) {
         for (int q = 0; q < kPfdrStages; q++) mbar_init(&full[q], 1);
         fence_barrier_init();

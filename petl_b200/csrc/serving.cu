@@ -20,11 +20,12 @@
 //    (the GPU is full with one of them), small ones overlap with them and
 //    with each other, and new requests join while others run;
 //  * batched launches: when a request of a geometry whose subset steps are
-//    too small to fill the device issues a step, up to seven younger active
-//    requests of its geometry and subset count with no step in flight join
-//    it, each at its own subset: one launch of each projector kernel (and of
-//    the image update) serves them all, on the first one's stream, ordered
-//    after and before each member's own stream by events;
+//    too small to fill the device issues a step with none in flight, up to
+//    seven younger active requests of its geometry and subset count with no
+//    step in flight join it, each at its own subset: one launch of each
+//    projector kernel (and of the image update) serves them all, on the
+//    first one's stream, ordered after and before each member's own stream
+//    by events;
 //  * completion: after the last step the image is copied to a pinned host
 //    buffer, the device memory is returned to the stream-ordered pool and
 //    the request's latency (submit to result on the host) is recorded;
@@ -627,12 +628,15 @@ void Server::run()
                 }
             }
             while (can_step(r) && (oldest || inflight_work + r.work <= cap)) {
-                // younger requests of the same geometry state with no step in
-                // flight join this one's launches (small steps of the split
-                // projector only)
+                // younger requests of the same geometry state join this one's
+                // launches (small steps of the split projector only) when
+                // neither has a step in flight: the batch then waits on no
+                // other stream, and no chain of batches ties the streams
+                // together (a leader with steps in flight measured 0.6x the
+                // throughput of unbatched steps at 200 small requests/s)
                 std::vector<Request*> ms{&r};
                 double w = r.work;
-                if (batch_max > 1 && r.gs && r.gs->batch)
+                if (batch_max > 1 && r.gs && r.gs->batch && r.inflight.empty())
                     for (size_t aj = ai + 1; aj < active.size() && int(ms.size()) < batch_max; aj++) {
                         Request& q = *active[aj];
                         if (q.gs != r.gs || !can_step(q) || !q.inflight.empty() || inflight_work + w + q.work > cap)

@@ -272,12 +272,12 @@ def study_storage(seed=0, iters=10, subsets=8):
             "proj_rel_l2_bf16_vs_fp32": float((p16 - p32).norm() / p32.norm())}
 
 
-def _serving_requests(n, rate, seed, device):
+def _serving_requests(n, rate, seed, device, sizes=(64, 128, 192, 256)):
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, n))
     reqs = []
     for i in range(n):
-        N = int(rng.choice([64, 128, 192, 256]))
+        N = int(rng.choice(list(sizes)))
         T = float(rng.choice([1.0, 1.5, 2.0]))
         D = float(rng.choice([200.0, 250.0, 300.0]))
         counts = float(math.exp(rng.uniform(math.log(1e5), math.log(5e7))))
@@ -287,7 +287,8 @@ def _serving_requests(n, rate, seed, device):
     return reqs
 
 
-def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, modes=("arrivals", "saturation")):
+def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, modes=("arrivals", "saturation"),
+                  sizes=(64, 128, 192, 256)):
     """The serving workload: n OSEM requests with seeded Poisson arrivals at
     `rate`/s (mode "arrivals") or all submitted at t = 0 ("saturation"),
     served (a) by the continuous-batching server (like-geometry requests in
@@ -295,9 +296,10 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, mode
     time by the plain device path (host data to the device, recon.osem, the
     image back to the host, in arrival order).  Latency is host wall clock
     from a request's arrival to its image on the host; recons/s is n over
-    the time from the first arrival to the last result."""
+    the time from the first arrival to the last result.  `sizes` restricts
+    the volume sizes N drawn (the workload draws all four)."""
     from .serving import ReconServer
-    reqs = _serving_requests(n, rate, seed, "cuda")
+    reqs = _serving_requests(n, rate, seed, "cuda", sizes)
     # geometry classes: N in {64,128,192,256}, T in {1,1.5,2} mm, D in
     # {200,250,300} mm (the workload draws T and D from [1,2] and [200,300];
     # a request's work depends on them only through its planogram shape and
@@ -382,15 +384,20 @@ def study_serving(n=200, rate=20.0, seed=0, max_active=16, budget_gb=150.0, mode
         torch.cuda.synchronize()
         gpu_s += a.elapsed_time(b) / 1e3
     out = {"study": "serving", "workload": f"{n} OSEM requests, Poisson arrivals {rate}/s (seed {seed}), "
-           "N in {64,128,192,256} (vol NxNxN/2 at pitch T in {1,1.5,2} mm), L=H=N*T/2, D in {200,250,300} mm, "
+           f"N in {{{','.join(str(v) for v in sizes)}}} (vol NxNxN/2 at pitch T in {{1,1.5,2}} mm), L=H=N*T/2, "
+           "D in {200,250,300} mm, "
            "4 or 8 subsets, 2-6 iterations", "geometry_classes": len(classes), "budget_gb": budget_gb,
            "gpu_seconds_per_request": gpu_s / n,
            "bound_recons_per_s": n / gpu_s,
            "bound_note": "device time of the requests run alone back to back: no schedule of them on one GPU "
                          "serves more than n / that many per second unless requests share launches"}
+    # an unmeasured pass first: the library's memory pool grows to the
+    # workload's peak in whichever pass runs first (about 10 % of that
+    # pass's throughput when measured)
+    serve_server("saturation", batch=1)
     for mode in modes:
-        srv = serve_server(mode)
         unb = serve_server(mode, batch=1)
+        srv = serve_server(mode)
         seq = serve_sequential(mode)
         out[mode] = {"server": srv, "server_unbatched": unb, "one_at_a_time": seq,
                      "throughput_ratio": srv["recons_per_s"] / seq["recons_per_s"],
@@ -557,12 +564,15 @@ def main(argv=None):
                                       "response", "kernels"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--sizes", default="64,128,192,256", help="serving: volume sizes N drawn")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     a = ap.parse_args(argv)
     fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
           "binning": study_binning, "corrections": study_corrections, "response": study_response,
           "kernels": study_kernels}
     if a.study == "serving":
-        res = study_serving(n=a.requests, seed=a.seed)
+        res = study_serving(n=a.requests, seed=a.seed, rate=a.rate,
+                            sizes=tuple(int(v) for v in a.sizes.split(",")))
     else:
         res = fn[a.study](seed=a.seed)
     print(json.dumps(res))
