@@ -32,6 +32,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "common.cuh"
 #include "projector.cuh"
@@ -544,6 +545,7 @@ struct XgatherArgs {
     float scale;
     Tables T;
     Members M;       // volumes (out) and views of the chunk
+    int bplanes;     // planes of the scratch: numY, or 1 when its z sums do not depend on the plane
 };
 
 constexpr int XR = 4;         // volume rows z per k_bwd_xgather thread
@@ -574,7 +576,8 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
     for (int r = 0; r < XR; r++)
         acc[r] = (!A.first && r < nz) ? part[(size_t(z0 + r) * NY + y) * NX + x] : 0.0f;
     const int rlast = nz - 1;
-    const float* Bm = B + size_t(mb) * A.M.nvm * NY * NZ * NUc;
+    const int yb = A.bplanes == 1 ? 0 : y;  // the scratch plane of y
+    const float* Bm = B + size_t(mb) * A.M.nvm * A.bplanes * NZ * NUc;
 #pragma unroll 4
     for (int vi = 0; vi < nvb; vi++) {
         const Shift xs = s_xs[vi];
@@ -583,7 +586,7 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
         const bool okm = unsigned(j0 - 1) < unsigned(NU0), ok0 = unsigned(j0) < unsigned(NU0);
         // in-bounds addresses for every tap; the out-of-range ones are selected away
         const int jm = min(max(j0 - 1, 0), NU0 - 1), jz = min(max(j0, 0), NU0 - 1);
-        const float* Bv = Bm + ((size_t(vi) * NY + y) * NZ + z0) * NUc;
+        const float* Bv = Bm + ((size_t(vi) * A.bplanes + yb) * NZ + z0) * NUc;
 #pragma unroll
         for (int r = 0; r < XR; r++) {
             const int rr = min(r, rlast);
@@ -600,6 +603,92 @@ __global__ void __launch_bounds__(256) k_bwd_xgather(const float* __restrict__ B
         else
             f[o] = A.accumulate ? f[o] + A.scale * acc[r] : A.scale * acc[r];
     }
+}
+
+// z sums of one slope with v1 = 0 (the rebinned planogram of FBP), whose
+// z taps and visible rows are the same on every plane: B[view][z][c] =
+// S (1 - w) g[z - d][c] then + S w g[z - d - 1][c], the operations and
+// masks of k_bwd_zgather for a single slope (rows outside the planogram
+// read zero; the adjoint zeroes rows outside the visible u1 range and
+// columns outside the view's visible u0 range, the reference semantics
+// leave rows z outside the voxel test at zero).  Thread = column c of row z
+// of one view; grid (ceil(N_u0 / 256), numZ, views).
+struct FlatArgs {
+    petl_geom G;
+    int iv1;    // the slope
+    int first;  // first view
+    int step;   // view step
+    int NUc;    // scratch row pitch
+    Tables T;
+};
+
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_bwd_zflat(const float* __restrict__ g, float* __restrict__ B, const FlatArgs A)
+{
+    const petl_geom& G = A.G;
+    const int c = blockIdx.x * 256 + threadIdx.x, z = blockIdx.y, vi = blockIdx.z;
+    if (c >= G.N_u0) return;
+    const int v0 = A.first + vi * A.step;
+    const Shift zs = A.T.zt[size_t(A.iv1) * G.numY];  // plane 0: every plane has the same
+    const float S = A.T.S[size_t(A.iv1) * G.N_v0 + v0];
+    const float w0 = S * (1.0f - zs.w), w1 = S * zs.w;
+    const int2 ub1 = A.T.ub1[A.iv1];
+    auto row = [&](int r) {
+        const bool in = r >= 0 && r < G.N_u1 && (!ADJ || (r >= ub1.x && r <= ub1.y));
+        return in ? g[((size_t(A.iv1) * G.N_v0 + v0) * G.N_u1 + r) * G.N_u0 + c] : 0.0f;
+    };
+    float zsum = 0.0f;
+    bool live;
+    if (ADJ) {
+        live = true;
+    } else {
+        const int2 zv = A.T.zvis[size_t(A.iv1) * G.numY];
+        live = z >= zv.x && z <= zv.y;
+    }
+    if (live) zsum = fmaf(w1, row(z - zs.d - 1), fmaf(w0, row(z - zs.d), 0.0f));
+    if (ADJ) {
+        const int2 u0r = A.T.ub0[v0];
+        if (c < u0r.x || c > u0r.y) zsum = 0.0f;
+    }
+    B[(size_t(vi) * G.numZ + z) * A.NUc + c] = zsum;
+}
+
+int backproject_flat(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
+                     const ViewRange& vr, const Tables& T, cudaStream_t st)
+{
+    const int n_v0 = vr.n_v0(G.N_v0);
+    if (n_v0 <= 0 || n_v0 > 4096 || n_v0 > 65535 || G.N_u0 > XMAXN || G.numZ > 65535 || G.numY > 65535)
+        return kNotApplicable;
+    const int NUc = (G.N_u0 + 3) & ~3;
+    float* B = nullptr;
+    if (scratch_alloc(reinterpret_cast<void**>(&B), size_t(n_v0) * G.numZ * NUc * 4, st) != cudaSuccess) {
+        cudaGetLastError();
+        return kNotApplicable;
+    }
+    const FlatArgs FA{G, vr.iv1_begin, vr.iv0_first, vr.iv0_step, NUc, T};
+    const dim3 grid(ceil_div(G.N_u0, 256), unsigned(G.numZ), unsigned(n_v0));
+    if (mode == PETL_BP_ADJOINT)
+        k_bwd_zflat<true><<<grid, 256, 0, st>>>(g, B, FA);
+    else
+        k_bwd_zflat<false><<<grid, 256, 0, st>>>(g, B, FA);
+    note_launch();
+    Members M;
+    M.nb = 1;
+    M.nvm = n_v0;
+    M.first[0] = vr.iv0_first;
+    M.nv[0] = n_v0;
+    M.out[0] = f;
+    const XgatherArgs X{G, vr.iv0_step, NUc, 1, 1, accumulate, scale, T, M, 1};
+    k_bwd_xgather<1><<<dim3(ceil_div(G.numX, 256), ceil_div(G.numZ, XR), unsigned(G.numY)), 256,
+                       size_t(n_v0) * sizeof(Shift), st>>>(B, nullptr, X);
+    note_launch();
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(B, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("backproject_flat: ") + cudaGetErrorString(e));
+        return int(e);
+    }
+    return 0;
 }
 
 }  // namespace
@@ -619,6 +708,12 @@ int backproject_split_m(const petl_geom& G, const Members& M0, int mode, int acc
     for (int b = 0; b < nb; b++) nvmax = std::max(nvmax, M0.nv[b]);
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (nvmax <= 0 || nv1 <= 0 || nv1 > GV1MAX) return kNotApplicable;
+    // one slope at v1 = 0 (FBP's rebinned planogram): z sums without a plane
+    // dimension
+    if (std::is_same<TG, float>::value && nb == 1 && nv1 == 1 && M0.first[0] == vr.iv0_first &&
+        M0.nv[0] == vr.n_v0(G.N_v0) && std::fmaf(float(vr.iv1_begin), G.T_v1, G.v1_0) == 0.0f)
+        return backproject_flat(G, static_cast<const float*>(M0.in[0]), static_cast<float*>(M0.out[0]), mode,
+                                accumulate, scale, vr, T, st);
     // the scratch holds a volume per view whatever the slope count: below
     // about ten slopes (the 2-D backprojection of FBP has one) the
     // single-pass kernel is cheaper than that round trip
@@ -721,7 +816,7 @@ int backproject_split_m(const petl_geom& G, const Members& M0, int mode, int acc
         else
             kzm<<<dim3(ntile, unsigned(A.gpm) * unsigned(nb)), GNT, smem, st>>>(maps, B, A);
         note_launch();
-        XgatherArgs X{G, vr.iv0_step, A.NUc, c == 0, c == nchunks - 1, accumulate, scale, T, M};
+        XgatherArgs X{G, vr.iv0_step, A.NUc, c == 0, c == nchunks - 1, accumulate, scale, T, M, G.numY};
         kx<<<dim3(ceil_div(G.numX, 256), ceil_div(G.numZ, XR), unsigned(G.numY) * unsigned(nb)), 256,
                         size_t(nvc) * sizeof(Shift), st>>>(B, part, X);
         note_launch();

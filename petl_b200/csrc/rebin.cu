@@ -24,8 +24,12 @@
 // memory (N_u0^2 FMAs per row, a few microseconds for the whole planogram),
 // fused with the inverse planogram weight that PETL::doFBP applies next
 // (src/planogram.cpp:304-333).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -545,12 +549,78 @@ k_ramp(float* __restrict__ g, int nrows, int N, int rows_per_view, const float* 
     }
 }
 
-template <class T>
-int upload(const std::vector<T>& v, T** d, cudaStream_t st)
+// Device copies of the host-computed tables of a geometry, kept for later
+// calls (per device, up to kTableCacheSize geometries, oldest dropped):
+// building and uploading them per call from pageable memory kept the device
+// idle for tens of microseconds before every PFDR launch.  An entry is one
+// allocation holding every table at 256-byte aligned offsets; its upload is
+// stream-ordered on the stream of the call that built it, and later calls
+// on any stream wait for its event.
+struct TableBlob {
+    std::vector<unsigned char> bytes;
+    size_t add(const void* src, size_t n)
+    {
+        const size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + n);
+        std::memcpy(bytes.data() + off, src, n);
+        return off;
+    }
+};
+
+struct CachedTables {
+    unsigned char* base = nullptr;
+    cudaEvent_t ready = nullptr;
+    unsigned long long last_use = 0;
+    std::vector<size_t> off;  // offsets of the tables in the allocation
+    std::vector<int> ints;    // host-side scalars the caller stores with them
+};
+
+constexpr size_t kTableCacheSize = 16;
+std::mutex g_table_mu;
+std::map<std::string, CachedTables> g_tables;
+unsigned long long g_table_clock = 0;
+
+// The cached tables under `key` (built by `make` on a miss: fills the blob
+// and the scalars), the stream made to wait for their upload; null on a
+// CUDA failure.  The caller holds g_table_mu until its launches that read
+// the tables are enqueued (an eviction waits for the device to finish them).
+template <class Make>
+const CachedTables* cached_tables(const std::string& key0, cudaStream_t st, Make make)
 {
-    PETL_CUDA(scratch_alloc(reinterpret_cast<void**>(d), sizeof(T) * v.size(), st));
-    PETL_CUDA(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
-    return 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    const std::string key = key0 + std::string(reinterpret_cast<const char*>(&dev), sizeof(dev));
+    auto it = g_tables.find(key);
+    if (it == g_tables.end()) {
+        if (g_tables.size() >= kTableCacheSize) {  // drop the least recently used
+            auto old = g_tables.begin();
+            for (auto jt = g_tables.begin(); jt != g_tables.end(); ++jt)
+                if (jt->second.last_use < old->second.last_use) old = jt;
+            cudaEventSynchronize(old->second.ready);  // its users' reads were enqueued after its upload
+            cudaDeviceSynchronize();                   // and have finished
+            cudaFree(old->second.base);
+            cudaEventDestroy(old->second.ready);
+            g_tables.erase(old);
+        }
+        CachedTables c;
+        TableBlob blob;
+        make(blob, c.off, c.ints);
+        if (cudaMalloc(reinterpret_cast<void**>(&c.base), std::max<size_t>(blob.bytes.size(), 256)) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        if (cudaMemcpyAsync(c.base, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(c.ready, st) != cudaSuccess) {
+            cudaFree(c.base);
+            return nullptr;
+        }
+        it = g_tables.emplace(key, std::move(c)).first;
+    } else if (cudaStreamWaitEvent(st, it->second.ready, 0) != cudaSuccess) {
+        return nullptr;
+    }
+    it->second.last_use = ++g_table_clock;
+    return &it->second;
 }
 
 // host float helpers that must not be contracted into fused multiply-adds
@@ -566,58 +636,43 @@ int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
     const FFTPlan plan = make_plan(NX);
     PETL_REQUIRE(plan.nstages > 0 && NX <= kMaxFFT, "PFDR: unsupported transform size");
     const int NXH = NX / 2 + 1;
-    // tables (src/pfdr.cu:16-40, 78-124, 126-142, 144-157)
-    const float T_U = float(1.0 / (NX * G.T_u0));
-    const float aperture = float(1 / (2.0 * G.T_u1 * 2.0 * G.v_m0));
-    std::vector<float> absU(NXH), v1ap(G.N_v1), row_w(size_t(G.N_v1) * G.N_v0), norm(NXH), out_w(G.N_v0);
-    std::vector<unsigned char> central(G.N_v1);
-    std::vector<float2> tw(NX);
-    for (int i = 0; i < NXH; i++) {
-        const float U = i < NX / 2 ? fmul_h(float(i), T_U) : fmul_h(float(i - NX), T_U);
-        absU[i] = std::fabs(U);
-    }
-    std::vector<int> count(NXH, 0);
-    for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
-        const float v1 = fadd_h(fmul_h(float(iv1), G.T_v1), G.v1_0);  // planogram::v1 on the host
-        const float av = std::fabs(v1);
-        central[iv1] = av <= fmul_h(0.5f, G.T_v1);
-        v1ap[iv1] = fmul_h(av, aperture);
-        for (int i = 0; i < NXH; i++)
-            if (central[iv1] || absU[i] > v1ap[iv1]) count[i]++;
-        for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
-            const float v0 = std::fmaf(G.T_v0, float(iv0), G.v0_0);  // device expression, contracted
-            row_w[size_t(iv1) * G.N_v0 + iv0] = float(1.0 / std::sqrt(1.0 + double(v1) * v1 + double(v0) * v0));
+    // the tables of the geometry (src/pfdr.cu:16-40, 78-124, 126-142,
+    // 144-157), built on the host once per geometry
+    auto make = [&](TableBlob& blob, std::vector<size_t>& off, std::vector<int>& ints) {
+        const float T_U = float(1.0 / (NX * G.T_u0));
+        const float aperture = float(1 / (2.0 * G.T_u1 * 2.0 * G.v_m0));
+        std::vector<float> absU(NXH), v1ap(G.N_v1), row_w(size_t(G.N_v1) * G.N_v0), norm(NXH), out_w(G.N_v0);
+        std::vector<unsigned char> central(G.N_v1);
+        std::vector<float2> tw(NX);
+        for (int i = 0; i < NXH; i++) {
+            const float U = i < NX / 2 ? fmul_h(float(i), T_U) : fmul_h(float(i - NX), T_U);
+            absU[i] = std::fabs(U);
         }
-    }
-    for (int i = 0; i < NXH; i++) norm[i] = float(1.0 / (double(NX) * ((i != 0 && count[i] > 0) ? count[i] : 1)));
-    for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
-        const float v0 = std::fmaf(G.T_v0, float(iv0), G.v0_0);
-        out_w[iv0] = float(std::sqrt(1.0 + double(v0) * v0));
-    }
-    const double PI = 3.14159265358979323846;
-    for (int m = 0; m < NX; m++) tw[m] = make_float2(float(std::cos(-2.0 * PI * m / NX)), float(std::sin(-2.0 * PI * m / NX)));
-
-    PfdrArgs A{};
-    A.g = g;
-    A.g_reb = g_reb;
-    A.N_v1 = G.N_v1; A.N_v0 = G.N_v0; A.N_u1 = G.N_u1; A.N_u0 = G.N_u0;
-    A.NX = NX;
-    A.plan = plan;
-    float *d_absU = nullptr, *d_v1ap = nullptr, *d_roww = nullptr, *d_norm = nullptr, *d_outw = nullptr;
-    unsigned char* d_central = nullptr;
-    float2* d_tw = nullptr;
-    int rc = 0;
-    if ((rc = upload(absU, &d_absU, st)) || (rc = upload(v1ap, &d_v1ap, st)) || (rc = upload(row_w, &d_roww, st)) ||
-        (rc = upload(norm, &d_norm, st)) || (rc = upload(out_w, &d_outw, st)) || (rc = upload(central, &d_central, st)) ||
-        (rc = upload(tw, &d_tw, st)))
-        return rc;
-    A.absU = d_absU; A.v1ap = d_v1ap; A.row_w = d_roww; A.norm = d_norm; A.out_w = d_outw; A.central = d_central;
-    A.tw = d_tw;
-    // processing order for the streamed kernel: slope iv1 with its mirror
-    // N_v1 - 1 - iv1 when both have bit-identical masks (central flag and
-    // threshold), else alone
-    std::vector<int> order, gfirst;
-    {
+        std::vector<int> count(NXH, 0);
+        for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
+            const float v1 = fadd_h(fmul_h(float(iv1), G.T_v1), G.v1_0);  // planogram::v1 on the host
+            const float av = std::fabs(v1);
+            central[iv1] = av <= fmul_h(0.5f, G.T_v1);
+            v1ap[iv1] = fmul_h(av, aperture);
+            for (int i = 0; i < NXH; i++)
+                if (central[iv1] || absU[i] > v1ap[iv1]) count[i]++;
+            for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+                const float v0 = std::fmaf(G.T_v0, float(iv0), G.v0_0);  // device expression, contracted
+                row_w[size_t(iv1) * G.N_v0 + iv0] = float(1.0 / std::sqrt(1.0 + double(v1) * v1 + double(v0) * v0));
+            }
+        }
+        for (int i = 0; i < NXH; i++) norm[i] = float(1.0 / (double(NX) * ((i != 0 && count[i] > 0) ? count[i] : 1)));
+        for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+            const float v0 = std::fmaf(G.T_v0, float(iv0), G.v0_0);
+            out_w[iv0] = float(std::sqrt(1.0 + double(v0) * v0));
+        }
+        const double PI = 3.14159265358979323846;
+        for (int m = 0; m < NX; m++)
+            tw[m] = make_float2(float(std::cos(-2.0 * PI * m / NX)), float(std::sin(-2.0 * PI * m / NX)));
+        // processing order for the streamed kernel: slope iv1 with its mirror
+        // N_v1 - 1 - iv1 when both have bit-identical masks (central flag and
+        // threshold), else alone
+        std::vector<int> order, gfirst;
         std::vector<char> done(G.N_v1, 0);
         for (int iv1 = 0; iv1 < G.N_v1; iv1++) {
             if (done[iv1]) continue;
@@ -632,13 +687,36 @@ int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
             }
         }
         gfirst.push_back(int(order.size()));
+        off = {blob.add(absU.data(), 4 * absU.size()), blob.add(v1ap.data(), 4 * v1ap.size()),
+               blob.add(row_w.data(), 4 * row_w.size()), blob.add(norm.data(), 4 * norm.size()),
+               blob.add(out_w.data(), 4 * out_w.size()), blob.add(central.data(), central.size()),
+               blob.add(tw.data(), 8 * tw.size()), blob.add(order.data(), 4 * order.size()),
+               blob.add(gfirst.data(), 4 * gfirst.size())};
+        ints = {int(gfirst.size()) - 1};
+    };
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    const CachedTables* c = cached_tables(std::string("pfdr") + std::string(reinterpret_cast<const char*>(&G), sizeof G),
+                                          st, make);
+    if (!c) {
+        set_error("PFDR: table upload failed");
+        return int(cudaErrorMemoryAllocation);
     }
-    int* d_order = nullptr;
-    int* d_gfirst = nullptr;
-    if ((rc = upload(order, &d_order, st)) || (rc = upload(gfirst, &d_gfirst, st))) return rc;
-    A.order = d_order;
-    A.gfirst = d_gfirst;
-    A.ngroups = int(gfirst.size()) - 1;
+    PfdrArgs A{};
+    A.g = g;
+    A.g_reb = g_reb;
+    A.N_v1 = G.N_v1; A.N_v0 = G.N_v0; A.N_u1 = G.N_u1; A.N_u0 = G.N_u0;
+    A.NX = NX;
+    A.plan = plan;
+    A.absU = reinterpret_cast<const float*>(c->base + c->off[0]);
+    A.v1ap = reinterpret_cast<const float*>(c->base + c->off[1]);
+    A.row_w = reinterpret_cast<const float*>(c->base + c->off[2]);
+    A.norm = reinterpret_cast<const float*>(c->base + c->off[3]);
+    A.out_w = reinterpret_cast<const float*>(c->base + c->off[4]);
+    A.central = c->base + c->off[5];
+    A.tw = reinterpret_cast<const float2*>(c->base + c->off[6]);
+    A.order = reinterpret_cast<const int*>(c->base + c->off[7]);
+    A.gfirst = reinterpret_cast<const int*>(c->base + c->off[8]);
+    A.ngroups = c->ints[0];
     // the streamed kernel: bulk copies need 16-byte aligned rows of slices
     const bool rows_ok = (G.N_u0 % 4) == 0 && (reinterpret_cast<uintptr_t>(g) & 15) == 0 && G.N_u0 <= NX &&
                          dispatch_mode() != 2;  // dispatch 2: the first-generation kernel
@@ -658,9 +736,6 @@ int pfdr(const petl_geom& G, const float* g, float* g_reb, cudaStream_t st)
             note_launch();
         }
     }
-    cudaFreeAsync(d_absU, st); cudaFreeAsync(d_v1ap, st); cudaFreeAsync(d_roww, st); cudaFreeAsync(d_norm, st);
-    cudaFreeAsync(d_outw, st); cudaFreeAsync(d_central, st); cudaFreeAsync(d_tw, st);
-    cudaFreeAsync(d_order, st); cudaFreeAsync(d_gfirst, st);
     if (e != cudaSuccess) {
         set_error(std::string("PFDR: ") + cudaGetErrorString(e));
         return int(e);
@@ -673,26 +748,36 @@ int ramp(const petl_geom& G, float* g_reb, int apply_weight, cudaStream_t st)
     const int N = G.N_u0;
     PETL_REQUIRE(N > 0 && N <= 4096, "ramp: unsupported row length");
     // h[s] = 1/(T pi (1/4 - s^2)) stored as float, as rampImpulseResponse
-    std::vector<float> h(2 * N - 1);
-    const double PI = 3.1415926535897932385;
-    const float T = G.T_u0;
-    for (int i = 0; i < 2 * N - 1; i++) {
-        const float s = float(i - (N - 1));
-        h[i] = float(1.0 / (T * PI * (0.25 - s * s)));
-    }
-    // inverse planogram weight per view (apply_planogram_weight(true))
-    std::vector<float> vw(G.N_v0, 1.0f);
-    if (apply_weight) {
-        const float v1 = fadd_h(fmul_h(0.0f, G.T_v1), G.v1_0);
-        for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
-            const float v0 = fadd_h(fmul_h(float(iv0), G.T_v0), G.v0_0);
-            const float c = float(1.0 / std::sqrt(1.0 + double(v1) * v1 + double(v0) * v0));
-            vw[iv0] = float(1.0 / c);
+    auto make = [&](TableBlob& blob, std::vector<size_t>& off, std::vector<int>&) {
+        std::vector<float> h(2 * N - 1);
+        const double PI = 3.1415926535897932385;
+        const float T = G.T_u0;
+        for (int i = 0; i < 2 * N - 1; i++) {
+            const float s = float(i - (N - 1));
+            h[i] = float(1.0 / (T * PI * (0.25 - s * s)));
         }
+        // inverse planogram weight per view (apply_planogram_weight(true))
+        std::vector<float> vw(G.N_v0, 1.0f);
+        if (apply_weight) {
+            const float v1 = fadd_h(fmul_h(0.0f, G.T_v1), G.v1_0);
+            for (int iv0 = 0; iv0 < G.N_v0; iv0++) {
+                const float v0 = fadd_h(fmul_h(float(iv0), G.T_v0), G.v0_0);
+                const float c = float(1.0 / std::sqrt(1.0 + double(v1) * v1 + double(v0) * v0));
+                vw[iv0] = float(1.0 / c);
+            }
+        }
+        off = {blob.add(h.data(), 4 * h.size()), blob.add(vw.data(), 4 * vw.size())};
+    };
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    const CachedTables* c = cached_tables(std::string(apply_weight ? "rampw" : "ramp") +
+                                              std::string(reinterpret_cast<const char*>(&G), sizeof G),
+                                          st, make);
+    if (!c) {
+        set_error("ramp: table upload failed");
+        return int(cudaErrorMemoryAllocation);
     }
-    float *d_h = nullptr, *d_vw = nullptr;
-    int rc = 0;
-    if ((rc = upload(h, &d_h, st)) || (rc = upload(vw, &d_vw, st))) return rc;
+    const float* d_h = reinterpret_cast<const float*>(c->base + c->off[0]);
+    const float* d_vw = reinterpret_cast<const float*>(c->base + c->off[1]);
     const int nrows = G.N_v0 * G.N_u1;
     const size_t smem = sizeof(float) * (size_t(2 * N - 1) + size_t(kRampRows) * N);
     cudaError_t e = cudaFuncSetAttribute(k_ramp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -701,8 +786,6 @@ int ramp(const petl_geom& G, float* g_reb, int apply_weight, cudaStream_t st)
         e = cudaGetLastError();
         note_launch();
     }
-    cudaFreeAsync(d_h, st);
-    cudaFreeAsync(d_vw, st);
     if (e != cudaSuccess) {
         set_error(std::string("ramp: ") + cudaGetErrorString(e));
         return int(e);

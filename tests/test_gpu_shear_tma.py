@@ -200,3 +200,36 @@ def test_tma_full_size_against_first_generation(cuda):
         assert (px, pz, pw) == (2, 1, 2)
         assert torch.equal(x, w)
         assert float(torch.linalg.vector_norm(x - z) / torch.linalg.vector_norm(z)) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["t2", "rag4", "odd", "wide", "p90rag"])
+@pytest.mark.parametrize("mode", ["reference", "adjoint"])
+def test_single_slope_backprojection(cuda, name, mode):
+    """The rebinned planogram of FBP (one slope, v1 = 0) backprojects through
+    z sums without a plane dimension; bit-equal to the single-pass kernel
+    and within 1e-5 of the oracle (reference semantics), with accumulate and
+    scale applied as the C ABI passes them."""
+    import torch
+    from petl_b200 import lib, ops
+    G, Go, f, rng = _setup(name, cuda)
+    Gr = G.rebinned()
+    Gro = O.make_geom(*CASES[name][0], CASES[name][1])
+    Gro.N_v1, Gro.v1_0 = 1, 0.0
+    y = _t(rng.random(Gr.shape), cuda)
+    a, pa = _under(0, lambda: _np(ops.backproject(Gr, y, mode=mode)))
+    d, pd = _under(3, lambda: _np(ops.backproject(Gr, y, mode=mode)))
+    assert pa == pd
+    assert np.array_equal(a, d)
+    if mode == "reference":
+        assert rel_l2(a, O.backproject(Gro, _np(y))) < 1e-5
+    # accumulate with a scale: f + 0.5 A^T y
+    L = lib()
+    base = _t(rng.random(Gr.vol_shape), cuda)
+    out = base.clone()
+    m = 0 if mode == "reference" else 1
+    assert L.petl_backproject_dev(Gr.ptr, y.data_ptr(), out.data_ptr(), m, 1, 0.5, 0, 1,
+                                  torch.cuda.current_stream().cuda_stream) == 0
+    torch.cuda.synchronize()
+    assert L.petl_device_error_flag() == 0
+    want = _np(base) + 0.5 * a
+    assert np.abs(_np(out) - want).max() <= 1e-6 * np.abs(want).max()
