@@ -77,16 +77,15 @@ __host__ __device__ constexpr int gpat_offsets(int pid)
 // (0..6: the straight-line pattern of fully visible planes; 8..14: the same
 // pattern with per-plane row intervals; kPatGen: per-plane taps), window row
 // in the stage << 20.  vm: window rows holding visible bins (adjoint).  ivl:
-// per plane the output rows that receive the slope, first | last << 4 (8, 8
-// for none): the rows inside the visible range (adjoint) or passing the
-// voxel test (reference).
+// per plane (8 bits each) the mask of output rows that receive the slope:
+// the rows inside the visible range (adjoint: all) or passing the voxel
+// test (reference).
 struct __align__(16) GEntry {
     uint32_t code;
     uint32_t vm;
     uint32_t ivl;
     uint32_t pad;
 };
-constexpr uint32_t kIvlNone = 0x88u;
 
 struct ZgatherArgs {
     petl_geom G;
@@ -145,21 +144,19 @@ __device__ __forceinline__ void g_taps4(float2 (&Z)[GP][GK], const float2 (&W)[G
     g_taps<(o >> 6) & 3, false>(Z[3], W, wb.z, wb.w, 0u, 0u);
 }
 
-// z taps of one plane restricted to output rows ka..kb (predicated; rows
-// outside receive nothing, as the masked taps' zero operands give)
+// z taps of one plane restricted to the output rows of mask m (predicated;
+// rows outside receive nothing, as the masked taps' zero operands give)
 template <int O>
 __device__ __forceinline__ void g_taps_ivl(float2 (&Z)[GK], const float2 (&W)[GWN], float w0, float w1,
-                                           uint32_t ivl)
+                                           uint32_t m)
 {
-    const int ka = int(ivl & 15u);
-    const unsigned span = unsigned(int((ivl >> 4) & 15u) - ka);
     const float2 a0 = dup(w0), a1 = dup(w1);
 #pragma unroll
     for (int k = 0; k < GK; k++)
-        if (unsigned(k - ka) <= span) Z[k] = fma2(a0, W[O + k + 1], Z[k]);
+        if ((m >> k) & 1u) Z[k] = fma2(a0, W[O + k + 1], Z[k]);
 #pragma unroll
     for (int k = 0; k < GK; k++)
-        if (unsigned(k - ka) <= span) Z[k] = fma2(a1, W[O + k], Z[k]);
+        if ((m >> k) & 1u) Z[k] = fma2(a1, W[O + k], Z[k]);
 }
 
 template <int PID>
@@ -314,15 +311,15 @@ k_bwd_zgather(const __grid_constant__ GMaps<NM> gmaps, float* __restrict__ B, co
 #pragma unroll
             for (int u = 0; u < GP; u++) {
                 const int o = dmx - dz[u];
-                uint32_t iv = kIvlNone;
+                uint32_t iv = 0u;  // no rows
                 if (mode[u]) {
                     if (o > GDW) bad = true;
                     code |= uint32_t(mode[u] | (min(o, 3) << 2)) << (4 * u);
                     if (ADJ || mode[u] == 1) {
-                        iv = 0x70u;  // rows 0..7 (adjoint: invisible window rows are zeroed instead)
+                        iv = 0xffu;  // rows 0..7 (adjoint: invisible window rows are zeroed instead)
                     } else {
                         const int ka = max(zv[u].x - zr, 0), kb = min(zv[u].y - zr, GK - 1);
-                        iv = uint32_t(ka) | uint32_t(kb) << 4;
+                        iv = kb >= ka ? (0xffu >> (7 - kb)) & (0xffu << ka) & 0xffu : 0u;
                     }
                 }
                 ivl |= iv << (8 * u);
@@ -496,9 +493,7 @@ k_bwd_zgather(const __grid_constant__ GMaps<NM> gmaps, float* __restrict__ B, co
                         }
                     } else {
                         // rows at the edge of the visible range: per-row masks
-                        const uint32_t iv = (en.ivl >> (8 * u)) & 0xffu;
-                        const uint32_t ka = iv & 15u, kb = iv >> 4;
-                        const uint32_t rows = kb >= ka && ka < 8u ? (0xffu >> (7u - kb)) & (0xffu << ka) : 0u;
+                        const uint32_t rows = (en.ivl >> (8 * u)) & 0xffu;
                         const uint32_t vm = ADJ ? en.vm : 0xffffffffu;
                         const uint32_t om = ADJ ? 0xffffffffu : rows;
                         switch (o) {
