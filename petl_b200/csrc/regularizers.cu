@@ -31,11 +31,13 @@ __device__ __forceinline__ size_t vidx(const Dims& d, int i, int j, int k)
 // --- relative differences (src/relative_differences.cu:13-28) -------------
 __device__ __forceinline__ float rd_clip(float v) { return v < 0.00000001f ? 0.0f : v; }
 
+// the division as the reference's --use_fast_math build computes it (as in
+// the gradient below)
 __device__ __forceinline__ float rd_pot(float x, float y, float delta)
 {
     if (x == y) return 0.0f;
     const float d = x - y;
-    return d * d / ((x + y) + delta * fabsf(d));
+    return __fdividef(d * d, (x + y) + delta * fabsf(d));
 }
 
 // --- p-Huber (src/total_variation.cu:33-78) --------------------------------
@@ -211,12 +213,20 @@ struct RdCostOp {
 struct TvCostOp {
     HuberP hb;
     float beta;
+    bool p_is_one;
     __device__ __forceinline__ float load(float v) const { return v; }
     template <class Nb>
     __device__ __forceinline__ double voxel(float x, float, Nb nb) const
     {
         float s[4] = {0.f, 0.f, 0.f, 0.f};
-        nb([&](int cls, float y, float) { s[cls] += hb.h(x - y); });
+        if (p_is_one) {  // slope * |t|^1 + shift beyond delta
+            nb([&](int cls, float y, float) {
+                const float t = x - y, a = fabsf(t);
+                s[cls] += a <= hb.delta ? 0.5f * t * t : hb.slope * a + hb.shift;
+            });
+        } else {
+            nb([&](int cls, float y, float) { s[cls] += hb.h(x - y); });
+        }
         return double(combine(s[1], s[2], s[3], beta));
     }
 };
@@ -224,15 +234,23 @@ struct TvCostOp {
 struct TvQuadOp {
     HuberP hb;
     float beta;
+    bool p_is_one;
     __device__ __forceinline__ float load(float v) const { return v; }
     template <class Nb>
     __device__ __forceinline__ double voxel(float x, float xd, Nb nb) const
     {
         float s[4] = {0.f, 0.f, 0.f, 0.f};
-        nb([&](int cls, float y, float yd) {
-            const float e = xd - yd;
-            s[cls] += hb.ddh(x - y) * e * e;
-        });
+        if (p_is_one) {  // p slope |t|^(p-2) = slope / |t| beyond delta
+            nb([&](int cls, float y, float yd) {
+                const float e = xd - yd, a = fabsf(x - y);
+                s[cls] += (a <= hb.delta ? 1.0f : hb.slope / a) * e * e;
+            });
+        } else {
+            nb([&](int cls, float y, float yd) {
+                const float e = xd - yd;
+                s[cls] += hb.ddh(x - y) * e * e;
+            });
+        }
         return double(combine(s[1], s[2], s[3], beta));
     }
 };
@@ -392,7 +410,7 @@ int petl_tv_cost_dev(const float* f, int N1, int N2, int N3, float delta, float 
     PETL_REQUIRE(f && out && dims_ok(N1, N2, N3), "tv_cost: invalid arguments");
     const HuberP hb = make_huber(delta, beta, p);
     const Dims d{N1, N2, N3};
-    return cost_tiled<TvCostOp, false>(f, nullptr, d, TvCostOp{hb, beta}, numNeighbors == 6 ? 6 : 26, N1 == 1, out,
+    return cost_tiled<TvCostOp, false>(f, nullptr, d, TvCostOp{hb, beta, p == 1.0f}, numNeighbors == 6 ? 6 : 26, N1 == 1, out,
                                        as_stream(stream), "tv_cost");
 }
 
@@ -402,7 +420,7 @@ int petl_tv_quadform_dev(const float* f, const float* dvec, int N1, int N2, int 
     PETL_REQUIRE(f && dvec && out && dims_ok(N1, N2, N3), "tv_quadform: invalid arguments");
     const HuberP hb = make_huber(delta, beta, p);
     const Dims d{N1, N2, N3};
-    return cost_tiled<TvQuadOp, true>(f, dvec, d, TvQuadOp{hb, beta}, numNeighbors == 6 ? 6 : 26, N1 == 1, out,
+    return cost_tiled<TvQuadOp, true>(f, dvec, d, TvQuadOp{hb, beta, p == 1.0f}, numNeighbors == 6 ? 6 : 26, N1 == 1, out,
                                       as_stream(stream), "tv_quadform");
 }
 
