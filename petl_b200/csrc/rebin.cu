@@ -549,6 +549,65 @@ k_ramp(float* __restrict__ g, int nrows, int N, int rows_per_view, const float* 
     }
 }
 
+// The same convolution with four adjacent outputs per thread: the taps of
+// columns i0..i0+3 at input k are h[N-1+i0+j-k], a window that moves by one
+// tap per k, so a thread loads one tap and eight row values per k for 32
+// FMAs (the kernel above loads nine values for 8).  Per output the same
+// fmaf chain over k in ascending order.  Block = 4 groups of 8 rows x 64
+// column quads; rows of up to kRamp4MaxN floats.
+constexpr int kRamp4Rows = 32;
+constexpr int kRamp4MaxN = 1024;
+__global__ void __launch_bounds__(256)
+k_ramp4(float* __restrict__ g, int nrows, int N, int rows_per_view, const float* __restrict__ h,
+        const float* __restrict__ view_w)
+{
+    extern __shared__ float rs[];
+    float* hs = rs;                // 2N + 4 taps, hs[N-1+s] = h(s), zero past the last
+    float* xs = hs + 2 * N + 4;    // kRamp4Rows * N
+    const int r0 = blockIdx.x * kRamp4Rows;
+    const int nr = min(kRamp4Rows, nrows - r0);
+    for (int i = threadIdx.x; i < 2 * N + 4; i += blockDim.x) hs[i] = i < 2 * N - 1 ? h[i] : 0.0f;
+    for (int i = threadIdx.x; i < kRamp4Rows * N; i += blockDim.x) {
+        const int r = i / N;
+        xs[i] = r < nr ? g[size_t(r0 + r) * N + (i - r * N)] : 0.0f;
+    }
+    __syncthreads();
+    const int grp = threadIdx.x >> 6, q0 = threadIdx.x & 63;
+    const float* xg = xs + grp * 8 * N;
+    for (int q = q0; 4 * q < N; q += 64) {
+        const int i0 = 4 * q;
+        float acc[8][4];
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[r][j] = 0.f;
+        float hw[4];  // hw[j] = h tap of column i0 + j at the current k
+#pragma unroll
+        for (int j = 0; j < 4; j++) hw[j] = hs[N - 1 + i0 + j];
+        for (int k = 0; k < N; k++) {
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const float xv = xg[r * N + k];
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[r][j] = fmaf(xv, hw[j], acc[r][j]);
+            }
+            hw[3] = hw[2];
+            hw[2] = hw[1];
+            hw[1] = hw[0];
+            hw[0] = k + 1 < N ? hs[N - 2 + i0 - k] : 0.0f;
+        }
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int row = r0 + grp * 8 + r;
+            if (grp * 8 + r >= nr) break;
+            const float w = view_w[row / rows_per_view];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (i0 + j < N) g[size_t(row) * N + i0 + j] = acc[r][j] * w;
+        }
+    }
+}
+
 // Device copies of the host-computed tables of a geometry, kept for later
 // calls (per device, up to kTableCacheSize geometries, oldest dropped):
 // building and uploading them per call from pageable memory kept the device
@@ -779,12 +838,30 @@ int ramp(const petl_geom& G, float* g_reb, int apply_weight, cudaStream_t st)
     const float* d_h = reinterpret_cast<const float*>(c->base + c->off[0]);
     const float* d_vw = reinterpret_cast<const float*>(c->base + c->off[1]);
     const int nrows = G.N_v0 * G.N_u1;
-    const size_t smem = sizeof(float) * (size_t(2 * N - 1) + size_t(kRampRows) * N);
-    cudaError_t e = cudaFuncSetAttribute(k_ramp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) {
-        k_ramp<<<ceil_div(nrows, kRampRows), 256, smem, st>>>(g_reb, nrows, N, G.N_u1, d_h, d_vw);
-        e = cudaGetLastError();
-        note_launch();
+    // four columns per thread where the blocks of 32 rows still fill the
+    // device twice over (at 4160 rows the 8-row blocks measured faster)
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    cudaError_t e;
+    if (N <= kRamp4MaxN && nrows >= 2 * kRamp4Rows * sms) {
+        const size_t smem = sizeof(float) * (size_t(2 * N + 4) + size_t(kRamp4Rows) * N);
+        e = cudaFuncSetAttribute(k_ramp4, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e == cudaSuccess) {
+            k_ramp4<<<ceil_div(nrows, kRamp4Rows), 256, smem, st>>>(g_reb, nrows, N, G.N_u1, d_h, d_vw);
+            e = cudaGetLastError();
+            note_launch();
+        }
+    } else {
+        const size_t smem = sizeof(float) * (size_t(2 * N - 1) + size_t(kRampRows) * N);
+        e = cudaFuncSetAttribute(k_ramp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e == cudaSuccess) {
+            k_ramp<<<ceil_div(nrows, kRampRows), 256, smem, st>>>(g_reb, nrows, N, G.N_u1, d_h, d_vw);
+            e = cudaGetLastError();
+            note_launch();
+        }
     }
     if (e != cudaSuccess) {
         set_error(std::string("ramp: ") + cudaGetErrorString(e));
