@@ -21,6 +21,10 @@
 // Both do the float operations of k_bwd_tma in the same order (per voxel:
 // z taps over the live slopes in ascending v1, tap 0 then tap 1; x taps over
 // the views in order; the scale last), so the two paths agree bit for bit.
+// As in the forward, a launch serves one call or up to kMaxMembers requests
+// of one geometry (one tensor map per member's planogram).  A single slope
+// at v1 = 0 (the rebinned planogram of FBP) takes k_bwd_zflat: its z sums
+// do not depend on the plane.
 // Every wait is bounded: a wait that gives up sets the device error word, the
 // CTA drains its copies in flight and returns without writing.
 #include <cuda.h>

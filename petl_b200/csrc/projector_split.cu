@@ -27,6 +27,12 @@
 // taps fmaf(w1, b, w0 * a); per ray, the z taps of the live planes in
 // ascending y, tap 0 then tap 1), so the two paths agree bit for bit.
 //
+// A launch serves the views of one call or, for the server's batched steps,
+// of up to kMaxMembers requests of one geometry (Members: per-member
+// volumes, planograms and view subsets; member b's views in scratch slots
+// b * nvm + v).  The kernels are compiled for one member (plain calls) and
+// for up to kMaxMembers.
+//
 // Every wait is bounded: a wait that gives up sets the device error word,
 // the CTA drains its copies in flight and returns without writing.
 #include <cuda.h>
