@@ -65,9 +65,10 @@ constexpr int ZWARPS = 16;
 constexpr int ZNT = 32 * ZWARPS;
 constexpr int ZDMAX = 3;              // largest shift difference among a warp's slopes
 constexpr int ZWN = ZK + ZDMAX + 1;   // register window rows
-// ring stages: two (of two planes each) measured fastest; deeper rings
-// (3-8 stages) ran 1-3 % slower at the 256x256x128 workload
-constexpr int ZNSMAX = 2;
+// ring stages (of two planes each): three measured 0.9 % faster than two at
+// the 256x256x128 workload once the tap offsets were dispatched per plane
+// (before that, deeper rings ran 1-3 % slower)
+constexpr int ZNSMAX = 3;
 constexpr int ZMAXPLANES = 1024;      // planes the per-CTA tables hold
 
 // code word of a (plane, slope group): tap offsets (2 bits per slope), the
