@@ -93,7 +93,13 @@ T project_ray(const oracle_geom& G, const T* f, int iv1, int iv0, int iu1, int i
     T val = T(0);
     double count = 0.0;
     const T* fz;
-    if (tabs(r_x) >= tabs(r_y)) {
+    // the driving axis is a yes/no decision that sits exactly on a tie for
+    // some views (|r_x| = |r_y|: psi = 135 degrees at v0 = 0), so it is taken
+    // in float with the contracted fma of the reference's compiled kernel,
+    // as the ray masks are (lines 62-65)
+    const float v0f = std::fma(float(iv0), G.T_v0, G.v0_0);
+    const float rxf = -std::fma(v0f, G.cos_psi, G.sin_psi), ryf = -std::fma(v0f, G.sin_psi, -G.cos_psi);
+    if (std::fabs(rxf) >= std::fabs(ryf)) {
         // x-driven branch, lines 77-130
         const T width_y = T(0.5) * Tg_z * tabs(sin_psi);
         const T sin_psi_inv = T(1) / sin_psi;
@@ -271,15 +277,22 @@ void backproject(const oracle_geom& G, const T* g, T* f, int texmode, int nthrea
                         const T width_x = cos_psi - v0 * sin_psi;
                         const T l_phi = T(1) / tmax(tabs(width_y), tabs(width_x)) *
                                         (T(1) / std::sqrt(T(1) + v0 * v0 + v1 * v1));
+                        // which corner pair bounds the footprint is a yes/no
+                        // decision with ties (|width_y| = |width_x| at psi = 135
+                        // degrees, v0 = 0): taken in float with the reference
+                        // kernel's contracted fmas
+                        const float v0f = std::fma(float(iv0), G.T_v0, G.v0_0);
+                        const float wyf = std::fma(v0f, G.cos_psi, G.sin_psi);
+                        const float wxf = std::fma(-v0f, G.sin_psi, G.cos_psi);
                         T A, B;
-                        if (tabs(width_y) > tabs(width_x)) {
+                        if (std::fabs(wyf) > std::fabs(wxf)) {
                             const T lo = (x_dot_theta - xdt_dy + v0 * (t - t_dy) - sg_z) * Tu0_inv;
                             const T hi = (x_dot_theta + xdt_dy + v0 * (t + t_dy) - sg_z) * Tu0_inv;
-                            if (width_y >= T(0)) { A = lo; B = hi; } else { A = hi; B = lo; }
+                            if (wyf >= 0.0f) { A = lo; B = hi; } else { A = hi; B = lo; }
                         } else {
                             const T lo = (x_dot_theta - xdt_dx + v0 * (t - t_dx) - sg_z) * Tu0_inv;
                             const T hi = (x_dot_theta + xdt_dx + v0 * (t + t_dx) - sg_z) * Tu0_inv;
-                            if (width_x >= T(0)) { A = lo; B = hi; } else { A = hi; B = lo; }
+                            if (wxf >= 0.0f) { A = lo; B = hi; } else { A = hi; B = lo; }
                         }
                         const int iu0_min = int(std::ceil(A - T(0.5)));
                         const int iu0_max = int(std::floor(B + T(0.5)));

@@ -149,6 +149,13 @@ int project_range(const petl_geom& G, const float* f, float* g, const ViewRange&
         cudaFreeAsync(ft, st);
         return rc;
     }
+    if (dispatch_mode() == 0) {
+        const int rc = project_gsplit(G, f, g, vr, meas, st);
+        if (rc != -2) {  // applied (-2: its layout rules fail)
+            note_path(3);
+            return rc;
+        }
+    }
     note_path(0);
     return launch_project_general(G, f, g, vr, meas, st);
 }

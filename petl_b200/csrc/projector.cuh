@@ -168,5 +168,10 @@ int launch_project_general(const petl_geom& G, const float* f, float* g, const V
 int launch_backproject_general(const petl_geom& G, const float* g, float* f, int mode, int accumulate, float scale,
                                const ViewRange& vr, cudaStream_t st);
 int launch_count_nnz(const petl_geom& G, unsigned long long* d_count, cudaStream_t st);
+// Split forward projection for any psi with equal voxel height and u1 pitch
+// (projector_gsplit.cu); -2 when its layout rules fail (the caller then runs
+// launch_project_general).
+int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                   cudaStream_t st);
 
 }  // namespace petl

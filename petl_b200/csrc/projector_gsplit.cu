@@ -1,0 +1,384 @@
+// Split forward projector for any psi (voxel height equal to the u1 bin
+// pitch), the counterpart of the shear-warp split kernels
+// (projector_split.cu) for orientations whose rays are not parallel to a
+// volume axis.
+//
+// The reference footprint (src/projectors.cu:11-238) of a ray at its
+// driving plane p (y = const for a y-driven view, x = const for an
+// x-driven one, |r_x| < |r_y| deciding per view v0) is the product of a u0
+// box overlap that depends on the ray parameter t and the in-plane voxel
+// index a, and a u1 box overlap that depends on t, the slope v1 and the
+// voxel row z.  t = (coordinate of plane p - p-coordinate of u0) / r_p
+// depends on (v0, u0, p) only.  So
+//   g[v1][v0][u1][u0] = l_phi rs sum_p sum_z w1(t, v1, u1, z) X[v0][p][z][u0],
+//   X[v0][p][z][u0]   = sum_a w0(t, a, u0) f(z, p, a),
+// and the two sums run as two kernels:
+//
+// * k_gx: a block stages 8 volume rows of plane p (from the volume, or from
+//   its x/y-transposed copy for x-driven views) in shared memory; a thread
+//   per column u0 evaluates the u0 taps of its ray on plane p once (the
+//   reference's tap range and box overlaps, taps with a positive weight)
+//   and applies them to the 8 rows.
+// * k_gz: CTA = one view x 16 slopes x 32 rows x 32 columns, 16 warps of
+//   4 slopes x 8 rows, one column per lane.  With equal pitch the u1 taps
+//   of row u1 are voxel rows u1 + s and u1 + s + 1 with weights 1 - fr and
+//   fr, where s + fr = (u1_0 - z_0 + t v1) / T_u1 depends on the lane's t
+//   and the slope but not on the row.  The lanes' shifts differ, so each
+//   lane reads its own rows of the staged plane: the CTA stages the rows
+//   every lane and slope of the tile needs (bounded on the host) for 32
+//   columns, row-major, so a lane's column is its bank whatever its row.
+//   The next plane is fetched into registers while the current one is
+//   summed; one CTA barrier per plane.
+// Epilogue: scale l_phi * rs, the reference's ray masks, optional MLEM
+// ratio.
+//
+// The sums are associated differently from the reference's (u0 taps summed
+// before the z taps), so results agree with it to float rounding, not bit
+// for bit.
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "common.cuh"
+#include "projector.cuh"
+#include "tma.cuh"
+
+namespace petl {
+
+size_t gsplit_scratch_budget();
+
+namespace {
+
+constexpr int GXZ = 8;        // volume rows per k_gx block
+constexpr int GZS = 16;       // slopes per k_gz CTA (4 per warp)
+constexpr int GZR = 32;       // rows per k_gz CTA (8 per warp)
+constexpr int GZC = 32;       // columns per k_gz CTA (one per lane)
+constexpr int GZT = 512;      // threads per k_gz CTA
+constexpr int GZRMAX = 160;   // staged rows per plane at most
+constexpr int GZPF = GZRMAX / (GZT / GZC);  // staged rows per warp (rows warp, warp + 16, ...)
+
+struct GxArgs {
+    petl_geom G;
+    ViewRange vr;
+    int vi0;    // first view of the chunk (index in vr)
+    int NPmax;  // planes per view slot of the scratch
+    int NUc;    // scratch row pitch
+};
+
+struct GzArgs {
+    petl_geom G;
+    ViewRange vr;
+    int vi0;
+    int NPmax;
+    int NUc;
+    int n_colblk, n_rowblk;
+    int nrows;  // staged rows per plane (32 + shift range + margins, <= GZRMAX)
+    int* err;
+};
+
+__device__ __forceinline__ bool view_xdriven(const petl_geom& G, int iv0)
+{
+    return ray_geom(G, 0, iv0, 0, 0).xdriven;
+}
+
+// X[vi][p][z][u0] for 8 rows z of plane p of one view.  Grid (ceil(NZ / 8),
+// NPmax, views of the chunk); dynamic shared memory 8 rows of the longest
+// in-plane axis.
+__global__ void __launch_bounds__(256) k_gx(const float* __restrict__ f, const float* __restrict__ fT,
+                                           float* __restrict__ X, const GxArgs A)
+{
+    extern __shared__ float rowbuf[];
+    const petl_geom& G = A.G;
+    const int z0 = blockIdx.x * GXZ, p = blockIdx.y, vi = blockIdx.z;
+    const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
+    const bool xd = view_xdriven(G, iv0);
+    const int NP = xd ? G.numX : G.numY, NA = xd ? G.numY : G.numX;
+    if (p >= NP) return;
+    const float* __restrict__ src = xd ? fT : f;  // [z][p][a]
+    const int nz = min(GXZ, G.numZ - z0);
+    for (int e = threadIdx.x; e < nz * NA; e += blockDim.x) {
+        const int r = e / NA, a = e - r * NA;
+        rowbuf[r * NA + a] = src[(size_t(z0 + r) * NP + p) * NA + a];
+    }
+    __syncthreads();
+    float* Xv = X + (size_t(vi) * A.NPmax + p) * G.numZ * A.NUc;
+    for (int iu0 = threadIdx.x; iu0 < G.N_u0; iu0 += blockDim.x) {
+        const RayGeom r = ray_geom(G, 0, iv0, 0, iu0);
+        const PlaneTaps pt = xd ? plane_taps_x(G, r, p) : plane_taps_y(G, r, p);
+        float acc[GXZ];
+#pragma unroll
+        for (int k = 0; k < GXZ; k++) acc[k] = 0.0f;
+        for (int a = pt.a_min; a <= pt.a_max; a++) {
+            const float w0 = xd ? tap_w0_x(G, r, pt.t, a, iu0) : tap_w0_y(G, r, pt.t, a, iu0);
+            if (!(w0 > 0.0f)) continue;
+#pragma unroll
+            for (int k = 0; k < GXZ; k++) acc[k] = fmaf(w0, rowbuf[k * NA + a], acc[k]);
+        }
+        for (int k = 0; k < nz; k++) Xv[size_t(z0 + k) * A.NUc + iu0] = acc[k];
+    }
+}
+
+// -(position of voxel row 0 in u1 bins) for ray parameter t and slope v1:
+// the row shift s = floor of it, the second tap's weight its fraction
+__device__ __forceinline__ float neg_c0(const petl_geom& G, float t, float v1, float Tu1_inv)
+{
+    return -fmul(fsub(fsub(G.z_0, fmul(t, -v1)), G.u1_0), Tu1_inv);
+}
+
+__device__ __forceinline__ float plane_t(const petl_geom& G, const RayGeom& r, int p)
+{
+    return r.xdriven ? fmul(fsub(ffma(float(p), G.T_x, G.x_0), r.px), r.inv)
+                     : fmul(fsub(ffma(float(p), G.T_x, G.y_0), r.py), r.inv);
+}
+
+__global__ void __launch_bounds__(GZT, 1) k_gz(const float* __restrict__ X, float* __restrict__ g,
+                                                const float* __restrict__ meas, const GzArgs A)
+{
+    extern __shared__ float zbuf[];  // two planes of nrows x 32 staged values
+    const petl_geom& G = A.G;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = warp & 3, rg = warp >> 2;
+    int t_ = blockIdx.x;
+    const int colblk = t_ % A.n_colblk;
+    t_ /= A.n_colblk;
+    const int rowblk = t_ % A.n_rowblk;
+    const int v1blk = t_ / A.n_rowblk;
+    const int vi = blockIdx.y;
+    const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
+    const int col0 = colblk * GZC, iu0 = col0 + lane;
+    const int row0c = rowblk * GZR, row0 = row0c + rg * GZR / 4;
+    const int v1c = A.vr.iv1_begin + v1blk * GZS;           // first slope of the CTA
+    const int v1c_last = min(v1c + GZS, A.vr.iv1_end) - 1;  // last slope of the CTA
+    const int v1w = v1c + q * 4;                            // first slope of the warp
+    const int NZ = G.numZ, NUc = A.NUc, nrows = A.nrows;
+    const float Tu1_inv = __frcp_rn(G.T_u1);
+    // the lane's ray geometry on this view (t depends on v0, u0 and the plane)
+    const RayGeom r = ray_geom(G, 0, iv0, 0, min(iu0, G.N_u0 - 1));
+    const RayGeom rc0 = ray_geom(G, 0, iv0, 0, col0);
+    const RayGeom rc1 = ray_geom(G, 0, iv0, 0, min(col0 + GZC - 1, G.N_u0 - 1));
+    const int NP = r.xdriven ? G.numX : G.numY;
+    float v1s[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) v1s[j] = ffma(float(min(v1w + j, A.vr.iv1_end - 1)), G.T_v1, G.v1_0);
+    const float v1lo = ffma(float(v1c), G.T_v1, G.v1_0), v1hi = ffma(float(v1c_last), G.T_v1, G.v1_0);
+    const float* Xv = X + size_t(vi) * A.NPmax * NZ * NUc;
+
+    // first staged row of plane p: the smallest shift of the tile's corners,
+    // less one row of margin (the shift is monotone in t and in v1)
+    auto first_row = [&](int p) {
+        const float ta = plane_t(G, rc0, p), tb = plane_t(G, rc1, p);
+        const float m = fminf(fminf(neg_c0(G, ta, v1lo, Tu1_inv), neg_c0(G, ta, v1hi, Tu1_inv)),
+                              fminf(neg_c0(G, tb, v1lo, Tu1_inv), neg_c0(G, tb, v1hi, Tu1_inv)));
+        return row0c + int(floorf(m)) - 1;
+    };
+    // staging: lane = column, warp w takes rows w, w + 16, ... of the window
+    float pf[GZPF];
+    const bool col_ok = iu0 < G.N_u0;
+    auto fetch = [&](int p, int wr0) {
+        const float* Xp = Xv + size_t(p) * NZ * NUc + iu0;
+#pragma unroll
+        for (int i = 0; i < GZPF; i++) {
+            const int rr = warp + 16 * i;
+            if (rr >= nrows) break;
+            const int z = wr0 + rr;
+            pf[i] = (col_ok && unsigned(z) < unsigned(NZ)) ? __ldg(Xp + size_t(z) * NUc) : 0.0f;
+        }
+    };
+    auto store = [&](int b) {
+        float* dst = zbuf + b * nrows * GZC + lane;
+#pragma unroll
+        for (int i = 0; i < GZPF; i++) {
+            const int rr = warp + 16 * i;
+            if (rr >= nrows) break;
+            dst[rr * GZC] = pf[i];
+        }
+    };
+
+    float acc[4][8];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[j][k] = 0.0f;
+
+    int wr0 = first_row(0);
+    fetch(0, wr0);
+    store(0);
+    __syncthreads();
+    for (int p = 0; p < NP; p++) {
+        const int b = p & 1;
+        int wr1 = 0;
+        if (p + 1 < NP) {
+            wr1 = first_row(p + 1);
+            fetch(p + 1, wr1);
+        }
+        const float t = plane_t(G, r, p);
+        const float* B = zbuf + b * nrows * GZC + lane;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float nc = neg_c0(G, t, v1s[j], Tu1_inv);
+            const float s = floorf(nc);
+            const float fr = nc - s, w0 = 1.0f - fr;
+            int base = row0 + int(s) - wr0;  // staged row of tap 0 of the warp's first row
+            if (base < 0 || base + 9 > nrows) {  // outside the staged rows: the host bound failed
+                atomicOr(A.err, kErrLayout);
+                base = 0;
+            }
+            float W[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) W[k] = B[(base + k) * GZC];
+#pragma unroll
+            for (int k = 0; k < 8; k++) acc[j][k] = fmaf(fr, W[k + 1], fmaf(w0, W[k], acc[j][k]));
+        }
+        if (p + 1 < NP) store(b ^ 1);
+        __syncthreads();
+        wr0 = wr1;
+    }
+
+    // epilogue: scale, ray masks, optional MLEM ratio
+    if (iu0 >= G.N_u0) return;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int iv1 = v1w + j;
+        if (iv1 >= A.vr.iv1_end) continue;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int iu1 = row0 + k;
+            if (iu1 >= G.N_u1) continue;
+            const RayGeom rr = ray_geom(G, iv1, iv0, iu1, iu0);
+            const float val = ray_visible(G, iv1, iv0, iu1, iu0) ? fmul(fmul(acc[j][k], rr.l_phi), rr.rs) : 0.0f;
+            const size_t o = ((size_t(iv1) * G.N_v0 + iv0) * G.N_u1 + iu1) * G.N_u0 + iu0;
+            g[o] = meas ? ratio_rule(__ldg(&meas[o]), val) : val;
+        }
+    }
+}
+
+// plain x/y transpose of every z slice: fT[z][x][y] = f[z][y][x]
+__global__ void k_transpose_xy(const float* __restrict__ f, float* __restrict__ fT, int nx, int ny)
+{
+    __shared__ float tile[32][33];
+    const int z = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const float* fz = f + size_t(z) * nx * ny;
+    float* tz = fT + size_t(z) * nx * ny;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int y = y0 + j, x = x0 + threadIdx.x;
+        if (y < ny && x < nx) tile[j][threadIdx.x] = fz[size_t(y) * nx + x];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int x = x0 + j, y = y0 + threadIdx.x;
+        if (x < nx && y < ny) tz[size_t(x) * ny + y] = tile[threadIdx.x][j];
+    }
+}
+
+// host: the ray quantities of view iv0 as ray_geom computes them
+struct HostView {
+    bool xd;
+    double inv, pscale;  // 1/r_p and |sin| or |cos| (p-coordinate of u0 = u0 * pscale)
+};
+
+HostView host_view(const petl_geom& G, int iv0)
+{
+    const float v0 = std::fmaf(float(iv0), G.T_v0, G.v0_0);
+    const float rx = -std::fmaf(v0, G.cos_psi, G.sin_psi), ry = -std::fmaf(v0, G.sin_psi, -G.cos_psi);
+    HostView h;
+    h.xd = std::fabs(rx) >= std::fabs(ry);
+    h.inv = 1.0 / double(h.xd ? rx : ry);
+    h.pscale = std::fabs(double(h.xd ? G.cos_psi : G.sin_psi));
+    return h;
+}
+
+}  // namespace
+
+size_t gsplit_scratch_budget() { return size_t(5) << 30; }
+
+// kNotApplicable when the layout rules fail (the caller then runs the
+// general kernel): voxel height != u1 pitch, a view whose shift range over a
+// tile exceeds the staged rows, or scratch that cannot be allocated.
+int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
+                   cudaStream_t st)
+{
+    constexpr int kNotApplicable = -2;
+    const int n_v0 = vr.n_v0(G.N_v0);
+    const int nv1 = vr.iv1_end - vr.iv1_begin;
+    if (n_v0 <= 0 || nv1 <= 0) return 0;
+    if (G.T_z != G.T_u1 || G.N_u0 > 4096 || G.numX > 4096 || G.numY > 4096) return kNotApplicable;
+    // staged rows per plane: 32 + the range of floor(-c0) over a tile's 32
+    // columns and 16 slopes + margins.  -c0 = (u1_0 - z_0 + t v1) / T_u1 with
+    // t = (coordinate of the plane - u0 pscale) * inv: bounded with the
+    // extremes of |t| and of its change over 32 columns.
+    const double vmax = std::max(std::fabs(double(G.v1_0)), std::fabs(double(G.v1_0) + (G.N_v1 - 1) * double(G.T_v1)));
+    const double dv1 = (GZS - 1) * std::fabs(double(G.T_v1));
+    const double xext = std::max(std::fabs(double(G.x_0)), std::fabs(double(G.x_0) + (G.numX - 1) * double(G.T_x)));
+    const double yext = std::max(std::fabs(double(G.y_0)), std::fabs(double(G.y_0) + (G.numY - 1) * double(G.T_x)));
+    const double uext = std::max(std::fabs(double(G.u0_0)), std::fabs(double(G.u0_0) + (G.N_u0 - 1) * double(G.T_u0)));
+    double spread = 0;
+    bool any_xd = false;
+    for (int k = 0; k < n_v0; k++) {
+        const HostView h = host_view(G, vr.iv0_first + k * vr.iv0_step);
+        any_xd = any_xd || h.xd;
+        const double tmax = (std::max(xext, yext) + uext * h.pscale) * std::fabs(h.inv);
+        const double dt = GZC * double(G.T_u0) * h.pscale * std::fabs(h.inv);
+        spread = std::max(spread, (dt * vmax + tmax * dv1 + dt * dv1) / double(G.T_u1));
+    }
+    const int nrows = GZR + int(std::ceil(spread * (1.0 + 1e-6))) + 5;  // + floors and the one-row margins
+    if (nrows > GZRMAX) return kNotApplicable;
+    int* err = device_error_ptr();
+    if (!err) return kNotApplicable;
+
+    const int NPmax = any_xd ? std::max(G.numX, G.numY) : G.numY;
+    const int NUc = (G.N_u0 + 3) & ~3;
+    const size_t per_view = size_t(NPmax) * G.numZ * NUc * 4;
+    int nv = int(std::max<size_t>(1, std::min<size_t>(size_t(n_v0), gsplit_scratch_budget() / per_view)));
+    nv = std::min(nv, 65535);
+    const int nchunks = (n_v0 + nv - 1) / nv;
+    nv = (n_v0 + nchunks - 1) / nchunks;
+    float* X = nullptr;
+    float* fT = nullptr;
+    if (scratch_alloc(reinterpret_cast<void**>(&X), per_view * nv, st) != cudaSuccess ||
+        (any_xd && scratch_alloc(reinterpret_cast<void**>(&fT), size_t(G.numX) * G.numY * G.numZ * 4, st) !=
+                       cudaSuccess)) {
+        cudaGetLastError();
+        if (X) cudaFreeAsync(X, st);
+        return kNotApplicable;
+    }
+    cudaError_t e = cudaSuccess;
+    if (any_xd) {
+        k_transpose_xy<<<dim3(ceil_div(G.numX, 32), ceil_div(G.numY, 32), unsigned(G.numZ)), dim3(32, 8), 0, st>>>(
+            f, fT, G.numX, G.numY);
+        note_launch();
+    }
+    const int NAmax = any_xd ? std::max(G.numX, G.numY) : G.numX;
+    const size_t xsmem = size_t(GXZ) * NAmax * 4;
+    e = cudaFuncSetAttribute(k_gx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(xsmem));
+    const size_t zsmem = size_t(2) * nrows * GZC * 4;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(zsmem));
+    GzArgs Z{};
+    Z.G = G;
+    Z.vr = vr;
+    Z.NPmax = NPmax;
+    Z.NUc = NUc;
+    Z.n_colblk = int(ceil_div(G.N_u0, GZC));
+    Z.n_rowblk = int(ceil_div(G.N_u1, GZR));
+    Z.nrows = nrows;
+    Z.err = err;
+    const unsigned nblk = unsigned(Z.n_colblk) * unsigned(Z.n_rowblk) * ceil_div(nv1, GZS);
+    for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
+        const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
+        const GxArgs XA{G, vr, vi0, NPmax, NUc};
+        k_gx<<<dim3(ceil_div(G.numZ, GXZ), unsigned(NPmax), unsigned(nvc)), 256, xsmem, st>>>(f, fT, X, XA);
+        note_launch();
+        Z.vi0 = vi0;
+        k_gz<<<dim3(nblk, unsigned(nvc)), GZT, zsmem, st>>>(X, g, meas, Z);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(X, st);
+    if (fT) cudaFreeAsync(fT, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("project_gsplit: ") + cudaGetErrorString(e));
+        return int(e);
+    }
+    return 0;
+}
+
+}  // namespace petl
