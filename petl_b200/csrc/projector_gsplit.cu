@@ -41,6 +41,7 @@
 
 #include "common.cuh"
 #include "projector.cuh"
+#include "storage.cuh"
 #include "tma.cuh"
 
 namespace petl {
@@ -54,8 +55,8 @@ constexpr int GZS = 16;       // slopes per k_gz CTA (4 per warp)
 constexpr int GZR = 32;       // rows per k_gz CTA (8 per warp)
 constexpr int GZC = 32;       // columns per k_gz CTA (one per lane)
 constexpr int GZT = 512;      // threads per k_gz CTA
-constexpr int GZRMAX = 160;   // staged rows per plane at most
-constexpr int GZPF = GZRMAX / (GZT / GZC);  // staged rows per warp (rows warp, warp + 16, ...)
+constexpr int GZRMAX = 224;   // staged rows per plane at most (TMA box rows <= 256)
+constexpr int GZNS = 3;       // ring stages (one plane each) at most
 
 struct GxArgs {
     petl_geom G;
@@ -73,7 +74,9 @@ struct GzArgs {
     int NUc;
     int n_colblk, n_rowblk;
     int nrows;  // staged rows per plane (32 + shift range + margins, <= GZRMAX)
+    int ns;     // ring stages
     int* err;
+    unsigned wait_limit;  // bound of the waits on staged data (wait_limit(): kWaitLimit or 0)
 };
 
 __device__ __forceinline__ bool view_xdriven(const petl_geom& G, int iv0)
@@ -118,23 +121,16 @@ __global__ void __launch_bounds__(256) k_gx(const float* __restrict__ f, const f
     }
 }
 
-// -(position of voxel row 0 in u1 bins) for ray parameter t and slope v1:
-// the row shift s = floor of it, the second tap's weight its fraction
-__device__ __forceinline__ float neg_c0(const petl_geom& G, float t, float v1, float Tu1_inv)
-{
-    return -fmul(fsub(fsub(G.z_0, fmul(t, -v1)), G.u1_0), Tu1_inv);
-}
-
 __device__ __forceinline__ float plane_t(const petl_geom& G, const RayGeom& r, int p)
 {
     return r.xdriven ? fmul(fsub(ffma(float(p), G.T_x, G.x_0), r.px), r.inv)
                      : fmul(fsub(ffma(float(p), G.T_x, G.y_0), r.py), r.inv);
 }
 
-__global__ void __launch_bounds__(GZT, 1) k_gz(const float* __restrict__ X, float* __restrict__ g,
+__global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorMap xmap, float* __restrict__ g,
                                                 const float* __restrict__ meas, const GzArgs A)
 {
-    extern __shared__ float zbuf[];  // two planes of nrows x 32 staged values
+    extern __shared__ __align__(128) unsigned char gsm[];
     const petl_geom& G = A.G;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = warp & 3, rg = warp >> 2;
@@ -150,49 +146,63 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const float* __restrict__ X, floa
     const int v1c = A.vr.iv1_begin + v1blk * GZS;           // first slope of the CTA
     const int v1c_last = min(v1c + GZS, A.vr.iv1_end) - 1;  // last slope of the CTA
     const int v1w = v1c + q * 4;                            // first slope of the warp
-    const int NZ = G.numZ, NUc = A.NUc, nrows = A.nrows;
+    const int nrows = A.nrows, ns = A.ns;
     const float Tu1_inv = __frcp_rn(G.T_u1);
+    const float K = fmul(fsub(G.u1_0, G.z_0), Tu1_inv);  // -(row 0 position) at t = 0
     // the lane's ray geometry on this view (t depends on v0, u0 and the plane)
     const RayGeom r = ray_geom(G, 0, iv0, 0, min(iu0, G.N_u0 - 1));
-    const RayGeom rc0 = ray_geom(G, 0, iv0, 0, col0);
-    const RayGeom rc1 = ray_geom(G, 0, iv0, 0, min(col0 + GZC - 1, G.N_u0 - 1));
     const int NP = r.xdriven ? G.numX : G.numY;
     float v1s[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) v1s[j] = ffma(float(min(v1w + j, A.vr.iv1_end - 1)), G.T_v1, G.v1_0);
-    const float v1lo = ffma(float(v1c), G.T_v1, G.v1_0), v1hi = ffma(float(v1c_last), G.T_v1, G.v1_0);
-    const float* Xv = X + size_t(vi) * A.NPmax * NZ * NUc;
+    for (int j = 0; j < 4; j++) v1s[j] = fmul(ffma(float(min(v1w + j, A.vr.iv1_end - 1)), G.T_v1, G.v1_0), Tu1_inv);
 
-    // first staged row of plane p: the smallest shift of the tile's corners,
-    // less one row of margin (the shift is monotone in t and in v1)
+    float* ring = reinterpret_cast<float*>(gsm);                        // [ns][nrows][32]
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + size_t(ns) * nrows * GZC);
+    uint64_t* empty = full + GZNS;
+    int* s_wr = reinterpret_cast<int*>(empty + GZNS);  // [GZNS] first staged row of the slot's plane
+    int* s_round = s_wr + GZNS;                        // [GZNS] round of the copy last started in a slot
+    volatile int* s_abort = s_round + GZNS;
+    if (tid == 0) {
+        for (int k = 0; k < ns; k++) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], GZT / 32);
+            s_round[k] = -1;
+        }
+        *s_abort = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    // first staged row of plane p: the smallest shift at the tile's corners
+    // (monotone in t and in v1), less one row of margin
+    const float v1lo = fmul(ffma(float(v1c), G.T_v1, G.v1_0), Tu1_inv);
+    const float v1hi = fmul(ffma(float(v1c_last), G.T_v1, G.v1_0), Tu1_inv);
     auto first_row = [&](int p) {
-        const float ta = plane_t(G, rc0, p), tb = plane_t(G, rc1, p);
-        const float m = fminf(fminf(neg_c0(G, ta, v1lo, Tu1_inv), neg_c0(G, ta, v1hi, Tu1_inv)),
-                              fminf(neg_c0(G, tb, v1lo, Tu1_inv), neg_c0(G, tb, v1hi, Tu1_inv)));
+        const RayGeom ra = ray_geom(G, 0, iv0, 0, col0);
+        const RayGeom rb = ray_geom(G, 0, iv0, 0, min(col0 + GZC - 1, G.N_u0 - 1));
+        const float ta = plane_t(G, ra, p), tb = plane_t(G, rb, p);
+        const float m = fminf(fminf(fmaf(-ta, v1lo, K), fmaf(-ta, v1hi, K)), fminf(fmaf(-tb, v1lo, K), fmaf(-tb, v1hi, K)));
         return row0c + int(floorf(m)) - 1;
     };
-    // staging: lane = column, warp w takes rows w, w + 16, ... of the window
-    float pf[GZPF];
-    const bool col_ok = iu0 < G.N_u0;
-    auto fetch = [&](int p, int wr0) {
-        const float* Xp = Xv + size_t(p) * NZ * NUc + iu0;
-#pragma unroll
-        for (int i = 0; i < GZPF; i++) {
-            const int rr = warp + 16 * i;
-            if (rr >= nrows) break;
-            const int z = wr0 + rr;
-            pf[i] = (col_ok && unsigned(z) < unsigned(NZ)) ? __ldg(Xp + size_t(z) * NUc) : 0.0f;
-        }
+    const uint32_t box_bytes = uint32_t(nrows) * GZC * 4u;
+    auto issue = [&](int p) {
+        const int slot = p % ns, round = p / ns;
+        if (round > 0 && !mbar_wait(&empty[slot], uint32_t((round - 1) & 1), A.err, A.wait_limit)) return false;
+        if (*s_abort) return false;
+        fence_proxy_async_smem();
+        const int wr = first_row(p);
+        s_wr[slot] = wr;
+        mbar_arrive_expect_tx(&full[slot], box_bytes);
+        tma_load_3d(ring + size_t(slot) * nrows * GZC, &xmap, &full[slot], col0, wr, vi * A.NPmax + p);
+        s_round[slot] = round;
+        return true;
     };
-    auto store = [&](int b) {
-        float* dst = zbuf + b * nrows * GZC + lane;
-#pragma unroll
-        for (int i = 0; i < GZPF; i++) {
-            const int rr = warp + 16 * i;
-            if (rr >= nrows) break;
-            dst[rr * GZC] = pf[i];
-        }
-    };
+    if (tid == 0)
+        for (int p = 0; p < ns - 1 && p < NP; p++) issue(p);
+    // the next plane this warp starts: the first p >= ns - 1 with p % 16 == warp
+    constexpr int NW = GZT / 32;
+    int my_next = warp + NW * ((ns - 1 - warp + NW - 1) / NW);
+    if (my_next < ns - 1) my_next += NW;
 
     float acc[4][8];
 #pragma unroll
@@ -200,38 +210,50 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const float* __restrict__ X, floa
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[j][k] = 0.0f;
 
-    int wr0 = first_row(0);
-    fetch(0, wr0);
-    store(0);
-    __syncthreads();
+    bool dead = false;
+    int slot = 0;
+    uint32_t phase = 0;
     for (int p = 0; p < NP; p++) {
-        const int b = p & 1;
-        int wr1 = 0;
-        if (p + 1 < NP) {
-            wr1 = first_row(p + 1);
-            fetch(p + 1, wr1);
+        if (p + ns - 1 == my_next) {
+            if (lane == 0 && !dead && my_next < NP && !issue(my_next)) dead = true;
+            my_next += NW;
         }
-        const float t = plane_t(G, r, p);
-        const float* B = zbuf + b * nrows * GZC + lane;
+        if (!dead) dead = !mbar_wait(&full[slot], phase, A.err, A.wait_limit);
+        if (dead) *s_abort = 1;  // before this warp releases the slot
+        if (!dead) {
+            const float tt = plane_t(G, r, p);
+            const float* B = ring + size_t(slot) * nrows * GZC + lane;
+            const int wr = s_wr[slot];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const float nc = neg_c0(G, t, v1s[j], Tu1_inv);
-            const float s = floorf(nc);
-            const float fr = nc - s, w0 = 1.0f - fr;
-            int base = row0 + int(s) - wr0;  // staged row of tap 0 of the warp's first row
-            if (base < 0 || base + 9 > nrows) {  // outside the staged rows: the host bound failed
-                atomicOr(A.err, kErrLayout);
-                base = 0;
+            for (int j = 0; j < 4; j++) {
+                const float nc = fmaf(-tt, v1s[j], K);
+                const float sf = floorf(nc);
+                const float fr = nc - sf, w0 = 1.0f - fr;
+                int base = row0 + int(sf) - wr;  // staged row of tap 0 of the warp's first row
+                if (base < 0 || base + 9 > nrows) {  // outside the staged rows: the host bound failed
+                    atomicOr(A.err, kErrLayout);
+                    base = 0;
+                }
+                float W[9];
+#pragma unroll
+                for (int k = 0; k < 9; k++) W[k] = B[(base + k) * GZC];
+#pragma unroll
+                for (int k = 0; k < 8; k++) acc[j][k] = fmaf(fr, W[k + 1], fmaf(w0, W[k], acc[j][k]));
             }
-            float W[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) W[k] = B[(base + k) * GZC];
-#pragma unroll
-            for (int k = 0; k < 8; k++) acc[j][k] = fmaf(fr, W[k + 1], fmaf(w0, W[k], acc[j][k]));
         }
-        if (p + 1 < NP) store(b ^ 1);
-        __syncthreads();
-        wr0 = wr1;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        if (++slot == ns) {
+            slot = 0;
+            phase ^= 1u;
+        }
+    }
+    if (__syncthreads_or(dead)) {
+        // a wait gave up: drain the copies still in flight, write nothing
+        if (tid == 0)
+            for (int k = 0; k < ns; k++)
+                if (s_round[k] >= 0) mbar_wait(&full[k], uint32_t(s_round[k] & 1), nullptr);
+        return;
     }
 
     // epilogue: scale, ray masks, optional MLEM ratio
@@ -350,7 +372,10 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
     const int NAmax = any_xd ? std::max(G.numX, G.numY) : G.numX;
     const size_t xsmem = size_t(GXZ) * NAmax * 4;
     e = cudaFuncSetAttribute(k_gx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(xsmem));
-    const size_t zsmem = size_t(2) * nrows * GZC * 4;
+    const size_t stage = size_t(nrows) * GZC * 4;
+    const int ns = int(std::min<size_t>(GZNS, (200 * 1024) / stage));
+    const size_t zsmem = size_t(ns) * stage + GZNS * 16 + GZNS * 8 + 16;
+    if (ns < 2) e = cudaErrorInvalidValue;
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(zsmem));
     GzArgs Z{};
     Z.G = G;
@@ -360,7 +385,16 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
     Z.n_colblk = int(ceil_div(G.N_u0, GZC));
     Z.n_rowblk = int(ceil_div(G.N_u1, GZR));
     Z.nrows = nrows;
+    Z.ns = ns;
     Z.err = err;
+    Z.wait_limit = wait_limit();
+    // the scratch as a 3-D tensor: columns, rows, view slot x plane; boxes of
+    // 32 columns x nrows rows (TMA, no multicast; rows outside read zero)
+    CUtensorMap map;
+    const uint64_t dims[3] = {uint64_t(NUc), uint64_t(G.numZ), uint64_t(NPmax) * uint64_t(nv)};
+    const uint64_t strides[2] = {uint64_t(NUc) * 4, uint64_t(NUc) * G.numZ * 4};
+    const uint32_t box[3] = {uint32_t(GZC), uint32_t(nrows), 1u};
+    if (e == cudaSuccess && !encode_tensor_map(&map, X, 3, dims, strides, box, 4)) e = cudaErrorInvalidValue;
     const unsigned nblk = unsigned(Z.n_colblk) * unsigned(Z.n_rowblk) * ceil_div(nv1, GZS);
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
@@ -368,7 +402,7 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
         k_gx<<<dim3(ceil_div(G.numZ, GXZ), unsigned(NPmax), unsigned(nvc)), 256, xsmem, st>>>(f, fT, X, XA);
         note_launch();
         Z.vi0 = vi0;
-        k_gz<<<dim3(nblk, unsigned(nvc)), GZT, zsmem, st>>>(X, g, meas, Z);
+        k_gz<<<dim3(nblk, unsigned(nvc)), GZT, zsmem, st>>>(map, g, meas, Z);
         note_launch();
         e = cudaGetLastError();
     }
