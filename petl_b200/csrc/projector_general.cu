@@ -175,14 +175,28 @@ k_backproject_ref_general_multi(const float* __restrict__ g, float* __restrict__
                 const int iu0_min = max(int(ceilf(A - 0.5f)), 0);
                 const int iu0_max = min(int(floorf(B + 0.5f)), G.N_u0 - 1);
                 const float* gv = gs + size_t(iv0) * G.N_u1 * G.N_u0;
+                // the u0 weights do not depend on the row: evaluated once for
+                // footprints of up to 4 bins (the same values in the same order)
+                const int nw = iu0_max - iu0_min + 1;
+                float w0a[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    w0a[i] = fmaxf(0.0f, fminf(float(iu0_min + i) + 0.5f, B) - fmaxf(float(iu0_min + i) - 0.5f, A));
                 float s0[kRows];
 #pragma unroll
                 for (int r = 0; r < kRows; r++) {
                     s0[r] = 0.0f;
                     if (lo + r > hi) continue;
-                    for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
-                        const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
-                        s0[r] = fmaf(w0, __ldg(&gv[size_t(lo + r) * G.N_u0 + iu0]), s0[r]);
+                    const float* gr = gv + size_t(lo + r) * G.N_u0;
+                    if (nw <= 4) {
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            if (i < nw) s0[r] = fmaf(w0a[i], __ldg(&gr[iu0_min + i]), s0[r]);
+                    } else {
+                        for (int iu0 = iu0_min; iu0 <= iu0_max; iu0++) {
+                            const float w0 = fmaxf(0.0f, fminf(float(iu0) + 0.5f, B) - fmaxf(float(iu0) - 0.5f, A));
+                            s0[r] = fmaf(w0, __ldg(&gr[iu0]), s0[r]);
+                        }
                     }
                 }
 #pragma unroll
