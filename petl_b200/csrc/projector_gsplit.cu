@@ -20,7 +20,7 @@
 //   reference's tap range and box overlaps, taps with a positive weight)
 //   and applies them to the 8 rows.
 // * k_gz: CTA = one view x 16 slopes x 32 rows x 32 columns, 16 warps of
-//   4 slopes x 8 rows, one column per lane.  With equal pitch the u1 taps
+//   2 slopes x 16 rows, one column per lane.  With equal pitch the u1 taps
 //   of row u1 are voxel rows u1 + s and u1 + s + 1 with weights 1 - fr and
 //   fr, where s + fr = (u1_0 - z_0 + t v1) / T_u1 depends on the lane's t
 //   and the slope but not on the row.  The lanes' shifts differ, so each
@@ -55,6 +55,8 @@ constexpr int GZS = 16;       // slopes per k_gz CTA (4 per warp)
 constexpr int GZR = 32;       // rows per k_gz CTA (8 per warp)
 constexpr int GZC = 32;       // columns per k_gz CTA (one per lane)
 constexpr int GZT = 512;      // threads per k_gz CTA
+constexpr int GJS = 2;        // slopes per warp
+constexpr int GRW = 16;       // rows per warp (GZS / GJS x GZR / GRW = 16 warps)
 constexpr int GZRMAX = 224;   // staged rows per plane at most (TMA box rows <= 256)
 constexpr int GZNS = 3;       // ring stages (one plane each) at most
 
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
     extern __shared__ __align__(128) unsigned char gsm[];
     const petl_geom& G = A.G;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = warp & 3, rg = warp >> 2;
+    const int q = warp % (GZS / GJS), rg = warp / (GZS / GJS);
     int t_ = blockIdx.x;
     const int colblk = t_ % A.n_colblk;
     t_ /= A.n_colblk;
@@ -142,19 +144,19 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
     const int vi = blockIdx.y;
     const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
     const int col0 = colblk * GZC, iu0 = col0 + lane;
-    const int row0c = rowblk * GZR, row0 = row0c + rg * GZR / 4;
+    const int row0c = rowblk * GZR, row0 = row0c + rg * GRW;
     const int v1c = A.vr.iv1_begin + v1blk * GZS;           // first slope of the CTA
     const int v1c_last = min(v1c + GZS, A.vr.iv1_end) - 1;  // last slope of the CTA
-    const int v1w = v1c + q * 4;                            // first slope of the warp
+    const int v1w = v1c + q * GJS;                          // first slope of the warp
     const int nrows = A.nrows, ns = A.ns;
     const float Tu1_inv = __frcp_rn(G.T_u1);
     const float K = fmul(fsub(G.u1_0, G.z_0), Tu1_inv);  // -(row 0 position) at t = 0
     // the lane's ray geometry on this view (t depends on v0, u0 and the plane)
     const RayGeom r = ray_geom(G, 0, iv0, 0, min(iu0, G.N_u0 - 1));
     const int NP = r.xdriven ? G.numX : G.numY;
-    float v1s[4];
+    float v1s[GJS];
 #pragma unroll
-    for (int j = 0; j < 4; j++) v1s[j] = fmul(ffma(float(min(v1w + j, A.vr.iv1_end - 1)), G.T_v1, G.v1_0), Tu1_inv);
+    for (int j = 0; j < GJS; j++) v1s[j] = fmul(ffma(float(min(v1w + j, A.vr.iv1_end - 1)), G.T_v1, G.v1_0), Tu1_inv);
 
     float* ring = reinterpret_cast<float*>(gsm);                        // [ns][nrows][32]
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + size_t(ns) * nrows * GZC);
@@ -204,11 +206,11 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
     int my_next = warp + NW * ((ns - 1 - warp + NW - 1) / NW);
     if (my_next < ns - 1) my_next += NW;
 
-    float acc[4][8];
+    float acc[GJS][GRW];
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+    for (int j = 0; j < GJS; j++)
 #pragma unroll
-        for (int k = 0; k < 8; k++) acc[j][k] = 0.0f;
+        for (int k = 0; k < GRW; k++) acc[j][k] = 0.0f;
 
     bool dead = false;
     int slot = 0;
@@ -225,20 +227,20 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
             const float* B = ring + size_t(slot) * nrows * GZC + lane;
             const int wr = s_wr[slot];
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
+            for (int j = 0; j < GJS; j++) {
                 const float nc = fmaf(-tt, v1s[j], K);
                 const float sf = floorf(nc);
                 const float fr = nc - sf, w0 = 1.0f - fr;
                 int base = row0 + int(sf) - wr;  // staged row of tap 0 of the warp's first row
-                if (base < 0 || base + 9 > nrows) {  // outside the staged rows: the host bound failed
+                if (base < 0 || base + GRW + 1 > nrows) {  // outside the staged rows: the host bound failed
                     atomicOr(A.err, kErrLayout);
                     base = 0;
                 }
-                float W[9];
+                float W[GRW + 1];
 #pragma unroll
-                for (int k = 0; k < 9; k++) W[k] = B[(base + k) * GZC];
+                for (int k = 0; k < GRW + 1; k++) W[k] = B[(base + k) * GZC];
 #pragma unroll
-                for (int k = 0; k < 8; k++) acc[j][k] = fmaf(fr, W[k + 1], fmaf(w0, W[k], acc[j][k]));
+                for (int k = 0; k < GRW; k++) acc[j][k] = fmaf(fr, W[k + 1], fmaf(w0, W[k], acc[j][k]));
             }
         }
         __syncwarp();
@@ -259,11 +261,11 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
     // epilogue: scale, ray masks, optional MLEM ratio
     if (iu0 >= G.N_u0) return;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < GJS; j++) {
         const int iv1 = v1w + j;
         if (iv1 >= A.vr.iv1_end) continue;
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
+        for (int k = 0; k < GRW; k++) {
             const int iu1 = row0 + k;
             if (iu1 >= G.N_u1) continue;
             const RayGeom rr = ray_geom(G, iv1, iv0, iu1, iu0);

@@ -20,6 +20,9 @@ CASES = {
     "p60": ((60.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (64, 64, 16, 2.0)),
     "p135rag": ((135.0, 100.0, 75.0, 27.0, 1.5, 0.45, 0.2), (52, 60, 18, 1.5, 1.5, 3.0, -4.5, 1.5)),
     "p17wide": ((17.0, 300.0, 128.0, 32.0, 1.0, 0.5, 0.25), (200, 96, 32, 1.0)),
+    # psi = 180 (y-driven, cos = -1) and -45 degrees (ties |r_x| = |r_y| at v0 = 0)
+    "p180": ((180.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (64, 48, 16, 2.0)),
+    "pm45": ((-45.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (48, 64, 16, 2.0, 2.0, -2.0, 3.0, 1.0)),
 }
 
 
