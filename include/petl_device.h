@@ -288,7 +288,8 @@ int petl_mlem_update_bf16_dev(void* f, const float* d, const float* sens, long l
  * has its own stream with up to `depth` subset steps in flight, issued
  * oldest request first while the work in flight stays under about two
  * full-size steps, so small requests overlap with large ones and new ones
- * join while others run.  Batched launches: when a request whose subset
+ * join while others run.  Batched launches (petl_server_set_batching, off
+ * by default): when a request whose subset
  * steps are too small to fill the device (under two waves of CTAs) issues a
  * step with none in flight, up to seven younger requests of its geometry
  * and subset count with no step in flight join it (each at its own
@@ -318,8 +319,8 @@ int petl_server_wait(void* server, long long id, float* f_host, double* latency_
 /* out[0..5]: completed, failed, active, pending, HBM bytes reserved now,
  * peak HBM bytes reserved */
 int petl_server_stats(void* server, double* out);
-/* Members of a batched step at most, 1 (no batched launches) to 8 (the
- * default). */
+/* Members of a batched step at most, 1 (no batched launches, the default)
+ * to 8. */
 int petl_server_set_batching(void* server, int max_members);
 /* out[0]: batched steps issued (two or more members), out[1]: member steps
  * they served */

@@ -102,20 +102,20 @@ def test_batched_launches_equal_alone(cuda):
         alone = [srv.wait(srv.submit(G, g, S, it))[0] for g, it in data]
         assert srv.batch_stats()["batched_steps"] == 0
     # all at once: like-geometry steps batched from the first step on
-    with ReconServer(hbm_budget_gb=60, max_active=8, depth=2) as srv:
+    with ReconServer(hbm_budget_gb=60, max_active=8, depth=2, batch=8) as srv:
         ids = [srv.submit(G, g, S, it) for g, it in data]
         together = [srv.wait(i)[0] for i in ids]
         bs = srv.batch_stats()
     assert bs["batched_steps"] > 0 and bs["member_steps"] >= 2 * bs["batched_steps"]
     # staggered: later requests join while the first ones are at other subsets
-    with ReconServer(hbm_budget_gb=60, max_active=8, depth=1) as srv:
+    with ReconServer(hbm_budget_gb=60, max_active=8, depth=1, batch=8) as srv:
         ids = []
         for g, it in data:
             ids.append(srv.submit(G, g, S, it))
             time.sleep(0.002)
         staggered = [srv.wait(i)[0] for i in ids]
-    # batching off: the same
-    with ReconServer(hbm_budget_gb=60, max_active=8, batch=1) as srv:
+    # batching off (the default): the same
+    with ReconServer(hbm_budget_gb=60, max_active=8) as srv:
         ids = [srv.submit(G, g, S, it) for g, it in data]
         unbatched = [srv.wait(i)[0] for i in ids]
         assert srv.batch_stats()["batched_steps"] == 0
