@@ -22,13 +22,15 @@
 // * k_gz: CTA = one view x 16 slopes x 32 rows x 32 columns, 16 warps of
 //   2 slopes x 16 rows, one column per lane.  With equal pitch the u1 taps
 //   of row u1 are voxel rows u1 + s and u1 + s + 1 with weights 1 - fr and
-//   fr, where s + fr = (u1_0 - z_0 + t v1) / T_u1 depends on the lane's t
+//   fr, where s + fr = (u1_0 - z_0 - t v1) / T_u1 depends on the lane's t
 //   and the slope but not on the row.  The lanes' shifts differ, so each
-//   lane reads its own rows of the staged plane: the CTA stages the rows
-//   every lane and slope of the tile needs (bounded on the host) for 32
-//   columns, row-major, so a lane's column is its bank whatever its row.
-//   The next plane is fetched into registers while the current one is
-//   summed; one CTA barrier per plane.
+//   lane reads its own rows of the staged plane: the rows every lane and
+//   slope of the tile needs (bounded on the host) for 32 columns, row-major,
+//   so a lane's column is its bank whatever its row.  They arrive per plane
+//   by a tiled TMA copy (no multicast; rows outside the scratch read zero)
+//   into a ring of three planes with full/empty mbarriers and a rotating
+//   issuer; every wait is bounded (a wait that gives up sets the device
+//   error word, the CTA drains its copies and writes nothing).
 // Epilogue: scale l_phi * rs, the reference's ray masks, optional MLEM
 // ratio.
 //
