@@ -91,14 +91,15 @@ k_project_general(const float* __restrict__ f, float* __restrict__ g, const petl
 // k_backproject_ref_general.  Columns whose union spans more than kRows
 // rows take the per-voxel form.
 // ---------------------------------------------------------------------------
-// six CTAs per SM (at most 85 registers, a few spilled) measured 19 % faster
-// than four (128 registers): the kernel waits on its L1-resident gathers
+// seven CTAs per SM (at most 73 registers, a few spilled) measured 25 %
+// faster than four (128 registers): the kernel waits on its L1-resident
+// gathers and needs the warps
 template <int KZ>
-__global__ void __launch_bounds__(128, 6)
+__global__ void __launch_bounds__(128, 7)
 k_backproject_ref_general_multi(const float* __restrict__ g, float* __restrict__ f, const petl_geom G,
                                 const ViewRange vr, int accumulate, float scale)
 {
-    constexpr int kRows = 8;
+    constexpr int kRows = 6;  // 4 voxels of equal pitch span at most 6 rows (8 measured 10 % slower)
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * 4 + threadIdx.y;
     const int iz0 = blockIdx.z * KZ;
