@@ -177,6 +177,13 @@ int backproject_range(const petl_geom& G, const float* g, float* f, int mode, in
         cudaFreeAsync(bt, st);
         return rc;
     }
+    if (mode == PETL_BP_ADJOINT && dispatch_mode() == 0) {
+        const int rc = backproject_gsplit_adjoint(G, g, f, accumulate, scale, vr, st);
+        if (rc != -2) {
+            note_path(3);
+            return rc;
+        }
+    }
     note_path(0);
     return launch_backproject_general(G, g, f, mode, accumulate, scale, vr, st);
 }

@@ -173,5 +173,9 @@ int launch_count_nnz(const petl_geom& G, unsigned long long* d_count, cudaStream
 // launch_project_general).
 int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange& vr, const float* meas,
                    cudaStream_t st);
+// Its exact transpose (backprojector_gsplit.cu, adjoint mode); -2 when the
+// layout rules fail (the caller then runs launch_backproject_general).
+int backproject_gsplit_adjoint(const petl_geom& G, const float* g, float* f, int accumulate, float scale,
+                               const ViewRange& vr, cudaStream_t st);
 
 }  // namespace petl

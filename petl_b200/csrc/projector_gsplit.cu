@@ -42,13 +42,12 @@
 #include <string>
 
 #include "common.cuh"
+#include "gsplit.cuh"
 #include "projector.cuh"
 #include "storage.cuh"
 #include "tma.cuh"
 
 namespace petl {
-
-size_t gsplit_scratch_budget();
 
 namespace {
 
@@ -125,11 +124,6 @@ __global__ void __launch_bounds__(256) k_gx(const float* __restrict__ f, const f
     }
 }
 
-__device__ __forceinline__ float plane_t(const petl_geom& G, const RayGeom& r, int p)
-{
-    return r.xdriven ? fmul(fsub(ffma(float(p), G.T_x, G.x_0), r.px), r.inv)
-                     : fmul(fsub(ffma(float(p), G.T_x, G.y_0), r.py), r.inv);
-}
 
 __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorMap xmap, float* __restrict__ g,
                                                 const float* __restrict__ meas, const GzArgs A)
@@ -278,13 +272,15 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
     }
 }
 
-// plain x/y transpose of every z slice: fT[z][x][y] = f[z][y][x]
-__global__ void k_transpose_xy(const float* __restrict__ f, float* __restrict__ fT, int nx, int ny)
+}  // namespace
+
+
+__global__ void k_transpose_xy(const float* __restrict__ in, float* __restrict__ out, int nx, int ny)
 {
     __shared__ float tile[32][33];
     const int z = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-    const float* fz = f + size_t(z) * nx * ny;
-    float* tz = fT + size_t(z) * nx * ny;
+    const float* fz = in + size_t(z) * nx * ny;
+    float* tz = out + size_t(z) * nx * ny;
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
         const int y = y0 + j, x = x0 + threadIdx.x;
         if (y < ny && x < nx) tile[j][threadIdx.x] = fz[size_t(y) * nx + x];
@@ -295,27 +291,6 @@ __global__ void k_transpose_xy(const float* __restrict__ f, float* __restrict__ 
         if (x < nx && y < ny) tz[size_t(x) * ny + y] = tile[threadIdx.x][j];
     }
 }
-
-// host: the ray quantities of view iv0 as ray_geom computes them
-struct HostView {
-    bool xd;
-    double inv, pscale;  // 1/r_p and |sin| or |cos| (p-coordinate of u0 = u0 * pscale)
-};
-
-HostView host_view(const petl_geom& G, int iv0)
-{
-    const float v0 = std::fmaf(float(iv0), G.T_v0, G.v0_0);
-    const float rx = -std::fmaf(v0, G.cos_psi, G.sin_psi), ry = -std::fmaf(v0, G.sin_psi, -G.cos_psi);
-    HostView h;
-    h.xd = std::fabs(rx) >= std::fabs(ry);
-    h.inv = 1.0 / double(h.xd ? rx : ry);
-    h.pscale = std::fabs(double(h.xd ? G.cos_psi : G.sin_psi));
-    return h;
-}
-
-}  // namespace
-
-size_t gsplit_scratch_budget() { return size_t(5) << 30; }
 
 // kNotApplicable when the layout rules fail (the caller then runs the
 // general kernel): voxel height != u1 pitch, a view whose shift range over a
