@@ -1,0 +1,368 @@
+// Split backprojector with the reference's semantics for any psi.
+//
+// The reference backprojector (src/projectors.cu:240-377) visits, per voxel
+// (x, y, z) and slope v1, the u1 rows of u1 = z + v1 t with
+// t = y cos(psi) - x sin(psi), and per view v0 the u0 bins of the voxel's
+// projected extent [A, B] (A, B from x cos + y sin + v0 t and the half
+// widths).  The depth t does not depend on the view, and the u0 extent does
+// not depend on z or v1, so
+//   f(x, y, z) = T_x sum_v1 vis sum_u1 w1(v1, t, z, u1) P[v1][u1](x, y),
+//   P[v1][u1](x, y) = sum_v0 l_phi(v0, v1) sum_u0 w0(v0, x, y, u0) g[v1][v0][u1][u0],
+// the same sums as the reference associated differently (float rounding).
+//
+// * k_rbp_xy: block = 16 x 16 voxel columns x 16 u1 rows of one slope; per
+//   view the rows' u0 window that the tile's extents reach (bounded on the
+//   host from the corners of the tile) is staged in shared memory, double
+//   buffered through registers (the next view's loads are in flight while
+//   the current one is summed); a thread sums its column's 2-4 u0 taps per
+//   row with the reference's box-overlap weights, the tap count chosen per
+//   view (uniform over the block).
+// * k_rbp_z: thread = voxel column x 16 z rows; per slope the reference's
+//   visibility test, u1 box and weights of each row, summed over P.
+// P takes N_u1 x numY x numX floats per slope; slopes run in chunks that
+// fit the scratch budget.
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "common.cuh"
+#include "gsplit.cuh"
+#include "projector.cuh"
+#include "storage.cuh"
+#include "tma.cuh"
+
+namespace petl {
+
+namespace {
+
+constexpr int RTX = 16, RTY = 16, RT = RTX * RTY;  // voxel columns per k_rbp_xy block (one per thread)
+constexpr int RRB = 16;                            // u1 rows per k_rbp_xy block
+constexpr int RWMAX = 128;                         // staged u0 columns per view at most
+constexpr int RPF = RRB * RWMAX / RT;              // staged values per thread at most
+constexpr int RZB = 16;                            // z rows per k_rbp_z thread
+
+struct RxyArgs {
+    petl_geom G;
+    ViewRange vr;
+    int jv1_0;     // first slope of the chunk (index in the range)
+    int W;         // staged u0 columns per view (<= RWMAX)
+    int ntx;       // tiles along x
+    int taps_max;  // taps per row and view at most (host bound)
+    int* err;
+};
+
+struct RzArgs {
+    petl_geom G;
+    ViewRange vr;
+    int jv1_0, nv1c;  // the chunk's slopes
+    int accumulate;
+    float scale;
+};
+
+// the voxel's view-independent quantities as the reference forms them
+__device__ __forceinline__ void voxel_tx(const petl_geom& G, int ix, int iy, float& t, float& xdt)
+{
+    const float x = fmaf(float(ix), G.T_x, G.x_0);
+    const float y = fmaf(float(iy), G.T_x, G.y_0);
+    t = fmaf(y, G.cos_psi, -(x * G.sin_psi));
+    xdt = fmaf(x, G.cos_psi, y * G.sin_psi);
+}
+
+struct ViewU0 {
+    float v0, l_phi;
+    bool ydom;  // |wy| > |wx|: the extent from the dy half widths
+    bool pos;   // the dominant w >= 0 (A from the lower end)
+};
+
+__device__ __forceinline__ ViewU0 view_u0(const petl_geom& G, int iv0, float v1)
+{
+    ViewU0 q;
+    q.v0 = fmaf(float(iv0), G.T_v0, G.v0_0);
+    const float wy = fmaf(q.v0, G.cos_psi, G.sin_psi);
+    const float wx = fmaf(-q.v0, G.sin_psi, G.cos_psi);
+    q.l_phi = 1.0f / fmaxf(fabsf(wy), fabsf(wx)) * rsqrtf(1.0f + q.v0 * q.v0 + v1 * v1);
+    q.ydom = fabsf(wy) > fabsf(wx);
+    q.pos = q.ydom ? wy >= 0.0f : wx >= 0.0f;
+    return q;
+}
+
+// [A, B]: the voxel's u0 extent in bin units (src/projectors.cu:318-345)
+__device__ __forceinline__ void u0_extent(const petl_geom& G, const ViewU0& q, float t, float xdt, float& A, float& B)
+{
+    const float Tu0_inv = 1.0f / G.T_u0;
+    const float sn = G.sin_psi, cs = G.cos_psi;
+    const float hx = q.ydom ? 0.5f * G.T_x * sn : 0.5f * G.T_x * cs;   // xdt_dy or xdt_dx
+    const float ht = q.ydom ? 0.5f * G.T_x * cs : -0.5f * G.T_x * sn;  // t_dy or t_dx
+    const float lo_ = (xdt - hx + q.v0 * (t - ht) - G.u0_0) * Tu0_inv;
+    const float hi_ = (xdt + hx + q.v0 * (t + ht) - G.u0_0) * Tu0_inv;
+    A = q.pos ? lo_ : hi_;
+    B = q.pos ? hi_ : lo_;
+}
+
+// B - A for every voxel of the view (the extent's width does not depend on
+// the voxel)
+__device__ __forceinline__ float u0_width(const petl_geom& G, const ViewU0& q)
+{
+    const float sn = G.sin_psi, cs = G.cos_psi;
+    const float hx = q.ydom ? 0.5f * G.T_x * sn : 0.5f * G.T_x * cs;
+    const float ht = q.ydom ? 0.5f * G.T_x * cs : -0.5f * G.T_x * sn;
+    return fabsf(fmaf(q.v0, 2.0f * ht, 2.0f * hx)) * (1.0f / G.T_u0);
+}
+
+template <int NT>
+__device__ __forceinline__ void sum_taps(const float* __restrict__ s, int W, int nw, int u0_min, float A, float B,
+                                         float l_phi, float (&acc)[RRB])
+{
+    float w[NT];
+#pragma unroll
+    for (int i = 0; i < NT; i++)
+        w[i] = fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, B) - fmaxf(float(u0_min + i) - 0.5f, A));
+#pragma unroll
+    for (int r = 0; r < RRB; r++) {
+        float s0 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < NT; i++) {
+            const float v = s[r * W + i];
+            if (i < nw) s0 = fmaf(w[i], v, s0);
+        }
+        acc[r] = fmaf(l_phi, s0, acc[r]);
+    }
+}
+
+// P[jv1][u1][y][x] for 16 x 16 columns and 16 rows of one slope.  Grid
+// (tiles, ceil(N_u1 / 16), slopes of the chunk); 256 threads.
+__global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, float* __restrict__ P, const RxyArgs A)
+{
+    __shared__ float sg[2][RRB * RWMAX];
+    const petl_geom& G = A.G;
+    const int tid = threadIdx.x, tx = tid % RTX, ty = tid / RTX;
+    const int tix = blockIdx.x % A.ntx, tiy = blockIdx.x / A.ntx;
+    const int x0 = tix * RTX, y0 = tiy * RTY;
+    const int xl = min(x0 + RTX, G.numX) - 1, yl = min(y0 + RTY, G.numY) - 1;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const bool live = ix < G.numX && iy < G.numY;
+    const int r0 = blockIdx.y * RRB;
+    const int jv1 = blockIdx.z;
+    const int iv1 = A.vr.iv1_begin + A.jv1_0 + jv1;
+    const int W = A.W;
+    const float v1 = fmaf(float(iv1), G.T_v1, G.v1_0);
+    float t, xdt;
+    voxel_tx(G, min(ix, G.numX - 1), min(iy, G.numY - 1), t, xdt);
+    // per view of the call: first staged column (the smallest first bin over
+    // the tile's corners, the extent being affine in x and y, less one of
+    // margin), l_phi and the taps a row takes at most (floor(width) + 2)
+    extern __shared__ int vtab[];  // [3][n_v0]
+    const int nv0 = A.vr.n_v0(G.N_v0);
+    int* s_lo = vtab;
+    float* s_lphi = reinterpret_cast<float*>(vtab + nv0);
+    int* s_nwv = vtab + 2 * nv0;
+    {
+        float tc[4], xc[4];
+        voxel_tx(G, x0, y0, tc[0], xc[0]);
+        voxel_tx(G, xl, y0, tc[1], xc[1]);
+        voxel_tx(G, x0, yl, tc[2], xc[2]);
+        voxel_tx(G, xl, yl, tc[3], xc[3]);
+        for (int k = tid; k < nv0; k += RT) {
+            const ViewU0 q = view_u0(G, A.vr.iv0_first + k * A.vr.iv0_step, v1);
+            float m = 3.0e38f;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                float a, b;
+                u0_extent(G, q, tc[c], xc[c], a, b);
+                m = fminf(m, a);
+            }
+            s_lo[k] = max(0, int(ceilf(m - 0.5f)) - 1);
+            s_lphi[k] = q.l_phi;
+            s_nwv[k] = min(A.taps_max, int(u0_width(G, q)) + 2);
+        }
+    }
+    __syncthreads();
+    float pf[RPF];
+    auto prefetch = [&](int iv0, int lo) {
+        const float* gv = g + (size_t(iv1) * G.N_v0 + iv0) * G.N_u1 * G.N_u0;
+#pragma unroll
+        for (int i = 0; i < RPF; i++) {
+            const int e = tid + i * RT;
+            float v = 0.0f;
+            if (e < RRB * W) {
+                const int row = e / W, col = e - row * W;
+                const int iu1 = r0 + row, iu0 = lo + col;
+                if (iu1 < G.N_u1 && iu0 < G.N_u0) v = __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]);
+            }
+            pf[i] = v;
+        }
+    };
+    auto commit = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < RPF; i++) {
+            const int e = tid + i * RT;
+            if (e < RRB * W) sg[buf][e] = pf[i];
+        }
+    };
+
+    float acc[RRB];
+#pragma unroll
+    for (int r = 0; r < RRB; r++) acc[r] = 0.0f;
+    prefetch(A.vr.iv0_first, s_lo[0]);
+    commit(0);
+    __syncthreads();
+    for (int k = 0; k < nv0; k++) {
+        const int iv0 = A.vr.iv0_first + k * A.vr.iv0_step;
+        const int buf = k & 1;
+        if (k + 1 < nv0) prefetch(iv0 + A.vr.iv0_step, s_lo[k + 1]);
+        if (live) {
+            ViewU0 q = view_u0(G, iv0, v1);
+            q.l_phi = s_lphi[k];
+            float a, b;
+            u0_extent(G, q, t, xdt, a, b);
+            const int u0_min = max(int(ceilf(a - 0.5f)), 0);
+            const int u0_max = min(int(floorf(b + 0.5f)), G.N_u0 - 1);
+            const int nw = u0_max - u0_min + 1;
+            const int nwv = s_nwv[k];  // uniform over the block
+            int off = u0_min - s_lo[k];
+            if (nw > 0) {
+                if (off < 0 || off + max(nw, nwv) > W) {  // outside the staged window: the host bound failed
+                    atomicOr(A.err, kErrLayout);
+                    off = 0;
+                }
+                const float* s = sg[buf] + off;
+                if (nw > nwv) {  // a rounding edge: the plain loop
+                    for (int r = 0; r < RRB; r++) {
+                        float s0 = 0.0f;
+                        for (int i = 0; i < nw && off + i < W; i++) {
+                            const float w0 = fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, b) - fmaxf(float(u0_min + i) - 0.5f, a));
+                            s0 = fmaf(w0, s[r * W + i], s0);
+                        }
+                        acc[r] = fmaf(q.l_phi, s0, acc[r]);
+                    }
+                } else if (nwv <= 2) {
+                    sum_taps<2>(s, W, nw, u0_min, a, b, q.l_phi, acc);
+                } else if (nwv == 3) {
+                    sum_taps<3>(s, W, nw, u0_min, a, b, q.l_phi, acc);
+                } else {
+                    sum_taps<4>(s, W, nw, u0_min, a, b, q.l_phi, acc);
+                }
+            }
+        }
+        if (k + 1 < nv0) commit(buf ^ 1);
+        __syncthreads();
+    }
+    if (!live) return;
+    const size_t plane = size_t(G.numX) * G.numY;
+    float* Pc = P + (size_t(jv1) * G.N_u1 + r0) * plane + size_t(iy) * G.numX + ix;
+#pragma unroll
+    for (int r = 0; r < RRB; r++)
+        if (r0 + r < G.N_u1) Pc[size_t(r) * plane] = acc[r];
+}
+
+// f(x, y, z) (+)= scale T_x sum over the chunk's slopes of the reference's
+// u1 taps of P.  Grid (ceil(numX / 32), ceil(numY / 8), ceil(numZ / 16));
+// block (32, 8).
+__global__ void __launch_bounds__(256) k_rbp_z(const float* __restrict__ P, float* __restrict__ f, const RzArgs A)
+{
+    const petl_geom& G = A.G;
+    const int ix = blockIdx.x * 32 + threadIdx.x, iy = blockIdx.y * 8 + threadIdx.y;
+    const int iz0 = blockIdx.z * RZB;
+    if (ix >= G.numX || iy >= G.numY) return;
+    float t, xdt;
+    voxel_tx(G, ix, iy, t, xdt);
+    const float Tu1_inv = 1.0f / G.T_u1;
+    const size_t plane = size_t(G.numX) * G.numY;
+    float acc[RZB];
+#pragma unroll
+    for (int k = 0; k < RZB; k++) acc[k] = 0.0f;
+    for (int jv1 = 0; jv1 < A.nv1c; jv1++) {
+        const int iv1 = A.vr.iv1_begin + A.jv1_0 + jv1;
+        const float v1 = fmaf(float(iv1), G.T_v1, G.v1_0);
+        const float* Pv = P + size_t(jv1) * G.N_u1 * plane + size_t(iy) * G.numX + ix;
+#pragma unroll
+        for (int k = 0; k < RZB; k++) {
+            if (iz0 + k >= G.numZ) break;
+            const float z = fmaf(float(iz0 + k), G.T_z, G.z_0);
+            const float u1 = fmaf(v1, t, z);
+            if (!(fabsf(u1) - 0.5f * G.T_u1 <= fmaf(-G.R, fabsf(v1), G.H))) continue;
+            const float iu1_mid = (u1 - G.u1_0) * Tu1_inv;
+            const float a = iu1_mid - 0.5f * G.T_z * Tu1_inv;
+            const float b = iu1_mid + 0.5f * G.T_z * Tu1_inv;
+            const int ua = max(int(ceilf(a - 0.5f)), 0);
+            const int ub = min(int(floorf(b + 0.5f)), G.N_u1 - 1);
+            float sv = 0.0f;
+            for (int iu1 = ua; iu1 <= ub; iu1++) {
+                const float w1 = fmaxf(0.0f, fminf(float(iu1) + 0.5f, b) - fmaxf(float(iu1) - 0.5f, a));
+                if (w1 > 0.0f) sv = fmaf(w1, __ldg(&Pv[size_t(iu1) * plane]), sv);
+            }
+            acc[k] = fmaf(sv, G.T_x, acc[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < RZB; k++) {
+        if (iz0 + k >= G.numZ) break;
+        const size_t o = (size_t(iz0 + k) * G.numY + iy) * G.numX + ix;
+        const float r = acc[k] * A.scale;
+        f[o] = A.accumulate ? f[o] + r : r;
+    }
+}
+
+}  // namespace
+
+// kNotApplicable when the layout rules fail (the caller then runs the
+// general kernel): a u0 extent of three bins or more, a tile window above
+// 128 columns, or scratch that cannot be allocated.
+int backproject_rsplit(const petl_geom& G, const float* g, float* f, int accumulate, float scale,
+                       const ViewRange& vr, cudaStream_t st)
+{
+    constexpr int kNotApplicable = -2;
+    const int n_v0 = vr.n_v0(G.N_v0);
+    const int nv1 = vr.iv1_end - vr.iv1_begin;
+    if (n_v0 <= 0 || nv1 <= 0) return kNotApplicable;
+    // per view: width of the u0 extent (T_x max(|wy|, |wx|) / T_u0) and the
+    // spread of its centre over a 16 x 16 tile (15 T_x (|wx| + |wy|) / T_u0)
+    double wmax = 0, need = 0;
+    for (int k = 0; k < n_v0; k++) {
+        const double v0 = std::fmaf(float(vr.iv0_first + k * vr.iv0_step), G.T_v0, G.v0_0);
+        const double wy = std::fabs(v0 * G.cos_psi + G.sin_psi), wx = std::fabs(-v0 * G.sin_psi + G.cos_psi);
+        const double width = double(G.T_x) * std::max(wy, wx) / double(G.T_u0);
+        wmax = std::max(wmax, width);
+        need = std::max(need, (RTX - 1) * double(G.T_x) * (wx + wy) / double(G.T_u0) + width);
+    }
+    const int taps_max = wmax < 1.99 ? 3 : wmax < 2.99 ? 4 : 0;
+    if (!taps_max) return kNotApplicable;
+    // + 2 for the bins' rounding, 1 of margin below, the taps beyond the
+    // extent a block reads with zero weight, 1 of slack
+    const int W = (int(std::ceil(need + 4.0 + taps_max)) + 15) & ~15;
+    if (W > RWMAX) return kNotApplicable;
+    const size_t tsmem = size_t(n_v0) * 12;  // view table
+    if (tsmem > 96 * 1024) return kNotApplicable;
+    int* err = device_error_ptr();
+    if (!err) return kNotApplicable;
+
+    const size_t per_slope = size_t(G.N_u1) * G.numX * G.numY * 4;
+    int nc = int(std::max<size_t>(1, std::min<size_t>(size_t(nv1), gsplit_scratch_budget() / per_slope)));
+    const int nchunks = (nv1 + nc - 1) / nc;
+    nc = (nv1 + nchunks - 1) / nchunks;
+    float* P = nullptr;
+    if (scratch_alloc(reinterpret_cast<void**>(&P), per_slope * nc, st) != cudaSuccess) {
+        cudaGetLastError();
+        return kNotApplicable;
+    }
+    const int ntx = int(ceil_div(G.numX, RTX)), nty = int(ceil_div(G.numY, RTY));
+    cudaError_t e = cudaFuncSetAttribute(k_rbp_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem));
+    for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
+        const int jv1_0 = c * nc, nvc = std::min(nc, nv1 - jv1_0);
+        const RxyArgs XA{G, vr, jv1_0, W, ntx, taps_max, err};
+        k_rbp_xy<<<dim3(unsigned(ntx * nty), ceil_div(G.N_u1, RRB), unsigned(nvc)), RT, tsmem, st>>>(g, P, XA);
+        note_launch();
+        const RzArgs ZA{G, vr, jv1_0, nvc, c == 0 ? accumulate : 1, scale};
+        k_rbp_z<<<dim3(ceil_div(G.numX, 32), ceil_div(G.numY, 8), ceil_div(G.numZ, RZB)), dim3(32, 8), 0, st>>>(P, f, ZA);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(P, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("backproject_rsplit: ") + cudaGetErrorString(e));
+        return int(e);
+    }
+    return 0;
+}
+
+}  // namespace petl

@@ -177,8 +177,9 @@ int backproject_range(const petl_geom& G, const float* g, float* f, int mode, in
         cudaFreeAsync(bt, st);
         return rc;
     }
-    if (mode == PETL_BP_ADJOINT && dispatch_mode() == 0) {
-        const int rc = backproject_gsplit_adjoint(G, g, f, accumulate, scale, vr, st);
+    if (dispatch_mode() == 0) {
+        const int rc = mode == PETL_BP_ADJOINT ? backproject_gsplit_adjoint(G, g, f, accumulate, scale, vr, st)
+                                               : backproject_rsplit(G, g, f, accumulate, scale, vr, st);
         if (rc != -2) {
             note_path(3);
             return rc;

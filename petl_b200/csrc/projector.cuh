@@ -177,5 +177,11 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
 // layout rules fail (the caller then runs launch_backproject_general).
 int backproject_gsplit_adjoint(const petl_geom& G, const float* g, float* f, int accumulate, float scale,
                                const ViewRange& vr, cudaStream_t st);
+// Backprojection with the reference's semantics for any psi, split into an
+// in-plane pass per (v1, u1) slice and a z pass (backprojector_rsplit.cu);
+// -2 when its layout rules fail (the caller then runs
+// launch_backproject_general).
+int backproject_rsplit(const petl_geom& G, const float* g, float* f, int accumulate, float scale,
+                       const ViewRange& vr, cudaStream_t st);
 
 }  // namespace petl
