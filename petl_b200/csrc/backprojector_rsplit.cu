@@ -36,16 +36,17 @@ namespace petl {
 namespace {
 
 constexpr int RTX = 16, RTY = 16, RT = RTX * RTY;  // voxel columns per k_rbp_xy block (one per thread)
-constexpr int RRB = 16;                            // u1 rows per k_rbp_xy block
+constexpr int RRB = 32;                            // u1 rows per k_rbp_xy block
+constexpr int RRP = RRB + 4;                       // staged floats per column (rows + 16 bytes of padding)
 constexpr int RWMAX = 128;                         // staged u0 columns per view at most
-constexpr int RPF = RRB * RWMAX / RT;              // staged values per thread at most
+constexpr int RSTG = 3;                            // views in flight (cp.async ring)
 constexpr int RZB = 16;                            // z rows per k_rbp_z thread
 
 struct RxyArgs {
     petl_geom G;
     ViewRange vr;
     int jv1_0;     // first slope of the chunk (index in the range)
-    int W;         // staged u0 columns per view (<= RWMAX)
+    int lgW;       // log2 of the staged u0 columns per view (W <= RWMAX)
     int ntx;       // tiles along x
     int taps_max;  // taps per row and view at most (host bound)
     int* err;
@@ -109,31 +110,47 @@ __device__ __forceinline__ float u0_width(const petl_geom& G, const ViewU0& q)
     return fabsf(fmaf(q.v0, 2.0f * ht, 2.0f * hx)) * (1.0f / G.T_u0);
 }
 
+// 4-byte asynchronous copy global -> shared, zero-filled when !ok
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// rows += the view's NT taps: a column's RRB rows are contiguous (16-byte
+// reads), the weights hold l_phi
 template <int NT>
-__device__ __forceinline__ void sum_taps(const float* __restrict__ s, int W, int nw, int u0_min, float A, float B,
+__device__ __forceinline__ void sum_taps(const float* __restrict__ s, int nw, int u0_min, float A, float B,
                                          float l_phi, float (&acc)[RRB])
 {
-    float w[NT];
 #pragma unroll
-    for (int i = 0; i < NT; i++)
-        w[i] = fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, B) - fmaxf(float(u0_min + i) - 0.5f, A));
+    for (int i = 0; i < NT; i++) {
+        if (i >= nw) break;
+        const float w = l_phi * fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, B) - fmaxf(float(u0_min + i) - 0.5f, A));
+        const float4* c = reinterpret_cast<const float4*>(s + i * RRP);
 #pragma unroll
-    for (int r = 0; r < RRB; r++) {
-        float s0 = 0.0f;
-#pragma unroll
-        for (int i = 0; i < NT; i++) {
-            const float v = s[r * W + i];
-            if (i < nw) s0 = fmaf(w[i], v, s0);
+        for (int j = 0; j < RRB / 4; j++) {
+            const float4 v = c[j];
+            acc[4 * j] = fmaf(w, v.x, acc[4 * j]);
+            acc[4 * j + 1] = fmaf(w, v.y, acc[4 * j + 1]);
+            acc[4 * j + 2] = fmaf(w, v.z, acc[4 * j + 2]);
+            acc[4 * j + 3] = fmaf(w, v.w, acc[4 * j + 3]);
         }
-        acc[r] = fmaf(l_phi, s0, acc[r]);
     }
 }
 
-// P[jv1][u1][y][x] for 16 x 16 columns and 16 rows of one slope.  Grid
-// (tiles, ceil(N_u1 / 16), slopes of the chunk); 256 threads.
+// P[jv1][u1][y][x] for 16 x 16 columns and 32 rows of one slope.  Grid
+// (tiles, ceil(N_u1 / 32), slopes of the chunk); 256 threads; dynamic shared
+// memory: a ring of RSTG views of W columns x RRP floats, then the view table.
 __global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, float* __restrict__ P, const RxyArgs A)
 {
-    __shared__ float sg[2][RRB * RWMAX];
+    extern __shared__ __align__(16) float rsm[];
     const petl_geom& G = A.G;
     const int tid = threadIdx.x, tx = tid % RTX, ty = tid / RTX;
     const int tix = blockIdx.x % A.ntx, tiy = blockIdx.x / A.ntx;
@@ -144,18 +161,18 @@ __global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, floa
     const int r0 = blockIdx.y * RRB;
     const int jv1 = blockIdx.z;
     const int iv1 = A.vr.iv1_begin + A.jv1_0 + jv1;
-    const int W = A.W;
+    const int lgW = A.lgW, W = 1 << lgW;
     const float v1 = fmaf(float(iv1), G.T_v1, G.v1_0);
     float t, xdt;
     voxel_tx(G, min(ix, G.numX - 1), min(iy, G.numY - 1), t, xdt);
+    float* ring = rsm;  // [RSTG][W][RRP]
     // per view of the call: first staged column (the smallest first bin over
     // the tile's corners, the extent being affine in x and y, less one of
     // margin), l_phi and the taps a row takes at most (floor(width) + 2)
-    extern __shared__ int vtab[];  // [3][n_v0]
     const int nv0 = A.vr.n_v0(G.N_v0);
-    int* s_lo = vtab;
-    float* s_lphi = reinterpret_cast<float*>(vtab + nv0);
-    int* s_nwv = vtab + 2 * nv0;
+    int* s_lo = reinterpret_cast<int*>(rsm + RSTG * W * RRP);
+    float* s_lphi = reinterpret_cast<float*>(s_lo + nv0);
+    int* s_nwv = s_lo + 2 * nv0;
     {
         float tc[4], xc[4];
         voxel_tx(G, x0, y0, tc[0], xc[0]);
@@ -177,76 +194,66 @@ __global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, floa
         }
     }
     __syncthreads();
-    float pf[RPF];
-    auto prefetch = [&](int iv0, int lo) {
+    // copies of view k into ring slot k % RSTG: thread e -> row e >> lgW,
+    // column e & (W - 1) (coalesced in u0), stored column-major
+    auto issue = [&](int k) {
+        const int iv0 = A.vr.iv0_first + k * A.vr.iv0_step, lo = s_lo[k];
+        float* dst = ring + (k % RSTG) * W * RRP;
         const float* gv = g + (size_t(iv1) * G.N_v0 + iv0) * G.N_u1 * G.N_u0;
-#pragma unroll
-        for (int i = 0; i < RPF; i++) {
-            const int e = tid + i * RT;
-            float v = 0.0f;
-            if (e < RRB * W) {
-                const int row = e / W, col = e - row * W;
-                const int iu1 = r0 + row, iu0 = lo + col;
-                if (iu1 < G.N_u1 && iu0 < G.N_u0) v = __ldg(&gv[size_t(iu1) * G.N_u0 + iu0]);
-            }
-            pf[i] = v;
+        for (int e = tid; e < (RRB << lgW); e += RT) {
+            const int row = e >> lgW, col = e & (W - 1);
+            const int iu1 = r0 + row, iu0 = lo + col;
+            const bool ok = iu1 < G.N_u1 && iu0 < G.N_u0;
+            cp_async4(dst + col * RRP + row, ok ? gv + size_t(iu1) * G.N_u0 + iu0 : g, ok);
         }
+        cp_async_commit();
     };
-    auto commit = [&](int buf) {
 #pragma unroll
-        for (int i = 0; i < RPF; i++) {
-            const int e = tid + i * RT;
-            if (e < RRB * W) sg[buf][e] = pf[i];
-        }
-    };
+    for (int k = 0; k < RSTG - 1; k++) {
+        if (k < nv0) issue(k);
+        else cp_async_commit();
+    }
 
     float acc[RRB];
 #pragma unroll
     for (int r = 0; r < RRB; r++) acc[r] = 0.0f;
-    prefetch(A.vr.iv0_first, s_lo[0]);
-    commit(0);
-    __syncthreads();
     for (int k = 0; k < nv0; k++) {
+        cp_async_wait<RSTG - 2>();  // this thread's copies of view k landed
+        __syncthreads();            // everyone's did; everyone finished reading view k - 1
+        if (k + RSTG - 1 < nv0) issue(k + RSTG - 1);  // into the slot of view k - 1
+        else cp_async_commit();
+        if (!live) continue;
         const int iv0 = A.vr.iv0_first + k * A.vr.iv0_step;
-        const int buf = k & 1;
-        if (k + 1 < nv0) prefetch(iv0 + A.vr.iv0_step, s_lo[k + 1]);
-        if (live) {
-            ViewU0 q = view_u0(G, iv0, v1);
-            q.l_phi = s_lphi[k];
-            float a, b;
-            u0_extent(G, q, t, xdt, a, b);
-            const int u0_min = max(int(ceilf(a - 0.5f)), 0);
-            const int u0_max = min(int(floorf(b + 0.5f)), G.N_u0 - 1);
-            const int nw = u0_max - u0_min + 1;
-            const int nwv = s_nwv[k];  // uniform over the block
-            int off = u0_min - s_lo[k];
-            if (nw > 0) {
-                if (off < 0 || off + max(nw, nwv) > W) {  // outside the staged window: the host bound failed
-                    atomicOr(A.err, kErrLayout);
-                    off = 0;
-                }
-                const float* s = sg[buf] + off;
-                if (nw > nwv) {  // a rounding edge: the plain loop
-                    for (int r = 0; r < RRB; r++) {
-                        float s0 = 0.0f;
-                        for (int i = 0; i < nw && off + i < W; i++) {
-                            const float w0 = fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, b) - fmaxf(float(u0_min + i) - 0.5f, a));
-                            s0 = fmaf(w0, s[r * W + i], s0);
-                        }
-                        acc[r] = fmaf(q.l_phi, s0, acc[r]);
-                    }
-                } else if (nwv <= 2) {
-                    sum_taps<2>(s, W, nw, u0_min, a, b, q.l_phi, acc);
-                } else if (nwv == 3) {
-                    sum_taps<3>(s, W, nw, u0_min, a, b, q.l_phi, acc);
-                } else {
-                    sum_taps<4>(s, W, nw, u0_min, a, b, q.l_phi, acc);
-                }
-            }
+        const ViewU0 q = view_u0(G, iv0, v1);
+        float a, b;
+        u0_extent(G, q, t, xdt, a, b);
+        const int u0_min = max(int(ceilf(a - 0.5f)), 0);
+        const int u0_max = min(int(floorf(b + 0.5f)), G.N_u0 - 1);
+        const int nw = u0_max - u0_min + 1;
+        if (nw <= 0) continue;
+        const int nwv = s_nwv[k];  // uniform over the block
+        int off = u0_min - s_lo[k];
+        if (off < 0 || off + nw > W) {  // outside the staged window: the host bound failed
+            atomicOr(A.err, kErrLayout);
+            continue;
         }
-        if (k + 1 < nv0) commit(buf ^ 1);
-        __syncthreads();
+        const float* s = ring + (k % RSTG) * W * RRP + off * RRP;
+        const float l_phi = s_lphi[k];
+        if (nw > nwv) {  // a rounding edge: the plain loop
+            for (int i = 0; i < nw; i++) {
+                const float w = l_phi * fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, b) - fmaxf(float(u0_min + i) - 0.5f, a));
+#pragma unroll
+                for (int r = 0; r < RRB; r++) acc[r] = fmaf(w, s[i * RRP + r], acc[r]);
+            }
+        } else if (nwv <= 2) {
+            sum_taps<2>(s, nw, u0_min, a, b, l_phi, acc);
+        } else if (nwv == 3) {
+            sum_taps<3>(s, nw, u0_min, a, b, l_phi, acc);
+        } else {
+            sum_taps<4>(s, nw, u0_min, a, b, l_phi, acc);
+        }
     }
+    cp_async_wait<0>();
     if (!live) return;
     const size_t plane = size_t(G.numX) * G.numY;
     float* Pc = P + (size_t(jv1) * G.N_u1 + r0) * plane + size_t(iy) * G.numX + ix;
@@ -327,12 +334,13 @@ int backproject_rsplit(const petl_geom& G, const float* g, float* f, int accumul
     }
     const int taps_max = wmax < 1.99 ? 3 : wmax < 2.99 ? 4 : 0;
     if (!taps_max) return kNotApplicable;
-    // + 2 for the bins' rounding, 1 of margin below, the taps beyond the
-    // extent a block reads with zero weight, 1 of slack
-    const int W = (int(std::ceil(need + 4.0 + taps_max)) + 15) & ~15;
-    if (W > RWMAX) return kNotApplicable;
-    const size_t tsmem = size_t(n_v0) * 12;  // view table
-    if (tsmem > 96 * 1024) return kNotApplicable;
+    // + 2 for the bins' rounding, 1 of margin below, 1 of slack; a power of two
+    const int wneed = int(std::ceil(need + 4.0));
+    int lgW = 4;
+    while ((1 << lgW) < wneed) lgW++;
+    if ((1 << lgW) > RWMAX) return kNotApplicable;
+    const size_t tsmem = size_t(RSTG) * (size_t(1) << lgW) * RRP * 4 + size_t(n_v0) * 12;  // ring + view table
+    if (tsmem > 160 * 1024) return kNotApplicable;
     int* err = device_error_ptr();
     if (!err) return kNotApplicable;
 
@@ -349,7 +357,7 @@ int backproject_rsplit(const petl_geom& G, const float* g, float* f, int accumul
     cudaError_t e = cudaFuncSetAttribute(k_rbp_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem));
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int jv1_0 = c * nc, nvc = std::min(nc, nv1 - jv1_0);
-        const RxyArgs XA{G, vr, jv1_0, W, ntx, taps_max, err};
+        const RxyArgs XA{G, vr, jv1_0, lgW, ntx, taps_max, err};
         k_rbp_xy<<<dim3(unsigned(ntx * nty), ceil_div(G.N_u1, RRB), unsigned(nvc)), RT, tsmem, st>>>(g, P, XA);
         note_launch();
         const RzArgs ZA{G, vr, jv1_0, nvc, c == 0 ? accumulate : 1, scale};
