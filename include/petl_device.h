@@ -82,9 +82,9 @@ int petl_model_solids(int modules, struct petl_solid* out, int capacity);
  * scratch + z-tap kernel).  All compute the same operator. */
 int petl_set_dispatch(int mode);
 /* Which projector kernels the calling thread's last projector call used:
- * 0 general, 1 shear-warp, 2 TMA-staged shear-warp, 3 split forward or
- * split exact-adjoint backprojection for any psi (two passes through
- * scratch); -1 before any call. */
+ * 0 general, 1 shear-warp, 2 TMA-staged shear-warp, 3 the split kernels
+ * for any psi (forward, reference-semantics or exact-adjoint
+ * backprojection; two passes through scratch); -1 before any call. */
 int petl_last_projector_path(void);
 
 /* List-mode binning (src/binning.cpp:614-790 with src/planogram.cpp:113-141):

@@ -174,8 +174,10 @@ def study_kernels(seed=0, reps=10):
         out[name] = r
     # projectors by planogram orientation at 256x256x128 (1 mm): psi = 0 and
     # 90 run the shear-warp kernels (90 on the volume with x and y
-    # exchanged), psi = 30 the general kernels; FP32 fraction of 2 nnz(A)
-    # flops per call at the nominal rate (148 SM x 128 FMA/clk at 1965 MHz)
+    # exchanged), psi = 30 the split kernels for any psi; backward in the
+    # reference's semantics and as the exact adjoint; FP32 fraction of
+    # 2 nnz(A) flops per call at the nominal rate (148 SM x 128 FMA/clk at
+    # 1965 MHz)
     fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
     from . import lib
     for psi in (0.0, 90.0, 30.0):
@@ -184,11 +186,14 @@ def study_kernels(seed=0, reps=10):
         g = torch.empty(G.shape, device="cuda")
         b = torch.empty_like(f)
         nnz = ops.nnz(G)
-        reps_p = reps if psi != 30.0 else 2
         ops.project(G, f, g)
         path = lib().petl_last_projector_path()
-        ts_f, ts_b = [], []
-        for _ in range(reps_p):
+        ops.backproject(G, g, b)
+        path_b = lib().petl_last_projector_path()
+        ops.backproject(G, g, b, mode="adjoint")
+        path_a = lib().petl_last_projector_path()
+        ts_f, ts_b, ts_a = [], [], []
+        for _ in range(reps):
             flush.zero_()
             with Timer() as t:
                 ops.project(G, f, g)
@@ -197,11 +202,17 @@ def study_kernels(seed=0, reps=10):
             with Timer() as t:
                 ops.backproject(G, g, b)
             ts_b.append(t.ms)
-        tf, tb = float(np.median(ts_f)), float(np.median(ts_b))
-        out[f"project_psi{int(psi)}"] = {"planogram": list(G.shape), "path": path, "forward_ms": tf,
-                                         "backward_ms": tb, "nnz": nnz,
+            flush.zero_()
+            with Timer() as t:
+                ops.backproject(G, g, b, mode="adjoint")
+            ts_a.append(t.ms)
+        tf, tb, ta = float(np.median(ts_f)), float(np.median(ts_b)), float(np.median(ts_a))
+        out[f"project_psi{int(psi)}"] = {"planogram": list(G.shape), "path": path, "path_backward": path_b,
+                                         "path_adjoint": path_a, "forward_ms": tf, "backward_ms": tb,
+                                         "adjoint_ms": ta, "nnz": nnz,
                                          "forward_fp32_frac": 2 * nnz / (tf * 1e-3) / 1e12 / fp32_peak,
-                                         "backward_fp32_frac": 2 * nnz / (tb * 1e-3) / 1e12 / fp32_peak}
+                                         "backward_fp32_frac": 2 * nnz / (tb * 1e-3) / 1e12 / fp32_peak,
+                                         "adjoint_fp32_frac": 2 * nnz / (ta * 1e-3) / 1e12 / fp32_peak}
     return out
 
 
@@ -567,6 +578,7 @@ def main(argv=None):
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--sizes", default="64,128,192,256", help="serving: volume sizes N drawn")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
+    ap.add_argument("--reps", type=int, default=0, help="kernels: timed calls per figure (0: the study's default)")
     a = ap.parse_args(argv)
     fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
           "binning": study_binning, "corrections": study_corrections, "response": study_response,
@@ -574,6 +586,8 @@ def main(argv=None):
     if a.study == "serving":
         res = study_serving(n=a.requests, seed=a.seed, rate=a.rate,
                             sizes=tuple(int(v) for v in a.sizes.split(",")))
+    elif a.study == "kernels" and a.reps > 0:
+        res = study_kernels(seed=a.seed, reps=a.reps)
     else:
         res = fn[a.study](seed=a.seed)
     print(json.dumps(res))
