@@ -86,26 +86,27 @@ struct GxTArgs {
 };
 
 // h[vi][v1 - v1_begin][u1][c] = g l_phi rs on visible rays, 0 elsewhere
-// (columns N_u0 .. NUc - 1 included)
+// (columns N_u0 .. NUc - 1 included).  l_phi and rs depend on the view and
+// the slope only; grid (column blocks, (view, slope) slabs), both strided.
 __global__ void k_gprep(const float* __restrict__ g, float* __restrict__ h, const GprepArgs A)
 {
     const petl_geom& G = A.G;
     const int nv1 = A.vr.iv1_end - A.vr.iv1_begin;
-    const size_t total = size_t(A.nvc) * nv1 * G.N_u1 * A.NUc;
-    for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += size_t(gridDim.x) * blockDim.x) {
-        size_t r = e / A.NUc;
-        const int c = int(e - r * A.NUc);
-        const int iu1 = int(r % G.N_u1);
-        r /= G.N_u1;
-        const int jv1 = int(r % nv1), vi = int(r / nv1);
+    const int per = G.N_u1 * A.NUc;  // elements per slab
+    for (int slab = blockIdx.y; slab < A.nvc * nv1; slab += gridDim.y) {
+        const int vi = slab / nv1, jv1 = slab - vi * nv1;
         const int iv1 = A.vr.iv1_begin + jv1;
         const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
-        float val = 0.0f;
-        if (c < G.N_u0 && ray_visible(G, iv1, iv0, iu1, c)) {
-            const RayGeom rr = ray_geom(G, iv1, iv0, iu1, c);
-            val = fmul(fmul(__ldg(&g[((size_t(iv1) * G.N_v0 + iv0) * G.N_u1 + iu1) * G.N_u0 + c]), rr.l_phi), rr.rs);
+        const RayGeom rr = ray_geom(G, iv1, iv0, 0, 0);
+        const float* gs = g + (size_t(iv1) * G.N_v0 + iv0) * G.N_u1 * G.N_u0;
+        float* hs = h + size_t(slab) * per;
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < per; e += gridDim.x * blockDim.x) {
+            const int iu1 = e / A.NUc, c = e - iu1 * A.NUc;
+            float val = 0.0f;
+            if (c < G.N_u0 && ray_visible(G, iv1, iv0, iu1, c))
+                val = fmul(fmul(__ldg(&gs[size_t(iu1) * G.N_u0 + c]), rr.l_phi), rr.rs);
+            hs[e] = val;
         }
-        h[e] = val;
     }
 }
 
@@ -474,8 +475,9 @@ int backproject_gsplit_adjoint(const petl_geom& G, const float* g, float* f, int
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
         const GprepArgs P{G, vr, vi0, nvc, NUc};
-        const size_t nh = size_t(nvc) * nv1 * G.N_u1 * NUc;
-        k_gprep<<<unsigned(std::min<size_t>(ceil_div(nh, size_t(256)), size_t(148) * 16)), 256, 0, st>>>(g, H, P);
+        const unsigned gx = unsigned(std::min<size_t>(ceil_div(size_t(G.N_u1) * NUc, size_t(256)), 32));
+        const unsigned gy = unsigned(std::min<size_t>(size_t(nvc) * nv1, 8192));
+        k_gprep<<<dim3(gx, gy), 256, 0, st>>>(g, H, P);
         note_launch();
         Z.vi0 = vi0;
         k_gzT<<<dim3(zblk, unsigned(nvc)), TZT, zsmem, st>>>(map, Y, Z);

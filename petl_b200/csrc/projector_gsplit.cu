@@ -52,12 +52,14 @@ namespace petl {
 namespace {
 
 constexpr int GXZ = 8;        // volume rows per k_gx block
-constexpr int GZS = 16;       // slopes per k_gz CTA (4 per warp)
-constexpr int GZR = 32;       // rows per k_gz CTA (8 per warp)
+constexpr int GZS = 16;       // slopes per k_gz CTA (2 per warp), main shape
+constexpr int GZR = 32;       // rows per k_gz CTA (16 per warp), main shape
+constexpr int GZS_T = 4;      // slopes per CTA of the tail shape (a last slope block of at most 8)
+constexpr int GZR_T = 128;    // rows per CTA of the tail shape
 constexpr int GZC = 32;       // columns per k_gz CTA (one per lane)
 constexpr int GZT = 512;      // threads per k_gz CTA
 constexpr int GJS = 2;        // slopes per warp
-constexpr int GRW = 16;       // rows per warp (GZS / GJS x GZR / GRW = 16 warps)
+constexpr int GRW = 16;       // rows per warp (GZS / GJS x GZR / GRW = 16 warps; GZS_T / GJS x GZR_T / GRW the same)
 constexpr int GZRMAX = 224;   // staged rows per plane at most (TMA box rows <= 256)
 constexpr int GZNS = 3;       // ring stages (one plane each) at most
 
@@ -125,13 +127,19 @@ __global__ void __launch_bounds__(256) k_gx(const float* __restrict__ f, const f
 }
 
 
+// NQ slope pairs x (16 / NQ) row groups of 16 per CTA: NQ = 8 is the main
+// shape (16 slopes x 32 rows), NQ = 2 the tail shape (4 slopes x 128 rows)
+// for a last block of few slopes, which would leave most warps of a
+// 16-slope CTA idle.
+template <int NQ>
 __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorMap xmap, float* __restrict__ g,
                                                 const float* __restrict__ meas, const GzArgs A)
 {
+    constexpr int SZ = NQ * GJS, RZ = (GZT / 32 / NQ) * GRW;
     extern __shared__ __align__(128) unsigned char gsm[];
     const petl_geom& G = A.G;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = warp % (GZS / GJS), rg = warp / (GZS / GJS);
+    const int q = warp % NQ, rg = warp / NQ;
     int t_ = blockIdx.x;
     const int colblk = t_ % A.n_colblk;
     t_ /= A.n_colblk;
@@ -140,9 +148,9 @@ __global__ void __launch_bounds__(GZT, 1) k_gz(const __grid_constant__ CUtensorM
     const int vi = blockIdx.y;
     const int iv0 = A.vr.iv0_first + (A.vi0 + vi) * A.vr.iv0_step;
     const int col0 = colblk * GZC, iu0 = col0 + lane;
-    const int row0c = rowblk * GZR, row0 = row0c + rg * GRW;
-    const int v1c = A.vr.iv1_begin + v1blk * GZS;           // first slope of the CTA
-    const int v1c_last = min(v1c + GZS, A.vr.iv1_end) - 1;  // last slope of the CTA
+    const int row0c = rowblk * RZ, row0 = row0c + rg * GRW;
+    const int v1c = A.vr.iv1_begin + v1blk * SZ;           // first slope of the CTA
+    const int v1c_last = min(v1c + SZ, A.vr.iv1_end) - 1;  // last slope of the CTA
     const int v1w = v1c + q * GJS;                          // first slope of the warp
     const int nrows = A.nrows, ns = A.ns;
     const float Tu1_inv = __frcp_rn(G.T_u1);
@@ -303,26 +311,34 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
     const int nv1 = vr.iv1_end - vr.iv1_begin;
     if (n_v0 <= 0 || nv1 <= 0) return 0;
     if (G.T_z != G.T_u1 || G.N_u0 > 4096 || G.numX > 4096 || G.numY > 4096) return kNotApplicable;
-    // staged rows per plane: 32 + the range of floor(-c0) over a tile's 32
-    // columns and 16 slopes + margins.  -c0 = (u1_0 - z_0 + t v1) / T_u1 with
-    // t = (coordinate of the plane - u0 pscale) * inv: bounded with the
-    // extremes of |t| and of its change over 32 columns.
+    // staged rows per plane: the CTA's rows + the range of floor(-c0) over a
+    // tile's 32 columns and its slopes + margins.  -c0 = (u1_0 - z_0 + t v1)
+    // / T_u1 with t = (coordinate of the plane - u0 pscale) * inv: bounded
+    // with the extremes of |t| and of its change over 32 columns.
     const double vmax = std::max(std::fabs(double(G.v1_0)), std::fabs(double(G.v1_0) + (G.N_v1 - 1) * double(G.T_v1)));
-    const double dv1 = (GZS - 1) * std::fabs(double(G.T_v1));
     const double xext = std::max(std::fabs(double(G.x_0)), std::fabs(double(G.x_0) + (G.numX - 1) * double(G.T_x)));
     const double yext = std::max(std::fabs(double(G.y_0)), std::fabs(double(G.y_0) + (G.numY - 1) * double(G.T_x)));
     const double uext = std::max(std::fabs(double(G.u0_0)), std::fabs(double(G.u0_0) + (G.N_u0 - 1) * double(G.T_u0)));
-    double spread = 0;
+    double tmax = 0, dtmax = 0;
     bool any_xd = false;
     for (int k = 0; k < n_v0; k++) {
         const HostView h = host_view(G, vr.iv0_first + k * vr.iv0_step);
         any_xd = any_xd || h.xd;
-        const double tmax = (std::max(xext, yext) + uext * h.pscale) * std::fabs(h.inv);
-        const double dt = GZC * double(G.T_u0) * h.pscale * std::fabs(h.inv);
-        spread = std::max(spread, (dt * vmax + tmax * dv1 + dt * dv1) / double(G.T_u1));
+        tmax = std::max(tmax, (std::max(xext, yext) + uext * h.pscale) * std::fabs(h.inv));
+        dtmax = std::max(dtmax, GZC * double(G.T_u0) * h.pscale * std::fabs(h.inv));
     }
-    const int nrows = GZR + int(std::ceil(spread * (1.0 + 1e-6))) + 5;  // + floors and the one-row margins
+    auto staged_rows = [&](int slopes, int rows) {
+        const double dv1 = (slopes - 1) * std::fabs(double(G.T_v1));
+        const double spread = (dtmax * vmax + tmax * dv1 + dtmax * dv1) / double(G.T_u1);
+        return rows + int(std::ceil(spread * (1.0 + 1e-6))) + 5;  // + floors and the one-row margins
+    };
+    const int nrows = staged_rows(GZS, GZR);
     if (nrows > GZRMAX) return kNotApplicable;
+    // a last block of at most 8 slopes runs in the tail shape
+    const int rem = nv1 % GZS;
+    const int nrows_t = staged_rows(GZS_T, GZR_T);
+    const bool tail = rem > 0 && rem <= 2 * GZS_T && nrows_t <= GZRMAX && G.N_u1 > GZR;
+    const int nv1_main = tail ? nv1 - rem : nv1;
     int* err = device_error_ptr();
     if (!err) return kNotApplicable;
 
@@ -351,38 +367,61 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
     const int NAmax = any_xd ? std::max(G.numX, G.numY) : G.numX;
     const size_t xsmem = size_t(GXZ) * NAmax * 4;
     e = cudaFuncSetAttribute(k_gx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(xsmem));
-    const size_t stage = size_t(nrows) * GZC * 4;
-    const int ns = int(std::min<size_t>(GZNS, (200 * 1024) / stage));
-    const size_t zsmem = size_t(ns) * stage + GZNS * 16 + GZNS * 8 + 16;
-    if (ns < 2) e = cudaErrorInvalidValue;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(zsmem));
-    GzArgs Z{};
-    Z.G = G;
-    Z.vr = vr;
-    Z.NPmax = NPmax;
-    Z.NUc = NUc;
-    Z.n_colblk = int(ceil_div(G.N_u0, GZC));
-    Z.n_rowblk = int(ceil_div(G.N_u1, GZR));
-    Z.nrows = nrows;
-    Z.ns = ns;
-    Z.err = err;
-    Z.wait_limit = wait_limit();
-    // the scratch as a 3-D tensor: columns, rows, view slot x plane; boxes of
-    // 32 columns x nrows rows (TMA, no multicast; rows outside read zero)
-    CUtensorMap map;
-    const uint64_t dims[3] = {uint64_t(NUc), uint64_t(G.numZ), uint64_t(NPmax) * uint64_t(nv)};
-    const uint64_t strides[2] = {uint64_t(NUc) * 4, uint64_t(NUc) * G.numZ * 4};
-    const uint32_t box[3] = {uint32_t(GZC), uint32_t(nrows), 1u};
-    if (e == cudaSuccess && !encode_tensor_map(&map, X, 3, dims, strides, box, 4)) e = cudaErrorInvalidValue;
-    const unsigned nblk = unsigned(Z.n_colblk) * unsigned(Z.n_rowblk) * ceil_div(nv1, GZS);
+    // one z launch shape: its argument block, tensor map (boxes of 32
+    // columns x its staged rows; TMA, no multicast; rows outside read zero)
+    // and shared memory
+    struct ZLaunch {
+        GzArgs Z;
+        CUtensorMap map;
+        size_t smem;
+        unsigned nblk;
+    };
+    auto z_setup = [&](ZLaunch& L, int rows_cta, int slopes_cta, int staged, int v1b, int v1e) -> cudaError_t {
+        const size_t stage = size_t(staged) * GZC * 4;
+        const int ns = int(std::min<size_t>(GZNS, (200 * 1024) / stage));
+        if (ns < 2) return cudaErrorInvalidValue;
+        L.smem = size_t(ns) * stage + GZNS * 16 + GZNS * 8 + 16;
+        L.Z = GzArgs{};
+        L.Z.G = G;
+        L.Z.vr = vr;
+        L.Z.vr.iv1_begin = v1b;
+        L.Z.vr.iv1_end = v1e;
+        L.Z.NPmax = NPmax;
+        L.Z.NUc = NUc;
+        L.Z.n_colblk = int(ceil_div(G.N_u0, GZC));
+        L.Z.n_rowblk = int(ceil_div(G.N_u1, rows_cta));
+        L.Z.nrows = staged;
+        L.Z.ns = ns;
+        L.Z.err = err;
+        L.Z.wait_limit = wait_limit();
+        L.nblk = unsigned(L.Z.n_colblk) * unsigned(L.Z.n_rowblk) * ceil_div(v1e - v1b, slopes_cta);
+        const uint64_t dims[3] = {uint64_t(NUc), uint64_t(G.numZ), uint64_t(NPmax) * uint64_t(nv)};
+        const uint64_t strides[2] = {uint64_t(NUc) * 4, uint64_t(NUc) * G.numZ * 4};
+        const uint32_t box[3] = {uint32_t(GZC), uint32_t(staged), 1u};
+        return encode_tensor_map(&L.map, X, 3, dims, strides, box, 4) ? cudaSuccess : cudaErrorInvalidValue;
+    };
+    ZLaunch zm{}, zt{};
+    if (e == cudaSuccess && nv1_main > 0) e = z_setup(zm, GZR, GZS, nrows, vr.iv1_begin, vr.iv1_begin + nv1_main);
+    if (e == cudaSuccess && tail) e = z_setup(zt, GZR_T, GZS_T, nrows_t, vr.iv1_begin + nv1_main, vr.iv1_end);
+    if (e == cudaSuccess && nv1_main > 0)
+        e = cudaFuncSetAttribute(k_gz<GZS / GJS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(zm.smem));
+    if (e == cudaSuccess && tail)
+        e = cudaFuncSetAttribute(k_gz<GZS_T / GJS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(zt.smem));
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int vi0 = c * nv, nvc = std::min(nv, n_v0 - vi0);
         const GxArgs XA{G, vr, vi0, NPmax, NUc};
         k_gx<<<dim3(ceil_div(G.numZ, GXZ), unsigned(NPmax), unsigned(nvc)), 256, xsmem, st>>>(f, fT, X, XA);
         note_launch();
-        Z.vi0 = vi0;
-        k_gz<<<dim3(nblk, unsigned(nvc)), GZT, zsmem, st>>>(map, g, meas, Z);
-        note_launch();
+        if (nv1_main > 0) {
+            zm.Z.vi0 = vi0;
+            k_gz<GZS / GJS><<<dim3(zm.nblk, unsigned(nvc)), GZT, zm.smem, st>>>(zm.map, g, meas, zm.Z);
+            note_launch();
+        }
+        if (tail) {
+            zt.Z.vi0 = vi0;
+            k_gz<GZS_T / GJS><<<dim3(zt.nblk, unsigned(nvc)), GZT, zt.smem, st>>>(zt.map, g, meas, zt.Z);
+            note_launch();
+        }
         e = cudaGetLastError();
     }
     cudaFreeAsync(X, st);
