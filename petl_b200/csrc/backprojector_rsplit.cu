@@ -35,7 +35,8 @@ namespace petl {
 
 namespace {
 
-constexpr int RTX = 16, RTY = 16, RT = RTX * RTY;  // voxel columns per k_rbp_xy block (one per thread)
+constexpr int RTX = 16, RTY = 16;                  // voxel columns per k_rbp_xy block
+constexpr int RT2 = RTX * RTY / 2;                 // threads per k_rbp_xy block (two columns each)
 constexpr int RRB = 32;                            // u1 rows per k_rbp_xy block
 constexpr int RRP = RRB + 4;                       // staged floats per column (rows + 16 bytes of padding)
 constexpr int RWMAX = 128;                         // staged u0 columns per view at most
@@ -48,7 +49,6 @@ struct RxyArgs {
     int jv1_0;     // first slope of the chunk (index in the range)
     int lgW;       // log2 of the staged u0 columns per view (W <= RWMAX)
     int ntx;       // tiles along x
-    int taps_max;  // taps per row and view at most (host bound)
     int* err;
 };
 
@@ -100,16 +100,6 @@ __device__ __forceinline__ void u0_extent(const petl_geom& G, const ViewU0& q, f
     B = q.pos ? hi_ : lo_;
 }
 
-// B - A for every voxel of the view (the extent's width does not depend on
-// the voxel)
-__device__ __forceinline__ float u0_width(const petl_geom& G, const ViewU0& q)
-{
-    const float sn = G.sin_psi, cs = G.cos_psi;
-    const float hx = q.ydom ? 0.5f * G.T_x * sn : 0.5f * G.T_x * cs;
-    const float ht = q.ydom ? 0.5f * G.T_x * cs : -0.5f * G.T_x * sn;
-    return fabsf(fmaf(q.v0, 2.0f * ht, 2.0f * hx)) * (1.0f / G.T_u0);
-}
-
 // 4-byte asynchronous copy global -> shared, zero-filled when !ok
 __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok)
 {
@@ -123,63 +113,61 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// rows += the view's NT taps: a column's RRB rows are contiguous (16-byte
-// reads), the weights hold l_phi
-template <int NT>
-__device__ __forceinline__ void sum_taps(const float* __restrict__ s, int nw, int u0_min, float A, float B,
-                                         float l_phi, float (&acc)[RRB])
-{
-#pragma unroll
-    for (int i = 0; i < NT; i++) {
-        if (i >= nw) break;
-        const float w = l_phi * fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, B) - fmaxf(float(u0_min + i) - 0.5f, A));
-        const float4* c = reinterpret_cast<const float4*>(s + i * RRP);
-#pragma unroll
-        for (int j = 0; j < RRB / 4; j++) {
-            const float4 v = c[j];
-            acc[4 * j] = fmaf(w, v.x, acc[4 * j]);
-            acc[4 * j + 1] = fmaf(w, v.y, acc[4 * j + 1]);
-            acc[4 * j + 2] = fmaf(w, v.z, acc[4 * j + 2]);
-            acc[4 * j + 3] = fmaf(w, v.w, acc[4 * j + 3]);
-        }
-    }
-}
-
-// P[jv1][u1][y][x] for 16 x 16 columns and 32 rows of one slope.  Grid
-// (tiles, ceil(N_u1 / 32), slopes of the chunk); 256 threads; dynamic shared
-// memory: a ring of RSTG views of W columns x RRP floats, then the view table.
-__global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, float* __restrict__ P, const RxyArgs A)
+// P[jv1][u1][y][x] for 16 x 16 columns and 32 rows of one slope.  A thread
+// takes two neighbouring voxel columns along y (PY) or x, the axis along
+// which the u0 extent moves less per voxel, so that their taps share most
+// staged columns: it walks the union of their u0 ranges in ascending order
+// and applies each staged column (32 rows, 16-byte reads) to both with their
+// own weights (predicated off outside a voxel's range, as the reference
+// reads no bin outside it).  Grid (tiles, ceil(N_u1 / 32), slopes of the
+// chunk); 128 threads; dynamic shared memory: a ring of RSTG views of
+// W columns x RRP floats, then the view table.
+template <bool PY>
+__global__ void __launch_bounds__(RT2, 4) k_rbp_xy(const float* __restrict__ g, float* __restrict__ P,
+                                                   const RxyArgs A)
 {
     extern __shared__ __align__(16) float rsm[];
     const petl_geom& G = A.G;
-    const int tid = threadIdx.x, tx = tid % RTX, ty = tid / RTX;
+    const int tid = threadIdx.x;
     const int tix = blockIdx.x % A.ntx, tiy = blockIdx.x / A.ntx;
     const int x0 = tix * RTX, y0 = tiy * RTY;
     const int xl = min(x0 + RTX, G.numX) - 1, yl = min(y0 + RTY, G.numY) - 1;
-    const int ix = x0 + tx, iy = y0 + ty;
-    const bool live = ix < G.numX && iy < G.numY;
+    int ix[2], iy[2];
+    if (PY) {
+        ix[0] = ix[1] = x0 + tid % RTX;
+        iy[0] = y0 + 2 * (tid / RTX);
+        iy[1] = iy[0] + 1;
+    } else {
+        ix[0] = x0 + 2 * (tid % (RTX / 2));
+        ix[1] = ix[0] + 1;
+        iy[0] = iy[1] = y0 + tid / (RTX / 2);
+    }
+    bool live[2];
+    float t[2], xdt[2];
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+        live[v] = ix[v] < G.numX && iy[v] < G.numY;
+        voxel_tx(G, min(ix[v], G.numX - 1), min(iy[v], G.numY - 1), t[v], xdt[v]);
+    }
     const int r0 = blockIdx.y * RRB;
     const int jv1 = blockIdx.z;
     const int iv1 = A.vr.iv1_begin + A.jv1_0 + jv1;
     const int lgW = A.lgW, W = 1 << lgW;
     const float v1 = fmaf(float(iv1), G.T_v1, G.v1_0);
-    float t, xdt;
-    voxel_tx(G, min(ix, G.numX - 1), min(iy, G.numY - 1), t, xdt);
     float* ring = rsm;  // [RSTG][W][RRP]
     // per view of the call: first staged column (the smallest first bin over
     // the tile's corners, the extent being affine in x and y, less one of
-    // margin), l_phi and the taps a row takes at most (floor(width) + 2)
+    // margin) and l_phi
     const int nv0 = A.vr.n_v0(G.N_v0);
     int* s_lo = reinterpret_cast<int*>(rsm + RSTG * W * RRP);
     float* s_lphi = reinterpret_cast<float*>(s_lo + nv0);
-    int* s_nwv = s_lo + 2 * nv0;
     {
         float tc[4], xc[4];
         voxel_tx(G, x0, y0, tc[0], xc[0]);
         voxel_tx(G, xl, y0, tc[1], xc[1]);
         voxel_tx(G, x0, yl, tc[2], xc[2]);
         voxel_tx(G, xl, yl, tc[3], xc[3]);
-        for (int k = tid; k < nv0; k += RT) {
+        for (int k = tid; k < nv0; k += RT2) {
             const ViewU0 q = view_u0(G, A.vr.iv0_first + k * A.vr.iv0_step, v1);
             float m = 3.0e38f;
 #pragma unroll
@@ -190,7 +178,6 @@ __global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, floa
             }
             s_lo[k] = max(0, int(ceilf(m - 0.5f)) - 1);
             s_lphi[k] = q.l_phi;
-            s_nwv[k] = min(A.taps_max, int(u0_width(G, q)) + 2);
         }
     }
     __syncthreads();
@@ -200,7 +187,7 @@ __global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, floa
         const int iv0 = A.vr.iv0_first + k * A.vr.iv0_step, lo = s_lo[k];
         float* dst = ring + (k % RSTG) * W * RRP;
         const float* gv = g + (size_t(iv1) * G.N_v0 + iv0) * G.N_u1 * G.N_u0;
-        for (int e = tid; e < (RRB << lgW); e += RT) {
+        for (int e = tid; e < (RRB << lgW); e += RT2) {
             const int row = e >> lgW, col = e & (W - 1);
             const int iu1 = r0 + row, iu0 = lo + col;
             const bool ok = iu1 < G.N_u1 && iu0 < G.N_u0;
@@ -214,52 +201,69 @@ __global__ void __launch_bounds__(RT) k_rbp_xy(const float* __restrict__ g, floa
         else cp_async_commit();
     }
 
-    float acc[RRB];
+    float acc[2][RRB];
 #pragma unroll
-    for (int r = 0; r < RRB; r++) acc[r] = 0.0f;
+    for (int v = 0; v < 2; v++)
+#pragma unroll
+        for (int r = 0; r < RRB; r++) acc[v][r] = 0.0f;
     for (int k = 0; k < nv0; k++) {
         cp_async_wait<RSTG - 2>();  // this thread's copies of view k landed
         __syncthreads();            // everyone's did; everyone finished reading view k - 1
         if (k + RSTG - 1 < nv0) issue(k + RSTG - 1);  // into the slot of view k - 1
         else cp_async_commit();
-        if (!live) continue;
-        const int iv0 = A.vr.iv0_first + k * A.vr.iv0_step;
-        const ViewU0 q = view_u0(G, iv0, v1);
-        float a, b;
-        u0_extent(G, q, t, xdt, a, b);
-        const int u0_min = max(int(ceilf(a - 0.5f)), 0);
-        const int u0_max = min(int(floorf(b + 0.5f)), G.N_u0 - 1);
-        const int nw = u0_max - u0_min + 1;
-        if (nw <= 0) continue;
-        const int nwv = s_nwv[k];  // uniform over the block
-        int off = u0_min - s_lo[k];
-        if (off < 0 || off + nw > W) {  // outside the staged window: the host bound failed
+        const ViewU0 q = view_u0(G, A.vr.iv0_first + k * A.vr.iv0_step, v1);
+        float a[2], b[2];
+        int umin[2], umax[2];
+#pragma unroll
+        for (int v = 0; v < 2; v++) {
+            u0_extent(G, q, t[v], xdt[v], a[v], b[v]);
+            umin[v] = max(int(ceilf(a[v] - 0.5f)), 0);
+            umax[v] = live[v] ? min(int(floorf(b[v] + 0.5f)), G.N_u0 - 1) : -1;
+        }
+        // the union of the live voxels' ranges
+        const int cmin = umax[0] < umin[0] ? umin[1] : umax[1] < umin[1] ? umin[0] : min(umin[0], umin[1]);
+        const int cmax = max(umax[0], umax[1]);
+        if (cmax < cmin) continue;
+        const int lo = s_lo[k];
+        if (cmin - lo < 0 || cmax - lo >= W) {  // outside the staged window: the host bound failed
             atomicOr(A.err, kErrLayout);
             continue;
         }
-        const float* s = ring + (k % RSTG) * W * RRP + off * RRP;
         const float l_phi = s_lphi[k];
-        if (nw > nwv) {  // a rounding edge: the plain loop
-            for (int i = 0; i < nw; i++) {
-                const float w = l_phi * fmaxf(0.0f, fminf(float(u0_min + i) + 0.5f, b) - fmaxf(float(u0_min + i) - 0.5f, a));
+        const float* s = ring + (k % RSTG) * W * RRP + (cmin - lo) * RRP;
+        for (int c = cmin; c <= cmax; c++, s += RRP) {
+            float w[2];
+            bool in[2];
 #pragma unroll
-                for (int r = 0; r < RRB; r++) acc[r] = fmaf(w, s[i * RRP + r], acc[r]);
+            for (int v = 0; v < 2; v++) {
+                in[v] = c >= umin[v] && c <= umax[v];
+                w[v] = l_phi * fmaxf(0.0f, fminf(float(c) + 0.5f, b[v]) - fmaxf(float(c) - 0.5f, a[v]));
             }
-        } else if (nwv <= 2) {
-            sum_taps<2>(s, nw, u0_min, a, b, l_phi, acc);
-        } else if (nwv == 3) {
-            sum_taps<3>(s, nw, u0_min, a, b, l_phi, acc);
-        } else {
-            sum_taps<4>(s, nw, u0_min, a, b, l_phi, acc);
+            const float4* col = reinterpret_cast<const float4*>(s);
+#pragma unroll
+            for (int j = 0; j < RRB / 4; j++) {
+                const float4 x = col[j];
+#pragma unroll
+                for (int v = 0; v < 2; v++) {
+                    if (!in[v]) continue;
+                    acc[v][4 * j] = fmaf(w[v], x.x, acc[v][4 * j]);
+                    acc[v][4 * j + 1] = fmaf(w[v], x.y, acc[v][4 * j + 1]);
+                    acc[v][4 * j + 2] = fmaf(w[v], x.z, acc[v][4 * j + 2]);
+                    acc[v][4 * j + 3] = fmaf(w[v], x.w, acc[v][4 * j + 3]);
+                }
+            }
         }
     }
     cp_async_wait<0>();
-    if (!live) return;
     const size_t plane = size_t(G.numX) * G.numY;
-    float* Pc = P + (size_t(jv1) * G.N_u1 + r0) * plane + size_t(iy) * G.numX + ix;
 #pragma unroll
-    for (int r = 0; r < RRB; r++)
-        if (r0 + r < G.N_u1) Pc[size_t(r) * plane] = acc[r];
+    for (int v = 0; v < 2; v++) {
+        if (!live[v]) continue;
+        float* Pc = P + (size_t(jv1) * G.N_u1 + r0) * plane + size_t(iy[v]) * G.numX + ix[v];
+#pragma unroll
+        for (int r = 0; r < RRB; r++)
+            if (r0 + r < G.N_u1) Pc[size_t(r) * plane] = acc[v][r];
+    }
 }
 
 // f(x, y, z) (+)= scale T_x sum over the chunk's slopes of the reference's
@@ -324,22 +328,28 @@ int backproject_rsplit(const petl_geom& G, const float* g, float* f, int accumul
     if (n_v0 <= 0 || nv1 <= 0) return kNotApplicable;
     // per view: width of the u0 extent (T_x max(|wy|, |wx|) / T_u0) and the
     // spread of its centre over a 16 x 16 tile (15 T_x (|wx| + |wy|) / T_u0)
-    double wmax = 0, need = 0;
+    // (|wy| is the shift per voxel along y, |wx| along x: a thread's two
+    // voxels lie along the axis with the smaller mean shift)
+    double wmax = 0, need = 0, sum_wx = 0, sum_wy = 0;
     for (int k = 0; k < n_v0; k++) {
         const double v0 = std::fmaf(float(vr.iv0_first + k * vr.iv0_step), G.T_v0, G.v0_0);
         const double wy = std::fabs(v0 * G.cos_psi + G.sin_psi), wx = std::fabs(-v0 * G.sin_psi + G.cos_psi);
         const double width = double(G.T_x) * std::max(wy, wx) / double(G.T_u0);
         wmax = std::max(wmax, width);
         need = std::max(need, (RTX - 1) * double(G.T_x) * (wx + wy) / double(G.T_u0) + width);
+        sum_wx += wx;
+        sum_wy += wy;
     }
-    const int taps_max = wmax < 1.99 ? 3 : wmax < 2.99 ? 4 : 0;
-    if (!taps_max) return kNotApplicable;
+    // extents of three bins or more (voxels wider than ~3 u0 bins) keep the
+    // general kernel
+    if (!(wmax < 2.99)) return kNotApplicable;
+    const bool pair_y = sum_wy <= sum_wx;
     // + 2 for the bins' rounding, 1 of margin below, 1 of slack; a power of two
     const int wneed = int(std::ceil(need + 4.0));
     int lgW = 4;
     while ((1 << lgW) < wneed) lgW++;
     if ((1 << lgW) > RWMAX) return kNotApplicable;
-    const size_t tsmem = size_t(RSTG) * (size_t(1) << lgW) * RRP * 4 + size_t(n_v0) * 12;  // ring + view table
+    const size_t tsmem = size_t(RSTG) * (size_t(1) << lgW) * RRP * 4 + size_t(n_v0) * 8;  // ring + view table
     if (tsmem > 160 * 1024) return kNotApplicable;
     int* err = device_error_ptr();
     if (!err) return kNotApplicable;
@@ -354,11 +364,12 @@ int backproject_rsplit(const petl_geom& G, const float* g, float* f, int accumul
         return kNotApplicable;
     }
     const int ntx = int(ceil_div(G.numX, RTX)), nty = int(ceil_div(G.numY, RTY));
-    cudaError_t e = cudaFuncSetAttribute(k_rbp_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem));
+    auto* kxy = pair_y ? k_rbp_xy<true> : k_rbp_xy<false>;
+    cudaError_t e = cudaFuncSetAttribute(kxy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem));
     for (int c = 0; c < nchunks && e == cudaSuccess; c++) {
         const int jv1_0 = c * nc, nvc = std::min(nc, nv1 - jv1_0);
-        const RxyArgs XA{G, vr, jv1_0, lgW, ntx, taps_max, err};
-        k_rbp_xy<<<dim3(unsigned(ntx * nty), ceil_div(G.N_u1, RRB), unsigned(nvc)), RT, tsmem, st>>>(g, P, XA);
+        const RxyArgs XA{G, vr, jv1_0, lgW, ntx, err};
+        kxy<<<dim3(unsigned(ntx * nty), ceil_div(G.N_u1, RRB), unsigned(nvc)), RT2, tsmem, st>>>(g, P, XA);
         note_launch();
         const RzArgs ZA{G, vr, jv1_0, nvc, c == 0 ? accumulate : 1, scale};
         k_rbp_z<<<dim3(ceil_div(G.numX, 32), ceil_div(G.numY, 8), ceil_div(G.numZ, RZB)), dim3(32, 8), 0, st>>>(P, f, ZA);
