@@ -10,14 +10,13 @@
 //   P[v1][u1](x, y) = sum_v0 l_phi(v0, v1) sum_u0 w0(v0, x, y, u0) g[v1][v0][u1][u0],
 // the same sums as the reference associated differently (float rounding).
 //
-// * k_rbp_xy: block = 16 x 16 voxel columns x 16 u1 rows of one slope; per
+// * k_rbp_xy: block = 16 x 16 voxel columns x 32 u1 rows of one slope; per
 //   view the rows' u0 window that the tile's extents reach (bounded on the
-//   host from the corners of the tile) is staged in shared memory, double
-//   buffered through registers (the next view's loads are in flight while
-//   the current one is summed); a thread sums its column's 2-4 u0 taps per
-//   row with the reference's box-overlap weights, the tap count chosen per
-//   view (uniform over the block).
-// * k_rbp_z: thread = voxel column x 16 z rows; per slope the reference's
+//   host from the corners of the tile) arrives by cp.async in a ring of
+//   three views, column-major (a column's rows contiguous, 16-byte reads);
+//   a thread sums two neighbouring voxel columns over the union of their
+//   u0 ranges with the reference's box-overlap weights (l_phi folded in).
+// * k_rbp_z: thread = voxel column x 8 z rows; per slope the reference's
 //   visibility test, u1 box and weights of each row, summed over P.
 // P takes N_u1 x numY x numX floats per slope; slopes run in chunks that
 // fit the scratch budget.
@@ -41,7 +40,7 @@ constexpr int RRB = 32;                            // u1 rows per k_rbp_xy block
 constexpr int RRP = RRB + 4;                       // staged floats per column (rows + 16 bytes of padding)
 constexpr int RWMAX = 128;                         // staged u0 columns per view at most
 constexpr int RSTG = 3;                            // views in flight (cp.async ring)
-constexpr int RZB = 16;                            // z rows per k_rbp_z thread
+constexpr int RZB = 8;                             // z rows per k_rbp_z thread (16: 1.1 ms slower at 256x256x128)
 
 struct RxyArgs {
     petl_geom G;
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(RT2, 4) k_rbp_xy(const float* __restrict__ g, 
 }
 
 // f(x, y, z) (+)= scale T_x sum over the chunk's slopes of the reference's
-// u1 taps of P.  Grid (ceil(numX / 32), ceil(numY / 8), ceil(numZ / 16));
+// u1 taps of P.  Grid (ceil(numX / 32), ceil(numY / 8), ceil(numZ / 8));
 // block (32, 8).
 __global__ void __launch_bounds__(256) k_rbp_z(const float* __restrict__ P, float* __restrict__ f, const RzArgs A)
 {
