@@ -19,8 +19,9 @@
 //   per column u0 evaluates the u0 taps of its ray on plane p once (the
 //   reference's tap range and box overlaps, taps with a positive weight)
 //   and applies them to the 8 rows.
-// * k_gz: CTA = one view x 16 slopes x 32 rows x 32 columns, 16 warps of
-//   2 slopes x 16 rows, one column per lane.  With equal pitch the u1 taps
+// * k_gz: CTA = one view x 16 slopes x 64 rows x 32 columns, 16 warps of
+//   2 slopes x 32 rows, one column per lane (a last block of at most 8
+//   slopes as 8 slopes x 128 rows).  With equal pitch the u1 taps
 //   of row u1 are voxel rows u1 + s and u1 + s + 1 with weights 1 - fr and
 //   fr, where s + fr = (u1_0 - z_0 - t v1) / T_u1 depends on the lane's t
 //   and the slope but not on the row.  The lanes' shifts differ, so each
@@ -53,13 +54,14 @@ namespace {
 
 constexpr int GXZ = 8;        // volume rows per k_gx block
 constexpr int GZS = 16;       // slopes per k_gz CTA (2 per warp), main shape
-constexpr int GZR = 32;       // rows per k_gz CTA (16 per warp), main shape
-constexpr int GZS_T = 4;      // slopes per CTA of the tail shape (a last slope block of at most 8)
+constexpr int GZR = 64;       // rows per k_gz CTA (32 per warp), main shape
+constexpr int GZS_T = 8;      // slopes per CTA of the tail shape (a last slope block of at most 8)
 constexpr int GZR_T = 128;    // rows per CTA of the tail shape
 constexpr int GZC = 32;       // columns per k_gz CTA (one per lane)
 constexpr int GZT = 512;      // threads per k_gz CTA
 constexpr int GJS = 2;        // slopes per warp
-constexpr int GRW = 16;       // rows per warp (GZS / GJS x GZR / GRW = 16 warps; GZS_T / GJS x GZR_T / GRW the same)
+constexpr int GRW = 32;       // rows per warp (GZS / GJS x GZR / GRW = 16 warps; GZS_T / GJS x GZR_T / GRW the same;
+                              // 16 rows per warp: 10 % slower at psi = 30, 256x256x128)
 constexpr int GZRMAX = 224;   // staged rows per plane at most (TMA box rows <= 256)
 constexpr int GZNS = 3;       // ring stages (one plane each) at most
 
@@ -127,8 +129,8 @@ __global__ void __launch_bounds__(256) k_gx(const float* __restrict__ f, const f
 }
 
 
-// NQ slope pairs x (16 / NQ) row groups of 16 per CTA: NQ = 8 is the main
-// shape (16 slopes x 32 rows), NQ = 2 the tail shape (4 slopes x 128 rows)
+// NQ slope pairs x (16 / NQ) row groups of 32 per CTA: NQ = 8 is the main
+// shape (16 slopes x 64 rows), NQ = 4 the tail shape (8 slopes x 128 rows)
 // for a last block of few slopes, which would leave most warps of a
 // 16-slope CTA idle.
 template <int NQ>
@@ -337,7 +339,7 @@ int project_gsplit(const petl_geom& G, const float* f, float* g, const ViewRange
     // a last block of at most 8 slopes runs in the tail shape
     const int rem = nv1 % GZS;
     const int nrows_t = staged_rows(GZS_T, GZR_T);
-    const bool tail = rem > 0 && rem <= 2 * GZS_T && nrows_t <= GZRMAX && G.N_u1 > GZR;
+    const bool tail = rem > 0 && rem <= GZS_T && nrows_t <= GZRMAX && G.N_u1 > GZR;
     const int nv1_main = tail ? nv1 - rem : nv1;
     int* err = device_error_ptr();
     if (!err) return kNotApplicable;

@@ -23,10 +23,10 @@ CASES = {
     # psi = 180 (y-driven, cos = -1) and -45 degrees (ties |r_x| = |r_y| at v0 = 0)
     "p180": ((180.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (64, 48, 16, 2.0)),
     "pm45": ((-45.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (48, 64, 16, 2.0, 2.0, -2.0, 3.0, 1.0)),
-    # 33 and 21 slopes over 64 and 48 u1 rows: the last 1 and 5 slopes run in
-    # the tail shape (4 slopes x 128 rows per CTA)
-    "p30tail1": ((30.0, 128.0, 64.0, 64.0, 1.0, 0.5, 0.25), (64, 64, 64, 1.0)),
-    "p60tail5": ((60.0, 96.0, 48.0, 48.0, 1.0, 0.5, 0.22), (48, 48, 48, 1.0)),
+    # 33 and 21 slopes over 80 and 72 u1 rows: the last 1 and 5 slopes run in
+    # the tail shape (8 slopes x 128 rows per CTA)
+    "p30tail1": ((30.0, 128.0, 64.0, 80.0, 1.0, 0.5, 0.25), (64, 64, 80, 1.0)),
+    "p60tail5": ((60.0, 96.0, 48.0, 72.0, 1.0, 0.5, 0.22), (48, 48, 72, 1.0)),
 }
 
 
