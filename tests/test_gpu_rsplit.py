@@ -2,8 +2,9 @@
 3 in reference mode: an in-plane pass per (v1, u1) slice, then a z pass)
 against the general kernel (dispatch 1) and the FP64 oracle: y- and
 x-dominant views, ragged and off-centre volumes, unequal voxel and u1
-pitch, four-tap extents, view subsets, slope ranges, accumulate, scale and
-FBP.  Voxels wider than three u0 bins keep the general kernel."""
+pitch (psi = 0, 30 and 90), four-tap extents, view subsets, slope ranges,
+accumulate, scale and FBP.  Voxels wider than three u0 bins keep the
+general kernel."""
 import ctypes
 
 import numpy as np
@@ -19,8 +20,11 @@ pytestmark = pytest.mark.gpu
 
 CASES = dict(GCASES)
 CASES.update({
-    # unequal voxel height and u1 pitch
+    # unequal voxel height and u1 pitch (at psi = 0 and 90 too: the shear
+    # kernels need equal pitch, so these take the split kernels)
     "p30pitch": ((30.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (40, 40, 12, 1.5, 1.25)),
+    "p0pitch": ((0.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (44, 40, 12, 1.0, 1.5, 0.5, -1.0, 0.0)),
+    "p90pitch": ((90.0, 128.0, 64.0, 32.0, 2.0, 0.5, 0.25), (40, 44, 12, 1.0, 1.5, -1.0, 0.5, 0.0)),
     # voxels 1.9 bins wide: extents of up to four u0 bins
     "p75wide": ((75.0, 128.0, 64.0, 32.0, 1.0, 0.5, 0.25), (40, 44, 12, 1.9, 1.0, 1.0, -2.0, 0.5)),
 })
