@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(TZT, 1) k_gzT(const __grid_constant__ CUtensor
 #pragma unroll
         for (int k = 0; k < TRW; k++) acc[j][k] = 0.0f;
 
-    bool dead = false;
+    bool dead = false, layout_bad = false;
     int slot = 0;
     uint32_t phase = 0;
     for (int jv1 = 0; jv1 < nv1; jv1++) {
@@ -218,10 +218,11 @@ __global__ void __launch_bounds__(TZT, 1) k_gzT(const __grid_constant__ CUtensor
                 const float sf = floorf(nc);
                 const float fr = nc - sf, w0 = 1.0f - fr;
                 int base = row0 - int(sf) - 1 - wr;  // staged row of h[z - s - 1] for the warp's first row z
-                if (base < 0 || base + TRW + 1 > nrows) {  // outside the staged rows: the host bound failed
-                    atomicOr(A.err, kErrLayout);
-                    base = 0;
-                }
+                // outside the staged rows (the host bound failed): read row 0,
+                // report once after the loop
+                const bool bad = base < 0 || base + TRW + 1 > nrows;
+                layout_bad |= bad;
+                base = bad ? 0 : base;
                 float W[TRW + 1];
 #pragma unroll
                 for (int k = 0; k < TRW + 1; k++) W[k] = B[(base + k) * TZC];
@@ -236,6 +237,7 @@ __global__ void __launch_bounds__(TZT, 1) k_gzT(const __grid_constant__ CUtensor
             phase ^= 1u;
         }
     }
+    if (layout_bad) atomicOr(A.err, kErrLayout);
     if (__syncthreads_or(dead)) {
         // a wait gave up: drain the copies still in flight, write nothing
         if (tid == 0)
