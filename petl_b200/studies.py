@@ -123,14 +123,16 @@ def _peak_hbm_gbs():
         return 6650.0, "fallback"
 
 
-def study_kernels(seed=0, reps=10):
+def study_kernels(seed=0, reps=10, proj_size=256):
     """Device time of the rebinning and regularizer kernels (CUDA events,
     median of `reps`, the L2 flushed before each) with their algorithmic
     bytes and the fraction of the measured HBM bandwidth: PFDR (reads the
     planogram once, writes the rebinned one), the ramp filter (reads and
     writes the rebinned planogram), FBP (PFDR + ramp + the N_v1 = 1
     backprojection), and the RD / TV gradients (read the volume, write the
-    gradient) at 128x128x64 and 256x256x128."""
+    gradient) at 128x128x64 and 256x256x128; then the projectors by
+    orientation on a proj_size^2 x proj_size/2 volume at 1 mm (256 by
+    default; 128 gives a small case for kernel captures)."""
     peak, kind = _peak_hbm_gbs()
     flush = torch.empty(64 * 1024 * 1024, device="cuda")
 
@@ -180,8 +182,9 @@ def study_kernels(seed=0, reps=10):
     # 1965 MHz)
     fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
     from . import lib
+    n = int(proj_size)
     for psi in (0.0, 90.0, 30.0):
-        G = Geometry(psi, 256.0, 128.0, 128.0, 1.0, 0.5, 0.25, volume=(256, 256, 128, 1.0))
+        G = Geometry(psi, float(n), n / 2.0, n / 2.0, 1.0, 0.5, 0.25, volume=(n, n, n // 2, 1.0))
         f = phantom(G.vol_shape, (1.0, 1.0), np.random.default_rng(seed), 12) + 0.01
         g = torch.empty(G.shape, device="cuda")
         b = torch.empty_like(f)
@@ -579,6 +582,7 @@ def main(argv=None):
     ap.add_argument("--sizes", default="64,128,192,256", help="serving: volume sizes N drawn")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--reps", type=int, default=0, help="kernels: timed calls per figure (0: the study's default)")
+    ap.add_argument("--proj-size", type=int, default=256, help="kernels: volume N x N x N/2 of the projector timings")
     a = ap.parse_args(argv)
     fn = {"pipeline": study_pipeline, "penalized": study_penalized, "storage": study_storage,
           "binning": study_binning, "corrections": study_corrections, "response": study_response,
@@ -586,8 +590,8 @@ def main(argv=None):
     if a.study == "serving":
         res = study_serving(n=a.requests, seed=a.seed, rate=a.rate,
                             sizes=tuple(int(v) for v in a.sizes.split(",")))
-    elif a.study == "kernels" and a.reps > 0:
-        res = study_kernels(seed=a.seed, reps=a.reps)
+    elif a.study == "kernels":
+        res = study_kernels(seed=a.seed, reps=a.reps if a.reps > 0 else 10, proj_size=a.proj_size)
     else:
         res = fn[a.study](seed=a.seed)
     print(json.dumps(res))
